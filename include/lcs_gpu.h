@@ -1,0 +1,246 @@
+/*
+ * lcs_gpu.h -- C ABI of the B200 (sm_100a) contact-and-solve path of LuisaComputeSimulator.
+ *
+ * The entry points replace the LuisaCompute shaders behind the reference's LBVH,
+ * NarrowPhasesDetector and ConjugateGradientSolver classes (citations per function, paths
+ * relative to the reference project).  All pointers are DEVICE pointers unless a parameter
+ * says "host"; every call is stream-ordered on the caller's cudaStream_t (NULL = legacy
+ * default stream) and returns an lcs_status.  Handles are not thread-safe.
+ *
+ * Data layouts (identical to LuisaCompute's buffers, so an LC-hosted caller can pass
+ * Buffer<T>::native_handle() pointers):
+ *   positions   float4 per vertex (x, y, z, pad)                       = Buffer<float3>
+ *   faces       uint4  per face   (v0, v1, v2, pad)                     = Buffer<uint3>
+ *   edges       uint2  per edge                                         = Buffer<uint2>
+ *   diag blocks 3 float4 columns per vertex (48 B)                      = Buffer<float3x3>
+ *   BSR blocks  9 floats per block, column-major                        (MatrixTriplet3x3 order)
+ *   pairs       lcs_pair, 48 B                                          = CollisionPairTemplate
+ *   per-vertex scalars (d_hat, offset, areas) float; body ids uint32 (0xFFFFFFFF = soft)
+ */
+#ifndef LCS_GPU_H
+#define LCS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LCS_API __attribute__((visibility("default")))
+#else
+#define LCS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* lcs_stream; /* = cudaStream_t */
+
+typedef enum lcs_status {
+    LCS_OK = 0,
+    LCS_ERR_INVALID = 1,        /* bad argument (null handle, size mismatch, ...) */
+    LCS_ERR_CUDA = 2,           /* a CUDA runtime call failed */
+    LCS_ERR_CAPACITY = 3,       /* an output did not fit; the required size was reported */
+    LCS_ERR_UNHEALTHY_BVH = 4,  /* parent/child links inconsistent (fn_check_construction) */
+    LCS_ERR_NAN = 5,            /* NaN / Inf met (PCG rz, barrier stiffness) */
+    LCS_ERR_CCD_NOCONVERGE = 6, /* an ACCD pair hit the 10000-iteration cap (toi 0.001) */
+    LCS_ERR_TIMEOUT = 7,        /* a bounded device-side wait gave up */
+    LCS_ERR_NO_DEVICE = 8       /* no CUDA device / not an sm_100 device */
+} lcs_status;
+
+enum { LCS_TREE_VERT = 0, LCS_TREE_EDGE = 1, LCS_TREE_FACE = 2 };
+
+/* flags for the CCD entry points */
+enum { LCS_CCD_FP64_FINAL = 1 };
+
+/* CollisionPairTemplate (Solver/SimulationCore/collision_data.h:48-126): indices with the
+ * pair type in bit 31 (VF: idx[2], EE: idx[3]); vec1 = (normal, kappa * area);
+ * vec2 = (k1, k2, bary0, bary1). */
+typedef struct lcs_pair {
+    uint32_t idx[4];
+    float vec1[4];
+    float vec2[4];
+} lcs_pair;
+
+/* 3x3-block CSR matrix (device arrays). */
+typedef struct lcs_bsr {
+    uint32_t n_rows;
+    const uint32_t* row_ptr; /* n_rows + 1 */
+    const uint32_t* col;     /* nnzb */
+    const float* val;        /* 9 * nnzb, column-major blocks */
+} lcs_bsr;
+
+/* ------------------------------------------------------------------------------------------
+ * Library / device
+ * ------------------------------------------------------------------------------------------ */
+/* Version string of the library ("lcs_b200 <ver> sm_100a"). Host pointer, static storage. */
+LCS_API const char* lcs_version(void);
+/* Checks that device `device` is usable (sm_100 family). */
+LCS_API int lcs_device_check(int device);
+/* Text of the last error recorded on this thread (host pointer, static storage). */
+LCS_API const char* lcs_last_error(void);
+
+/* ------------------------------------------------------------------------------------------
+ * LBVH  (replaces class LBVH, Solver/CollisionDetector/lbvh.h:166-229)
+ * ------------------------------------------------------------------------------------------ */
+typedef struct lcs_bvh lcs_bvh;
+
+/* LbvhData::allocate (lbvh.h:95-139): a tree over n_leaves vertices, edges or faces. */
+LCS_API int lcs_bvh_create(int kind, uint32_t n_leaves, lcs_bvh** out);
+LCS_API int lcs_bvh_destroy(lcs_bvh* h);
+
+/* LBVH::reduce_{vert,edge,face}_tree_aabb (lbvh.cpp:939-973): leaf centres and the global
+ * AABB used to normalise Morton codes.  The second pass of the reference covers the first
+ * ceil(n_verts / 256) block partials for every tree kind; that is reproduced.
+ * elems: NULL (vert tree), uint2 edges (edge tree) or uint4 faces (face tree). */
+LCS_API int lcs_bvh_reduce_aabb(lcs_bvh* h, const float* x, const uint32_t* elems, uint32_t n_verts,
+                        lcs_stream stream);
+
+/* LBVH::construct_tree (lbvh.cpp:974-998): Morton codes, a device radix sort (the reference
+ * sorts on the host), Karras inner nodes, health check.  The health flag stays on the
+ * device; read it with lcs_bvh_health. */
+LCS_API int lcs_bvh_construct(lcs_bvh* h, lcs_stream stream);
+
+/* LBVH::update_{vert,edge,face}_tree_leave_aabb (lbvh.cpp:1001-1031): swept leaf boxes
+ * [x0, x1] +- thickness of the element's first vertex. */
+LCS_API int lcs_bvh_update_leaves(lcs_bvh* h, const float* thickness, const float* x0, const float* x1,
+                          const uint32_t* elems, lcs_stream stream);
+
+/* LBVH::refit (lbvh.cpp:1038-1045): bottom-up union of the inner boxes. */
+LCS_API int lcs_bvh_refit(lcs_bvh* h, lcs_stream stream);
+
+/* update_*_tree_leave_aabb + refit in one launch (no reference counterpart as one call). */
+LCS_API int lcs_bvh_update_refit(lcs_bvh* h, const float* thickness, const float* x0, const float* x1,
+                         const uint32_t* elems, lcs_stream stream);
+
+/* LBVH::broad_phase_query_from_verts (lbvh.cpp:1146-1167): every vertex box [x0,x1] +-
+ * (thickness + d_hat) against a FACE tree; appends (vid, fid) to pairs (uint2) and adds the
+ * number found to *d_count (device; the caller resets it).  Pairs beyond `capacity` are
+ * counted but not written (the reference writes one pair past the end, lbvh.cpp:329-334). */
+LCS_API int lcs_bvh_query_vf(const lcs_bvh* face_tree, const float* x0, const float* x1, uint32_t n_verts,
+                     const float* d_hat, const float* thickness, uint32_t* pairs, uint32_t capacity,
+                     uint32_t* d_count, lcs_stream stream);
+
+/* LBVH::broad_phase_query_from_edges (lbvh.cpp:1168-1192): every edge's swept box +-
+ * (thickness + d_hat of its first vertex) against an EDGE tree; keeps eid < adj_eid. */
+LCS_API int lcs_bvh_query_ee(const lcs_bvh* edge_tree, const float* x0, const float* x1,
+                     const uint32_t* edges, uint32_t n_edges, const float* d_hat,
+                     const float* thickness, uint32_t* pairs, uint32_t capacity, uint32_t* d_count,
+                     lcs_stream stream);
+
+/* LBVH::check_health (lbvh.cpp:1033-1036).  Synchronises `stream`. host out. */
+LCS_API int lcs_bvh_health(lcs_bvh* h, int* healthy, lcs_stream stream);
+
+/* Copies the tree out in the reference's LbvhData layout (lbvh.h:79-152), for tests and
+ * interop; any pointer may be NULL.  node_aabb: 8 floats per node {min.xyz, 0, max.xyz, 0};
+ * children: uint2 per node (leaves: (elem, elem)); parent[0] = 0xFFFFFFFF. */
+LCS_API int lcs_bvh_export(const lcs_bvh* h, uint32_t* parent, uint32_t* children, uint32_t* object_idx,
+                   uint64_t* morton, uint64_t* morton_sorted, uint32_t* sorted_get_original,
+                   float* node_aabb, float* global_aabb6, lcs_stream stream);
+LCS_API uint32_t lcs_bvh_num_leaves(const lcs_bvh* h);
+
+/* ------------------------------------------------------------------------------------------
+ * Narrow phase  (replaces NarrowPhasesDetector, Solver/CollisionDetector/narrow_phase.h:54-201)
+ * Pair lists are the broad phase's uint2 lists; *d_count (device) holds how many are valid and
+ * at most `capacity` of them are read.
+ * ------------------------------------------------------------------------------------------ */
+
+/* NarrowPhasesDetector::vf_ccd_query (narrow_phase.cpp:293-436, 609-676): ACCD on every
+ * (vid, fid) candidate; d_toi[0] becomes min(d_toi[0], toi / 1.25) (the caller initialises it
+ * to 1.0, as fn_reset_toi does).  toi_per_pair (optional) receives each pair's toi. */
+LCS_API int lcs_ccd_vf(const uint32_t* pairs, const uint32_t* d_count, uint32_t capacity, const float* x0,
+               const float* x1, const uint32_t* faces, const uint32_t* body, const float* offset,
+               float* d_toi, float* toi_per_pair, int flags, lcs_stream stream);
+
+/* NarrowPhasesDetector::ee_ccd_query (narrow_phase.cpp:438-593, 678-740). */
+LCS_API int lcs_ccd_ee(const uint32_t* pairs, const uint32_t* d_count, uint32_t capacity, const float* x0,
+               const float* x1, const uint32_t* edges, const uint32_t* body, const float* offset,
+               float* d_toi, float* toi_per_pair, int flags, lcs_stream stream);
+
+/* NarrowPhasesDetector::vf_dcd_query_repulsion (narrow_phase.cpp:771-933, 1102-1170): barrier
+ * contact pairs with d^2 < (offset + d_hat)^2; appended to out, count added to *d_out_count. */
+LCS_API int lcs_dcd_vf(const uint32_t* pairs, const uint32_t* d_count, uint32_t capacity, const float* x,
+               const uint32_t* faces, const uint32_t* body, const float* vert_area,
+               const float* face_area, const float* d_hat, const float* offset, float kappa,
+               lcs_pair* out, uint32_t out_capacity, uint32_t* d_out_count, lcs_stream stream);
+
+/* NarrowPhasesDetector::ee_dcd_query_repulsion (narrow_phase.cpp:935-1098, 1171-1249). */
+LCS_API int lcs_dcd_ee(const uint32_t* pairs, const uint32_t* d_count, uint32_t capacity, const float* x,
+               const uint32_t* edges, const uint32_t* body, const float* edge_area,
+               const float* d_hat, const float* offset, float kappa, lcs_pair* out,
+               uint32_t out_capacity, uint32_t* d_out_count, lcs_stream stream);
+
+/* NarrowPhasesDetector::device_perPair_evaluate_gradient_hessian (narrow_phase.cpp:2550-2676,
+ * 2817-2843): b[v] += k1 w_v n and diag[v] += k2 w_v^2 n n^T for every pair (soft vertices). */
+LCS_API int lcs_contact_grad_diag(const lcs_pair* pairs, const uint32_t* d_count, uint32_t capacity,
+                          float* b, float* diag, lcs_stream stream);
+
+/* NarrowPhasesDetector::compute_contact_energy_from_iter_start_list + download_energy
+ * (narrow_phase.cpp:2968-3070, 123-130): sum of kappa * area * barrier over the pairs at
+ * positions x, accumulated in FP64 into *d_energy (device double, caller resets). */
+LCS_API int lcs_contact_energy(const lcs_pair* pairs, const uint32_t* d_count, uint32_t capacity,
+                       const float* x, const float* d_hat, const float* offset, double* d_energy,
+                       lcs_stream stream);
+
+/* Contact off-diagonal blocks: the per-vertex adjacency + two-level triplet sort + assembly
+ * (prescan_pervert_adj_list, construct_pervert_adj_list, device_sort_contact_triplet,
+ * device_assemble_contact_triplet; narrow_phase.cpp:1264-1426, 1434-2362) as one device radix
+ * sort of (row, col) keys and a segmented sum.  The assembler owns the output BSR. */
+typedef struct lcs_assembler lcs_assembler;
+LCS_API int lcs_assembler_create(uint32_t n_rows, uint32_t pair_capacity, lcs_assembler** out);
+LCS_API int lcs_assembler_destroy(lcs_assembler* a);
+LCS_API int lcs_contact_offdiag_bsr(lcs_assembler* a, const lcs_pair* pairs, const uint32_t* d_count,
+                            uint32_t capacity, lcs_stream stream);
+/* Device pointers of the assembled BSR; *d_nnzb is a device uint32. */
+LCS_API int lcs_assembler_bsr(const lcs_assembler* a, lcs_bsr* out, const uint32_t** d_nnzb);
+/* NarrowPhasesDetector::download_contact_triplet (narrow_phase.cpp:207-233): copies the BSR
+ * into caller device buffers (at most max_blocks blocks) and returns the block count in
+ * *nnzb (host).  Synchronises `stream`. */
+LCS_API int lcs_assembler_export(const lcs_assembler* a, uint32_t* row_ptr, uint32_t* col, float* val,
+                                 uint32_t max_blocks, uint32_t* nnzb, lcs_stream stream);
+
+/* ------------------------------------------------------------------------------------------
+ * SpMV + Jacobi PCG  (replaces ConjugateGradientSolver, Solver/LinearSolver/precond_cg.h:17-71,
+ * and NewtonSolver::device_SpMV, Solver/SimulationSolver/newton_solver.cpp:3397-3427)
+ * ------------------------------------------------------------------------------------------ */
+
+/* y = D x + A x + B x (A, B may be NULL): fn_pcg_spmv_diag + fn_pcg_spmv_offdiag_block_rbk on the
+ * material and the contact triplets (newton_solver.cpp:259-270, 347-472). */
+LCS_API int lcs_spmv(uint32_t n, const float* diag, const lcs_bsr* A, const lcs_bsr* B, const float* x,
+             float* y, lcs_stream stream);
+
+enum {
+    LCS_PCG_FP64_DOTS = 1, /* precision form: FP64 dot products and residual reductions */
+    LCS_PCG_PLAIN = 2,     /* reference dispatch structure: one kernel per op, host check */
+    LCS_PCG_NO_STATS = 4   /* fused path: do not synchronise to fill *stats */
+};
+
+typedef struct lcs_pcg_opts {
+    int32_t max_iter;    /* pcg_iter_count (reference default 100) */
+    float rel_tol;       /* stop when ||r|| <= rel_tol * ||r0|| (<= 0: off) */
+    float abs_rz_tol;    /* stop when r.z < abs_rz_tol (reference: 1e-10) */
+    int32_t check_every; /* reference: 25 */
+    int32_t flags;
+} lcs_pcg_opts;
+
+typedef struct lcs_pcg_stats {
+    int32_t iterations;
+    float rel_residual; /* ||r|| / ||r0|| at the last check */
+    float dot_rz;
+    int32_t status;     /* lcs_status of the solve (NaN -> LCS_ERR_NAN) */
+} lcs_pcg_stats;
+
+typedef struct lcs_pcg lcs_pcg;
+LCS_API int lcs_pcg_create(uint32_t n, lcs_pcg** out);
+LCS_API int lcs_pcg_destroy(lcs_pcg* p);
+/* ConjugateGradientSolver::device_solve (precond_cg.cpp:626-771): x = A^-1 b with x0 = 0.
+ * stats (host, may be NULL) is filled after the solve (synchronises the stream unless
+ * LCS_PCG_NO_STATS).  Device copy of the stats: lcs_pcg_device_stats. */
+LCS_API int lcs_pcg_solve(lcs_pcg* p, const float* diag, const lcs_bsr* A, const lcs_bsr* B,
+                  const float* b, float* x, const lcs_pcg_opts* opts, lcs_pcg_stats* stats,
+                  lcs_stream stream);
+LCS_API const lcs_pcg_stats* lcs_pcg_device_stats(const lcs_pcg* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LCS_GPU_H */

@@ -1,0 +1,104 @@
+"""ctypes binding of liblcs_b200.so (the C ABI declared in include/lcs_gpu.h).
+
+Loading the library needs no GPU; calling its compute entry points does.  There is no CPU
+fallback: if the library is missing the import of this module fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblcs_b200.so")
+
+P = C.c_void_p
+U32 = C.c_uint32
+I32 = C.c_int
+F32 = C.c_float
+
+
+class LcsError(RuntimeError):
+    pass
+
+
+STATUS = {0: "LCS_OK", 1: "LCS_ERR_INVALID", 2: "LCS_ERR_CUDA", 3: "LCS_ERR_CAPACITY", 4: "LCS_ERR_UNHEALTHY_BVH",
+          5: "LCS_ERR_NAN", 6: "LCS_ERR_CCD_NOCONVERGE", 7: "LCS_ERR_TIMEOUT", 8: "LCS_ERR_NO_DEVICE"}
+LCS_TREE_VERT, LCS_TREE_EDGE, LCS_TREE_FACE = 0, 1, 2
+LCS_CCD_FP64_FINAL = 1
+LCS_PCG_FP64_DOTS, LCS_PCG_PLAIN, LCS_PCG_NO_STATS = 1, 2, 4
+
+
+class Bsr(C.Structure):
+    _fields_ = [("n_rows", C.c_uint32), ("row_ptr", P), ("col", P), ("val", P)]
+
+
+class PcgOpts(C.Structure):
+    _fields_ = [("max_iter", C.c_int32), ("rel_tol", C.c_float), ("abs_rz_tol", C.c_float),
+                ("check_every", C.c_int32), ("flags", C.c_int32)]
+
+
+class PcgStats(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("rel_residual", C.c_float), ("dot_rz", C.c_float),
+                ("status", C.c_int32)]
+
+
+# name -> (restype, argtypes); must list every function of include/lcs_gpu.h
+SIGNATURES = {
+    "lcs_version": (C.c_char_p, []),
+    "lcs_device_check": (I32, [I32]),
+    "lcs_last_error": (C.c_char_p, []),
+    "lcs_bvh_create": (I32, [I32, U32, C.POINTER(P)]),
+    "lcs_bvh_destroy": (I32, [P]),
+    "lcs_bvh_reduce_aabb": (I32, [P, P, P, U32, P]),
+    "lcs_bvh_construct": (I32, [P, P]),
+    "lcs_bvh_update_leaves": (I32, [P, P, P, P, P, P]),
+    "lcs_bvh_refit": (I32, [P, P]),
+    "lcs_bvh_update_refit": (I32, [P, P, P, P, P, P]),
+    "lcs_bvh_query_vf": (I32, [P, P, P, U32, P, P, P, U32, P, P]),
+    "lcs_bvh_query_ee": (I32, [P, P, P, P, U32, P, P, P, U32, P, P]),
+    "lcs_bvh_health": (I32, [P, C.POINTER(C.c_int), P]),
+    "lcs_bvh_export": (I32, [P, P, P, P, P, P, P, P, P, P]),
+    "lcs_bvh_num_leaves": (U32, [P]),
+    "lcs_ccd_vf": (I32, [P, P, U32, P, P, P, P, P, P, P, I32, P]),
+    "lcs_ccd_ee": (I32, [P, P, U32, P, P, P, P, P, P, P, I32, P]),
+    "lcs_dcd_vf": (I32, [P, P, U32, P, P, P, P, P, P, P, F32, P, U32, P, P]),
+    "lcs_dcd_ee": (I32, [P, P, U32, P, P, P, P, P, P, F32, P, U32, P, P]),
+    "lcs_contact_grad_diag": (I32, [P, P, U32, P, P, P]),
+    "lcs_contact_energy": (I32, [P, P, U32, P, P, P, P, P]),
+    "lcs_assembler_create": (I32, [U32, U32, C.POINTER(P)]),
+    "lcs_assembler_destroy": (I32, [P]),
+    "lcs_contact_offdiag_bsr": (I32, [P, P, P, U32, P]),
+    "lcs_assembler_bsr": (I32, [P, C.POINTER(Bsr), C.POINTER(P)]),
+    "lcs_assembler_export": (I32, [P, P, P, P, U32, C.POINTER(C.c_uint32), P]),
+    "lcs_spmv": (I32, [U32, P, C.POINTER(Bsr), C.POINTER(Bsr), P, P, P]),
+    "lcs_pcg_create": (I32, [U32, C.POINTER(P)]),
+    "lcs_pcg_destroy": (I32, [P]),
+    "lcs_pcg_solve": (I32, [P, P, C.POINTER(Bsr), C.POINTER(Bsr), P, P, C.POINTER(PcgOpts), C.POINTER(PcgStats), P]),
+    "lcs_pcg_device_stats": (P, [P]),
+}
+
+_lib = None
+
+
+def load():
+    """Loads liblcs_b200.so (building it first when the sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build as _build
+        _build.build()
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(code, what=""):
+    if code != 0:
+        msg = load().lcs_last_error().decode(errors="replace")
+        raise LcsError(f"{what}: {STATUS.get(code, code)} {msg}")
+    return code

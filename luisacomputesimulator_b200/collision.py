@@ -1,0 +1,244 @@
+"""Host-side mirror of the reference's collision-detector interface over the C ABI.
+
+``LBVH`` keeps the method names of class LBVH (Solver/CollisionDetector/lbvh.h:166-229) and
+``NarrowPhasesDetector`` those of class NarrowPhasesDetector
+(Solver/CollisionDetector/narrow_phase.h:54-201), so code written against the reference
+reads the same.  All tensors are CUDA tensors; the work runs on torch's current stream.
+Errors raise ``LcsError`` with the library's status; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import _capi as A
+
+PAIR_BYTES = 48
+
+
+def ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _dev(t, dtype):
+    assert t.is_cuda and t.dtype == dtype and t.is_contiguous(), f"expected contiguous CUDA {dtype}"
+    return t
+
+
+class LBVH:
+    """One LBVH over vertices, edges or faces (LbvhData + LBVH, lbvh.h:79-229)."""
+
+    def __init__(self, kind: int, n_leaves: int):
+        self.lib = A.load()
+        self.kind, self.n = kind, int(n_leaves)
+        h = C.c_void_p()
+        A.check(self.lib.lcs_bvh_create(kind, self.n, C.byref(h)), "lcs_bvh_create")
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.lcs_bvh_destroy(self.h)
+            self.h = None
+
+    # -- construct (lbvh.cpp:939-998)
+    def reduce_vert_tree_aabb(self, x):
+        A.check(self.lib.lcs_bvh_reduce_aabb(self.h, ptr(x), None, x.shape[0], stream()), "reduce_aabb")
+
+    def reduce_edge_tree_aabb(self, x, edges):
+        A.check(self.lib.lcs_bvh_reduce_aabb(self.h, ptr(x), ptr(edges), x.shape[0], stream()), "reduce_aabb")
+
+    def reduce_face_tree_aabb(self, x, faces):
+        A.check(self.lib.lcs_bvh_reduce_aabb(self.h, ptr(x), ptr(faces), x.shape[0], stream()), "reduce_aabb")
+
+    def construct_tree(self):
+        A.check(self.lib.lcs_bvh_construct(self.h, stream()), "construct_tree")
+
+    # -- refit (lbvh.cpp:1001-1045)
+    def update_leaves(self, thickness, x0, x1, elems=None):
+        A.check(self.lib.lcs_bvh_update_leaves(self.h, ptr(thickness), ptr(x0), ptr(x1), ptr(elems), stream()),
+                "update_leaves")
+
+    update_vert_tree_leave_aabb = update_leaves
+
+    def update_edge_tree_leave_aabb(self, thickness, x0, x1, edges):
+        self.update_leaves(thickness, x0, x1, edges)
+
+    def update_face_tree_leave_aabb(self, thickness, x0, x1, faces):
+        self.update_leaves(thickness, x0, x1, faces)
+
+    def refit(self):
+        A.check(self.lib.lcs_bvh_refit(self.h, stream()), "refit")
+
+    def update_and_refit(self, thickness, x0, x1, elems=None):
+        A.check(self.lib.lcs_bvh_update_refit(self.h, ptr(thickness), ptr(x0), ptr(x1), ptr(elems), stream()),
+                "update_refit")
+
+    def check_health(self) -> bool:
+        ok = C.c_int(0)
+        A.check(self.lib.lcs_bvh_health(self.h, C.byref(ok), stream()), "check_health")
+        return bool(ok.value)
+
+    # -- queries (lbvh.cpp:1146-1192)
+    def broad_phase_query_from_verts(self, x0, x1, count, pairs, d_hat, thickness):
+        """Appends (vid, fid) pairs; `count` is a 1-element uint32 CUDA tensor (not reset here)."""
+        A.check(self.lib.lcs_bvh_query_vf(self.h, ptr(x0), ptr(x1), x0.shape[0], ptr(d_hat), ptr(thickness),
+                                          ptr(pairs), pairs.shape[0], ptr(count), stream()), "query_vf")
+
+    def broad_phase_query_from_edges(self, x0, x1, edges, count, pairs, d_hat, thickness):
+        A.check(self.lib.lcs_bvh_query_ee(self.h, ptr(x0), ptr(x1), ptr(edges), edges.shape[0], ptr(d_hat),
+                                          ptr(thickness), ptr(pairs), pairs.shape[0], ptr(count), stream()),
+                "query_ee")
+
+    def export(self):
+        """The tree in the reference's LbvhData layout (CUDA tensors)."""
+        n = self.n
+        nn = max(2 * n - 1, 1)
+        dev = "cuda"
+        out = dict(parent=torch.empty(nn, dtype=torch.int32, device=dev),
+                   children=torch.empty((nn, 2), dtype=torch.int32, device=dev),
+                   object_idx=torch.empty(nn, dtype=torch.int32, device=dev),
+                   morton=torch.empty(max(n, 1), dtype=torch.int64, device=dev),
+                   morton_sorted=torch.empty(max(n, 1), dtype=torch.int64, device=dev),
+                   sorted_get_original=torch.empty(max(n, 1), dtype=torch.int32, device=dev),
+                   node_aabb=torch.empty((nn, 8), dtype=torch.float32, device=dev),
+                   global_aabb=torch.empty(6, dtype=torch.float32, device=dev))
+        A.check(self.lib.lcs_bvh_export(self.h, ptr(out["parent"]), ptr(out["children"]), ptr(out["object_idx"]),
+                                        ptr(out["morton"]), ptr(out["morton_sorted"]),
+                                        ptr(out["sorted_get_original"]), ptr(out["node_aabb"]),
+                                        ptr(out["global_aabb"]), stream()), "export")
+        return out
+
+
+class NarrowPhasesDetector:
+    """CollisionData buffers + the narrow-phase entry points (narrow_phase.h:54-201).
+
+    Capacities follow CollisionData::resize_collision_data_list (collision_data.h:445-485):
+    4 x verts / 4 x edges broad-phase pairs, 2 x (verts + edges) contact pairs; they grow
+    by doubling when a count comes back above capacity (NarrowPhasesDetector::resize_buffers).
+    """
+
+    def __init__(self, num_verts, num_edges, device="cuda"):
+        self.lib = A.load()
+        self.nv, self.ne = int(num_verts), int(num_edges)
+        self.device = device
+        self.cap_vf = max(4 * self.nv, 1024)
+        self.cap_ee = max(4 * self.ne, 1024)
+        self.cap_pairs = max(2 * (self.nv + self.ne), 1024)
+        # counts: 0 vf broad, 1 ee broad, 2 narrow pairs, 3 spare
+        self.counts = torch.zeros(4, dtype=torch.int32, device=device)
+        self.toi = torch.ones(1, dtype=torch.float32, device=device)
+        self.energy = torch.zeros(1, dtype=torch.float64, device=device)
+        self._alloc()
+        self.assembler = None
+
+    def _alloc(self):
+        self.broad_phase_list_vf = torch.zeros((self.cap_vf, 2), dtype=torch.int32, device=self.device)
+        self.broad_phase_list_ee = torch.zeros((self.cap_ee, 2), dtype=torch.int32, device=self.device)
+        self.narrow_phase_list = torch.zeros((self.cap_pairs, 12), dtype=torch.int32, device=self.device)
+
+    def count_view(self, k):
+        return self.counts[k:k + 1]
+
+    def reset_broadphase_count(self):
+        self.counts[0:2].zero_()
+
+    def reset_narrowphase_count(self):
+        self.counts[2:3].zero_()
+
+    def reset_toi(self):
+        self.toi.fill_(1.0)
+
+    def reset_energy(self):
+        self.energy.zero_()
+
+    def download_counts(self):
+        return [int(v) for v in self.counts.cpu()]
+
+    def resize_buffers(self):
+        """Doubles whatever overflowed (NarrowPhasesDetector::resize_buffers, narrow_phase.cpp:61-95)."""
+        c = self.download_counts()
+        grew = False
+        while c[0] > self.cap_vf:
+            self.cap_vf *= 2; grew = True
+        while c[1] > self.cap_ee:
+            self.cap_ee *= 2; grew = True
+        while c[2] > self.cap_pairs:
+            self.cap_pairs *= 2; grew = True
+            self.assembler = None
+        if grew:
+            self._alloc()
+        return grew
+
+    # -- CCD (narrow_phase.cpp:293-740)
+    def vf_ccd_query(self, x0, x1, faces, body, offset, toi_per_pair=None, fp64_final=False):
+        A.check(self.lib.lcs_ccd_vf(ptr(self.broad_phase_list_vf), ptr(self.count_view(0)), self.cap_vf, ptr(x0),
+                                    ptr(x1), ptr(faces), ptr(body), ptr(offset), ptr(self.toi), ptr(toi_per_pair),
+                                    int(bool(fp64_final)), stream()), "ccd_vf")
+
+    def ee_ccd_query(self, x0, x1, edges, body, offset, toi_per_pair=None, fp64_final=False):
+        A.check(self.lib.lcs_ccd_ee(ptr(self.broad_phase_list_ee), ptr(self.count_view(1)), self.cap_ee, ptr(x0),
+                                    ptr(x1), ptr(edges), ptr(body), ptr(offset), ptr(self.toi), ptr(toi_per_pair),
+                                    int(bool(fp64_final)), stream()), "ccd_ee")
+
+    # -- DCD (narrow_phase.cpp:771-1249)
+    def vf_dcd_query_repulsion(self, x, faces, body, vert_area, face_area, d_hat, offset, kappa):
+        A.check(self.lib.lcs_dcd_vf(ptr(self.broad_phase_list_vf), ptr(self.count_view(0)), self.cap_vf, ptr(x),
+                                    ptr(faces), ptr(body), ptr(vert_area), ptr(face_area), ptr(d_hat), ptr(offset),
+                                    float(kappa), ptr(self.narrow_phase_list), self.cap_pairs,
+                                    ptr(self.count_view(2)), stream()), "dcd_vf")
+
+    def ee_dcd_query_repulsion(self, x, edges, body, edge_area, d_hat, offset, kappa):
+        A.check(self.lib.lcs_dcd_ee(ptr(self.broad_phase_list_ee), ptr(self.count_view(1)), self.cap_ee, ptr(x),
+                                    ptr(edges), ptr(body), ptr(edge_area), ptr(d_hat), ptr(offset), float(kappa),
+                                    ptr(self.narrow_phase_list), self.cap_pairs, ptr(self.count_view(2)), stream()),
+                "dcd_ee")
+
+    # -- assembly (narrow_phase.cpp:1264-2362, 2550-2843)
+    def device_perPair_evaluate_gradient_hessian(self, b, diag):
+        A.check(self.lib.lcs_contact_grad_diag(ptr(self.narrow_phase_list), ptr(self.count_view(2)), self.cap_pairs,
+                                               ptr(b), ptr(diag), stream()), "grad_diag")
+
+    def device_assemble_contact_triplet(self):
+        """Off-diagonal contact blocks as BSR; returns (lcs_bsr struct, nnzb device pointer)."""
+        if self.assembler is None:
+            h = C.c_void_p()
+            A.check(self.lib.lcs_assembler_create(self.nv, self.cap_pairs, C.byref(h)), "assembler_create")
+            self.assembler = _Assembler(self.lib, h)
+        A.check(self.lib.lcs_contact_offdiag_bsr(self.assembler.h, ptr(self.narrow_phase_list),
+                                                 ptr(self.count_view(2)), self.cap_pairs, stream()), "offdiag_bsr")
+        return self.assembler.bsr()
+
+    def compute_contact_energy(self, x, d_hat, offset):
+        A.check(self.lib.lcs_contact_energy(ptr(self.narrow_phase_list), ptr(self.count_view(2)), self.cap_pairs,
+                                            ptr(x), ptr(d_hat), ptr(offset), ptr(self.energy), stream()), "energy")
+
+
+class _Assembler:
+    def __init__(self, lib, h):
+        self.lib, self.h = lib, h
+
+    def bsr(self):
+        m = A.Bsr()
+        nnzb = C.c_void_p()
+        A.check(self.lib.lcs_assembler_bsr(self.h, C.byref(m), C.byref(nnzb)), "assembler_bsr")
+        return m, nnzb.value
+
+    def export(self, n_rows, max_blocks):
+        """(row_ptr, col, val) CUDA tensors of the assembled off-diagonal BSR."""
+        rp = torch.empty(n_rows + 1, dtype=torch.int32, device="cuda")
+        col = torch.empty(max(max_blocks, 1), dtype=torch.int32, device="cuda")
+        val = torch.empty((max(max_blocks, 1), 9), dtype=torch.float32, device="cuda")
+        nb = C.c_uint32(0)
+        A.check(self.lib.lcs_assembler_export(self.h, ptr(rp), ptr(col), ptr(val), max_blocks, C.byref(nb), stream()),
+                "assembler_export")
+        return rp, col[: nb.value], val[: nb.value]
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.lcs_assembler_destroy(self.h)
+            self.h = None

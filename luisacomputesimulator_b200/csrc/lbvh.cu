@@ -1,0 +1,618 @@
+// lbvh.cu -- LBVH over vertices, edges or faces: build, refit and broad-phase traversal.
+//
+// Follows Solver/CollisionDetector/lbvh.cpp of the reference (citations per kernel) with a
+// B200 layout for traversal: every inner node is one 64-byte record holding the boxes of
+// both children, {min.xyz | child code}, {max.xyz}, {min.xyz | child code}, {max.xyz}, where
+// a child code is the inner node index, or 0x80000000 | element id for a leaf.  One
+// traversal step is therefore one 64-byte load instead of the reference's three dependent
+// loads (children, child AABB, object_idx).  The reference's LbvhData layout is produced on
+// demand by lcs_bvh_export for tests and interop.
+#include <cuda_runtime.h>
+
+#include <new>
+
+#include "lcs_common.cuh"
+#include "lcs_internal.h"
+#include "radix_sort.cuh"
+
+using namespace lcs;
+
+struct lcs_bvh {
+    int kind = 0;
+    uint32_t n = 0, ni = 0, nb = 0;  // leaves, inner nodes, 256-element blocks
+    float4* centers = nullptr;       // n
+    float* block_aabb = nullptr;     // 6 * nb
+    float* gaabb = nullptr;          // 6
+    uint32_t* m30 = nullptr;         // n, unsorted 30-bit Morton codes
+    uint32_t* keys = nullptr;        // n, sort buffers
+    uint32_t* keys_alt = nullptr;
+    uint32_t* vals = nullptr;
+    uint32_t* vals_alt = nullptr;
+    uint32_t* hist = nullptr;
+    uint32_t* sgo = nullptr;         // sorted_get_original (points into vals or vals_alt)
+    uint32_t* m30_sorted = nullptr;  // (points into keys or keys_alt)
+    uint64_t* ms64 = nullptr;        // n, sorted morton64 = m30 << 32 | element id
+    uint32_t* parent = nullptr;      // 2n - 1
+    uint2* children = nullptr;       // 2n - 1, reference layout
+    uint32_t* slot = nullptr;        // 2n - 1, 2 * parent + side
+    float4* wide = nullptr;          // 4 * max(ni, 1)
+    uint32_t* counters = nullptr;    // max(ni, 1), refit arrival counters (self-resetting)
+    uint32_t* healthy = nullptr;     // 1
+};
+
+namespace {
+
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v)
+{
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    return (v | (v << 2)) & 0x09249249u;
+}
+
+// make_morton32, lbvh.cpp:112-124
+__device__ __forceinline__ uint32_t morton32(float px, float py, float pz)
+{
+    float x = fmn(fmx(px * 1024.0f, 0.0f), 1023.0f);
+    float y = fmn(fmx(py * 1024.0f, 0.0f), 1023.0f);
+    float z = fmn(fmx(pz * 1024.0f, 0.0f), 1023.0f);
+    return (expand_bits((uint32_t)x) << 2) | (expand_bits((uint32_t)y) << 1) | expand_bits((uint32_t)z);
+}
+
+__device__ __forceinline__ void elem_box(int kind, const float4* __restrict__ x, const uint32_t* __restrict__ elems,
+                                         uint32_t e, v3& mn, v3& mx, v3& c)
+{
+    if (kind == LCS_TREE_VERT) {
+        v3 p = ld3(x, e);
+        mn = p; mx = p; c = p;
+    } else if (kind == LCS_TREE_EDGE) {
+        uint2 ed = __ldg(reinterpret_cast<const uint2*>(elems) + e);
+        v3 p0 = ld3(x, ed.x), p1 = ld3(x, ed.y);
+        mn = min3(p0, p1);
+        mx = max3(p0, p1);
+        c = 0.5f * (p0 + p1);  // lbvh.cpp:468
+    } else {
+        uint4 f = __ldg(reinterpret_cast<const uint4*>(elems) + e);
+        v3 p0 = ld3(x, f.x), p1 = ld3(x, f.y), p2 = ld3(x, f.z);
+        mn = min3(p0, min3(p1, p2));
+        mx = max3(p0, max3(p1, p2));
+        c = 0.333333f * ((p0 + p1) + p2);  // lbvh.cpp:488
+    }
+}
+
+// fn_reduce_{vert,edge,face}_tree_global_aabb, lbvh.cpp:449-491: centres + per-256 partials
+__global__ void __launch_bounds__(256) k_reduce_pass1(int kind, const float4* __restrict__ x,
+                                                      const uint32_t* __restrict__ elems, uint32_t n,
+                                                      float4* __restrict__ centers, float* __restrict__ block_aabb)
+{
+    __shared__ float red[8][6];
+    const uint32_t e = blockIdx.x * 256 + threadIdx.x;
+    v3 mn = mk3(INFINITY, INFINITY, INFINITY), mx = mk3(-INFINITY, -INFINITY, -INFINITY);
+    if (e < n) {
+        v3 c;
+        elem_box(kind, x, elems, e, mn, mx, c);
+        centers[e] = make_float4(c.x, c.y, c.z, 0.0f);
+    }
+    float v[6] = {mn.x, mn.y, mn.z, mx.x, mx.y, mx.z};
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            float t = __shfl_xor_sync(0xFFFFFFFFu, v[k], o);
+            v[k] = k < 3 ? fmn(v[k], t) : fmx(v[k], t);
+        }
+    if (lane_id() == 0)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) red[threadIdx.x >> 5][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        float r = red[0][threadIdx.x];
+        for (int w = 1; w < 8; ++w) r = threadIdx.x < 3 ? fmn(r, red[w][threadIdx.x]) : fmx(r, red[w][threadIdx.x]);
+        block_aabb[6 * blockIdx.x + threadIdx.x] = r;
+    }
+}
+
+// fn_reduce_aabb_2_pass(_atomic), lbvh.cpp:396-447, over the first nb_cover partials
+__global__ void __launch_bounds__(256) k_reduce_pass2(const float* __restrict__ block_aabb, uint32_t nb_cover,
+                                                      float* __restrict__ gaabb)
+{
+    __shared__ float red[8][6];
+    float v[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t b = threadIdx.x; b < nb_cover; b += 256)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) v[k] = k < 3 ? fmn(v[k], block_aabb[6 * b + k]) : fmx(v[k], block_aabb[6 * b + k]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            float t = __shfl_xor_sync(0xFFFFFFFFu, v[k], o);
+            v[k] = k < 3 ? fmn(v[k], t) : fmx(v[k], t);
+        }
+    if (lane_id() == 0)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) red[threadIdx.x >> 5][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        float r = red[0][threadIdx.x];
+        for (int w = 1; w < 8; ++w) r = threadIdx.x < 3 ? fmn(r, red[w][threadIdx.x]) : fmx(r, red[w][threadIdx.x]);
+        gaabb[threadIdx.x] = r;
+    }
+}
+
+// fn_compute_mortons, lbvh.cpp:507-523 (30-bit code; the element id is the sort value)
+__global__ void k_mortons(const float4* __restrict__ centers, const float* __restrict__ gaabb, uint32_t n,
+                          uint32_t* __restrict__ m30, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals)
+{
+    const float inv0 = 1.0f / fmx(gaabb[3] - gaabb[0], 1e-6f);
+    const float inv1 = 1.0f / fmx(gaabb[4] - gaabb[1], 1e-6f);
+    const float inv2 = 1.0f / fmx(gaabb[5] - gaabb[2], 1e-6f);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 c = centers[i];
+        uint32_t m = morton32((c.x - gaabb[0]) * inv0, (c.y - gaabb[1]) * inv1, (c.z - gaabb[2]) * inv2);
+        m30[i] = m;
+        keys[i] = m;
+        vals[i] = i;
+    }
+}
+
+// fn_reset_tree + fn_apply_sorted, lbvh.cpp:493-539
+__global__ void k_apply_sorted(const uint32_t* __restrict__ m30s, const uint32_t* __restrict__ sgo, uint32_t n,
+                               uint64_t* __restrict__ ms64, uint2* __restrict__ children, uint32_t* __restrict__ parent,
+                               uint32_t* __restrict__ healthy)
+{
+    const uint32_t ni = n - 1;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t o = sgo[i];
+        ms64[i] = ((uint64_t)m30s[i] << 32) | (uint64_t)o;
+        children[ni + i] = make_uint2(o, o);
+        if (i == 0) {
+            parent[0] = kInvalid;
+            *healthy = 1u;
+        }
+    }
+}
+
+__device__ __forceinline__ int cp_ij(uint64_t mi, int j, const uint64_t* __restrict__ ms, int n)
+{
+    return (j >= 0 && j < n) ? __clzll((long long)(mi ^ ms[j])) : -1;
+}
+
+// fn_build_inner_nodes with determineRange / findSplit, lbvh.cpp:204-291, 541-596; also the
+// traversal records' child codes and the child -> parent slot map
+__global__ void k_build_inner(const uint64_t* __restrict__ ms, const uint32_t* __restrict__ sgo, uint32_t n,
+                              uint32_t* __restrict__ parent, uint2* __restrict__ children,
+                              uint32_t* __restrict__ slot, float4* __restrict__ wide)
+{
+    const int ni = (int)n - 1;
+    for (int nid = blockIdx.x * blockDim.x + threadIdx.x; nid < ni; nid += gridDim.x * blockDim.x) {
+        int i = 0, j = ni;
+        if (nid != 0) {
+            const uint64_t mi = ms[nid];
+            const int cl = __clzll((long long)(mi ^ ms[nid - 1]));
+            const int cr = __clzll((long long)(mi ^ ms[nid + 1]));
+            const int d = cl < cr ? 1 : -1;
+            const int cp_min = cl < cr ? cl : cr;
+            int lmax = 2;
+            while (cp_ij(mi, nid + lmax * d, ms, (int)n) > cp_min) lmax <<= 1;
+            int l = 0;
+            for (int t = lmax >> 1; t >= 1; t >>= 1)
+                if (cp_ij(mi, nid + (l + t) * d, ms, (int)n) > cp_min) l += t;
+            i = nid;
+            j = nid + l * d;
+        }
+        int a = i < j ? i : j, b = i < j ? j : i;
+        int split;
+        {
+            const uint64_t ma = ms[a], mb = ms[b];
+            if (ma == mb) {
+                split = (a + b) >> 1;
+            } else {
+                const int cp_node = __clzll((long long)(ma ^ mb));
+                int t = b - a;
+                split = a;
+                for (;;) {
+                    t = (t + 1) >> 1;
+                    const int ns = split + t;
+                    if (ns < b && __clzll((long long)(ma ^ ms[ns])) > cp_node) split = ns;
+                    if (!(t > 1)) break;
+                }
+            }
+        }
+        int cleft = (a == split) ? ni + split : split;
+        int cright = (b == split + 1) ? ni + split + 1 : split + 1;
+        if (cright >= ni) {
+            int t = cleft;
+            cleft = cright;
+            cright = t;
+        }
+        parent[cleft] = (uint32_t)nid;
+        parent[cright] = (uint32_t)nid;
+        children[nid] = make_uint2((uint32_t)cleft, (uint32_t)cright);
+        slot[cleft] = 2u * (uint32_t)nid + 0u;
+        slot[cright] = 2u * (uint32_t)nid + 1u;
+        const uint32_t code_l = cleft < ni ? (uint32_t)cleft : (0x80000000u | sgo[cleft - ni]);
+        const uint32_t code_r = cright < ni ? (uint32_t)cright : (0x80000000u | sgo[cright - ni]);
+        wide[4 * nid + 0].w = __uint_as_float(code_l);
+        wide[4 * nid + 2].w = __uint_as_float(code_r);
+    }
+}
+
+// fn_check_construction, lbvh.cpp:598-611
+__global__ void k_check(const uint2* __restrict__ children, const uint32_t* __restrict__ parent, uint32_t ni,
+                        uint32_t* __restrict__ healthy)
+{
+    for (uint32_t nid = blockIdx.x * blockDim.x + threadIdx.x; nid < ni; nid += gridDim.x * blockDim.x) {
+        uint2 c = children[nid];
+        if (parent[c.x] != nid || parent[c.y] != nid) *healthy = 0u;
+    }
+}
+
+__device__ __forceinline__ void leaf_box(int kind, uint32_t e, const float* __restrict__ thickness,
+                                         const float4* __restrict__ x0, const float4* __restrict__ x1,
+                                         const uint32_t* __restrict__ elems, v3& mn, v3& mx)
+{
+    float th;
+    if (kind == LCS_TREE_VERT) {
+        v3 a = ld3(x0, e), b = ld3(x1, e);
+        mn = min3(a, b);
+        mx = max3(a, b);
+        th = __ldg(&thickness[e]);
+    } else if (kind == LCS_TREE_EDGE) {
+        uint2 ed = __ldg(reinterpret_cast<const uint2*>(elems) + e);
+        v3 s0 = ld3(x0, ed.x), s1 = ld3(x0, ed.y), e0 = ld3(x1, ed.x), e1 = ld3(x1, ed.y);
+        mn = min3(min3(s0, s1), min3(e0, e1));
+        mx = max3(max3(s0, s1), max3(e0, e1));
+        th = __ldg(&thickness[ed.x]);
+    } else {
+        uint4 f = __ldg(reinterpret_cast<const uint4*>(elems) + e);
+        v3 s0 = ld3(x0, f.x), s1 = ld3(x0, f.y), s2 = ld3(x0, f.z);
+        v3 e0 = ld3(x1, f.x), e1 = ld3(x1, f.y), e2 = ld3(x1, f.z);
+        mn = min3(min3(s0, min3(s1, s2)), min3(e0, min3(e1, e2)));
+        mx = max3(max3(s0, max3(s1, s2)), max3(e0, max3(e1, e2)));
+        th = __ldg(&thickness[f.x]);
+    }
+    mn = mk3(mn.x - th, mn.y - th, mn.z - th);
+    mx = mk3(mx.x + th, mx.y + th, mx.z + th);
+}
+
+__device__ __forceinline__ void store_slot(float4* wide, uint32_t s, v3 mn, v3 mx, uint32_t code)
+{
+    float4* r = wide + 4 * (s >> 1) + 2 * (s & 1u);
+    __stcg(r, make_float4(mn.x, mn.y, mn.z, __uint_as_float(code)));
+    __stcg(r + 1, make_float4(mx.x, mx.y, mx.z, 0.0f));
+}
+
+// fn_update_*_tree_leave_aabb_v2 (lbvh.cpp:617-683) and, when `climb`, fn_refit_tree_aabb
+// (lbvh.cpp:702-754): the second child to arrive at a parent unions the two slot boxes and
+// carries on upwards; arrival counters reset themselves, so no init pass is needed.
+__global__ void k_leaves_refit(int kind, uint32_t n, const uint32_t* __restrict__ sgo,
+                               const uint32_t* __restrict__ slot, const uint32_t* __restrict__ parent,
+                               const float* __restrict__ thickness, const float4* __restrict__ x0,
+                               const float4* __restrict__ x1, const uint32_t* __restrict__ elems, float4* wide,
+                               uint32_t* counters, uint32_t* healthy, int write_leaf, int climb)
+{
+    const uint32_t ni = n - 1;
+    for (uint32_t lid = blockIdx.x * blockDim.x + threadIdx.x; lid < n; lid += gridDim.x * blockDim.x) {
+        const uint32_t e = sgo[lid];
+        if (write_leaf) {
+            v3 mn, mx;
+            leaf_box(kind, e, thickness, x0, x1, elems, mn, mx);
+            if (n == 1) {
+                store_slot(wide, 0, mn, mx, 0x80000000u | e);
+                store_slot(wide, 1, mn, mx, 0x80000000u | e);
+            } else {
+                store_slot(wide, slot[ni + lid], mn, mx, 0x80000000u | e);
+            }
+        }
+        if (!climb || n == 1) continue;
+        uint32_t p = parent[ni + lid];
+        for (int guard = 0;; ++guard) {
+            if (guard > 256 || p >= ni) {  // deeper than any Karras tree over 62-bit keys: links are broken
+                *healthy = 0u;
+                break;
+            }
+            __threadfence();
+            if (atomicAdd(&counters[p], 1u) == 0u) break;  // first arrival: the sibling finishes
+            counters[p] = 0u;
+            __threadfence();
+            const float4* r = wide + 4 * p;
+            float4 a0 = __ldcg(r + 0), a1 = __ldcg(r + 1), b0 = __ldcg(r + 2), b1 = __ldcg(r + 3);
+            v3 mn = mk3(fmn(a0.x, b0.x), fmn(a0.y, b0.y), fmn(a0.z, b0.z));
+            v3 mx = mk3(fmx(a1.x, b1.x), fmx(a1.y, b1.y), fmx(a1.z, b1.z));
+            if (p == 0) break;
+            store_slot(wide, slot[p], mn, mx, p);
+            p = parent[p];
+        }
+    }
+}
+
+__device__ __forceinline__ bool overlap(float4 mn, float4 mx, const float* q)
+{
+    return mn.x < q[3] && mn.y < q[4] && mn.z < q[5] && mx.x > q[0] && mx.y > q[1] && mx.z > q[2];
+}
+
+// query_template2 (lbvh.cpp:293-360) for fn_query_from_verts_v2 (EE = false, lbvh.cpp:776-808)
+// and fn_query_from_edges_v2 (EE = true, lbvh.cpp:810-846)
+template <bool EE>
+__global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide, uint32_t n_leaves,
+                                               const float4* __restrict__ x0, const float4* __restrict__ x1,
+                                               const uint2* __restrict__ edges, uint32_t n_queries,
+                                               const float* __restrict__ dhat, const float* __restrict__ thickness,
+                                               uint2* __restrict__ pairs, uint32_t capacity, uint32_t* d_count)
+{
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n_queries; q += gridDim.x * blockDim.x) {
+        float box[6];
+        {
+            v3 mn, mx;
+            uint32_t v0;
+            if (EE) {
+                uint2 ed = __ldg(&edges[q]);
+                v3 s0 = ld3(x0, ed.x), s1 = ld3(x0, ed.y), e0 = ld3(x1, ed.x), e1 = ld3(x1, ed.y);
+                mn = min3(min3(s0, s1), min3(e0, e1));
+                mx = max3(max3(s0, s1), max3(e0, e1));
+                v0 = ed.x;
+            } else {
+                v3 a = ld3(x0, q), b = ld3(x1, q);
+                mn = min3(a, b);
+                mx = max3(a, b);
+                v0 = q;
+            }
+            const float r = __ldg(&thickness[v0]) + __ldg(&dhat[v0]);
+            box[0] = mn.x - r; box[1] = mn.y - r; box[2] = mn.z - r;
+            box[3] = mx.x + r; box[4] = mx.y + r; box[5] = mx.z + r;
+        }
+        uint32_t stack[32];
+        int sp = 0;
+        uint32_t loop = 0;
+        stack[sp++] = 0;
+        while (sp > 0) {
+            const uint32_t node = stack[--sp];
+            const float4* r = wide + 4 * node;
+            const float4 a0 = __ldg(r + 0), a1 = __ldg(r + 1), b0 = __ldg(r + 2), b1 = __ldg(r + 3);
+            bool stop = false;
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const float4 mn = side ? b0 : a0, mx = side ? b1 : a1;
+                if (!stop && overlap(mn, mx, box)) {
+                    const uint32_t code = __float_as_uint(mn.w);
+                    if (code & 0x80000000u) {
+                        const uint32_t obj = code & 0x7FFFFFFFu;
+                        if (!EE || q < obj) {
+                            const uint32_t s = atomicAdd(d_count, 1u);
+                            if (s < capacity) pairs[s] = make_uint2(q, obj);
+                        }
+                    } else if (sp < 32) {
+                        stack[sp++] = code;
+                    } else {
+                        stop = true;
+                    }
+                }
+            }
+            if (stop) break;
+            if (++loop > 100000u) break;
+        }
+    }
+}
+
+__global__ void k_export(const lcs_bvh h_in, uint32_t* __restrict__ object_idx, uint64_t* __restrict__ morton,
+                         float* __restrict__ node_aabb)
+{
+    const uint32_t n = h_in.n, ni = h_in.ni, nn = 2 * n - 1;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+        if (object_idx) object_idx[k] = k >= ni ? h_in.sgo[k - ni] : kInvalid;
+        if (morton && k < n) morton[k] = ((uint64_t)h_in.m30[k] << 32) | k;
+        if (node_aabb) {
+            float4 mn, mx;
+            if (n == 1) {
+                mn = h_in.wide[0];
+                mx = h_in.wide[1];
+            } else if (k == 0) {
+                float4 a0 = h_in.wide[0], a1 = h_in.wide[1], b0 = h_in.wide[2], b1 = h_in.wide[3];
+                mn = make_float4(fmn(a0.x, b0.x), fmn(a0.y, b0.y), fmn(a0.z, b0.z), 0.0f);
+                mx = make_float4(fmx(a1.x, b1.x), fmx(a1.y, b1.y), fmx(a1.z, b1.z), 0.0f);
+            } else {
+                uint32_t s = h_in.slot[k];
+                mn = h_in.wide[4 * (s >> 1) + 2 * (s & 1u)];
+                mx = h_in.wide[4 * (s >> 1) + 2 * (s & 1u) + 1];
+            }
+            float* o = node_aabb + 8 * (size_t)k;
+            o[0] = mn.x; o[1] = mn.y; o[2] = mn.z; o[3] = 0.0f;
+            o[4] = mx.x; o[5] = mx.y; o[6] = mx.z; o[7] = 0.0f;
+        }
+    }
+}
+
+template <typename T>
+cudaError_t alloc(T*& p, size_t count)
+{
+    return cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * (count ? count : 1));
+}
+
+}  // namespace
+
+extern "C" int lcs_bvh_create(int kind, uint32_t n_leaves, lcs_bvh** out)
+{
+    if (!out || kind < LCS_TREE_VERT || kind > LCS_TREE_FACE) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_create: bad argument");
+    lcs_bvh* h = new (std::nothrow) lcs_bvh();
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_create: out of host memory");
+    h->kind = kind;
+    h->n = n_leaves;
+    h->ni = n_leaves ? n_leaves - 1 : 0;
+    h->nb = (n_leaves + 255) / 256;
+    const size_t nn = n_leaves ? 2 * (size_t)n_leaves - 1 : 1;
+    const size_t nw = h->ni ? h->ni : 1;
+    cudaError_t e = cudaSuccess;
+    auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    A(alloc(h->centers, n_leaves));
+    A(alloc(h->block_aabb, 6 * (size_t)(h->nb ? h->nb : 1)));
+    A(alloc(h->gaabb, 6));
+    A(alloc(h->m30, n_leaves));
+    A(alloc(h->keys, n_leaves));
+    A(alloc(h->keys_alt, n_leaves));
+    A(alloc(h->vals, n_leaves));
+    A(alloc(h->vals_alt, n_leaves));
+    A(alloc(h->hist, rs::hist_words(n_leaves)));
+    A(alloc(h->ms64, n_leaves));
+    A(alloc(h->parent, nn));
+    A(alloc(h->children, nn));
+    A(alloc(h->slot, nn));
+    A(alloc(h->wide, 4 * nw));
+    A(alloc(h->counters, nw));
+    A(alloc(h->healthy, 1));
+    if (e == cudaSuccess) e = cudaMemset(h->counters, 0, sizeof(uint32_t) * nw);
+    if (e == cudaSuccess) e = cudaMemset(h->wide, 0, sizeof(float4) * 4 * nw);
+    if (e == cudaSuccess) e = cudaMemset(h->slot, 0xFF, sizeof(uint32_t) * nn);
+    if (e != cudaSuccess) {
+        lcs_bvh_destroy(h);
+        return lcs_fail(LCS_ERR_CUDA, "lcs_bvh_create: cudaMalloc failed");
+    }
+    h->sgo = h->vals;
+    h->m30_sorted = h->keys;
+    *out = h;
+    return LCS_OK;
+}
+
+extern "C" int lcs_bvh_destroy(lcs_bvh* h)
+{
+    if (!h) return LCS_OK;
+    void* ptrs[] = {h->centers, h->block_aabb, h->gaabb, h->m30, h->keys, h->keys_alt, h->vals, h->vals_alt,
+                    h->hist, h->ms64, h->parent, h->children, h->slot, h->wide, h->counters, h->healthy};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete h;
+    return LCS_OK;
+}
+
+extern "C" uint32_t lcs_bvh_num_leaves(const lcs_bvh* h) { return h ? h->n : 0; }
+
+extern "C" int lcs_bvh_reduce_aabb(lcs_bvh* h, const float* x, const uint32_t* elems, uint32_t n_verts,
+                                   lcs_stream stream)
+{
+    if (!h || !x || (h->kind != LCS_TREE_VERT && !elems) || n_verts == 0)
+        return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_reduce_aabb: bad argument");
+    if (h->kind == LCS_TREE_VERT && n_verts > 256u * 256u)
+        return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_reduce_aabb: vertex tree over 65536 vertices (lbvh.cpp:941-945)");
+    if (h->n == 0) return LCS_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    k_reduce_pass1<<<h->nb, 256, 0, s>>>(h->kind, reinterpret_cast<const float4*>(x), elems, h->n, h->centers,
+                                         h->block_aabb);
+    uint32_t nb_verts = (n_verts + 255) / 256;
+    uint32_t cover = nb_verts < h->nb ? nb_verts : h->nb;
+    k_reduce_pass2<<<1, 256, 0, s>>>(h->block_aabb, cover, h->gaabb);
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+extern "C" int lcs_bvh_construct(lcs_bvh* h, lcs_stream stream)
+{
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_construct: null handle");
+    if (h->n == 0) return LCS_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int g = grid_for(h->n, 256);
+    k_mortons<<<g, 256, 0, s>>>(h->centers, h->gaabb, h->n, h->m30, h->keys, h->vals);
+    bool alt = rs::sort_pairs<uint32_t>(h->keys, h->vals, h->keys_alt, h->vals_alt, nullptr, h->n, h->n, 0, 30,
+                                        h->hist, s);
+    h->m30_sorted = alt ? h->keys_alt : h->keys;
+    h->sgo = alt ? h->vals_alt : h->vals;
+    k_apply_sorted<<<g, 256, 0, s>>>(h->m30_sorted, h->sgo, h->n, h->ms64, h->children, h->parent, h->healthy);
+    if (h->ni > 0) {
+        const int gi = grid_for(h->ni, 256);
+        k_build_inner<<<gi, 256, 0, s>>>(h->ms64, h->sgo, h->n, h->parent, h->children, h->slot, h->wide);
+        k_check<<<gi, 256, 0, s>>>(h->children, h->parent, h->ni, h->healthy);
+    } else {
+        cudaMemcpyAsync(h->slot, &kInvalid, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    }
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+static int leaves_refit(lcs_bvh* h, const float* thickness, const float* x0, const float* x1, const uint32_t* elems,
+                        int write_leaf, int climb, lcs_stream stream)
+{
+    if (!h || (write_leaf && (!thickness || !x0 || !x1 || (h->kind != LCS_TREE_VERT && !elems))))
+        return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_update/refit: bad argument");
+    if (h->n == 0) return LCS_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    k_leaves_refit<<<grid_for(h->n, 256), 256, 0, s>>>(h->kind, h->n, h->sgo, h->slot, h->parent, thickness,
+                                                       reinterpret_cast<const float4*>(x0),
+                                                       reinterpret_cast<const float4*>(x1), elems, h->wide,
+                                                       h->counters, h->healthy, write_leaf, climb);
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+extern "C" int lcs_bvh_update_leaves(lcs_bvh* h, const float* thickness, const float* x0, const float* x1,
+                                     const uint32_t* elems, lcs_stream stream)
+{
+    return leaves_refit(h, thickness, x0, x1, elems, 1, 0, stream);
+}
+
+extern "C" int lcs_bvh_refit(lcs_bvh* h, lcs_stream stream)
+{
+    return leaves_refit(h, nullptr, nullptr, nullptr, nullptr, 0, 1, stream);
+}
+
+extern "C" int lcs_bvh_update_refit(lcs_bvh* h, const float* thickness, const float* x0, const float* x1,
+                                    const uint32_t* elems, lcs_stream stream)
+{
+    return leaves_refit(h, thickness, x0, x1, elems, 1, 1, stream);
+}
+
+extern "C" int lcs_bvh_query_vf(const lcs_bvh* t, const float* x0, const float* x1, uint32_t n_verts,
+                                const float* d_hat, const float* thickness, uint32_t* pairs, uint32_t capacity,
+                                uint32_t* d_count, lcs_stream stream)
+{
+    if (!t || t->kind != LCS_TREE_FACE || !x0 || !x1 || !d_hat || !thickness || !d_count || (capacity && !pairs))
+        return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_vf: bad argument (needs a face tree)");
+    if (t->n == 0 || n_verts == 0) return LCS_OK;
+    k_query<false><<<grid_for(n_verts, 128, 16), 128, 0, (cudaStream_t)stream>>>(
+        t->wide, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1), nullptr, n_verts,
+        d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count);
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+extern "C" int lcs_bvh_query_ee(const lcs_bvh* t, const float* x0, const float* x1, const uint32_t* edges,
+                                uint32_t n_edges, const float* d_hat, const float* thickness, uint32_t* pairs,
+                                uint32_t capacity, uint32_t* d_count, lcs_stream stream)
+{
+    if (!t || t->kind != LCS_TREE_EDGE || !x0 || !x1 || !edges || !d_hat || !thickness || !d_count ||
+        (capacity && !pairs))
+        return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_ee: bad argument (needs an edge tree)");
+    if (t->n == 0 || n_edges == 0) return LCS_OK;
+    k_query<true><<<grid_for(n_edges, 128, 16), 128, 0, (cudaStream_t)stream>>>(
+        t->wide, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
+        reinterpret_cast<const uint2*>(edges), n_edges, d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity,
+        d_count);
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+extern "C" int lcs_bvh_health(lcs_bvh* h, int* healthy, lcs_stream stream)
+{
+    if (!h || !healthy) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_health: bad argument");
+    if (h->n == 0) { *healthy = 1; return LCS_OK; }
+    uint32_t v = 0;
+    LCS_CUDA_TRY(cudaMemcpyAsync(&v, h->healthy, sizeof(uint32_t), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    LCS_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    *healthy = (int)v;
+    return LCS_OK;
+}
+
+extern "C" int lcs_bvh_export(const lcs_bvh* h, uint32_t* parent, uint32_t* children, uint32_t* object_idx,
+                              uint64_t* morton, uint64_t* morton_sorted, uint32_t* sorted_get_original,
+                              float* node_aabb, float* global_aabb6, lcs_stream stream)
+{
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_export: null handle");
+    if (h->n == 0) return LCS_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t nn = 2 * (size_t)h->n - 1;
+    if (parent) LCS_CUDA_TRY(cudaMemcpyAsync(parent, h->parent, 4 * nn, cudaMemcpyDeviceToDevice, s));
+    if (children) LCS_CUDA_TRY(cudaMemcpyAsync(children, h->children, 8 * nn, cudaMemcpyDeviceToDevice, s));
+    if (morton_sorted) LCS_CUDA_TRY(cudaMemcpyAsync(morton_sorted, h->ms64, 8 * (size_t)h->n, cudaMemcpyDeviceToDevice, s));
+    if (sorted_get_original) LCS_CUDA_TRY(cudaMemcpyAsync(sorted_get_original, h->sgo, 4 * (size_t)h->n, cudaMemcpyDeviceToDevice, s));
+    if (global_aabb6) LCS_CUDA_TRY(cudaMemcpyAsync(global_aabb6, h->gaabb, 24, cudaMemcpyDeviceToDevice, s));
+    if (object_idx || morton || node_aabb) k_export<<<grid_for(nn, 256), 256, 0, s>>>(*h, object_idx, morton, node_aabb);
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}

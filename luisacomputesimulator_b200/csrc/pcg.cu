@@ -1,0 +1,576 @@
+// pcg.cu -- 3x3 block SpMV and block-Jacobi preconditioned CG.
+//
+// Reference: ConjugateGradientSolver (Solver/LinearSolver/precond_cg.cpp:33-331, 626-771) and
+// the SpMV NewtonSolver hands it (newton_solver.cpp:259-270, 347-472, 3397-3427).
+//
+// Two executions of the same recurrences:
+//  * plain  -- the reference's dispatch structure: one kernel per operation (apply
+//              preconditioner, its second pass, update p, SpMV, p.q, its second pass, step)
+//              and a host read-back of r.z every `check_every` iterations;
+//  * fused  -- one persistent cooperative launch for the whole solve: rows are owned by
+//              threads, the three grid-wide reductions per iteration go through bounded
+//              software grid barriers, and every block reduces the per-block partials in the
+//              same fixed order, so all blocks agree on alpha / beta / convergence.
+// Reductions are FP32 (the reference) or FP64 (precision form, LCS_PCG_FP64_DOTS).
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <new>
+
+#include "lcs_common.cuh"
+#include "lcs_internal.h"
+
+using namespace lcs;
+
+namespace {
+
+constexpr float kPcgEps = 1e-10f;  // pcg_epsilon, precond_cg.cpp:12
+
+__device__ __forceinline__ float safe_div(float a, float b) { return b < kPcgEps ? 0.0f : a / b; }
+
+struct Bsr {
+    const uint32_t* rp;
+    const uint32_t* col;
+    const float* val;
+};
+
+__device__ __forceinline__ float3 mv9(const float* __restrict__ m, float4 x)
+{
+    float3 y;
+    y.x = __fmaf_rn(m[6], x.z, __fmaf_rn(m[3], x.y, m[0] * x.x));
+    y.y = __fmaf_rn(m[7], x.z, __fmaf_rn(m[4], x.y, m[1] * x.x));
+    y.z = __fmaf_rn(m[8], x.z, __fmaf_rn(m[5], x.y, m[2] * x.x));
+    return y;
+}
+
+__device__ __forceinline__ float3 mv12(const float4* __restrict__ m, float4 x)
+{
+    const float4 c0 = m[0], c1 = m[1], c2 = m[2];
+    float3 y;
+    y.x = __fmaf_rn(c2.x, x.z, __fmaf_rn(c1.x, x.y, c0.x * x.x));
+    y.y = __fmaf_rn(c2.y, x.z, __fmaf_rn(c1.y, x.y, c0.y * x.x));
+    y.z = __fmaf_rn(c2.z, x.z, __fmaf_rn(c1.z, x.y, c0.z * x.x));
+    return y;
+}
+
+// G lanes per row; returns the full row product on every lane of the group
+template <int G>
+__device__ __forceinline__ float3 row_product(uint32_t row, uint32_t lig, const float4* __restrict__ diag,
+                                              const Bsr A, const Bsr B, const float4* x)
+{
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    if (A.rp) {
+        const uint32_t e = __ldg(&A.rp[row + 1]);
+        for (uint32_t k = __ldg(&A.rp[row]) + lig; k < e; k += G) {
+            const float3 t = mv9(A.val + 9 * (size_t)k, __ldcg(&x[__ldg(&A.col[k])]));
+            acc.x += t.x; acc.y += t.y; acc.z += t.z;
+        }
+    }
+    if (B.rp) {
+        const uint32_t e = __ldcg(&B.rp[row + 1]);
+        for (uint32_t k = __ldcg(&B.rp[row]) + lig; k < e; k += G) {
+            const float3 t = mv9(B.val + 9 * (size_t)k, __ldcg(&x[__ldcg(&B.col[k])]));
+            acc.x += t.x; acc.y += t.y; acc.z += t.z;
+        }
+    }
+#pragma unroll
+    for (int o = G >> 1; o > 0; o >>= 1) {
+        acc.x += __shfl_xor_sync(0xFFFFFFFFu, acc.x, o);
+        acc.y += __shfl_xor_sync(0xFFFFFFFFu, acc.y, o);
+        acc.z += __shfl_xor_sync(0xFFFFFFFFu, acc.z, o);
+    }
+    const float3 d = mv12(diag + 3 * (size_t)row, __ldcg(&x[row]));
+    return make_float3(d.x + acc.x, d.y + acc.y, d.z + acc.z);
+}
+
+template <int G>
+__global__ void __launch_bounds__(256) k_spmv(uint32_t n, const float4* __restrict__ diag, Bsr A, Bsr B,
+                                              const float4* x, float4* y)
+{
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t lig = gtid % G;
+    const uint32_t ngroups = gridDim.x * blockDim.x / G;
+    const uint32_t rows_round = (n + ngroups - 1) / ngroups * ngroups;
+    for (uint32_t row = gtid / G; row < rows_round; row += ngroups) {
+        const uint32_t r = row < n ? row : n - 1;  // whole groups stay converged for the shuffles
+        const float3 v = row_product<G>(r, lig, diag, A, B, x);
+        if (row < n && lig == 0) y[row] = make_float4(v.x, v.y, v.z, 0.0f);
+    }
+}
+
+// ------------------------------------------------------------------------------------ plain
+template <typename T>
+__device__ __forceinline__ T block_sum(T v)
+{
+    __shared__ T red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    if (lane_id() == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    T s = 0;
+    if (threadIdx.x == 0)
+        for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) s += red[w];
+    __syncthreads();
+    return s;
+}
+
+// fn_pcg_init + fn_pcg_make_preconditioner (precond_cg.cpp:118-177, 256-267), x0 = 0
+__global__ void k_plain_init(uint32_t n, const float4* __restrict__ b, const float4* __restrict__ diag, float4* x,
+                             float4* r, float4* p, float4* minv, float* scal)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        r[i] = b[i];
+        p[i] = make_float4(0, 0, 0, 0);
+        x[i] = make_float4(0, 0, 0, 0);
+        const float4 c0 = diag[3 * i], c1 = diag[3 * i + 1], c2 = diag[3 * i + 2];
+        const float a = c0.x, bb = c1.x, c = c2.x, d = c0.y, e = c1.y, f = c2.y, g = c0.z, h = c1.z, k = c2.z;
+        const float A = e * k - f * h, B = f * g - d * k, C = d * h - e * g;
+        const float det = a * A + bb * B + c * C;
+        const float id = 1.0f / det;
+        minv[3 * i + 0] = make_float4(A * id, B * id, C * id, 0.0f);
+        minv[3 * i + 1] = make_float4((c * h - bb * k) * id, (a * k - c * g) * id, (bb * g - a * h) * id, 0.0f);
+        minv[3 * i + 2] = make_float4((bb * f - c * e) * id, (c * d - a * f) * id, (a * e - bb * d) * id, 0.0f);
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 8) scal[threadIdx.x] = 0.0f;
+}
+
+// fn_pcg_apply_preconditioner (precond_cg.cpp:269-294): z = Minv r, partials of r.r and r.z
+template <typename T>
+__global__ void __launch_bounds__(256) k_plain_precond(uint32_t n, const float4* __restrict__ minv, const float4* r,
+                                                       float4* z, T* part)
+{
+    T rr = 0, rz = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 rv = r[i];
+        const float3 zv = mv12(minv + 3 * (size_t)i, rv);
+        z[i] = make_float4(zv.x, zv.y, zv.z, 0.0f);
+        rr += (T)__fmaf_rn(rv.z, rv.z, __fmaf_rn(rv.y, rv.y, rv.x * rv.x));
+        rz += (T)__fmaf_rn(rv.z, zv.z, __fmaf_rn(rv.y, zv.y, rv.x * zv.x));
+    }
+    rr = block_sum(rr);
+    rz = block_sum(rz);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = rr;
+        part[2 * blockIdx.x + 1] = rz;
+    }
+}
+
+// fn_pcg_apply_preconditioner_second_pass (precond_cg.cpp:296-330): beta, r.z, |r| history.
+// scal: 0 rr0, 1 rz, 2 alpha, 3 beta, 4 |r|, 5 |r0|, 6 nan flag
+template <typename T>
+__global__ void k_plain_precond2(const T* part, uint32_t nblocks, float* scal, int first)
+{
+    T rr = 0, rz = 0;
+    for (uint32_t k = threadIdx.x; k < nblocks; k += blockDim.x) {
+        rr += part[2 * k];
+        rz += part[2 * k + 1];
+    }
+    rr = block_sum(rr);
+    rz = block_sum(rz);
+    if (threadIdx.x == 0) {
+        const float frr = (float)rr, frz = (float)rz;
+        scal[3] = safe_div(frz, scal[1]);
+        scal[1] = frz;
+        scal[4] = sqrtf(frr);
+        if (first) scal[5] = sqrtf(frr);
+    }
+}
+
+__global__ void k_plain_update_p(uint32_t n, const float4* z, float4* p, const float* scal)
+{
+    const float beta = scal[3];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 zv = z[i], pv = p[i];
+        p[i] = make_float4(zv.x + beta * pv.x, zv.y + beta * pv.y, zv.z + beta * pv.z, 0.0f);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_plain_dot(uint32_t n, const float4* a, const float4* b, T* part)
+{
+    T s = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 u = a[i], v = b[i];
+        s += (T)__fmaf_rn(u.z, v.z, __fmaf_rn(u.y, v.y, u.x * v.x));
+    }
+    s = block_sum(s);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+template <typename T>
+__global__ void k_plain_alpha(const T* part, uint32_t nblocks, float* scal)
+{
+    T s = 0;
+    for (uint32_t k = threadIdx.x; k < nblocks; k += blockDim.x) s += part[k];
+    s = block_sum(s);
+    if (threadIdx.x == 0) scal[2] = safe_div(scal[1], (float)s);
+}
+
+// fn_pcg_step (precond_cg.cpp:240-253)
+__global__ void k_plain_step(uint32_t n, float4* x, float4* r, const float4* p, const float4* q, const float* scal)
+{
+    const float alpha = scal[2];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 pv = p[i], qv = q[i], xv = x[i], rv = r[i];
+        x[i] = make_float4(xv.x + alpha * pv.x, xv.y + alpha * pv.y, xv.z + alpha * pv.z, 0.0f);
+        r[i] = make_float4(rv.x - alpha * qv.x, rv.y - alpha * qv.y, rv.z - alpha * qv.z, 0.0f);
+    }
+}
+
+// -------------------------------------------------------------------------------- fused
+struct FusedArgs {
+    uint32_t n;
+    const float4* diag;
+    Bsr A, B;
+    const float4* b;
+    float4* x;
+    float4 *r, *z, *p, *q, *minv;
+    double* part;        // 3 * gridDim
+    unsigned* bar_count;
+    unsigned* bar_gen;
+    int max_iter;
+    float rel_tol, abs_rz_tol;
+    int check_every;
+    int fp64;
+    lcs_pcg_stats* stats;
+};
+
+constexpr unsigned kBarrierSpinLimit = 1u << 24;
+
+// software grid barrier for a cooperative launch; gives up (status LCS_ERR_TIMEOUT) after a
+// bounded number of polls so that a stuck block can never hang the GPU
+__device__ __forceinline__ bool grid_barrier(const FusedArgs& a, volatile int* s_fail)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = a.bar_gen;
+        const unsigned g = *gen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(a.bar_count, 1u);
+        if (arrived == gridDim.x - 1) {
+            *a.bar_count = 0u;
+            __threadfence();
+            atomicAdd(a.bar_gen, 1u);
+        } else {
+            unsigned it = 0;
+            while (*gen == g) {
+                if (++it > kBarrierSpinLimit) {
+                    *s_fail = 1;
+                    a.stats->status = LCS_ERR_TIMEOUT;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *s_fail == 0;
+}
+
+// every block sums the per-block partials in the same order -> identical scalars everywhere
+__device__ __forceinline__ void reduce_partials(const FusedArgs& a, int k, int count, double* out)
+{
+    __shared__ double s_out[3];
+    if (threadIdx.x < 32) {
+        double v[3] = {0.0, 0.0, 0.0};
+        for (uint32_t b = threadIdx.x; b < gridDim.x; b += 32)
+            for (int c = 0; c < count; ++c) v[c] += __ldcg(&a.part[3 * b + k + c]);
+        for (int c = 0; c < count; ++c) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xFFFFFFFFu, v[c], o);
+        }
+        if (threadIdx.x == 0)
+            for (int c = 0; c < count; ++c) s_out[c] = v[c];
+    }
+    __syncthreads();
+    for (int c = 0; c < count; ++c) out[c] = s_out[c];
+    __syncthreads();
+}
+
+template <int G>
+__global__ void __launch_bounds__(256) k_pcg_fused(FusedArgs a)
+{
+    __shared__ int s_fail;
+    __shared__ double s_red[8][3];
+    if (threadIdx.x == 0) s_fail = 0;
+    const uint32_t n = a.n;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+
+    // x = 0, r = b, p = 0, Minv = inverse(D)
+    for (uint32_t i = tid; i < n; i += nthreads) {
+        a.r[i] = a.b[i];
+        a.p[i] = make_float4(0, 0, 0, 0);
+        a.x[i] = make_float4(0, 0, 0, 0);
+        const float4 c0 = a.diag[3 * i], c1 = a.diag[3 * i + 1], c2 = a.diag[3 * i + 2];
+        const float aa = c0.x, bb = c1.x, c = c2.x, d = c0.y, e = c1.y, f = c2.y, g = c0.z, h = c1.z, k = c2.z;
+        const float A = e * k - f * h, B = f * g - d * k, C = d * h - e * g;
+        const float id = 1.0f / (aa * A + bb * B + c * C);
+        a.minv[3 * i + 0] = make_float4(A * id, B * id, C * id, 0.0f);
+        a.minv[3 * i + 1] = make_float4((c * h - bb * k) * id, (aa * k - c * g) * id, (bb * g - aa * h) * id, 0.0f);
+        a.minv[3 * i + 2] = make_float4((bb * f - c * e) * id, (c * d - aa * f) * id, (aa * e - bb * d) * id, 0.0f);
+    }
+
+    float rz_old = 0.0f, norm_r0 = 0.0f, norm_r = 0.0f, rz = 0.0f;
+    int iter = 0, status = 0;
+    for (iter = 0; iter < a.max_iter; ++iter) {
+        // z = Minv r ; r.r ; r.z
+        double rr_d = 0.0, rz_d = 0.0;
+        float rr_f = 0.0f, rz_f = 0.0f;
+        for (uint32_t i = tid; i < n; i += nthreads) {
+            const float4 rv = a.r[i];
+            const float3 zv = mv12(a.minv + 3 * (size_t)i, rv);
+            a.z[i] = make_float4(zv.x, zv.y, zv.z, 0.0f);
+            const float drr = __fmaf_rn(rv.z, rv.z, __fmaf_rn(rv.y, rv.y, rv.x * rv.x));
+            const float drz = __fmaf_rn(rv.z, zv.z, __fmaf_rn(rv.y, zv.y, rv.x * zv.x));
+            rr_d += drr; rz_d += drz; rr_f += drr; rz_f += drz;
+        }
+        {
+            double v0 = a.fp64 ? rr_d : (double)rr_f, v1 = a.fp64 ? rz_d : (double)rz_f;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                v0 += __shfl_xor_sync(0xFFFFFFFFu, v0, o);
+                v1 += __shfl_xor_sync(0xFFFFFFFFu, v1, o);
+            }
+            if (lane_id() == 0) { s_red[threadIdx.x >> 5][0] = v0; s_red[threadIdx.x >> 5][1] = v1; }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double t0 = 0, t1 = 0;
+                for (int w = 0; w < 8; ++w) { t0 += s_red[w][0]; t1 += s_red[w][1]; }
+                a.part[3 * blockIdx.x + 0] = t0;
+                a.part[3 * blockIdx.x + 1] = t1;
+            }
+        }
+        if (!grid_barrier(a, &s_fail)) return;
+        double red[2];
+        reduce_partials(a, 0, 2, red);
+        const float rr = (float)red[0];
+        rz = (float)red[1];
+        const float beta = safe_div(rz, rz_old);
+        rz_old = rz;
+        norm_r = sqrtf(rr);
+        if (iter == 0) norm_r0 = norm_r;
+        if (iter % a.check_every == 0) {
+            if (isnan(rz) || isinf(rz)) { status = LCS_ERR_NAN; break; }
+            if (rz < a.abs_rz_tol) break;
+            if (a.rel_tol > 0.0f && norm_r <= a.rel_tol * norm_r0) break;
+        }
+        // p = z + beta p
+        for (uint32_t i = tid; i < n; i += nthreads) {
+            const float4 zv = a.z[i], pv = a.p[i];
+            a.p[i] = make_float4(zv.x + beta * pv.x, zv.y + beta * pv.y, zv.z + beta * pv.z, 0.0f);
+        }
+        if (!grid_barrier(a, &s_fail)) return;
+        // q = A p ; p.q
+        double pq_d = 0.0;
+        float pq_f = 0.0f;
+        {
+            const uint32_t lig = tid % G, ngroups = nthreads / G;
+            const uint32_t rows_round = (n + ngroups - 1) / ngroups * ngroups;
+            for (uint32_t row = tid / G; row < rows_round; row += ngroups) {
+                const uint32_t rr_ = row < n ? row : n - 1;
+                const float3 qv = row_product<G>(rr_, lig, a.diag, a.A, a.B, a.p);
+                if (row < n && lig == 0) {
+                    a.q[row] = make_float4(qv.x, qv.y, qv.z, 0.0f);
+                    const float4 pv = __ldcg(&a.p[row]);
+                    const float d = __fmaf_rn(pv.z, qv.z, __fmaf_rn(pv.y, qv.y, pv.x * qv.x));
+                    pq_d += d;
+                    pq_f += d;
+                }
+            }
+            double v = a.fp64 ? pq_d : (double)pq_f;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+            if (lane_id() == 0) s_red[threadIdx.x >> 5][2] = v;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double t = 0;
+                for (int w = 0; w < 8; ++w) t += s_red[w][2];
+                a.part[3 * blockIdx.x + 2] = t;
+            }
+        }
+        if (!grid_barrier(a, &s_fail)) return;
+        double pq;
+        reduce_partials(a, 2, 1, &pq);
+        const float alpha = safe_div(rz, (float)pq);
+        // x += alpha p ; r -= alpha q
+        for (uint32_t i = tid; i < n; i += nthreads) {
+            const float4 pv = a.p[i], qv = __ldcg(&a.q[i]), xv = a.x[i], rv = a.r[i];
+            a.x[i] = make_float4(xv.x + alpha * pv.x, xv.y + alpha * pv.y, xv.z + alpha * pv.z, 0.0f);
+            a.r[i] = make_float4(rv.x - alpha * qv.x, rv.y - alpha * qv.y, rv.z - alpha * qv.z, 0.0f);
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.stats->iterations = iter;
+        a.stats->rel_residual = norm_r0 > 0.0f ? norm_r / norm_r0 : 0.0f;
+        a.stats->dot_rz = rz_old;
+        if (a.stats->status == LCS_OK) a.stats->status = status;
+    }
+}
+
+}  // namespace
+
+struct lcs_pcg {
+    uint32_t n = 0;
+    float4 *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *minv = nullptr;
+    double* part = nullptr;
+    float* part_f = nullptr;
+    float* scal = nullptr;       // plain-mode scalars
+    float* h_scal = nullptr;     // pinned host copy
+    unsigned* bar = nullptr;     // [count, gen]
+    lcs_pcg_stats* d_stats = nullptr;
+    int fused_grid = 0;
+};
+
+static constexpr int kRowLanes = 4;
+static constexpr int kPlainBlocks = 256;
+
+extern "C" int lcs_pcg_create(uint32_t n, lcs_pcg** out)
+{
+    if (!out || n == 0) return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_create: bad argument");
+    lcs_pcg* p = new (std::nothrow) lcs_pcg();
+    if (!p) return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_create: out of host memory");
+    p->n = n;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_fused<kRowLanes>, 256, 0);
+    if (per_sm > 4) per_sm = 4;
+    p->fused_grid = sms * (per_sm > 0 ? per_sm : 1);
+    const int parts = p->fused_grid > kPlainBlocks ? p->fused_grid : kPlainBlocks;
+    cudaError_t e = cudaSuccess;
+    auto A = [&](void** q, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(q, bytes); };
+    A((void**)&p->r, 16 * (size_t)n);
+    A((void**)&p->z, 16 * (size_t)n);
+    A((void**)&p->p, 16 * (size_t)n);
+    A((void**)&p->q, 16 * (size_t)n);
+    A((void**)&p->minv, 48 * (size_t)n);
+    A((void**)&p->part, 3 * sizeof(double) * parts);
+    A((void**)&p->part_f, 3 * sizeof(float) * parts);
+    A((void**)&p->scal, 16 * sizeof(float));
+    A((void**)&p->bar, 2 * sizeof(unsigned));
+    A((void**)&p->d_stats, sizeof(lcs_pcg_stats));
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&p->h_scal, 16 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(p->bar, 0, 2 * sizeof(unsigned));
+    if (e != cudaSuccess) {
+        lcs_pcg_destroy(p);
+        return lcs_fail(LCS_ERR_CUDA, "lcs_pcg_create: allocation failed");
+    }
+    *out = p;
+    return LCS_OK;
+}
+
+extern "C" int lcs_pcg_destroy(lcs_pcg* p)
+{
+    if (!p) return LCS_OK;
+    void* ptrs[] = {p->r, p->z, p->p, p->q, p->minv, p->part, p->part_f, p->scal, p->bar, p->d_stats};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    if (p->h_scal) cudaFreeHost(p->h_scal);
+    delete p;
+    return LCS_OK;
+}
+
+extern "C" const lcs_pcg_stats* lcs_pcg_device_stats(const lcs_pcg* p) { return p ? p->d_stats : nullptr; }
+
+static Bsr to_bsr(const lcs_bsr* m) { return m ? Bsr{m->row_ptr, m->col, m->val} : Bsr{nullptr, nullptr, nullptr}; }
+
+extern "C" int lcs_spmv(uint32_t n, const float* diag, const lcs_bsr* A, const lcs_bsr* B, const float* x, float* y,
+                        lcs_stream stream)
+{
+    if (!diag || !x || !y || n == 0) return lcs_fail(LCS_ERR_INVALID, "lcs_spmv: bad argument");
+    if ((A && A->n_rows != n) || (B && B->n_rows != n)) return lcs_fail(LCS_ERR_INVALID, "lcs_spmv: row count mismatch");
+    k_spmv<kRowLanes><<<grid_for((uint64_t)n * kRowLanes, 256), 256, 0, (cudaStream_t)stream>>>(
+        n, reinterpret_cast<const float4*>(diag), to_bsr(A), to_bsr(B), reinterpret_cast<const float4*>(x),
+        reinterpret_cast<float4*>(y));
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+template <typename T>
+static int plain_solve(lcs_pcg* P, const float4* diag, Bsr A, Bsr B, const float4* b, float4* x,
+                       const lcs_pcg_opts& o, lcs_pcg_stats* stats, cudaStream_t s)
+{
+    const uint32_t n = P->n;
+    const int g = grid_for(n, 256);
+    const int nb = g < kPlainBlocks ? g : kPlainBlocks;
+    T* part = reinterpret_cast<T*>(sizeof(T) == 8 ? (void*)P->part : (void*)P->part_f);
+    k_plain_init<<<g, 256, 0, s>>>(n, b, diag, x, P->r, P->p, P->minv, P->scal);
+    int iter = 0, status = LCS_OK;
+    float norm_r0 = 0.0f, norm_r = 0.0f, rz = 0.0f;
+    const int check = o.check_every > 0 ? o.check_every : 1;
+    for (iter = 0; iter < o.max_iter; ++iter) {
+        k_plain_precond<T><<<nb, 256, 0, s>>>(n, P->minv, P->r, P->z, part);
+        k_plain_precond2<T><<<1, 256, 0, s>>>(part, nb, P->scal, iter == 0);
+        if (iter % check == 0) {
+            LCS_CUDA_TRY(cudaMemcpyAsync(P->h_scal, P->scal, 8 * sizeof(float), cudaMemcpyDeviceToHost, s));
+            LCS_CUDA_TRY(cudaStreamSynchronize(s));
+            rz = P->h_scal[1];
+            norm_r = P->h_scal[4];
+            if (iter == 0) norm_r0 = norm_r;
+            if (isnan(rz) || isinf(rz)) { status = LCS_ERR_NAN; break; }
+            if (rz < o.abs_rz_tol) break;
+            if (o.rel_tol > 0.0f && norm_r <= o.rel_tol * norm_r0) break;
+        }
+        k_plain_update_p<<<g, 256, 0, s>>>(n, P->z, P->p, P->scal);
+        k_spmv<kRowLanes><<<grid_for((uint64_t)n * kRowLanes, 256), 256, 0, s>>>(n, diag, A, B, P->p, P->q);
+        k_plain_dot<T><<<nb, 256, 0, s>>>(n, P->p, P->q, part);
+        k_plain_alpha<T><<<1, 256, 0, s>>>(part, nb, P->scal);
+        k_plain_step<<<g, 256, 0, s>>>(n, x, P->r, P->p, P->q, P->scal);
+    }
+    LCS_LAUNCH_CHECK();
+    LCS_CUDA_TRY(cudaMemcpyAsync(P->h_scal, P->scal, 8 * sizeof(float), cudaMemcpyDeviceToHost, s));
+    LCS_CUDA_TRY(cudaStreamSynchronize(s));
+    if (stats) {
+        stats->iterations = iter;
+        stats->rel_residual = norm_r0 > 0.0f ? P->h_scal[4] / norm_r0 : 0.0f;
+        stats->dot_rz = P->h_scal[1];
+        stats->status = status;
+    }
+    return status == LCS_OK ? LCS_OK : lcs_fail(status, "lcs_pcg_solve: NaN/Inf in r.z");
+}
+
+extern "C" int lcs_pcg_solve(lcs_pcg* P, const float* diag, const lcs_bsr* A, const lcs_bsr* B, const float* b,
+                             float* x, const lcs_pcg_opts* opts, lcs_pcg_stats* stats, lcs_stream stream)
+{
+    if (!P || !diag || !b || !x) return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve: bad argument");
+    if ((A && A->n_rows != P->n) || (B && B->n_rows != P->n)) return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve: row count mismatch");
+    lcs_pcg_opts o = opts ? *opts : lcs_pcg_opts{100, 1e-4f, 1e-10f, 25, 0};
+    if (o.check_every <= 0) o.check_every = 1;
+    cudaStream_t s = (cudaStream_t)stream;
+    const float4* d4 = reinterpret_cast<const float4*>(diag);
+    const float4* b4 = reinterpret_cast<const float4*>(b);
+    float4* x4 = reinterpret_cast<float4*>(x);
+    if (o.flags & LCS_PCG_PLAIN) {
+        if (o.flags & LCS_PCG_FP64_DOTS) return plain_solve<double>(P, d4, to_bsr(A), to_bsr(B), b4, x4, o, stats, s);
+        return plain_solve<float>(P, d4, to_bsr(A), to_bsr(B), b4, x4, o, stats, s);
+    }
+    FusedArgs a;
+    a.n = P->n;
+    a.diag = d4;
+    a.A = to_bsr(A);
+    a.B = to_bsr(B);
+    a.b = b4;
+    a.x = x4;
+    a.r = P->r; a.z = P->z; a.p = P->p; a.q = P->q; a.minv = P->minv;
+    a.part = P->part;
+    a.bar_count = P->bar;
+    a.bar_gen = P->bar + 1;
+    a.max_iter = o.max_iter;
+    a.rel_tol = o.rel_tol;
+    a.abs_rz_tol = o.abs_rz_tol;
+    a.check_every = o.check_every;
+    a.fp64 = (o.flags & LCS_PCG_FP64_DOTS) ? 1 : 0;
+    a.stats = P->d_stats;
+    LCS_CUDA_TRY(cudaMemsetAsync(P->d_stats, 0, sizeof(lcs_pcg_stats), s));
+    LCS_CUDA_TRY(cudaMemsetAsync(P->bar, 0, sizeof(unsigned), s));
+    void* args[] = {&a};
+    LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_fused<kRowLanes>, dim3(P->fused_grid), dim3(256), args,
+                                             0, s));
+    if (stats && !(o.flags & LCS_PCG_NO_STATS)) {
+        LCS_CUDA_TRY(cudaMemcpyAsync(stats, P->d_stats, sizeof(lcs_pcg_stats), cudaMemcpyDeviceToHost, s));
+        LCS_CUDA_TRY(cudaStreamSynchronize(s));
+        if (stats->status != LCS_OK) return lcs_fail(stats->status, "lcs_pcg_solve: fused solve failed");
+    }
+    return LCS_OK;
+}

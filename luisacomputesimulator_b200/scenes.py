@@ -1,0 +1,331 @@
+"""Seeded synthetic scenes with the shapes of the reference's benchmark configurations.
+
+No mesh file or dataset is read: the cloth grids, the icosphere and the twisted tube are
+generated here, and the per-element data the contact path consumes is derived the way the
+reference's initialisers derive it:
+
+* edges: unique (min, max) vertex pairs in lexicographic order, the order
+  ``extract_edges_from_surface`` produces (Solver/MeshOperation/mesh_reader.cpp:219-300);
+* dihedral (bending) stencils ``(e0, e1, opposite-of-first-face, opposite-of-second-face)``
+  for every interior edge (mesh_reader.cpp:219-300);
+* rest areas: face area, vertex area = sum(adjacent face area / 3) in double, edge area =
+  sum(adjacent face area / 3) (Solver/Initializer/init_mesh_data.cpp:780-870);
+* contact offset and d_hat per vertex, scaled down when offset + d_hat reaches 0.9 x the
+  smallest rest edge length / triangle altitude of the mesh
+  (Solver/Initializer/init_collision_data.cpp:67-171);
+* pinned vertices and their animated targets (Solver/Initializer/init_mesh_data.cpp:116-170,
+  Solver/SimulationSolver/solver_interface.cpp:130-162).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class MeshPart:
+    x: np.ndarray          # (n, 3) float32
+    faces: np.ndarray      # (f, 3) uint32, local indices
+    pinned: np.ndarray     # (n,) bool
+    thickness: float = 0.0
+    d_hat: float = 1e-3
+    density: float = 1e3   # kg per m^2 of rest area (MaterialBase::density)
+    rotate: tuple | None = None  # pinned-vertex animation: (axis_point(3), axis(3), ang_vel, mask)
+
+
+@dataclasses.dataclass
+class Scene:
+    name: str
+    x: np.ndarray            # (V, 4) float32 rest / initial positions
+    faces: np.ndarray        # (F, 4) uint32
+    edges: np.ndarray        # (E, 2) uint32
+    bending: np.ndarray      # (B, 4) uint32
+    vert_area: np.ndarray    # (V,) float32
+    face_area: np.ndarray    # (F,) float32
+    edge_area: np.ndarray    # (E,) float32
+    mass: np.ndarray         # (V,) float32
+    pinned: np.ndarray       # (V,) uint8
+    d_hat: np.ndarray        # (V,) float32
+    offset: np.ndarray       # (V,) float32
+    body: np.ndarray         # (V,) uint32, 0xFFFFFFFF = soft
+    rest_len: np.ndarray     # (E,) float32
+    bending_Q: np.ndarray    # (B, 4, 4) float32
+    dt: float = 1.0 / 60.0
+    gravity: tuple = (0.0, -9.8, 0.0)
+    kappa: float = 1e7
+    spring_k: float = 1e4
+    bending_k: float = 5e-3
+    dirichlet: float = 1e9
+    anims: list = dataclasses.field(default_factory=list)  # (vertex ids, center, axis, omega)
+
+    @property
+    def num_verts(self):
+        return self.x.shape[0]
+
+    def targets(self, t):
+        """Positions of the pinned vertices at time t (others: rest position)."""
+        out = self.x[:, :3].astype(np.float64).copy()
+        for vids, center, axis, omega in self.anims:
+            p = self.x[vids, :3].astype(np.float64) - center
+            out[vids] = _rotate(p, axis, omega * t) + center
+        return out.astype(np.float32)
+
+
+def _rotate(p, axis, ang):
+    axis = np.asarray(axis, np.float64)
+    axis = axis / np.linalg.norm(axis)
+    c, s = math.cos(ang), math.sin(ang)
+    return p * c + np.cross(axis, p) * s + np.outer(p @ axis, axis) * (1 - c)
+
+
+def cloth_grid(nx, nz, spacing, origin=(0.0, 0.0, 0.0), jitter=1e-4, seed=0):
+    """nx x nz vertex grid in the x-z plane, row-major, each quad split on its (i,j)-(i+1,j+1)
+    diagonal; out-of-plane (y) jitter U(-jitter, jitter)."""
+    rng = np.random.default_rng(seed)
+    ii, jj = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+    x = np.zeros((nx * nz, 3), np.float64)
+    x[:, 0] = origin[0] + (ii.ravel() - (nx - 1) / 2.0) * spacing
+    x[:, 2] = origin[2] + (jj.ravel() - (nz - 1) / 2.0) * spacing
+    x[:, 1] = origin[1] + rng.uniform(-jitter, jitter, nx * nz)
+    vid = lambda i, j: i * nz + j  # noqa: E731
+    faces = []
+    for i in range(nx - 1):
+        for j in range(nz - 1):
+            a, b, c, d = vid(i, j), vid(i + 1, j), vid(i + 1, j + 1), vid(i, j + 1)
+            faces.append((a, b, c))
+            faces.append((a, c, d))
+    return x.astype(np.float32), np.asarray(faces, np.uint32)
+
+
+def icosphere(subdiv, radius, center=(0.0, 0.0, 0.0)):
+    t = (1.0 + 5 ** 0.5) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    verts = [np.asarray(v, np.float64) / np.linalg.norm(v) for v in verts]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+             (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdiv):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    x = np.asarray(verts) * radius + np.asarray(center)
+    return x.astype(np.float32), np.asarray(faces, np.uint32)
+
+
+def tube(n_around, n_along, radius, length, center=(0.0, 0.0, 0.0)):
+    """Periodic cylinder around the x axis: n_around x n_along grid, vertex (i around, j along)
+    at index j * n_around + i; quads split on their (i,j)-(i+1,j+1) diagonal."""
+    th = 2.0 * np.pi * np.arange(n_around) / n_around
+    xs = -length / 2.0 + length * np.arange(n_along) / (n_along - 1)
+    J, I = np.meshgrid(np.arange(n_along), np.arange(n_around), indexing="ij")
+    x = np.zeros((n_along * n_around, 3), np.float64)
+    x[:, 0] = center[0] + xs[J.ravel()]
+    x[:, 1] = center[1] + radius * np.cos(th[I.ravel()])
+    x[:, 2] = center[2] + radius * np.sin(th[I.ravel()])
+    vid = lambda i, j: j * n_around + (i % n_around)  # noqa: E731
+    faces = []
+    for j in range(n_along - 1):
+        for i in range(n_around):
+            a, b, c, d = vid(i, j), vid(i + 1, j), vid(i + 1, j + 1), vid(i, j + 1)
+            faces.append((a, b, c))
+            faces.append((a, c, d))
+    return x.astype(np.float32), np.asarray(faces, np.uint32)
+
+
+def box_mesh(size, center):
+    """Closed box surface (8 vertices, 12 triangles)."""
+    h = np.asarray(size, np.float64) / 2.0
+    c = np.asarray(center, np.float64)
+    x = np.asarray([[sx, sy, sz] for sx in (-1, 1) for sy in (-1, 1) for sz in (-1, 1)], np.float64) * h + c
+    f = [(0, 1, 3), (0, 3, 2), (4, 6, 7), (4, 7, 5), (0, 4, 5), (0, 5, 1), (2, 3, 7), (2, 7, 6), (0, 2, 6),
+         (0, 6, 4), (1, 5, 7), (1, 7, 3)]
+    return x.astype(np.float32), np.asarray(f, np.uint32)
+
+
+def extract_edges(faces):
+    """Unique sorted edges and dihedral stencils (mesh_reader.cpp:219-300 ordering)."""
+    f = np.sort(faces.astype(np.int64), axis=1)
+    nf = f.shape[0]
+    fid = np.arange(nf)
+    half = np.concatenate([np.stack([f[:, 0], f[:, 1], fid], 1), np.stack([f[:, 0], f[:, 2], fid], 1),
+                           np.stack([f[:, 1], f[:, 2], fid], 1)])
+    order = np.lexsort((half[:, 2], half[:, 1], half[:, 0]))
+    half = half[order]
+    same_next = np.zeros(len(half), bool)
+    same_next[:-1] = (half[1:, 0] == half[:-1, 0]) & (half[1:, 1] == half[:-1, 1])
+    same_prev = np.zeros(len(half), bool)
+    same_prev[1:] = same_next[:-1]
+    keep = ~same_next  # types 0 (boundary) and 2 (second of an interior pair)
+    edges = half[keep][:, :2].astype(np.uint32)
+    # dihedral stencils from interior pairs (first element of each pair)
+    firsts = np.nonzero(same_next)[0]
+    bend = []
+    fa = faces.astype(np.int64)
+    for k in firsts:
+        a, b, f1 = half[k]
+        f2 = half[k + 1, 2]
+        o1 = [v for v in fa[f1] if v != a and v != b][0]
+        o2 = [v for v in fa[f2] if v != a and v != b][0]
+        bend.append((a, b, o1, o2))
+    bending = np.asarray(bend, np.uint32).reshape(-1, 4)
+    # adjacency edge -> faces for edge areas
+    edge_faces = np.full((edges.shape[0], 2), -1, np.int64)
+    eidx = np.cumsum(keep) - 1  # index of the edge each half belongs to (pairs share the later one)
+    eidx_first = np.where(same_next, eidx + 1, eidx)
+    for k in range(len(half)):
+        e = eidx_first[k]
+        slot = 0 if edge_faces[e, 0] < 0 else 1
+        edge_faces[e, slot] = half[k, 2]
+    return edges, bending, edge_faces
+
+
+def _face_area(x, faces):
+    x = x.astype(np.float32)
+    v0 = x[faces[:, 1]] - x[faces[:, 0]]
+    v1 = x[faces[:, 2]] - x[faces[:, 0]]
+    return (np.linalg.norm(np.cross(v0, v1), axis=1) * np.float32(0.5)).astype(np.float32)
+
+
+def _bending_Q(x, bend):
+    """Q = 3/(A0+A1) K K^T of the quadratic bending model (init_sim_data.cpp:455-480)."""
+    x = x.astype(np.float64)
+    p = [x[bend[:, k]] for k in range(4)]
+    e0, e1, e2, e3, e4 = p[1] - p[0], p[2] - p[0], p[3] - p[0], p[2] - p[1], p[3] - p[1]
+
+    def cot(a, b):
+        return np.einsum("ij,ij->i", a, b) / np.linalg.norm(np.cross(a, b), axis=1)
+
+    c01, c02, c03, c04 = cot(e0, -e1), cot(e0, -e2), cot(e0, e3), cot(e0, e4)
+    K = np.stack([c03 + c04, c01 + c02, -c01 - c03, -c02 - c04], 1)
+    A0 = 0.5 * np.linalg.norm(np.cross(e0, e1), axis=1)
+    A1 = 0.5 * np.linalg.norm(np.cross(e0, e2), axis=1)
+    Q = (3.0 / (A0 + A1))[:, None, None] * K[:, :, None] * K[:, None, :]
+    return Q.astype(np.float32)
+
+
+def _min_rest_dist(x, faces, edges):
+    x = x.astype(np.float32)
+    lens = np.linalg.norm(x[edges[:, 0]] - x[edges[:, 1]], axis=1)
+    best = float(lens.min()) if len(lens) else 1e10
+    for k in range(3):
+        v0, v1, v2 = x[faces[:, k]], x[faces[:, (k + 1) % 3]], x[faces[:, (k + 2) % 3]]
+        r = v2 - v1
+        d = np.einsum("ij,ij->i", r, r)
+        t = np.where(d > 1.19209290e-7, np.einsum("ij,ij->i", r, v0 - v1) / np.maximum(d, 1e-30), 0.5)
+        cp = (1 - t)[:, None] * v1 + t[:, None] * v2
+        best = min(best, float(np.linalg.norm(cp - v0, axis=1).min()))
+    return best
+
+
+def assemble(name, parts, dt, gravity, kappa, spring_k=1e4, bending_k=5e-3, bodies=None):
+    """Merge mesh parts into one Scene (vertex/face order = part order)."""
+    xs, fs, pins, vmesh, anims = [], [], [], [], []
+    off = 0
+    for m, part in enumerate(parts):
+        xs.append(part.x)
+        fs.append(part.faces.astype(np.int64) + off)
+        pins.append(part.pinned)
+        vmesh.append(np.full(part.x.shape[0], m))
+        if part.rotate is not None:
+            center, axis, omega, mask = part.rotate
+            anims.append((np.nonzero(mask)[0] + off, np.asarray(center), np.asarray(axis), float(omega)))
+        off += part.x.shape[0]
+    x3 = np.concatenate(xs).astype(np.float32)
+    faces = np.concatenate(fs).astype(np.uint32)
+    edges, bending, edge_faces = extract_edges(faces)
+    face_area = _face_area(x3, faces)
+    V = x3.shape[0]
+    vert_area = np.zeros(V, np.float64)
+    for k in range(3):
+        np.add.at(vert_area, faces[:, k], face_area.astype(np.float64) / 3.0)
+    ef = edge_faces
+    edge_area = np.where(ef[:, 0] >= 0, face_area[np.maximum(ef[:, 0], 0)] / 3.0, 0.0) + \
+        np.where(ef[:, 1] >= 0, face_area[np.maximum(ef[:, 1], 0)] / 3.0, 0.0)
+    vmesh = np.concatenate(vmesh)
+    d_hat = np.zeros(V, np.float32)
+    offset = np.zeros(V, np.float32)
+    mass = np.zeros(V, np.float32)
+    foff = 0
+    for m, part in enumerate(parts):
+        nfm = part.faces.shape[0]
+        sel_f = slice(foff, foff + nfm)
+        foff += nfm
+        vm = vmesh == m
+        fe = faces[sel_f]
+        emask = vm[edges[:, 0]]
+        safe = 0.9 * _min_rest_dist(x3, fe, edges[emask])
+        so, sd = 0.5 * part.thickness, part.d_hat
+        if not (so + sd < safe):
+            if so > 0.5 * safe:
+                so = 0.5 * safe
+            if sd > safe - so:
+                sd = safe - so
+        d_hat[vm] = sd
+        offset[vm] = so
+        area_m = vert_area[vm].sum()
+        mass[vm] = (vert_area[vm] / area_m * area_m * part.density).astype(np.float32)
+    x4 = np.zeros((V, 4), np.float32)
+    x4[:, :3] = x3
+    f4 = np.zeros((faces.shape[0], 4), np.uint32)
+    f4[:, :3] = faces
+    body = np.full(V, 0xFFFFFFFF, np.uint32) if bodies is None else bodies.astype(np.uint32)
+    rest_len = np.linalg.norm(x3[edges[:, 0]] - x3[edges[:, 1]], axis=1).astype(np.float32)
+    return Scene(name=name, x=x4, faces=f4, edges=edges.astype(np.uint32), bending=bending,
+                 vert_area=vert_area.astype(np.float32), face_area=face_area, edge_area=edge_area.astype(np.float32),
+                 mass=mass, pinned=np.concatenate(pins).astype(np.uint8), d_hat=d_hat, offset=offset, body=body,
+                 rest_len=rest_len, bending_Q=_bending_Q(x3, bending), dt=dt, gravity=tuple(gravity), kappa=kappa,
+                 spring_k=spring_k, bending_k=bending_k, anims=anims)
+
+
+def cloth_on_sphere(n=64, spacing=0.01, seed=0, subdiv=4, radius=0.2, drop=0.05):
+    """Config 1: n x n cloth (1 cm spacing) dropped from 5 cm above a pinned icosphere."""
+    cx, cf = cloth_grid(n, n, spacing, origin=(0.0, radius + drop, 0.0), jitter=1e-4, seed=seed)
+    sx, sf = icosphere(subdiv, radius)
+    cloth = MeshPart(cx, cf, np.zeros(cx.shape[0], bool))
+    sphere = MeshPart(sx, sf, np.ones(sx.shape[0], bool))
+    return assemble(f"cloth{n}x{n}_on_sphere", [cloth, sphere], dt=1.0 / 60.0, gravity=(0, -9.8, 0), kappa=1e7)
+
+
+def twisted_tube(n_around=300, n_along=296, radius=0.15, length=0.6, omega=2.0):
+    """Config 2: periodic tube whose two end rings rotate at -+omega rad/s about the x axis."""
+    x, f = tube(n_around, n_along, radius, length)
+    V = x.shape[0]
+    xn = (x[:, 0] - x[:, 0].min()) / (x[:, 0].max() - x[:, 0].min())
+    left = xn < 0.001
+    right = xn > 0.999
+    part = MeshPart(x, f, left | right)
+    sc = assemble(f"tube{n_around}x{n_along}", [part], dt=1.0 / 100.0, gravity=(0, 0, 0), kappa=1e9)
+    sc.anims = [(np.nonzero(left)[0], np.zeros(3), np.array([1.0, 0, 0]), -omega),
+                (np.nonzero(right)[0], np.zeros(3), np.array([1.0, 0, 0]), omega)]
+    assert V == sc.num_verts
+    return sc
+
+
+def random_cloth_scene(n_verts, seed, collider="sphere"):
+    """Batching/serving scenes: square cloth of ~n_verts over a seeded sphere or box collider."""
+    side = max(4, int(round(math.sqrt(n_verts))))
+    rng = np.random.default_rng(seed)
+    spacing = 0.6 / side
+    cx, cf = cloth_grid(side, side, spacing, origin=(0.0, 0.25, 0.0), jitter=1e-4, seed=seed)
+    if collider == "sphere":
+        sx, sf = icosphere(3, 0.2 * float(rng.uniform(0.8, 1.2)))
+    else:
+        sx, sf = box_mesh((0.3, 0.3, 0.3), (0.0, 0.0, 0.0))
+    return assemble(f"cloth{side}_{collider}_{seed}",
+                    [MeshPart(cx, cf, np.zeros(cx.shape[0], bool)), MeshPart(sx, sf, np.ones(sx.shape[0], bool))],
+                    dt=1.0 / 60.0, gravity=(0, -9.8, 0), kappa=1e7)

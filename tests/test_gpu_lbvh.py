@@ -1,0 +1,148 @@
+"""LBVH parity: the CUDA build / refit / traversal against the oracle, bit for bit.
+
+Sizes: config 1 (6,658 verts), a folded cloth (self contact), and config 2's 88,800-vertex
+tube at full size (177,000-face and 265,800-edge trees)."""
+import numpy as np
+import pytest
+import torch
+
+from luisacomputesimulator_b200.collision import LBVH
+from oracle import oracle as O
+from tests import scenarios as SC
+from tests.gpu_util import SceneOnDevice, counts, dev, host
+
+pytestmark = pytest.mark.gpu
+
+KINDS = {"face": (O.TREE_FACE, "faces"), "edge": (O.TREE_EDGE, "edges")}
+
+
+def _scene(name):
+    if name == "cloth_sphere":
+        return SC.cloth_touching_sphere(gap=5e-4)
+    if name == "folded":
+        return SC.folded_cloth(n=48, gap=4e-4)
+    if name == "tube":
+        return SC.twisted_tube_state(angle=1.2)
+    raise KeyError(name)
+
+
+def _build_both(sc, x, kind_name):
+    kind, attr = KINDS[kind_name]
+    elems = getattr(sc, attr)
+    t_o = O.lbvh_build(kind, x, elems, sc.num_verts)
+    bvh = LBVH(kind, elems.shape[0])
+    xd, ed = dev(x), dev(elems)
+    if kind == O.TREE_FACE:
+        bvh.reduce_face_tree_aabb(xd, ed)
+    else:
+        bvh.reduce_edge_tree_aabb(xd, ed)
+    bvh.construct_tree()
+    return t_o, bvh, xd, ed
+
+
+@pytest.mark.parametrize("scene", ["cloth_sphere", "folded", "tube"])
+@pytest.mark.parametrize("kind_name", ["face", "edge"])
+def test_topology_bit_exact(scene, kind_name):
+    sc, x = _scene(scene)
+    t_o, bvh, _, _ = _build_both(sc, x, kind_name)
+    assert bvh.check_health()
+    e = bvh.export()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(host(e["global_aabb"]), np.concatenate([t_o.gmin, t_o.gmax]))
+    np.testing.assert_array_equal(host(e["morton"], np.uint64), t_o.morton)
+    np.testing.assert_array_equal(host(e["morton_sorted"], np.uint64), t_o.morton_sorted)
+    np.testing.assert_array_equal(host(e["sorted_get_original"], np.uint32), t_o.sorted_get_original)
+    np.testing.assert_array_equal(host(e["parent"], np.uint32), t_o.parent)
+    np.testing.assert_array_equal(host(e["children"], np.uint32), t_o.children)
+    np.testing.assert_array_equal(host(e["object_idx"], np.uint32), t_o.object_idx)
+
+
+@pytest.mark.parametrize("scene", ["cloth_sphere", "folded", "tube"])
+@pytest.mark.parametrize("kind_name", ["face", "edge"])
+@pytest.mark.parametrize("fused", [False, True])
+def test_refit_bit_exact(scene, kind_name, fused):
+    sc, x = _scene(scene)
+    t_o, bvh, xd, ed = _build_both(sc, x, kind_name)
+    x1 = SC.random_motion(x, 1e-3, seed=7)
+    x1d = dev(x1)
+    off = dev(sc.offset + np.float32(1e-4))
+    O.lbvh_refit(t_o, x, x1, getattr(sc, KINDS[kind_name][1]), sc.offset + np.float32(1e-4))
+    for _ in range(2):  # twice: the arrival counters must have reset themselves
+        if fused:
+            bvh.update_and_refit(off, xd, x1d, ed)
+        else:
+            bvh.update_leaves(off, xd, x1d, ed)
+            bvh.refit()
+    e = bvh.export()
+    torch.cuda.synchronize()
+    got = host(e["node_aabb"])
+    np.testing.assert_array_equal(got[:, 0:3], t_o.node_aabb[:, 0:3])
+    np.testing.assert_array_equal(got[:, 4:7], t_o.node_aabb[:, 4:7])
+
+
+@pytest.mark.parametrize("scene", ["cloth_sphere", "folded", "tube"])
+@pytest.mark.parametrize("swept", [False, True])
+def test_candidate_sets_bit_exact(scene, swept):
+    sc, x = _scene(scene)
+    x1 = SC.random_motion(x, 2e-3, seed=11) if swept else x
+    D = SceneOnDevice(sc)
+    xd, x1d = dev(x), dev(x1)
+    for kind_name in ("face", "edge"):
+        t_o, bvh, _, ed = _build_both(sc, x, kind_name)
+        elems = getattr(sc, KINDS[kind_name][1])
+        O.lbvh_refit(t_o, x, x1, elems, sc.offset)
+        bvh.update_and_refit(D.offset, xd, x1d, ed)
+        cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+        if kind_name == "face":
+            want, n_want = O.lbvh_query_vf(t_o, x, x1, sc.d_hat, sc.offset)
+            pairs = torch.zeros((n_want + 64, 2), dtype=torch.int32, device="cuda")
+            bvh.broad_phase_query_from_verts(xd, x1d, cnt, pairs, D.d_hat, D.offset)
+        else:
+            want, n_want = O.lbvh_query_ee(t_o, x, x1, sc.edges, sc.d_hat, sc.offset)
+            pairs = torch.zeros((n_want + 64, 2), dtype=torch.int32, device="cuda")
+            bvh.broad_phase_query_from_edges(xd, x1d, D.edges, cnt, pairs, D.d_hat, D.offset)
+        n = int(counts(cnt)[0])
+        assert n == n_want
+        got = host(pairs, np.uint32)[:n]
+        np.testing.assert_array_equal(SC.sorted_pairs(got), SC.sorted_pairs(want))
+
+
+def test_query_overflow_counts_without_writing_past_capacity():
+    sc, x = _scene("cloth_sphere")
+    D = SceneOnDevice(sc)
+    t_o, bvh, xd, ed = _build_both(sc, x, "edge")
+    bvh.update_and_refit(D.offset, xd, xd, ed)
+    O.lbvh_refit(t_o, x, x, sc.edges, sc.offset)
+    want, n_want = O.lbvh_query_ee(t_o, x, x, sc.edges, sc.d_hat, sc.offset)
+    cap = 1000
+    guard = torch.full((cap + 16, 2), -7, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    bvh.broad_phase_query_from_edges(xd, xd, D.edges, cnt, guard[:cap], D.d_hat, D.offset)
+    n = int(counts(cnt)[0])
+    assert n == n_want and n > cap
+    g = host(guard)
+    assert np.all(g[cap:] == -7)  # nothing past capacity
+    full = {tuple(p) for p in SC.sorted_pairs(want).tolist()}
+    assert all(tuple(p) in full for p in g[:cap].astype(np.int64).tolist())
+
+
+def test_single_leaf_tree_and_empty_queries():
+    # one face: the reference's root is the leaf itself and both child reads hit it
+    x = np.array([[0, 0, 0, 0], [1, 0, 0, 0], [0, 1, 0, 0], [0.2, 0.2, 0.0005, 0]], np.float32)
+    faces = np.array([[0, 1, 2, 0]], np.uint32)
+    t_o = O.lbvh_build(O.TREE_FACE, x, faces, 4)
+    thick = np.zeros(4, np.float32)
+    dhat = np.full(4, 1e-3, np.float32)
+    O.lbvh_refit(t_o, x, x, faces, thick)
+    want, n_want = O.lbvh_query_vf(t_o, x, x, dhat, thick)
+    bvh = LBVH(O.TREE_FACE, 1)
+    xd, fd = dev(x), dev(faces)
+    bvh.reduce_face_tree_aabb(xd, fd)
+    bvh.construct_tree()
+    bvh.update_and_refit(dev(thick), xd, xd, fd)
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    pairs = torch.zeros((16, 2), dtype=torch.int32, device="cuda")
+    bvh.broad_phase_query_from_verts(xd, xd, cnt, pairs, dev(dhat), dev(thick))
+    n = int(counts(cnt)[0])
+    assert n == n_want
+    np.testing.assert_array_equal(SC.sorted_pairs(host(pairs, np.uint32)[:n]), SC.sorted_pairs(want))

@@ -1,0 +1,115 @@
+"""SpMV and Jacobi-PCG parity against the oracle on a contact system: inertia + edge springs
+(material BSR) + barrier contacts (contact BSR from the GPU assembler)."""
+import numpy as np
+import pytest
+import torch
+
+from luisacomputesimulator_b200.linear import ConjugateGradientSolver, make_bsr, spmv
+from oracle import oracle as O
+from tests import scenarios as SC
+from tests.gpu_util import dev, host
+
+pytestmark = pytest.mark.gpu
+
+
+def spring_system(sc, x, k=1e4, h=1 / 60):
+    """Diagonal blocks (3 float4 columns) and the off-diagonal BSR of inertia + springs."""
+    n = sc.num_verts
+    xv = x[:, :3].astype(np.float64)
+    e = sc.edges.astype(np.int64)
+    d = xv[e[:, 0]] - xv[e[:, 1]]
+    l = np.maximum(np.linalg.norm(d, axis=1), 1.19209290e-7)
+    L = sc.rest_len.astype(np.float64)
+    xxT = d[:, :, None] * d[:, None, :]
+    H = k * xxT / l[:, None, None] ** 2 + k * np.maximum(1 - L / l, 0)[:, None, None] * (
+        np.eye(3)[None] - xxT / l[:, None, None] ** 2)
+    D = np.zeros((n, 3, 3))
+    D[:] = np.eye(3) * (sc.mass[:, None, None] / h ** 2)
+    np.add.at(D, e[:, 0], H)
+    np.add.at(D, e[:, 1], H)
+    rows = np.concatenate([e[:, 0], e[:, 1]])
+    cols = np.concatenate([e[:, 1], e[:, 0]])
+    blocks = np.concatenate([-H, -H])
+    order = np.lexsort((cols, rows))
+    rows, cols, blocks = rows[order], cols[order], blocks[order]
+    rp = np.zeros(n + 1, np.int64)
+    np.add.at(rp, rows + 1, 1)
+    rp = np.cumsum(rp).astype(np.uint32)
+    val = np.stack([b.T.reshape(9) for b in blocks]).astype(np.float32)  # column-major
+    diag = np.zeros((n, 3, 4), np.float32)
+    diag[:, :, :3] = np.transpose(D, (0, 2, 1))
+    return diag, (rp, cols.astype(np.uint32), val)
+
+
+def contact_system():
+    sc, x = SC.folded_cloth(n=40, gap=4e-4)
+    tf = O.lbvh_build(O.TREE_FACE, x, sc.faces, sc.num_verts)
+    O.lbvh_refit(tf, x, x, sc.faces, sc.offset)
+    vf, _ = O.lbvh_query_vf(tf, x, x, sc.d_hat, sc.offset)
+    te = O.lbvh_build(O.TREE_EDGE, x, sc.edges, sc.num_verts)
+    O.lbvh_refit(te, x, x, sc.edges, sc.offset)
+    ee, _ = O.lbvh_query_ee(te, x, x, sc.edges, sc.d_hat, sc.offset)
+    pairs = np.concatenate([O.dcd_vf(vf, x, sc.faces, sc.body, sc.vert_area, sc.face_area, sc.d_hat, sc.offset,
+                                     sc.kappa),
+                            O.dcd_ee(ee, x, sc.edges, sc.body, sc.edge_area, sc.d_hat, sc.offset, sc.kappa)])
+    diag, A = spring_system(sc, x)
+    b = np.zeros((sc.num_verts, 4), np.float32)
+    b, diag = O.contact_grad_diag(pairs, sc.num_verts, b, diag)
+    rng = np.random.default_rng(0)
+    b[:, :3] += rng.normal(0, 1e-3, (sc.num_verts, 3)).astype(np.float32)
+    B = O.contact_offdiag_bsr(pairs, sc.num_verts)
+    return sc, diag, A, B, b
+
+
+@pytest.fixture(scope="module")
+def system():
+    return contact_system()
+
+
+def _dev_bsr(n, m):
+    rp, col, val = m
+    return make_bsr(n, dev(rp), dev(col), dev(val))
+
+
+def test_spmv_matches_oracle(system):
+    sc, diag, A, B, b = system
+    n = sc.num_verts
+    x = np.zeros((n, 4), np.float32)
+    x[:, :3] = np.random.default_rng(1).normal(size=(n, 3))
+    y = spmv(dev(diag), _dev_bsr(n, A), _dev_bsr(n, B), dev(x))
+    want = O.bsr_spmv(diag, A, B, x)
+    got = host(y)
+    scale = np.abs(want).max()
+    np.testing.assert_allclose(got[:, :3], want[:, :3], rtol=1e-5, atol=1e-6 * scale)
+
+
+@pytest.mark.parametrize("plain", [True, False])
+@pytest.mark.parametrize("fp64", [False, True])
+def test_pcg_matches_oracle(system, plain, fp64):
+    sc, diag, A, B, b = system
+    n = sc.num_verts
+    solver = ConjugateGradientSolver(n)
+    x = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    st = solver.device_solve(dev(diag), _dev_bsr(n, A), _dev_bsr(n, B), dev(b), x, max_iter=500, rel_tol=1e-4,
+                             check_every=25 if plain else 1, fp64_dots=fp64, plain=plain)
+    ox, ost = O.pcg(diag, A, B, b, max_iter=500, rel_tol=1e-4, check_every=25 if plain else 1, fp64_dots=fp64)
+    assert st["status"] == 0 and ost["status"] == 0
+    assert st["rel_residual"] <= 1e-4
+    # same recurrences, different summation order: iteration counts within a few percent
+    assert abs(st["iterations"] - ost["iterations"]) <= max(3, ost["iterations"] // 20 + 1)
+    # true residual of the GPU solution, in FP64 on the host
+    xr = host(x)
+    r = b[:, :3].astype(np.float64) - O.bsr_spmv(diag, A, B, xr)[:, :3].astype(np.float64)
+    assert np.linalg.norm(r) <= 2e-4 * np.linalg.norm(b[:, :3])
+    np.testing.assert_allclose(xr[:, :3], ox[:, :3], rtol=0, atol=2e-3 * np.abs(ox).max())
+
+
+def test_pcg_stop_rule_absolute_rz():
+    # the reference's own rule: stop when r.z < 1e-10, checked every 25 iterations
+    sc, diag, A, B, b = contact_system()
+    n = sc.num_verts
+    solver = ConjugateGradientSolver(n)
+    x = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    st = solver.device_solve(dev(diag), _dev_bsr(n, A), _dev_bsr(n, B), dev(b), x, max_iter=100, rel_tol=0.0,
+                             abs_rz_tol=1e-10, check_every=25, plain=True)
+    assert st["iterations"] % 25 == 0 or st["iterations"] == 100
