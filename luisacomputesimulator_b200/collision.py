@@ -136,10 +136,13 @@ class NarrowPhasesDetector:
         self._alloc()
         self.assembler = None
 
-    def _alloc(self):
-        self.broad_phase_list_vf = torch.zeros((self.cap_vf, 2), dtype=torch.int32, device=self.device)
-        self.broad_phase_list_ee = torch.zeros((self.cap_ee, 2), dtype=torch.int32, device=self.device)
-        self.narrow_phase_list = torch.zeros((self.cap_pairs, 12), dtype=torch.int32, device=self.device)
+    def _alloc(self, which=("vf", "ee", "pairs")):
+        if "vf" in which:
+            self.broad_phase_list_vf = torch.zeros((self.cap_vf, 2), dtype=torch.int32, device=self.device)
+        if "ee" in which:
+            self.broad_phase_list_ee = torch.zeros((self.cap_ee, 2), dtype=torch.int32, device=self.device)
+        if "pairs" in which:
+            self.narrow_phase_list = torch.zeros((self.cap_pairs, 12), dtype=torch.int32, device=self.device)
 
     def count_view(self, k):
         return self.counts[k:k + 1]
@@ -162,17 +165,20 @@ class NarrowPhasesDetector:
     def resize_buffers(self):
         """Doubles whatever overflowed (NarrowPhasesDetector::resize_buffers, narrow_phase.cpp:61-95)."""
         c = self.download_counts()
-        grew = False
+        grew = []
         while c[0] > self.cap_vf:
-            self.cap_vf *= 2; grew = True
+            self.cap_vf *= 2
+            grew.append("vf")
         while c[1] > self.cap_ee:
-            self.cap_ee *= 2; grew = True
+            self.cap_ee *= 2
+            grew.append("ee")
         while c[2] > self.cap_pairs:
-            self.cap_pairs *= 2; grew = True
+            self.cap_pairs *= 2
+            grew.append("pairs")
             self.assembler = None
         if grew:
-            self._alloc()
-        return grew
+            self._alloc(set(grew))
+        return bool(grew)
 
     # -- CCD (narrow_phase.cpp:293-740)
     def vf_ccd_query(self, x0, x1, faces, body, offset, toi_per_pair=None, fp64_final=False):

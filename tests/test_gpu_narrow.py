@@ -88,9 +88,15 @@ def _dcd(name):
     det = NarrowPhasesDetector(sc.num_verts, sc.edges.shape[0])
     _load(det, vf, ee)
     xd = dev(x0)
-    det.vf_dcd_query_repulsion(xd, D.faces, D.body, D.vert_area, D.face_area, D.d_hat, D.offset, sc.kappa)
-    det.ee_dcd_query_repulsion(xd, D.edges, D.body, D.edge_area, D.d_hat, D.offset, sc.kappa)
+    for attempt in range(2):  # resize-and-retry on overflow, as device_update_contact_list does
+        det.reset_narrowphase_count()
+        det.vf_dcd_query_repulsion(xd, D.faces, D.body, D.vert_area, D.face_area, D.d_hat, D.offset, sc.kappa)
+        det.ee_dcd_query_repulsion(xd, D.edges, D.body, D.edge_area, D.d_hat, D.offset, sc.kappa)
+        if not det.resize_buffers():
+            break
+        assert attempt == 0
     n = int(counts(det.counts)[2])
+    assert n <= det.cap_pairs
     got = host(det.narrow_phase_list).view(O.PAIR_DTYPE).reshape(-1)[:n]
     want = np.concatenate([O.dcd_vf(vf, x0, sc.faces, sc.body, sc.vert_area, sc.face_area, sc.d_hat, sc.offset,
                                     sc.kappa),
