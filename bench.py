@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""Newton iterations/s on the 88,800-vertex twisted cloth tube.
+
+Workload: a 300 x 296 periodic tube (88,800 vertices, 177,000 faces, 265,800 edges), radius
+0.15 m, length 0.6 m, the two end rings pinned and rotated at -/+2 rad/s about the tube axis;
+dt = 1/100 s, d_hat = 1e-3 m, thickness 0, kappa = 1e9, 3 Newton iterations per step,
+Jacobi-PCG up to 100 iterations / relative residual 1e-4, CCD line search.  Synthetic, seeded
+geometry (no mesh file).  A bench step is one time step; the metric counts the Newton
+iterations those steps ran.  State stays on the GPU; the working set (~150 MB: BVHs,
+candidate lists, block matrix) is larger than L2 and L2 is also flushed between steps.
+
+--impl reference runs the CPU restatement of the same Newton iteration (the oracle, OpenMP on
+all host cores) on the tube at the state the 60-step run reaches (end rings at -/+1.2 rad).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Newton iters/s at 88K-vert cloth"
+UNIT = "newton_iters/s"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def args_():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=57)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--mode", choices=["fused", "plain"], default="fused")
+    p.add_argument("--fp64", action="store_true", help="precision form")
+    p.add_argument("--e2e-steps", type=int, default=10)
+    p.add_argument("--cpu-iters", type=int, default=0, help="CPU baseline sample (0: auto, ~10-30 s)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--n-around", type=int, default=300)
+    p.add_argument("--n-along", type=int, default=296)
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def tube_config(a):
+    return {"workload": f"twisted tube {a.n_around}x{a.n_along} ({a.n_around * a.n_along} verts), 60-step run, "
+                        "rings -/+2 rad/s, dt 1/100, d_hat 1e-3, kappa 1e9, 3 Newton/step, PCG <=100 it rel 1e-4",
+            "verts": a.n_around * a.n_along, "dt": 0.01, "d_hat": 1e-3, "kappa": 1e9, "newton_per_step": 3,
+            "pcg": "Jacobi, max 100 iterations, rel 1e-4", "l2": "flushed between steps (256 MB write)"}
+
+
+# --------------------------------------------------------------------------- clocks sampling
+class Clocks:
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+        self.index = index
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms",
+                                       "200", "-i", str(self.index)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        try:
+            for ln in open(self.f.name):
+                parts = [s.strip() for s in ln.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        finally:
+            os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """DRAM bytes per launch of the fused PCG kernel from the committed ncu summary (or None)."""
+    path = os.path.join(ROOT, "profiles", "pcg_fused_tube_traffic.txt")
+    try:
+        for ln in open(path):
+            if ln.startswith("bytes_per_iteration="):
+                return float(ln.split("=")[1])
+    except Exception:
+        return None
+    return None
+
+
+# ------------------------------------------------------------------------------ CPU baseline
+def cpu_sample(a, iters=0, budget_s=20.0):
+    """Newton iterations/s of the oracle (CPU restatement) on the tube state of the 60-step run."""
+    import numpy as np
+
+    from oracle import newton_cpu as N
+    from tests import scenarios as SC
+    sc, x = SC.twisted_tube_state(angle=1.2, n_around=a.n_around, n_along=a.n_along)
+    pat = N.MaterialPattern(sc)
+    xt = x.copy()
+    done, t0 = 0, time.perf_counter()
+    while True:
+        x, toi, st, cnt = N.newton_iteration(sc, x, xt, sc.dt, pattern=pat)
+        done += 1
+        el = time.perf_counter() - t0
+        if (iters and done >= iters) or (not iters and (el > budget_s or done >= 20)):
+            break
+    cores = os.cpu_count()
+    return done / el, done, el, cores, np.float32(toi)
+
+
+def run_reference(a):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import numpy as np
+
+    from oracle import newton_cpu as N
+    from tests import scenarios as SC
+    sc, x = SC.twisted_tube_state(angle=1.2, n_around=a.n_around, n_along=a.n_along)
+    pat = N.MaterialPattern(sc)
+    xt = x.copy()
+    for _ in range(a.warmup):
+        N.newton_iteration(sc, x, xt, sc.dt, pattern=pat)
+    # one bench step = one Newton iteration of the CPU restatement (a bounded sample of the
+    # 3-iteration time step); cap the timed count so the run ends within a few minutes
+    steps = min(a.steps, 40)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        x, toi, st, cnt = N.newton_iteration(sc, x, xt, sc.dt, pattern=pat)
+    el = time.perf_counter() - t0
+    v = steps / el
+    cores = os.cpu_count()
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": steps, "warmup": a.warmup,
+            "ms_per_step": 1e3 * el / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "impl": "reference", "config": tube_config(a),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{steps} Newton iterations of the CPU restatement (oracle, OpenMP) on the "
+                                       "tube at its 60-step state; one bench step = one Newton iteration"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    _ = np
+
+
+# --------------------------------------------------------------------------------- our arm
+def run_ours(a):
+    import numpy as np
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from luisacomputesimulator_b200 import _capi, scenes
+    from luisacomputesimulator_b200.newton import NewtonSolver
+
+    lib = _capi.load()
+    _capi.check(lib.lcs_device_check(local), "device check")
+    sc = scenes.twisted_tube(a.n_around, a.n_along)
+    solver = NewtonSolver(sc, plain=(a.mode == "plain"), fp64=a.fp64, profile=True)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    for _ in range(a.warmup):
+        solver.step()
+    torch.cuda.synchronize()
+    solver.reset_profile()
+    if world > 1:
+        torch.distributed.barrier()
+
+    newton, pcg, ms_total = 0, 0, 0.0
+    per_step = []
+    launches0 = lib.lcs_launch_count()
+    with Clocks(local) as clk:
+        for _ in range(a.steps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = solver.step()
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            per_step.append(ms)
+            ms_total += ms
+            newton += st.newton_iters
+            pcg += st.pcg_iters
+    launches = lib.lcs_launch_count() - launches0
+    torch.cuda.synchronize()
+    clocks = clk.summary()
+    prof = solver.profile()
+    last = dict(vf=st.vf_candidates, ee=st.ee_candidates, pairs=st.contact_pairs, ccd_vf=st.ccd_vf_candidates,
+                ccd_ee=st.ccd_ee_candidates, last_toi=st.last_toi, last_rel_residual=st.last_rel_residual)
+    cnt = solver.counts()
+
+    # end to end through the public host-buffer call (x, v in from pinned host, x, v out)
+    V = sc.num_verts
+    hx = torch.empty((V, 4), dtype=torch.float32).pin_memory()
+    hv = torch.empty((V, 4), dtype=torch.float32).pin_memory()
+    hx.numpy()[:] = solver.positions()
+    hv.numpy()[:] = solver.velocities()
+    e2e_ms, e2e_newton = 0.0, 0
+    for _ in range(a.e2e_steps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s2 = solver.step_host(hx.numpy(), hv.numpy(), hx.numpy(), hv.numpy())
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+        e2e_newton += s2.newton_iters
+
+    # max over ranks of the time, sum of the work
+    t_s = ms_total / 1e3
+    e2e_s = e2e_ms / 1e3
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([t_s, e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        nn = torch.tensor([newton, e2e_newton], device="cuda", dtype=torch.float64)
+        dist.all_reduce(nn, op=dist.ReduceOp.SUM)
+        t_s, e2e_s = float(tt[0]), float(tt[1])
+        newton_all, e2e_all = float(nn[0]), float(nn[1])
+    else:
+        newton_all, e2e_all = float(newton), float(e2e_newton)
+
+    if rank == 0:
+        value = newton_all / t_s
+        # roofline of the dominant kernel: the persistent PCG solve (one launch per Newton iteration)
+        pcg_ms, pcg_launches = prof["pcg"]
+        nnz = cnt["nnz_material"] + 12 * last["pairs"]
+        it_per_launch = pcg / max(pcg_launches, 1)
+        bytes_per_iter = 40.0 * nnz + 312.0 * V
+        bytes_per_launch = it_per_launch * bytes_per_iter + 160.0 * V
+        achieved = bytes_per_launch / (pcg_ms / max(pcg_launches, 1) / 1e3) / 1e9
+        peak, peak_kind = measured_peak()
+        traffic = committed_traffic()
+        cpu = None
+        if not a.no_cpu_baseline and world == 1:
+            v_cpu, n_cpu, el_cpu, cores, _ = cpu_sample(a, a.cpu_iters)
+            cpu = {"value": v_cpu, "unit": UNIT, "cores": cores, "kind": "port",
+                   "sample": f"{n_cpu} Newton iterations ({el_cpu:.1f} s) of the CPU restatement (oracle, OpenMP, "
+                             "all host cores) on the tube at its 60-step state"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms_total / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" + ("+f64 reductions" if a.fp64 else ""), "data": "synthetic (seeded tube mesh)",
+            "impl": "ours", "mode": a.mode,
+            "config": {**tube_config(a), "parallelism": f"replicas x{world}" if world > 1 else "single scene"},
+            "e2e": {"value": e2e_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * 16 * V,
+                    "d2h_bytes_per_step": 2 * 16 * V, "steps": a.e2e_steps},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "k_pcg_fused (persistent Jacobi-PCG solve)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind,
+                         "traffic": None if traffic is None else traffic * it_per_launch,
+                         "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "pcg_iters_per_launch": it_per_launch, "avg_launch_ms": pcg_ms / max(pcg_launches, 1)},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "newton_iters": newton, "pcg_iters": pcg,
+            "phase_ms": {k: round(v[0], 3) for k, v in prof.items()},
+            "last_step": last,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    _ = np
+
+
+def main():
+    a = args_()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -78,6 +78,8 @@ LCS_API const char* lcs_version(void);
 LCS_API int lcs_device_check(int device);
 /* Text of the last error recorded on this thread (host pointer, static storage). */
 LCS_API const char* lcs_last_error(void);
+/* Number of kernels this library has launched in this process (all threads). */
+LCS_API uint64_t lcs_launch_count(void);
 
 /* ------------------------------------------------------------------------------------------
  * LBVH  (replaces class LBVH, Solver/CollisionDetector/lbvh.h:166-229)
@@ -239,6 +241,84 @@ LCS_API int lcs_pcg_solve(lcs_pcg* p, const float* diag, const lcs_bsr* A, const
                   const float* b, float* x, const lcs_pcg_opts* opts, lcs_pcg_stats* stats,
                   lcs_stream stream);
 LCS_API const lcs_pcg_stats* lcs_pcg_device_stats(const lcs_pcg* p);
+
+/* ------------------------------------------------------------------------------------------
+ * Newton loop  (replaces NewtonSolver::physics_step_GPU and its contact glue,
+ * Solver/SimulationSolver/newton_solver.cpp:3174-3375, 3685-3884, 4051-4345)
+ * ------------------------------------------------------------------------------------------ */
+typedef struct lcs_scene_desc {
+    uint32_t n_verts, n_faces, n_edges, n_bending;
+    const float* x;             /* host float4 per vertex: rest = initial positions */
+    const float* v;             /* host float4 per vertex, or NULL (at rest) */
+    const uint32_t* faces;      /* host uint4 */
+    const uint32_t* edges;      /* host uint2 (springs and the edge tree) */
+    const uint32_t* bending;    /* host uint4 stencils (e0, e1, opposite of face 0, of face 1) */
+    const float* bending_Q;     /* host 16 floats per stencil (init_sim_data.cpp:455-480) */
+    const float* rest_len;      /* host, per edge */
+    const float* vert_area;     /* host, per vertex (init_mesh_data.cpp:780-870) */
+    const float* face_area;
+    const float* edge_area;
+    const float* mass;          /* host, per vertex */
+    const float* d_hat;         /* host, per vertex (init_collision_data.cpp:67-171) */
+    const float* offset;        /* host, per vertex */
+    const uint32_t* body;       /* host affine-body id per vertex, or NULL (all soft) */
+    const uint8_t* pinned;      /* host, or NULL */
+    const int8_t* anim_group;   /* host, per vertex animation group of pinned vertices (-1 none) */
+    uint32_t n_anim;
+    const float* anim;          /* host, 8 floats per group: centre xyz, axis xyz, rad/s, pad */
+    float dt;
+    float gravity[3];
+    float kappa;                /* stiffness_collision */
+    float spring_k;             /* stiffness_spring */
+    float bending_k;            /* area_bending_stiffness */
+    float dirichlet;            /* stiffness_dirichlet */
+    float damping;              /* damping_cloth */
+    int32_t use_floor;
+    float floor_y;
+    int32_t nonlinear_iters;    /* nonlinear_iter_count */
+    int32_t pcg_max_iter;       /* pcg_iter_count */
+    float pcg_rel_tol;
+    float pcg_abs_rz_tol;
+    int32_t pcg_check_every;    /* host check cadence of the plain loop (reference: 25) */
+} lcs_scene_desc;
+
+enum {
+    LCS_NEWTON_PLAIN = 1,   /* the reference's dispatch structure (one-scene comparator) */
+    LCS_NEWTON_FP64 = 2,    /* precision form: FP64 PCG reductions, FP64-checked final ACCD distance */
+    LCS_NEWTON_PROFILE = 4  /* per-phase CUDA-event timing (lcs_newton_profile) */
+};
+
+typedef struct lcs_newton_stats {
+    int32_t newton_iters;
+    int32_t pcg_iters;
+    float last_toi;
+    float last_rel_residual;
+    uint32_t vf_candidates, ee_candidates, contact_pairs, ccd_vf_candidates, ccd_ee_candidates;
+    int32_t status;
+} lcs_newton_stats;
+
+typedef struct lcs_newton lcs_newton;
+/* NewtonSolver::init_solver (newton_solver.h:31-51): uploads the scene, builds the material
+ * block pattern, allocates the contact buffers (CollisionData sizing, collision_data.h:445-485).
+ * stream: the stream all work of this solver goes to (NULL: the solver creates one). */
+LCS_API int lcs_newton_create(const lcs_scene_desc* desc, int flags, lcs_stream stream, lcs_newton** out);
+LCS_API int lcs_newton_destroy(lcs_newton* h);
+/* NewtonSolver::physics_step_GPU (newton_solver.cpp:4051-4345) on the device-resident state. */
+LCS_API int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats);
+/* The same step with host positions / velocities in and out (float4 per vertex, any may be NULL). */
+LCS_API int lcs_newton_step_host(lcs_newton* h, const float* x_in, const float* v_in, float* x_out, float* v_out,
+                                 lcs_newton_stats* stats);
+/* Copies the positions / velocities (float4 per vertex) to host buffers; either may be NULL.
+ * Synchronises the solver's stream. */
+LCS_API int lcs_newton_download(const lcs_newton* h, float* x_out, float* v_out);
+/* Device pointers of the solver's positions and velocities (float4 per vertex). */
+LCS_API int lcs_newton_state(const lcs_newton* h, float** d_x, float** d_v);
+/* Accumulated per-phase GPU time (LCS_NEWTON_PROFILE): build, material, DCD broad, DCD narrow,
+ * assembly, PCG, CCD broad, CCD narrow, apply -- and how many times each ran. */
+LCS_API int lcs_newton_profile(const lcs_newton* h, double* phase_ms, int32_t* launches, int n);
+LCS_API int lcs_newton_reset_profile(lcs_newton* h);
+LCS_API int lcs_newton_counts(const lcs_newton* h, uint32_t* nnz_material, uint32_t* cap_vf, uint32_t* cap_ee,
+                              uint32_t* cap_pairs);
 
 #ifdef __cplusplus
 }

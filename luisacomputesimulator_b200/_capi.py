@@ -37,6 +37,25 @@ class PcgOpts(C.Structure):
                 ("check_every", C.c_int32), ("flags", C.c_int32)]
 
 
+class SceneDesc(C.Structure):
+    _fields_ = [("n_verts", C.c_uint32), ("n_faces", C.c_uint32), ("n_edges", C.c_uint32), ("n_bending", C.c_uint32),
+                ("x", P), ("v", P), ("faces", P), ("edges", P), ("bending", P), ("bending_Q", P), ("rest_len", P),
+                ("vert_area", P), ("face_area", P), ("edge_area", P), ("mass", P), ("d_hat", P), ("offset", P),
+                ("body", P), ("pinned", P), ("anim_group", P), ("n_anim", C.c_uint32), ("anim", P),
+                ("dt", C.c_float), ("gravity", C.c_float * 3), ("kappa", C.c_float), ("spring_k", C.c_float),
+                ("bending_k", C.c_float), ("dirichlet", C.c_float), ("damping", C.c_float),
+                ("use_floor", C.c_int32), ("floor_y", C.c_float), ("nonlinear_iters", C.c_int32),
+                ("pcg_max_iter", C.c_int32), ("pcg_rel_tol", C.c_float), ("pcg_abs_rz_tol", C.c_float),
+                ("pcg_check_every", C.c_int32)]
+
+
+class NewtonStats(C.Structure):
+    _fields_ = [("newton_iters", C.c_int32), ("pcg_iters", C.c_int32), ("last_toi", C.c_float),
+                ("last_rel_residual", C.c_float), ("vf_candidates", C.c_uint32), ("ee_candidates", C.c_uint32),
+                ("contact_pairs", C.c_uint32), ("ccd_vf_candidates", C.c_uint32),
+                ("ccd_ee_candidates", C.c_uint32), ("status", C.c_int32)]
+
+
 class PcgStats(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("rel_residual", C.c_float), ("dot_rz", C.c_float),
                 ("status", C.c_int32)]
@@ -47,6 +66,7 @@ SIGNATURES = {
     "lcs_version": (C.c_char_p, []),
     "lcs_device_check": (I32, [I32]),
     "lcs_last_error": (C.c_char_p, []),
+    "lcs_launch_count": (C.c_uint64, []),
     "lcs_bvh_create": (I32, [I32, U32, C.POINTER(P)]),
     "lcs_bvh_destroy": (I32, [P]),
     "lcs_bvh_reduce_aabb": (I32, [P, P, P, U32, P]),
@@ -75,7 +95,19 @@ SIGNATURES = {
     "lcs_pcg_destroy": (I32, [P]),
     "lcs_pcg_solve": (I32, [P, P, C.POINTER(Bsr), C.POINTER(Bsr), P, P, C.POINTER(PcgOpts), C.POINTER(PcgStats), P]),
     "lcs_pcg_device_stats": (P, [P]),
+    "lcs_newton_create": (I32, [C.POINTER(SceneDesc), I32, P, C.POINTER(P)]),
+    "lcs_newton_destroy": (I32, [P]),
+    "lcs_newton_step": (I32, [P, C.POINTER(NewtonStats)]),
+    "lcs_newton_step_host": (I32, [P, P, P, P, P, C.POINTER(NewtonStats)]),
+    "lcs_newton_state": (I32, [P, C.POINTER(P), C.POINTER(P)]),
+    "lcs_newton_download": (I32, [P, P, P]),
+    "lcs_newton_profile": (I32, [P, C.POINTER(C.c_double), C.POINTER(C.c_int32), I32]),
+    "lcs_newton_reset_profile": (I32, [P]),
+    "lcs_newton_counts": (I32, [P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                C.POINTER(C.c_uint32)]),
 }
+LCS_NEWTON_PLAIN, LCS_NEWTON_FP64, LCS_NEWTON_PROFILE = 1, 2, 4
+PHASES = ["build", "material", "dcd_broad", "dcd_narrow", "assembly", "pcg", "ccd_broad", "ccd_narrow", "apply"]
 
 _lib = None
 

@@ -1,6 +1,7 @@
 // capi.cu -- library-level C-ABI entry points (version, device check, error text).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 
@@ -8,7 +9,12 @@
 
 namespace {
 thread_local char g_last_error[512] = "";
+std::atomic<unsigned long long> g_launches{0};
 }
+
+void lcs_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+extern "C" uint64_t lcs_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int lcs_fail(int code, const char* msg)
 {

@@ -9,7 +9,9 @@
 // demand by lcs_bvh_export for tests and interop.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <new>
+#include <vector>
 
 #include "lcs_common.cuh"
 #include "lcs_internal.h"
@@ -496,9 +498,11 @@ extern "C" int lcs_bvh_reduce_aabb(lcs_bvh* h, const float* x, const uint32_t* e
     cudaStream_t s = (cudaStream_t)stream;
     k_reduce_pass1<<<h->nb, 256, 0, s>>>(h->kind, reinterpret_cast<const float4*>(x), elems, h->n, h->centers,
                                          h->block_aabb);
+    lcs_count_launch();
     uint32_t nb_verts = (n_verts + 255) / 256;
     uint32_t cover = nb_verts < h->nb ? nb_verts : h->nb;
     k_reduce_pass2<<<1, 256, 0, s>>>(h->block_aabb, cover, h->gaabb);
+    lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }
@@ -510,18 +514,58 @@ extern "C" int lcs_bvh_construct(lcs_bvh* h, lcs_stream stream)
     cudaStream_t s = (cudaStream_t)stream;
     const int g = grid_for(h->n, 256);
     k_mortons<<<g, 256, 0, s>>>(h->centers, h->gaabb, h->n, h->m30, h->keys, h->vals);
+    lcs_count_launch();
     bool alt = rs::sort_pairs<uint32_t>(h->keys, h->vals, h->keys_alt, h->vals_alt, nullptr, h->n, h->n, 0, 30,
                                         h->hist, s);
     h->m30_sorted = alt ? h->keys_alt : h->keys;
     h->sgo = alt ? h->vals_alt : h->vals;
     k_apply_sorted<<<g, 256, 0, s>>>(h->m30_sorted, h->sgo, h->n, h->ms64, h->children, h->parent, h->healthy);
+    lcs_count_launch();
     if (h->ni > 0) {
         const int gi = grid_for(h->ni, 256);
         k_build_inner<<<gi, 256, 0, s>>>(h->ms64, h->sgo, h->n, h->parent, h->children, h->slot, h->wide);
+        lcs_count_launch();
         k_check<<<gi, 256, 0, s>>>(h->children, h->parent, h->ni, h->healthy);
+        lcs_count_launch();
     } else {
         cudaMemcpyAsync(h->slot, &kInvalid, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
     }
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+int lcs_bvh_construct_host_sort(lcs_bvh* h, lcs_stream stream)
+{
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_construct_host_sort: null handle");
+    if (h->n == 0) return LCS_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    k_mortons<<<grid_for(h->n, 256), 256, 0, s>>>(h->centers, h->gaabb, h->n, h->m30, h->keys, h->vals);
+    lcs_count_launch();
+    std::vector<uint32_t> m(h->n), idx(h->n);
+    LCS_CUDA_TRY(cudaMemcpyAsync(m.data(), h->m30, 4 * (size_t)h->n, cudaMemcpyDeviceToHost, s));
+    LCS_CUDA_TRY(cudaStreamSynchronize(s));
+    for (uint32_t i = 0; i < h->n; ++i) idx[i] = i;
+    std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) {
+        const uint64_t ka = ((uint64_t)m[a] << 32) | a, kb = ((uint64_t)m[b] << 32) | b;
+        return ka < kb;
+    });
+    std::vector<uint32_t> ms(h->n);
+    for (uint32_t i = 0; i < h->n; ++i) ms[i] = m[idx[i]];
+    h->m30_sorted = h->keys;
+    h->sgo = h->vals;
+    LCS_CUDA_TRY(cudaMemcpyAsync(h->m30_sorted, ms.data(), 4 * (size_t)h->n, cudaMemcpyHostToDevice, s));
+    LCS_CUDA_TRY(cudaMemcpyAsync(h->sgo, idx.data(), 4 * (size_t)h->n, cudaMemcpyHostToDevice, s));
+    const int g = grid_for(h->n, 256);
+    k_apply_sorted<<<g, 256, 0, s>>>(h->m30_sorted, h->sgo, h->n, h->ms64, h->children, h->parent, h->healthy);
+    lcs_count_launch();
+    if (h->ni > 0) {
+        const int gi = grid_for(h->ni, 256);
+        k_build_inner<<<gi, 256, 0, s>>>(h->ms64, h->sgo, h->n, h->parent, h->children, h->slot, h->wide);
+        lcs_count_launch();
+        k_check<<<gi, 256, 0, s>>>(h->children, h->parent, h->ni, h->healthy);
+        lcs_count_launch();
+    }
+    LCS_CUDA_TRY(cudaStreamSynchronize(s));  // host buffers go out of scope
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }
@@ -537,6 +581,7 @@ static int leaves_refit(lcs_bvh* h, const float* thickness, const float* x0, con
                                                        reinterpret_cast<const float4*>(x0),
                                                        reinterpret_cast<const float4*>(x1), elems, h->wide,
                                                        h->counters, h->healthy, write_leaf, climb);
+    lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }
@@ -568,6 +613,7 @@ extern "C" int lcs_bvh_query_vf(const lcs_bvh* t, const float* x0, const float* 
     k_query<false><<<grid_for(n_verts, 128, 16), 128, 0, (cudaStream_t)stream>>>(
         t->wide, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1), nullptr, n_verts,
         d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count);
+    lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }
@@ -584,6 +630,7 @@ extern "C" int lcs_bvh_query_ee(const lcs_bvh* t, const float* x0, const float* 
         t->wide, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
         reinterpret_cast<const uint2*>(edges), n_edges, d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity,
         d_count);
+    lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }
@@ -612,7 +659,10 @@ extern "C" int lcs_bvh_export(const lcs_bvh* h, uint32_t* parent, uint32_t* chil
     if (morton_sorted) LCS_CUDA_TRY(cudaMemcpyAsync(morton_sorted, h->ms64, 8 * (size_t)h->n, cudaMemcpyDeviceToDevice, s));
     if (sorted_get_original) LCS_CUDA_TRY(cudaMemcpyAsync(sorted_get_original, h->sgo, 4 * (size_t)h->n, cudaMemcpyDeviceToDevice, s));
     if (global_aabb6) LCS_CUDA_TRY(cudaMemcpyAsync(global_aabb6, h->gaabb, 24, cudaMemcpyDeviceToDevice, s));
-    if (object_idx || morton || node_aabb) k_export<<<grid_for(nn, 256), 256, 0, s>>>(*h, object_idx, morton, node_aabb);
+    if (object_idx || morton || node_aabb) {
+        k_export<<<grid_for(nn, 256), 256, 0, s>>>(*h, object_idx, morton, node_aabb);
+        lcs_count_launch();
+    }
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }

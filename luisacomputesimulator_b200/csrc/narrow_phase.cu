@@ -447,16 +447,20 @@ extern "C" int lcs_contact_offdiag_bsr(lcs_assembler* a, const lcs_pair* pairs, 
     const uint32_t tcap = 12u * capacity;
     k_trip_keys<<<grid_for(capacity, 256), 256, 0, s>>>(pairs, d_count, capacity, a->bits, a->n_rows, a->keys,
                                                         a->vals, a->d_ntrip);
+    lcs_count_launch();
     const bool alt = rs::sort_pairs<uint64_t>(a->keys, a->vals, a->keys_alt, a->vals_alt, a->d_ntrip, 0, tcap, 0,
                                               2 * a->bits, a->hist, s);
     const uint64_t* keys = alt ? a->keys_alt : a->keys;
     const uint32_t* vals = alt ? a->vals_alt : a->vals;
     const int g = grid_for(tcap, 256);
     k_heads<<<g, 256, 0, s>>>(keys, a->d_ntrip, tcap, a->bits, a->n_rows, a->flags);
+    lcs_count_launch();
     scan::exclusive_u32(a->flags, a->excl, a->d_ntrip, tcap, a->scan_tmp, s);
     k_segments<<<g, 256, 0, s>>>(keys, vals, a->flags, a->excl, a->d_ntrip, tcap, a->bits, a->n_rows, pairs, a->col,
                                  a->brow, a->val, a->d_nnzb);
+    lcs_count_launch();
     k_row_ptr<<<grid_for(a->n_rows + 1, 256), 256, 0, s>>>(a->brow, a->d_nnzb, a->n_rows, a->row_ptr);
+    lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }
@@ -497,6 +501,7 @@ extern "C" int lcs_ccd_vf(const uint32_t* pairs, const uint32_t* d_count, uint32
     k_ccd<false><<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
         reinterpret_cast<const uint2*>(pairs), d_count, capacity, reinterpret_cast<const float4*>(x0),
         reinterpret_cast<const float4*>(x1), faces, body, offset, d_toi, toi_per_pair, (flags & LCS_CCD_FP64_FINAL) != 0);
+    lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }
@@ -511,6 +516,7 @@ extern "C" int lcs_ccd_ee(const uint32_t* pairs, const uint32_t* d_count, uint32
     k_ccd<true><<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
         reinterpret_cast<const uint2*>(pairs), d_count, capacity, reinterpret_cast<const float4*>(x0),
         reinterpret_cast<const float4*>(x1), edges, body, offset, d_toi, toi_per_pair, (flags & LCS_CCD_FP64_FINAL) != 0);
+    lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }
@@ -528,6 +534,7 @@ extern "C" int lcs_dcd_vf(const uint32_t* pairs, const uint32_t* d_count, uint32
         reinterpret_cast<const uint2*>(pairs), d_count, capacity, reinterpret_cast<const float4*>(x),
         reinterpret_cast<const uint4*>(faces), body, vert_area, face_area, d_hat, offset, kappa, out, out_capacity,
         d_out_count);
+    lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }
@@ -544,6 +551,7 @@ extern "C" int lcs_dcd_ee(const uint32_t* pairs, const uint32_t* d_count, uint32
     k_dcd_ee<<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
         reinterpret_cast<const uint2*>(pairs), d_count, capacity, reinterpret_cast<const float4*>(x),
         reinterpret_cast<const uint2*>(edges), body, edge_area, d_hat, offset, kappa, out, out_capacity, d_out_count);
+    lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }
@@ -554,6 +562,7 @@ extern "C" int lcs_contact_grad_diag(const lcs_pair* pairs, const uint32_t* d_co
     if (!d_count || !b || !diag || (capacity && !pairs)) return lcs_fail(LCS_ERR_INVALID, "lcs_contact_grad_diag: bad argument");
     if (capacity == 0) return LCS_OK;
     k_grad_diag<<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(pairs, d_count, capacity, b, diag);
+    lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }
@@ -566,6 +575,7 @@ extern "C" int lcs_contact_energy(const lcs_pair* pairs, const uint32_t* d_count
     if (capacity == 0) return LCS_OK;
     k_energy<<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
         pairs, d_count, capacity, reinterpret_cast<const float4*>(x), d_hat, offset, d_energy);
+    lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }

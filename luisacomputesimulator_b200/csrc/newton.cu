@@ -1,0 +1,890 @@
+// newton.cu -- the Newton loop around the contact path (NewtonSolver::physics_step_GPU,
+// Solver/SimulationSolver/newton_solver.cpp:4051-4345) and the glue the reference keeps in
+// NewtonSolver: broad/narrow phase drivers with resize-and-retry, CCD line search, apply dx
+// (newton_solver.cpp:3174-3375, 3685-3884), plus the per-vertex producers that feed it
+// (inertia with Dirichlet pinning, edge springs, quadratic bending; newton_solver.cpp:819-851,
+// 1003-1175; init_sim_data.cpp:455-480).
+//
+// Two executions of the same algorithm:
+//  * fused (default): device Morton sort, leaf update fused with the refit, candidate and pair
+//    counts kept on the device, the whole PCG solve in one persistent launch, and a single
+//    host synchronisation per Newton iteration (a 64-byte status read from pinned memory);
+//    a capacity overflow anywhere in the iteration is detected there and the iteration is
+//    re-run with grown buffers;
+//  * plain (LCS_NEWTON_PLAIN): the reference's dispatch structure -- host Morton sort,
+//    separate leaf-update and refit launches, one kernel per PCG operation with a host check
+//    of r.z every check_every iterations, and the reference's host read-backs (broad counts,
+//    narrow counts, adjacency prescan, triplet sort, TOI, positions) -- used as the
+//    one-scene-at-a-time GPU comparator.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <utility>
+#include <vector>
+
+#include "lcs_common.cuh"
+#include "lcs_internal.h"
+
+using namespace lcs;
+
+namespace {
+
+struct Status {
+    uint32_t cnt[6];  // 0 DCD vf, 1 DCD ee, 2 contact pairs, 3 CCD vf, 4 CCD ee, 5 spare
+    float toi;
+    float max_dx;     // max_v |dx_v| (before the step bound)
+    float dirichlet;  // max over pinned vertices |x - x_tilde| after the step
+    int32_t pcg_iters;
+    float pcg_rel;
+    int32_t pcg_status;
+    float pad[4];
+};
+
+struct Anim {
+    float cx, cy, cz, ax, ay, az, omega, pad;
+};
+
+__device__ __forceinline__ void atomic_max_pos(float* a, float v) { atomicMax(reinterpret_cast<int*>(a), __float_as_int(v)); }
+
+__global__ void k_reset_status(Status* s)
+{
+    if (threadIdx.x < 6) s->cnt[threadIdx.x] = 0;
+    if (threadIdx.x == 0) {
+        s->toi = 1.0f;
+        s->max_dx = 0.0f;
+        s->dirichlet = 0.0f;
+    }
+}
+
+// targets of animated pinned vertices: rotation of the rest position about an axis
+__global__ void k_targets(uint32_t n, const float4* __restrict__ rest, const int8_t* __restrict__ group,
+                          const Anim* __restrict__ anim, float t, float4* __restrict__ target)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 p = rest[i];
+        const int g = group ? group[i] : -1;
+        if (g >= 0) {
+            const Anim A = anim[g];
+            const float ang = A.omega * t;
+            const float c = cosf(ang), s = sinf(ang);
+            const float px = p.x - A.cx, py = p.y - A.cy, pz = p.z - A.cz;
+            const float d = A.ax * px + A.ay * py + A.az * pz;
+            const float kx = A.ay * pz - A.az * py, ky = A.az * px - A.ax * pz, kz = A.ax * py - A.ay * px;
+            p.x = A.cx + px * c + kx * s + A.ax * d * (1.0f - c);
+            p.y = A.cy + py * c + ky * s + A.ay * d * (1.0f - c);
+            p.z = A.cz + pz * c + kz * s + A.az * d * (1.0f - c);
+        }
+        target[i] = p;
+    }
+}
+
+// physics_step_prev_operation + fn_predict_position (solver_interface.cpp:130-162,
+// newton_solver.cpp:576-604): pinned vertices get v = (target - x) / dt
+__global__ void k_predict(uint32_t n, float dt, float gx, float gy, float gz, const uint8_t* __restrict__ pinned,
+                          const float4* __restrict__ target, const float4* __restrict__ x, float4* __restrict__ v,
+                          float4* __restrict__ x_step_start, float4* __restrict__ x_tilde)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 xp = x[i];
+        float4 vp = v[i];
+        float3 vpred;
+        if (pinned && pinned[i]) {
+            const float4 tg = target[i];
+            vp = make_float4((tg.x - xp.x) / dt, (tg.y - xp.y) / dt, (tg.z - xp.z) / dt, 0.0f);
+            v[i] = vp;
+            vpred = make_float3(vp.x, vp.y, vp.z);
+        } else {
+            vpred = make_float3(vp.x + dt * gx, vp.y + dt * gy, vp.z + dt * gz);
+        }
+        x_step_start[i] = xp;
+        x_tilde[i] = make_float4(xp.x + dt * vpred.x, xp.y + dt * vpred.y, xp.z + dt * vpred.z, 0.0f);
+    }
+}
+
+// fn_evaluate_inertia (+ fn_evaluate_ground_collision when the floor is on), newton_solver.cpp:819-951;
+// also x_iter_start = x and dx = 0
+__global__ void k_inertia(uint32_t n, float h, float dirichlet, const float* __restrict__ mass,
+                          const uint8_t* __restrict__ pinned, const float4* __restrict__ x,
+                          const float4* __restrict__ x_tilde, float4* __restrict__ x_iter_start, float4* __restrict__ b,
+                          float4* __restrict__ diag, int use_floor, float floor_y, float kappa,
+                          const float* __restrict__ vert_area, const float* __restrict__ dhat,
+                          const float* __restrict__ offset)
+{
+    const float h2inv = 1.0f / (h * h);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 xk = x[i], xt = x_tilde[i];
+        const float m = mass[i];
+        const float s = -m * h2inv;
+        float3 g = make_float3(s * (xk.x - xt.x), s * (xk.y - xt.y), s * (xk.z - xt.z));
+        float hd = m * h2inv;
+        const bool fixed = pinned && pinned[i];
+        if (fixed) {
+            g = make_float3(g.x + dirichlet * g.x, g.y + dirichlet * g.y, g.z + dirichlet * g.z);
+            hd = hd + dirichlet * hd;
+        }
+        float hyy = hd;
+        if (use_floor && !fixed) {
+            const float dh = dhat[i], th = offset[i], dist = xk.y - floor_y;
+            if (dist - th < dh) {
+                const float stiff = kappa * vert_area[i];
+                const float d = dist - th;
+                const float k1 = stiff * ((dh - d) * (2.0f * logf(d / dh) - dh / d + 1.0f));
+                const float q = dh / d;
+                const float k2 = stiff * ((q + 2.0f) * q - 2.0f * logf(d / dh) - 3.0f);
+                g.y -= k1;
+                hyy += k2;
+            }
+        }
+        x_iter_start[i] = xk;
+        b[i] = make_float4(g.x, g.y, g.z, 0.0f);
+        diag[3 * i + 0] = make_float4(hd, 0.0f, 0.0f, 0.0f);
+        diag[3 * i + 1] = make_float4(0.0f, hyy, 0.0f, 0.0f);
+        diag[3 * i + 2] = make_float4(0.0f, 0.0f, hd, 0.0f);
+    }
+}
+
+__device__ __forceinline__ void atomic_add3(float4* p, float x, float y, float z)
+{
+    float* f = reinterpret_cast<float*>(p);
+    atomicAdd(f + 0, x);
+    atomicAdd(f + 1, y);
+    atomicAdd(f + 2, z);
+}
+
+// fn_evaluate_spring + its assembly (newton_solver.cpp:1003-1045): projected spring Hessian
+__global__ void k_springs(uint32_t ne, const uint2* __restrict__ edges, const float* __restrict__ rest_len, float k,
+                          const float4* __restrict__ x, float4* b, float4* diag, const uint32_t* __restrict__ slots,
+                          float* mat_val)
+{
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+        const uint2 ed = edges[e];
+        const float4 p0 = x[ed.x], p1 = x[ed.y];
+        const float dx = p0.x - p1.x, dy = p0.y - p1.y, dz = p0.z - p1.z;
+        const float l = fmaxf(sqrtf(dx * dx + dy * dy + dz * dz), 1.19209290E-7f);
+        const float L = rest_len[e];
+        const float C = l - L;
+        const float il = 1.0f / l, il2 = il * il;
+        const float gx = k * dx * il * C, gy = k * dy * il * C, gz = k * dz * il * C;
+        atomic_add3(&b[ed.x], -gx, -gy, -gz);
+        atomic_add3(&b[ed.y], gx, gy, gz);
+        const float a = k * il2, c = k * fmaxf(1.0f - L * il, 0.0f);
+        const float d[3] = {dx, dy, dz};
+        float H[9];
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+            for (int r = 0; r < 3; ++r) H[3 * cc + r] = a * d[r] * d[cc] + c * ((r == cc ? 1.0f : 0.0f) - il2 * d[r] * d[cc]);
+        float* D0 = reinterpret_cast<float*>(diag + 3 * (size_t)ed.x);
+        float* D1 = reinterpret_cast<float*>(diag + 3 * (size_t)ed.y);
+        float* O0 = mat_val + 9 * (size_t)slots[2 * e];
+        float* O1 = mat_val + 9 * (size_t)slots[2 * e + 1];
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                atomicAdd(D0 + 4 * cc + r, H[3 * cc + r]);
+                atomicAdd(D1 + 4 * cc + r, H[3 * cc + r]);
+                atomicAdd(O0 + 3 * cc + r, -H[3 * cc + r]);
+                atomicAdd(O1 + 3 * cc + r, -H[3 * cc + r]);
+            }
+    }
+}
+
+// quadratic bending (init_sim_data.cpp:455-480 Q; newton_solver.cpp:3014-3040) measured from the
+// rest shape: grad_i = k sum_j Q_ij (x_j - X_j), Hessian block (i, j) = k Q_ij I
+__global__ void k_bending(uint32_t nb, const uint4* __restrict__ stencil, const float* __restrict__ Q, float k,
+                          const float4* __restrict__ x, const float4* __restrict__ rest, float4* b, float4* diag,
+                          const uint32_t* __restrict__ slots, float* mat_val)
+{
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nb; s += gridDim.x * blockDim.x) {
+        const uint4 st = stencil[s];
+        const uint32_t v[4] = {st.x, st.y, st.z, st.w};
+        float3 u[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float4 p = x[v[j]], r = rest[v[j]];
+            u[j] = make_float3(p.x - r.x, p.y - r.y, p.z - r.z);
+        }
+        const float* q = Q + 16 * (size_t)s;
+        int t = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            float3 g = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float qij = k * q[4 * i + j];
+                g.x += qij * u[j].x;
+                g.y += qij * u[j].y;
+                g.z += qij * u[j].z;
+                if (i == j) {
+                    float* D = reinterpret_cast<float*>(diag + 3 * (size_t)v[i]);
+                    atomicAdd(D + 0, qij);
+                    atomicAdd(D + 5, qij);
+                    atomicAdd(D + 10, qij);
+                } else {
+                    float* O = mat_val + 9 * (size_t)slots[12 * s + t];
+                    atomicAdd(O + 0, qij);
+                    atomicAdd(O + 4, qij);
+                    atomicAdd(O + 8, qij);
+                    ++t;
+                }
+            }
+            atomic_add3(&b[v[i]], -g.x, -g.y, -g.z);
+        }
+    }
+}
+
+// fn_apply_dx (newton_solver.cpp:491-503) with alpha = 1, and the |dx|_inf of the small-step test
+__global__ void k_apply_unit(uint32_t n, const float4* __restrict__ x0, const float4* __restrict__ dx, float4* __restrict__ x,
+                             Status* st)
+{
+    float m = 0.0f;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 a = x0[i], d = dx[i];
+        x[i] = make_float4(a.x + d.x, a.y + d.y, a.z + d.z, 0.0f);
+        m = fmaxf(m, sqrtf(d.x * d.x + d.y * d.y + d.z * d.z));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    if (lane_id() == 0) atomic_max_pos(&st->max_dx, m);
+}
+
+// apply_final_dx with alpha = the CCD step bound, and the Dirichlet check (newton_solver.cpp:3741-3752, 3858-3882)
+__global__ void k_apply_final(uint32_t n, const float4* __restrict__ x0, const float4* __restrict__ dx,
+                              float4* __restrict__ x, const uint8_t* __restrict__ pinned,
+                              const float4* __restrict__ x_tilde, Status* st)
+{
+    const float alpha = st->toi;
+    float m = 0.0f;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 a = x0[i], d = dx[i];
+        const float4 r = make_float4(a.x + alpha * d.x, a.y + alpha * d.y, a.z + alpha * d.z, 0.0f);
+        x[i] = r;
+        if (pinned && pinned[i]) {
+            const float4 t = x_tilde[i];
+            const float ex = r.x - t.x, ey = r.y - t.y, ez = r.z - t.z;
+            m = fmaxf(m, sqrtf(ex * ex + ey * ey + ez * ez));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    if (lane_id() == 0) atomic_max_pos(&st->dirichlet, m);
+}
+
+// fn_gound_collision_ccd, newton_solver.cpp:952-1000
+__global__ void k_floor_ccd(uint32_t n, const float4* __restrict__ x0, const float4* __restrict__ x,
+                            const float* __restrict__ offset, const uint8_t* __restrict__ pinned, float floor_y,
+                            Status* st)
+{
+    float m = 1.0f;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (pinned && pinned[i]) continue;
+        const float off = offset[i], cy = x[i].y;
+        if (cy - off < floor_y) {
+            const float iy = x0[i].y;
+            m = fminf(m, (iy - off - floor_y) / (iy - cy) / 1.25f);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    if (lane_id() == 0 && m < 1.0f) atomicMin(reinterpret_cast<int*>(&st->toi), __float_as_int(fmaxf(m, 0.0f)));
+}
+
+// fn_update_velocity, newton_solver.cpp:606-633
+__global__ void k_update_velocity(uint32_t n, float dt, float damping, const float4* __restrict__ x,
+                                  const float4* __restrict__ x_step_start, float4* __restrict__ v)
+{
+    const float f = expf(-damping * dt);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 a = x_step_start[i], c = x[i];
+        v[i] = make_float4((c.x - a.x) / dt * f, (c.y - a.y) / dt * f, (c.z - a.z) / dt * f, 0.0f);
+    }
+}
+
+__global__ void k_copy4(uint32_t n, const float4* __restrict__ a, float4* __restrict__ b)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
+}
+
+__global__ void k_pcg_to_status(const lcs_pcg_stats* ps, Status* st)
+{
+    st->pcg_iters = ps->iterations;
+    st->pcg_rel = ps->rel_residual;
+    st->pcg_status = ps->status;
+}
+
+template <typename T>
+cudaError_t dalloc(T*& p, size_t count)
+{
+    return cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * (count ? count : 1));
+}
+
+template <typename T>
+cudaError_t upload(T*& p, const T* host, size_t count)
+{
+    cudaError_t e = dalloc(p, count);
+    if (e == cudaSuccess && host && count) e = cudaMemcpy(p, host, sizeof(T) * count, cudaMemcpyHostToDevice);
+    return e;
+}
+
+}  // namespace
+
+enum { kPhBuild, kPhMaterial, kPhDcdBroad, kPhDcdNarrow, kPhAssembly, kPhPcg, kPhCcdBroad, kPhCcdNarrow, kPhApply, kPhases };
+
+struct lcs_newton {
+    lcs_scene_desc d{};
+    int flags = 0;
+    bool plain = false, fp64 = false, profile = false;
+    uint32_t V = 0, F = 0, E = 0, B = 0;
+    cudaStream_t s = nullptr;
+    bool own_stream = false;
+    // mesh
+    uint4* faces = nullptr;
+    uint2* edges = nullptr;
+    uint4* bend = nullptr;
+    float *Q = nullptr, *rest_len = nullptr, *vert_area = nullptr, *face_area = nullptr, *edge_area = nullptr;
+    float *mass = nullptr, *dhat = nullptr, *offset = nullptr;
+    uint32_t* body = nullptr;
+    uint8_t* pinned = nullptr;
+    int8_t* group = nullptr;
+    Anim* anim = nullptr;
+    float4 *rest = nullptr, *x = nullptr, *v = nullptr, *x_step = nullptr, *x_iter = nullptr, *x_tilde = nullptr;
+    float4 *target = nullptr, *dx = nullptr, *b = nullptr, *diag = nullptr;
+    // material BSR
+    uint32_t nnz_mat = 0;
+    uint32_t *mat_rp = nullptr, *mat_col = nullptr, *spring_slots = nullptr, *bend_slots = nullptr;
+    float* mat_val = nullptr;
+    // contact
+    lcs_bvh *face_tree = nullptr, *edge_tree = nullptr;
+    uint32_t cap_vf = 0, cap_ee = 0, cap_pairs = 0;
+    uint2 *bp_vf = nullptr, *bp_ee = nullptr;
+    lcs_pair* pairs = nullptr;
+    lcs_assembler* asmb = nullptr;
+    lcs_pcg* pcg = nullptr;
+    Status *st = nullptr, *h_st = nullptr;
+    float4 *h_x = nullptr, *h_v = nullptr, *h_x_iter = nullptr;  // pinned host mirrors (plain loop)
+    // bookkeeping
+    double time = 0.0;
+    int64_t total_newton = 0, total_pcg = 0;
+    cudaEvent_t ev[kPhases + 1] = {};
+    double phase_ms[kPhases] = {};
+    int32_t phase_launch_count[kPhases] = {};
+};
+
+namespace {
+
+void free_contact(lcs_newton* h)
+{
+    if (h->bp_vf) cudaFree(h->bp_vf);
+    if (h->bp_ee) cudaFree(h->bp_ee);
+    if (h->pairs) cudaFree(h->pairs);
+    if (h->asmb) lcs_assembler_destroy(h->asmb);
+    h->bp_vf = nullptr;
+    h->bp_ee = nullptr;
+    h->pairs = nullptr;
+    h->asmb = nullptr;
+}
+
+int alloc_contact(lcs_newton* h)
+{
+    free_contact(h);
+    if (dalloc(h->bp_vf, h->cap_vf) != cudaSuccess || dalloc(h->bp_ee, h->cap_ee) != cudaSuccess ||
+        dalloc(h->pairs, h->cap_pairs) != cudaSuccess)
+        return lcs_fail(LCS_ERR_CUDA, "lcs_newton: contact buffer allocation failed");
+    return lcs_assembler_create(h->V, h->cap_pairs, &h->asmb);
+}
+
+// material off-diagonal pattern: springs (both directions) + every ordered pair of each
+// bending stencil; slots of each contribution found by binary search in the sorted rows
+int build_material_pattern(lcs_newton* h, const lcs_scene_desc* d)
+{
+    std::vector<uint64_t> keys;
+    keys.reserve(2 * (size_t)h->E + 12 * (size_t)h->B);
+    for (uint32_t e = 0; e < h->E; ++e) {
+        const uint64_t a = d->edges[2 * e], c = d->edges[2 * e + 1];
+        keys.push_back(a << 32 | c);
+        keys.push_back(c << 32 | a);
+    }
+    for (uint32_t s = 0; s < h->B; ++s)
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j)
+                if (i != j) keys.push_back((uint64_t)d->bending[4 * s + i] << 32 | d->bending[4 * s + j]);
+    std::vector<uint64_t> uniq(keys);
+    std::sort(uniq.begin(), uniq.end());
+    uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+    h->nnz_mat = (uint32_t)uniq.size();
+    std::vector<uint32_t> rp(h->V + 1, 0), col(uniq.size());
+    for (size_t k = 0; k < uniq.size(); ++k) {
+        rp[(uniq[k] >> 32) + 1]++;
+        col[k] = (uint32_t)(uniq[k] & 0xFFFFFFFFu);
+    }
+    for (uint32_t r = 0; r < h->V; ++r) rp[r + 1] += rp[r];
+    auto slot_of = [&](uint64_t key) { return (uint32_t)(std::lower_bound(uniq.begin(), uniq.end(), key) - uniq.begin()); };
+    std::vector<uint32_t> ss(2 * (size_t)h->E), bs(12 * (size_t)h->B);
+    for (size_t k = 0; k < 2 * (size_t)h->E; ++k) ss[k] = slot_of(keys[k]);
+    for (size_t k = 0; k < 12 * (size_t)h->B; ++k) bs[k] = slot_of(keys[2 * (size_t)h->E + k]);
+    if (upload(h->mat_rp, rp.data(), rp.size()) != cudaSuccess || upload(h->mat_col, col.data(), col.size()) != cudaSuccess ||
+        upload(h->spring_slots, ss.data(), ss.size()) != cudaSuccess ||
+        upload(h->bend_slots, bs.data(), bs.size()) != cudaSuccess || dalloc(h->mat_val, 9 * (size_t)h->nnz_mat) != cudaSuccess)
+        return lcs_fail(LCS_ERR_CUDA, "lcs_newton: material pattern upload failed");
+    return LCS_OK;
+}
+
+inline int G(uint64_t n) { return grid_for(n, 256); }
+
+void mark(lcs_newton* h, int phase)
+{
+    if (h->profile) cudaEventRecord(h->ev[phase], h->s);
+}
+
+// counts the plain comparator reads back where the reference does (download_*_count)
+int host_readback(lcs_newton* h)
+{
+    LCS_CUDA_TRY(cudaMemcpyAsync(h->h_st, h->st, sizeof(Status), cudaMemcpyDeviceToHost, h->s));
+    LCS_CUDA_TRY(cudaStreamSynchronize(h->s));
+    return LCS_OK;
+}
+
+// the plain loop's host copies of a position-sized vector (pinned mirror)
+int copy_x_to_host(lcs_newton* h, const float4* src)
+{
+    LCS_CUDA_TRY(cudaMemcpyAsync(h->h_x_iter, src, 16 * (size_t)h->V, cudaMemcpyDeviceToHost, h->s));
+    LCS_CUDA_TRY(cudaStreamSynchronize(h->s));
+    return LCS_OK;
+}
+
+int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint32_t* cnt_vf, uint32_t* cnt_ee)
+{
+    const float* X0 = reinterpret_cast<const float*>(x0);
+    const float* X1 = reinterpret_cast<const float*>(x1);
+    int rc;
+    if (h->plain) {
+        if ((rc = lcs_bvh_update_leaves(h->face_tree, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->faces), h->s))) return rc;
+        if ((rc = lcs_bvh_refit(h->face_tree, h->s))) return rc;
+    } else if ((rc = lcs_bvh_update_refit(h->face_tree, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->faces), h->s))) {
+        return rc;
+    }
+    if ((rc = lcs_bvh_query_vf(h->face_tree, X0, X1, h->V, h->dhat, h->offset, reinterpret_cast<uint32_t*>(h->bp_vf), h->cap_vf, cnt_vf, h->s)))
+        return rc;
+    if (h->plain) {
+        if ((rc = lcs_bvh_update_leaves(h->edge_tree, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->edges), h->s))) return rc;
+        if ((rc = lcs_bvh_refit(h->edge_tree, h->s))) return rc;
+    } else if ((rc = lcs_bvh_update_refit(h->edge_tree, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->edges), h->s))) {
+        return rc;
+    }
+    return lcs_bvh_query_ee(h->edge_tree, X0, X1, reinterpret_cast<const uint32_t*>(h->edges), h->E, h->dhat, h->offset, reinterpret_cast<uint32_t*>(h->bp_ee), h->cap_ee,
+                            cnt_ee, h->s);
+}
+
+bool grow(lcs_newton* h)
+{
+    const Status& s = *h->h_st;
+    bool g = false;
+    const uint32_t need_vf = std::max(s.cnt[0], s.cnt[3]), need_ee = std::max(s.cnt[1], s.cnt[4]);
+    while (need_vf > h->cap_vf) { h->cap_vf *= 2; g = true; }
+    while (need_ee > h->cap_ee) { h->cap_ee *= 2; g = true; }
+    while (s.cnt[2] > h->cap_pairs) { h->cap_pairs *= 2; g = true; }
+    return g;
+}
+
+// one Newton iteration (the body of the loop in physics_step_GPU); returns LCS_OK or an error
+int newton_iteration(lcs_newton* h)
+{
+    const uint32_t V = h->V;
+    const lcs_scene_desc& d = h->d;
+    int rc;
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        mark(h, kPhMaterial);
+        k_reset_status<<<1, 32, 0, h->s>>>(h->st);
+        lcs_count_launch();
+        if (h->plain) {  // x_iter_start copied to the host for host_apply_dx (newton_solver.cpp:4196-4198)
+            if ((rc = copy_x_to_host(h, h->x))) return rc;
+        }
+        k_inertia<<<G(V), 256, 0, h->s>>>(V, d.dt, d.dirichlet, h->mass, h->pinned, h->x, h->x_tilde, h->x_iter, h->b,
+                                          h->diag, d.use_floor, d.floor_y, d.kappa, h->vert_area, h->dhat, h->offset);
+        lcs_count_launch();
+        LCS_CUDA_TRY(cudaMemsetAsync(h->mat_val, 0, 36 * (size_t)h->nnz_mat, h->s));
+        if (h->E) {
+            k_springs<<<G(h->E), 256, 0, h->s>>>(h->E, h->edges, h->rest_len, d.spring_k, h->x, h->b, h->diag,
+                                                 h->spring_slots, h->mat_val);
+            lcs_count_launch();
+        }
+        if (h->B) {
+            k_bending<<<G(h->B), 256, 0, h->s>>>(h->B, h->bend, h->Q, d.bending_k, h->x, h->rest, h->b, h->diag,
+                                                 h->bend_slots, h->mat_val);
+            lcs_count_launch();
+        }
+        // update_contact_set (newton_solver.cpp:4093-4104)
+        mark(h, kPhDcdBroad);
+        if ((rc = broad_phase(h, h->x, h->x, &h->st->cnt[0], &h->st->cnt[1]))) return rc;
+        if (h->plain) {
+            if ((rc = host_readback(h))) return rc;  // download_broadphase_collision_count
+            if (grow(h)) { if ((rc = alloc_contact(h))) return rc; continue; }
+        }
+        mark(h, kPhDcdNarrow);
+        const float* X = reinterpret_cast<const float*>(h->x);
+        if ((rc = lcs_dcd_vf(reinterpret_cast<uint32_t*>(h->bp_vf), &h->st->cnt[0], h->cap_vf, X, reinterpret_cast<const uint32_t*>(h->faces), h->body, h->vert_area,
+                             h->face_area, h->dhat, h->offset, d.kappa, h->pairs, h->cap_pairs, &h->st->cnt[2], h->s)))
+            return rc;
+        if ((rc = lcs_dcd_ee(reinterpret_cast<uint32_t*>(h->bp_ee), &h->st->cnt[1], h->cap_ee, X, reinterpret_cast<const uint32_t*>(h->edges), h->body, h->edge_area, h->dhat,
+                             h->offset, d.kappa, h->pairs, h->cap_pairs, &h->st->cnt[2], h->s)))
+            return rc;
+        if (h->plain) {
+            if ((rc = host_readback(h))) return rc;  // download_narrowphase_collision_count
+            if (grow(h)) { if ((rc = alloc_contact(h))) return rc; continue; }
+        }
+        // evaluate_contact (newton_solver.cpp:4105-4120)
+        mark(h, kPhAssembly);
+        if ((rc = lcs_contact_grad_diag(h->pairs, &h->st->cnt[2], h->cap_pairs, reinterpret_cast<float*>(h->b),
+                                        reinterpret_cast<float*>(h->diag), h->s)))
+            return rc;
+        if ((rc = lcs_contact_offdiag_bsr(h->asmb, h->pairs, &h->st->cnt[2], h->cap_pairs, h->s))) return rc;
+        if (h->plain) {  // prescan + construct adjacency + the two-level triplet sort read back counts 4 times
+            for (int k = 0; k < 4; ++k)
+                if ((rc = host_readback(h))) return rc;
+        }
+        // linear solve
+        mark(h, kPhPcg);
+        lcs_bsr A{h->V, h->mat_rp, h->mat_col, h->mat_val};
+        lcs_bsr Bc;
+        const uint32_t* d_nnzb = nullptr;
+        lcs_assembler_bsr(h->asmb, &Bc, &d_nnzb);
+        lcs_pcg_opts o{d.pcg_max_iter, d.pcg_rel_tol, d.pcg_abs_rz_tol, h->plain ? d.pcg_check_every : 1,
+                       (h->fp64 ? LCS_PCG_FP64_DOTS : 0) | (h->plain ? LCS_PCG_PLAIN : LCS_PCG_NO_STATS)};
+        lcs_pcg_stats ps;
+        rc = lcs_pcg_solve(h->pcg, reinterpret_cast<const float*>(h->diag), h->nnz_mat ? &A : nullptr, &Bc,
+                           reinterpret_cast<const float*>(h->b), reinterpret_cast<float*>(h->dx), &o,
+                           h->plain ? &ps : nullptr, h->s);
+        if (rc != LCS_OK && rc != LCS_ERR_NAN) return rc;
+        k_pcg_to_status<<<1, 1, 0, h->s>>>(lcs_pcg_device_stats(h->pcg), h->st);
+        lcs_count_launch();
+        if (h->plain) {  // device_solve copies cgX to the host at its end (precond_cg.cpp:757-758)
+            if ((rc = copy_x_to_host(h, h->dx))) return rc;
+        }
+        // line_search (newton_solver.cpp:3685-3884): CCD step bound
+        mark(h, kPhCcdBroad);
+        k_apply_unit<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->st);
+        lcs_count_launch();
+        if ((rc = broad_phase(h, h->x_iter, h->x, &h->st->cnt[3], &h->st->cnt[4]))) return rc;
+        if (h->plain) {
+            if ((rc = host_readback(h))) return rc;
+            if (grow(h)) {
+                k_copy4<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->x);
+                lcs_count_launch();
+                if ((rc = alloc_contact(h))) return rc;
+                continue;
+            }
+        }
+        mark(h, kPhCcdNarrow);
+        const float* XI = reinterpret_cast<const float*>(h->x_iter);
+        const int ccd_flags = h->fp64 ? LCS_CCD_FP64_FINAL : 0;
+        if (d.use_floor) {
+            k_floor_ccd<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->x, h->offset, h->pinned, d.floor_y, h->st);
+            lcs_count_launch();
+        }
+            lcs_count_launch();
+        if ((rc = lcs_ccd_vf(reinterpret_cast<uint32_t*>(h->bp_vf), &h->st->cnt[3], h->cap_vf, XI, X, reinterpret_cast<const uint32_t*>(h->faces), h->body, h->offset,
+                             &h->st->toi, nullptr, ccd_flags, h->s)))
+            return rc;
+        if ((rc = lcs_ccd_ee(reinterpret_cast<uint32_t*>(h->bp_ee), &h->st->cnt[4], h->cap_ee, XI, X, reinterpret_cast<const uint32_t*>(h->edges), h->body, h->offset,
+                             &h->st->toi, nullptr, ccd_flags, h->s)))
+            return rc;
+        if (h->plain)
+            if ((rc = host_readback(h))) return rc;  // ccd_get_toi
+        mark(h, kPhApply);
+        k_apply_final<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->pinned, h->x_tilde, h->st);
+        lcs_count_launch();
+        LCS_LAUNCH_CHECK();
+        mark(h, kPhases);
+        if ((rc = host_readback(h))) return rc;  // the one read-back of the fused loop
+        if (h->profile) {
+            for (int p = kPhMaterial; p < kPhases; ++p) {
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, h->ev[p], h->ev[p + 1 < kPhases ? p + 1 : kPhases]);
+                h->phase_ms[p] += ms;
+                h->phase_launch_count[p] += 1;
+            }
+        }
+        if (grow(h)) {  // an overflow anywhere: undo the step and run the iteration again
+            k_copy4<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->x);
+            lcs_count_launch();
+            if ((rc = alloc_contact(h))) return rc;
+            continue;
+        }
+        if (h->h_st->pcg_status == LCS_ERR_NAN) return lcs_fail(LCS_ERR_NAN, "lcs_newton: NaN/Inf in PCG");
+        return LCS_OK;
+    }
+    return lcs_fail(LCS_ERR_CAPACITY, "lcs_newton: buffers kept overflowing");
+}
+
+}  // namespace
+
+extern "C" int lcs_newton_create(const lcs_scene_desc* d, int flags, lcs_stream stream, lcs_newton** out)
+{
+    if (!d || !out || !d->x || !d->faces || !d->edges || !d->mass || !d->d_hat || !d->offset || !d->vert_area ||
+        !d->face_area || !d->edge_area || d->n_verts == 0 || (d->n_bending && (!d->bending || !d->bending_Q)) ||
+        (d->n_edges && !d->rest_len))
+        return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create: incomplete scene description");
+    lcs_newton* h = new (std::nothrow) lcs_newton();
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create: out of host memory");
+    h->d = *d;
+    h->flags = flags;
+    h->plain = (flags & LCS_NEWTON_PLAIN) != 0;
+    h->fp64 = (flags & LCS_NEWTON_FP64) != 0;
+    h->profile = (flags & LCS_NEWTON_PROFILE) != 0;
+    h->V = d->n_verts;
+    h->F = d->n_faces;
+    h->E = d->n_edges;
+    h->B = d->n_bending;
+    if (stream) {
+        h->s = (cudaStream_t)stream;
+    } else {
+        cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking);
+        h->own_stream = true;
+    }
+    const size_t V = h->V;
+    cudaError_t e = cudaSuccess;
+    auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    A(upload(h->faces, reinterpret_cast<const uint4*>(d->faces), h->F));
+    A(upload(h->edges, reinterpret_cast<const uint2*>(d->edges), h->E));
+    A(upload(h->bend, reinterpret_cast<const uint4*>(d->bending), h->B));
+    A(upload(h->Q, d->bending_Q, 16 * (size_t)h->B));
+    A(upload(h->rest_len, d->rest_len, h->E));
+    A(upload(h->vert_area, d->vert_area, V));
+    A(upload(h->face_area, d->face_area, h->F));
+    A(upload(h->edge_area, d->edge_area, h->E));
+    A(upload(h->mass, d->mass, V));
+    A(upload(h->dhat, d->d_hat, V));
+    A(upload(h->offset, d->offset, V));
+    {
+        std::vector<uint32_t> body(V, kInvalid);
+        if (d->body) std::memcpy(body.data(), d->body, 4 * V);
+        A(upload(h->body, body.data(), V));
+    }
+    if (d->pinned) A(upload(h->pinned, d->pinned, V));
+    if (d->anim_group && d->n_anim) {
+        A(upload(h->group, d->anim_group, V));
+        A(upload(h->anim, reinterpret_cast<const Anim*>(d->anim), d->n_anim));
+    }
+    A(upload(h->rest, reinterpret_cast<const float4*>(d->x), V));
+    A(upload(h->x, reinterpret_cast<const float4*>(d->x), V));
+    A(dalloc(h->v, V));
+    if (e == cudaSuccess) e = d->v ? cudaMemcpy(h->v, d->v, 16 * V, cudaMemcpyHostToDevice) : cudaMemset(h->v, 0, 16 * V);
+    A(dalloc(h->x_step, V));
+    A(dalloc(h->x_iter, V));
+    A(dalloc(h->x_tilde, V));
+    A(dalloc(h->target, V));
+    A(dalloc(h->dx, V));
+    A(dalloc(h->b, V));
+    A(dalloc(h->diag, 3 * V));
+    A(dalloc(h->st, 1));
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->h_st), sizeof(Status));
+    if (h->plain) {
+        if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->h_x), 16 * V);
+        if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->h_v), 16 * V);
+        if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->h_x_iter), 16 * V);
+        if (e == cudaSuccess) std::memcpy(h->h_x, d->x, 16 * V);
+        if (e == cudaSuccess) {
+            if (d->v) std::memcpy(h->h_v, d->v, 16 * V);
+            else std::memset(h->h_v, 0, 16 * V);
+        }
+    }
+    if (e != cudaSuccess) {
+        lcs_newton_destroy(h);
+        return lcs_fail(LCS_ERR_CUDA, "lcs_newton_create: allocation failed");
+    }
+    std::memset(h->h_st, 0, sizeof(Status));
+    int rc;
+    if ((rc = build_material_pattern(h, d)) || (rc = lcs_bvh_create(LCS_TREE_FACE, h->F, &h->face_tree)) ||
+        (rc = lcs_bvh_create(LCS_TREE_EDGE, h->E, &h->edge_tree)) || (rc = lcs_pcg_create(h->V, &h->pcg))) {
+        lcs_newton_destroy(h);
+        return rc;
+    }
+    // CollisionData::resize_collision_data_list (collision_data.h:445-485)
+    h->cap_vf = std::max<uint32_t>(4 * h->V, 1024);
+    h->cap_ee = std::max<uint32_t>(4 * h->E, 1024);
+    h->cap_pairs = std::max<uint32_t>(2 * (h->V + h->E), 1024);
+    if ((rc = alloc_contact(h))) {
+        lcs_newton_destroy(h);
+        return rc;
+    }
+    if (h->profile)
+        for (auto& ev : h->ev) cudaEventCreate(&ev);
+    *out = h;
+    return LCS_OK;
+}
+
+extern "C" int lcs_newton_destroy(lcs_newton* h)
+{
+    if (!h) return LCS_OK;
+    if (h->s) cudaStreamSynchronize(h->s);
+    free_contact(h);
+    lcs_bvh_destroy(h->face_tree);
+    lcs_bvh_destroy(h->edge_tree);
+    lcs_pcg_destroy(h->pcg);
+    void* ptrs[] = {h->faces, h->edges, h->bend, h->Q, h->rest_len, h->vert_area, h->face_area, h->edge_area,
+                    h->mass, h->dhat, h->offset, h->body, h->pinned, h->group, h->anim, h->rest, h->x, h->v,
+                    h->x_step, h->x_iter, h->x_tilde, h->target, h->dx, h->b, h->diag, h->mat_rp, h->mat_col,
+                    h->spring_slots, h->bend_slots, h->mat_val, h->st};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (h->h_st) cudaFreeHost(h->h_st);
+    if (h->h_x) cudaFreeHost(h->h_x);
+    if (h->h_v) cudaFreeHost(h->h_v);
+    if (h->h_x_iter) cudaFreeHost(h->h_x_iter);
+    for (auto& ev : h->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (h->own_stream) cudaStreamDestroy(h->s);
+    delete h;
+    return LCS_OK;
+}
+
+extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
+{
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_step: null handle");
+    const lcs_scene_desc& d = h->d;
+    const uint32_t V = h->V;
+    int rc;
+    h->time += d.dt;
+    if (h->plain) {  // physics_step_GPU uploads x_step_start, x and v from the host every step
+        const size_t bytes = 16 * (size_t)V;
+        LCS_CUDA_TRY(cudaMemcpyAsync(h->x_step, h->h_x, bytes, cudaMemcpyHostToDevice, h->s));
+        LCS_CUDA_TRY(cudaMemcpyAsync(h->x, h->h_x, bytes, cudaMemcpyHostToDevice, h->s));
+        LCS_CUDA_TRY(cudaMemcpyAsync(h->v, h->h_v, bytes, cudaMemcpyHostToDevice, h->s));
+        LCS_CUDA_TRY(cudaStreamSynchronize(h->s));
+    }
+    mark(h, kPhBuild);
+    k_targets<<<G(V), 256, 0, h->s>>>(V, h->rest, h->group, h->anim, (float)h->time, h->target);
+    lcs_count_launch();
+    k_predict<<<G(V), 256, 0, h->s>>>(V, d.dt, d.gravity[0], d.gravity[1], d.gravity[2], h->pinned, h->target, h->x,
+                                      h->v, h->x_step, h->x_tilde);
+    lcs_count_launch();
+    // Init LBVH once per step (newton_solver.cpp:4152-4161)
+    const float* XS = reinterpret_cast<const float*>(h->x_step);
+    if ((rc = lcs_bvh_reduce_aabb(h->face_tree, XS, reinterpret_cast<const uint32_t*>(h->faces), V, h->s))) return rc;
+    if ((rc = lcs_bvh_reduce_aabb(h->edge_tree, XS, reinterpret_cast<const uint32_t*>(h->edges), V, h->s))) return rc;
+    if (h->plain) {
+        if ((rc = lcs_bvh_construct_host_sort(h->face_tree, h->s))) return rc;
+        if ((rc = lcs_bvh_construct_host_sort(h->edge_tree, h->s))) return rc;
+    } else {
+        if ((rc = lcs_bvh_construct(h->face_tree, h->s))) return rc;
+        if ((rc = lcs_bvh_construct(h->edge_tree, h->s))) return rc;
+    }
+    if (h->profile) {
+        mark(h, kPhMaterial);
+        cudaEventSynchronize(h->ev[kPhMaterial]);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, h->ev[kPhBuild], h->ev[kPhMaterial]);
+        h->phase_ms[kPhBuild] += ms;
+        h->phase_launch_count[kPhBuild] += 1;
+    }
+    bool global_converged = false, dirichlet_converged = false;
+    int iter = 0, pcg_total = 0;
+    float last_toi = 1.0f, last_rel = 0.0f;
+    for (iter = 0; iter < 100; ++iter) {
+        if (global_converged || (iter >= d.nonlinear_iters && dirichlet_converged)) break;
+        if ((rc = newton_iteration(h))) return rc;
+        const Status& s = *h->h_st;
+        pcg_total += s.pcg_iters;
+        last_toi = s.toi;
+        last_rel = s.pcg_rel;
+        global_converged = s.max_dx < 1e-2f * d.dt;
+        dirichlet_converged = s.dirichlet < 1e-3f;
+    }
+    k_update_velocity<<<G(V), 256, 0, h->s>>>(V, d.dt, d.damping, h->x, h->x_step, h->v);
+    lcs_count_launch();
+    LCS_LAUNCH_CHECK();
+    if (h->plain) {  // x, v copied back to the host at the end of the step
+        const size_t bytes = 16 * (size_t)V;
+        LCS_CUDA_TRY(cudaMemcpyAsync(h->h_x, h->x, bytes, cudaMemcpyDeviceToHost, h->s));
+        LCS_CUDA_TRY(cudaMemcpyAsync(h->h_v, h->v, bytes, cudaMemcpyDeviceToHost, h->s));
+        LCS_CUDA_TRY(cudaStreamSynchronize(h->s));
+    }
+    h->total_newton += iter;
+    h->total_pcg += pcg_total;
+    if (stats) {
+        const Status& s = *h->h_st;
+        stats->newton_iters = iter;
+        stats->pcg_iters = pcg_total;
+        stats->last_toi = last_toi;
+        stats->last_rel_residual = last_rel;
+        stats->vf_candidates = s.cnt[0];
+        stats->ee_candidates = s.cnt[1];
+        stats->contact_pairs = s.cnt[2];
+        stats->ccd_vf_candidates = s.cnt[3];
+        stats->ccd_ee_candidates = s.cnt[4];
+        stats->status = LCS_OK;
+    }
+    return LCS_OK;
+}
+
+extern "C" int lcs_newton_step_host(lcs_newton* h, const float* x_in, const float* v_in, float* x_out, float* v_out,
+                                    lcs_newton_stats* stats)
+{
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_step_host: null handle");
+    const size_t bytes = 16 * (size_t)h->V;
+    if (x_in) LCS_CUDA_TRY(cudaMemcpyAsync(h->x, x_in, bytes, cudaMemcpyHostToDevice, h->s));
+    if (v_in) LCS_CUDA_TRY(cudaMemcpyAsync(h->v, v_in, bytes, cudaMemcpyHostToDevice, h->s));
+    if (h->plain) {
+        if (x_in) std::memcpy(h->h_x, x_in, bytes);
+        if (v_in) std::memcpy(h->h_v, v_in, bytes);
+    }
+    int rc = lcs_newton_step(h, stats);
+    if (rc) return rc;
+    if (x_out) LCS_CUDA_TRY(cudaMemcpyAsync(x_out, h->x, bytes, cudaMemcpyDeviceToHost, h->s));
+    if (v_out) LCS_CUDA_TRY(cudaMemcpyAsync(v_out, h->v, bytes, cudaMemcpyDeviceToHost, h->s));
+    LCS_CUDA_TRY(cudaStreamSynchronize(h->s));
+    return LCS_OK;
+}
+
+extern "C" int lcs_newton_download(const lcs_newton* h, float* x_out, float* v_out)
+{
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_download: null handle");
+    const size_t bytes = 16 * (size_t)h->V;
+    if (x_out) LCS_CUDA_TRY(cudaMemcpyAsync(x_out, h->x, bytes, cudaMemcpyDeviceToHost, h->s));
+    if (v_out) LCS_CUDA_TRY(cudaMemcpyAsync(v_out, h->v, bytes, cudaMemcpyDeviceToHost, h->s));
+    LCS_CUDA_TRY(cudaStreamSynchronize(h->s));
+    return LCS_OK;
+}
+
+extern "C" int lcs_newton_state(const lcs_newton* h, float** d_x, float** d_v)
+{
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_state: null handle");
+    if (d_x) *d_x = reinterpret_cast<float*>(h->x);
+    if (d_v) *d_v = reinterpret_cast<float*>(h->v);
+    return LCS_OK;
+}
+
+extern "C" int lcs_newton_profile(const lcs_newton* h, double* phase_ms, int32_t* launches, int n)
+{
+    if (!h || !phase_ms) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_profile: bad argument");
+    for (int p = 0; p < n && p < kPhases; ++p) {
+        phase_ms[p] = h->phase_ms[p];
+        if (launches) launches[p] = h->phase_launch_count[p];
+    }
+    return LCS_OK;
+}
+
+extern "C" int lcs_newton_reset_profile(lcs_newton* h)
+{
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_reset_profile: null handle");
+    for (int p = 0; p < kPhases; ++p) {
+        h->phase_ms[p] = 0.0;
+        h->phase_launch_count[p] = 0;
+    }
+    return LCS_OK;
+}
+
+extern "C" int lcs_newton_counts(const lcs_newton* h, uint32_t* nnz_material, uint32_t* cap_vf, uint32_t* cap_ee,
+                                 uint32_t* cap_pairs)
+{
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_counts: null handle");
+    if (nnz_material) *nnz_material = h->nnz_mat;
+    if (cap_vf) *cap_vf = h->cap_vf;
+    if (cap_ee) *cap_ee = h->cap_ee;
+    if (cap_pairs) *cap_pairs = h->cap_pairs;
+    return LCS_OK;
+}

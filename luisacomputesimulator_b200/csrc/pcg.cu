@@ -483,6 +483,7 @@ extern "C" int lcs_spmv(uint32_t n, const float* diag, const lcs_bsr* A, const l
     k_spmv<kRowLanes><<<grid_for((uint64_t)n * kRowLanes, 256), 256, 0, (cudaStream_t)stream>>>(
         n, reinterpret_cast<const float4*>(diag), to_bsr(A), to_bsr(B), reinterpret_cast<const float4*>(x),
         reinterpret_cast<float4*>(y));
+    lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }
@@ -496,12 +497,15 @@ static int plain_solve(lcs_pcg* P, const float4* diag, Bsr A, Bsr B, const float
     const int nb = g < kPlainBlocks ? g : kPlainBlocks;
     T* part = reinterpret_cast<T*>(sizeof(T) == 8 ? (void*)P->part : (void*)P->part_f);
     k_plain_init<<<g, 256, 0, s>>>(n, b, diag, x, P->r, P->p, P->minv, P->scal);
+    lcs_count_launch();
     int iter = 0, status = LCS_OK;
     float norm_r0 = 0.0f, norm_r = 0.0f, rz = 0.0f;
     const int check = o.check_every > 0 ? o.check_every : 1;
     for (iter = 0; iter < o.max_iter; ++iter) {
         k_plain_precond<T><<<nb, 256, 0, s>>>(n, P->minv, P->r, P->z, part);
+        lcs_count_launch();
         k_plain_precond2<T><<<1, 256, 0, s>>>(part, nb, P->scal, iter == 0);
+        lcs_count_launch();
         if (iter % check == 0) {
             LCS_CUDA_TRY(cudaMemcpyAsync(P->h_scal, P->scal, 8 * sizeof(float), cudaMemcpyDeviceToHost, s));
             LCS_CUDA_TRY(cudaStreamSynchronize(s));
@@ -513,20 +517,27 @@ static int plain_solve(lcs_pcg* P, const float4* diag, Bsr A, Bsr B, const float
             if (o.rel_tol > 0.0f && norm_r <= o.rel_tol * norm_r0) break;
         }
         k_plain_update_p<<<g, 256, 0, s>>>(n, P->z, P->p, P->scal);
+        lcs_count_launch();
         k_spmv<kRowLanes><<<grid_for((uint64_t)n * kRowLanes, 256), 256, 0, s>>>(n, diag, A, B, P->p, P->q);
+        lcs_count_launch();
         k_plain_dot<T><<<nb, 256, 0, s>>>(n, P->p, P->q, part);
+        lcs_count_launch();
         k_plain_alpha<T><<<1, 256, 0, s>>>(part, nb, P->scal);
+        lcs_count_launch();
         k_plain_step<<<g, 256, 0, s>>>(n, x, P->r, P->p, P->q, P->scal);
+        lcs_count_launch();
     }
     LCS_LAUNCH_CHECK();
     LCS_CUDA_TRY(cudaMemcpyAsync(P->h_scal, P->scal, 8 * sizeof(float), cudaMemcpyDeviceToHost, s));
     LCS_CUDA_TRY(cudaStreamSynchronize(s));
-    if (stats) {
-        stats->iterations = iter;
-        stats->rel_residual = norm_r0 > 0.0f ? P->h_scal[4] / norm_r0 : 0.0f;
-        stats->dot_rz = P->h_scal[1];
-        stats->status = status;
-    }
+    lcs_pcg_stats local;
+    local.iterations = iter;
+    local.rel_residual = norm_r0 > 0.0f ? P->h_scal[4] / norm_r0 : 0.0f;
+    local.dot_rz = P->h_scal[1];
+    local.status = status;
+    if (stats) *stats = local;
+    // keep the device copy of the stats current too (pageable source: staged before return)
+    LCS_CUDA_TRY(cudaMemcpyAsync(P->d_stats, &local, sizeof(local), cudaMemcpyHostToDevice, s));
     return status == LCS_OK ? LCS_OK : lcs_fail(status, "lcs_pcg_solve: NaN/Inf in r.z");
 }
 
@@ -567,6 +578,7 @@ extern "C" int lcs_pcg_solve(lcs_pcg* P, const float* diag, const lcs_bsr* A, co
     void* args[] = {&a};
     LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_fused<kRowLanes>, dim3(P->fused_grid), dim3(256), args,
                                              0, s));
+    lcs_count_launch();
     if (stats && !(o.flags & LCS_PCG_NO_STATS)) {
         LCS_CUDA_TRY(cudaMemcpyAsync(stats, P->d_stats, sizeof(lcs_pcg_stats), cudaMemcpyDeviceToHost, s));
         LCS_CUDA_TRY(cudaStreamSynchronize(s));

@@ -177,8 +177,11 @@ inline bool sort_pairs(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt,
     bool in_alt = false;
     for (int shift = begin_bit; shift < end_bit; shift += 8) {
         upsweep<K><<<grid, kThreads, 0, s>>>(kin, d_n, n_host, cap, shift, hist);
+        lcs_count_launch();
         scan_rows<<<256, kThreads, 0, s>>>(hist, totals, d_n, n_host, cap);
+        lcs_count_launch();
         scatter<K><<<grid, kThreads, 0, s>>>(kin, vin, kout, vout, hist, totals, d_n, n_host, cap, shift);
+        lcs_count_launch();
         K* tk = kin; kin = kout; kout = tk;
         uint32_t* tv = vin; vin = vout; vout = tv;
         in_alt = !in_alt;

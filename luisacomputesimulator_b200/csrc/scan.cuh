@@ -113,8 +113,11 @@ inline void exclusive_u32(const uint32_t* in, uint32_t* out, const uint32_t* d_n
     if (!max_tiles) return;
     const int grid = (int)(max_tiles < 4u * kNumSMs ? max_tiles : 4u * kNumSMs);
     k_tile_sums<<<grid, kThreads, 0, s>>>(in, d_n, cap, tmp);
+    lcs_count_launch();
     k_scan_sums<<<1, kThreads, 0, s>>>(tmp, d_n, cap);
+    lcs_count_launch();
     k_tile_scan<<<grid, kThreads, 0, s>>>(in, out, d_n, cap, tmp);
+    lcs_count_launch();
 }
 
 }  // namespace scan

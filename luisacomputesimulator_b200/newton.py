@@ -1,0 +1,129 @@
+"""Host-side mirror of NewtonSolver (Solver/SimulationSolver/newton_solver.h:29-51) over the C ABI:
+``NewtonSolver(scene).physics_step_GPU()`` advances one time step on the device."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _capi as A
+
+
+def _c(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+class NewtonSolver:
+    """One scene, state resident on the device.
+
+    plain=True selects the reference's dispatch structure (the one-scene comparator);
+    fp64=True the precision form; profile=True per-phase CUDA-event timing.
+    """
+
+    def __init__(self, scene, plain=False, fp64=False, profile=False, nonlinear_iters=3, pcg_max_iter=100,
+                 pcg_rel_tol=1e-4, pcg_abs_rz_tol=1e-10, pcg_check_every=25, damping=2.0, use_floor=False,
+                 floor_y=0.0, stream=None):
+        self.lib = A.load()
+        self.scene = scene
+        sc = scene
+        self._keep = []
+
+        def arr(a, dtype):
+            a = _c(a, dtype)
+            self._keep.append(a)
+            return a.ctypes.data_as(C.c_void_p)
+
+        d = A.SceneDesc()
+        d.n_verts, d.n_faces, d.n_edges, d.n_bending = sc.num_verts, sc.faces.shape[0], sc.edges.shape[0], \
+            sc.bending.shape[0]
+        d.x = arr(sc.x, np.float32)
+        d.v = None
+        d.faces = arr(sc.faces, np.uint32)
+        d.edges = arr(sc.edges, np.uint32)
+        d.bending = arr(sc.bending, np.uint32)
+        d.bending_Q = arr(sc.bending_Q.reshape(-1, 16), np.float32)
+        d.rest_len = arr(sc.rest_len, np.float32)
+        d.vert_area = arr(sc.vert_area, np.float32)
+        d.face_area = arr(sc.face_area, np.float32)
+        d.edge_area = arr(sc.edge_area, np.float32)
+        d.mass = arr(sc.mass, np.float32)
+        d.d_hat = arr(sc.d_hat, np.float32)
+        d.offset = arr(sc.offset, np.float32)
+        d.body = arr(sc.body, np.uint32)
+        d.pinned = arr(sc.pinned, np.uint8)
+        groups = np.full(sc.num_verts, -1, np.int8)
+        anim = np.zeros((max(len(sc.anims), 1), 8), np.float32)
+        for gi, (vids, center, axis, omega) in enumerate(sc.anims):
+            groups[vids] = gi
+            ax = np.asarray(axis, np.float64)
+            ax = ax / np.linalg.norm(ax)
+            anim[gi, :3] = center
+            anim[gi, 3:6] = ax
+            anim[gi, 6] = omega
+        d.anim_group = arr(groups, np.int8)
+        d.n_anim = len(sc.anims)
+        d.anim = arr(anim, np.float32)
+        d.dt = sc.dt
+        d.gravity = (C.c_float * 3)(*sc.gravity)
+        d.kappa, d.spring_k, d.bending_k, d.dirichlet, d.damping = sc.kappa, sc.spring_k, sc.bending_k, \
+            sc.dirichlet, damping
+        d.use_floor, d.floor_y = int(use_floor), floor_y
+        d.nonlinear_iters, d.pcg_max_iter = nonlinear_iters, pcg_max_iter
+        d.pcg_rel_tol, d.pcg_abs_rz_tol, d.pcg_check_every = pcg_rel_tol, pcg_abs_rz_tol, pcg_check_every
+        self.desc = d
+        flags = (A.LCS_NEWTON_PLAIN if plain else 0) | (A.LCS_NEWTON_FP64 if fp64 else 0) | \
+            (A.LCS_NEWTON_PROFILE if profile else 0)
+        s = C.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+        h = C.c_void_p()
+        A.check(self.lib.lcs_newton_create(C.byref(d), flags, s, C.byref(h)), "lcs_newton_create")
+        self.h = h
+        self.plain, self.fp64 = plain, fp64
+        self.stats = A.NewtonStats()
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.lcs_newton_destroy(self.h)
+            self.h = None
+
+    def physics_step_GPU(self):
+        A.check(self.lib.lcs_newton_step(self.h, C.byref(self.stats)), "lcs_newton_step")
+        return self.stats
+
+    step = physics_step_GPU
+
+    def step_host(self, x_in=None, v_in=None, x_out=None, v_out=None):
+        p = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        A.check(self.lib.lcs_newton_step_host(self.h, p(x_in), p(v_in), p(x_out), p(v_out), C.byref(self.stats)),
+                "lcs_newton_step_host")
+        return self.stats
+
+    def state_ptrs(self):
+        x, v = C.c_void_p(), C.c_void_p()
+        A.check(self.lib.lcs_newton_state(self.h, C.byref(x), C.byref(v)), "lcs_newton_state")
+        return x.value, v.value
+
+    def positions(self):
+        """Copy of the device positions, float32 (V, 4); synchronises."""
+        out = np.zeros((self.scene.num_verts, 4), np.float32)
+        A.check(self.lib.lcs_newton_download(self.h, out.ctypes.data_as(C.c_void_p), None), "lcs_newton_download")
+        return out
+
+    def velocities(self):
+        out = np.zeros((self.scene.num_verts, 4), np.float32)
+        A.check(self.lib.lcs_newton_download(self.h, None, out.ctypes.data_as(C.c_void_p)), "lcs_newton_download")
+        return out
+
+    def profile(self):
+        ms = (C.c_double * 9)()
+        n = (C.c_int32 * 9)()
+        A.check(self.lib.lcs_newton_profile(self.h, ms, n, 9), "lcs_newton_profile")
+        return {A.PHASES[i]: (ms[i], n[i]) for i in range(9)}
+
+    def reset_profile(self):
+        A.check(self.lib.lcs_newton_reset_profile(self.h), "lcs_newton_reset_profile")
+
+    def counts(self):
+        v = [C.c_uint32() for _ in range(4)]
+        A.check(self.lib.lcs_newton_counts(self.h, *[C.byref(a) for a in v]), "lcs_newton_counts")
+        return dict(nnz_material=v[0].value, cap_vf=v[1].value, cap_ee=v[2].value, cap_pairs=v[3].value)

@@ -1021,3 +1021,114 @@ int orc_pcg(uint32_t n, const float* diag12, const uint32_t* rp_a, const uint32_
     free(r); free(z); free(p); free(q); free(minv);
     return status;
 }
+
+/* =========================================================================================
+ * Material producers of the Newton loop (inertia + Dirichlet pinning, springs, quadratic
+ * bending relative to rest): newton_solver.cpp:819-851, 1003-1045; init_sim_data.cpp:455-480.
+ * The off-diagonal pattern is fixed per mesh; spring_slots / bend_slots give each
+ * contribution's block.  b = -gradient, diag = 3 float4 columns, val9 column-major.
+ * ========================================================================================= */
+void orc_material_fill(uint32_t V, uint32_t E, uint32_t B, const float* x4, const float* rest4,
+                       const float* xt4, const float* mass, const uint8_t* pinned, float dt,
+                       float dirichlet, const uint32_t* edges, const float* rest_len, float spring_k,
+                       const uint32_t* stencil, const float* Q16, float bending_k,
+                       const uint32_t* spring_slots, const uint32_t* bend_slots, uint32_t nnz,
+                       float* b4, float* diag12, float* val9)
+{
+    const float h2inv = 1.0f / (dt * dt);
+    memset(val9, 0, sizeof(float) * 9 * (size_t)nnz);
+#pragma omp parallel for schedule(static)
+    for (long long il = 0; il < (long long)V; ++il) {
+        size_t i = (size_t)il;
+        float m = mass[i], s = -m * h2inv, hd = m * h2inv;
+        float g[3];
+        for (int k = 0; k < 3; ++k) g[k] = s * (x4[4 * i + k] - xt4[4 * i + k]);
+        if (pinned && pinned[i]) {
+            for (int k = 0; k < 3; ++k) g[k] = g[k] + dirichlet * g[k];
+            hd = hd + dirichlet * hd;
+        }
+        for (int k = 0; k < 3; ++k) b4[4 * i + k] = g[k];
+        b4[4 * i + 3] = 0.0f;
+        for (int k = 0; k < 12; ++k) diag12[12 * i + k] = 0.0f;
+        diag12[12 * i + 0] = hd;
+        diag12[12 * i + 5] = hd;
+        diag12[12 * i + 10] = hd;
+    }
+    for (uint32_t e = 0; e < E; ++e) {
+        uint32_t a = edges[2 * e], c = edges[2 * e + 1];
+        float d[3] = {x4[4 * a] - x4[4 * c], x4[4 * a + 1] - x4[4 * c + 1], x4[4 * a + 2] - x4[4 * c + 2]};
+        float l = sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        if (l < 1.19209290E-7f) l = 1.19209290E-7f;
+        float L = rest_len[e], il = 1.0f / l, il2 = il * il;
+        float C = l - L;
+        for (int k = 0; k < 3; ++k) {
+            float gk = spring_k * d[k] * il * C;
+            b4[4 * a + k] -= gk;
+            b4[4 * c + k] += gk;
+        }
+        float aa = spring_k * il2, cc = spring_k * (1.0f - L * il > 0.0f ? 1.0f - L * il : 0.0f);
+        float* O0 = val9 + 9 * (size_t)spring_slots[2 * e];
+        float* O1 = val9 + 9 * (size_t)spring_slots[2 * e + 1];
+        for (int col = 0; col < 3; ++col)
+            for (int r = 0; r < 3; ++r) {
+                float h = aa * d[r] * d[col] + cc * ((r == col ? 1.0f : 0.0f) - il2 * d[r] * d[col]);
+                diag12[12 * (size_t)a + 4 * col + r] += h;
+                diag12[12 * (size_t)c + 4 * col + r] += h;
+                O0[3 * col + r] -= h;
+                O1[3 * col + r] -= h;
+            }
+    }
+    for (uint32_t s = 0; s < B; ++s) {
+        const uint32_t* v = stencil + 4 * (size_t)s;
+        const float* q = Q16 + 16 * (size_t)s;
+        float u[4][3];
+        for (int j = 0; j < 4; ++j)
+            for (int k = 0; k < 3; ++k) u[j][k] = x4[4 * (size_t)v[j] + k] - rest4[4 * (size_t)v[j] + k];
+        int t = 0;
+        for (int i = 0; i < 4; ++i) {
+            float g[3] = {0.0f, 0.0f, 0.0f};
+            for (int j = 0; j < 4; ++j) {
+                float qij = bending_k * q[4 * i + j];
+                for (int k = 0; k < 3; ++k) g[k] += qij * u[j][k];
+                if (i == j) {
+                    diag12[12 * (size_t)v[i] + 0] += qij;
+                    diag12[12 * (size_t)v[i] + 5] += qij;
+                    diag12[12 * (size_t)v[i] + 10] += qij;
+                } else {
+                    float* O = val9 + 9 * (size_t)bend_slots[12 * (size_t)s + t];
+                    O[0] += qij;
+                    O[4] += qij;
+                    O[8] += qij;
+                    ++t;
+                }
+            }
+            for (int k = 0; k < 3; ++k) b4[4 * (size_t)v[i] + k] -= g[k];
+        }
+    }
+}
+
+/* Smallest unsigned VF / EE distance over candidate pairs (incident pairs skipped): the
+ * post-step penetration check (NewtonSolver::device_post_dist_check, newton_solver.cpp:3364-3375). */
+float orc_min_distance(const uint32_t* vf, uint32_t n_vf, const uint32_t* ee, uint32_t n_ee, const float* x,
+                       const uint32_t* faces, const uint32_t* edges)
+{
+    float best = 3.402823466e+38F;
+#pragma omp parallel for reduction(min : best) schedule(static)
+    for (long long k = 0; k < (long long)n_vf; ++k) {
+        uint32_t v = vf[2 * k], f = vf[2 * k + 1];
+        uint32_t a = faces[4 * (size_t)f], b = faces[4 * (size_t)f + 1], c = faces[4 * (size_t)f + 2];
+        if (v == a || v == b || v == c) continue;
+        float d = sqrtf(pt_dist2_f(ld3(x, v), ld3(x, a), ld3(x, b), ld3(x, c)));
+        if (d < best) best = d;
+    }
+#pragma omp parallel for reduction(min : best) schedule(static)
+    for (long long k = 0; k < (long long)n_ee; ++k) {
+        uint32_t l = ee[2 * k], r = ee[2 * k + 1];
+        uint32_t a0 = edges[2 * (size_t)l], a1 = edges[2 * (size_t)l + 1];
+        uint32_t b0 = edges[2 * (size_t)r], b1 = edges[2 * (size_t)r + 1];
+        if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1) continue;
+        float d = sqrtf(ee_dist2_f(ld3(x, a0), ld3(x, a1), ld3(x, b0), ld3(x, b1)));
+        if (d < best) best = d;
+    }
+    return best;
+}

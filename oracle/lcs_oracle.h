@@ -116,6 +116,17 @@ int orc_pcg(uint32_t n, const float* diag12, const uint32_t* rp_a, const uint32_
             const float* b4, float* x4, int max_iter, float rel_tol, float abs_rz_tol,
             int check_every, int fp64_dots, orc_pcg_stats* stats);
 
+float orc_min_distance(const uint32_t* vf, uint32_t n_vf, const uint32_t* ee, uint32_t n_ee, const float* x,
+                       const uint32_t* faces, const uint32_t* edges);
+
+/* ---------------- material producers of the Newton loop ---------------- */
+void orc_material_fill(uint32_t V, uint32_t E, uint32_t B, const float* x4, const float* rest4,
+                       const float* xt4, const float* mass, const uint8_t* pinned, float dt,
+                       float dirichlet, const uint32_t* edges, const float* rest_len, float spring_k,
+                       const uint32_t* stencil, const float* Q16, float bending_k,
+                       const uint32_t* spring_slots, const uint32_t* bend_slots, uint32_t nnz,
+                       float* b4, float* diag12, float* val9);
+
 #ifdef __cplusplus
 }
 #endif

@@ -78,6 +78,9 @@ def _declare(L):
         "orc_contact_offdiag_bsr": (U32, [P, U32, U32, P, P, P, U32]),
         "orc_contact_energy": (C.c_double, [P, U32, P, P, P, I32]),
         "orc_bsr_spmv": (None, [U32, P, P, P, P, P, P, P, P, P]),
+        "orc_material_fill": (None, [U32, U32, U32, P, P, P, P, P, F32, F32, P, P, F32, P, P, F32, P, P, U32, P, P,
+                                     P]),
+        "orc_min_distance": (F32, [P, U32, P, U32, P, P, P]),
         "orc_pcg": (I32, [U32, P, P, P, P, P, P, P, P, P, I32, F32, F32, I32, I32, C.POINTER(PcgStats)]),
     }
     for name, (res, args) in sig.items():
@@ -315,3 +318,21 @@ def pcg(diag, A, B, b, max_iter=100, rel_tol=1e-4, abs_rz_tol=1e-10, check_every
                   _p(b), _p(x), int(max_iter), float(rel_tol), float(abs_rz_tol), int(check_every),
                   int(fp64_dots), C.byref(st))
     return x, dict(iterations=st.iterations, rel_residual=st.rel_residual, dot_rz=st.dot_rz, status=st.status)
+
+
+def min_distance(sc, x, radius=5e-3):
+    """Smallest VF / EE distance of the mesh at x (candidates within `radius`); > 0 means no
+    intersection (device_post_dist_check, newton_solver.cpp:3364-3375)."""
+    x = f4(x)
+    r = np.full(sc.num_verts, radius, np.float32)
+    z = np.zeros(sc.num_verts, np.float32)
+    tf = lbvh_build(TREE_FACE, x, sc.faces, sc.num_verts)
+    lbvh_refit(tf, x, x, sc.faces, z)
+    vf, _ = lbvh_query_vf(tf, x, x, r, z)
+    te = lbvh_build(TREE_EDGE, x, sc.edges, sc.num_verts)
+    lbvh_refit(te, x, x, sc.edges, z)
+    ee, _ = lbvh_query_ee(te, x, x, sc.edges, r, z)
+    vf = np.ascontiguousarray(vf, np.uint32)
+    ee = np.ascontiguousarray(ee, np.uint32)
+    return lib().orc_min_distance(_p(vf), vf.shape[0], _p(ee), ee.shape[0], _p(x), _p(u4(sc.faces)),
+                                  _p(np.ascontiguousarray(sc.edges, np.uint32)))

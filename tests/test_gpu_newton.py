@@ -1,0 +1,86 @@
+"""Newton loop on the GPU: one iteration against the CPU restatement from the same contact-rich
+state, plain vs fused agreement, and trajectories that stay intersection-free."""
+import numpy as np
+import pytest
+
+from luisacomputesimulator_b200 import scenes as S
+from luisacomputesimulator_b200.newton import NewtonSolver
+from oracle import newton_cpu as N
+from oracle import oracle as O
+from tests import scenarios as SC
+
+pytestmark = pytest.mark.gpu
+
+
+def touching_scene(n=32, gap=5e-4):
+    sc, x = SC.cloth_touching_sphere(gap=gap, n=n)
+    sc.x = x.copy()  # start (and rest) on the sphere, inside d_hat
+    return sc
+
+
+def _predict(sc):
+    x = sc.x.copy()
+    xt = x.copy().astype(np.float32)
+    free = ~sc.pinned.astype(bool)
+    g = np.asarray(sc.gravity, np.float32)
+    # v = 0: x_tilde = x + dt * (dt * g) for free vertices, the rest target for pinned ones
+    xt[free, :3] = x[free, :3] + np.float32(sc.dt) * (np.float32(sc.dt) * g)
+    return x, xt
+
+
+def test_one_newton_iteration_matches_cpu_restatement():
+    sc = touching_scene()
+    gpu = NewtonSolver(sc, plain=True, nonlinear_iters=1, pcg_check_every=25)
+    st = gpu.step()
+    assert st.newton_iters == 1
+    assert st.contact_pairs > 0
+    xg = gpu.positions()
+    x0, xt = _predict(sc)
+    pat = N.MaterialPattern(sc)
+    xc, toi, pst, cnt = N.newton_iteration(sc, x0, xt, sc.dt, pattern=pat)
+    assert cnt["pairs"] == st.contact_pairs
+    assert st.vf_candidates == cnt["vf"] and st.ee_candidates == cnt["ee"]
+    dx_scale = np.abs(xc[:, :3] - x0[:, :3]).max()
+    np.testing.assert_allclose(xg[:, :3], xc[:, :3], rtol=0, atol=2e-3 * dx_scale + 1e-7)
+    assert abs(st.last_toi - toi) <= 1e-3 * toi + 1e-6
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_drop_stays_intersection_free(fp64):
+    sc = S.cloth_on_sphere(n=32)
+    gpu = NewtonSolver(sc, fp64=fp64)
+    d0 = O.min_distance(sc, sc.x)
+    for k in range(40):
+        st = gpu.step()
+        assert st.status == 0
+        if k % 10 == 9:
+            x = gpu.positions()
+            assert np.isfinite(x).all()
+            assert O.min_distance(sc, x) > 0.0
+    x = gpu.positions()
+    assert x[: 32 * 32, 1].min() < sc.x[: 32 * 32, 1].min()  # the cloth did fall
+    assert O.min_distance(sc, x) > 0.0 and d0 > 0.0
+
+
+def test_plain_and_fused_agree_on_a_step():
+    sc = touching_scene()
+    a = NewtonSolver(sc, plain=True, pcg_check_every=1)
+    b = NewtonSolver(sc, plain=False)
+    sa, sb = a.step(), b.step()
+    assert sa.newton_iters == sb.newton_iters
+    xa, xb = a.positions(), b.positions()
+    scale = np.abs(xa[:, :3] - sc.x[:, :3]).max()
+    np.testing.assert_allclose(xa[:, :3], xb[:, :3], rtol=0, atol=5e-3 * scale + 1e-7)
+
+
+def test_twisted_tube_steps_small():
+    # a reduced tube (60 x 60) through the full step path, both modes
+    for plain in (False, True):
+        sc = S.twisted_tube(60, 60)
+        gpu = NewtonSolver(sc, plain=plain)
+        for _ in range(5):
+            st = gpu.step()
+            assert st.newton_iters >= 3
+        x = gpu.positions()
+        assert np.isfinite(x).all()
+        assert O.min_distance(sc, x) > 0.0
