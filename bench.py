@@ -223,7 +223,7 @@ def run_ours(a):
             e1.record(stream)
             e1.synchronize()
             ms = e0.elapsed_time(e1)
-            per_step.append(ms)
+            per_step.append((ms, st.newton_iters, st.retries, st.host_ms))
             ms_total += ms
             newton += st.newton_iters
             pcg += st.pcg_iters
@@ -302,6 +302,9 @@ def run_ours(a):
             "cpu_baseline": cpu,
             "clocks": clocks,
             "newton_iters": newton, "pcg_iters": pcg,
+            "step_ms": {"min": min(p[0] for p in per_step), "median": statistics.median(p[0] for p in per_step),
+                        "max": max(p[0] for p in per_step), "retries": sum(p[2] for p in per_step),
+                        "host_ms_median": statistics.median(p[3] for p in per_step)},
             "phase_ms": {k: round(v[0], 3) for k, v in prof.items()},
             "last_step": last,
         }

@@ -295,6 +295,8 @@ typedef struct lcs_newton_stats {
     float last_rel_residual;
     uint32_t vf_candidates, ee_candidates, contact_pairs, ccd_vf_candidates, ccd_ee_candidates;
     int32_t status;
+    int32_t retries;  /* iterations re-run after a buffer grew */
+    float host_ms;    /* host wall time of the step */
 } lcs_newton_stats;
 
 typedef struct lcs_newton lcs_newton;

@@ -53,7 +53,8 @@ class NewtonStats(C.Structure):
     _fields_ = [("newton_iters", C.c_int32), ("pcg_iters", C.c_int32), ("last_toi", C.c_float),
                 ("last_rel_residual", C.c_float), ("vf_candidates", C.c_uint32), ("ee_candidates", C.c_uint32),
                 ("contact_pairs", C.c_uint32), ("ccd_vf_candidates", C.c_uint32),
-                ("ccd_ee_candidates", C.c_uint32), ("status", C.c_int32)]
+                ("ccd_ee_candidates", C.c_uint32), ("status", C.c_int32), ("retries", C.c_int32),
+                ("host_ms", C.c_float)]
 
 
 class PcgStats(C.Structure):

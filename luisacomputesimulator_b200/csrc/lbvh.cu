@@ -372,6 +372,8 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide, 
             const float4* r = wide + 4 * node;
             const float4 a0 = __ldg(r + 0), a1 = __ldg(r + 1), b0 = __ldg(r + 2), b1 = __ldg(r + 3);
             bool stop = false;
+            uint32_t hit[2];
+            uint32_t nhit = 0;
 #pragma unroll
             for (int side = 0; side < 2; ++side) {
                 const float4 mn = side ? b0 : a0, mx = side ? b1 : a1;
@@ -379,17 +381,25 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide, 
                     const uint32_t code = __float_as_uint(mn.w);
                     if (code & 0x80000000u) {
                         const uint32_t obj = code & 0x7FFFFFFFu;
-                        if (!EE || q < obj) {
-                            const uint32_t s = atomicAdd(d_count, 1u);
-                            if (s < capacity) pairs[s] = make_uint2(q, obj);
-                        }
+                        if (!EE || q < obj) hit[nhit++] = obj;
                     } else if (sp < 32) {
                         stack[sp++] = code;
                     } else {
-                        stop = true;
+                        stop = true;  // a full stack ends the whole traversal (lbvh.cpp:344-351)
                     }
                 }
             }
+            // one warp-aggregated reservation for the (up to two) pairs of this step
+            const uint32_t active = __activemask();
+            const uint32_t lt = (1u << lane_id()) - 1u;
+            const uint32_t one = __ballot_sync(active, nhit >= 1), two = __ballot_sync(active, nhit == 2);
+            const uint32_t total = __popc(one) + __popc(two);
+            const uint32_t leader = __ffs(active) - 1;
+            uint32_t base = 0;
+            if (lane_id() == leader && total) base = atomicAdd(d_count, total);
+            base = __shfl_sync(active, base, leader) + __popc(one & lt) + __popc(two & lt);
+            for (uint32_t k = 0; k < nhit; ++k)
+                if (base + k < capacity) pairs[base + k] = make_uint2(q, hit[k]);
             if (stop) break;
             if (++loop > 100000u) break;
         }

