@@ -242,6 +242,20 @@ LCS_API int lcs_pcg_solve(lcs_pcg* p, const float* diag, const lcs_bsr* A, const
                   lcs_stream stream);
 LCS_API const lcs_pcg_stats* lcs_pcg_device_stats(const lcs_pcg* p);
 
+/* Allocation-free variant of lcs_pcg_solve (fused solve only); it has no counterpart in the
+ * reference.  For callers that cannot allocate device memory while they run: cudaMalloc and
+ * cudaFree synchronise the whole device, which a fixed-latency loop cannot afford, and a host
+ * that gives all device memory to its own pool allocator leaves none to allocate.  Needs no
+ * handle: the working vectors live in one static device array the library reserves when it is
+ * loaded (7.3 MB per GPU, kept until the process exits).  At most 65,536 block rows (larger
+ * systems: LCS_ERR_CAPACITY).  Calls on one device share that array, so calls whose work
+ * overlaps on the GPU race and must be ordered by the caller.  The first call on each device
+ * does a one-time set-up (it looks up the array's device address); make it before any stream
+ * capture.  LCS_PCG_PLAIN is rejected. */
+LCS_API int lcs_pcg_solve_noalloc(uint32_t n, const float* diag, const lcs_bsr* A, const lcs_bsr* B,
+                                  const float* b, float* x, const lcs_pcg_opts* opts, lcs_pcg_stats* stats,
+                                  lcs_stream stream);
+
 /* ------------------------------------------------------------------------------------------
  * Newton loop  (replaces NewtonSolver::physics_step_GPU and its contact glue,
  * Solver/SimulationSolver/newton_solver.cpp:3174-3375, 3685-3884, 4051-4345)

@@ -96,6 +96,8 @@ SIGNATURES = {
     "lcs_pcg_destroy": (I32, [P]),
     "lcs_pcg_solve": (I32, [P, P, C.POINTER(Bsr), C.POINTER(Bsr), P, P, C.POINTER(PcgOpts), C.POINTER(PcgStats), P]),
     "lcs_pcg_device_stats": (P, [P]),
+    "lcs_pcg_solve_noalloc": (I32, [U32, P, C.POINTER(Bsr), C.POINTER(Bsr), P, P, C.POINTER(PcgOpts),
+                                    C.POINTER(PcgStats), P]),
     "lcs_newton_create": (I32, [C.POINTER(SceneDesc), I32, P, C.POINTER(P)]),
     "lcs_newton_destroy": (I32, [P]),
     "lcs_newton_step": (I32, [P, C.POINTER(NewtonStats)]),

@@ -15,6 +15,7 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <new>
 
 #include "lcs_common.cuh"
@@ -584,6 +585,121 @@ extern "C" int lcs_pcg_solve(lcs_pcg* P, const float* diag, const lcs_bsr* A, co
         LCS_CUDA_TRY(cudaMemcpyAsync(stats, P->d_stats, sizeof(lcs_pcg_stats), cudaMemcpyDeviceToHost, s));
         LCS_CUDA_TRY(cudaStreamSynchronize(s));
         if (stats->status != LCS_OK) return lcs_fail(stats->status, "lcs_pcg_solve: fused solve failed");
+    }
+    return LCS_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Allocation-free PCG solve.
+//
+// Some callers cannot allocate device memory at solve time: cudaMalloc / cudaFree synchronise
+// the whole device, which a fixed-latency simulation loop cannot afford, and a host framework
+// that hands the whole GPU to its own pool allocator leaves nothing for a library to
+// cudaMalloc.  lcs_pcg_solve_noalloc runs the same persistent solve as lcs_pcg_solve, but its
+// working vectors live in one file-scope device array, g_pcg_scratch, reserved when the
+// library is loaded (7.3 MB on every GPU that loads it, held until the process exits), so it
+// needs no handle and allocates nothing.
+//
+// Limits and sharing rules:
+//  * at most kNoAllocMaxRows (65,536) block rows; larger systems are rejected with
+//    LCS_ERR_CAPACITY;
+//  * every call on a device shares the one array and leaves the last call's contents in it:
+//    two calls whose work overlaps on the GPU (different streams, or different host threads)
+//    race on it and give wrong results, so the caller must order them;
+//  * the first call on each device resolves the array's device address with
+//    cudaGetSymbolAddress (host code cannot use the symbol itself as a pointer) and caches it;
+//    make that first call before any stream capture.
+// ------------------------------------------------------------------------------------------
+constexpr uint32_t kNoAllocMaxRows = 65536;
+constexpr uint32_t kNoAllocMaxBlocks = 1024;
+constexpr size_t kNaVec = 16ull * kNoAllocMaxRows;              // one float4 per row
+constexpr size_t kNaOffR = 0, kNaOffZ = kNaVec, kNaOffP = 2 * kNaVec, kNaOffQ = 3 * kNaVec;
+constexpr size_t kNaOffMinv = 4 * kNaVec;                        // three float4 per row
+constexpr size_t kNaOffPart = 7 * kNaVec;                        // 3 doubles per block
+constexpr size_t kNaOffBar = kNaOffPart + 24ull * kNoAllocMaxBlocks;
+constexpr size_t kNaOffStats = kNaOffBar + 256;
+constexpr size_t kNaBytes = kNaOffStats + 256;
+
+static __device__ __align__(256) unsigned char g_pcg_scratch[kNaBytes];
+
+namespace {
+struct NoAllocDevice {
+    unsigned char* base = nullptr;
+    int grid = 0;
+};
+std::mutex g_noalloc_mutex;
+NoAllocDevice g_noalloc[64];
+}  // namespace
+
+extern "C" int lcs_pcg_solve_noalloc(uint32_t n, const float* diag, const lcs_bsr* A, const lcs_bsr* B,
+                                     const float* b, float* x, const lcs_pcg_opts* opts, lcs_pcg_stats* stats,
+                                     lcs_stream stream)
+{
+    if (!diag || !b || !x || n == 0) return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_noalloc: bad argument");
+    if (n > kNoAllocMaxRows)
+        return lcs_fail(LCS_ERR_CAPACITY, "lcs_pcg_solve_noalloc: more than 65536 block rows (static scratch limit)");
+    if ((A && A->n_rows != n) || (B && B->n_rows != n))
+        return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_noalloc: row count mismatch");
+    lcs_pcg_opts o = opts ? *opts : lcs_pcg_opts{100, 1e-4f, 1e-10f, 1, 0};
+    if (o.flags & LCS_PCG_PLAIN)
+        return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_noalloc: only the fused solve is allocation-free");
+    if (o.check_every <= 0) o.check_every = 1;
+    int dev = 0;
+    LCS_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_noalloc: device index out of range");
+    NoAllocDevice nd;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc[dev].base) {  // one-time set-up on this device, with it current
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_pcg_scratch) != cudaSuccess || !p)
+                return lcs_fail(LCS_ERR_CUDA, "lcs_pcg_solve_noalloc: cudaGetSymbolAddress failed");
+            int sms = 0, per_sm = 0;
+            LCS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            LCS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_fused<kRowLanes>, kFusedThreads, 0));
+            int grid = sms * (per_sm > 0 ? 1 : 0);
+            if (grid <= 0 || grid > (int)kNoAllocMaxBlocks)
+                return lcs_fail(LCS_ERR_CUDA, "lcs_pcg_solve_noalloc: no co-resident launch shape");
+            g_noalloc[dev].base = static_cast<unsigned char*>(p);
+            g_noalloc[dev].grid = grid;
+        }
+        nd = g_noalloc[dev];
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char* base = nd.base;
+    FusedArgs a;
+    a.n = n;
+    a.diag = reinterpret_cast<const float4*>(diag);
+    a.A = to_bsr(A);
+    a.B = to_bsr(B);
+    a.b = reinterpret_cast<const float4*>(b);
+    a.x = reinterpret_cast<float4*>(x);
+    a.r = reinterpret_cast<float4*>(base + kNaOffR);
+    a.z = reinterpret_cast<float4*>(base + kNaOffZ);
+    a.p = reinterpret_cast<float4*>(base + kNaOffP);
+    a.q = reinterpret_cast<float4*>(base + kNaOffQ);
+    a.minv = reinterpret_cast<float4*>(base + kNaOffMinv);
+    a.part = reinterpret_cast<double*>(base + kNaOffPart);
+    a.bar_count = reinterpret_cast<unsigned*>(base + kNaOffBar);
+    a.bar_gen = reinterpret_cast<unsigned*>(base + kNaOffBar) + 1;
+    a.max_iter = o.max_iter;
+    a.rel_tol = o.rel_tol;
+    a.abs_rz_tol = o.abs_rz_tol;
+    a.check_every = o.check_every;
+    a.fp64 = (o.flags & LCS_PCG_FP64_DOTS) ? 1 : 0;
+    a.stats = reinterpret_cast<lcs_pcg_stats*>(base + kNaOffStats);
+    // the barrier arrival counter and the stats must start at zero; the rest is written
+    // before it is read
+    LCS_CUDA_TRY(cudaMemsetAsync(a.bar_count, 0, sizeof(unsigned), s));
+    LCS_CUDA_TRY(cudaMemsetAsync(a.stats, 0, sizeof(lcs_pcg_stats), s));
+    void* args[] = {&a};
+    LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_fused<kRowLanes>, dim3(nd.grid), dim3(kFusedThreads),
+                                             args, 0, s));
+    lcs_count_launch();
+    if (stats && !(o.flags & LCS_PCG_NO_STATS)) {
+        LCS_CUDA_TRY(cudaMemcpyAsync(stats, a.stats, sizeof(lcs_pcg_stats), cudaMemcpyDeviceToHost, s));
+        LCS_CUDA_TRY(cudaStreamSynchronize(s));
+        if (stats->status != LCS_OK) return lcs_fail(stats->status, "lcs_pcg_solve_noalloc: solve failed");
     }
     return LCS_OK;
 }
