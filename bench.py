@@ -290,8 +290,9 @@ def run_ours(a):
             "dtype": "f32" + ("+f64 reductions" if a.fp64 else ""), "data": "synthetic (seeded tube mesh)",
             "impl": "ours", "mode": a.mode,
             "config": {**tube_config(a), "parallelism": f"replicas x{world}" if world > 1 else "single scene"},
-            "e2e": {"value": e2e_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * 16 * V,
-                    "d2h_bytes_per_step": 2 * 16 * V, "steps": a.e2e_steps},
+            "e2e": None if a.e2e_steps == 0 else {
+                "value": e2e_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * 16 * V,
+                "d2h_bytes_per_step": 2 * 16 * V, "steps": a.e2e_steps},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": "k_pcg_fused (persistent Jacobi-PCG solve)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

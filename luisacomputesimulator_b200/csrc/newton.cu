@@ -361,6 +361,7 @@ struct lcs_newton {
     // contact
     lcs_bvh *face_tree = nullptr, *edge_tree = nullptr;
     uint32_t cap_vf = 0, cap_ee = 0, cap_pairs = 0;
+    uint32_t alloc_vf = 0, alloc_ee = 0, alloc_pairs = 0;  // capacities the buffers were allocated with
     uint2 *bp_vf = nullptr, *bp_ee = nullptr;
     lcs_pair* pairs = nullptr;
     lcs_assembler* asmb = nullptr;
@@ -390,13 +391,33 @@ void free_contact(lcs_newton* h)
     h->asmb = nullptr;
 }
 
+// (re)allocates the contact buffers whose capacity changed since they were allocated; the
+// others keep their memory (resize_template grows one buffer at a time, narrow_phase.h:71-91)
 int alloc_contact(lcs_newton* h)
 {
-    free_contact(h);
-    if (dalloc(h->bp_vf, h->cap_vf) != cudaSuccess || dalloc(h->bp_ee, h->cap_ee) != cudaSuccess ||
-        dalloc(h->pairs, h->cap_pairs) != cudaSuccess)
-        return lcs_fail(LCS_ERR_CUDA, "lcs_newton: contact buffer allocation failed");
-    return lcs_assembler_create(h->V, h->cap_pairs, &h->asmb);
+    cudaError_t e = cudaSuccess;
+    if (!h->bp_vf || h->alloc_vf != h->cap_vf) {
+        if (h->bp_vf) cudaFree(h->bp_vf);
+        h->bp_vf = nullptr;
+        e = dalloc(h->bp_vf, h->cap_vf);
+        h->alloc_vf = h->cap_vf;
+    }
+    if (e == cudaSuccess && (!h->bp_ee || h->alloc_ee != h->cap_ee)) {
+        if (h->bp_ee) cudaFree(h->bp_ee);
+        h->bp_ee = nullptr;
+        e = dalloc(h->bp_ee, h->cap_ee);
+        h->alloc_ee = h->cap_ee;
+    }
+    if (e == cudaSuccess && (!h->pairs || h->alloc_pairs != h->cap_pairs)) {
+        if (h->pairs) cudaFree(h->pairs);
+        if (h->asmb) lcs_assembler_destroy(h->asmb);
+        h->pairs = nullptr;
+        h->asmb = nullptr;
+        e = dalloc(h->pairs, h->cap_pairs);
+        h->alloc_pairs = h->cap_pairs;
+        if (e == cudaSuccess) return lcs_assembler_create(h->V, h->cap_pairs, &h->asmb);
+    }
+    return e == cudaSuccess ? LCS_OK : lcs_fail(LCS_ERR_CUDA, "lcs_newton: contact buffer allocation failed");
 }
 
 // material off-diagonal pattern: springs (both directions) + every ordered pair of each
