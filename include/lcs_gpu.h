@@ -213,7 +213,9 @@ LCS_API int lcs_spmv(uint32_t n, const float* diag, const lcs_bsr* A, const lcs_
 enum {
     LCS_PCG_FP64_DOTS = 1, /* precision form: FP64 dot products and residual reductions */
     LCS_PCG_PLAIN = 2,     /* reference dispatch structure: one kernel per op, host check */
-    LCS_PCG_NO_STATS = 4   /* fused path: do not synchronise to fill *stats */
+    LCS_PCG_NO_STATS = 4,  /* fused path: do not synchronise to fill *stats */
+    LCS_PCG_ROWS = 8       /* row-resident persistent solve (one thread per block row, state in registers);
+                              falls back to the persistent solve when the rows exceed one thread each */
 };
 
 typedef struct lcs_pcg_opts {

@@ -25,7 +25,7 @@ STATUS = {0: "LCS_OK", 1: "LCS_ERR_INVALID", 2: "LCS_ERR_CUDA", 3: "LCS_ERR_CAPA
           5: "LCS_ERR_NAN", 6: "LCS_ERR_CCD_NOCONVERGE", 7: "LCS_ERR_TIMEOUT", 8: "LCS_ERR_NO_DEVICE"}
 LCS_TREE_VERT, LCS_TREE_EDGE, LCS_TREE_FACE = 0, 1, 2
 LCS_CCD_FP64_FINAL = 1
-LCS_PCG_FP64_DOTS, LCS_PCG_PLAIN, LCS_PCG_NO_STATS = 1, 2, 4
+LCS_PCG_FP64_DOTS, LCS_PCG_PLAIN, LCS_PCG_NO_STATS, LCS_PCG_ROWS = 1, 2, 4, 8
 
 
 class Bsr(C.Structure):

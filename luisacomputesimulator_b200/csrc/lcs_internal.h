@@ -8,6 +8,15 @@ void lcs_count_launch();
 // Records `msg` as this thread's last error and returns `code`.
 int lcs_fail(int code, const char* msg);
 
+// Row-resident PCG solve with the material matrix in SELL-32 (slices of 32 rows; slot k of a
+// slice at col[32 * k + lane], value component c at val[(9 * k + c) * 32 + lane], k counted from
+// slice_ptr[slice]) and the contact blocks in CSR.  LCS_ERR_CAPACITY if the rows do not fit.
+int lcs_pcg_solve_sell(lcs_pcg* P, const float* diag, const uint32_t* slice_ptr, const uint32_t* col,
+                       const float* val, const lcs_bsr* B, const float* b, float* x, const lcs_pcg_opts* opts,
+                       lcs_pcg_stats* stats, lcs_stream stream);
+// Most block rows the row-resident solve holds on the current device (one thread per row).
+int64_t lcs_pcg_rows_capacity();
+
 // construct_tree with the reference's host sort (Morton codes downloaded, sorted on the CPU,
 // uploaded; lbvh.cpp:983-993) -- used by the plain one-scene comparator loop only.
 int lcs_bvh_construct_host_sort(lcs_bvh* h, lcs_stream stream);

@@ -158,7 +158,7 @@ __device__ __forceinline__ void atomic_add3(float4* p, float x, float y, float z
 // fn_evaluate_spring + its assembly (newton_solver.cpp:1003-1045): projected spring Hessian
 __global__ void k_springs(uint32_t ne, const uint2* __restrict__ edges, const float* __restrict__ rest_len, float k,
                           const float4* __restrict__ x, float4* b, float4* diag, const uint32_t* __restrict__ slots,
-                          float* mat_val)
+                          uint32_t cs, float* mat_val)
 {
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
         const uint2 ed = edges[e];
@@ -180,16 +180,16 @@ __global__ void k_springs(uint32_t ne, const uint2* __restrict__ edges, const fl
             for (int r = 0; r < 3; ++r) H[3 * cc + r] = a * d[r] * d[cc] + c * ((r == cc ? 1.0f : 0.0f) - il2 * d[r] * d[cc]);
         float* D0 = reinterpret_cast<float*>(diag + 3 * (size_t)ed.x);
         float* D1 = reinterpret_cast<float*>(diag + 3 * (size_t)ed.y);
-        float* O0 = mat_val + 9 * (size_t)slots[2 * e];
-        float* O1 = mat_val + 9 * (size_t)slots[2 * e + 1];
+        float* O0 = mat_val + slots[2 * e];  // block bases; component c at c * cs
+        float* O1 = mat_val + slots[2 * e + 1];
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc)
 #pragma unroll
             for (int r = 0; r < 3; ++r) {
                 atomicAdd(D0 + 4 * cc + r, H[3 * cc + r]);
                 atomicAdd(D1 + 4 * cc + r, H[3 * cc + r]);
-                atomicAdd(O0 + 3 * cc + r, -H[3 * cc + r]);
-                atomicAdd(O1 + 3 * cc + r, -H[3 * cc + r]);
+                atomicAdd(O0 + cs * (3 * cc + r), -H[3 * cc + r]);
+                atomicAdd(O1 + cs * (3 * cc + r), -H[3 * cc + r]);
             }
     }
 }
@@ -198,7 +198,7 @@ __global__ void k_springs(uint32_t ne, const uint2* __restrict__ edges, const fl
 // rest shape: grad_i = k sum_j Q_ij (x_j - X_j), Hessian block (i, j) = k Q_ij I
 __global__ void k_bending(uint32_t nb, const uint4* __restrict__ stencil, const float* __restrict__ Q, float k,
                           const float4* __restrict__ x, const float4* __restrict__ rest, float4* b, float4* diag,
-                          const uint32_t* __restrict__ slots, float* mat_val)
+                          const uint32_t* __restrict__ slots, uint32_t cs, float* mat_val)
 {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nb; s += gridDim.x * blockDim.x) {
         const uint4 st = stencil[s];
@@ -226,10 +226,10 @@ __global__ void k_bending(uint32_t nb, const uint4* __restrict__ stencil, const 
                     atomicAdd(D + 5, qij);
                     atomicAdd(D + 10, qij);
                 } else {
-                    float* O = mat_val + 9 * (size_t)slots[12 * s + t];
-                    atomicAdd(O + 0, qij);
-                    atomicAdd(O + 4, qij);
-                    atomicAdd(O + 8, qij);
+                    float* O = mat_val + slots[12 * s + t];
+                    atomicAdd(O, qij);
+                    atomicAdd(O + 4 * cs, qij);
+                    atomicAdd(O + 8 * cs, qij);
                     ++t;
                 }
             }
@@ -358,6 +358,9 @@ struct lcs_newton {
     uint32_t nnz_mat = 0;
     uint32_t *mat_rp = nullptr, *mat_col = nullptr, *spring_slots = nullptr, *bend_slots = nullptr;
     float* mat_val = nullptr;
+    bool sell = false;             // material matrix in SELL-32 for the row-resident PCG (fused mode)
+    size_t sell_vals = 0;          // floats in mat_val
+    uint32_t *sell_ptr = nullptr, *sell_col = nullptr;
     // contact
     lcs_bvh *face_tree = nullptr, *edge_tree = nullptr;
     uint32_t cap_vf = 0, cap_ee = 0, cap_pairs = 0;
@@ -446,13 +449,45 @@ int build_material_pattern(lcs_newton* h, const lcs_scene_desc* d)
     }
     for (uint32_t r = 0; r < h->V; ++r) rp[r + 1] += rp[r];
     auto slot_of = [&](uint64_t key) { return (uint32_t)(std::lower_bound(uniq.begin(), uniq.end(), key) - uniq.begin()); };
+    // block base offset into mat_val for CSR block j: CSR 9 j (components contiguous) or, in
+    // SELL-32, ((slice_ptr[s] + k) * 9) * 32 + lane (components 32 floats apart)
+    std::vector<uint32_t> base(uniq.size());
+    std::vector<uint32_t> sell_ptr, sell_col;
+    if (h->sell) {
+        const uint32_t ns = (h->V + 31) / 32;
+        sell_ptr.assign(ns + 1, 0);
+        for (uint32_t s = 0; s < ns; ++s) {
+            uint32_t w = 0;
+            for (uint32_t r = 32 * s; r < std::min(h->V, 32 * s + 32); ++r) w = std::max(w, rp[r + 1] - rp[r]);
+            sell_ptr[s + 1] = sell_ptr[s] + w;
+        }
+        sell_col.assign(32 * (size_t)sell_ptr[ns], 0);
+        for (uint32_t s = 0; s < ns; ++s)
+            for (uint32_t lane = 0; lane < 32; ++lane) {
+                const uint32_t r = 32 * s + lane;
+                const uint32_t len = r < h->V ? rp[r + 1] - rp[r] : 0;
+                const uint32_t pad = r < h->V ? r : h->V - 1;  // zero block against a valid row
+                for (uint32_t k = 0; k < sell_ptr[s + 1] - sell_ptr[s]; ++k) {
+                    const size_t slot = (size_t)sell_ptr[s] + k;
+                    sell_col[32 * slot + lane] = k < len ? col[rp[r] + k] : pad;
+                    if (k < len) base[rp[r] + k] = (uint32_t)(9 * 32 * slot + lane);
+                }
+            }
+        h->sell_vals = 9ull * 32 * sell_ptr[ns];
+    } else {
+        for (size_t j = 0; j < uniq.size(); ++j) base[j] = (uint32_t)(9 * j);
+        h->sell_vals = 9ull * uniq.size();
+    }
     std::vector<uint32_t> ss(2 * (size_t)h->E), bs(12 * (size_t)h->B);
-    for (size_t k = 0; k < 2 * (size_t)h->E; ++k) ss[k] = slot_of(keys[k]);
-    for (size_t k = 0; k < 12 * (size_t)h->B; ++k) bs[k] = slot_of(keys[2 * (size_t)h->E + k]);
+    for (size_t k = 0; k < 2 * (size_t)h->E; ++k) ss[k] = base[slot_of(keys[k])];
+    for (size_t k = 0; k < 12 * (size_t)h->B; ++k) bs[k] = base[slot_of(keys[2 * (size_t)h->E + k])];
     if (upload(h->mat_rp, rp.data(), rp.size()) != cudaSuccess || upload(h->mat_col, col.data(), col.size()) != cudaSuccess ||
         upload(h->spring_slots, ss.data(), ss.size()) != cudaSuccess ||
-        upload(h->bend_slots, bs.data(), bs.size()) != cudaSuccess || dalloc(h->mat_val, 9 * (size_t)h->nnz_mat) != cudaSuccess)
+        upload(h->bend_slots, bs.data(), bs.size()) != cudaSuccess || dalloc(h->mat_val, h->sell_vals) != cudaSuccess)
         return lcs_fail(LCS_ERR_CUDA, "lcs_newton: material pattern upload failed");
+    if (h->sell && (upload(h->sell_ptr, sell_ptr.data(), sell_ptr.size()) != cudaSuccess ||
+                    upload(h->sell_col, sell_col.data(), sell_col.size()) != cudaSuccess))
+        return lcs_fail(LCS_ERR_CUDA, "lcs_newton: SELL pattern upload failed");
     return LCS_OK;
 }
 
@@ -530,15 +565,15 @@ int newton_iteration(lcs_newton* h)
         k_inertia<<<G(V), 256, 0, h->s>>>(V, d.dt, d.dirichlet, h->mass, h->pinned, h->x, h->x_tilde, h->x_iter, h->b,
                                           h->diag, d.use_floor, d.floor_y, d.kappa, h->vert_area, h->dhat, h->offset);
         lcs_count_launch();
-        LCS_CUDA_TRY(cudaMemsetAsync(h->mat_val, 0, 36 * (size_t)h->nnz_mat, h->s));
+        LCS_CUDA_TRY(cudaMemsetAsync(h->mat_val, 0, sizeof(float) * h->sell_vals, h->s));
         if (h->E) {
             k_springs<<<G(h->E), 256, 0, h->s>>>(h->E, h->edges, h->rest_len, d.spring_k, h->x, h->b, h->diag,
-                                                 h->spring_slots, h->mat_val);
+                                                 h->spring_slots, h->sell ? 32u : 1u, h->mat_val);
             lcs_count_launch();
         }
         if (h->B) {
             k_bending<<<G(h->B), 256, 0, h->s>>>(h->B, h->bend, h->Q, d.bending_k, h->x, h->rest, h->b, h->diag,
-                                                 h->bend_slots, h->mat_val);
+                                                 h->bend_slots, h->sell ? 32u : 1u, h->mat_val);
             lcs_count_launch();
         }
         // update_contact_set (newton_solver.cpp:4093-4104)
@@ -579,9 +614,14 @@ int newton_iteration(lcs_newton* h)
         lcs_pcg_opts o{d.pcg_max_iter, d.pcg_rel_tol, d.pcg_abs_rz_tol, h->plain ? d.pcg_check_every : 1,
                        (h->fp64 ? LCS_PCG_FP64_DOTS : 0) | (h->plain ? LCS_PCG_PLAIN : LCS_PCG_NO_STATS)};
         lcs_pcg_stats ps;
-        rc = lcs_pcg_solve(h->pcg, reinterpret_cast<const float*>(h->diag), h->nnz_mat ? &A : nullptr, &Bc,
-                           reinterpret_cast<const float*>(h->b), reinterpret_cast<float*>(h->dx), &o,
-                           h->plain ? &ps : nullptr, h->s);
+        if (h->sell)
+            rc = lcs_pcg_solve_sell(h->pcg, reinterpret_cast<const float*>(h->diag), h->sell_ptr, h->sell_col,
+                                    h->mat_val, &Bc, reinterpret_cast<const float*>(h->b),
+                                    reinterpret_cast<float*>(h->dx), &o, nullptr, h->s);
+        else
+            rc = lcs_pcg_solve(h->pcg, reinterpret_cast<const float*>(h->diag), h->nnz_mat ? &A : nullptr, &Bc,
+                               reinterpret_cast<const float*>(h->b), reinterpret_cast<float*>(h->dx), &o,
+                               h->plain ? &ps : nullptr, h->s);
         if (rc != LCS_OK && rc != LCS_ERR_NAN) return rc;
         k_pcg_to_status<<<1, 1, 0, h->s>>>(lcs_pcg_device_stats(h->pcg), h->st);
         lcs_count_launch();
@@ -722,6 +762,7 @@ extern "C" int lcs_newton_create(const lcs_scene_desc* d, int flags, lcs_stream 
     }
     std::memset(h->h_st, 0, sizeof(Status));
     int rc;
+    h->sell = !h->plain && (int64_t)h->V <= lcs_pcg_rows_capacity();
     if ((rc = build_material_pattern(h, d)) || (rc = lcs_bvh_create(LCS_TREE_FACE, h->F, &h->face_tree)) ||
         (rc = lcs_bvh_create(LCS_TREE_EDGE, h->E, &h->edge_tree)) || (rc = lcs_pcg_create(h->V, &h->pcg))) {
         lcs_newton_destroy(h);
@@ -752,7 +793,7 @@ extern "C" int lcs_newton_destroy(lcs_newton* h)
     void* ptrs[] = {h->faces, h->edges, h->bend, h->Q, h->rest_len, h->vert_area, h->face_area, h->edge_area,
                     h->mass, h->dhat, h->offset, h->body, h->pinned, h->group, h->anim, h->rest, h->x, h->v,
                     h->x_step, h->x_iter, h->x_tilde, h->target, h->dx, h->b, h->diag, h->mat_rp, h->mat_col,
-                    h->spring_slots, h->bend_slots, h->mat_val, h->st};
+                    h->spring_slots, h->bend_slots, h->mat_val, h->st, h->sell_ptr, h->sell_col};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_st) cudaFreeHost(h->h_st);

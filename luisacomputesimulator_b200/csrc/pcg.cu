@@ -410,6 +410,228 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_pcg_fused(FusedArgs a)
     }
 }
 
+// ----------------------------------------------------------------------- row-resident solve
+// One thread owns one block row for the whole solve: x, r, p and the inverted diagonal block
+// live in registers, and only p crosses the grid (written once per iteration, gathered by
+// the rows that reference it).  The material matrix is CSR or sliced ELL with 32-row slices
+// (slot k of the 32 rows of a slice contiguous), which makes the thread-per-row loads of a
+// warp coalesced.  Same recurrences, same stop rules and the same three grid-wide
+// synchronisation points per iteration as k_pcg_fused.
+struct RowArgs {
+    uint32_t n;
+    const float4* diag;
+    int sell;              // material format: 0 CSR, 1 SELL-32
+    const uint32_t* m_ptr; // CSR row_ptr (n + 1) | SELL slot offset of each slice (n_slices + 1)
+    const uint32_t* m_col; // CSR col | SELL col[(off + k) * 32 + lane]
+    const float* m_val;    // CSR 9 floats per block | SELL val[((off + k) * 9 + c) * 32 + lane]
+    Bsr B;                 // contact blocks (CSR)
+    const float4* b;
+    float4* x;
+    float4* pg;            // p of every row, exchanged through L2
+    double* part;          // 4 doubles per block
+    unsigned* bar_count;
+    unsigned* bar_gen;
+    int max_iter;
+    float rel_tol, abs_rz_tol;
+    int check_every;
+    int fp64;
+    lcs_pcg_stats* stats;
+};
+
+__device__ __forceinline__ bool row_barrier(const RowArgs& a, volatile int* s_fail)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = a.bar_gen;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(a.bar_count, 1u) == gridDim.x - 1) {
+            *a.bar_count = 0u;
+            __threadfence();
+            atomicAdd(a.bar_gen, 1u);
+        } else {
+            unsigned it = 0;
+            while (*gen == g) {
+                if (++it > kBarrierSpinLimit) {
+                    *s_fail = 1;
+                    a.stats->status = LCS_ERR_TIMEOUT;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *s_fail == 0;
+}
+
+template <int BS>
+__device__ __forceinline__ void block_partial(double v0, double v1, double* dst)
+{
+    __shared__ double s[BS / 32][2];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v0 += __shfl_xor_sync(0xFFFFFFFFu, v0, o);
+        v1 += __shfl_xor_sync(0xFFFFFFFFu, v1, o);
+    }
+    if (lane_id() == 0) {
+        s[threadIdx.x >> 5][0] = v0;
+        s[threadIdx.x >> 5][1] = v1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t0 = 0.0, t1 = 0.0;
+#pragma unroll
+        for (int w = 0; w < BS / 32; ++w) {
+            t0 += s[w][0];
+            t1 += s[w][1];
+        }
+        dst[0] = t0;
+        dst[1] = t1;
+    }
+}
+
+// the same fixed-order sum of the per-block partials in every block
+__device__ __forceinline__ void grid_sum(const double* part, int k, double& o0, double& o1)
+{
+    __shared__ double so[2];
+    if (threadIdx.x < 32) {
+        double v0 = 0.0, v1 = 0.0;
+        for (uint32_t b = threadIdx.x; b < gridDim.x; b += 32) {
+            v0 += __ldcg(&part[4 * b + k]);
+            v1 += __ldcg(&part[4 * b + k + 1]);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            v0 += __shfl_xor_sync(0xFFFFFFFFu, v0, o);
+            v1 += __shfl_xor_sync(0xFFFFFFFFu, v1, o);
+        }
+        if (threadIdx.x == 0) {
+            so[0] = v0;
+            so[1] = v1;
+        }
+    }
+    __syncthreads();
+    o0 = so[0];
+    o1 = so[1];
+    __syncthreads();
+}
+
+__device__ __forceinline__ void acc_block(const float* m, int stride, float4 v, float& q0, float& q1, float& q2)
+{
+    q0 += __fmaf_rn(m[6 * stride], v.z, __fmaf_rn(m[3 * stride], v.y, m[0] * v.x));
+    q1 += __fmaf_rn(m[7 * stride], v.z, __fmaf_rn(m[4 * stride], v.y, m[1 * stride] * v.x));
+    q2 += __fmaf_rn(m[8 * stride], v.z, __fmaf_rn(m[5 * stride], v.y, m[2 * stride] * v.x));
+}
+
+template <int BS>
+__global__ void __launch_bounds__(BS) k_pcg_rows(RowArgs a)
+{
+    __shared__ int s_fail;
+    if (threadIdx.x == 0) s_fail = 0;
+    const uint32_t i = blockIdx.x * BS + threadIdx.x;
+    const bool own = i < a.n;
+    const uint32_t row = own ? i : a.n - 1;
+    float x0 = 0.f, x1 = 0.f, x2 = 0.f, r0 = 0.f, r1 = 0.f, r2 = 0.f, p0 = 0.f, p1 = 0.f, p2 = 0.f;
+    float m0, m1, m2, m3, m4, m5, m6, m7, m8;  // inverse diagonal block, column-major
+    {
+        const float4 bv = a.b[row];
+        if (own) { r0 = bv.x; r1 = bv.y; r2 = bv.z; }
+        const float4 c0 = a.diag[3 * row], c1 = a.diag[3 * row + 1], c2 = a.diag[3 * row + 2];
+        const float aa = c0.x, bb = c1.x, c = c2.x, d = c0.y, e = c1.y, f = c2.y, g = c0.z, h = c1.z, k = c2.z;
+        const float A = e * k - f * h, B = f * g - d * k, C = d * h - e * g;
+        const float id = 1.0f / (aa * A + bb * B + c * C);
+        m0 = A * id; m1 = B * id; m2 = C * id;
+        m3 = (c * h - bb * k) * id; m4 = (aa * k - c * g) * id; m5 = (bb * g - aa * h) * id;
+        m6 = (bb * f - c * e) * id; m7 = (c * d - aa * f) * id; m8 = (aa * e - bb * d) * id;
+    }
+    const uint32_t lane = threadIdx.x & 31u, slice = i >> 5;
+    float rz_old = 0.0f, norm_r0 = 0.0f, norm_r = 0.0f;
+    int iter = 0, status = 0;
+    for (iter = 0; iter < a.max_iter; ++iter) {
+        // z = Minv r ; r.r ; r.z
+        const float z0 = __fmaf_rn(m6, r2, __fmaf_rn(m3, r1, m0 * r0));
+        const float z1 = __fmaf_rn(m7, r2, __fmaf_rn(m4, r1, m1 * r0));
+        const float z2 = __fmaf_rn(m8, r2, __fmaf_rn(m5, r1, m2 * r0));
+        double drr, drz;
+        if (a.fp64) {
+            drr = (double)r0 * r0 + (double)r1 * r1 + (double)r2 * r2;
+            drz = (double)r0 * z0 + (double)r1 * z1 + (double)r2 * z2;
+        } else {
+            drr = __fmaf_rn(r2, r2, __fmaf_rn(r1, r1, r0 * r0));
+            drz = __fmaf_rn(r2, z2, __fmaf_rn(r1, z1, r0 * z0));
+        }
+        block_partial<BS>(drr, drz, &a.part[4 * blockIdx.x]);
+        if (!row_barrier(a, &s_fail)) return;
+        double srr, srz;
+        grid_sum(a.part, 0, srr, srz);
+        const float rr = (float)srr, rz = (float)srz;
+        const float beta = safe_div(rz, rz_old);
+        rz_old = rz;
+        norm_r = sqrtf(rr);
+        if (iter == 0) norm_r0 = norm_r;
+        if (iter % a.check_every == 0) {
+            if (isnan(rz) || isinf(rz)) { status = LCS_ERR_NAN; break; }
+            if (rz < a.abs_rz_tol) break;
+            if (a.rel_tol > 0.0f && norm_r <= a.rel_tol * norm_r0) break;
+        }
+        // p = z + beta p, published for the rows that reference it
+        p0 = z0 + beta * p0;
+        p1 = z1 + beta * p1;
+        p2 = z2 + beta * p2;
+        if (own) __stcg(&a.pg[i], make_float4(p0, p1, p2, 0.0f));
+        if (!row_barrier(a, &s_fail)) return;
+        // q = A p
+        float q0, q1, q2;
+        {
+            const float4 c0 = __ldg(&a.diag[3 * row]), c1 = __ldg(&a.diag[3 * row + 1]), c2 = __ldg(&a.diag[3 * row + 2]);
+            q0 = __fmaf_rn(c2.x, p2, __fmaf_rn(c1.x, p1, c0.x * p0));
+            q1 = __fmaf_rn(c2.y, p2, __fmaf_rn(c1.y, p1, c0.y * p0));
+            q2 = __fmaf_rn(c2.z, p2, __fmaf_rn(c1.z, p1, c0.z * p0));
+        }
+        float o0 = 0.f, o1 = 0.f, o2 = 0.f;
+        if (a.sell) {
+            const uint32_t off = __ldg(&a.m_ptr[slice]), end = __ldg(&a.m_ptr[slice + 1]);
+            for (uint32_t k = off; k < end; ++k) {
+                const uint32_t cj = __ldg(&a.m_col[32 * k + lane]);
+                acc_block(a.m_val + (size_t)9 * 32 * k + lane, 32, __ldcg(&a.pg[cj]), o0, o1, o2);
+            }
+        } else if (a.m_ptr && own) {
+            const uint32_t end = __ldg(&a.m_ptr[i + 1]);
+            for (uint32_t k = __ldg(&a.m_ptr[i]); k < end; ++k)
+                acc_block(a.m_val + 9 * (size_t)k, 1, __ldcg(&a.pg[__ldg(&a.m_col[k])]), o0, o1, o2);
+        }
+        if (a.B.rp && own) {
+            const uint32_t end = __ldcg(&a.B.rp[i + 1]);
+            for (uint32_t k = __ldcg(&a.B.rp[i]); k < end; ++k)
+                acc_block(a.B.val + 9 * (size_t)k, 1, __ldcg(&a.pg[__ldcg(&a.B.col[k])]), o0, o1, o2);
+        }
+        q0 += o0;
+        q1 += o1;
+        q2 += o2;
+        double dpq;
+        if (!own) dpq = 0.0;
+        else if (a.fp64) dpq = (double)p0 * q0 + (double)p1 * q1 + (double)p2 * q2;
+        else dpq = __fmaf_rn(p2, q2, __fmaf_rn(p1, q1, p0 * q0));
+        block_partial<BS>(dpq, 0.0, &a.part[4 * blockIdx.x + 2]);
+        if (!row_barrier(a, &s_fail)) return;
+        double spq, unused;
+        grid_sum(a.part, 2, spq, unused);
+        const float alpha = safe_div(rz, (float)spq);
+        x0 += alpha * p0; x1 += alpha * p1; x2 += alpha * p2;
+        r0 -= alpha * q0; r1 -= alpha * q1; r2 -= alpha * q2;
+    }
+    if (own) a.x[i] = make_float4(x0, x1, x2, 0.0f);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.stats->iterations = iter;
+        a.stats->rel_residual = norm_r0 > 0.0f ? norm_r / norm_r0 : 0.0f;
+        a.stats->dot_rz = rz_old;
+        if (a.stats->status == LCS_OK) a.stats->status = status;
+    }
+}
+
+constexpr int kRowThreads = 256;
+
 }  // namespace
 
 struct lcs_pcg {
@@ -422,6 +644,7 @@ struct lcs_pcg {
     unsigned* bar = nullptr;     // [count, gen]
     lcs_pcg_stats* d_stats = nullptr;
     int fused_grid = 0;
+    int rows_capacity = -1;  // most rows the row-resident solve can hold co-resident (-1: not queried)
 };
 
 static constexpr int kRowLanes = 4;
@@ -439,7 +662,7 @@ extern "C" int lcs_pcg_create(uint32_t n, lcs_pcg** out)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_fused<kRowLanes>, kFusedThreads, 0);
     if (per_sm > 1) per_sm = 1;
     p->fused_grid = sms * (per_sm > 0 ? per_sm : 1);
-    const int parts = p->fused_grid > kPlainBlocks ? p->fused_grid : kPlainBlocks;
+    const int parts = 1024 + (p->fused_grid > kPlainBlocks ? p->fused_grid : kPlainBlocks);  // >= 4 per rows block
     cudaError_t e = cudaSuccess;
     auto A = [&](void** q, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(q, bytes); };
     A((void**)&p->r, 16 * (size_t)n);
@@ -543,6 +766,77 @@ static int plain_solve(lcs_pcg* P, const float4* diag, Bsr A, Bsr B, const float
     return status == LCS_OK ? LCS_OK : lcs_fail(status, "lcs_pcg_solve: NaN/Inf in r.z");
 }
 
+// row-resident solve; LCS_ERR_CAPACITY when one thread per row does not fit co-resident
+static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* m_ptr, const uint32_t* m_col,
+                      const float* m_val, Bsr B, const float4* b, float4* x, const lcs_pcg_opts& o,
+                      lcs_pcg_stats* stats, cudaStream_t s)
+{
+    if (P->rows_capacity < 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_rows<kRowThreads>, kRowThreads, 0);
+        int blocks = sms * per_sm;
+        if (blocks > 1024) blocks = 1024;  // partial-sum space
+        P->rows_capacity = blocks * kRowThreads;
+    }
+    if ((int64_t)P->n > P->rows_capacity) return LCS_ERR_CAPACITY;
+    RowArgs a;
+    a.n = P->n;
+    a.diag = diag;
+    a.sell = sell;
+    a.m_ptr = m_ptr;
+    a.m_col = m_col;
+    a.m_val = m_val;
+    a.B = B;
+    a.b = b;
+    a.x = x;
+    a.pg = P->p;
+    a.part = P->part;
+    a.bar_count = P->bar;
+    a.bar_gen = P->bar + 1;
+    a.max_iter = o.max_iter;
+    a.rel_tol = o.rel_tol;
+    a.abs_rz_tol = o.abs_rz_tol;
+    a.check_every = o.check_every;
+    a.fp64 = (o.flags & LCS_PCG_FP64_DOTS) ? 1 : 0;
+    a.stats = P->d_stats;
+    LCS_CUDA_TRY(cudaMemsetAsync(P->d_stats, 0, sizeof(lcs_pcg_stats), s));
+    LCS_CUDA_TRY(cudaMemsetAsync(P->bar, 0, sizeof(unsigned), s));
+    void* args[] = {&a};
+    const int grid = (int)((P->n + kRowThreads - 1) / kRowThreads);
+    LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_rows<kRowThreads>, dim3(grid), dim3(kRowThreads), args,
+                                             0, s));
+    lcs_count_launch();
+    if (stats && !(o.flags & LCS_PCG_NO_STATS)) {
+        LCS_CUDA_TRY(cudaMemcpyAsync(stats, P->d_stats, sizeof(lcs_pcg_stats), cudaMemcpyDeviceToHost, s));
+        LCS_CUDA_TRY(cudaStreamSynchronize(s));
+        if (stats->status != LCS_OK) return lcs_fail(stats->status, "lcs_pcg_solve: row-resident solve failed");
+    }
+    return LCS_OK;
+}
+
+int64_t lcs_pcg_rows_capacity()
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_rows<kRowThreads>, kRowThreads, 0);
+    int64_t blocks = (int64_t)sms * per_sm;
+    if (blocks > 1024) blocks = 1024;
+    return blocks * kRowThreads;
+}
+
+int lcs_pcg_solve_sell(lcs_pcg* P, const float* diag, const uint32_t* slice_ptr, const uint32_t* col,
+                       const float* val, const lcs_bsr* B, const float* b, float* x, const lcs_pcg_opts* opts,
+                       lcs_pcg_stats* stats, lcs_stream stream)
+{
+    if (!P || !diag || !b || !x || !opts) return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_sell: bad argument");
+    return rows_solve(P, reinterpret_cast<const float4*>(diag), 1, slice_ptr, col, val, to_bsr(B),
+                      reinterpret_cast<const float4*>(b), reinterpret_cast<float4*>(x), *opts, stats,
+                      (cudaStream_t)stream);
+}
+
 extern "C" int lcs_pcg_solve(lcs_pcg* P, const float* diag, const lcs_bsr* A, const lcs_bsr* B, const float* b,
                              float* x, const lcs_pcg_opts* opts, lcs_pcg_stats* stats, lcs_stream stream)
 {
@@ -554,6 +848,11 @@ extern "C" int lcs_pcg_solve(lcs_pcg* P, const float* diag, const lcs_bsr* A, co
     const float4* d4 = reinterpret_cast<const float4*>(diag);
     const float4* b4 = reinterpret_cast<const float4*>(b);
     float4* x4 = reinterpret_cast<float4*>(x);
+    if ((o.flags & LCS_PCG_ROWS) && !(o.flags & LCS_PCG_PLAIN)) {
+        const Bsr Am = to_bsr(A);
+        const int rc = rows_solve(P, d4, 0, Am.rp, Am.col, Am.val, to_bsr(B), b4, x4, o, stats, s);
+        if (rc != LCS_ERR_CAPACITY) return rc;  // too many rows for one thread each: persistent solve below
+    }
     if (o.flags & LCS_PCG_PLAIN) {
         if (o.flags & LCS_PCG_FP64_DOTS) return plain_solve<double>(P, d4, to_bsr(A), to_bsr(B), b4, x4, o, stats, s);
         return plain_solve<float>(P, d4, to_bsr(A), to_bsr(B), b4, x4, o, stats, s);

@@ -83,15 +83,16 @@ def test_spmv_matches_oracle(system):
     np.testing.assert_allclose(got[:, :3], want[:, :3], rtol=1e-5, atol=1e-6 * scale)
 
 
-@pytest.mark.parametrize("plain", [True, False])
+@pytest.mark.parametrize("mode", ["plain", "fused", "rows"])
 @pytest.mark.parametrize("fp64", [False, True])
-def test_pcg_matches_oracle(system, plain, fp64):
+def test_pcg_matches_oracle(system, mode, fp64):
     sc, diag, A, B, b = system
     n = sc.num_verts
+    plain = mode == "plain"
     solver = ConjugateGradientSolver(n)
     x = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
     st = solver.device_solve(dev(diag), _dev_bsr(n, A), _dev_bsr(n, B), dev(b), x, max_iter=500, rel_tol=1e-4,
-                             check_every=25 if plain else 1, fp64_dots=fp64, plain=plain)
+                             check_every=25 if plain else 1, fp64_dots=fp64, plain=plain, rows=mode == "rows")
     ox, ost = O.pcg(diag, A, B, b, max_iter=500, rel_tol=1e-4, check_every=25 if plain else 1, fp64_dots=fp64)
     assert st["status"] == 0 and ost["status"] == 0
     assert st["rel_residual"] <= 1e-4
