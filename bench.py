@@ -39,6 +39,8 @@ def args_():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--mode", choices=["fused", "plain"], default="fused")
     p.add_argument("--fp64", action="store_true", help="precision form")
+    p.add_argument("--pcg", choices=["rows", "pipelined"], default="rows",
+                   help="fused mode: row-resident PCG recurrences (classic: 3 grid syncs/iter; pipelined: 1)")
     p.add_argument("--e2e-steps", type=int, default=10)
     p.add_argument("--cpu-iters", type=int, default=0, help="CPU baseline sample (0: auto, ~10-30 s)")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -199,7 +201,7 @@ def run_ours(a):
     lib = _capi.load()
     _capi.check(lib.lcs_device_check(local), "device check")
     sc = scenes.twisted_tube(a.n_around, a.n_along)
-    solver = NewtonSolver(sc, plain=(a.mode == "plain"), fp64=a.fp64, profile=True)
+    solver = NewtonSolver(sc, plain=(a.mode == "plain"), fp64=a.fp64, profile=True, pipelined=(a.pcg == "pipelined"))
     stream = torch.cuda.current_stream()
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
 
@@ -269,11 +271,20 @@ def run_ours(a):
 
     if rank == 0:
         value = newton_all / t_s
+        solver_uses_rows = solver.uses_row_pcg()
+        pcg_kernel_name = ("k_pcg_pipe (pipelined row-resident Jacobi-PCG)" if a.pcg == "pipelined" else
+                           "k_pcg_rows (row-resident Jacobi-PCG)") if solver_uses_rows else \
+            ("k_pcg_fused (persistent Jacobi-PCG solve)" if a.mode == "fused" else "plain PCG kernels")
         # roofline of the dominant kernel: the persistent PCG solve (one launch per Newton iteration)
         pcg_ms, pcg_launches = prof["pcg"]
         nnz = cnt["nnz_material"] + 12 * last["pairs"]
         it_per_launch = pcg / max(pcg_launches, 1)
-        bytes_per_iter = 40.0 * nnz + 312.0 * V
+        # algorithmic bytes of one PCG iteration: every matrix block once (36 B values + 4 B
+        # column), the diagonal blocks (48 B/row) and the exchanged direction written and read
+        # once (32 B/row) when the row state stays in registers (row-resident kernels); the
+        # CSR-vector kernel also streams r, z, p, q, x (312 B/row in all)
+        rows_kind = a.mode == "fused" and solver_uses_rows
+        bytes_per_iter = 40.0 * nnz + (80.0 if rows_kind else 312.0) * V
         bytes_per_launch = it_per_launch * bytes_per_iter + 160.0 * V
         achieved = bytes_per_launch / (pcg_ms / max(pcg_launches, 1) / 1e3) / 1e9
         peak, peak_kind = measured_peak()
@@ -288,13 +299,13 @@ def run_ours(a):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms_total / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" + ("+f64 reductions" if a.fp64 else ""), "data": "synthetic (seeded tube mesh)",
-            "impl": "ours", "mode": a.mode,
+            "impl": "ours", "mode": a.mode, "pcg": solver.pcg_kind(),
             "config": {**tube_config(a), "parallelism": f"replicas x{world}" if world > 1 else "single scene"},
             "e2e": None if a.e2e_steps == 0 else {
                 "value": e2e_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * 16 * V,
                 "d2h_bytes_per_step": 2 * 16 * V, "steps": a.e2e_steps},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "k_pcg_fused (persistent Jacobi-PCG solve)",
+            "roofline": {"bound": "hbm", "kernel": pcg_kernel_name,
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind,
                          "traffic": None if traffic is None else traffic * it_per_launch,

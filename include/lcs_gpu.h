@@ -50,7 +50,10 @@ typedef enum lcs_status {
 enum { LCS_TREE_VERT = 0, LCS_TREE_EDGE = 1, LCS_TREE_FACE = 2 };
 
 /* flags for the CCD entry points */
-enum { LCS_CCD_FP64_FINAL = 1 };
+enum {
+    LCS_CCD_FP64_FINAL = 1, /* FP32 iteration, final iterate re-checked in FP64 (backs off if it fails) */
+    LCS_CCD_FP64 = 2        /* the whole iteration in FP64; per-pair TOI rounded toward zero to float */
+};
 
 /* CollisionPairTemplate (Solver/SimulationCore/collision_data.h:48-126): indices with the
  * pair type in bit 31 (VF: idx[2], EE: idx[3]); vec1 = (normal, kappa * area);
@@ -214,8 +217,11 @@ enum {
     LCS_PCG_FP64_DOTS = 1, /* precision form: FP64 dot products and residual reductions */
     LCS_PCG_PLAIN = 2,     /* reference dispatch structure: one kernel per op, host check */
     LCS_PCG_NO_STATS = 4,  /* fused path: do not synchronise to fill *stats */
-    LCS_PCG_ROWS = 8       /* row-resident persistent solve (one thread per block row, state in registers);
+    LCS_PCG_ROWS = 8,      /* row-resident persistent solve (one thread per block row, state in registers);
                               falls back to the persistent solve when the rows exceed one thread each */
+    LCS_PCG_PIPELINED = 16 /* with LCS_PCG_ROWS: pipelined recurrences (Ghysels-Vanroose), one grid-wide
+                              synchronisation per iteration instead of three; the same Krylov iterates in
+                              exact arithmetic, different rounding */
 };
 
 typedef struct lcs_pcg_opts {
@@ -300,8 +306,9 @@ typedef struct lcs_scene_desc {
 
 enum {
     LCS_NEWTON_PLAIN = 1,   /* the reference's dispatch structure (one-scene comparator) */
-    LCS_NEWTON_FP64 = 2,    /* precision form: FP64 PCG reductions, FP64-checked final ACCD distance */
-    LCS_NEWTON_PROFILE = 4  /* per-phase CUDA-event timing (lcs_newton_profile) */
+    LCS_NEWTON_FP64 = 2,    /* precision form: FP64 PCG reductions, ACCD step bound in FP64 */
+    LCS_NEWTON_PROFILE = 4, /* per-phase CUDA-event timing (lcs_newton_profile) */
+    LCS_NEWTON_PCG_PIPELINED = 8 /* fused mode: pipelined row-resident PCG (LCS_PCG_PIPELINED) */
 };
 
 typedef struct lcs_newton_stats {
@@ -337,6 +344,9 @@ LCS_API int lcs_newton_profile(const lcs_newton* h, double* phase_ms, int32_t* l
 LCS_API int lcs_newton_reset_profile(lcs_newton* h);
 LCS_API int lcs_newton_counts(const lcs_newton* h, uint32_t* nnz_material, uint32_t* cap_vf, uint32_t* cap_ee,
                               uint32_t* cap_pairs);
+/* Which PCG the Newton loop runs: 0 plain kernels, 1 persistent CSR solve, 2 row-resident,
+ * 3 pipelined row-resident (-1: null handle).  No counterpart in the reference. */
+LCS_API int lcs_newton_pcg_kind(const lcs_newton* h);
 
 #ifdef __cplusplus
 }

@@ -24,8 +24,8 @@ class LcsError(RuntimeError):
 STATUS = {0: "LCS_OK", 1: "LCS_ERR_INVALID", 2: "LCS_ERR_CUDA", 3: "LCS_ERR_CAPACITY", 4: "LCS_ERR_UNHEALTHY_BVH",
           5: "LCS_ERR_NAN", 6: "LCS_ERR_CCD_NOCONVERGE", 7: "LCS_ERR_TIMEOUT", 8: "LCS_ERR_NO_DEVICE"}
 LCS_TREE_VERT, LCS_TREE_EDGE, LCS_TREE_FACE = 0, 1, 2
-LCS_CCD_FP64_FINAL = 1
-LCS_PCG_FP64_DOTS, LCS_PCG_PLAIN, LCS_PCG_NO_STATS, LCS_PCG_ROWS = 1, 2, 4, 8
+LCS_CCD_FP64_FINAL, LCS_CCD_FP64 = 1, 2
+LCS_PCG_FP64_DOTS, LCS_PCG_PLAIN, LCS_PCG_NO_STATS, LCS_PCG_ROWS, LCS_PCG_PIPELINED = 1, 2, 4, 8, 16
 
 
 class Bsr(C.Structure):
@@ -106,10 +106,11 @@ SIGNATURES = {
     "lcs_newton_download": (I32, [P, P, P]),
     "lcs_newton_profile": (I32, [P, C.POINTER(C.c_double), C.POINTER(C.c_int32), I32]),
     "lcs_newton_reset_profile": (I32, [P]),
+    "lcs_newton_pcg_kind": (I32, [P]),
     "lcs_newton_counts": (I32, [P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                 C.POINTER(C.c_uint32)]),
 }
-LCS_NEWTON_PLAIN, LCS_NEWTON_FP64, LCS_NEWTON_PROFILE = 1, 2, 4
+LCS_NEWTON_PLAIN, LCS_NEWTON_FP64, LCS_NEWTON_PROFILE, LCS_NEWTON_PCG_PIPELINED = 1, 2, 4, 8
 PHASES = ["build", "material", "dcd_broad", "dcd_narrow", "assembly", "pcg", "ccd_broad", "ccd_narrow", "apply"]
 
 _lib = None

@@ -181,15 +181,17 @@ class NarrowPhasesDetector:
         return bool(grew)
 
     # -- CCD (narrow_phase.cpp:293-740)
-    def vf_ccd_query(self, x0, x1, faces, body, offset, toi_per_pair=None, fp64_final=False):
+    def vf_ccd_query(self, x0, x1, faces, body, offset, toi_per_pair=None, fp64_final=False, fp64=False):
+        flags = (A.LCS_CCD_FP64_FINAL if fp64_final else 0) | (A.LCS_CCD_FP64 if fp64 else 0)
         A.check(self.lib.lcs_ccd_vf(ptr(self.broad_phase_list_vf), ptr(self.count_view(0)), self.cap_vf, ptr(x0),
                                     ptr(x1), ptr(faces), ptr(body), ptr(offset), ptr(self.toi), ptr(toi_per_pair),
-                                    int(bool(fp64_final)), stream()), "ccd_vf")
+                                    flags, stream()), "ccd_vf")
 
-    def ee_ccd_query(self, x0, x1, edges, body, offset, toi_per_pair=None, fp64_final=False):
+    def ee_ccd_query(self, x0, x1, edges, body, offset, toi_per_pair=None, fp64_final=False, fp64=False):
+        flags = (A.LCS_CCD_FP64_FINAL if fp64_final else 0) | (A.LCS_CCD_FP64 if fp64 else 0)
         A.check(self.lib.lcs_ccd_ee(ptr(self.broad_phase_list_ee), ptr(self.count_view(1)), self.cap_ee, ptr(x0),
                                     ptr(x1), ptr(edges), ptr(body), ptr(offset), ptr(self.toi), ptr(toi_per_pair),
-                                    int(bool(fp64_final)), stream()), "ccd_ee")
+                                    flags, stream()), "ccd_ee")
 
     # -- DCD (narrow_phase.cpp:771-1249)
     def vf_dcd_query_repulsion(self, x, faces, body, vert_area, face_area, d_hat, offset, kappa):

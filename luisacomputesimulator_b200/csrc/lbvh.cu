@@ -340,9 +340,13 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide, 
                                                const float4* __restrict__ x0, const float4* __restrict__ x1,
                                                const uint2* __restrict__ edges, uint32_t n_queries,
                                                const float* __restrict__ dhat, const float* __restrict__ thickness,
-                                               uint2* __restrict__ pairs, uint32_t capacity, uint32_t* d_count)
+                                               uint2* __restrict__ pairs, uint32_t capacity, uint32_t* d_count,
+                                               const uint32_t* __restrict__ order)
 {
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n_queries; q += gridDim.x * blockDim.x) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_queries; t += gridDim.x * blockDim.x) {
+        // queries in the order of `order` (the tree's Morton order when the queries are its own
+        // leaves): neighbouring threads then walk nearly the same nodes
+        const uint32_t q = order ? __ldg(&order[t]) : t;
         float box[6];
         {
             v3 mn, mx;
@@ -622,7 +626,7 @@ extern "C" int lcs_bvh_query_vf(const lcs_bvh* t, const float* x0, const float* 
     if (t->n == 0 || n_verts == 0) return LCS_OK;
     k_query<false><<<grid_for(n_verts, 128, 16), 128, 0, (cudaStream_t)stream>>>(
         t->wide, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1), nullptr, n_verts,
-        d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count);
+        d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count, nullptr);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
@@ -639,7 +643,7 @@ extern "C" int lcs_bvh_query_ee(const lcs_bvh* t, const float* x0, const float* 
     k_query<true><<<grid_for(n_edges, 128, 16), 128, 0, (cudaStream_t)stream>>>(
         t->wide, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
         reinterpret_cast<const uint2*>(edges), n_edges, d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity,
-        d_count);
+        d_count, n_edges == t->n ? t->sgo : nullptr);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;

@@ -263,6 +263,62 @@ __device__ __forceinline__ float accd_ccd(const v3* a, const v3* b, float offset
     return toi;
 }
 
+// The same additive CCD carried out entirely in double precision (positions promoted exactly,
+// offset promoted): the precision form's step bound.  Returns the FP64 time of impact; the
+// caller rounds it toward zero so the float it stores never exceeds it.
+template <bool EE>
+__device__ __forceinline__ double accd_ccd_f64(const v3* a, const v3* b, float offset_f)
+{
+    vd x0[4], dx[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        x0[k] = vd{a[k].x, a[k].y, a[k].z};
+        dx[k] = Gd::sub(vd{b[k].x, b[k].y, b[k].z}, x0[k]);
+    }
+    vd m0 = vd{0.0, 0.0, 0.0}, m1 = vd{0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        m0 = Gd::add(m0, Gd::scl(0.25, x0[k]));
+        m1 = Gd::add(m1, Gd::scl(0.25, dx[k]));
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        x0[k] = Gd::sub(x0[k], m0);
+        dx[k] = Gd::sub(dx[k], m1);
+    }
+    double m = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = i + 1; j < 4; ++j) {
+            const vd du = Gd::sub(dx[i], dx[j]);
+            const double q = Gd::dot(du, du);
+            m = q > m ? q : m;
+        }
+    const double u_max = sqrt(m);
+    const double max_t = 1.25;
+    if (u_max == 0.0) return max_t;
+    const double offset = offset_f;
+    double toi = 0.0;
+    const double eps = 0.01 * (sqrt(Gd::dist2<EE>(x0)) - offset);
+    const double target = eps + offset, eps_sqr = eps * eps, inv_u_max = 1.0 / u_max;
+    for (unsigned iter = 0;; ++iter) {
+        if (iter > 10000u) return 0.001;
+        vd xt[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) xt[k] = Gd::add(x0[k], Gd::scl(toi, dx[k]));
+        const double d2 = Gd::dist2<EE>(xt);
+        const double dmt = (d2 - target * target) / (sqrt(d2) + target);
+        if ((max_t - toi) * u_max < dmt - eps) return max_t;
+        if (toi > 0.0 && dmt * dmt < eps_sqr) break;
+        const double nt = toi + dmt * inv_u_max;
+        if (nt == toi) break;
+        toi = nt;
+        if (toi > max_t) return max_t;
+    }
+    return toi;
+}
+
 // cipc_kernel.hpp:16-36
 __device__ __forceinline__ float barrier_e(float d, float dhat)
 {

@@ -55,8 +55,9 @@ __global__ void __launch_bounds__(256) k_ccd(const uint2* __restrict__ pairs, co
                                              const float4* __restrict__ x0, const float4* __restrict__ x1,
                                              const uint32_t* __restrict__ elems, const uint32_t* __restrict__ body,
                                              const float* __restrict__ offset, float* d_toi,
-                                             float* __restrict__ toi_per_pair, bool fp64_final)
+                                             float* __restrict__ toi_per_pair, int flags)
 {
+    const bool fp64_final = (flags & LCS_CCD_FP64_FINAL) != 0, fp64 = (flags & LCS_CCD_FP64) != 0;
     const uint32_t n = pair_count(d_count, cap);
     float local = 1.0f;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
@@ -84,7 +85,7 @@ __global__ void __launch_bounds__(256) k_ccd(const uint2* __restrict__ pairs, co
                 b[k] = ld3(x1, v[k]);
             }
             const float th = __ldg(&offset[v[0]]) + __ldg(&offset[EE ? v[2] : v[1]]);
-            toi = accd_ccd<EE>(a, b, th, fp64_final);
+            toi = fp64 ? __double2float_rz(accd_ccd_f64<EE>(a, b, th)) : accd_ccd<EE>(a, b, th, fp64_final);
         }
         if (toi_per_pair) toi_per_pair[p] = toi;
         local = fmn(local, toi / 1.25f);
@@ -500,7 +501,7 @@ extern "C" int lcs_ccd_vf(const uint32_t* pairs, const uint32_t* d_count, uint32
     if (capacity == 0) return LCS_OK;
     k_ccd<false><<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
         reinterpret_cast<const uint2*>(pairs), d_count, capacity, reinterpret_cast<const float4*>(x0),
-        reinterpret_cast<const float4*>(x1), faces, body, offset, d_toi, toi_per_pair, (flags & LCS_CCD_FP64_FINAL) != 0);
+        reinterpret_cast<const float4*>(x1), faces, body, offset, d_toi, toi_per_pair, flags);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
@@ -515,7 +516,7 @@ extern "C" int lcs_ccd_ee(const uint32_t* pairs, const uint32_t* d_count, uint32
     if (capacity == 0) return LCS_OK;
     k_ccd<true><<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
         reinterpret_cast<const uint2*>(pairs), d_count, capacity, reinterpret_cast<const float4*>(x0),
-        reinterpret_cast<const float4*>(x1), edges, body, offset, d_toi, toi_per_pair, (flags & LCS_CCD_FP64_FINAL) != 0);
+        reinterpret_cast<const float4*>(x1), edges, body, offset, d_toi, toi_per_pair, flags);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;

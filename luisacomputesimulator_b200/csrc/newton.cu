@@ -359,6 +359,7 @@ struct lcs_newton {
     uint32_t *mat_rp = nullptr, *mat_col = nullptr, *spring_slots = nullptr, *bend_slots = nullptr;
     float* mat_val = nullptr;
     bool sell = false;             // material matrix in SELL-32 for the row-resident PCG (fused mode)
+    bool pipelined = false;        // pipelined row-resident PCG (one grid synchronisation per iteration)
     size_t sell_vals = 0;          // floats in mat_val
     uint32_t *sell_ptr = nullptr, *sell_col = nullptr;
     // contact
@@ -612,7 +613,8 @@ int newton_iteration(lcs_newton* h)
         const uint32_t* d_nnzb = nullptr;
         lcs_assembler_bsr(h->asmb, &Bc, &d_nnzb);
         lcs_pcg_opts o{d.pcg_max_iter, d.pcg_rel_tol, d.pcg_abs_rz_tol, h->plain ? d.pcg_check_every : 1,
-                       (h->fp64 ? LCS_PCG_FP64_DOTS : 0) | (h->plain ? LCS_PCG_PLAIN : LCS_PCG_NO_STATS)};
+                       (h->fp64 ? LCS_PCG_FP64_DOTS : 0) | (h->plain ? LCS_PCG_PLAIN : LCS_PCG_NO_STATS) |
+                           (h->pipelined ? LCS_PCG_PIPELINED : 0)};
         lcs_pcg_stats ps;
         if (h->sell)
             rc = lcs_pcg_solve_sell(h->pcg, reinterpret_cast<const float*>(h->diag), h->sell_ptr, h->sell_col,
@@ -644,7 +646,7 @@ int newton_iteration(lcs_newton* h)
         }
         mark(h, kPhCcdNarrow);
         const float* XI = reinterpret_cast<const float*>(h->x_iter);
-        const int ccd_flags = h->fp64 ? LCS_CCD_FP64_FINAL : 0;
+        const int ccd_flags = h->fp64 ? LCS_CCD_FP64 : 0;
         if (d.use_floor) {
             k_floor_ccd<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->x, h->offset, h->pinned, d.floor_y, h->st);
             lcs_count_launch();
@@ -699,6 +701,7 @@ extern "C" int lcs_newton_create(const lcs_scene_desc* d, int flags, lcs_stream 
     h->plain = (flags & LCS_NEWTON_PLAIN) != 0;
     h->fp64 = (flags & LCS_NEWTON_FP64) != 0;
     h->profile = (flags & LCS_NEWTON_PROFILE) != 0;
+    h->pipelined = (flags & LCS_NEWTON_PCG_PIPELINED) != 0;
     h->V = d->n_verts;
     h->F = d->n_faces;
     h->E = d->n_edges;
@@ -946,6 +949,14 @@ extern "C" int lcs_newton_reset_profile(lcs_newton* h)
         h->phase_launch_count[p] = 0;
     }
     return LCS_OK;
+}
+
+extern "C" int lcs_newton_pcg_kind(const lcs_newton* h)
+{
+    if (!h) return -1;
+    if (h->plain) return 0;
+    if (!h->sell) return 1;
+    return h->pipelined ? 3 : 2;
 }
 
 extern "C" int lcs_newton_counts(const lcs_newton* h, uint32_t* nnz_material, uint32_t* cap_vf, uint32_t* cap_ee,

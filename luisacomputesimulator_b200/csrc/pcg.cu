@@ -632,6 +632,247 @@ __global__ void __launch_bounds__(BS) k_pcg_rows(RowArgs a)
 
 constexpr int kRowThreads = 256;
 
+// ---------------------------------------------------------------- pipelined row-resident solve
+// Pipelined PCG (Ghysels & Vanroose, "Hiding global synchronization latency in the
+// preconditioned conjugate gradient algorithm", Parallel Computing 40, 2014): the same Krylov
+// iterates as CG in exact arithmetic, rearranged so that the three dot products of an
+// iteration (r.u, w.u, r.r) and the exchange of the next SpMV input m = M w share ONE grid-wide
+// synchronisation.  With the block-Jacobi preconditioner M is row-local, so every vector but m
+// stays in the registers of the thread that owns the row.  m and the partial sums are double
+// buffered across iterations (a block that runs ahead must not overwrite what a slower block
+// still reads).  Stop rules as in device_solve: r.z (= r.u) and |r| checked before the update.
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v)
+{
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ void red_add_release(unsigned* p, unsigned v)
+{
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// grid barrier with release/acquire ordering (the block's writes, ordered by __syncthreads,
+// are released by thread 0's arrival); bounded spin -> LCS_ERR_TIMEOUT
+__device__ __forceinline__ bool pipe_barrier(unsigned* count, unsigned* gen, lcs_pcg_stats* stats, volatile int* s_fail)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned g = ld_acquire(gen);
+        if (atom_add_acq_rel(count, 1u) == gridDim.x - 1) {
+            *count = 0u;  // ordered before the release below; no block reads it until the next arrival
+            red_add_release(gen, 1u);
+        } else {
+            unsigned it = 0;
+            while (ld_acquire(gen) == g) {
+                if (++it > kBarrierSpinLimit) {
+                    *s_fail = 1;
+                    stats->status = LCS_ERR_TIMEOUT;
+                    break;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    return *s_fail == 0;
+}
+
+template <int BS>
+__device__ __forceinline__ void block_partial3(double v0, double v1, double v2, double* dst)
+{
+    __shared__ double s[BS / 32][3];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v0 += __shfl_xor_sync(0xFFFFFFFFu, v0, o);
+        v1 += __shfl_xor_sync(0xFFFFFFFFu, v1, o);
+        v2 += __shfl_xor_sync(0xFFFFFFFFu, v2, o);
+    }
+    if (lane_id() == 0) {
+        s[threadIdx.x >> 5][0] = v0;
+        s[threadIdx.x >> 5][1] = v1;
+        s[threadIdx.x >> 5][2] = v2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+#pragma unroll
+        for (int w = 0; w < BS / 32; ++w) {
+            t0 += s[w][0];
+            t1 += s[w][1];
+            t2 += s[w][2];
+        }
+        dst[0] = t0;
+        dst[1] = t1;
+        dst[2] = t2;
+    }
+}
+
+__device__ __forceinline__ void grid_sum3(const double* part, double& o0, double& o1, double& o2)
+{
+    __shared__ double so[3];
+    if (threadIdx.x < 32) {
+        double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+        for (uint32_t b = threadIdx.x; b < gridDim.x; b += 32) {
+            v0 += __ldcg(&part[4 * b + 0]);
+            v1 += __ldcg(&part[4 * b + 1]);
+            v2 += __ldcg(&part[4 * b + 2]);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            v0 += __shfl_xor_sync(0xFFFFFFFFu, v0, o);
+            v1 += __shfl_xor_sync(0xFFFFFFFFu, v1, o);
+            v2 += __shfl_xor_sync(0xFFFFFFFFu, v2, o);
+        }
+        if (threadIdx.x == 0) {
+            so[0] = v0;
+            so[1] = v1;
+            so[2] = v2;
+        }
+    }
+    __syncthreads();
+    o0 = so[0];
+    o1 = so[1];
+    o2 = so[2];
+    __syncthreads();
+}
+
+// A v for the owned row: diagonal block + material (CSR or SELL-32) + contact (CSR)
+__device__ __forceinline__ void row_matvec(const RowArgs& a, uint32_t i, uint32_t row, bool own, uint32_t slice,
+                                          uint32_t lane, const float4* src, float v0, float v1, float v2, float& q0,
+                                          float& q1, float& q2)
+{
+    const float4 c0 = __ldg(&a.diag[3 * row]), c1 = __ldg(&a.diag[3 * row + 1]), c2 = __ldg(&a.diag[3 * row + 2]);
+    q0 = __fmaf_rn(c2.x, v2, __fmaf_rn(c1.x, v1, c0.x * v0));
+    q1 = __fmaf_rn(c2.y, v2, __fmaf_rn(c1.y, v1, c0.y * v0));
+    q2 = __fmaf_rn(c2.z, v2, __fmaf_rn(c1.z, v1, c0.z * v0));
+    float o0 = 0.f, o1 = 0.f, o2 = 0.f;
+    if (a.sell) {
+        const uint32_t off = __ldg(&a.m_ptr[slice]), end = __ldg(&a.m_ptr[slice + 1]);
+        for (uint32_t k = off; k < end; ++k) {
+            const uint32_t cj = __ldg(&a.m_col[32 * k + lane]);
+            acc_block(a.m_val + (size_t)9 * 32 * k + lane, 32, __ldcg(&src[cj]), o0, o1, o2);
+        }
+    } else if (a.m_ptr && own) {
+        const uint32_t end = __ldg(&a.m_ptr[i + 1]);
+        for (uint32_t k = __ldg(&a.m_ptr[i]); k < end; ++k)
+            acc_block(a.m_val + 9 * (size_t)k, 1, __ldcg(&src[__ldg(&a.m_col[k])]), o0, o1, o2);
+    }
+    if (a.B.rp && own) {
+        const uint32_t end = __ldcg(&a.B.rp[i + 1]);
+        for (uint32_t k = __ldcg(&a.B.rp[i]); k < end; ++k)
+            acc_block(a.B.val + 9 * (size_t)k, 1, __ldcg(&src[__ldcg(&a.B.col[k])]), o0, o1, o2);
+    }
+    q0 += o0;
+    q1 += o1;
+    q2 += o2;
+}
+
+template <int BS>
+__global__ void __launch_bounds__(BS) k_pcg_pipe(RowArgs a, float4* pg2)
+{
+    __shared__ int s_fail;
+    if (threadIdx.x == 0) s_fail = 0;
+    const uint32_t i = blockIdx.x * BS + threadIdx.x;
+    const bool own = i < a.n;
+    const uint32_t row = own ? i : a.n - 1;
+    const uint32_t lane = threadIdx.x & 31u, slice = i >> 5;
+    float m0, m1, m2, m3, m4, m5, m6, m7, m8;  // inverse diagonal block, column-major
+    float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+    {
+        const float4 bv = a.b[row];
+        if (own) { r0 = bv.x; r1 = bv.y; r2 = bv.z; }
+        const float4 c0 = a.diag[3 * row], c1 = a.diag[3 * row + 1], c2 = a.diag[3 * row + 2];
+        const float aa = c0.x, bb = c1.x, c = c2.x, d = c0.y, e = c1.y, f = c2.y, g = c0.z, h = c1.z, k = c2.z;
+        const float A = e * k - f * h, B = f * g - d * k, C = d * h - e * g;
+        const float id = 1.0f / (aa * A + bb * B + c * C);
+        m0 = A * id; m1 = B * id; m2 = C * id;
+        m3 = (c * h - bb * k) * id; m4 = (aa * k - c * g) * id; m5 = (bb * g - aa * h) * id;
+        m6 = (bb * f - c * e) * id; m7 = (c * d - aa * f) * id; m8 = (aa * e - bb * d) * id;
+    }
+#define LCS_MINV(v0, v1, v2, o0, o1, o2)                        \
+    o0 = __fmaf_rn(m6, v2, __fmaf_rn(m3, v1, m0 * v0));          \
+    o1 = __fmaf_rn(m7, v2, __fmaf_rn(m4, v1, m1 * v0));          \
+    o2 = __fmaf_rn(m8, v2, __fmaf_rn(m5, v1, m2 * v0));
+    float x0 = 0.f, x1 = 0.f, x2 = 0.f;
+    float u0, u1, u2, w0, w1, w2;
+    LCS_MINV(r0, r1, r2, u0, u1, u2)
+    // w = A u (one extra synchronisation before the loop)
+    if (own) __stcg(&pg2[i], make_float4(u0, u1, u2, 0.0f));
+    if (!pipe_barrier(a.bar_count, a.bar_gen, a.stats, &s_fail)) return;
+    row_matvec(a, i, row, own, slice, lane, pg2, u0, u1, u2, w0, w1, w2);
+    float p0 = 0.f, p1 = 0.f, p2 = 0.f, s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    float q0 = 0.f, q1 = 0.f, q2 = 0.f, z0 = 0.f, z1 = 0.f, z2 = 0.f;
+    float gamma_old = 0.0f, alpha_old = 0.0f, norm_r0 = 0.0f, norm_r = 0.0f, gamma = 0.0f;
+    int iter = 0, status = 0;
+    for (iter = 0; iter < a.max_iter; ++iter) {
+        double dg, dd, dr;
+        if (a.fp64) {
+            dg = (double)r0 * u0 + (double)r1 * u1 + (double)r2 * u2;
+            dd = (double)w0 * u0 + (double)w1 * u1 + (double)w2 * u2;
+            dr = (double)r0 * r0 + (double)r1 * r1 + (double)r2 * r2;
+        } else {
+            dg = __fmaf_rn(r2, u2, __fmaf_rn(r1, u1, r0 * u0));
+            dd = __fmaf_rn(w2, u2, __fmaf_rn(w1, u1, w0 * u0));
+            dr = __fmaf_rn(r2, r2, __fmaf_rn(r1, r1, r0 * r0));
+        }
+        if (!own) dg = dd = dr = 0.0;
+        double* part = a.part + 4 * (size_t)gridDim.x * (iter & 1);
+        block_partial3<BS>(dg, dd, dr, &part[4 * blockIdx.x]);
+        float mm0, mm1, mm2;
+        LCS_MINV(w0, w1, w2, mm0, mm1, mm2)
+        float4* mbuf = (iter & 1) ? pg2 : a.pg;
+        if (own) __stcg(&mbuf[i], make_float4(mm0, mm1, mm2, 0.0f));
+        if (!pipe_barrier(a.bar_count, a.bar_gen, a.stats, &s_fail)) return;
+        double sg, sd, sr;
+        grid_sum3(part, sg, sd, sr);
+        gamma = (float)sg;
+        const float delta = (float)sd;
+        norm_r = sqrtf((float)sr);
+        if (iter == 0) norm_r0 = norm_r;
+        if (iter % a.check_every == 0) {
+            if (isnan(gamma) || isinf(gamma)) { status = LCS_ERR_NAN; break; }
+            if (gamma < a.abs_rz_tol) break;
+            if (a.rel_tol > 0.0f && norm_r <= a.rel_tol * norm_r0) break;
+        }
+        float beta, alpha;
+        if (iter == 0) {
+            beta = 0.0f;
+            alpha = safe_div(gamma, delta);
+        } else {
+            beta = safe_div(gamma, gamma_old);
+            const float den = delta - (alpha_old != 0.0f ? beta * gamma / alpha_old : 0.0f);
+            alpha = safe_div(gamma, den);
+        }
+        float n0, n1, n2;
+        row_matvec(a, i, row, own, slice, lane, mbuf, mm0, mm1, mm2, n0, n1, n2);
+        z0 = n0 + beta * z0; z1 = n1 + beta * z1; z2 = n2 + beta * z2;
+        q0 = mm0 + beta * q0; q1 = mm1 + beta * q1; q2 = mm2 + beta * q2;
+        s0 = w0 + beta * s0; s1 = w1 + beta * s1; s2 = w2 + beta * s2;
+        p0 = u0 + beta * p0; p1 = u1 + beta * p1; p2 = u2 + beta * p2;
+        x0 += alpha * p0; x1 += alpha * p1; x2 += alpha * p2;
+        r0 -= alpha * s0; r1 -= alpha * s1; r2 -= alpha * s2;
+        u0 -= alpha * q0; u1 -= alpha * q1; u2 -= alpha * q2;
+        w0 -= alpha * z0; w1 -= alpha * z1; w2 -= alpha * z2;
+        gamma_old = gamma;
+        alpha_old = alpha;
+    }
+#undef LCS_MINV
+    if (own) a.x[i] = make_float4(x0, x1, x2, 0.0f);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.stats->iterations = iter;
+        a.stats->rel_residual = norm_r0 > 0.0f ? norm_r / norm_r0 : 0.0f;
+        a.stats->dot_rz = gamma;
+        if (a.stats->status == LCS_OK) a.stats->status = status;
+    }
+}
+
 }  // namespace
 
 struct lcs_pcg {
@@ -649,6 +890,7 @@ struct lcs_pcg {
 
 static constexpr int kRowLanes = 4;
 static constexpr int kPlainBlocks = 256;
+static constexpr int kRowMaxBlocks = 1024;
 
 extern "C" int lcs_pcg_create(uint32_t n, lcs_pcg** out)
 {
@@ -662,7 +904,8 @@ extern "C" int lcs_pcg_create(uint32_t n, lcs_pcg** out)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_fused<kRowLanes>, kFusedThreads, 0);
     if (per_sm > 1) per_sm = 1;
     p->fused_grid = sms * (per_sm > 0 ? per_sm : 1);
-    const int parts = 1024 + (p->fused_grid > kPlainBlocks ? p->fused_grid : kPlainBlocks);  // >= 4 per rows block
+    // fused: 3 doubles per block; row-resident: 4 per block, twice (pipelined) for up to kRowMaxBlocks
+    const int parts = 8 * kRowMaxBlocks / 3 + 1 + (p->fused_grid > kPlainBlocks ? p->fused_grid : kPlainBlocks);
     cudaError_t e = cudaSuccess;
     auto A = [&](void** q, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(q, bytes); };
     A((void**)&p->r, 16 * (size_t)n);
@@ -771,16 +1014,9 @@ static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* 
                       const float* m_val, Bsr B, const float4* b, float4* x, const lcs_pcg_opts& o,
                       lcs_pcg_stats* stats, cudaStream_t s)
 {
-    if (P->rows_capacity < 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_rows<kRowThreads>, kRowThreads, 0);
-        int blocks = sms * per_sm;
-        if (blocks > 1024) blocks = 1024;  // partial-sum space
-        P->rows_capacity = blocks * kRowThreads;
-    }
+    if (P->rows_capacity < 0) P->rows_capacity = (int)lcs_pcg_rows_capacity();
     if ((int64_t)P->n > P->rows_capacity) return LCS_ERR_CAPACITY;
+    const bool pipe = (o.flags & LCS_PCG_PIPELINED) != 0;
     RowArgs a;
     a.n = P->n;
     a.diag = diag;
@@ -805,8 +1041,14 @@ static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* 
     LCS_CUDA_TRY(cudaMemsetAsync(P->bar, 0, sizeof(unsigned), s));
     void* args[] = {&a};
     const int grid = (int)((P->n + kRowThreads - 1) / kRowThreads);
-    LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_rows<kRowThreads>, dim3(grid), dim3(kRowThreads), args,
-                                             0, s));
+    float4* pg2 = P->q;  // second buffer of the exchanged vector (pipelined form)
+    void* pargs[] = {&a, &pg2};
+    if (pipe)
+        LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_pipe<kRowThreads>, dim3(grid), dim3(kRowThreads),
+                                                 pargs, 0, s));
+    else
+        LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_rows<kRowThreads>, dim3(grid), dim3(kRowThreads),
+                                                 args, 0, s));
     lcs_count_launch();
     if (stats && !(o.flags & LCS_PCG_NO_STATS)) {
         LCS_CUDA_TRY(cudaMemcpyAsync(stats, P->d_stats, sizeof(lcs_pcg_stats), cudaMemcpyDeviceToHost, s));
@@ -816,14 +1058,17 @@ static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* 
     return LCS_OK;
 }
 
+// rows both row-resident kernels hold co-resident (the smaller of their occupancies)
 int64_t lcs_pcg_rows_capacity()
 {
-    int dev = 0, sms = 0, per_sm = 0;
+    int dev = 0, sms = 0, per_sm = 0, per_sm2 = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_rows<kRowThreads>, kRowThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_pcg_pipe<kRowThreads>, kRowThreads, 0);
+    if (per_sm2 < per_sm) per_sm = per_sm2;
     int64_t blocks = (int64_t)sms * per_sm;
-    if (blocks > 1024) blocks = 1024;
+    if (blocks > kRowMaxBlocks) blocks = kRowMaxBlocks;  // partial-sum space
     return blocks * kRowThreads;
 }
 

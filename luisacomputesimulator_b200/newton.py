@@ -18,12 +18,13 @@ class NewtonSolver:
     """One scene, state resident on the device.
 
     plain=True selects the reference's dispatch structure (the one-scene comparator);
-    fp64=True the precision form; profile=True per-phase CUDA-event timing.
+    fp64=True the precision form; profile=True per-phase CUDA-event timing;
+    pipelined=True the pipelined row-resident PCG (fused mode).
     """
 
     def __init__(self, scene, plain=False, fp64=False, profile=False, nonlinear_iters=3, pcg_max_iter=100,
                  pcg_rel_tol=1e-4, pcg_abs_rz_tol=1e-10, pcg_check_every=25, damping=2.0, use_floor=False,
-                 floor_y=0.0, stream=None):
+                 floor_y=0.0, stream=None, pipelined=False):
         self.lib = A.load()
         self.scene = scene
         sc = scene
@@ -73,7 +74,7 @@ class NewtonSolver:
         d.pcg_rel_tol, d.pcg_abs_rz_tol, d.pcg_check_every = pcg_rel_tol, pcg_abs_rz_tol, pcg_check_every
         self.desc = d
         flags = (A.LCS_NEWTON_PLAIN if plain else 0) | (A.LCS_NEWTON_FP64 if fp64 else 0) | \
-            (A.LCS_NEWTON_PROFILE if profile else 0)
+            (A.LCS_NEWTON_PROFILE if profile else 0) | (A.LCS_NEWTON_PCG_PIPELINED if pipelined else 0)
         s = C.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
         h = C.c_void_p()
         A.check(self.lib.lcs_newton_create(C.byref(d), flags, s, C.byref(h)), "lcs_newton_create")
@@ -122,6 +123,13 @@ class NewtonSolver:
 
     def reset_profile(self):
         A.check(self.lib.lcs_newton_reset_profile(self.h), "lcs_newton_reset_profile")
+
+    def pcg_kind(self):
+        """'plain', 'fused' (persistent CSR solve), 'rows' or 'pipelined' (row-resident)."""
+        return ["plain", "fused", "rows", "pipelined"][self.lib.lcs_newton_pcg_kind(self.h)]
+
+    def uses_row_pcg(self):
+        return self.pcg_kind() in ("rows", "pipelined")
 
     def counts(self):
         v = [C.c_uint32() for _ in range(4)]

@@ -585,6 +585,90 @@ float orc_edge_edge_ccd(const float* ea00, const float* ea01, const float* eb00,
     return toi;
 }
 
+/* ---- all-FP64 ACCD: the same algorithm with every quantity in double (the error reference of
+ * the precision form; inputs are the FP32 positions promoted exactly) ---- */
+static void centerize_d(v3_d* x)
+{
+    v3_d mov = mk_d(0.0, 0.0, 0.0);
+    for (int k = 0; k < 4; ++k) mov = add_d(mov, scl_d(0.25, x[k]));
+    for (int k = 0; k < 4; ++k) x[k] = sub_d(x[k], mov);
+}
+
+static double ccd_helper_d(const v3_d* x0, const v3_d* dx, double u_max, int is_ee, double offset)
+{
+    double toi = 0.0;
+    const double max_t = 1.25;
+    double eps = 0.01 * (sqrt(dist2_of_d(is_ee, x0)) - offset);
+    double target = eps + offset, eps_sqr = eps * eps, inv_u_max = 1.0 / u_max;
+    for (unsigned iter = 0;; ++iter) {
+        if (iter > 10000u) return 0.001;
+        v3_d xt[4];
+        for (int k = 0; k < 4; ++k) xt[k] = add_d(x0[k], scl_d(toi, dx[k]));
+        double d2 = dist2_of_d(is_ee, xt);
+        double dmt = (d2 - target * target) / (sqrt(d2) + target);
+        if ((max_t - toi) * u_max < dmt - eps) return max_t;
+        if (toi > 0.0 && dmt * dmt < eps_sqr) break;
+        double nt = toi + dmt * inv_u_max;
+        if (nt == toi) break;
+        toi = nt;
+        if (toi > max_t) return max_t;
+    }
+    return toi;
+}
+
+double orc_ccd_f64(int is_ee, const float* a0, const float* a1, const float* a2, const float* a3,
+                   const float* b0, const float* b1, const float* b2, const float* b3, float offset)
+{
+    const float* A[4] = {a0, a1, a2, a3};
+    const float* Bv[4] = {b0, b1, b2, b3};
+    v3_d x0[4], dx[4];
+    for (int k = 0; k < 4; ++k) {
+        x0[k] = mk_d(A[k][0], A[k][1], A[k][2]);
+        dx[k] = sub_d(mk_d(Bv[k][0], Bv[k][1], Bv[k][2]), x0[k]);
+    }
+    centerize_d(x0);
+    centerize_d(dx);
+    double m = 0.0;
+    for (int i = 0; i < 4; ++i)
+        for (int j = i + 1; j < 4; ++j) {
+            v3_d du = sub_d(dx[i], dx[j]);
+            double q = dot_d(du, du);
+            if (q > m) m = q;
+        }
+    double u_max = sqrt(m);
+    if (u_max == 0.0) return 1.25;
+    return ccd_helper_d(x0, dx, u_max, is_ee, (double)offset);
+}
+
+/* per-pair FP64 TOI over a candidate list (VF: vid, fid over faces; EE: edge pairs) */
+void orc_ccd_f64_list(int is_ee, const uint32_t* pairs, uint32_t n_pairs, const float* x0, const float* x1,
+                      const uint32_t* elems, const uint32_t* body, const float* offset, double* toi)
+{
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (long long pl = 0; pl < (long long)n_pairs; ++pl) {
+        uint32_t v[4];
+        int skip;
+        if (is_ee) {
+            uint32_t l = pairs[2 * pl], r = pairs[2 * pl + 1];
+            v[0] = elems[2 * (size_t)l]; v[1] = elems[2 * (size_t)l + 1];
+            v[2] = elems[2 * (size_t)r]; v[3] = elems[2 * (size_t)r + 1];
+            skip = v[0] == v[2] || v[0] == v[3] || v[1] == v[2] || v[1] == v[3] ||
+                   (body[v[0]] != 0xFFFFFFFFu && body[v[0]] == body[v[2]]);
+        } else {
+            uint32_t f = pairs[2 * pl + 1];
+            v[0] = pairs[2 * pl];
+            v[1] = elems[4 * (size_t)f]; v[2] = elems[4 * (size_t)f + 1]; v[3] = elems[4 * (size_t)f + 2];
+            skip = v[0] == v[1] || v[0] == v[2] || v[0] == v[3] ||
+                   (body[v[0]] != 0xFFFFFFFFu && body[v[0]] == body[v[1]]);
+        }
+        if (skip) { toi[pl] = 1.25; continue; }
+        float th = offset[v[0]] + offset[is_ee ? v[2] : v[1]];
+        toi[pl] = orc_ccd_f64(is_ee, x0 + 4 * (size_t)v[0], x0 + 4 * (size_t)v[1], x0 + 4 * (size_t)v[2],
+                              x0 + 4 * (size_t)v[3], x1 + 4 * (size_t)v[0], x1 + 4 * (size_t)v[1],
+                              x1 + 4 * (size_t)v[2], x1 + 4 * (size_t)v[3], th);
+    }
+}
+
 float orc_pt_dist2(const float* p, const float* t0, const float* t1, const float* t2)
 {
     return pt_dist2_f(ldp(p), ldp(t0), ldp(t1), ldp(t2));

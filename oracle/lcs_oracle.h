@@ -86,6 +86,12 @@ float orc_ccd_vf(const uint32_t* pairs, uint32_t n_pairs, const float* x0, const
 float orc_ccd_ee(const uint32_t* pairs, uint32_t n_pairs, const float* x0, const float* x1,
                  const uint32_t* edges, const uint32_t* body, const float* offset,
                  float* toi_per_pair, int fp64_final);
+/* all-FP64 ACCD (every quantity in double; error reference for the precision form, not a
+ * restatement of a reference function): is_ee 0 = point (a0) vs triangle (a1..a3) */
+double orc_ccd_f64(int is_ee, const float* a0, const float* a1, const float* a2, const float* a3,
+                   const float* b0, const float* b1, const float* b2, const float* b3, float offset);
+void orc_ccd_f64_list(int is_ee, const uint32_t* pairs, uint32_t n_pairs, const float* x0, const float* x1,
+                      const uint32_t* elems, const uint32_t* body, const float* offset, double* toi);
 uint32_t orc_dcd_vf(const uint32_t* pairs, uint32_t n_pairs, const float* x, const uint32_t* faces,
                     const uint32_t* body, const float* vert_area, const float* face_area,
                     const float* dhat, const float* offset, float kappa, orc_pair* out,

@@ -72,6 +72,7 @@ def _declare(L):
         "orc_barrier": (None, [F32, F32, P, P, P]),
         "orc_ccd_vf": (F32, [P, U32, P, P, P, P, P, P, I32]),
         "orc_ccd_ee": (F32, [P, U32, P, P, P, P, P, P, I32]),
+        "orc_ccd_f64_list": (None, [I32, P, U32, P, P, P, P, P, P]),
         "orc_dcd_vf": (U32, [P, U32, P, P, P, P, P, P, P, F32, P, U32]),
         "orc_dcd_ee": (U32, [P, U32, P, P, P, P, P, P, F32, P, U32]),
         "orc_contact_grad_diag": (None, [P, U32, P, P]),
@@ -244,6 +245,18 @@ def ccd_ee(pairs, x0, x1, edges, body, offset, per_pair=True, fp64_final=False):
     g = lib().orc_ccd_ee(_p(pairs), n, _p(f4(x0)), _p(f4(x1)), _p(np.ascontiguousarray(edges, np.uint32)),
                          _p(np.ascontiguousarray(body, np.uint32)), _p(_v(offset)), _p(toi), int(fp64_final))
     return g, toi
+
+
+def ccd_f64(is_ee, pairs, x0, x1, elems, body, offset):
+    """Per-pair TOI of the same ACCD iteration carried out entirely in double precision (the
+    error reference of the precision form).  elems: faces (n, 4) for VF, edges (n, 2) for EE."""
+    pairs = np.ascontiguousarray(pairs, np.uint32)
+    n = pairs.shape[0]
+    toi = np.zeros(max(n, 1), np.float64)
+    el = u4(elems) if not is_ee else np.ascontiguousarray(elems, np.uint32)
+    lib().orc_ccd_f64_list(int(is_ee), _p(pairs), n, _p(f4(x0)), _p(f4(x1)), _p(el),
+                           _p(np.ascontiguousarray(body, np.uint32)), _p(_v(offset)), _p(toi))
+    return toi[:n]
 
 
 def dcd_vf(pairs, x, faces, body, vert_area, face_area, dhat, offset, kappa):

@@ -150,3 +150,30 @@ def test_contact_assembly(name):
     e = float(host(det.energy)[0])
     oe = O.contact_energy(got, x0, sc.d_hat, sc.offset, fp64=True)
     assert e == pytest.approx(oe, rel=1e-5)
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_ccd_fp64_form_matches_fp64_oracle(name):
+    """The precision form's step bound: the ACCD iteration in FP64, bit-exact against the all-FP64
+    oracle after rounding toward zero, so no per-pair TOI exceeds the FP64 value."""
+    sc, x0, x1 = SCENES[name]
+    vf, ee = _candidates(sc, x0, x1)
+    D = SceneOnDevice(sc)
+    det = NarrowPhasesDetector(sc.num_verts, sc.edges.shape[0])
+    _load(det, vf, ee)
+    tvf = torch.zeros(det.cap_vf, dtype=torch.float32, device="cuda")
+    tee = torch.zeros(det.cap_ee, dtype=torch.float32, device="cuda")
+    det.reset_toi()
+    det.vf_ccd_query(dev(x0), dev(x1), D.faces, D.body, D.offset, tvf, fp64=True)
+    det.ee_ccd_query(dev(x0), dev(x1), D.edges, D.body, D.offset, tee, fp64=True)
+    torch.cuda.synchronize()
+    for got, p, el, is_ee in ((host(tvf)[: len(vf)], vf, sc.faces, 0), (host(tee)[: len(ee)], ee, sc.edges, 1)):
+        ref = O.ccd_f64(is_ee, p, x0, x1, el, sc.body, sc.offset)
+        want = ref.astype(np.float32)
+        want = np.where(want.astype(np.float64) > ref, np.nextafter(want, np.float32(0)), want)
+        np.testing.assert_array_equal(got, want)
+        assert np.all(got.astype(np.float64) <= ref)
+        # and the FP32 form stays within 1e-6 relative of the FP64 iteration on these scenes
+        _, t32 = (O.ccd_ee if is_ee else O.ccd_vf)(p, x0, x1, el, sc.body, sc.offset)
+        m = ref < 1.25
+        assert np.all(np.abs(t32[m] - ref[m]) <= 1e-6 * ref[m])

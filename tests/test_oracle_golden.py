@@ -157,3 +157,28 @@ def test_pcg_solves_spd_system():
     ref = np.linalg.solve(K, b[:, :3].reshape(-1).astype(np.float64))
     assert st["status"] == 0 and st["rel_residual"] <= 1e-6
     np.testing.assert_allclose(x[:, :3].reshape(-1), ref, rtol=1e-4, atol=1e-5)
+
+
+def test_fp64_ccd_oracle_close_to_fp32_and_known_answer():
+    """The all-FP64 ACCD (error reference of the precision form) agrees with the FP32 iteration to
+    about float precision and reproduces the point-triangle known answer."""
+    import numpy as np
+    from tests import scenarios as SC
+    sc, x = SC.cloth_touching_sphere(gap=2e-3)
+    x1 = x.copy()
+    x1[: 64 * 64, 1] -= 6e-3
+    tf = O.lbvh_build(O.TREE_FACE, x, sc.faces, sc.num_verts)
+    O.lbvh_refit(tf, x, x1, sc.faces, sc.offset)
+    vf, _ = O.lbvh_query_vf(tf, x, x1, sc.d_hat, sc.offset)
+    ref = O.ccd_f64(0, vf, x, x1, sc.faces, sc.body, sc.offset)
+    _, t32 = O.ccd_vf(vf, x, x1, sc.faces, sc.body, sc.offset)
+    m = ref < 1.25
+    assert m.sum() > 50
+    assert np.all(np.abs(t32[m] - ref[m]) <= 1e-6 * ref[m])
+    g = GOLD["vf_ccd"]
+    x0 = np.array([g["t0_p"], g["t0_f0"], g["t0_f1"], g["t0_f2"]], np.float32)
+    x1 = np.array([g["t1_p"], g["t1_f0"], g["t1_f1"], g["t1_f2"]], np.float32)
+    off = np.array([g["offset"] / 2] * 4, np.float32)
+    toi = O.ccd_f64(0, np.array([[0, 0]], np.uint32), x0, x1, np.array([[1, 2, 3, 0]], np.uint32),
+                    np.full(4, 0xFFFFFFFF, np.uint32), off)[0]
+    assert abs(toi - g["desire_toi"]) <= 1e-6 * g["desire_toi"]
