@@ -39,7 +39,7 @@ def args_():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--mode", choices=["fused", "plain"], default="fused")
     p.add_argument("--fp64", action="store_true", help="precision form")
-    p.add_argument("--pcg", choices=["rows", "pipelined"], default="rows",
+    p.add_argument("--pcg", choices=["rows", "pipelined"], default="pipelined",
                    help="fused mode: row-resident PCG recurrences (classic: 3 grid syncs/iter; pipelined: 1)")
     p.add_argument("--e2e-steps", type=int, default=10)
     p.add_argument("--cpu-iters", type=int, default=0, help="CPU baseline sample (0: auto, ~10-30 s)")

@@ -50,14 +50,16 @@ __device__ __forceinline__ float block_min(float v)
 
 // fn_narrow_phase_vf_ccd_query (EE = false, narrow_phase.cpp:293-436) and
 // fn_narrow_phase_ee_ccd_query (EE = true, narrow_phase.cpp:438-593)
-template <bool EE>
+// F64: the precision form's all-FP64 iteration (LCS_CCD_FP64), a separate instantiation so the
+// FP32 kernel keeps its register budget
+template <bool EE, bool F64>
 __global__ void __launch_bounds__(256) k_ccd(const uint2* __restrict__ pairs, const uint32_t* d_count, uint32_t cap,
                                              const float4* __restrict__ x0, const float4* __restrict__ x1,
                                              const uint32_t* __restrict__ elems, const uint32_t* __restrict__ body,
                                              const float* __restrict__ offset, float* d_toi,
                                              float* __restrict__ toi_per_pair, int flags)
 {
-    const bool fp64_final = (flags & LCS_CCD_FP64_FINAL) != 0, fp64 = (flags & LCS_CCD_FP64) != 0;
+    const bool fp64_final = (flags & LCS_CCD_FP64_FINAL) != 0;
     const uint32_t n = pair_count(d_count, cap);
     float local = 1.0f;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
@@ -85,7 +87,7 @@ __global__ void __launch_bounds__(256) k_ccd(const uint2* __restrict__ pairs, co
                 b[k] = ld3(x1, v[k]);
             }
             const float th = __ldg(&offset[v[0]]) + __ldg(&offset[EE ? v[2] : v[1]]);
-            toi = fp64 ? __double2float_rz(accd_ccd_f64<EE>(a, b, th)) : accd_ccd<EE>(a, b, th, fp64_final);
+            toi = F64 ? __double2float_rz(accd_ccd_f64<EE>(a, b, th)) : accd_ccd<EE>(a, b, th, fp64_final);
         }
         if (toi_per_pair) toi_per_pair[p] = toi;
         local = fmn(local, toi / 1.25f);
@@ -499,7 +501,8 @@ extern "C" int lcs_ccd_vf(const uint32_t* pairs, const uint32_t* d_count, uint32
     if (!d_count || !x0 || !x1 || !faces || !body || !offset || !d_toi || (capacity && !pairs))
         return lcs_fail(LCS_ERR_INVALID, "lcs_ccd_vf: bad argument");
     if (capacity == 0) return LCS_OK;
-    k_ccd<false><<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
+    auto kern = (flags & LCS_CCD_FP64) ? k_ccd<false, true> : k_ccd<false, false>;
+    kern<<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
         reinterpret_cast<const uint2*>(pairs), d_count, capacity, reinterpret_cast<const float4*>(x0),
         reinterpret_cast<const float4*>(x1), faces, body, offset, d_toi, toi_per_pair, flags);
     lcs_count_launch();
@@ -514,7 +517,8 @@ extern "C" int lcs_ccd_ee(const uint32_t* pairs, const uint32_t* d_count, uint32
     if (!d_count || !x0 || !x1 || !edges || !body || !offset || !d_toi || (capacity && !pairs))
         return lcs_fail(LCS_ERR_INVALID, "lcs_ccd_ee: bad argument");
     if (capacity == 0) return LCS_OK;
-    k_ccd<true><<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
+    auto kern = (flags & LCS_CCD_FP64) ? k_ccd<true, true> : k_ccd<true, false>;
+    kern<<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
         reinterpret_cast<const uint2*>(pairs), d_count, capacity, reinterpret_cast<const float4*>(x0),
         reinterpret_cast<const float4*>(x1), edges, body, offset, d_toi, toi_per_pair, flags);
     lcs_count_launch();

@@ -590,7 +590,7 @@ __global__ void __launch_bounds__(BS) k_pcg_rows(RowArgs a)
             q2 = __fmaf_rn(c2.z, p2, __fmaf_rn(c1.z, p1, c0.z * p0));
         }
         float o0 = 0.f, o1 = 0.f, o2 = 0.f;
-        if (a.sell) {
+        if (a.sell && slice * 32 < a.n) {  // threads past the last slice have no slot range
             const uint32_t off = __ldg(&a.m_ptr[slice]), end = __ldg(&a.m_ptr[slice + 1]);
             for (uint32_t k = off; k < end; ++k) {
                 const uint32_t cj = __ldg(&a.m_col[32 * k + lane]);
@@ -714,27 +714,49 @@ __device__ __forceinline__ void block_partial3(double v0, double v1, double v2, 
     }
 }
 
-__device__ __forceinline__ void grid_sum3(const double* part, double& o0, double& o1, double& o2)
+// Grid-wide sums of the per-block partials, split in two so that the loads overlap other work:
+// grid_fetch3 issues this thread's share of the loads (blocks t, t + BS, ... in that order),
+// grid_reduce3 combines them in a fixed order (warp shuffles, then warps in index order).  Every
+// block performs the same operations on the same data, so all get bit-identical sums.
+struct Fetch3 {
+    double v0, v1, v2;
+};
+
+template <int BS>
+__device__ __forceinline__ Fetch3 grid_fetch3(const double* part)
 {
+    Fetch3 f{0.0, 0.0, 0.0};
+#pragma unroll 2
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += BS) {
+        f.v0 += __ldcg(&part[4 * b + 0]);
+        f.v1 += __ldcg(&part[4 * b + 1]);
+        f.v2 += __ldcg(&part[4 * b + 2]);
+    }
+    return f;
+}
+
+template <int BS>
+__device__ __forceinline__ void grid_reduce3(Fetch3 f, double& o0, double& o1, double& o2)
+{
+    __shared__ double s[BS / 32][3];
     __shared__ double so[3];
-    if (threadIdx.x < 32) {
-        double v0 = 0.0, v1 = 0.0, v2 = 0.0;
-        for (uint32_t b = threadIdx.x; b < gridDim.x; b += 32) {
-            v0 += __ldcg(&part[4 * b + 0]);
-            v1 += __ldcg(&part[4 * b + 1]);
-            v2 += __ldcg(&part[4 * b + 2]);
-        }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            v0 += __shfl_xor_sync(0xFFFFFFFFu, v0, o);
-            v1 += __shfl_xor_sync(0xFFFFFFFFu, v1, o);
-            v2 += __shfl_xor_sync(0xFFFFFFFFu, v2, o);
-        }
-        if (threadIdx.x == 0) {
-            so[0] = v0;
-            so[1] = v1;
-            so[2] = v2;
-        }
+    for (int o = 16; o > 0; o >>= 1) {
+        f.v0 += __shfl_xor_sync(0xFFFFFFFFu, f.v0, o);
+        f.v1 += __shfl_xor_sync(0xFFFFFFFFu, f.v1, o);
+        f.v2 += __shfl_xor_sync(0xFFFFFFFFu, f.v2, o);
+    }
+    if (lane_id() == 0) {
+        s[threadIdx.x >> 5][0] = f.v0;
+        s[threadIdx.x >> 5][1] = f.v1;
+        s[threadIdx.x >> 5][2] = f.v2;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < BS / 32; ++w) t += s[w][threadIdx.x];
+        so[threadIdx.x] = t;
     }
     __syncthreads();
     o0 = so[0];
@@ -743,7 +765,26 @@ __device__ __forceinline__ void grid_sum3(const double* part, double& o0, double
     __syncthreads();
 }
 
-// A v for the owned row: diagonal block + material (CSR or SELL-32) + contact (CSR)
+// streamed read-only load that does not displace L1 lines (matrix values: read once per iteration)
+__device__ __forceinline__ float ld_stream(const float* p)
+{
+    float v;
+    asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ void acc_block_s(const float* m, float4 v, float& q0, float& q1, float& q2)
+{
+    // SELL-32 slot: component c of the slot at m[c * 32]
+    q0 += __fmaf_rn(ld_stream(m + 6 * 32), v.z, __fmaf_rn(ld_stream(m + 3 * 32), v.y, ld_stream(m) * v.x));
+    q1 += __fmaf_rn(ld_stream(m + 7 * 32), v.z, __fmaf_rn(ld_stream(m + 4 * 32), v.y, ld_stream(m + 32) * v.x));
+    q2 += __fmaf_rn(ld_stream(m + 8 * 32), v.z, __fmaf_rn(ld_stream(m + 5 * 32), v.y, ld_stream(m + 2 * 32) * v.x));
+}
+
+// A v for the owned row: diagonal block + material (CSR or SELL-32) + contact (CSR).  The SELL
+// and contact loops issue the column loads and the gathers of several blocks before using them
+// (the gathers depend on the columns, the products on the gathers: unrolled, a row pays two
+// memory latencies per four blocks instead of two per block); the sum order is unchanged.
 __device__ __forceinline__ void row_matvec(const RowArgs& a, uint32_t i, uint32_t row, bool own, uint32_t slice,
                                           uint32_t lane, const float4* src, float v0, float v1, float v2, float& q0,
                                           float& q1, float& q2)
@@ -753,11 +794,22 @@ __device__ __forceinline__ void row_matvec(const RowArgs& a, uint32_t i, uint32_
     q1 = __fmaf_rn(c2.y, v2, __fmaf_rn(c1.y, v1, c0.y * v0));
     q2 = __fmaf_rn(c2.z, v2, __fmaf_rn(c1.z, v1, c0.z * v0));
     float o0 = 0.f, o1 = 0.f, o2 = 0.f;
-    if (a.sell) {
+    if (a.sell && slice * 32 < a.n) {  // threads past the last slice have no slot range
         const uint32_t off = __ldg(&a.m_ptr[slice]), end = __ldg(&a.m_ptr[slice + 1]);
-        for (uint32_t k = off; k < end; ++k) {
+        uint32_t k = off;
+        for (; k + 4 <= end; k += 4) {
+            const uint32_t j0 = __ldg(&a.m_col[32 * k + lane]), j1 = __ldg(&a.m_col[32 * (k + 1) + lane]);
+            const uint32_t j2 = __ldg(&a.m_col[32 * (k + 2) + lane]), j3 = __ldg(&a.m_col[32 * (k + 3) + lane]);
+            const float4 p0 = __ldcg(&src[j0]), p1 = __ldcg(&src[j1]), p2 = __ldcg(&src[j2]), p3 = __ldcg(&src[j3]);
+            const float* m = a.m_val + (size_t)9 * 32 * k + lane;
+            acc_block_s(m, p0, o0, o1, o2);
+            acc_block_s(m + 9 * 32, p1, o0, o1, o2);
+            acc_block_s(m + 18 * 32, p2, o0, o1, o2);
+            acc_block_s(m + 27 * 32, p3, o0, o1, o2);
+        }
+        for (; k < end; ++k) {
             const uint32_t cj = __ldg(&a.m_col[32 * k + lane]);
-            acc_block(a.m_val + (size_t)9 * 32 * k + lane, 32, __ldcg(&src[cj]), o0, o1, o2);
+            acc_block_s(a.m_val + (size_t)9 * 32 * k + lane, __ldcg(&src[cj]), o0, o1, o2);
         }
     } else if (a.m_ptr && own) {
         const uint32_t end = __ldg(&a.m_ptr[i + 1]);
@@ -766,8 +818,14 @@ __device__ __forceinline__ void row_matvec(const RowArgs& a, uint32_t i, uint32_
     }
     if (a.B.rp && own) {
         const uint32_t end = __ldcg(&a.B.rp[i + 1]);
-        for (uint32_t k = __ldcg(&a.B.rp[i]); k < end; ++k)
-            acc_block(a.B.val + 9 * (size_t)k, 1, __ldcg(&src[__ldcg(&a.B.col[k])]), o0, o1, o2);
+        uint32_t k = __ldcg(&a.B.rp[i]);
+        for (; k + 2 <= end; k += 2) {
+            const uint32_t j0 = __ldcg(&a.B.col[k]), j1 = __ldcg(&a.B.col[k + 1]);
+            const float4 p0 = __ldcg(&src[j0]), p1 = __ldcg(&src[j1]);
+            acc_block(a.B.val + 9 * (size_t)k, 1, p0, o0, o1, o2);
+            acc_block(a.B.val + 9 * (size_t)(k + 1), 1, p1, o0, o1, o2);
+        }
+        if (k < end) acc_block(a.B.val + 9 * (size_t)k, 1, __ldcg(&src[__ldcg(&a.B.col[k])]), o0, o1, o2);
     }
     q0 += o0;
     q1 += o1;
@@ -775,7 +833,7 @@ __device__ __forceinline__ void row_matvec(const RowArgs& a, uint32_t i, uint32_
 }
 
 template <int BS>
-__global__ void __launch_bounds__(BS) k_pcg_pipe(RowArgs a, float4* pg2)
+__global__ void __launch_bounds__(BS, 3) k_pcg_pipe(RowArgs a, float4* pg2)
 {
     __shared__ int s_fail;
     if (threadIdx.x == 0) s_fail = 0;
@@ -830,8 +888,13 @@ __global__ void __launch_bounds__(BS) k_pcg_pipe(RowArgs a, float4* pg2)
         float4* mbuf = (iter & 1) ? pg2 : a.pg;
         if (own) __stcg(&mbuf[i], make_float4(mm0, mm1, mm2, 0.0f));
         if (!pipe_barrier(a.bar_count, a.bar_gen, a.stats, &s_fail)) return;
+        // the partial-sum loads are in flight while this row computes n = A m (which needs no
+        // scalar of this iteration)
+        const Fetch3 f = grid_fetch3<BS>(part);
+        float n0, n1, n2;
+        row_matvec(a, i, row, own, slice, lane, mbuf, mm0, mm1, mm2, n0, n1, n2);
         double sg, sd, sr;
-        grid_sum3(part, sg, sd, sr);
+        grid_reduce3<BS>(f, sg, sd, sr);
         gamma = (float)sg;
         const float delta = (float)sd;
         norm_r = sqrtf((float)sr);
@@ -841,17 +904,22 @@ __global__ void __launch_bounds__(BS) k_pcg_pipe(RowArgs a, float4* pg2)
             if (gamma < a.abs_rz_tol) break;
             if (a.rel_tol > 0.0f && norm_r <= a.rel_tol * norm_r0) break;
         }
-        float beta, alpha;
-        if (iter == 0) {
+        // alpha = gamma / (p.Ap) with p.Ap = delta - beta gamma / alpha_old.  That difference can
+        // cancel to below pcg_epsilon near convergence; a zero step there would leave the search
+        // directions inconsistent and the recurrences diverge, so the iteration restarts from
+        // the current residual instead (beta = 0, p = u), as on the first iteration.
+        float beta = 0.0f, alpha = 0.0f;
+        bool restart = iter == 0 || alpha_old == 0.0f;
+        if (!restart) {
+            beta = safe_div(gamma, gamma_old);
+            const float den = delta - beta * gamma / alpha_old;
+            restart = !(den >= kPcgEps);
+            if (!restart) alpha = gamma / den;
+        }
+        if (restart) {
             beta = 0.0f;
             alpha = safe_div(gamma, delta);
-        } else {
-            beta = safe_div(gamma, gamma_old);
-            const float den = delta - (alpha_old != 0.0f ? beta * gamma / alpha_old : 0.0f);
-            alpha = safe_div(gamma, den);
         }
-        float n0, n1, n2;
-        row_matvec(a, i, row, own, slice, lane, mbuf, mm0, mm1, mm2, n0, n1, n2);
         z0 = n0 + beta * z0; z1 = n1 + beta * z1; z2 = n2 + beta * z2;
         q0 = mm0 + beta * q0; q1 = mm1 + beta * q1; q2 = mm2 + beta * q2;
         s0 = w0 + beta * s0; s1 = w1 + beta * s1; s2 = w2 + beta * s2;

@@ -45,10 +45,11 @@ def test_one_newton_iteration_matches_cpu_restatement():
     assert abs(st.last_toi - toi) <= 1e-3 * toi + 1e-6
 
 
-@pytest.mark.parametrize("fp64", [False, True])
-def test_drop_stays_intersection_free(fp64):
+@pytest.mark.parametrize("fp64,pipelined", [(False, False), (True, False), (False, True)])
+def test_drop_stays_intersection_free(fp64, pipelined):
     sc = S.cloth_on_sphere(n=32)
-    gpu = NewtonSolver(sc, fp64=fp64)
+    gpu = NewtonSolver(sc, fp64=fp64, pipelined=pipelined)
+    assert gpu.pcg_kind() == ("pipelined" if pipelined else "rows")
     d0 = O.min_distance(sc, sc.x)
     for k in range(40):
         st = gpu.step()
@@ -62,10 +63,11 @@ def test_drop_stays_intersection_free(fp64):
     assert O.min_distance(sc, x) > 0.0 and d0 > 0.0
 
 
-def test_plain_and_fused_agree_on_a_step():
+@pytest.mark.parametrize("pipelined", [False, True])
+def test_plain_and_fused_agree_on_a_step(pipelined):
     sc = touching_scene()
     a = NewtonSolver(sc, plain=True, pcg_check_every=1)
-    b = NewtonSolver(sc, plain=False)
+    b = NewtonSolver(sc, plain=False, pipelined=pipelined)
     sa, sb = a.step(), b.step()
     assert sa.newton_iters == sb.newton_iters
     xa, xb = a.positions(), b.positions()
@@ -74,10 +76,10 @@ def test_plain_and_fused_agree_on_a_step():
 
 
 def test_twisted_tube_steps_small():
-    # a reduced tube (60 x 60) through the full step path, both modes
-    for plain in (False, True):
+    # a reduced tube (60 x 60) through the full step path, every mode
+    for plain, pipelined in ((False, False), (False, True), (True, False)):
         sc = S.twisted_tube(60, 60)
-        gpu = NewtonSolver(sc, plain=plain)
+        gpu = NewtonSolver(sc, plain=plain, pipelined=pipelined)
         for _ in range(5):
             st = gpu.step()
             assert 1 <= st.newton_iters <= 100  # the small-step rule may end the loop early
