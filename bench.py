@@ -118,8 +118,8 @@ def measured_peak():
 
 
 def committed_traffic():
-    """DRAM bytes per launch of the fused PCG kernel from the committed ncu summary (or None)."""
-    path = os.path.join(ROOT, "profiles", "pcg_fused_tube_traffic.txt")
+    """DRAM bytes per PCG iteration of the row-resident solve from the committed ncu capture (or None)."""
+    path = os.path.join(ROOT, "profiles", "k_pcg_pipe_tube88k_traffic.txt")
     try:
         for ln in open(path):
             if ln.startswith("bytes_per_iteration="):
