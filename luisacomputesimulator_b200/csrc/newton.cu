@@ -450,8 +450,9 @@ int build_material_pattern(lcs_newton* h, const lcs_scene_desc* d)
     }
     for (uint32_t r = 0; r < h->V; ++r) rp[r + 1] += rp[r];
     auto slot_of = [&](uint64_t key) { return (uint32_t)(std::lower_bound(uniq.begin(), uniq.end(), key) - uniq.begin()); };
-    // block base offset into mat_val for CSR block j: CSR 9 j (components contiguous) or, in
-    // SELL-32, ((slice_ptr[s] + k) * 9) * 32 + lane (components 32 floats apart)
+    // block base offset into mat_val for CSR block j: CSR 9 j (components contiguous) or, in the
+    // SELL-32 layout with 4-slot groups, ((g * 9) * 32 + lane) * 4 + slot % 4 for group g = slot / 4
+    // (components 128 floats apart; the row-resident PCG reads a group with float4 loads)
     std::vector<uint32_t> base(uniq.size());
     std::vector<uint32_t> sell_ptr, sell_col;
     if (h->sell) {
@@ -460,7 +461,7 @@ int build_material_pattern(lcs_newton* h, const lcs_scene_desc* d)
         for (uint32_t s = 0; s < ns; ++s) {
             uint32_t w = 0;
             for (uint32_t r = 32 * s; r < std::min(h->V, 32 * s + 32); ++r) w = std::max(w, rp[r + 1] - rp[r]);
-            sell_ptr[s + 1] = sell_ptr[s] + w;
+            sell_ptr[s + 1] = sell_ptr[s] + ((w + 3u) & ~3u);
         }
         sell_col.assign(32 * (size_t)sell_ptr[ns], 0);
         for (uint32_t s = 0; s < ns; ++s)
@@ -469,9 +470,9 @@ int build_material_pattern(lcs_newton* h, const lcs_scene_desc* d)
                 const uint32_t len = r < h->V ? rp[r + 1] - rp[r] : 0;
                 const uint32_t pad = r < h->V ? r : h->V - 1;  // zero block against a valid row
                 for (uint32_t k = 0; k < sell_ptr[s + 1] - sell_ptr[s]; ++k) {
-                    const size_t slot = (size_t)sell_ptr[s] + k;
-                    sell_col[32 * slot + lane] = k < len ? col[rp[r] + k] : pad;
-                    if (k < len) base[rp[r] + k] = (uint32_t)(9 * 32 * slot + lane);
+                    const size_t slot = (size_t)sell_ptr[s] + k, g = slot / 4, j = slot % 4;
+                    sell_col[(g * 32 + lane) * 4 + j] = k < len ? col[rp[r] + k] : pad;
+                    if (k < len) base[rp[r] + k] = (uint32_t)((g * 9 * 32 + lane) * 4 + j);
                 }
             }
         h->sell_vals = 9ull * 32 * sell_ptr[ns];
@@ -569,12 +570,12 @@ int newton_iteration(lcs_newton* h)
         LCS_CUDA_TRY(cudaMemsetAsync(h->mat_val, 0, sizeof(float) * h->sell_vals, h->s));
         if (h->E) {
             k_springs<<<G(h->E), 256, 0, h->s>>>(h->E, h->edges, h->rest_len, d.spring_k, h->x, h->b, h->diag,
-                                                 h->spring_slots, h->sell ? 32u : 1u, h->mat_val);
+                                                 h->spring_slots, h->sell ? 128u : 1u, h->mat_val);
             lcs_count_launch();
         }
         if (h->B) {
             k_bending<<<G(h->B), 256, 0, h->s>>>(h->B, h->bend, h->Q, d.bending_k, h->x, h->rest, h->b, h->diag,
-                                                 h->bend_slots, h->sell ? 32u : 1u, h->mat_val);
+                                                 h->bend_slots, h->sell ? 128u : 1u, h->mat_val);
             lcs_count_launch();
         }
         // update_contact_set (newton_solver.cpp:4093-4104)

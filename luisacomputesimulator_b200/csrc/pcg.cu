@@ -421,9 +421,9 @@ struct RowArgs {
     uint32_t n;
     const float4* diag;
     int sell;              // material format: 0 CSR, 1 SELL-32
-    const uint32_t* m_ptr; // CSR row_ptr (n + 1) | SELL slot offset of each slice (n_slices + 1)
-    const uint32_t* m_col; // CSR col | SELL col[(off + k) * 32 + lane]
-    const float* m_val;    // CSR 9 floats per block | SELL val[((off + k) * 9 + c) * 32 + lane]
+    const uint32_t* m_ptr; // CSR row_ptr (n + 1) | SELL slot offset of each slice (n_slices + 1, multiples of 4)
+    const uint32_t* m_col; // CSR col | SELL col[(g * 32 + lane) * 4 + j], slot 4g + j (see row_matvec)
+    const float* m_val;    // CSR 9 floats per block | SELL val[((g * 9 + c) * 32 + lane) * 4 + j]
     Bsr B;                 // contact blocks (CSR)
     const float4* b;
     float4* x;
@@ -524,6 +524,74 @@ __device__ __forceinline__ void acc_block(const float* m, int stride, float4 v, 
     q2 += __fmaf_rn(m[8 * stride], v.z, __fmaf_rn(m[5 * stride], v.y, m[2 * stride] * v.x));
 }
 
+// streamed read-only 16-B load that does not displace L1 lines (matrix values: read once per iteration)
+__device__ __forceinline__ float4 ld_stream4(const float4* p)
+{
+    float4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ float comp(const float4& v, int j) { return j == 0 ? v.x : j == 1 ? v.y : j == 2 ? v.z : v.w; }
+
+// A v for the owned row: diagonal block + material (CSR or SELL) + contact (CSR).
+//
+// SELL material layout ("SELL-32, 4-slot groups"): a slice is 32 consecutive rows, its width (slots)
+// padded to a multiple of 4; group g holds slots 4g..4g+3 of the 32 rows.  Column j of lane l is
+// col[(g * 32 + l) * 4 + j] (one uint4 per lane), component c of slot j is
+// val[((g * 9 + c) * 32 + l) * 4 + j] (one float4 per lane and component).  A warp therefore reads
+// each group with one 512-B coalesced uint4 load and nine 512-B float4 loads, 2.5 load instructions per
+// block instead of 10.  Padding slots hold zero blocks against the row itself.  The blocks are summed in
+// slot order, the order of the CSR row.
+__device__ __forceinline__ void row_matvec(const RowArgs& a, uint32_t i, uint32_t row, bool own, uint32_t slice,
+                                          uint32_t lane, const float4* src, float v0, float v1, float v2, float& q0,
+                                          float& q1, float& q2)
+{
+    const float4 c0 = __ldg(&a.diag[3 * row]), c1 = __ldg(&a.diag[3 * row + 1]), c2 = __ldg(&a.diag[3 * row + 2]);
+    q0 = __fmaf_rn(c2.x, v2, __fmaf_rn(c1.x, v1, c0.x * v0));
+    q1 = __fmaf_rn(c2.y, v2, __fmaf_rn(c1.y, v1, c0.y * v0));
+    q2 = __fmaf_rn(c2.z, v2, __fmaf_rn(c1.z, v1, c0.z * v0));
+    float o0 = 0.f, o1 = 0.f, o2 = 0.f;
+    if (a.sell && slice * 32 < a.n) {  // threads past the last slice have no slot range
+        const uint32_t g0 = __ldg(&a.m_ptr[slice]) >> 2, g1 = __ldg(&a.m_ptr[slice + 1]) >> 2;
+        const uint4* C4 = reinterpret_cast<const uint4*>(a.m_col);
+        const float4* V4 = reinterpret_cast<const float4*>(a.m_val);
+        for (uint32_t g = g0; g < g1; ++g) {
+            const uint4 jc = __ldg(&C4[(size_t)g * 32 + lane]);
+            const float4 pv[4] = {__ldcg(&src[jc.x]), __ldcg(&src[jc.y]), __ldcg(&src[jc.z]), __ldcg(&src[jc.w])};
+            const float4* vg = V4 + (size_t)g * 9 * 32 + lane;
+            // one output component at a time (block row r uses components r, r + 3, r + 6): three
+            // value vectors live at once instead of nine
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const float4 ma = ld_stream4(vg + 32 * r), mb = ld_stream4(vg + 32 * (r + 3)),
+                             mc = ld_stream4(vg + 32 * (r + 6));
+                float o = r == 0 ? o0 : r == 1 ? o1 : o2;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    o += __fmaf_rn(comp(mc, j), pv[j].z, __fmaf_rn(comp(mb, j), pv[j].y, comp(ma, j) * pv[j].x));
+                if (r == 0) o0 = o;
+                else if (r == 1) o1 = o;
+                else o2 = o;
+            }
+        }
+    } else if (a.m_ptr && own) {
+        const uint32_t end = __ldg(&a.m_ptr[i + 1]);
+        for (uint32_t k = __ldg(&a.m_ptr[i]); k < end; ++k)
+            acc_block(a.m_val + 9 * (size_t)k, 1, __ldcg(&src[__ldg(&a.m_col[k])]), o0, o1, o2);
+    }
+    if (a.B.rp && own) {
+        const uint32_t end = __ldcg(&a.B.rp[i + 1]);
+        for (uint32_t k = __ldcg(&a.B.rp[i]); k < end; ++k)
+            acc_block(a.B.val + 9 * (size_t)k, 1, __ldcg(&src[__ldcg(&a.B.col[k])]), o0, o1, o2);
+    }
+    q0 += o0;
+    q1 += o1;
+    q2 += o2;
+}
+
 template <int BS>
 __global__ void __launch_bounds__(BS) k_pcg_rows(RowArgs a)
 {
@@ -583,32 +651,7 @@ __global__ void __launch_bounds__(BS) k_pcg_rows(RowArgs a)
         if (!row_barrier(a, &s_fail)) return;
         // q = A p
         float q0, q1, q2;
-        {
-            const float4 c0 = __ldg(&a.diag[3 * row]), c1 = __ldg(&a.diag[3 * row + 1]), c2 = __ldg(&a.diag[3 * row + 2]);
-            q0 = __fmaf_rn(c2.x, p2, __fmaf_rn(c1.x, p1, c0.x * p0));
-            q1 = __fmaf_rn(c2.y, p2, __fmaf_rn(c1.y, p1, c0.y * p0));
-            q2 = __fmaf_rn(c2.z, p2, __fmaf_rn(c1.z, p1, c0.z * p0));
-        }
-        float o0 = 0.f, o1 = 0.f, o2 = 0.f;
-        if (a.sell && slice * 32 < a.n) {  // threads past the last slice have no slot range
-            const uint32_t off = __ldg(&a.m_ptr[slice]), end = __ldg(&a.m_ptr[slice + 1]);
-            for (uint32_t k = off; k < end; ++k) {
-                const uint32_t cj = __ldg(&a.m_col[32 * k + lane]);
-                acc_block(a.m_val + (size_t)9 * 32 * k + lane, 32, __ldcg(&a.pg[cj]), o0, o1, o2);
-            }
-        } else if (a.m_ptr && own) {
-            const uint32_t end = __ldg(&a.m_ptr[i + 1]);
-            for (uint32_t k = __ldg(&a.m_ptr[i]); k < end; ++k)
-                acc_block(a.m_val + 9 * (size_t)k, 1, __ldcg(&a.pg[__ldg(&a.m_col[k])]), o0, o1, o2);
-        }
-        if (a.B.rp && own) {
-            const uint32_t end = __ldcg(&a.B.rp[i + 1]);
-            for (uint32_t k = __ldcg(&a.B.rp[i]); k < end; ++k)
-                acc_block(a.B.val + 9 * (size_t)k, 1, __ldcg(&a.pg[__ldcg(&a.B.col[k])]), o0, o1, o2);
-        }
-        q0 += o0;
-        q1 += o1;
-        q2 += o2;
+        row_matvec(a, i, row, own, slice, lane, a.pg, p0, p1, p2, q0, q1, q2);
         double dpq;
         if (!own) dpq = 0.0;
         else if (a.fp64) dpq = (double)p0 * q0 + (double)p1 * q1 + (double)p2 * q2;
@@ -659,19 +702,21 @@ __device__ __forceinline__ void red_add_release(unsigned* p, unsigned v)
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// grid barrier with release/acquire ordering (the block's writes, ordered by __syncthreads,
-// are released by thread 0's arrival); bounded spin -> LCS_ERR_TIMEOUT
-__device__ __forceinline__ bool pipe_barrier(unsigned* count, unsigned* gen, lcs_pcg_stats* stats, volatile int* s_fail)
+// grid barrier with release/acquire ordering (the block's writes, ordered by __syncthreads, are
+// released by thread 0's arrival).  Thread 0 of each block tracks the barrier generation in `gen_seen`
+// (read once at kernel start: no block can pass the first barrier before every block has arrived, so
+// all read the same value), which saves a round trip per barrier.  Bounded spin -> LCS_ERR_TIMEOUT.
+__device__ __forceinline__ bool pipe_barrier(unsigned* count, unsigned* gen, unsigned& gen_seen, lcs_pcg_stats* stats,
+                                             volatile int* s_fail)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned g = ld_acquire(gen);
         if (atom_add_acq_rel(count, 1u) == gridDim.x - 1) {
-            *count = 0u;  // ordered before the release below; no block reads it until the next arrival
+            *count = 0u;  // ordered before the release below; no block arrives again before it
             red_add_release(gen, 1u);
         } else {
             unsigned it = 0;
-            while (ld_acquire(gen) == g) {
+            while (ld_acquire(gen) == gen_seen) {
                 if (++it > kBarrierSpinLimit) {
                     *s_fail = 1;
                     stats->status = LCS_ERR_TIMEOUT;
@@ -679,6 +724,7 @@ __device__ __forceinline__ bool pipe_barrier(unsigned* count, unsigned* gen, lcs
                 }
             }
         }
+        ++gen_seen;
     }
     __syncthreads();
     return *s_fail == 0;
@@ -714,6 +760,26 @@ __device__ __forceinline__ void block_partial3(double v0, double v1, double v2, 
     }
 }
 
+// Partial sums copied to shared memory by cp.async (no registers held while the SpMV runs): block b's
+// four doubles land in dst[b]; grid_collect3 waits for the copies and reduces them in a fixed order.
+constexpr int kPipeMaxBlocks = 448;  // 3 blocks on each of 148 SMs, rounded up
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+template <int BS>
+__device__ __forceinline__ void grid_prefetch3(const double* part, double (*dst)[4])
+{
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += BS) {
+        cp_async16(&dst[b][0], part + 4 * b);
+        cp_async16(&dst[b][2], part + 4 * b + 2);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
 // Grid-wide sums of the per-block partials, split in two so that the loads overlap other work:
 // grid_fetch3 issues this thread's share of the loads (blocks t, t + BS, ... in that order),
 // grid_reduce3 combines them in a fixed order (warp shuffles, then warps in index order).  Every
@@ -733,6 +799,23 @@ __device__ __forceinline__ Fetch3 grid_fetch3(const double* part)
         f.v2 += __ldcg(&part[4 * b + 2]);
     }
     return f;
+}
+
+template <int BS>
+__device__ __forceinline__ void grid_reduce3(Fetch3 f, double& o0, double& o1, double& o2);
+
+template <int BS>
+__device__ __forceinline__ void grid_collect3(double (*src)[4], double& o0, double& o1, double& o2)
+{
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    Fetch3 f{0.0, 0.0, 0.0};
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += BS) {
+        f.v0 += src[b][0];
+        f.v1 += src[b][1];
+        f.v2 += src[b][2];
+    }
+    grid_reduce3<BS>(f, o0, o1, o2);
 }
 
 template <int BS>
@@ -765,83 +848,24 @@ __device__ __forceinline__ void grid_reduce3(Fetch3 f, double& o0, double& o1, d
     __syncthreads();
 }
 
-// streamed read-only load that does not displace L1 lines (matrix values: read once per iteration)
-__device__ __forceinline__ float ld_stream(const float* p)
-{
-    float v;
-    asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
-    return v;
-}
-
-__device__ __forceinline__ void acc_block_s(const float* m, float4 v, float& q0, float& q1, float& q2)
-{
-    // SELL-32 slot: component c of the slot at m[c * 32]
-    q0 += __fmaf_rn(ld_stream(m + 6 * 32), v.z, __fmaf_rn(ld_stream(m + 3 * 32), v.y, ld_stream(m) * v.x));
-    q1 += __fmaf_rn(ld_stream(m + 7 * 32), v.z, __fmaf_rn(ld_stream(m + 4 * 32), v.y, ld_stream(m + 32) * v.x));
-    q2 += __fmaf_rn(ld_stream(m + 8 * 32), v.z, __fmaf_rn(ld_stream(m + 5 * 32), v.y, ld_stream(m + 2 * 32) * v.x));
-}
-
-// A v for the owned row: diagonal block + material (CSR or SELL-32) + contact (CSR).  The SELL
-// and contact loops issue the column loads and the gathers of several blocks before using them
-// (the gathers depend on the columns, the products on the gathers: unrolled, a row pays two
-// memory latencies per four blocks instead of two per block); the sum order is unchanged.
-__device__ __forceinline__ void row_matvec(const RowArgs& a, uint32_t i, uint32_t row, bool own, uint32_t slice,
-                                          uint32_t lane, const float4* src, float v0, float v1, float v2, float& q0,
-                                          float& q1, float& q2)
-{
-    const float4 c0 = __ldg(&a.diag[3 * row]), c1 = __ldg(&a.diag[3 * row + 1]), c2 = __ldg(&a.diag[3 * row + 2]);
-    q0 = __fmaf_rn(c2.x, v2, __fmaf_rn(c1.x, v1, c0.x * v0));
-    q1 = __fmaf_rn(c2.y, v2, __fmaf_rn(c1.y, v1, c0.y * v0));
-    q2 = __fmaf_rn(c2.z, v2, __fmaf_rn(c1.z, v1, c0.z * v0));
-    float o0 = 0.f, o1 = 0.f, o2 = 0.f;
-    if (a.sell && slice * 32 < a.n) {  // threads past the last slice have no slot range
-        const uint32_t off = __ldg(&a.m_ptr[slice]), end = __ldg(&a.m_ptr[slice + 1]);
-        uint32_t k = off;
-        for (; k + 4 <= end; k += 4) {
-            const uint32_t j0 = __ldg(&a.m_col[32 * k + lane]), j1 = __ldg(&a.m_col[32 * (k + 1) + lane]);
-            const uint32_t j2 = __ldg(&a.m_col[32 * (k + 2) + lane]), j3 = __ldg(&a.m_col[32 * (k + 3) + lane]);
-            const float4 p0 = __ldcg(&src[j0]), p1 = __ldcg(&src[j1]), p2 = __ldcg(&src[j2]), p3 = __ldcg(&src[j3]);
-            const float* m = a.m_val + (size_t)9 * 32 * k + lane;
-            acc_block_s(m, p0, o0, o1, o2);
-            acc_block_s(m + 9 * 32, p1, o0, o1, o2);
-            acc_block_s(m + 18 * 32, p2, o0, o1, o2);
-            acc_block_s(m + 27 * 32, p3, o0, o1, o2);
-        }
-        for (; k < end; ++k) {
-            const uint32_t cj = __ldg(&a.m_col[32 * k + lane]);
-            acc_block_s(a.m_val + (size_t)9 * 32 * k + lane, __ldcg(&src[cj]), o0, o1, o2);
-        }
-    } else if (a.m_ptr && own) {
-        const uint32_t end = __ldg(&a.m_ptr[i + 1]);
-        for (uint32_t k = __ldg(&a.m_ptr[i]); k < end; ++k)
-            acc_block(a.m_val + 9 * (size_t)k, 1, __ldcg(&src[__ldg(&a.m_col[k])]), o0, o1, o2);
-    }
-    if (a.B.rp && own) {
-        const uint32_t end = __ldcg(&a.B.rp[i + 1]);
-        uint32_t k = __ldcg(&a.B.rp[i]);
-        for (; k + 2 <= end; k += 2) {
-            const uint32_t j0 = __ldcg(&a.B.col[k]), j1 = __ldcg(&a.B.col[k + 1]);
-            const float4 p0 = __ldcg(&src[j0]), p1 = __ldcg(&src[j1]);
-            acc_block(a.B.val + 9 * (size_t)k, 1, p0, o0, o1, o2);
-            acc_block(a.B.val + 9 * (size_t)(k + 1), 1, p1, o0, o1, o2);
-        }
-        if (k < end) acc_block(a.B.val + 9 * (size_t)k, 1, __ldcg(&src[__ldcg(&a.B.col[k])]), o0, o1, o2);
-    }
-    q0 += o0;
-    q1 += o1;
-    q2 += o2;
-}
-
 template <int BS>
 __global__ void __launch_bounds__(BS, 3) k_pcg_pipe(RowArgs a, float4* pg2)
 {
     __shared__ int s_fail;
+    // x, p, s, q, z of this block's rows: each read and written once per iteration, so they live in
+    // shared memory (private slot per thread, no synchronisation) and leave registers to the SpMV
+    __shared__ float4 sv[5][BS];
+    __shared__ float4 sminv[3][BS];  // inverse diagonal block, column-major (read once per iteration)
+    __shared__ __align__(16) double spart[kPipeMaxBlocks][4];  // every block's partial sums
     if (threadIdx.x == 0) s_fail = 0;
-    const uint32_t i = blockIdx.x * BS + threadIdx.x;
+    unsigned gen_seen = threadIdx.x == 0 ? ld_acquire(a.bar_gen) : 0u;
+    const uint32_t t = threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) sv[k][t] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t i = blockIdx.x * BS + t;
     const bool own = i < a.n;
     const uint32_t row = own ? i : a.n - 1;
-    const uint32_t lane = threadIdx.x & 31u, slice = i >> 5;
-    float m0, m1, m2, m3, m4, m5, m6, m7, m8;  // inverse diagonal block, column-major
+    const uint32_t lane = t & 31u, slice = i >> 5;
     float r0 = 0.f, r1 = 0.f, r2 = 0.f;
     {
         const float4 bv = a.b[row];
@@ -850,23 +874,23 @@ __global__ void __launch_bounds__(BS, 3) k_pcg_pipe(RowArgs a, float4* pg2)
         const float aa = c0.x, bb = c1.x, c = c2.x, d = c0.y, e = c1.y, f = c2.y, g = c0.z, h = c1.z, k = c2.z;
         const float A = e * k - f * h, B = f * g - d * k, C = d * h - e * g;
         const float id = 1.0f / (aa * A + bb * B + c * C);
-        m0 = A * id; m1 = B * id; m2 = C * id;
-        m3 = (c * h - bb * k) * id; m4 = (aa * k - c * g) * id; m5 = (bb * g - aa * h) * id;
-        m6 = (bb * f - c * e) * id; m7 = (c * d - aa * f) * id; m8 = (aa * e - bb * d) * id;
+        sminv[0][t] = make_float4(A * id, B * id, C * id, 0.f);
+        sminv[1][t] = make_float4((c * h - bb * k) * id, (aa * k - c * g) * id, (bb * g - aa * h) * id, 0.f);
+        sminv[2][t] = make_float4((bb * f - c * e) * id, (c * d - aa * f) * id, (aa * e - bb * d) * id, 0.f);
     }
-#define LCS_MINV(v0, v1, v2, o0, o1, o2)                        \
-    o0 = __fmaf_rn(m6, v2, __fmaf_rn(m3, v1, m0 * v0));          \
-    o1 = __fmaf_rn(m7, v2, __fmaf_rn(m4, v1, m1 * v0));          \
-    o2 = __fmaf_rn(m8, v2, __fmaf_rn(m5, v1, m2 * v0));
-    float x0 = 0.f, x1 = 0.f, x2 = 0.f;
+#define LCS_MINV(v0, v1, v2, o0, o1, o2)                                                 \
+    {                                                                                     \
+        const float4 mc0 = sminv[0][t], mc1 = sminv[1][t], mc2 = sminv[2][t];             \
+        o0 = __fmaf_rn(mc2.x, v2, __fmaf_rn(mc1.x, v1, mc0.x * v0));                      \
+        o1 = __fmaf_rn(mc2.y, v2, __fmaf_rn(mc1.y, v1, mc0.y * v0));                      \
+        o2 = __fmaf_rn(mc2.z, v2, __fmaf_rn(mc1.z, v1, mc0.z * v0));                      \
+    }
     float u0, u1, u2, w0, w1, w2;
     LCS_MINV(r0, r1, r2, u0, u1, u2)
     // w = A u (one extra synchronisation before the loop)
     if (own) __stcg(&pg2[i], make_float4(u0, u1, u2, 0.0f));
-    if (!pipe_barrier(a.bar_count, a.bar_gen, a.stats, &s_fail)) return;
+    if (!pipe_barrier(a.bar_count, a.bar_gen, gen_seen, a.stats, &s_fail)) return;
     row_matvec(a, i, row, own, slice, lane, pg2, u0, u1, u2, w0, w1, w2);
-    float p0 = 0.f, p1 = 0.f, p2 = 0.f, s0 = 0.f, s1 = 0.f, s2 = 0.f;
-    float q0 = 0.f, q1 = 0.f, q2 = 0.f, z0 = 0.f, z1 = 0.f, z2 = 0.f;
     float gamma_old = 0.0f, alpha_old = 0.0f, norm_r0 = 0.0f, norm_r = 0.0f, gamma = 0.0f;
     int iter = 0, status = 0;
     for (iter = 0; iter < a.max_iter; ++iter) {
@@ -887,14 +911,14 @@ __global__ void __launch_bounds__(BS, 3) k_pcg_pipe(RowArgs a, float4* pg2)
         LCS_MINV(w0, w1, w2, mm0, mm1, mm2)
         float4* mbuf = (iter & 1) ? pg2 : a.pg;
         if (own) __stcg(&mbuf[i], make_float4(mm0, mm1, mm2, 0.0f));
-        if (!pipe_barrier(a.bar_count, a.bar_gen, a.stats, &s_fail)) return;
+        if (!pipe_barrier(a.bar_count, a.bar_gen, gen_seen, a.stats, &s_fail)) return;
         // the partial-sum loads are in flight while this row computes n = A m (which needs no
         // scalar of this iteration)
-        const Fetch3 f = grid_fetch3<BS>(part);
+        grid_prefetch3<BS>(part, spart);
         float n0, n1, n2;
         row_matvec(a, i, row, own, slice, lane, mbuf, mm0, mm1, mm2, n0, n1, n2);
         double sg, sd, sr;
-        grid_reduce3<BS>(f, sg, sd, sr);
+        grid_collect3<BS>(spart, sg, sd, sr);
         gamma = (float)sg;
         const float delta = (float)sd;
         norm_r = sqrtf((float)sr);
@@ -920,19 +944,21 @@ __global__ void __launch_bounds__(BS, 3) k_pcg_pipe(RowArgs a, float4* pg2)
             beta = 0.0f;
             alpha = safe_div(gamma, delta);
         }
-        z0 = n0 + beta * z0; z1 = n1 + beta * z1; z2 = n2 + beta * z2;
-        q0 = mm0 + beta * q0; q1 = mm1 + beta * q1; q2 = mm2 + beta * q2;
-        s0 = w0 + beta * s0; s1 = w1 + beta * s1; s2 = w2 + beta * s2;
-        p0 = u0 + beta * p0; p1 = u1 + beta * p1; p2 = u2 + beta * p2;
-        x0 += alpha * p0; x1 += alpha * p1; x2 += alpha * p2;
-        r0 -= alpha * s0; r1 -= alpha * s1; r2 -= alpha * s2;
-        u0 -= alpha * q0; u1 -= alpha * q1; u2 -= alpha * q2;
-        w0 -= alpha * z0; w1 -= alpha * z1; w2 -= alpha * z2;
+        float4 z = sv[4][t], q = sv[3][t], sd4 = sv[2][t], p = sv[1][t], x = sv[0][t];
+        z = make_float4(n0 + beta * z.x, n1 + beta * z.y, n2 + beta * z.z, 0.f);
+        q = make_float4(mm0 + beta * q.x, mm1 + beta * q.y, mm2 + beta * q.z, 0.f);
+        sd4 = make_float4(w0 + beta * sd4.x, w1 + beta * sd4.y, w2 + beta * sd4.z, 0.f);
+        p = make_float4(u0 + beta * p.x, u1 + beta * p.y, u2 + beta * p.z, 0.f);
+        x = make_float4(x.x + alpha * p.x, x.y + alpha * p.y, x.z + alpha * p.z, 0.f);
+        sv[4][t] = z; sv[3][t] = q; sv[2][t] = sd4; sv[1][t] = p; sv[0][t] = x;
+        r0 -= alpha * sd4.x; r1 -= alpha * sd4.y; r2 -= alpha * sd4.z;
+        u0 -= alpha * q.x; u1 -= alpha * q.y; u2 -= alpha * q.z;
+        w0 -= alpha * z.x; w1 -= alpha * z.y; w2 -= alpha * z.z;
         gamma_old = gamma;
         alpha_old = alpha;
     }
 #undef LCS_MINV
-    if (own) a.x[i] = make_float4(x0, x1, x2, 0.0f);
+    if (own) a.x[i] = sv[0][t];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.stats->iterations = iter;
         a.stats->rel_residual = norm_r0 > 0.0f ? norm_r / norm_r0 : 0.0f;
@@ -1085,6 +1111,7 @@ static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* 
     if (P->rows_capacity < 0) P->rows_capacity = (int)lcs_pcg_rows_capacity();
     if ((int64_t)P->n > P->rows_capacity) return LCS_ERR_CAPACITY;
     const bool pipe = (o.flags & LCS_PCG_PIPELINED) != 0;
+    if (pipe && (P->n + kRowThreads - 1) / kRowThreads > (uint32_t)kPipeMaxBlocks) return LCS_ERR_CAPACITY;
     RowArgs a;
     a.n = P->n;
     a.diag = diag;
