@@ -284,6 +284,13 @@ __device__ __forceinline__ void store_slot(float4* wide, uint32_t s, v3 mn, v3 m
     __stcg(r + 1, make_float4(mx.x, mx.y, mx.z, 0.0f));
 }
 
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v)
+{
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // fn_update_*_tree_leave_aabb_v2 (lbvh.cpp:617-683) and, when `climb`, fn_refit_tree_aabb
 // (lbvh.cpp:702-754): the second child to arrive at a parent unions the two slot boxes and
 // carries on upwards; arrival counters reset themselves, so no init pass is needed.
@@ -313,10 +320,10 @@ __global__ void k_leaves_refit(int kind, uint32_t n, const uint32_t* __restrict_
                 *healthy = 0u;
                 break;
             }
-            __threadfence();
-            if (atomicAdd(&counters[p], 1u) == 0u) break;  // first arrival: the sibling finishes
-            counters[p] = 0u;
-            __threadfence();
+            // acq_rel arrival: releases this child's box to the sibling and, for the second
+            // arrival, acquires the sibling's box (no full fences)
+            if (atom_add_acq_rel_gpu(&counters[p], 1u) == 0u) break;  // first arrival: the sibling finishes
+            counters[p] = 0u;  // re-armed for the next refit (launch boundary orders it)
             const float4* r = wide + 4 * p;
             float4 a0 = __ldcg(r + 0), a1 = __ldcg(r + 1), b0 = __ldcg(r + 2), b1 = __ldcg(r + 3);
             v3 mn = mk3(fmn(a0.x, b0.x), fmn(a0.y, b0.y), fmn(a0.z, b0.z));

@@ -342,6 +342,9 @@ struct lcs_newton {
     uint32_t V = 0, F = 0, E = 0, B = 0;
     cudaStream_t s = nullptr;
     bool own_stream = false;
+    // fused mode: the edge-tree lane of the broad phase runs on s2, forked from and joined back to s
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     // mesh
     uint4* faces = nullptr;
     uint2* edges = nullptr;
@@ -521,6 +524,25 @@ int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint32_t* cnt
     const float* X0 = reinterpret_cast<const float*>(x0);
     const float* X1 = reinterpret_cast<const float*>(x1);
     int rc;
+    if (!h->plain && h->s2) {
+        // two independent lanes: face tree + VF queries here, edge tree + EE queries on s2; both are
+        // latency-bound tree walks that leave most of the GPU idle when run one after the other
+        LCS_CUDA_TRY(cudaEventRecord(h->fork, h->s));
+        LCS_CUDA_TRY(cudaStreamWaitEvent(h->s2, h->fork, 0));
+        if ((rc = lcs_bvh_update_refit(h->edge_tree, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->edges), h->s2)))
+            return rc;
+        if ((rc = lcs_bvh_query_ee(h->edge_tree, X0, X1, reinterpret_cast<const uint32_t*>(h->edges), h->E, h->dhat,
+                                   h->offset, reinterpret_cast<uint32_t*>(h->bp_ee), h->cap_ee, cnt_ee, h->s2)))
+            return rc;
+        if ((rc = lcs_bvh_update_refit(h->face_tree, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->faces), h->s)))
+            return rc;
+        if ((rc = lcs_bvh_query_vf(h->face_tree, X0, X1, h->V, h->dhat, h->offset, reinterpret_cast<uint32_t*>(h->bp_vf),
+                                   h->cap_vf, cnt_vf, h->s)))
+            return rc;
+        LCS_CUDA_TRY(cudaEventRecord(h->join, h->s2));
+        LCS_CUDA_TRY(cudaStreamWaitEvent(h->s, h->join, 0));
+        return LCS_OK;
+    }
     if (h->plain) {
         if ((rc = lcs_bvh_update_leaves(h->face_tree, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->faces), h->s))) return rc;
         if ((rc = lcs_bvh_refit(h->face_tree, h->s))) return rc;
@@ -652,13 +674,23 @@ int newton_iteration(lcs_newton* h)
             k_floor_ccd<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->x, h->offset, h->pinned, d.floor_y, h->st);
             lcs_count_launch();
         }
-            lcs_count_launch();
+        // fused mode: the EE step bound runs beside the VF one (both only lower the same minimum)
+        const bool lanes = !h->plain && h->s2;
+        cudaStream_t s_ee = lanes ? h->s2 : h->s;
+        if (lanes) {
+            LCS_CUDA_TRY(cudaEventRecord(h->fork, h->s));
+            LCS_CUDA_TRY(cudaStreamWaitEvent(h->s2, h->fork, 0));
+        }
+        if ((rc = lcs_ccd_ee(reinterpret_cast<uint32_t*>(h->bp_ee), &h->st->cnt[4], h->cap_ee, XI, X, reinterpret_cast<const uint32_t*>(h->edges), h->body, h->offset,
+                             &h->st->toi, nullptr, ccd_flags, s_ee)))
+            return rc;
         if ((rc = lcs_ccd_vf(reinterpret_cast<uint32_t*>(h->bp_vf), &h->st->cnt[3], h->cap_vf, XI, X, reinterpret_cast<const uint32_t*>(h->faces), h->body, h->offset,
                              &h->st->toi, nullptr, ccd_flags, h->s)))
             return rc;
-        if ((rc = lcs_ccd_ee(reinterpret_cast<uint32_t*>(h->bp_ee), &h->st->cnt[4], h->cap_ee, XI, X, reinterpret_cast<const uint32_t*>(h->edges), h->body, h->offset,
-                             &h->st->toi, nullptr, ccd_flags, h->s)))
-            return rc;
+        if (lanes) {
+            LCS_CUDA_TRY(cudaEventRecord(h->join, h->s2));
+            LCS_CUDA_TRY(cudaStreamWaitEvent(h->s, h->join, 0));
+        }
         if (h->plain)
             if ((rc = host_readback(h))) return rc;  // ccd_get_toi
         mark(h, kPhApply);
@@ -782,6 +814,12 @@ extern "C" int lcs_newton_create(const lcs_scene_desc* d, int flags, lcs_stream 
     }
     if (h->profile)
         for (auto& ev : h->ev) cudaEventCreate(&ev);
+    if (!h->plain && (cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking) != cudaSuccess ||
+                      cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming) != cudaSuccess ||
+                      cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming) != cudaSuccess)) {
+        lcs_newton_destroy(h);
+        return lcs_fail(LCS_ERR_CUDA, "lcs_newton_create: stream/event creation failed");
+    }
     *out = h;
     return LCS_OK;
 }
@@ -806,6 +844,12 @@ extern "C" int lcs_newton_destroy(lcs_newton* h)
     if (h->h_x_iter) cudaFreeHost(h->h_x_iter);
     for (auto& ev : h->ev)
         if (ev) cudaEventDestroy(ev);
+    if (h->s2) {
+        cudaStreamSynchronize(h->s2);
+        cudaStreamDestroy(h->s2);
+    }
+    if (h->fork) cudaEventDestroy(h->fork);
+    if (h->join) cudaEventDestroy(h->join);
     if (h->own_stream) cudaStreamDestroy(h->s);
     delete h;
     return LCS_OK;
