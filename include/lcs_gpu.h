@@ -144,6 +144,41 @@ LCS_API int lcs_bvh_export(const lcs_bvh* h, uint32_t* parent, uint32_t* childre
 LCS_API uint32_t lcs_bvh_num_leaves(const lcs_bvh* h);
 
 /* ------------------------------------------------------------------------------------------
+ * Forest of per-scene LBVHs (batched solver; no counterpart in the reference, which holds one
+ * LBVH per tree kind).  Scenes are concatenated: element e of scene s is global element
+ * elem_offsets[s] + e and refers to global vertex ids.  Each scene's tree is bit-identical to
+ * the lcs_bvh tree of that scene alone (same global-AABB cover rule, Morton codes, sort order,
+ * Karras topology over local element ids, refit boxes and query results).  Every scene needs at
+ * least two elements.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct lcs_forest lcs_forest;
+/* elem_offsets / vert_offsets: host arrays of n_scenes + 1 prefix offsets (elem_offsets[0] = 0);
+ * kind LCS_TREE_EDGE or LCS_TREE_FACE. */
+LCS_API int lcs_forest_create(int kind, uint32_t n_scenes, const uint32_t* elem_offsets,
+                              const uint32_t* vert_offsets, lcs_forest** out);
+LCS_API int lcs_forest_destroy(lcs_forest* f);
+/* reduce_*_tree_aabb + construct_tree for every scene in one set of launches */
+LCS_API int lcs_forest_build(lcs_forest* f, const float* x, const uint32_t* elems, lcs_stream stream);
+/* update_*_tree_leave_aabb + refit for every scene */
+LCS_API int lcs_forest_update_refit(lcs_forest* f, const float* thickness, const float* x0, const float* x1,
+                                    const uint32_t* elems, lcs_stream stream);
+/* broad_phase_query_from_verts for all scenes: vertex v queries the tree of vert_scene[v] */
+LCS_API int lcs_forest_query_vf(const lcs_forest* face_forest, const float* x0, const float* x1,
+                                uint32_t n_verts, const uint32_t* vert_scene, const float* d_hat,
+                                const float* thickness, uint32_t* pairs, uint32_t capacity,
+                                uint32_t* d_count, lcs_stream stream);
+/* broad_phase_query_from_edges for all scenes (the forest's own edges are the queries) */
+LCS_API int lcs_forest_query_ee(const lcs_forest* edge_forest, const float* x0, const float* x1,
+                                const uint32_t* edges, const float* d_hat, const float* thickness,
+                                uint32_t* pairs, uint32_t capacity, uint32_t* d_count, lcs_stream stream);
+LCS_API int lcs_forest_health(lcs_forest* f, int* healthy, lcs_stream stream);
+/* one scene's tree in the layout of lcs_bvh_export (local node and element ids) */
+LCS_API int lcs_forest_export_scene(const lcs_forest* f, uint32_t scene, uint32_t* parent, uint32_t* children,
+                                    uint32_t* object_idx, uint64_t* morton_sorted,
+                                    uint32_t* sorted_get_original, float* node_aabb, float* global_aabb6,
+                                    lcs_stream stream);
+
+/* ------------------------------------------------------------------------------------------
  * Narrow phase  (replaces NarrowPhasesDetector, Solver/CollisionDetector/narrow_phase.h:54-201)
  * Pair lists are the broad phase's uint2 lists; *d_count (device) holds how many are valid and
  * at most `capacity` of them are read.
@@ -160,6 +195,13 @@ LCS_API int lcs_ccd_vf(const uint32_t* pairs, const uint32_t* d_count, uint32_t 
 LCS_API int lcs_ccd_ee(const uint32_t* pairs, const uint32_t* d_count, uint32_t capacity, const float* x0,
                const float* x1, const uint32_t* edges, const uint32_t* body, const float* offset,
                float* d_toi, float* toi_per_pair, int flags, lcs_stream stream);
+/* Batched scenes (no counterpart in the reference): the VF (is_ee = 0, elems = faces) or EE
+ * (is_ee = 1, elems = edges) step bound of every candidate, lowered into the bound of the pair's
+ * own scene, d_toi_per_scene[vert_scene[first vertex]] (each initialised to 1 by the caller). */
+LCS_API int lcs_ccd_batch(int is_ee, const uint32_t* pairs, const uint32_t* d_count, uint32_t capacity,
+                          const float* x0, const float* x1, const uint32_t* elems, const uint32_t* body,
+                          const float* offset, const uint32_t* vert_scene, float* d_toi_per_scene,
+                          float* toi_per_pair, int flags, lcs_stream stream);
 
 /* NarrowPhasesDetector::vf_dcd_query_repulsion (narrow_phase.cpp:771-933, 1102-1170): barrier
  * contact pairs with d^2 < (offset + d_hat)^2; appended to out, count added to *d_out_count. */
@@ -264,6 +306,20 @@ LCS_API int lcs_pcg_solve_noalloc(uint32_t n, const float* diag, const lcs_bsr* 
                                   const float* b, float* x, const lcs_pcg_opts* opts, lcs_pcg_stats* stats,
                                   lcs_stream stream);
 
+/* Batched scenes (no counterpart in the reference): n_scenes independent systems, scene s owning
+ * block rows [row_offsets[s], row_offsets[s+1]) of one BSR pair (device array of n_scenes + 1;
+ * *host_row_end = row_offsets[n_scenes], read on the host), solved in one launch with one
+ * thread-block cluster of `cluster` CTAs (1, 2, 4, 8 or 16) per scene.  Each scene has its own
+ * alpha, beta and stop decision (the rules of lcs_pcg_solve); its result does not depend on
+ * `cluster` or on the other scenes.  active: device flags per scene (0: skip, x = 0) or NULL.
+ * stats_per_scene: device array of n_scenes.  Asynchronous; the handle must hold at least
+ * *host_row_end rows. */
+LCS_API int lcs_pcg_solve_batch(lcs_pcg* p, uint32_t n_scenes, const uint32_t* row_offsets,
+                                const uint32_t* host_row_end, const uint32_t* active, const float* diag,
+                                const lcs_bsr* A, const lcs_bsr* B, const float* b, float* x,
+                                const lcs_pcg_opts* opts, lcs_pcg_stats* stats_per_scene, int cluster,
+                                lcs_stream stream);
+
 /* ------------------------------------------------------------------------------------------
  * Newton loop  (replaces NewtonSolver::physics_step_GPU and its contact glue,
  * Solver/SimulationSolver/newton_solver.cpp:3174-3375, 3685-3884, 4051-4345)
@@ -327,6 +383,21 @@ typedef struct lcs_newton lcs_newton;
  * block pattern, allocates the contact buffers (CollisionData sizing, collision_data.h:445-485).
  * stream: the stream all work of this solver goes to (NULL: the solver creates one). */
 LCS_API int lcs_newton_create(const lcs_scene_desc* desc, int flags, lcs_stream stream, lcs_newton** out);
+/* Batched scenes (no counterpart in the reference): n_scenes independent scenes stepped
+ * together, one set of launches per Newton phase for all of them (forests of per-scene LBVHs,
+ * per-scene step bounds, per-scene PCG on thread-block clusters of pcg_cluster CTAs: 1, 2, 4, 8
+ * or 16).  Every scene runs its own Newton loop (its own small-step and Dirichlet tests); a scene
+ * that has finished is switched off for the rest of the step.  The scenes must share dt,
+ * gravity, stiffnesses and solver settings and run with the floor off; LCS_NEWTON_PLAIN is
+ * rejected.  A scene's trajectory does not depend on the other scenes of the batch (up to the
+ * summation order of atomic accumulations). */
+LCS_API int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_scenes, int flags, lcs_stream stream,
+                                    int pcg_cluster, lcs_newton** out);
+LCS_API uint32_t lcs_newton_num_scenes(const lcs_newton* h);
+/* per-scene figures of the last step: newton_iters, pcg_iters, last_toi, last_rel_residual */
+LCS_API int lcs_newton_scene_stats(const lcs_newton* h, uint32_t scene, lcs_newton_stats* stats);
+/* one scene's x, v (float4 per vertex) to host memory; synchronises the solver's stream */
+LCS_API int lcs_newton_download_scene(const lcs_newton* h, uint32_t scene, float* x_out, float* v_out);
 LCS_API int lcs_newton_destroy(lcs_newton* h);
 /* NewtonSolver::physics_step_GPU (newton_solver.cpp:4051-4345) on the device-resident state. */
 LCS_API int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats);

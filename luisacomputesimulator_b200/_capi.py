@@ -99,6 +99,21 @@ SIGNATURES = {
     "lcs_pcg_solve_noalloc": (I32, [U32, P, C.POINTER(Bsr), C.POINTER(Bsr), P, P, C.POINTER(PcgOpts),
                                     C.POINTER(PcgStats), P]),
     "lcs_newton_create": (I32, [C.POINTER(SceneDesc), I32, P, C.POINTER(P)]),
+    "lcs_newton_create_batch": (I32, [C.POINTER(SceneDesc), U32, I32, P, I32, C.POINTER(P)]),
+    "lcs_newton_num_scenes": (U32, [P]),
+    "lcs_newton_scene_stats": (I32, [P, U32, C.POINTER(NewtonStats)]),
+    "lcs_newton_download_scene": (I32, [P, U32, P, P]),
+    "lcs_forest_create": (I32, [I32, U32, P, P, C.POINTER(P)]),
+    "lcs_forest_destroy": (I32, [P]),
+    "lcs_forest_build": (I32, [P, P, P, P]),
+    "lcs_forest_update_refit": (I32, [P, P, P, P, P, P]),
+    "lcs_forest_query_vf": (I32, [P, P, P, U32, P, P, P, P, U32, P, P]),
+    "lcs_forest_query_ee": (I32, [P, P, P, P, P, P, P, U32, P, P]),
+    "lcs_forest_health": (I32, [P, C.POINTER(C.c_int), P]),
+    "lcs_forest_export_scene": (I32, [P, U32, P, P, P, P, P, P, P, P]),
+    "lcs_ccd_batch": (I32, [I32, P, P, U32, P, P, P, P, P, P, P, P, I32, P]),
+    "lcs_pcg_solve_batch": (I32, [P, U32, P, C.POINTER(C.c_uint32), P, P, C.POINTER(Bsr), C.POINTER(Bsr), P, P,
+                                  C.POINTER(PcgOpts), P, I32, P]),
     "lcs_newton_destroy": (I32, [P]),
     "lcs_newton_step": (I32, [P, C.POINTER(NewtonStats)]),
     "lcs_newton_step_host": (I32, [P, P, P, P, P, C.POINTER(NewtonStats)]),

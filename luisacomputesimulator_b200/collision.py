@@ -30,6 +30,63 @@ def _dev(t, dtype):
     return t
 
 
+class Forest:
+    """Per-scene LBVHs of many concatenated scenes in one set of arrays (batched solver).
+
+    elem_offsets / vert_offsets: n_scenes + 1 prefix offsets of the scenes' elements and
+    vertices.  Each scene's tree equals ``LBVH`` built on that scene alone."""
+
+    def __init__(self, kind: int, elem_offsets, vert_offsets):
+        import numpy as np
+        self.lib = A.load()
+        self.kind = kind
+        eo = np.ascontiguousarray(elem_offsets, np.uint32)
+        vo = np.ascontiguousarray(vert_offsets, np.uint32)
+        self.elem_offsets, self.vert_offsets = eo, vo
+        self.n_scenes = len(eo) - 1
+        h = C.c_void_p()
+        A.check(self.lib.lcs_forest_create(kind, self.n_scenes, eo.ctypes.data_as(C.c_void_p),
+                                           vo.ctypes.data_as(C.c_void_p), C.byref(h)), "lcs_forest_create")
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.lcs_forest_destroy(self.h)
+            self.h = None
+
+    def build(self, x, elems):
+        A.check(self.lib.lcs_forest_build(self.h, ptr(x), ptr(elems), stream()), "lcs_forest_build")
+
+    def update_refit(self, thickness, x0, x1, elems):
+        A.check(self.lib.lcs_forest_update_refit(self.h, ptr(thickness), ptr(x0), ptr(x1), ptr(elems), stream()),
+                "lcs_forest_update_refit")
+
+    def query_vf(self, x0, x1, vert_scene, d_hat, thickness, pairs, d_count):
+        A.check(self.lib.lcs_forest_query_vf(self.h, ptr(x0), ptr(x1), x0.shape[0], ptr(vert_scene), ptr(d_hat),
+                                             ptr(thickness), ptr(pairs), pairs.shape[0], ptr(d_count), stream()),
+                "lcs_forest_query_vf")
+
+    def query_ee(self, x0, x1, edges, d_hat, thickness, pairs, d_count):
+        A.check(self.lib.lcs_forest_query_ee(self.h, ptr(x0), ptr(x1), ptr(edges), ptr(d_hat), ptr(thickness),
+                                             ptr(pairs), pairs.shape[0], ptr(d_count), stream()), "lcs_forest_query_ee")
+
+    def check_health(self):
+        ok = C.c_int(0)
+        A.check(self.lib.lcs_forest_health(self.h, C.byref(ok), stream()), "lcs_forest_health")
+        return bool(ok.value)
+
+    def export_scene(self, scene):
+        """(parent, children, object_idx, morton_sorted, sorted_get_original, node_aabb, global_aabb) of one
+        scene's tree in the layout of LBVH.export (local ids)."""
+        n = int(self.elem_offsets[scene + 1] - self.elem_offsets[scene])
+        nn = 2 * n - 1
+        d = lambda *shape, dt=torch.int32: torch.zeros(shape, dtype=dt, device="cuda")  # noqa: E731
+        out = (d(nn), d(nn, 2), d(nn), d(n, dt=torch.int64), d(n), d(nn, 8, dt=torch.float32), d(6, dt=torch.float32))
+        A.check(self.lib.lcs_forest_export_scene(self.h, scene, *[ptr(t) for t in out], stream()),
+                "lcs_forest_export_scene")
+        return out
+
+
 class LBVH:
     """One LBVH over vertices, edges or faces (LbvhData + LBVH, lbvh.h:79-229)."""
 
@@ -192,6 +249,13 @@ class NarrowPhasesDetector:
         A.check(self.lib.lcs_ccd_ee(ptr(self.broad_phase_list_ee), ptr(self.count_view(1)), self.cap_ee, ptr(x0),
                                     ptr(x1), ptr(edges), ptr(body), ptr(offset), ptr(self.toi), ptr(toi_per_pair),
                                     flags, stream()), "ccd_ee")
+
+    def batched_ccd_query(self, is_ee, pairs, d_count, x0, x1, elems, body, offset, vert_scene, toi_per_scene,
+                          fp64=False):
+        """Batched scenes: the step bound of each candidate lowered into its own scene's bound."""
+        A.check(self.lib.lcs_ccd_batch(int(bool(is_ee)), ptr(pairs), ptr(d_count), pairs.shape[0], ptr(x0), ptr(x1),
+                                       ptr(elems), ptr(body), ptr(offset), ptr(vert_scene), ptr(toi_per_scene), None,
+                                       A.LCS_CCD_FP64 if fp64 else 0, stream()), "lcs_ccd_batch")
 
     # -- DCD (narrow_phase.cpp:771-1249)
     def vf_dcd_query_repulsion(self, x, faces, body, vert_area, face_area, d_hat, offset, kappa):

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "lcs_common.cuh"
+#include "lbvh_common.cuh"
 #include "lcs_internal.h"
 #include "radix_sort.cuh"
 
@@ -43,44 +44,6 @@ struct lcs_bvh {
 };
 
 namespace {
-
-__device__ __forceinline__ uint32_t expand_bits(uint32_t v)
-{
-    v = (v | (v << 16)) & 0x030000FFu;
-    v = (v | (v << 8)) & 0x0300F00Fu;
-    v = (v | (v << 4)) & 0x030C30C3u;
-    return (v | (v << 2)) & 0x09249249u;
-}
-
-// make_morton32, lbvh.cpp:112-124
-__device__ __forceinline__ uint32_t morton32(float px, float py, float pz)
-{
-    float x = fmn(fmx(px * 1024.0f, 0.0f), 1023.0f);
-    float y = fmn(fmx(py * 1024.0f, 0.0f), 1023.0f);
-    float z = fmn(fmx(pz * 1024.0f, 0.0f), 1023.0f);
-    return (expand_bits((uint32_t)x) << 2) | (expand_bits((uint32_t)y) << 1) | expand_bits((uint32_t)z);
-}
-
-__device__ __forceinline__ void elem_box(int kind, const float4* __restrict__ x, const uint32_t* __restrict__ elems,
-                                         uint32_t e, v3& mn, v3& mx, v3& c)
-{
-    if (kind == LCS_TREE_VERT) {
-        v3 p = ld3(x, e);
-        mn = p; mx = p; c = p;
-    } else if (kind == LCS_TREE_EDGE) {
-        uint2 ed = __ldg(reinterpret_cast<const uint2*>(elems) + e);
-        v3 p0 = ld3(x, ed.x), p1 = ld3(x, ed.y);
-        mn = min3(p0, p1);
-        mx = max3(p0, p1);
-        c = 0.5f * (p0 + p1);  // lbvh.cpp:468
-    } else {
-        uint4 f = __ldg(reinterpret_cast<const uint4*>(elems) + e);
-        v3 p0 = ld3(x, f.x), p1 = ld3(x, f.y), p2 = ld3(x, f.z);
-        mn = min3(p0, min3(p1, p2));
-        mx = max3(p0, max3(p1, p2));
-        c = 0.333333f * ((p0 + p1) + p2);  // lbvh.cpp:488
-    }
-}
 
 // fn_reduce_{vert,edge,face}_tree_global_aabb, lbvh.cpp:449-491: centres + per-256 partials
 __global__ void __launch_bounds__(256) k_reduce_pass1(int kind, const float4* __restrict__ x,
@@ -174,11 +137,6 @@ __global__ void k_apply_sorted(const uint32_t* __restrict__ m30s, const uint32_t
     }
 }
 
-__device__ __forceinline__ int cp_ij(uint64_t mi, int j, const uint64_t* __restrict__ ms, int n)
-{
-    return (j >= 0 && j < n) ? __clzll((long long)(mi ^ ms[j])) : -1;
-}
-
 // fn_build_inner_nodes with determineRange / findSplit, lbvh.cpp:204-291, 541-596; also the
 // traversal records' child codes and the child -> parent slot map
 __global__ void k_build_inner(const uint64_t* __restrict__ ms, const uint32_t* __restrict__ sgo, uint32_t n,
@@ -249,41 +207,6 @@ __global__ void k_check(const uint2* __restrict__ children, const uint32_t* __re
     }
 }
 
-__device__ __forceinline__ void leaf_box(int kind, uint32_t e, const float* __restrict__ thickness,
-                                         const float4* __restrict__ x0, const float4* __restrict__ x1,
-                                         const uint32_t* __restrict__ elems, v3& mn, v3& mx)
-{
-    float th;
-    if (kind == LCS_TREE_VERT) {
-        v3 a = ld3(x0, e), b = ld3(x1, e);
-        mn = min3(a, b);
-        mx = max3(a, b);
-        th = __ldg(&thickness[e]);
-    } else if (kind == LCS_TREE_EDGE) {
-        uint2 ed = __ldg(reinterpret_cast<const uint2*>(elems) + e);
-        v3 s0 = ld3(x0, ed.x), s1 = ld3(x0, ed.y), e0 = ld3(x1, ed.x), e1 = ld3(x1, ed.y);
-        mn = min3(min3(s0, s1), min3(e0, e1));
-        mx = max3(max3(s0, s1), max3(e0, e1));
-        th = __ldg(&thickness[ed.x]);
-    } else {
-        uint4 f = __ldg(reinterpret_cast<const uint4*>(elems) + e);
-        v3 s0 = ld3(x0, f.x), s1 = ld3(x0, f.y), s2 = ld3(x0, f.z);
-        v3 e0 = ld3(x1, f.x), e1 = ld3(x1, f.y), e2 = ld3(x1, f.z);
-        mn = min3(min3(s0, min3(s1, s2)), min3(e0, min3(e1, e2)));
-        mx = max3(max3(s0, max3(s1, s2)), max3(e0, max3(e1, e2)));
-        th = __ldg(&thickness[f.x]);
-    }
-    mn = mk3(mn.x - th, mn.y - th, mn.z - th);
-    mx = mk3(mx.x + th, mx.y + th, mx.z + th);
-}
-
-__device__ __forceinline__ void store_slot(float4* wide, uint32_t s, v3 mn, v3 mx, uint32_t code)
-{
-    float4* r = wide + 4 * (s >> 1) + 2 * (s & 1u);
-    __stcg(r, make_float4(mn.x, mn.y, mn.z, __uint_as_float(code)));
-    __stcg(r + 1, make_float4(mx.x, mx.y, mx.z, 0.0f));
-}
-
 __device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v)
 {
     unsigned old;
@@ -333,11 +256,6 @@ __global__ void k_leaves_refit(int kind, uint32_t n, const uint32_t* __restrict_
             p = parent[p];
         }
     }
-}
-
-__device__ __forceinline__ bool overlap(float4 mn, float4 mx, const float* q)
-{
-    return mn.x < q[3] && mn.y < q[4] && mn.z < q[5] && mx.x > q[0] && mx.y > q[1] && mx.z > q[2];
 }
 
 // query_template2 (lbvh.cpp:293-360) for fn_query_from_verts_v2 (EE = false, lbvh.cpp:776-808)

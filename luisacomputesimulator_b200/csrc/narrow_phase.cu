@@ -57,7 +57,8 @@ __global__ void __launch_bounds__(256) k_ccd(const uint2* __restrict__ pairs, co
                                              const float4* __restrict__ x0, const float4* __restrict__ x1,
                                              const uint32_t* __restrict__ elems, const uint32_t* __restrict__ body,
                                              const float* __restrict__ offset, float* d_toi,
-                                             float* __restrict__ toi_per_pair, int flags)
+                                             float* __restrict__ toi_per_pair, int flags,
+                                             const uint32_t* __restrict__ vscene)
 {
     const bool fp64_final = (flags & LCS_CCD_FP64_FINAL) != 0;
     const uint32_t n = pair_count(d_count, cap);
@@ -90,8 +91,14 @@ __global__ void __launch_bounds__(256) k_ccd(const uint2* __restrict__ pairs, co
             toi = F64 ? __double2float_rz(accd_ccd_f64<EE>(a, b, th)) : accd_ccd<EE>(a, b, th, fp64_final);
         }
         if (toi_per_pair) toi_per_pair[p] = toi;
-        local = fmn(local, toi / 1.25f);
+        if (vscene) {  // batched scenes: the bound of the pair's own scene
+            const float g = toi / 1.25f;
+            if (g < 1.0f) atomic_min_float(d_toi + __ldg(&vscene[EE ? v[0] : pr.x]), g);
+        } else {
+            local = fmn(local, toi / 1.25f);
+        }
     }
+    if (vscene) return;
     const float m = block_min(local);
     if (threadIdx.x == 0 && m < 1.0f) atomic_min_float(d_toi, m);
 }
@@ -504,7 +511,7 @@ extern "C" int lcs_ccd_vf(const uint32_t* pairs, const uint32_t* d_count, uint32
     auto kern = (flags & LCS_CCD_FP64) ? k_ccd<false, true> : k_ccd<false, false>;
     kern<<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
         reinterpret_cast<const uint2*>(pairs), d_count, capacity, reinterpret_cast<const float4*>(x0),
-        reinterpret_cast<const float4*>(x1), faces, body, offset, d_toi, toi_per_pair, flags);
+        reinterpret_cast<const float4*>(x1), faces, body, offset, d_toi, toi_per_pair, flags, nullptr);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
@@ -520,7 +527,25 @@ extern "C" int lcs_ccd_ee(const uint32_t* pairs, const uint32_t* d_count, uint32
     auto kern = (flags & LCS_CCD_FP64) ? k_ccd<true, true> : k_ccd<true, false>;
     kern<<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
         reinterpret_cast<const uint2*>(pairs), d_count, capacity, reinterpret_cast<const float4*>(x0),
-        reinterpret_cast<const float4*>(x1), edges, body, offset, d_toi, toi_per_pair, flags);
+        reinterpret_cast<const float4*>(x1), edges, body, offset, d_toi, toi_per_pair, flags, nullptr);
+    lcs_count_launch();
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+extern "C" int lcs_ccd_batch(int is_ee, const uint32_t* pairs, const uint32_t* d_count, uint32_t capacity,
+                             const float* x0, const float* x1, const uint32_t* elems, const uint32_t* body,
+                             const float* offset, const uint32_t* vert_scene, float* d_toi_per_scene,
+                             float* toi_per_pair, int flags, lcs_stream stream)
+{
+    if (!d_count || !x0 || !x1 || !elems || !body || !offset || !vert_scene || !d_toi_per_scene || (capacity && !pairs))
+        return lcs_fail(LCS_ERR_INVALID, "lcs_ccd_batch: bad argument");
+    if (capacity == 0) return LCS_OK;
+    const bool f64 = (flags & LCS_CCD_FP64) != 0;
+    auto kern = is_ee ? (f64 ? k_ccd<true, true> : k_ccd<true, false>) : (f64 ? k_ccd<false, true> : k_ccd<false, false>);
+    kern<<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
+        reinterpret_cast<const uint2*>(pairs), d_count, capacity, reinterpret_cast<const float4*>(x0),
+        reinterpret_cast<const float4*>(x1), elems, body, offset, d_toi_per_scene, toi_per_pair, flags, vert_scene);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;

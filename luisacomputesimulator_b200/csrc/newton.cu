@@ -317,6 +317,63 @@ __global__ void k_pcg_to_status(const lcs_pcg_stats* ps, Status* st)
     st->pcg_status = ps->status;
 }
 
+// ---- batched scenes: per-scene step bound, small-step and Dirichlet tests
+__global__ void k_b_reset(uint32_t S, float* bsc)
+{
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+        bsc[s] = 1.0f;          // toi
+        bsc[S + s] = 0.0f;      // max |dx|
+        bsc[2 * S + s] = 0.0f;  // Dirichlet error
+    }
+}
+
+// lane-aggregated max into per-scene slots (vertices of a warp usually share a scene)
+__device__ __forceinline__ void scene_max(float* slots, uint32_t s, float m)
+{
+    const uint32_t mask = __activemask();
+    if (mask == 0xFFFFFFFFu) {  // the same for every lane of the warp
+        const uint32_t s0 = __shfl_sync(mask, s, 0);
+        if (__all_sync(mask, s == s0)) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(mask, m, o));
+            if (lane_id() == 0 && m > 0.0f) atomic_max_pos(slots + s, m);
+            return;
+        }
+    }
+    if (m > 0.0f) atomic_max_pos(slots + s, m);
+}
+
+__global__ void k_b_apply_unit(uint32_t n, const uint32_t* __restrict__ vscene, uint32_t S,
+                               const float4* __restrict__ x0, const float4* __restrict__ dx, float4* __restrict__ x,
+                               float* bsc)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 a = x0[i], d = dx[i];
+        x[i] = make_float4(a.x + d.x, a.y + d.y, a.z + d.z, 0.0f);
+        scene_max(bsc + S, vscene[i], sqrtf(d.x * d.x + d.y * d.y + d.z * d.z));
+    }
+}
+
+__global__ void k_b_apply_final(uint32_t n, const uint32_t* __restrict__ vscene, uint32_t S,
+                                const float4* __restrict__ x0, const float4* __restrict__ dx, float4* __restrict__ x,
+                                const uint8_t* __restrict__ pinned, const float4* __restrict__ x_tilde, float* bsc)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t s = vscene[i];
+        const float alpha = bsc[s];
+        const float4 a = x0[i], d = dx[i];
+        const float4 r = make_float4(a.x + alpha * d.x, a.y + alpha * d.y, a.z + alpha * d.z, 0.0f);
+        x[i] = r;
+        float m = 0.0f;
+        if (pinned && pinned[i]) {
+            const float4 t = x_tilde[i];
+            const float ex = r.x - t.x, ey = r.y - t.y, ez = r.z - t.z;
+            m = sqrtf(ex * ex + ey * ey + ez * ez);
+        }
+        scene_max(bsc + 2 * S, s, m);
+    }
+}
+
 template <typename T>
 cudaError_t dalloc(T*& p, size_t count)
 {
@@ -375,6 +432,20 @@ struct lcs_newton {
     lcs_pcg* pcg = nullptr;
     Status *st = nullptr, *h_st = nullptr;
     float4 *h_x = nullptr, *h_v = nullptr, *h_x_iter = nullptr;  // pinned host mirrors (plain loop)
+    // batched scenes (lcs_newton_create_batch): scene s owns vertices [voff[s], voff[s+1]) and
+    // its faces/edges; trees are forests, step bounds, small-step tests and PCG are per scene
+    bool batch = false;
+    uint32_t S = 1;
+    int cluster = 4;
+    std::vector<uint32_t> h_voff, h_foff, h_eoff;
+    uint32_t *vscene = nullptr, *voff_d = nullptr, *active = nullptr, *h_active = nullptr;
+    lcs_forest *face_forest = nullptr, *edge_forest = nullptr;
+    float* bsc = nullptr;           // device: toi[S], max_dx[S], dirichlet[S]
+    float* h_bsc = nullptr;         // pinned mirror
+    lcs_pcg_stats *bpcg = nullptr, *h_bpcg = nullptr;
+    std::vector<int32_t> sc_iters, sc_pcg;  // this step, per scene
+    std::vector<float> sc_toi, sc_rel;
+    std::vector<uint8_t> sc_done;
     // bookkeeping
     double time = 0.0;
     int64_t total_newton = 0, total_pcg = 0;
@@ -507,6 +578,10 @@ void mark(lcs_newton* h, int phase)
 int host_readback(lcs_newton* h)
 {
     LCS_CUDA_TRY(cudaMemcpyAsync(h->h_st, h->st, sizeof(Status), cudaMemcpyDeviceToHost, h->s));
+    if (h->batch) {
+        LCS_CUDA_TRY(cudaMemcpyAsync(h->h_bsc, h->bsc, 3 * sizeof(float) * h->S, cudaMemcpyDeviceToHost, h->s));
+        LCS_CUDA_TRY(cudaMemcpyAsync(h->h_bpcg, h->bpcg, sizeof(lcs_pcg_stats) * h->S, cudaMemcpyDeviceToHost, h->s));
+    }
     LCS_CUDA_TRY(cudaStreamSynchronize(h->s));
     return LCS_OK;
 }
@@ -524,6 +599,23 @@ int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint32_t* cnt
     const float* X0 = reinterpret_cast<const float*>(x0);
     const float* X1 = reinterpret_cast<const float*>(x1);
     int rc;
+    if (h->batch) {  // forests of per-scene trees, same two lanes
+        LCS_CUDA_TRY(cudaEventRecord(h->fork, h->s));
+        LCS_CUDA_TRY(cudaStreamWaitEvent(h->s2, h->fork, 0));
+        if ((rc = lcs_forest_update_refit(h->edge_forest, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->edges), h->s2)))
+            return rc;
+        if ((rc = lcs_forest_query_ee(h->edge_forest, X0, X1, reinterpret_cast<const uint32_t*>(h->edges), h->dhat,
+                                      h->offset, reinterpret_cast<uint32_t*>(h->bp_ee), h->cap_ee, cnt_ee, h->s2)))
+            return rc;
+        if ((rc = lcs_forest_update_refit(h->face_forest, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->faces), h->s)))
+            return rc;
+        if ((rc = lcs_forest_query_vf(h->face_forest, X0, X1, h->V, h->vscene, h->dhat, h->offset,
+                                      reinterpret_cast<uint32_t*>(h->bp_vf), h->cap_vf, cnt_vf, h->s)))
+            return rc;
+        LCS_CUDA_TRY(cudaEventRecord(h->join, h->s2));
+        LCS_CUDA_TRY(cudaStreamWaitEvent(h->s, h->join, 0));
+        return LCS_OK;
+    }
     if (!h->plain && h->s2) {
         // two independent lanes: face tree + VF queries here, edge tree + EE queries on s2; both are
         // latency-bound tree walks that leave most of the GPU idle when run one after the other
@@ -583,6 +675,10 @@ int newton_iteration(lcs_newton* h)
         mark(h, kPhMaterial);
         k_reset_status<<<1, 32, 0, h->s>>>(h->st);
         lcs_count_launch();
+        if (h->batch) {
+            k_b_reset<<<grid_for(h->S, 256), 256, 0, h->s>>>(h->S, h->bsc);
+            lcs_count_launch();
+        }
         if (h->plain) {  // x_iter_start copied to the host for host_apply_dx (newton_solver.cpp:4196-4198)
             if ((rc = copy_x_to_host(h, h->x))) return rc;
         }
@@ -639,7 +735,12 @@ int newton_iteration(lcs_newton* h)
                        (h->fp64 ? LCS_PCG_FP64_DOTS : 0) | (h->plain ? LCS_PCG_PLAIN : LCS_PCG_NO_STATS) |
                            (h->pipelined ? LCS_PCG_PIPELINED : 0)};
         lcs_pcg_stats ps;
-        if (h->sell)
+        if (h->batch)
+            rc = lcs_pcg_solve_batch(h->pcg, h->S, h->voff_d, &h->h_voff[h->S], h->active,
+                                     reinterpret_cast<const float*>(h->diag), h->nnz_mat ? &A : nullptr, &Bc,
+                                     reinterpret_cast<const float*>(h->b), reinterpret_cast<float*>(h->dx), &o, h->bpcg,
+                                     h->cluster, h->s);
+        else if (h->sell)
             rc = lcs_pcg_solve_sell(h->pcg, reinterpret_cast<const float*>(h->diag), h->sell_ptr, h->sell_col,
                                     h->mat_val, &Bc, reinterpret_cast<const float*>(h->b),
                                     reinterpret_cast<float*>(h->dx), &o, nullptr, h->s);
@@ -648,14 +749,19 @@ int newton_iteration(lcs_newton* h)
                                reinterpret_cast<const float*>(h->b), reinterpret_cast<float*>(h->dx), &o,
                                h->plain ? &ps : nullptr, h->s);
         if (rc != LCS_OK && rc != LCS_ERR_NAN) return rc;
-        k_pcg_to_status<<<1, 1, 0, h->s>>>(lcs_pcg_device_stats(h->pcg), h->st);
-        lcs_count_launch();
+        if (!h->batch) {
+            k_pcg_to_status<<<1, 1, 0, h->s>>>(lcs_pcg_device_stats(h->pcg), h->st);
+            lcs_count_launch();
+        }
         if (h->plain) {  // device_solve copies cgX to the host at its end (precond_cg.cpp:757-758)
             if ((rc = copy_x_to_host(h, h->dx))) return rc;
         }
         // line_search (newton_solver.cpp:3685-3884): CCD step bound
         mark(h, kPhCcdBroad);
-        k_apply_unit<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->st);
+        if (h->batch)
+            k_b_apply_unit<<<G(V), 256, 0, h->s>>>(V, h->vscene, h->S, h->x_iter, h->dx, h->x, h->bsc);
+        else
+            k_apply_unit<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->st);
         lcs_count_launch();
         if ((rc = broad_phase(h, h->x_iter, h->x, &h->st->cnt[3], &h->st->cnt[4]))) return rc;
         if (h->plain) {
@@ -681,12 +787,23 @@ int newton_iteration(lcs_newton* h)
             LCS_CUDA_TRY(cudaEventRecord(h->fork, h->s));
             LCS_CUDA_TRY(cudaStreamWaitEvent(h->s2, h->fork, 0));
         }
-        if ((rc = lcs_ccd_ee(reinterpret_cast<uint32_t*>(h->bp_ee), &h->st->cnt[4], h->cap_ee, XI, X, reinterpret_cast<const uint32_t*>(h->edges), h->body, h->offset,
-                             &h->st->toi, nullptr, ccd_flags, s_ee)))
-            return rc;
-        if ((rc = lcs_ccd_vf(reinterpret_cast<uint32_t*>(h->bp_vf), &h->st->cnt[3], h->cap_vf, XI, X, reinterpret_cast<const uint32_t*>(h->faces), h->body, h->offset,
-                             &h->st->toi, nullptr, ccd_flags, h->s)))
-            return rc;
+        if (h->batch) {
+            if ((rc = lcs_ccd_batch(1, reinterpret_cast<uint32_t*>(h->bp_ee), &h->st->cnt[4], h->cap_ee, XI, X,
+                                    reinterpret_cast<const uint32_t*>(h->edges), h->body, h->offset, h->vscene, h->bsc,
+                                    nullptr, ccd_flags, s_ee)))
+                return rc;
+            if ((rc = lcs_ccd_batch(0, reinterpret_cast<uint32_t*>(h->bp_vf), &h->st->cnt[3], h->cap_vf, XI, X,
+                                    reinterpret_cast<const uint32_t*>(h->faces), h->body, h->offset, h->vscene, h->bsc,
+                                    nullptr, ccd_flags, h->s)))
+                return rc;
+        } else {
+            if ((rc = lcs_ccd_ee(reinterpret_cast<uint32_t*>(h->bp_ee), &h->st->cnt[4], h->cap_ee, XI, X, reinterpret_cast<const uint32_t*>(h->edges), h->body, h->offset,
+                                 &h->st->toi, nullptr, ccd_flags, s_ee)))
+                return rc;
+            if ((rc = lcs_ccd_vf(reinterpret_cast<uint32_t*>(h->bp_vf), &h->st->cnt[3], h->cap_vf, XI, X, reinterpret_cast<const uint32_t*>(h->faces), h->body, h->offset,
+                                 &h->st->toi, nullptr, ccd_flags, h->s)))
+                return rc;
+        }
         if (lanes) {
             LCS_CUDA_TRY(cudaEventRecord(h->join, h->s2));
             LCS_CUDA_TRY(cudaStreamWaitEvent(h->s, h->join, 0));
@@ -694,7 +811,11 @@ int newton_iteration(lcs_newton* h)
         if (h->plain)
             if ((rc = host_readback(h))) return rc;  // ccd_get_toi
         mark(h, kPhApply);
-        k_apply_final<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->pinned, h->x_tilde, h->st);
+        if (h->batch)
+            k_b_apply_final<<<G(V), 256, 0, h->s>>>(V, h->vscene, h->S, h->x_iter, h->dx, h->x, h->pinned, h->x_tilde,
+                                                    h->bsc);
+        else
+            k_apply_final<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->pinned, h->x_tilde, h->st);
         lcs_count_launch();
         LCS_LAUNCH_CHECK();
         mark(h, kPhases);
@@ -713,7 +834,12 @@ int newton_iteration(lcs_newton* h)
             if ((rc = alloc_contact(h))) return rc;
             continue;
         }
-        if (h->h_st->pcg_status == LCS_ERR_NAN) return lcs_fail(LCS_ERR_NAN, "lcs_newton: NaN/Inf in PCG");
+        if (h->batch) {
+            for (uint32_t sc = 0; sc < h->S; ++sc)
+                if (h->h_bpcg[sc].status == LCS_ERR_NAN) return lcs_fail(LCS_ERR_NAN, "lcs_newton: NaN/Inf in PCG");
+        } else if (h->h_st->pcg_status == LCS_ERR_NAN) {
+            return lcs_fail(LCS_ERR_NAN, "lcs_newton: NaN/Inf in PCG");
+        }
         return LCS_OK;
     }
     return lcs_fail(LCS_ERR_CAPACITY, "lcs_newton: buffers kept overflowing");
@@ -721,7 +847,17 @@ int newton_iteration(lcs_newton* h)
 
 }  // namespace
 
+namespace {
+int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batch, lcs_newton** out);
+}
+
 extern "C" int lcs_newton_create(const lcs_scene_desc* d, int flags, lcs_stream stream, lcs_newton** out)
+{
+    return create_impl(d, flags, stream, false, out);
+}
+
+namespace {
+int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batch, lcs_newton** out)
 {
     if (!d || !out || !d->x || !d->faces || !d->edges || !d->mass || !d->d_hat || !d->offset || !d->vert_area ||
         !d->face_area || !d->edge_area || d->n_verts == 0 || (d->n_bending && (!d->bending || !d->bending_Q)) ||
@@ -735,6 +871,7 @@ extern "C" int lcs_newton_create(const lcs_scene_desc* d, int flags, lcs_stream 
     h->fp64 = (flags & LCS_NEWTON_FP64) != 0;
     h->profile = (flags & LCS_NEWTON_PROFILE) != 0;
     h->pipelined = (flags & LCS_NEWTON_PCG_PIPELINED) != 0;
+    h->batch = batch;
     h->V = d->n_verts;
     h->F = d->n_faces;
     h->E = d->n_edges;
@@ -798,9 +935,10 @@ extern "C" int lcs_newton_create(const lcs_scene_desc* d, int flags, lcs_stream 
     }
     std::memset(h->h_st, 0, sizeof(Status));
     int rc;
-    h->sell = !h->plain && (int64_t)h->V <= lcs_pcg_rows_capacity();
-    if ((rc = build_material_pattern(h, d)) || (rc = lcs_bvh_create(LCS_TREE_FACE, h->F, &h->face_tree)) ||
-        (rc = lcs_bvh_create(LCS_TREE_EDGE, h->E, &h->edge_tree)) || (rc = lcs_pcg_create(h->V, &h->pcg))) {
+    h->sell = !h->plain && !h->batch && (int64_t)h->V <= lcs_pcg_rows_capacity();
+    if ((rc = build_material_pattern(h, d)) ||
+        (!h->batch && (rc = lcs_bvh_create(LCS_TREE_FACE, h->F, &h->face_tree))) ||
+        (!h->batch && (rc = lcs_bvh_create(LCS_TREE_EDGE, h->E, &h->edge_tree))) || (rc = lcs_pcg_create(h->V, &h->pcg))) {
         lcs_newton_destroy(h);
         return rc;
     }
@@ -823,6 +961,146 @@ extern "C" int lcs_newton_create(const lcs_scene_desc* d, int flags, lcs_stream 
     *out = h;
     return LCS_OK;
 }
+}  // namespace
+
+extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_scenes, int flags, lcs_stream stream,
+                                       int pcg_cluster, lcs_newton** out)
+{
+    if (!descs || !out || n_scenes == 0) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: bad argument");
+    if (flags & LCS_NEWTON_PLAIN) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: the batch runs fused only");
+    if (pcg_cluster != 1 && pcg_cluster != 2 && pcg_cluster != 4 && pcg_cluster != 8 && pcg_cluster != 16)
+        return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: cluster size must be 1, 2, 4, 8 or 16");
+    const lcs_scene_desc& d0 = descs[0];
+    // concatenate the scenes: indices shifted by the vertex offset, animation groups renumbered
+    std::vector<uint32_t> voff(n_scenes + 1, 0), foff(n_scenes + 1, 0), eoff(n_scenes + 1, 0), boff(n_scenes + 1, 0);
+    uint32_t groups = 0;
+    for (uint32_t s = 0; s < n_scenes; ++s) {
+        const lcs_scene_desc& d = descs[s];
+        if (!d.x || !d.faces || !d.edges || !d.mass || !d.d_hat || !d.offset || !d.vert_area || !d.face_area ||
+            !d.edge_area || d.n_verts == 0 || d.n_faces < 2 || d.n_edges < 2 ||
+            (d.n_bending && (!d.bending || !d.bending_Q)) || !d.rest_len)
+            return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: incomplete scene description");
+        if (d.dt != d0.dt || d.gravity[0] != d0.gravity[0] || d.gravity[1] != d0.gravity[1] ||
+            d.gravity[2] != d0.gravity[2] || d.kappa != d0.kappa || d.spring_k != d0.spring_k ||
+            d.bending_k != d0.bending_k || d.dirichlet != d0.dirichlet || d.damping != d0.damping ||
+            d.nonlinear_iters != d0.nonlinear_iters || d.pcg_max_iter != d0.pcg_max_iter ||
+            d.pcg_rel_tol != d0.pcg_rel_tol || d.pcg_abs_rz_tol != d0.pcg_abs_rz_tol || d.use_floor)
+            return lcs_fail(LCS_ERR_INVALID,
+                            "lcs_newton_create_batch: scenes must share dt, gravity, stiffnesses and solver settings (floor off)");
+        voff[s + 1] = voff[s] + d.n_verts;
+        foff[s + 1] = foff[s] + d.n_faces;
+        eoff[s + 1] = eoff[s] + d.n_edges;
+        boff[s + 1] = boff[s] + d.n_bending;
+        groups += d.anim_group ? d.n_anim : 0;
+    }
+    if (groups > 127) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: more than 127 animation groups");
+    const uint32_t V = voff[n_scenes], F = foff[n_scenes], E = eoff[n_scenes], B = boff[n_scenes];
+    std::vector<float> x(4 * (size_t)V), v(4 * (size_t)V, 0.0f), Q(16 * (size_t)B), rest_len(E), vert_area(V),
+        face_area(F), edge_area(E), mass(V), dhat(V), offset(V), anim(8 * (size_t)std::max(groups, 1u), 0.0f);
+    std::vector<uint32_t> faces(4 * (size_t)F), edges(2 * (size_t)E), bend(4 * (size_t)B), body(V, kInvalid);
+    std::vector<uint8_t> pinned(V, 0);
+    std::vector<int8_t> group(V, -1);
+    uint32_t g0 = 0;
+    for (uint32_t s = 0; s < n_scenes; ++s) {
+        const lcs_scene_desc& d = descs[s];
+        const uint32_t vo = voff[s];
+        std::memcpy(&x[4 * (size_t)vo], d.x, 16 * (size_t)d.n_verts);
+        if (d.v) std::memcpy(&v[4 * (size_t)vo], d.v, 16 * (size_t)d.n_verts);
+        for (size_t k = 0; k < 4 * (size_t)d.n_faces; ++k)
+            faces[4 * (size_t)foff[s] + k] = (k % 4 == 3) ? d.faces[k] : d.faces[k] + vo;
+        for (size_t k = 0; k < 2 * (size_t)d.n_edges; ++k) edges[2 * (size_t)eoff[s] + k] = d.edges[k] + vo;
+        for (size_t k = 0; k < 4 * (size_t)d.n_bending; ++k) bend[4 * (size_t)boff[s] + k] = d.bending[k] + vo;
+        if (d.n_bending) std::memcpy(&Q[16 * (size_t)boff[s]], d.bending_Q, 64 * (size_t)d.n_bending);
+        std::memcpy(&rest_len[eoff[s]], d.rest_len, 4 * (size_t)d.n_edges);
+        std::memcpy(&vert_area[vo], d.vert_area, 4 * (size_t)d.n_verts);
+        std::memcpy(&face_area[foff[s]], d.face_area, 4 * (size_t)d.n_faces);
+        std::memcpy(&edge_area[eoff[s]], d.edge_area, 4 * (size_t)d.n_edges);
+        std::memcpy(&mass[vo], d.mass, 4 * (size_t)d.n_verts);
+        std::memcpy(&dhat[vo], d.d_hat, 4 * (size_t)d.n_verts);
+        std::memcpy(&offset[vo], d.offset, 4 * (size_t)d.n_verts);
+        if (d.body) std::memcpy(&body[vo], d.body, 4 * (size_t)d.n_verts);
+        if (d.pinned) std::memcpy(&pinned[vo], d.pinned, d.n_verts);
+        if (d.anim_group && d.n_anim) {
+            for (uint32_t k = 0; k < d.n_verts; ++k)
+                group[vo + k] = d.anim_group[k] >= 0 ? (int8_t)(d.anim_group[k] + (int)g0) : (int8_t)-1;
+            std::memcpy(&anim[8 * (size_t)g0], d.anim, 32 * (size_t)d.n_anim);
+            g0 += d.n_anim;
+        }
+    }
+    lcs_scene_desc D = d0;
+    D.n_verts = V; D.n_faces = F; D.n_edges = E; D.n_bending = B;
+    D.x = x.data(); D.v = v.data(); D.faces = faces.data(); D.edges = edges.data(); D.bending = bend.data();
+    D.bending_Q = Q.data(); D.rest_len = rest_len.data(); D.vert_area = vert_area.data();
+    D.face_area = face_area.data(); D.edge_area = edge_area.data(); D.mass = mass.data(); D.d_hat = dhat.data();
+    D.offset = offset.data(); D.body = body.data(); D.pinned = pinned.data();
+    D.anim_group = groups ? group.data() : nullptr; D.n_anim = groups; D.anim = groups ? anim.data() : nullptr;
+    lcs_newton* h = nullptr;
+    int rc = create_impl(&D, flags, stream, true, &h);
+    if (rc) return rc;
+    h->S = n_scenes;
+    h->cluster = pcg_cluster;
+    h->h_voff = voff;
+    h->h_foff = foff;
+    h->h_eoff = eoff;
+    h->sc_iters.assign(n_scenes, 0);
+    h->sc_pcg.assign(n_scenes, 0);
+    h->sc_toi.assign(n_scenes, 1.0f);
+    h->sc_rel.assign(n_scenes, 0.0f);
+    h->sc_done.assign(n_scenes, 0);
+    std::vector<uint32_t> vscene(V);
+    for (uint32_t s = 0; s < n_scenes; ++s) std::fill(vscene.begin() + voff[s], vscene.begin() + voff[s + 1], s);
+    cudaError_t e = cudaSuccess;
+    auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    A(upload(h->vscene, vscene.data(), V));
+    A(upload(h->voff_d, voff.data(), n_scenes + 1));
+    A(dalloc(h->active, n_scenes));
+    A(dalloc(h->bsc, 3 * (size_t)n_scenes));
+    A(dalloc(h->bpcg, n_scenes));
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->h_active), 4 * (size_t)n_scenes);
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->h_bsc), 12 * (size_t)n_scenes);
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->h_bpcg), sizeof(lcs_pcg_stats) * n_scenes);
+    if (e != cudaSuccess) {
+        lcs_newton_destroy(h);
+        return lcs_fail(LCS_ERR_CUDA, "lcs_newton_create_batch: allocation failed");
+    }
+    if ((rc = lcs_forest_create(LCS_TREE_FACE, n_scenes, foff.data(), voff.data(), &h->face_forest)) ||
+        (rc = lcs_forest_create(LCS_TREE_EDGE, n_scenes, eoff.data(), voff.data(), &h->edge_forest))) {
+        lcs_newton_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return LCS_OK;
+}
+
+extern "C" uint32_t lcs_newton_num_scenes(const lcs_newton* h) { return h ? h->S : 0; }
+
+extern "C" int lcs_newton_scene_stats(const lcs_newton* h, uint32_t scene, lcs_newton_stats* stats)
+{
+    if (!h || !stats || scene >= h->S) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_scene_stats: bad argument");
+    *stats = lcs_newton_stats{};
+    if (!h->batch) {
+        stats->newton_iters = (int32_t)h->total_newton;
+        stats->status = LCS_OK;
+        return LCS_OK;
+    }
+    stats->newton_iters = h->sc_iters[scene];
+    stats->pcg_iters = h->sc_pcg[scene];
+    stats->last_toi = h->sc_toi[scene];
+    stats->last_rel_residual = h->sc_rel[scene];
+    stats->status = LCS_OK;
+    return LCS_OK;
+}
+
+extern "C" int lcs_newton_download_scene(const lcs_newton* h, uint32_t scene, float* x_out, float* v_out)
+{
+    if (!h || scene >= h->S) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_download_scene: bad argument");
+    const uint32_t v0 = h->batch ? h->h_voff[scene] : 0, nv = h->batch ? h->h_voff[scene + 1] - v0 : h->V;
+    const size_t bytes = 16 * (size_t)nv;
+    if (x_out) LCS_CUDA_TRY(cudaMemcpyAsync(x_out, h->x + v0, bytes, cudaMemcpyDeviceToHost, h->s));
+    if (v_out) LCS_CUDA_TRY(cudaMemcpyAsync(v_out, h->v + v0, bytes, cudaMemcpyDeviceToHost, h->s));
+    LCS_CUDA_TRY(cudaStreamSynchronize(h->s));
+    return LCS_OK;
+}
 
 extern "C" int lcs_newton_destroy(lcs_newton* h)
 {
@@ -831,7 +1109,17 @@ extern "C" int lcs_newton_destroy(lcs_newton* h)
     free_contact(h);
     lcs_bvh_destroy(h->face_tree);
     lcs_bvh_destroy(h->edge_tree);
+    lcs_forest_destroy(h->face_forest);
+    lcs_forest_destroy(h->edge_forest);
     lcs_pcg_destroy(h->pcg);
+    {
+        void* bp[] = {h->vscene, h->voff_d, h->active, h->bsc, h->bpcg};
+        for (void* p : bp)
+            if (p) cudaFree(p);
+        if (h->h_active) cudaFreeHost(h->h_active);
+        if (h->h_bsc) cudaFreeHost(h->h_bsc);
+        if (h->h_bpcg) cudaFreeHost(h->h_bpcg);
+    }
     void* ptrs[] = {h->faces, h->edges, h->bend, h->Q, h->rest_len, h->vert_area, h->face_area, h->edge_area,
                     h->mass, h->dhat, h->offset, h->body, h->pinned, h->group, h->anim, h->rest, h->x, h->v,
                     h->x_step, h->x_iter, h->x_tilde, h->target, h->dx, h->b, h->diag, h->mat_rp, h->mat_col,
@@ -879,9 +1167,14 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
     lcs_count_launch();
     // Init LBVH once per step (newton_solver.cpp:4152-4161)
     const float* XS = reinterpret_cast<const float*>(h->x_step);
-    if ((rc = lcs_bvh_reduce_aabb(h->face_tree, XS, reinterpret_cast<const uint32_t*>(h->faces), V, h->s))) return rc;
-    if ((rc = lcs_bvh_reduce_aabb(h->edge_tree, XS, reinterpret_cast<const uint32_t*>(h->edges), V, h->s))) return rc;
-    if (h->plain) {
+    if (!h->batch) {
+        if ((rc = lcs_bvh_reduce_aabb(h->face_tree, XS, reinterpret_cast<const uint32_t*>(h->faces), V, h->s))) return rc;
+        if ((rc = lcs_bvh_reduce_aabb(h->edge_tree, XS, reinterpret_cast<const uint32_t*>(h->edges), V, h->s))) return rc;
+    }
+    if (h->batch) {
+        if ((rc = lcs_forest_build(h->face_forest, XS, reinterpret_cast<const uint32_t*>(h->faces), h->s))) return rc;
+        if ((rc = lcs_forest_build(h->edge_forest, XS, reinterpret_cast<const uint32_t*>(h->edges), h->s))) return rc;
+    } else if (h->plain) {
         if ((rc = lcs_bvh_construct_host_sort(h->face_tree, h->s))) return rc;
         if ((rc = lcs_bvh_construct_host_sort(h->edge_tree, h->s))) return rc;
     } else {
@@ -895,6 +1188,57 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
         cudaEventElapsedTime(&ms, h->ev[kPhBuild], h->ev[kPhMaterial]);
         h->phase_ms[kPhBuild] += ms;
         h->phase_launch_count[kPhBuild] += 1;
+    }
+    if (h->batch) {  // every scene runs its own Newton loop; finished scenes are switched off
+        const uint32_t S = h->S;
+        std::fill(h->sc_done.begin(), h->sc_done.end(), 0);
+        std::fill(h->sc_iters.begin(), h->sc_iters.end(), 0);
+        std::fill(h->sc_pcg.begin(), h->sc_pcg.end(), 0);
+        for (uint32_t sc = 0; sc < S; ++sc) h->h_active[sc] = 1u;
+        LCS_CUDA_TRY(cudaMemcpyAsync(h->active, h->h_active, 4 * (size_t)S, cudaMemcpyHostToDevice, h->s));
+        int iter = 0, pcg_total = 0;
+        for (iter = 0; iter < 100; ++iter) {
+            bool all = true;
+            for (uint32_t sc = 0; sc < S; ++sc) all = all && h->sc_done[sc];
+            if (all) break;
+            if ((rc = newton_iteration(h))) return rc;
+            for (uint32_t sc = 0; sc < S; ++sc) {
+                if (h->sc_done[sc]) continue;
+                h->sc_iters[sc] += 1;
+                h->sc_pcg[sc] += h->h_bpcg[sc].iterations;
+                pcg_total += h->h_bpcg[sc].iterations;
+                h->sc_toi[sc] = h->h_bsc[sc];
+                h->sc_rel[sc] = h->h_bpcg[sc].rel_residual;
+                const bool global_converged = h->h_bsc[S + sc] < 1e-2f * d.dt;
+                const bool dirichlet_converged = h->h_bsc[2 * S + sc] < 1e-3f;
+                if (global_converged || (h->sc_iters[sc] >= d.nonlinear_iters && dirichlet_converged)) {
+                    h->sc_done[sc] = 1;
+                    h->h_active[sc] = 0u;
+                }
+            }
+            LCS_CUDA_TRY(cudaMemcpyAsync(h->active, h->h_active, 4 * (size_t)S, cudaMemcpyHostToDevice, h->s));
+        }
+        k_update_velocity<<<G(V), 256, 0, h->s>>>(V, d.dt, d.damping, h->x, h->x_step, h->v);
+        lcs_count_launch();
+        LCS_LAUNCH_CHECK();
+        h->total_newton += iter;
+        h->total_pcg += pcg_total;
+        if (stats) {
+            const Status& st = *h->h_st;
+            *stats = lcs_newton_stats{};
+            stats->newton_iters = iter;
+            stats->pcg_iters = pcg_total;
+            stats->vf_candidates = st.cnt[0];
+            stats->ee_candidates = st.cnt[1];
+            stats->contact_pairs = st.cnt[2];
+            stats->ccd_vf_candidates = st.cnt[3];
+            stats->ccd_ee_candidates = st.cnt[4];
+            stats->status = LCS_OK;
+            stats->retries = h->retries;
+            stats->host_ms =
+                std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_host0).count();
+        }
+        return LCS_OK;
     }
     bool global_converged = false, dirichlet_converged = false;
     int iter = 0, pcg_total = 0;

@@ -967,6 +967,211 @@ __global__ void __launch_bounds__(BS, 3) k_pcg_pipe(RowArgs a, float4* pg2)
     }
 }
 
+// ------------------------------------------------------------------------ batched scenes
+// Many independent systems (one per scene, rows [roff[s], roff[s+1])) solved in one launch: one
+// thread-block cluster per scene, synchronised by the hardware cluster barrier, with the scene's
+// own alpha, beta and stop decision (the recurrences and stop rules of k_pcg_fused).  The rows of a
+// scene are cut into chunks of 256; chunk k belongs to CTA k mod C of the cluster, thread t to row
+// 256k + t (the SpMV uses 4 lanes per row).  Every dot product is summed per chunk in a fixed tree
+// and then over the chunks in a fixed order, so a scene's result does not depend on the cluster
+// size C nor on the other scenes of the launch.  Vectors live in global memory (L2-resident per
+// scene); cross-CTA reads use ld.cg.
+constexpr int kBatchThreads = 256;
+constexpr int kBatchLanes = 4;
+
+struct BatchArgs {
+    const uint32_t* roff;    // S + 1
+    const uint32_t* active;  // S (0: skip the scene, x = 0) or null
+    const float4* diag;
+    Bsr A, B;
+    const float4* b;
+    float4* x;
+    float4 *r, *z, *p, *q, *minv;
+    double* cpart;           // 4 doubles per chunk; chunk k of scene s at (roff[s] >> 8) + s + k
+    int max_iter;
+    float rel_tol, abs_rz_tol;
+    int check_every;
+    int fp64;
+    lcs_pcg_stats* stats;    // S
+};
+
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t cluster_ctas()
+{
+    uint32_t n;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(n));
+    return n;
+}
+
+// fixed-tree sum of one value per thread (256 threads) -> thread 0
+__device__ __forceinline__ double chunk_sum(double v, double* s_w)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    if (lane_id() == 0) s_w[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int w = 0; w < kBatchThreads / 32; ++w) t += s_w[w];
+    __syncthreads();
+    return t;
+}
+
+// sum over a scene's chunks in a fixed order, the same in every CTA of the cluster
+__device__ __forceinline__ void scene_sum(const double* cp, uint32_t nchunks, int k, int count, double* out,
+                                          double* s_out)
+{
+    if (threadIdx.x < 32) {
+        double v[2] = {0.0, 0.0};
+        for (uint32_t c = threadIdx.x; c < nchunks; c += 32)
+            for (int j = 0; j < count; ++j) v[j] += __ldcg(&cp[4 * c + k + j]);
+        for (int j = 0; j < count; ++j) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v[j] += __shfl_xor_sync(0xFFFFFFFFu, v[j], o);
+        }
+        if (threadIdx.x == 0)
+            for (int j = 0; j < count; ++j) s_out[j] = v[j];
+    }
+    __syncthreads();
+    for (int j = 0; j < count; ++j) out[j] = s_out[j];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kBatchThreads) k_pcg_batch(BatchArgs a)
+{
+    __shared__ double s_w[kBatchThreads / 32];
+    __shared__ double s_out[2];
+    __shared__ double s_pq[kBatchThreads];
+    const uint32_t C = cluster_ctas(), rank = cluster_rank();
+    const uint32_t s = blockIdx.x / C;
+    const uint32_t r0 = a.roff[s], r1 = a.roff[s + 1], nrows = r1 - r0;
+    const uint32_t nchunks = (nrows + kBatchThreads - 1) / kBatchThreads;
+    double* cp = a.cpart + 4 * (size_t)((r0 >> 8) + s);
+    const uint32_t t = threadIdx.x;
+    const bool on = !a.active || a.active[s] != 0u;  // uniform over the cluster
+    for (uint32_t k = rank; k < nchunks; k += C) {
+        const uint32_t i = r0 + k * kBatchThreads + t;
+        if (i >= r1) continue;
+        a.x[i] = make_float4(0, 0, 0, 0);
+        if (!on) continue;
+        a.r[i] = a.b[i];
+        a.p[i] = make_float4(0, 0, 0, 0);
+        const float4 c0 = a.diag[3 * i], c1 = a.diag[3 * i + 1], c2 = a.diag[3 * i + 2];
+        const float aa = c0.x, bb = c1.x, c = c2.x, d = c0.y, e = c1.y, f = c2.y, g = c0.z, h = c1.z, kk = c2.z;
+        const float A = e * kk - f * h, B = f * g - d * kk, Cc = d * h - e * g;
+        const float id = 1.0f / (aa * A + bb * B + c * Cc);
+        a.minv[3 * i + 0] = make_float4(A * id, B * id, Cc * id, 0.0f);
+        a.minv[3 * i + 1] = make_float4((c * h - bb * kk) * id, (aa * kk - c * g) * id, (bb * g - aa * h) * id, 0.0f);
+        a.minv[3 * i + 2] = make_float4((bb * f - c * e) * id, (c * d - aa * f) * id, (aa * e - bb * d) * id, 0.0f);
+    }
+    if (!on) {
+        if (rank == 0 && t == 0) a.stats[s] = lcs_pcg_stats{0, 0.0f, 0.0f, LCS_OK};
+        return;
+    }
+    float rz_old = 0.0f, norm_r0 = 0.0f, norm_r = 0.0f, rz = 0.0f;
+    int iter = 0, status = 0;
+    for (iter = 0; iter < a.max_iter; ++iter) {
+        // z = Minv r ; r.r ; r.z per chunk
+        for (uint32_t k = rank; k < nchunks; k += C) {
+            const uint32_t i = r0 + k * kBatchThreads + t;
+            double drr = 0.0, drz = 0.0;
+            if (i < r1) {
+                const float4 rv = a.r[i];
+                const float3 zv = mv12(a.minv + 3 * (size_t)i, rv);
+                a.z[i] = make_float4(zv.x, zv.y, zv.z, 0.0f);
+                if (a.fp64) {
+                    drr = (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z;
+                    drz = (double)rv.x * zv.x + (double)rv.y * zv.y + (double)rv.z * zv.z;
+                } else {
+                    drr = __fmaf_rn(rv.z, rv.z, __fmaf_rn(rv.y, rv.y, rv.x * rv.x));
+                    drz = __fmaf_rn(rv.z, zv.z, __fmaf_rn(rv.y, zv.y, rv.x * zv.x));
+                }
+            }
+            const double srr = chunk_sum(drr, s_w), srz = chunk_sum(drz, s_w);
+            if (t == 0) {
+                cp[4 * k + 0] = srr;
+                cp[4 * k + 1] = srz;
+            }
+        }
+        cluster_sync_all();
+        double red[2];
+        scene_sum(cp, nchunks, 0, 2, red, s_out);
+        const float rr = (float)red[0];
+        rz = (float)red[1];
+        const float beta = safe_div(rz, rz_old);
+        rz_old = rz;
+        norm_r = sqrtf(rr);
+        if (iter == 0) norm_r0 = norm_r;
+        if (iter % a.check_every == 0) {
+            if (isnan(rz) || isinf(rz)) { status = LCS_ERR_NAN; break; }
+            if (rz < a.abs_rz_tol) break;
+            if (a.rel_tol > 0.0f && norm_r <= a.rel_tol * norm_r0) break;
+        }
+        for (uint32_t k = rank; k < nchunks; k += C) {
+            const uint32_t i = r0 + k * kBatchThreads + t;
+            if (i < r1) {
+                const float4 zv = a.z[i], pv = a.p[i];
+                a.p[i] = make_float4(zv.x + beta * pv.x, zv.y + beta * pv.y, zv.z + beta * pv.z, 0.0f);
+            }
+        }
+        cluster_sync_all();
+        // q = A p (4 lanes per row) ; p.q per chunk
+        for (uint32_t k = rank; k < nchunks; k += C) {
+            const uint32_t base = r0 + k * kBatchThreads;
+            const uint32_t lig = t % kBatchLanes;
+            for (uint32_t rr_ = t / kBatchLanes; rr_ < (uint32_t)kBatchThreads; rr_ += kBatchThreads / kBatchLanes) {
+                const uint32_t row = base + rr_ < r1 ? base + rr_ : r1 - 1;  // whole groups stay converged
+                const float3 qv = row_product<kBatchLanes>(row, lig, a.diag, a.A, a.B, a.p);
+                if (lig == 0) {
+                    double d = 0.0;
+                    if (base + rr_ < r1) {
+                        a.q[row] = make_float4(qv.x, qv.y, qv.z, 0.0f);
+                        const float4 pv = __ldcg(&a.p[row]);
+                        d = a.fp64 ? (double)pv.x * qv.x + (double)pv.y * qv.y + (double)pv.z * qv.z
+                                   : (double)__fmaf_rn(pv.z, qv.z, __fmaf_rn(pv.y, qv.y, pv.x * qv.x));
+                    }
+                    s_pq[rr_] = d;
+                }
+            }
+            __syncthreads();
+            const double spq = chunk_sum(s_pq[t], s_w);
+            if (t == 0) cp[4 * k + 2] = spq;
+        }
+        cluster_sync_all();
+        double pq;
+        scene_sum(cp, nchunks, 2, 1, &pq, s_out);
+        const float alpha = safe_div(rz, (float)pq);
+        for (uint32_t k = rank; k < nchunks; k += C) {
+            const uint32_t i = r0 + k * kBatchThreads + t;
+            if (i < r1) {
+                const float4 pv = a.p[i], qv = __ldcg(&a.q[i]), xv = a.x[i], rv = a.r[i];
+                a.x[i] = make_float4(xv.x + alpha * pv.x, xv.y + alpha * pv.y, xv.z + alpha * pv.z, 0.0f);
+                a.r[i] = make_float4(rv.x - alpha * qv.x, rv.y - alpha * qv.y, rv.z - alpha * qv.z, 0.0f);
+            }
+        }
+    }
+    if (rank == 0 && t == 0) {
+        lcs_pcg_stats st;
+        st.iterations = iter;
+        st.rel_residual = norm_r0 > 0.0f ? norm_r / norm_r0 : 0.0f;
+        st.dot_rz = rz_old;
+        st.status = status;
+        a.stats[s] = st;
+    }
+}
+
 }  // namespace
 
 struct lcs_pcg {
@@ -980,6 +1185,8 @@ struct lcs_pcg {
     lcs_pcg_stats* d_stats = nullptr;
     int fused_grid = 0;
     int rows_capacity = -1;  // most rows the row-resident solve can hold co-resident (-1: not queried)
+    double* cpart = nullptr;  // batched solve: per-chunk partial sums
+    size_t cpart_cap = 0;     // chunks
 };
 
 static constexpr int kRowLanes = 4;
@@ -1025,7 +1232,7 @@ extern "C" int lcs_pcg_create(uint32_t n, lcs_pcg** out)
 extern "C" int lcs_pcg_destroy(lcs_pcg* p)
 {
     if (!p) return LCS_OK;
-    void* ptrs[] = {p->r, p->z, p->p, p->q, p->minv, p->part, p->part_f, p->scal, p->bar, p->d_stats};
+    void* ptrs[] = {p->r, p->z, p->p, p->q, p->minv, p->part, p->part_f, p->scal, p->bar, p->d_stats, p->cpart};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (p->h_scal) cudaFreeHost(p->h_scal);
@@ -1340,5 +1547,60 @@ extern "C" int lcs_pcg_solve_noalloc(uint32_t n, const float* diag, const lcs_bs
         LCS_CUDA_TRY(cudaStreamSynchronize(s));
         if (stats->status != LCS_OK) return lcs_fail(stats->status, "lcs_pcg_solve_noalloc: solve failed");
     }
+    return LCS_OK;
+}
+
+extern "C" int lcs_pcg_solve_batch(lcs_pcg* P, uint32_t n_scenes, const uint32_t* row_offsets, const uint32_t* host_row_end,
+                                   const uint32_t* active, const float* diag, const lcs_bsr* A, const lcs_bsr* B,
+                                   const float* b, float* x, const lcs_pcg_opts* opts, lcs_pcg_stats* stats_per_scene,
+                                   int cluster, lcs_stream stream)
+{
+    if (!P || !row_offsets || !host_row_end || !diag || !b || !x || !stats_per_scene || n_scenes == 0)
+        return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_batch: bad argument");
+    if (*host_row_end > P->n || (A && A->n_rows != P->n) || (B && B->n_rows != P->n))
+        return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_batch: row count mismatch");
+    if (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8 && cluster != 16)
+        return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_batch: cluster size must be 1, 2, 4, 8 or 16");
+    lcs_pcg_opts o = opts ? *opts : lcs_pcg_opts{100, 1e-4f, 1e-10f, 1, 0};
+    if (o.check_every <= 0) o.check_every = 1;
+    const size_t chunks = (size_t)(*host_row_end >> 8) + n_scenes + 1;
+    if (chunks > P->cpart_cap) {
+        if (P->cpart) cudaFree(P->cpart);
+        P->cpart = nullptr;
+        P->cpart_cap = 0;
+        LCS_CUDA_TRY(cudaMalloc((void**)&P->cpart, 4 * sizeof(double) * chunks));
+        P->cpart_cap = chunks;
+    }
+    BatchArgs a;
+    a.roff = row_offsets;
+    a.active = active;
+    a.diag = reinterpret_cast<const float4*>(diag);
+    a.A = to_bsr(A);
+    a.B = to_bsr(B);
+    a.b = reinterpret_cast<const float4*>(b);
+    a.x = reinterpret_cast<float4*>(x);
+    a.r = P->r; a.z = P->z; a.p = P->p; a.q = P->q; a.minv = P->minv;
+    a.cpart = P->cpart;
+    a.max_iter = o.max_iter;
+    a.rel_tol = o.rel_tol;
+    a.abs_rz_tol = o.abs_rz_tol;
+    a.check_every = o.check_every;
+    a.fp64 = (o.flags & LCS_PCG_FP64_DOTS) ? 1 : 0;
+    a.stats = stats_per_scene;
+    if (cluster == 16) LCS_CUDA_TRY(cudaFuncSetAttribute(k_pcg_batch, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(n_scenes * (uint32_t)cluster);
+    cfg.blockDim = dim3(kBatchThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = (cudaStream_t)stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    LCS_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_pcg_batch, a));
+    lcs_count_launch();
     return LCS_OK;
 }

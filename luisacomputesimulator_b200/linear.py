@@ -55,3 +55,17 @@ class ConjugateGradientSolver:
                                        C.byref(B_bsr) if B_bsr is not None else None, ptr(b), ptr(x), C.byref(o),
                                        C.byref(st), stream()), "pcg_solve")
         return dict(iterations=st.iterations, rel_residual=st.rel_residual, dot_rz=st.dot_rz, status=st.status)
+
+
+def solve_batch(solver, row_offsets, diag, A_bsr, B_bsr, b, x, stats, active=None, max_iter=100, rel_tol=1e-4,
+                abs_rz_tol=1e-10, check_every=1, fp64_dots=False, cluster=4):
+    """Independent per-scene Jacobi-PCG solves in one launch (lcs_pcg_solve_batch).  row_offsets: CUDA
+    int32 tensor of n_scenes + 1 offsets; stats: CUDA int32 tensor (n_scenes, 4) receiving lcs_pcg_stats."""
+    lib = A.load()
+    n_scenes = row_offsets.shape[0] - 1
+    end = C.c_uint32(int(row_offsets[-1].item()))
+    o = A.PcgOpts(max_iter, rel_tol, abs_rz_tol, check_every, A.LCS_PCG_FP64_DOTS if fp64_dots else 0)
+    A.check(lib.lcs_pcg_solve_batch(solver.h, n_scenes, ptr(row_offsets), C.byref(end), ptr(active), ptr(diag),
+                                    C.byref(A_bsr) if A_bsr is not None else None,
+                                    C.byref(B_bsr) if B_bsr is not None else None, ptr(b), ptr(x), C.byref(o),
+                                    ptr(stats), cluster, stream()), "lcs_pcg_solve_batch")

@@ -14,6 +14,54 @@ def _c(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
 
 
+def scene_desc(sc, keep, nonlinear_iters=3, pcg_max_iter=100, pcg_rel_tol=1e-4, pcg_abs_rz_tol=1e-10,
+               pcg_check_every=25, damping=2.0, use_floor=False, floor_y=0.0):
+    """lcs_scene_desc of a scene (host arrays appended to `keep`, which must outlive the call that reads it)."""
+    def arr(a, dtype):
+        a = _c(a, dtype)
+        keep.append(a)
+        return a.ctypes.data_as(C.c_void_p)
+
+    d = A.SceneDesc()
+    d.n_verts, d.n_faces, d.n_edges, d.n_bending = sc.num_verts, sc.faces.shape[0], sc.edges.shape[0], \
+        sc.bending.shape[0]
+    d.x = arr(sc.x, np.float32)
+    d.v = None
+    d.faces = arr(sc.faces, np.uint32)
+    d.edges = arr(sc.edges, np.uint32)
+    d.bending = arr(sc.bending, np.uint32)
+    d.bending_Q = arr(sc.bending_Q.reshape(-1, 16), np.float32)
+    d.rest_len = arr(sc.rest_len, np.float32)
+    d.vert_area = arr(sc.vert_area, np.float32)
+    d.face_area = arr(sc.face_area, np.float32)
+    d.edge_area = arr(sc.edge_area, np.float32)
+    d.mass = arr(sc.mass, np.float32)
+    d.d_hat = arr(sc.d_hat, np.float32)
+    d.offset = arr(sc.offset, np.float32)
+    d.body = arr(sc.body, np.uint32)
+    d.pinned = arr(sc.pinned, np.uint8)
+    groups = np.full(sc.num_verts, -1, np.int8)
+    anim = np.zeros((max(len(sc.anims), 1), 8), np.float32)
+    for gi, (vids, center, axis, omega) in enumerate(sc.anims):
+        groups[vids] = gi
+        ax = np.asarray(axis, np.float64)
+        ax = ax / np.linalg.norm(ax)
+        anim[gi, :3] = center
+        anim[gi, 3:6] = ax
+        anim[gi, 6] = omega
+    d.anim_group = arr(groups, np.int8)
+    d.n_anim = len(sc.anims)
+    d.anim = arr(anim, np.float32)
+    d.dt = sc.dt
+    d.gravity = (C.c_float * 3)(*sc.gravity)
+    d.kappa, d.spring_k, d.bending_k, d.dirichlet, d.damping = sc.kappa, sc.spring_k, sc.bending_k, \
+        sc.dirichlet, damping
+    d.use_floor, d.floor_y = int(use_floor), floor_y
+    d.nonlinear_iters, d.pcg_max_iter = nonlinear_iters, pcg_max_iter
+    d.pcg_rel_tol, d.pcg_abs_rz_tol, d.pcg_check_every = pcg_rel_tol, pcg_abs_rz_tol, pcg_check_every
+    return d
+
+
 class NewtonSolver:
     """One scene, state resident on the device.
 
@@ -30,48 +78,8 @@ class NewtonSolver:
         sc = scene
         self._keep = []
 
-        def arr(a, dtype):
-            a = _c(a, dtype)
-            self._keep.append(a)
-            return a.ctypes.data_as(C.c_void_p)
-
-        d = A.SceneDesc()
-        d.n_verts, d.n_faces, d.n_edges, d.n_bending = sc.num_verts, sc.faces.shape[0], sc.edges.shape[0], \
-            sc.bending.shape[0]
-        d.x = arr(sc.x, np.float32)
-        d.v = None
-        d.faces = arr(sc.faces, np.uint32)
-        d.edges = arr(sc.edges, np.uint32)
-        d.bending = arr(sc.bending, np.uint32)
-        d.bending_Q = arr(sc.bending_Q.reshape(-1, 16), np.float32)
-        d.rest_len = arr(sc.rest_len, np.float32)
-        d.vert_area = arr(sc.vert_area, np.float32)
-        d.face_area = arr(sc.face_area, np.float32)
-        d.edge_area = arr(sc.edge_area, np.float32)
-        d.mass = arr(sc.mass, np.float32)
-        d.d_hat = arr(sc.d_hat, np.float32)
-        d.offset = arr(sc.offset, np.float32)
-        d.body = arr(sc.body, np.uint32)
-        d.pinned = arr(sc.pinned, np.uint8)
-        groups = np.full(sc.num_verts, -1, np.int8)
-        anim = np.zeros((max(len(sc.anims), 1), 8), np.float32)
-        for gi, (vids, center, axis, omega) in enumerate(sc.anims):
-            groups[vids] = gi
-            ax = np.asarray(axis, np.float64)
-            ax = ax / np.linalg.norm(ax)
-            anim[gi, :3] = center
-            anim[gi, 3:6] = ax
-            anim[gi, 6] = omega
-        d.anim_group = arr(groups, np.int8)
-        d.n_anim = len(sc.anims)
-        d.anim = arr(anim, np.float32)
-        d.dt = sc.dt
-        d.gravity = (C.c_float * 3)(*sc.gravity)
-        d.kappa, d.spring_k, d.bending_k, d.dirichlet, d.damping = sc.kappa, sc.spring_k, sc.bending_k, \
-            sc.dirichlet, damping
-        d.use_floor, d.floor_y = int(use_floor), floor_y
-        d.nonlinear_iters, d.pcg_max_iter = nonlinear_iters, pcg_max_iter
-        d.pcg_rel_tol, d.pcg_abs_rz_tol, d.pcg_check_every = pcg_rel_tol, pcg_abs_rz_tol, pcg_check_every
+        d = scene_desc(sc, self._keep, nonlinear_iters, pcg_max_iter, pcg_rel_tol, pcg_abs_rz_tol,
+                       pcg_check_every, damping, use_floor, floor_y)
         self.desc = d
         flags = (A.LCS_NEWTON_PLAIN if plain else 0) | (A.LCS_NEWTON_FP64 if fp64 else 0) | \
             (A.LCS_NEWTON_PROFILE if profile else 0) | (A.LCS_NEWTON_PCG_PIPELINED if pipelined else 0)
@@ -135,3 +143,60 @@ class NewtonSolver:
         v = [C.c_uint32() for _ in range(4)]
         A.check(self.lib.lcs_newton_counts(self.h, *[C.byref(a) for a in v]), "lcs_newton_counts")
         return dict(nnz_material=v[0].value, cap_vf=v[1].value, cap_ee=v[2].value, cap_pairs=v[3].value)
+
+
+class NewtonBatch:
+    """Many independent scenes stepped together (lcs_newton_create_batch): one set of launches per
+    Newton phase for all scenes, per-scene trees, step bounds and PCG (one thread-block cluster of
+    `cluster` CTAs per scene).  A scene's trajectory does not depend on the other scenes."""
+
+    def __init__(self, scenes, fp64=False, profile=False, cluster=4, nonlinear_iters=3, pcg_max_iter=100,
+                 pcg_rel_tol=1e-4, pcg_abs_rz_tol=1e-10, damping=2.0, stream=None):
+        self.lib = A.load()
+        self.scenes = list(scenes)
+        keep = []
+        descs = (A.SceneDesc * len(self.scenes))()
+        for k, sc in enumerate(self.scenes):
+            descs[k] = scene_desc(sc, keep, nonlinear_iters, pcg_max_iter, pcg_rel_tol, pcg_abs_rz_tol, 1, damping)
+        flags = (A.LCS_NEWTON_FP64 if fp64 else 0) | (A.LCS_NEWTON_PROFILE if profile else 0)
+        s = C.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+        h = C.c_void_p()
+        A.check(self.lib.lcs_newton_create_batch(descs, len(self.scenes), flags, s, int(cluster), C.byref(h)),
+                "lcs_newton_create_batch")
+        self.h = h
+        self.stats = A.NewtonStats()
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.lcs_newton_destroy(self.h)
+            self.h = None
+
+    def step(self):
+        A.check(self.lib.lcs_newton_step(self.h, C.byref(self.stats)), "lcs_newton_step")
+        return self.stats
+
+    def scene_stats(self, k):
+        st = A.NewtonStats()
+        A.check(self.lib.lcs_newton_scene_stats(self.h, k, C.byref(st)), "lcs_newton_scene_stats")
+        return st
+
+    def positions(self, k):
+        out = np.zeros((self.scenes[k].num_verts, 4), np.float32)
+        A.check(self.lib.lcs_newton_download_scene(self.h, k, out.ctypes.data_as(C.c_void_p), None),
+                "lcs_newton_download_scene")
+        return out
+
+    def velocities(self, k):
+        out = np.zeros((self.scenes[k].num_verts, 4), np.float32)
+        A.check(self.lib.lcs_newton_download_scene(self.h, k, None, out.ctypes.data_as(C.c_void_p)),
+                "lcs_newton_download_scene")
+        return out
+
+    def profile(self):
+        ms = (C.c_double * 9)()
+        n = (C.c_int32 * 9)()
+        A.check(self.lib.lcs_newton_profile(self.h, ms, n, 9), "lcs_newton_profile")
+        return {A.PHASES[i]: (ms[i], n[i]) for i in range(9)}
+
+    def reset_profile(self):
+        A.check(self.lib.lcs_newton_reset_profile(self.h), "lcs_newton_reset_profile")
