@@ -46,6 +46,14 @@ def args_():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--n-around", type=int, default=300)
     p.add_argument("--n-along", type=int, default=296)
+    p.add_argument("--workload", choices=["tube", "batch", "serve"], default="tube",
+                   help="tube: the headline Newton iters/s line; batch: batched drape solves/s (256 scenes); "
+                        "serve: Poisson drape requests, p50/p99 latency and solves/s")
+    p.add_argument("--n-scenes", type=int, default=256, help="batch workload: scenes")
+    p.add_argument("--solve-steps", type=int, default=20, help="time steps of one drape solve")
+    p.add_argument("--plain-sample", type=int, default=16, help="requests/scenes timed through the plain loop")
+    p.add_argument("--requests", type=int, default=64, help="serve workload: requests")
+    p.add_argument("--rate", type=float, default=200.0, help="serve workload: Poisson arrival rate (1/s)")
     return p.parse_args()
 
 
@@ -327,8 +335,172 @@ def run_ours(a):
     _ = np
 
 
+# ------------------------------------------------------------------------- batching / serving
+def _log_uniform_sizes(n, lo, hi, seed):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return [int(round(v)) for v in np.exp(rng.uniform(np.log(lo), np.log(hi), n))]
+
+
+def _plain_service(scene, steps, plain=True):
+    """Wall time of one drape solve through the one-scene-at-a-time loop (create, steps, read back)."""
+    import torch
+    from luisacomputesimulator_b200.newton import NewtonSolver
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    s = NewtonSolver(scene, plain=plain)
+    for _ in range(steps):
+        s.step()
+    s.positions()
+    del s
+    return time.perf_counter() - t
+
+
+def _stratified(items, key, k):
+    order = sorted(range(len(items)), key=lambda i: key(items[i]))
+    if k >= len(items):
+        return order
+    return [order[int((j + 0.5) * len(items) / k)] for j in range(k)]
+
+
+def run_batch(a):
+    """Batching form: n_scenes cloth-on-sphere drapes (vertex counts log-uniform in [1K, 32K], seeds 0..n-1)
+    stepped together for solve_steps time steps; against the plain one-scene-at-a-time loop."""
+    import numpy as np
+    import torch
+    from luisacomputesimulator_b200 import _capi, scenes
+    from luisacomputesimulator_b200.newton import NewtonBatch
+    torch.cuda.set_device(0)
+    lib = _capi.load()
+    _capi.check(lib.lcs_device_check(0), "device check")
+    sizes = _log_uniform_sizes(a.n_scenes, 1000, 32000, seed=0)
+    scs = [scenes.random_cloth_scene(v, k, "sphere") for k, v in enumerate(sizes)]
+    V = sum(sc.num_verts for sc in scs)
+    warm = NewtonBatch(scs[:4])  # warm-up: first-call set-up paths
+    for _ in range(max(a.warmup, 1)):
+        warm.step()
+    del warm
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter()
+    batch = NewtonBatch(scs)
+    t_create = time.perf_counter() - t_e2e
+    launches0 = lib.lcs_launch_count()
+    newton = 0
+    stream = torch.cuda.current_stream()
+    with Clocks(0) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t_steps = time.perf_counter()
+        for _ in range(a.solve_steps):
+            st = batch.step()
+            newton += st.newton_iters
+        e1.record(stream)
+        e1.synchronize()
+        t_steps = time.perf_counter() - t_steps
+    launches = lib.lcs_launch_count() - launches0
+    clocks = clk.summary()
+    xs = [batch.positions(k) for k in range(len(scs))]
+    t_e2e = time.perf_counter() - t_e2e
+    assert all(np.isfinite(x).all() for x in xs)
+    del batch
+    ms = e0.elapsed_time(e1)
+    sample = _stratified(scs, lambda sc: sc.num_verts, a.plain_sample)
+    plain_t = [_plain_service(scs[i], a.solve_steps, plain=True) for i in sample]
+    fused_t = [_plain_service(scs[i], a.solve_steps, plain=False) for i in sample]
+    value = len(scs) / (ms / 1e3)
+    line = {
+        "metric": f"batched drape solves/s ({len(scs)} cloth-on-sphere scenes, 1K-32K verts, {a.solve_steps} steps)",
+        "value": value, "unit": "solves/s", "n_gpus": 1, "steps": a.solve_steps, "warmup": max(a.warmup, 1),
+        "ms_per_step": ms / a.solve_steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded cloth grids over icospheres)", "impl": "ours",
+        "config": {"workload": f"C4 batching: {len(scs)} scenes, {V} vertices in all, sizes log-uniform [1K, 32K] "
+                               "(seed 0), scene k seeded k, dt 1/60, kappa 1e7, 3 Newton/step, PCG <=100 it rel 1e-4; "
+                               "the 16 affine-box scenes are not run (affine bodies not built)",
+                   "scenes": len(scs), "verts": V, "pcg_cluster": 4},
+        "e2e": {"value": len(scs) / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": 16 * V, "includes": "batch creation (host upload), all steps, read-back"},
+        "gpu_launches": int(launches), "newton_iters": newton, "create_s": t_create,
+        "plain_loop": {"value": 1.0 / float(np.mean(plain_t)), "unit": "solves/s", "sample": len(sample),
+                       "kind": "plain one-scene-at-a-time GPU loop (reference dispatch structure), create + steps + "
+                               "read-back per scene, size-stratified sample"},
+        "fused_single_loop": {"value": 1.0 / float(np.mean(fused_t)), "unit": "solves/s", "sample": len(sample)},
+        "clocks": clocks,
+    }
+    line["ratio_vs_plain"] = line["value"] / line["plain_loop"]["value"]
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(a):
+    """Serving form: Poisson drape requests (2K-64K verts, sphere or box collider, solve_steps steps) through
+    the continuous-batching server; p50/p99 latency and solves/s against the one-at-a-time plain loop."""
+    import numpy as np
+    import torch
+    from luisacomputesimulator_b200 import _capi
+    from luisacomputesimulator_b200.newton import NewtonBatch
+    from luisacomputesimulator_b200.serving import Server, fifo_latencies, poisson_drapes
+    torch.cuda.set_device(0)
+    lib = _capi.load()
+    _capi.check(lib.lcs_device_check(0), "device check")
+    warm = poisson_drapes(3, a.rate, seed=99, v_max=4000, steps=2)
+    Server(max_batches=2).run(warm)
+    reqs = poisson_drapes(a.requests, a.rate, seed=0, steps=a.solve_steps)
+    server = Server()
+    launches0 = lib.lcs_launch_count()
+    with Clocks(0) as clk:
+        t0 = time.perf_counter()
+        done = [r for r in server.run(reqs) if not r.rejected and r.done >= 0]
+        wall = time.perf_counter() - t0
+    launches = lib.lcs_launch_count() - launches0
+    clocks = clk.summary()
+    lat = np.array([r.latency for r in done])
+    span = max(r.done for r in done) - min(r.arrival for r in done)
+    # alone == in the mix: two requests re-run alone through the same batched solver
+    dev = []
+    for r in done[:2]:
+        b = NewtonBatch([r.scene])
+        for _ in range(r.steps):
+            b.step()
+        xa = b.positions(0)
+        scale = max(float(np.abs(xa[:, :3] - r.scene.x[:, :3]).max()), 1e-12)
+        dev.append(float(np.abs(xa[:, :3] - r.x[:, :3]).max() / scale))
+        del b
+    sample = _stratified(done, lambda r: r.scene.num_verts, min(a.plain_sample, len(done)))
+    service = {i: _plain_service(done[i].scene, a.solve_steps, plain=True) for i in sample}
+    mean_service = float(np.mean(list(service.values())))
+    # one-at-a-time FIFO over the same arrivals; requests outside the timed sample get the sample mean
+    plain_lat = fifo_latencies([r.arrival for r in done], [service.get(i, mean_service) for i in range(len(done))])
+    line = {
+        "metric": f"served drape solves/s ({len(done)} Poisson requests at {a.rate:g}/s, 2K-64K verts)",
+        "value": len(done) / span, "unit": "solves/s", "n_gpus": 1, "steps": a.solve_steps, "warmup": 1,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded cloth grids over icospheres / boxes)", "impl": "ours",
+        "config": {"workload": f"C5 serving: {len(done)} requests, Poisson {a.rate:g}/s (seed 0), cloth 2K-64K verts "
+                               f"log-uniform over a sphere or box, {a.solve_steps} steps each, admission by free HBM "
+                               "against a 150 GB budget, up to 4 batches in flight", "requests": len(done)},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "max": float(lat.max())},
+        "batches": server.launched, "wall_s": wall, "gpu_launches": int(launches),
+        "alone_vs_mix_max_rel_dev": max(dev) if dev else None,
+        "plain_loop": {"value": 1.0 / mean_service, "unit": "solves/s",
+                       "latency_s": {"p50": float(np.percentile(plain_lat, 50)),
+                                     "p99": float(np.percentile(plain_lat, 99))},
+                       "sample": len(sample),
+                       "kind": "plain one-at-a-time GPU loop; service times measured on a size-stratified sample, "
+                               "FIFO queue over the same arrivals"},
+        "e2e": {"value": len(done) / span, "unit": "solves/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "includes": "request admission, host upload, all steps, read-back of every request"},
+        "clocks": clocks,
+    }
+    line["ratio_vs_plain"] = line["value"] / line["plain_loop"]["value"]
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = args_()
+    if a.workload == "batch" and a.impl == "ours":
+        return run_batch(a)
+    if a.workload == "serve" and a.impl == "ours":
+        return run_serve(a)
     if a.impl == "reference":
         run_reference(a)
     else:
