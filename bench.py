@@ -51,7 +51,7 @@ def args_():
                         "serve: Poisson drape requests, p50/p99 latency and solves/s")
     p.add_argument("--n-scenes", type=int, default=256, help="batch workload: scenes")
     p.add_argument("--solve-steps", type=int, default=20, help="time steps of one drape solve")
-    p.add_argument("--plain-sample", type=int, default=16, help="requests/scenes timed through the plain loop")
+    p.add_argument("--plain-sample", type=int, default=32, help="requests/scenes timed through the plain loop")
     p.add_argument("--requests", type=int, default=64, help="serve workload: requests")
     p.add_argument("--rate", type=float, default=200.0, help="serve workload: Poisson arrival rate (1/s)")
     return p.parse_args()
@@ -454,16 +454,20 @@ def run_serve(a):
     clocks = clk.summary()
     lat = np.array([r.latency for r in done])
     span = max(r.done for r in done) - min(r.arrival for r in done)
-    # alone == in the mix: two requests re-run alone through the same batched solver
-    dev = []
+    # alone == in the mix: two requests re-run alone through the same batched solver, and one of them alone
+    # twice (the run-to-run spread that float atomics alone produce over the solve)
+    dev, rerun = [], []
     for r in done[:2]:
-        b = NewtonBatch([r.scene])
-        for _ in range(r.steps):
-            b.step()
-        xa = b.positions(0)
-        scale = max(float(np.abs(xa[:, :3] - r.scene.x[:, :3]).max()), 1e-12)
-        dev.append(float(np.abs(xa[:, :3] - r.x[:, :3]).max() / scale))
-        del b
+        xs = []
+        for _ in range(2):
+            b = NewtonBatch([r.scene])
+            for _ in range(r.steps):
+                b.step()
+            xs.append(b.positions(0))
+            del b
+        scale = max(float(np.abs(xs[0][:, :3] - r.scene.x[:, :3]).max()), 1e-12)
+        dev.append(float(np.abs(xs[0][:, :3] - r.x[:, :3]).max() / scale))
+        rerun.append(float(np.abs(xs[0][:, :3] - xs[1][:, :3]).max() / scale))
     sample = _stratified(done, lambda r: r.scene.num_verts, min(a.plain_sample, len(done)))
     service = {i: _plain_service(done[i].scene, a.solve_steps, plain=True) for i in sample}
     mean_service = float(np.mean(list(service.values())))
@@ -481,6 +485,7 @@ def run_serve(a):
                       "max": float(lat.max())},
         "batches": server.launched, "wall_s": wall, "gpu_launches": int(launches),
         "alone_vs_mix_max_rel_dev": max(dev) if dev else None,
+        "alone_vs_alone_max_rel_dev": max(rerun) if rerun else None,
         "plain_loop": {"value": 1.0 / mean_service, "unit": "solves/s",
                        "latency_s": {"p50": float(np.percentile(plain_lat, 50)),
                                      "p99": float(np.percentile(plain_lat, 99))},

@@ -24,6 +24,7 @@
 #include <new>
 #include <utility>
 #include <chrono>
+#include <thread>
 #include <vector>
 
 #include "lcs_common.cuh"
@@ -500,34 +501,86 @@ int alloc_contact(lcs_newton* h)
 
 // material off-diagonal pattern: springs (both directions) + every ordered pair of each
 // bending stencil; slots of each contribution found by binary search in the sorted rows
+// runs f(begin, end) over [0, n) on the host's cores
+template <typename F>
+void parallel_ranges(size_t n, F f)
+{
+    unsigned t = std::thread::hardware_concurrency();
+    t = t ? std::min(t, 32u) : 4u;
+    if (n < 65536 || t == 1) {
+        f((size_t)0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const size_t chunk = (n + t - 1) / t;
+    for (unsigned k = 0; k < t; ++k) {
+        const size_t b = k * chunk, e = std::min(n, b + chunk);
+        if (b < e) pool.emplace_back(f, b, e);
+    }
+    for (auto& th : pool) th.join();
+}
+
 int build_material_pattern(lcs_newton* h, const lcs_scene_desc* d)
 {
-    std::vector<uint64_t> keys;
-    keys.reserve(2 * (size_t)h->E + 12 * (size_t)h->B);
-    for (uint32_t e = 0; e < h->E; ++e) {
-        const uint64_t a = d->edges[2 * e], c = d->edges[2 * e + 1];
-        keys.push_back(a << 32 | c);
-        keys.push_back(c << 32 | a);
+    // contributions: key k < 2E is spring k/2 (a->c, then c->a); the rest are the ordered pairs
+    // (i, j), i != j, of each bending stencil, 12 per stencil
+    const size_t KE = 2 * (size_t)h->E, K = KE + 12 * (size_t)h->B;
+    auto key_rc = [&](size_t k, uint32_t& r, uint32_t& c) {
+        if (k < KE) {
+            const uint32_t* e = d->edges + 2 * (k >> 1);
+            r = e[k & 1];
+            c = e[(k & 1) ^ 1];
+        } else {
+            const size_t q = k - KE, st = q / 12, m = q % 12, i = m / 3, jj = m % 3, j = jj < i ? jj : jj + 1;
+            r = d->bending[4 * st + i];
+            c = d->bending[4 * st + j];
+        }
+    };
+    // bucket the columns by row (counting sort), then sort and de-duplicate each row
+    std::vector<uint32_t> start(h->V + 1, 0);
+    for (size_t k = 0; k < K; ++k) {
+        uint32_t r, c;
+        key_rc(k, r, c);
+        start[r + 1]++;
     }
-    for (uint32_t s = 0; s < h->B; ++s)
-        for (int i = 0; i < 4; ++i)
-            for (int j = 0; j < 4; ++j)
-                if (i != j) keys.push_back((uint64_t)d->bending[4 * s + i] << 32 | d->bending[4 * s + j]);
-    std::vector<uint64_t> uniq(keys);
-    std::sort(uniq.begin(), uniq.end());
-    uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
-    h->nnz_mat = (uint32_t)uniq.size();
-    std::vector<uint32_t> rp(h->V + 1, 0), col(uniq.size());
-    for (size_t k = 0; k < uniq.size(); ++k) {
-        rp[(uniq[k] >> 32) + 1]++;
-        col[k] = (uint32_t)(uniq[k] & 0xFFFFFFFFu);
+    for (uint32_t r = 0; r < h->V; ++r) start[r + 1] += start[r];
+    std::vector<uint32_t> bucket(K ? K : 1), cursor(start.begin(), start.end() - 1);
+    for (size_t k = 0; k < K; ++k) {
+        uint32_t r, c;
+        key_rc(k, r, c);
+        bucket[cursor[r]++] = c;
     }
-    for (uint32_t r = 0; r < h->V; ++r) rp[r + 1] += rp[r];
-    auto slot_of = [&](uint64_t key) { return (uint32_t)(std::lower_bound(uniq.begin(), uniq.end(), key) - uniq.begin()); };
+    std::vector<uint32_t> ucount(h->V, 0);
+    parallel_ranges(h->V, [&](size_t rb, size_t re) {
+        for (size_t r = rb; r < re; ++r) {
+            uint32_t* b0 = bucket.data() + start[r];
+            uint32_t* b1 = bucket.data() + start[r + 1];
+            std::sort(b0, b1);
+            ucount[r] = (uint32_t)(std::unique(b0, b1) - b0);
+        }
+    });
+    std::vector<uint32_t> rp(h->V + 1, 0);
+    for (uint32_t r = 0; r < h->V; ++r) rp[r + 1] = rp[r] + ucount[r];
+    const size_t nnz = rp[h->V];
+    h->nnz_mat = (uint32_t)nnz;
+    std::vector<uint32_t> col(nnz ? nnz : 1);
+    parallel_ranges(h->V, [&](size_t rb, size_t re) {
+        for (size_t r = rb; r < re; ++r) std::copy(bucket.begin() + start[r], bucket.begin() + start[r] + ucount[r], col.begin() + rp[r]);
+    });
+    // CSR slot of contribution k: its column's position in its row (rows hold about a dozen blocks)
+    auto slot_of = [&](size_t k) -> uint32_t {
+        uint32_t r, c;
+        key_rc(k, r, c);
+        const uint32_t* b = col.data() + rp[r];
+        const uint32_t n = rp[r + 1] - rp[r];
+        uint32_t j = 0;
+        while (j < n && b[j] != c) ++j;
+        return rp[r] + j;
+    };
     // block base offset into mat_val for CSR block j: CSR 9 j (components contiguous) or, in the
     // SELL-32 layout with 4-slot groups, ((g * 9) * 32 + lane) * 4 + slot % 4 for group g = slot / 4
     // (components 128 floats apart; the row-resident PCG reads a group with float4 loads)
-    std::vector<uint32_t> base(uniq.size());
+    std::vector<uint32_t> base(nnz ? nnz : 1);
     std::vector<uint32_t> sell_ptr, sell_col;
     if (h->sell) {
         const uint32_t ns = (h->V + 31) / 32;
@@ -551,12 +604,17 @@ int build_material_pattern(lcs_newton* h, const lcs_scene_desc* d)
             }
         h->sell_vals = 9ull * 32 * sell_ptr[ns];
     } else {
-        for (size_t j = 0; j < uniq.size(); ++j) base[j] = (uint32_t)(9 * j);
-        h->sell_vals = 9ull * uniq.size();
+        for (size_t j = 0; j < nnz; ++j) base[j] = (uint32_t)(9 * j);
+        h->sell_vals = 9ull * nnz;
     }
-    std::vector<uint32_t> ss(2 * (size_t)h->E), bs(12 * (size_t)h->B);
-    for (size_t k = 0; k < 2 * (size_t)h->E; ++k) ss[k] = base[slot_of(keys[k])];
-    for (size_t k = 0; k < 12 * (size_t)h->B; ++k) bs[k] = base[slot_of(keys[2 * (size_t)h->E + k])];
+    std::vector<uint32_t> ss(KE ? KE : 1), bs(K - KE ? K - KE : 1);
+    parallel_ranges(K, [&](size_t kb, size_t ke) {
+        for (size_t k = kb; k < ke; ++k) {
+            const uint32_t v = base[slot_of(k)];
+            if (k < KE) ss[k] = v;
+            else bs[k - KE] = v;
+        }
+    });
     if (upload(h->mat_rp, rp.data(), rp.size()) != cudaSuccess || upload(h->mat_col, col.data(), col.size()) != cudaSuccess ||
         upload(h->spring_slots, ss.data(), ss.size()) != cudaSuccess ||
         upload(h->bend_slots, bs.data(), bs.size()) != cudaSuccess || dalloc(h->mat_val, h->sell_vals) != cudaSuccess)

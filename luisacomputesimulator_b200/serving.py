@@ -48,7 +48,7 @@ class Server:
     max_batch_verts: vertices in one batch."""
 
     def __init__(self, budget_bytes=150e9, max_batches=4, max_batch_verts=1_500_000, cluster=4,
-                 bytes_per_vertex=4096.0, device=0, solve=None, free_bytes=None):
+                 bytes_per_vertex=4096.0, device=0, solve=None, free_bytes=None, gather_s=0.1):
         self.budget = float(budget_bytes)
         self.max_batches = int(max_batches)
         self.max_batch_verts = int(max_batch_verts)
@@ -56,6 +56,9 @@ class Server:
         self.bpv = float(bytes_per_vertex)  # refined from measurements
         self.device = device
         # the batch runner and the free-memory query (replaceable, e.g. by fakes in host-only tests)
+        # admission: requests that arrive within gather_s of the oldest queued one are batched with it,
+        # and the queue is shared evenly among the free batch slots
+        self.gather_s = float(gather_s)
         self.solve = solve or self._solve_gpu
         self.free_bytes = free_bytes or (lambda: torch.cuda.mem_get_info()[0])
         self.lock = threading.Lock()
@@ -117,11 +120,19 @@ class Server:
                     can = self.active < self.max_batches
                     free = self.free_bytes()
                     room = min(self.budget - self.reserved, free * 0.9)
-                if can:
+                waited = now - queue[0].arrival
+                more = i < len(pending) and pending[i].arrival - queue[0].arrival <= self.gather_s
+                if can and (waited >= self.gather_s or not more):
+                    with self.lock:
+                        free_slots = max(self.max_batches - self.active, 1)
+                    share = -(-sum(r.scene.num_verts for r in queue) // free_slots)  # ceil
+                    cap = min(self.max_batch_verts, max(share, 1))
                     take, verts = [], 0
                     for r in queue:  # admit in arrival order while the memory budget allows
                         est = self.bpv * r.scene.num_verts
-                        if verts + r.scene.num_verts > self.max_batch_verts or self._estimate(take) + est > room:
+                        if take and (verts + r.scene.num_verts > cap or self._estimate(take) + est > room):
+                            break
+                        if not take and self._estimate(take) + est > room:
                             break
                         take.append(r)
                         verts += r.scene.num_verts

@@ -77,3 +77,13 @@ def test_memory_budget_limits_concurrency_and_rejects_oversize():
 def test_fifo_latency_model():
     lat = fifo_latencies([0.0, 0.1, 0.2, 5.0], [1.0, 1.0, 1.0, 1.0])
     np.testing.assert_allclose(lat, [1.0, 1.9, 2.8, 1.0])
+
+
+def test_burst_is_shared_among_free_slots():
+    gpu = FakeGpu(per_vert_s=1e-6)
+    reqs = [_req(k, 2000, 0.001 * k) for k in range(8)]
+    srv = Server(max_batches=4, gather_s=0.05, solve=gpu.solve, free_bytes=lambda: 1 << 40)
+    srv.run(reqs)
+    # the eight requests arrive within the gather window and are spread over the four slots
+    assert len(gpu.batches) == 4 and all(len(b) == 2 for b in gpu.batches)
+    assert gpu.peak == 4
