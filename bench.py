@@ -483,7 +483,8 @@ def run_serve(a):
                                "against a 150 GB budget, up to 4 batches in flight", "requests": len(done)},
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                       "max": float(lat.max())},
-        "batches": server.launched, "wall_s": wall, "gpu_launches": int(launches),
+        "batches": [{k: round(v, 3) if isinstance(v, float) else v for k, v in b.items()} for b in server.log],
+        "wall_s": wall, "gpu_launches": int(launches),
         "alone_vs_mix_max_rel_dev": max(dev) if dev else None,
         "alone_vs_alone_max_rel_dev": max(rerun) if rerun else None,
         "plain_loop": {"value": 1.0 / mean_service, "unit": "solves/s",

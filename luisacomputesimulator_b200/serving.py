@@ -56,8 +56,7 @@ class Server:
         self.bpv = float(bytes_per_vertex)  # refined from measurements
         self.device = device
         # the batch runner and the free-memory query (replaceable, e.g. by fakes in host-only tests)
-        # admission: requests that arrive within gather_s of the oldest queued one are batched with it,
-        # and the queue is shared evenly among the free batch slots
+        # admission: requests that arrive within gather_s of the oldest queued one are batched with it
         self.gather_s = float(gather_s)
         self.solve = solve or self._solve_gpu
         self.free_bytes = free_bytes or (lambda: torch.cuda.mem_get_info()[0])
@@ -67,6 +66,7 @@ class Server:
         self.peak_active = 0
         self.peak_reserved = 0.0
         self.launched = []
+        self.log = []
 
     def _estimate(self, reqs):
         return self.bpv * sum(r.scene.num_verts for r in reqs)
@@ -91,8 +91,11 @@ class Server:
 
     def _run_batch(self, reqs, t0, est):
         try:
+            start = time.perf_counter() - t0
             xs = self.solve(reqs)
             now = time.perf_counter() - t0
+            with self.lock:
+                self.log.append(dict(start=start, done=now, n=len(reqs), verts=sum(r.scene.num_verts for r in reqs)))
             for r, x in zip(reqs, xs):
                 r.x, r.done, r.batch_size = x, now, len(reqs)
         finally:
@@ -123,10 +126,7 @@ class Server:
                 waited = now - queue[0].arrival
                 more = i < len(pending) and pending[i].arrival - queue[0].arrival <= self.gather_s
                 if can and (waited >= self.gather_s or not more):
-                    with self.lock:
-                        free_slots = max(self.max_batches - self.active, 1)
-                    share = -(-sum(r.scene.num_verts for r in queue) // free_slots)  # ceil
-                    cap = min(self.max_batch_verts, max(share, 1))
+                    cap = self.max_batch_verts
                     take, verts = [], 0
                     for r in queue:  # admit in arrival order while the memory budget allows
                         est = self.bpv * r.scene.num_verts

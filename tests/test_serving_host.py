@@ -56,7 +56,7 @@ def test_all_requests_served_in_arrival_order_within_limits():
 def test_late_arrivals_join_while_others_run():
     gpu = FakeGpu(per_vert_s=2e-5)  # ~0.2 s per 10K-vertex batch
     reqs = [_req(0, 10_000, 0.0), _req(1, 1000, 0.05), _req(2, 1000, 0.06)]
-    srv = Server(max_batches=2, solve=gpu.solve, free_bytes=lambda: 1 << 40)
+    srv = Server(max_batches=2, gather_s=0.01, solve=gpu.solve, free_bytes=lambda: 1 << 40)
     out = srv.run(reqs)
     # request 0 runs alone; 1 and 2 arrive while it runs and are admitted before it finishes
     assert gpu.batches[0] == [0]
@@ -79,11 +79,11 @@ def test_fifo_latency_model():
     np.testing.assert_allclose(lat, [1.0, 1.9, 2.8, 1.0])
 
 
-def test_burst_is_shared_among_free_slots():
+def test_burst_within_gather_window_is_one_batch():
     gpu = FakeGpu(per_vert_s=1e-6)
     reqs = [_req(k, 2000, 0.001 * k) for k in range(8)]
     srv = Server(max_batches=4, gather_s=0.05, solve=gpu.solve, free_bytes=lambda: 1 << 40)
     srv.run(reqs)
-    # the eight requests arrive within the gather window and are spread over the four slots
-    assert len(gpu.batches) == 4 and all(len(b) == 2 for b in gpu.batches)
-    assert gpu.peak == 4
+    # the eight requests arrive within the gather window of the first one and run as one batch
+    assert gpu.batches == [list(range(8))]
+    assert len(srv.log) == 1 and srv.log[0]["n"] == 8
