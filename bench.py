@@ -54,6 +54,9 @@ def args_():
     p.add_argument("--plain-sample", type=int, default=32, help="requests/scenes timed through the plain loop")
     p.add_argument("--requests", type=int, default=64, help="serve workload: requests")
     p.add_argument("--rate", type=float, default=200.0, help="serve workload: Poisson arrival rate (1/s)")
+    p.add_argument("--max-batches", type=int, default=4, help="serve workload: batches in flight")
+    p.add_argument("--gather", type=float, default=0.1, help="serve workload: admission gather window (s)")
+    p.add_argument("--no-plain", action="store_true", help="batch/serve: skip the plain-loop comparator")
     return p.parse_args()
 
 
@@ -416,7 +419,7 @@ def run_batch(a):
         "config": {"workload": f"C4 batching: {len(scs)} scenes, {V} vertices in all, sizes log-uniform [1K, 32K] "
                                "(seed 0), scene k seeded k, dt 1/60, kappa 1e7, 3 Newton/step, PCG <=100 it rel 1e-4; "
                                "the 16 affine-box scenes are not run (affine bodies not built)",
-                   "scenes": len(scs), "verts": V, "pcg_cluster": 4},
+                   "scenes": len(scs), "verts": V, "pcg_cluster": "auto"},
         "e2e": {"value": len(scs) / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": None,
                 "d2h_bytes_per_step": 16 * V, "includes": "batch creation (host upload), all steps, read-back"},
         "gpu_launches": int(launches), "newton_iters": newton, "create_s": t_create,
@@ -444,7 +447,7 @@ def run_serve(a):
     warm = poisson_drapes(3, a.rate, seed=99, v_max=4000, steps=2)
     Server(max_batches=2).run(warm)
     reqs = poisson_drapes(a.requests, a.rate, seed=0, steps=a.solve_steps)
-    server = Server()
+    server = Server(max_batches=a.max_batches, gather_s=a.gather)
     launches0 = lib.lcs_launch_count()
     with Clocks(0) as clk:
         t0 = time.perf_counter()
@@ -468,7 +471,7 @@ def run_serve(a):
         scale = max(float(np.abs(xs[0][:, :3] - r.scene.x[:, :3]).max()), 1e-12)
         dev.append(float(np.abs(xs[0][:, :3] - r.x[:, :3]).max() / scale))
         rerun.append(float(np.abs(xs[0][:, :3] - xs[1][:, :3]).max() / scale))
-    sample = _stratified(done, lambda r: r.scene.num_verts, min(a.plain_sample, len(done)))
+    sample = _stratified(done, lambda r: r.scene.num_verts, 1 if a.no_plain else min(a.plain_sample, len(done)))
     service = {i: _plain_service(done[i].scene, a.solve_steps, plain=True) for i in sample}
     mean_service = float(np.mean(list(service.values())))
     # one-at-a-time FIFO over the same arrivals; requests outside the timed sample get the sample mean
@@ -480,7 +483,8 @@ def run_serve(a):
         "data": "synthetic (seeded cloth grids over icospheres / boxes)", "impl": "ours",
         "config": {"workload": f"C5 serving: {len(done)} requests, Poisson {a.rate:g}/s (seed 0), cloth 2K-64K verts "
                                f"log-uniform over a sphere or box, {a.solve_steps} steps each, admission by free HBM "
-                               "against a 150 GB budget, up to 4 batches in flight", "requests": len(done)},
+                               f"against a 150 GB budget, up to {a.max_batches} batches in flight, gather window "
+                               f"{a.gather:g} s", "requests": len(done)},
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                       "max": float(lat.max())},
         "batches": [{k: round(v, 3) if isinstance(v, float) else v for k, v in b.items()} for b in server.log],

@@ -307,15 +307,16 @@ LCS_API int lcs_pcg_solve_noalloc(uint32_t n, const float* diag, const lcs_bsr* 
                                   lcs_stream stream);
 
 /* Batched scenes (no counterpart in the reference): n_scenes independent systems, scene s owning
- * block rows [row_offsets[s], row_offsets[s+1]) of one BSR pair (device array of n_scenes + 1;
- * *host_row_end = row_offsets[n_scenes], read on the host), solved in one launch with one
- * thread-block cluster of `cluster` CTAs (1, 2, 4, 8 or 16) per scene.  Each scene has its own
+ * block rows [row_offsets[s], row_offsets[s+1]) of one BSR pair (row_offsets: device array of
+ * n_scenes + 1; host_row_offsets: the same offsets in host memory), solved in one launch with one
+ * thread-block cluster of `cluster` CTAs (1, 2, 4, 8 or 16; 0 picks the smallest size that gives
+ * the largest scene at most 8 chunks of 256 rows per CTA) per scene.  Each scene has its own
  * alpha, beta and stop decision (the rules of lcs_pcg_solve); its result does not depend on
  * `cluster` or on the other scenes.  active: device flags per scene (0: skip, x = 0) or NULL.
  * stats_per_scene: device array of n_scenes.  Asynchronous; the handle must hold at least
- * *host_row_end rows. */
+ * host_row_offsets[n_scenes] rows. */
 LCS_API int lcs_pcg_solve_batch(lcs_pcg* p, uint32_t n_scenes, const uint32_t* row_offsets,
-                                const uint32_t* host_row_end, const uint32_t* active, const float* diag,
+                                const uint32_t* host_row_offsets, const uint32_t* active, const float* diag,
                                 const lcs_bsr* A, const lcs_bsr* B, const float* b, float* x,
                                 const lcs_pcg_opts* opts, lcs_pcg_stats* stats_per_scene, int cluster,
                                 lcs_stream stream);
@@ -386,7 +387,7 @@ LCS_API int lcs_newton_create(const lcs_scene_desc* desc, int flags, lcs_stream 
 /* Batched scenes (no counterpart in the reference): n_scenes independent scenes stepped
  * together, one set of launches per Newton phase for all of them (forests of per-scene LBVHs,
  * per-scene step bounds, per-scene PCG on thread-block clusters of pcg_cluster CTAs: 1, 2, 4, 8
- * or 16).  Every scene runs its own Newton loop (its own small-step and Dirichlet tests); a scene
+ * or 16, or 0 to size the clusters from the largest scene).  Every scene runs its own Newton loop (its own small-step and Dirichlet tests); a scene
  * that has finished is switched off for the rest of the step.  The scenes must share dt,
  * gravity, stiffnesses and solver settings and run with the floor off; LCS_NEWTON_PLAIN is
  * rejected.  A scene's trajectory does not depend on the other scenes of the batch (up to the

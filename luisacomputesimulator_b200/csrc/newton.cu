@@ -794,7 +794,7 @@ int newton_iteration(lcs_newton* h)
                            (h->pipelined ? LCS_PCG_PIPELINED : 0)};
         lcs_pcg_stats ps;
         if (h->batch)
-            rc = lcs_pcg_solve_batch(h->pcg, h->S, h->voff_d, &h->h_voff[h->S], h->active,
+            rc = lcs_pcg_solve_batch(h->pcg, h->S, h->voff_d, h->h_voff.data(), h->active,
                                      reinterpret_cast<const float*>(h->diag), h->nnz_mat ? &A : nullptr, &Bc,
                                      reinterpret_cast<const float*>(h->b), reinterpret_cast<float*>(h->dx), &o, h->bpcg,
                                      h->cluster, h->s);
@@ -1026,8 +1026,9 @@ extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_s
 {
     if (!descs || !out || n_scenes == 0) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: bad argument");
     if (flags & LCS_NEWTON_PLAIN) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: the batch runs fused only");
-    if (pcg_cluster != 1 && pcg_cluster != 2 && pcg_cluster != 4 && pcg_cluster != 8 && pcg_cluster != 16)
-        return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: cluster size must be 1, 2, 4, 8 or 16");
+    if (pcg_cluster != 0 && pcg_cluster != 1 && pcg_cluster != 2 && pcg_cluster != 4 && pcg_cluster != 8 &&
+        pcg_cluster != 16)
+        return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: cluster size must be 0 (auto), 1, 2, 4, 8 or 16");
     const lcs_scene_desc& d0 = descs[0];
     // concatenate the scenes: indices shifted by the vertex offset, animation groups renumbered
     std::vector<uint32_t> voff(n_scenes + 1, 0), foff(n_scenes + 1, 0), eoff(n_scenes + 1, 0), boff(n_scenes + 1, 0);

@@ -15,6 +15,8 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <mutex>
 #include <new>
 
@@ -1550,17 +1552,26 @@ extern "C" int lcs_pcg_solve_noalloc(uint32_t n, const float* diag, const lcs_bs
     return LCS_OK;
 }
 
-extern "C" int lcs_pcg_solve_batch(lcs_pcg* P, uint32_t n_scenes, const uint32_t* row_offsets, const uint32_t* host_row_end,
+extern "C" int lcs_pcg_solve_batch(lcs_pcg* P, uint32_t n_scenes, const uint32_t* row_offsets, const uint32_t* host_row_offsets,
                                    const uint32_t* active, const float* diag, const lcs_bsr* A, const lcs_bsr* B,
                                    const float* b, float* x, const lcs_pcg_opts* opts, lcs_pcg_stats* stats_per_scene,
                                    int cluster, lcs_stream stream)
 {
-    if (!P || !row_offsets || !host_row_end || !diag || !b || !x || !stats_per_scene || n_scenes == 0)
+    if (!P || !row_offsets || !host_row_offsets || !diag || !b || !x || !stats_per_scene || n_scenes == 0)
         return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_batch: bad argument");
+    const uint32_t* host_row_end = host_row_offsets + n_scenes;
     if (*host_row_end > P->n || (A && A->n_rows != P->n) || (B && B->n_rows != P->n))
         return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_batch: row count mismatch");
-    if (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8 && cluster != 16)
-        return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_batch: cluster size must be 1, 2, 4, 8 or 16");
+    if (cluster != 0 && cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8 && cluster != 16)
+        return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_batch: cluster size must be 0 (auto), 1, 2, 4, 8 or 16");
+    if (cluster == 0) {  // auto: at most 8 chunks of 256 rows per CTA for the largest scene, up to 16 CTAs
+        if (!host_row_offsets) return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_batch: auto cluster needs host row offsets");
+        uint32_t most = 0;
+        for (uint32_t s = 0; s < n_scenes; ++s) most = std::max(most, host_row_offsets[s + 1] - host_row_offsets[s]);
+        const uint32_t chunks_most = (most + 255) / 256;
+        cluster = 1;
+        while (cluster < 16 && chunks_most > 8u * (uint32_t)cluster) cluster *= 2;
+    }
     lcs_pcg_opts o = opts ? *opts : lcs_pcg_opts{100, 1e-4f, 1e-10f, 1, 0};
     if (o.check_every <= 0) o.check_every = 1;
     const size_t chunks = (size_t)(*host_row_end >> 8) + n_scenes + 1;

@@ -61,11 +61,13 @@ def solve_batch(solver, row_offsets, diag, A_bsr, B_bsr, b, x, stats, active=Non
                 abs_rz_tol=1e-10, check_every=1, fp64_dots=False, cluster=4):
     """Independent per-scene Jacobi-PCG solves in one launch (lcs_pcg_solve_batch).  row_offsets: CUDA
     int32 tensor of n_scenes + 1 offsets; stats: CUDA int32 tensor (n_scenes, 4) receiving lcs_pcg_stats."""
+    import numpy as np
     lib = A.load()
     n_scenes = row_offsets.shape[0] - 1
-    end = C.c_uint32(int(row_offsets[-1].item()))
+    host_offs = np.ascontiguousarray(row_offsets.cpu().numpy().view(np.uint32))
     o = A.PcgOpts(max_iter, rel_tol, abs_rz_tol, check_every, A.LCS_PCG_FP64_DOTS if fp64_dots else 0)
-    A.check(lib.lcs_pcg_solve_batch(solver.h, n_scenes, ptr(row_offsets), C.byref(end), ptr(active), ptr(diag),
+    A.check(lib.lcs_pcg_solve_batch(solver.h, n_scenes, ptr(row_offsets), host_offs.ctypes.data_as(C.c_void_p),
+                                    ptr(active), ptr(diag),
                                     C.byref(A_bsr) if A_bsr is not None else None,
                                     C.byref(B_bsr) if B_bsr is not None else None, ptr(b), ptr(x), C.byref(o),
                                     ptr(stats), cluster, stream()), "lcs_pcg_solve_batch")

@@ -150,7 +150,7 @@ class NewtonBatch:
     Newton phase for all scenes, per-scene trees, step bounds and PCG (one thread-block cluster of
     `cluster` CTAs per scene).  A scene's trajectory does not depend on the other scenes."""
 
-    def __init__(self, scenes, fp64=False, profile=False, cluster=4, nonlinear_iters=3, pcg_max_iter=100,
+    def __init__(self, scenes, fp64=False, profile=False, cluster=0, nonlinear_iters=3, pcg_max_iter=100,
                  pcg_rel_tol=1e-4, pcg_abs_rz_tol=1e-10, damping=2.0, stream=None):
         self.lib = A.load()
         self.scenes = list(scenes)
