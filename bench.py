@@ -54,8 +54,8 @@ def args_():
     p.add_argument("--plain-sample", type=int, default=32, help="requests/scenes timed through the plain loop")
     p.add_argument("--requests", type=int, default=64, help="serve workload: requests")
     p.add_argument("--rate", type=float, default=200.0, help="serve workload: Poisson arrival rate (1/s)")
-    p.add_argument("--max-batches", type=int, default=4, help="serve workload: batches in flight")
-    p.add_argument("--gather", type=float, default=0.1, help="serve workload: admission gather window (s)")
+    p.add_argument("--max-batches", type=int, default=2, help="serve workload: batches in flight")
+    p.add_argument("--gather", type=float, default=0.4, help="serve workload: admission gather window (s)")
     p.add_argument("--no-plain", action="store_true", help="batch/serve: skip the plain-loop comparator")
     return p.parse_args()
 

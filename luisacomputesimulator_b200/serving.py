@@ -47,8 +47,8 @@ class Server:
     max_batches: batches stepping at the same time (one host thread and one stream each);
     max_batch_verts: vertices in one batch."""
 
-    def __init__(self, budget_bytes=150e9, max_batches=4, max_batch_verts=1_500_000, cluster=0,
-                 bytes_per_vertex=4096.0, device=0, solve=None, free_bytes=None, gather_s=0.1):
+    def __init__(self, budget_bytes=150e9, max_batches=2, max_batch_verts=1_500_000, cluster=0,
+                 bytes_per_vertex=4096.0, device=0, solve=None, free_bytes=None, gather_s=0.4):
         self.budget = float(budget_bytes)
         self.max_batches = int(max_batches)
         self.max_batch_verts = int(max_batch_verts)
