@@ -133,6 +133,17 @@ LCS_API int lcs_bvh_query_ee(const lcs_bvh* edge_tree, const float* x0, const fl
                      lcs_stream stream);
 
 /* LBVH::check_health (lbvh.cpp:1033-1036).  Synchronises `stream`. host out. */
+/* Candidate filter (no counterpart in the reference): the pairs of a VF (is_ee = 0, elems = faces)
+ * or EE (is_ee = 1, elems = edges) candidate list whose boxes overlap at positions x, with the
+ * boxes and the strict test of the queries above (query box +- thickness + d_hat of its first
+ * vertex, leaf box +- thickness of its element's first vertex).  Applied to a swept-box list of a
+ * tree it yields exactly the static-box list of the same tree at any x on the sweep, provided the
+ * swept traversal did not end early.  Counts pairs beyond out_capacity without writing them. */
+LCS_API int lcs_candidates_filter(int is_ee, const uint32_t* in_pairs, const uint32_t* in_count,
+                                  uint32_t in_capacity, const float* x, const uint32_t* elems, const float* d_hat,
+                                  const float* thickness, uint32_t* out_pairs, uint32_t out_capacity,
+                                  uint32_t* out_count, lcs_stream stream);
+
 LCS_API int lcs_bvh_health(lcs_bvh* h, int* healthy, lcs_stream stream);
 
 /* Copies the tree out in the reference's LbvhData layout (lbvh.h:79-152), for tests and

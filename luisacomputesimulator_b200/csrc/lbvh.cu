@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide, 
                                                const uint2* __restrict__ edges, uint32_t n_queries,
                                                const float* __restrict__ dhat, const float* __restrict__ thickness,
                                                uint2* __restrict__ pairs, uint32_t capacity, uint32_t* d_count,
-                                               const uint32_t* __restrict__ order)
+                                               const uint32_t* __restrict__ order, uint32_t* capped)
 {
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_queries; t += gridDim.x * blockDim.x) {
         // queries in the order of `order` (the tree's Morton order when the queries are its own
@@ -329,9 +329,62 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide, 
             base = __shfl_sync(active, base, leader) + __popc(one & lt) + __popc(two & lt);
             for (uint32_t k = 0; k < nhit; ++k)
                 if (base + k < capacity) pairs[base + k] = make_uint2(q, hit[k]);
-            if (stop) break;
-            if (++loop > 100000u) break;
+            if (stop || ++loop > 100000u) {  // the reference's early exits; reported so callers know the
+                if (capped) atomicOr(capped, 1u);  // list may lack pairs a complete traversal would find
+                break;
+            }
         }
+    }
+}
+
+// Candidate filter: the pairs of `in` whose boxes overlap at positions x (static boxes, the
+// query inflated by thickness + d_hat of its first vertex, the leaf by the thickness of its
+// element's first vertex, strict test), i.e. exactly what query_template2 reports at x when no
+// early exit happens.  Used when `in` is a superset (the swept-box list of the same tree).
+template <bool EE>
+__global__ void __launch_bounds__(256) k_filter(const uint2* __restrict__ in, const uint32_t* __restrict__ in_count,
+                                                uint32_t in_cap, const float4* __restrict__ x,
+                                                const uint32_t* __restrict__ elems, const float* __restrict__ dhat,
+                                                const float* __restrict__ thickness, uint2* __restrict__ out,
+                                                uint32_t out_cap, uint32_t* out_count)
+{
+    uint32_t n = *in_count;
+    n = n < in_cap ? n : in_cap;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t n_round = (n + stride - 1) / stride * stride;  // whole warps stay in the loop for the ballot
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += stride) {
+        bool keep = false;
+        uint2 pr = make_uint2(0, 0);
+        if (i < n) {
+            pr = __ldg(&in[i]);
+            v3 qa;
+            uint32_t v0;
+            if (EE) {
+                const uint2 ed = __ldg(reinterpret_cast<const uint2*>(elems) + pr.x);
+                const v3 s0 = ld3(x, ed.x), s1 = ld3(x, ed.y);
+                const v3 mn = min3(min3(s0, s1), min3(s0, s1)), mx = max3(max3(s0, s1), max3(s0, s1));
+                v0 = ed.x;
+                const float r = __ldg(&thickness[v0]) + __ldg(&dhat[v0]);
+                const float q[6] = {mn.x - r, mn.y - r, mn.z - r, mx.x + r, mx.y + r, mx.z + r};
+                v3 lm, lx;
+                leaf_box(LCS_TREE_EDGE, pr.y, thickness, x, x, elems, lm, lx);
+                keep = overlap(make_float4(lm.x, lm.y, lm.z, 0.f), make_float4(lx.x, lx.y, lx.z, 0.f), q);
+            } else {
+                qa = ld3(x, pr.x);
+                const v3 mn = min3(qa, qa), mx = max3(qa, qa);
+                v0 = pr.x;
+                const float r = __ldg(&thickness[v0]) + __ldg(&dhat[v0]);
+                const float q[6] = {mn.x - r, mn.y - r, mn.z - r, mx.x + r, mx.y + r, mx.z + r};
+                v3 lm, lx;
+                leaf_box(LCS_TREE_FACE, pr.y, thickness, x, x, elems, lm, lx);
+                keep = overlap(make_float4(lm.x, lm.y, lm.z, 0.f), make_float4(lx.x, lx.y, lx.z, 0.f), q);
+            }
+        }
+        const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, keep);
+        uint32_t base = 0;
+        if (lane_id() == 0 && ballot) base = atomicAdd(out_count, __popc(ballot));
+        base = __shfl_sync(0xFFFFFFFFu, base, 0) + __popc(ballot & ((1u << lane_id()) - 1u));
+        if (keep && base < out_cap) out[base] = pr;
     }
 }
 
@@ -546,12 +599,19 @@ extern "C" int lcs_bvh_query_vf(const lcs_bvh* t, const float* x0, const float* 
                                 const float* d_hat, const float* thickness, uint32_t* pairs, uint32_t capacity,
                                 uint32_t* d_count, lcs_stream stream)
 {
+    return lcs_bvh_query_vf_capped(t, x0, x1, n_verts, d_hat, thickness, pairs, capacity, d_count, nullptr, stream);
+}
+
+int lcs_bvh_query_vf_capped(const lcs_bvh* t, const float* x0, const float* x1, uint32_t n_verts, const float* d_hat,
+                            const float* thickness, uint32_t* pairs, uint32_t capacity, uint32_t* d_count,
+                            uint32_t* capped, lcs_stream stream)
+{
     if (!t || t->kind != LCS_TREE_FACE || !x0 || !x1 || !d_hat || !thickness || !d_count || (capacity && !pairs))
         return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_vf: bad argument (needs a face tree)");
     if (t->n == 0 || n_verts == 0) return LCS_OK;
     k_query<false><<<grid_for(n_verts, 128, 16), 128, 0, (cudaStream_t)stream>>>(
         t->wide, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1), nullptr, n_verts,
-        d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count, nullptr);
+        d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count, nullptr, capped);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
@@ -561,6 +621,14 @@ extern "C" int lcs_bvh_query_ee(const lcs_bvh* t, const float* x0, const float* 
                                 uint32_t n_edges, const float* d_hat, const float* thickness, uint32_t* pairs,
                                 uint32_t capacity, uint32_t* d_count, lcs_stream stream)
 {
+    return lcs_bvh_query_ee_capped(t, x0, x1, edges, n_edges, d_hat, thickness, pairs, capacity, d_count, nullptr,
+                                   stream);
+}
+
+int lcs_bvh_query_ee_capped(const lcs_bvh* t, const float* x0, const float* x1, const uint32_t* edges, uint32_t n_edges,
+                            const float* d_hat, const float* thickness, uint32_t* pairs, uint32_t capacity,
+                            uint32_t* d_count, uint32_t* capped, lcs_stream stream)
+{
     if (!t || t->kind != LCS_TREE_EDGE || !x0 || !x1 || !edges || !d_hat || !thickness || !d_count ||
         (capacity && !pairs))
         return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_ee: bad argument (needs an edge tree)");
@@ -568,7 +636,7 @@ extern "C" int lcs_bvh_query_ee(const lcs_bvh* t, const float* x0, const float* 
     k_query<true><<<grid_for(n_edges, 128, 16), 128, 0, (cudaStream_t)stream>>>(
         t->wide, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
         reinterpret_cast<const uint2*>(edges), n_edges, d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity,
-        d_count, n_edges == t->n ? t->sgo : nullptr);
+        d_count, n_edges == t->n ? t->sgo : nullptr, capped);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
@@ -602,6 +670,23 @@ extern "C" int lcs_bvh_export(const lcs_bvh* h, uint32_t* parent, uint32_t* chil
         k_export<<<grid_for(nn, 256), 256, 0, s>>>(*h, object_idx, morton, node_aabb);
         lcs_count_launch();
     }
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+extern "C" int lcs_candidates_filter(int is_ee, const uint32_t* in_pairs, const uint32_t* in_count, uint32_t in_capacity,
+                                     const float* x, const uint32_t* elems, const float* d_hat, const float* thickness,
+                                     uint32_t* out_pairs, uint32_t out_capacity, uint32_t* out_count, lcs_stream stream)
+{
+    if (!in_count || !x || !elems || !d_hat || !thickness || !out_count || (in_capacity && !in_pairs) ||
+        (out_capacity && !out_pairs))
+        return lcs_fail(LCS_ERR_INVALID, "lcs_candidates_filter: bad argument");
+    if (in_capacity == 0) return LCS_OK;
+    auto kern = is_ee ? k_filter<true> : k_filter<false>;
+    kern<<<grid_for(in_capacity, 256), 256, 0, (cudaStream_t)stream>>>(
+        reinterpret_cast<const uint2*>(in_pairs), in_count, in_capacity, reinterpret_cast<const float4*>(x), elems,
+        d_hat, thickness, reinterpret_cast<uint2*>(out_pairs), out_capacity, out_count);
+    lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }

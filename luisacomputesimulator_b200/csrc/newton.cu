@@ -35,7 +35,7 @@ using namespace lcs;
 namespace {
 
 struct Status {
-    uint32_t cnt[6];  // 0 DCD vf, 1 DCD ee, 2 contact pairs, 3 CCD vf, 4 CCD ee, 5 spare
+    uint32_t cnt[6];  // 0 DCD vf, 1 DCD ee, 2 contact pairs, 3 CCD vf, 4 CCD ee, 5 a CCD traversal ended early
     float toi;
     float max_dx;     // max_v |dx_v| (before the step bound)
     float dirichlet;  // max over pinned vertices |x - x_tilde| after the step
@@ -311,6 +311,12 @@ __global__ void k_copy4(uint32_t n, const float4* __restrict__ a, float4* __rest
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
 }
 
+__global__ void k_save_ccd_counts(const Status* st, uint32_t* prev)
+{
+    prev[0] = st->cnt[3];
+    prev[1] = st->cnt[4];
+}
+
 __global__ void k_pcg_to_status(const lcs_pcg_stats* ps, Status* st)
 {
     st->pcg_iters = ps->iterations;
@@ -428,6 +434,11 @@ struct lcs_newton {
     uint32_t cap_vf = 0, cap_ee = 0, cap_pairs = 0;
     uint32_t alloc_vf = 0, alloc_ee = 0, alloc_pairs = 0;  // capacities the buffers were allocated with
     uint2 *bp_vf = nullptr, *bp_ee = nullptr;
+    // fused mode: DCD candidate lists (filled by traversal, or by filtering the previous iteration's
+    // CCD lists, which hold every DCD candidate of the next iterate when that traversal ran to the end)
+    uint2 *dcd_vf = nullptr, *dcd_ee = nullptr;
+    uint32_t* prev_ccd = nullptr;  // device: the CCD candidate counts of the previous iteration
+    bool filter_ok = false;
     lcs_pair* pairs = nullptr;
     lcs_assembler* asmb = nullptr;
     lcs_pcg* pcg = nullptr;
@@ -462,10 +473,14 @@ void free_contact(lcs_newton* h)
 {
     if (h->bp_vf) cudaFree(h->bp_vf);
     if (h->bp_ee) cudaFree(h->bp_ee);
+    if (h->dcd_vf) cudaFree(h->dcd_vf);
+    if (h->dcd_ee) cudaFree(h->dcd_ee);
     if (h->pairs) cudaFree(h->pairs);
     if (h->asmb) lcs_assembler_destroy(h->asmb);
     h->bp_vf = nullptr;
     h->bp_ee = nullptr;
+    h->dcd_vf = nullptr;
+    h->dcd_ee = nullptr;
     h->pairs = nullptr;
     h->asmb = nullptr;
 }
@@ -477,14 +492,20 @@ int alloc_contact(lcs_newton* h)
     cudaError_t e = cudaSuccess;
     if (!h->bp_vf || h->alloc_vf != h->cap_vf) {
         if (h->bp_vf) cudaFree(h->bp_vf);
+        if (h->dcd_vf) cudaFree(h->dcd_vf);
         h->bp_vf = nullptr;
+        h->dcd_vf = nullptr;
         e = dalloc(h->bp_vf, h->cap_vf);
+        if (e == cudaSuccess && !h->plain) e = dalloc(h->dcd_vf, h->cap_vf);
         h->alloc_vf = h->cap_vf;
     }
     if (e == cudaSuccess && (!h->bp_ee || h->alloc_ee != h->cap_ee)) {
         if (h->bp_ee) cudaFree(h->bp_ee);
+        if (h->dcd_ee) cudaFree(h->dcd_ee);
         h->bp_ee = nullptr;
+        h->dcd_ee = nullptr;
         e = dalloc(h->bp_ee, h->cap_ee);
+        if (e == cudaSuccess && !h->plain) e = dalloc(h->dcd_ee, h->cap_ee);
         h->alloc_ee = h->cap_ee;
     }
     if (e == cudaSuccess && (!h->pairs || h->alloc_pairs != h->cap_pairs)) {
@@ -652,23 +673,27 @@ int copy_x_to_host(lcs_newton* h, const float4* src)
     return LCS_OK;
 }
 
-int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint32_t* cnt_vf, uint32_t* cnt_ee)
+// refit + queries of both trees; lists into out_vf / out_ee; *capped |= 1 when a traversal ended early
+int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint2* out_vf, uint2* out_ee, uint32_t* cnt_vf,
+                uint32_t* cnt_ee, uint32_t* capped)
 {
     const float* X0 = reinterpret_cast<const float*>(x0);
     const float* X1 = reinterpret_cast<const float*>(x1);
+    uint32_t* PV = reinterpret_cast<uint32_t*>(out_vf);
+    uint32_t* PE = reinterpret_cast<uint32_t*>(out_ee);
+    const uint32_t* FA = reinterpret_cast<const uint32_t*>(h->faces);
+    const uint32_t* ED = reinterpret_cast<const uint32_t*>(h->edges);
     int rc;
     if (h->batch) {  // forests of per-scene trees, same two lanes
         LCS_CUDA_TRY(cudaEventRecord(h->fork, h->s));
         LCS_CUDA_TRY(cudaStreamWaitEvent(h->s2, h->fork, 0));
-        if ((rc = lcs_forest_update_refit(h->edge_forest, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->edges), h->s2)))
+        if ((rc = lcs_forest_update_refit(h->edge_forest, h->offset, X0, X1, ED, h->s2))) return rc;
+        if ((rc = lcs_forest_query_ee_capped(h->edge_forest, X0, X1, ED, h->dhat, h->offset, PE, h->cap_ee, cnt_ee,
+                                             capped, h->s2)))
             return rc;
-        if ((rc = lcs_forest_query_ee(h->edge_forest, X0, X1, reinterpret_cast<const uint32_t*>(h->edges), h->dhat,
-                                      h->offset, reinterpret_cast<uint32_t*>(h->bp_ee), h->cap_ee, cnt_ee, h->s2)))
-            return rc;
-        if ((rc = lcs_forest_update_refit(h->face_forest, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->faces), h->s)))
-            return rc;
-        if ((rc = lcs_forest_query_vf(h->face_forest, X0, X1, h->V, h->vscene, h->dhat, h->offset,
-                                      reinterpret_cast<uint32_t*>(h->bp_vf), h->cap_vf, cnt_vf, h->s)))
+        if ((rc = lcs_forest_update_refit(h->face_forest, h->offset, X0, X1, FA, h->s))) return rc;
+        if ((rc = lcs_forest_query_vf_capped(h->face_forest, X0, X1, h->V, h->vscene, h->dhat, h->offset, PV, h->cap_vf,
+                                             cnt_vf, capped, h->s)))
             return rc;
         LCS_CUDA_TRY(cudaEventRecord(h->join, h->s2));
         LCS_CUDA_TRY(cudaStreamWaitEvent(h->s, h->join, 0));
@@ -679,36 +704,55 @@ int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint32_t* cnt
         // latency-bound tree walks that leave most of the GPU idle when run one after the other
         LCS_CUDA_TRY(cudaEventRecord(h->fork, h->s));
         LCS_CUDA_TRY(cudaStreamWaitEvent(h->s2, h->fork, 0));
-        if ((rc = lcs_bvh_update_refit(h->edge_tree, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->edges), h->s2)))
+        if ((rc = lcs_bvh_update_refit(h->edge_tree, h->offset, X0, X1, ED, h->s2))) return rc;
+        if ((rc = lcs_bvh_query_ee_capped(h->edge_tree, X0, X1, ED, h->E, h->dhat, h->offset, PE, h->cap_ee, cnt_ee,
+                                          capped, h->s2)))
             return rc;
-        if ((rc = lcs_bvh_query_ee(h->edge_tree, X0, X1, reinterpret_cast<const uint32_t*>(h->edges), h->E, h->dhat,
-                                   h->offset, reinterpret_cast<uint32_t*>(h->bp_ee), h->cap_ee, cnt_ee, h->s2)))
-            return rc;
-        if ((rc = lcs_bvh_update_refit(h->face_tree, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->faces), h->s)))
-            return rc;
-        if ((rc = lcs_bvh_query_vf(h->face_tree, X0, X1, h->V, h->dhat, h->offset, reinterpret_cast<uint32_t*>(h->bp_vf),
-                                   h->cap_vf, cnt_vf, h->s)))
+        if ((rc = lcs_bvh_update_refit(h->face_tree, h->offset, X0, X1, FA, h->s))) return rc;
+        if ((rc = lcs_bvh_query_vf_capped(h->face_tree, X0, X1, h->V, h->dhat, h->offset, PV, h->cap_vf, cnt_vf, capped,
+                                          h->s)))
             return rc;
         LCS_CUDA_TRY(cudaEventRecord(h->join, h->s2));
         LCS_CUDA_TRY(cudaStreamWaitEvent(h->s, h->join, 0));
         return LCS_OK;
     }
     if (h->plain) {
-        if ((rc = lcs_bvh_update_leaves(h->face_tree, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->faces), h->s))) return rc;
+        if ((rc = lcs_bvh_update_leaves(h->face_tree, h->offset, X0, X1, FA, h->s))) return rc;
         if ((rc = lcs_bvh_refit(h->face_tree, h->s))) return rc;
-    } else if ((rc = lcs_bvh_update_refit(h->face_tree, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->faces), h->s))) {
+    } else if ((rc = lcs_bvh_update_refit(h->face_tree, h->offset, X0, X1, FA, h->s))) {
         return rc;
     }
-    if ((rc = lcs_bvh_query_vf(h->face_tree, X0, X1, h->V, h->dhat, h->offset, reinterpret_cast<uint32_t*>(h->bp_vf), h->cap_vf, cnt_vf, h->s)))
+    if ((rc = lcs_bvh_query_vf_capped(h->face_tree, X0, X1, h->V, h->dhat, h->offset, PV, h->cap_vf, cnt_vf, capped, h->s)))
         return rc;
     if (h->plain) {
-        if ((rc = lcs_bvh_update_leaves(h->edge_tree, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->edges), h->s))) return rc;
+        if ((rc = lcs_bvh_update_leaves(h->edge_tree, h->offset, X0, X1, ED, h->s))) return rc;
         if ((rc = lcs_bvh_refit(h->edge_tree, h->s))) return rc;
-    } else if ((rc = lcs_bvh_update_refit(h->edge_tree, h->offset, X0, X1, reinterpret_cast<const uint32_t*>(h->edges), h->s))) {
+    } else if ((rc = lcs_bvh_update_refit(h->edge_tree, h->offset, X0, X1, ED, h->s))) {
         return rc;
     }
-    return lcs_bvh_query_ee(h->edge_tree, X0, X1, reinterpret_cast<const uint32_t*>(h->edges), h->E, h->dhat, h->offset, reinterpret_cast<uint32_t*>(h->bp_ee), h->cap_ee,
-                            cnt_ee, h->s);
+    return lcs_bvh_query_ee_capped(h->edge_tree, X0, X1, ED, h->E, h->dhat, h->offset, PE, h->cap_ee, cnt_ee, capped,
+                                   h->s);
+}
+
+// DCD candidates of iterate x from the previous iteration's CCD lists (swept from x_iter to x_iter + dx,
+// so they contain every static-box overlap at x = x_iter + toi dx, 0 <= toi <= 1), in the two lanes
+int dcd_by_filter(lcs_newton* h)
+{
+    const float* X = reinterpret_cast<const float*>(h->x);
+    int rc;
+    LCS_CUDA_TRY(cudaEventRecord(h->fork, h->s));
+    LCS_CUDA_TRY(cudaStreamWaitEvent(h->s2, h->fork, 0));
+    if ((rc = lcs_candidates_filter(1, reinterpret_cast<const uint32_t*>(h->bp_ee), h->prev_ccd + 1, h->cap_ee, X,
+                                    reinterpret_cast<const uint32_t*>(h->edges), h->dhat, h->offset,
+                                    reinterpret_cast<uint32_t*>(h->dcd_ee), h->cap_ee, &h->st->cnt[1], h->s2)))
+        return rc;
+    if ((rc = lcs_candidates_filter(0, reinterpret_cast<const uint32_t*>(h->bp_vf), h->prev_ccd, h->cap_vf, X,
+                                    reinterpret_cast<const uint32_t*>(h->faces), h->dhat, h->offset,
+                                    reinterpret_cast<uint32_t*>(h->dcd_vf), h->cap_vf, &h->st->cnt[0], h->s)))
+        return rc;
+    LCS_CUDA_TRY(cudaEventRecord(h->join, h->s2));
+    LCS_CUDA_TRY(cudaStreamWaitEvent(h->s, h->join, 0));
+    return LCS_OK;
 }
 
 bool grow(lcs_newton* h)
@@ -729,7 +773,15 @@ int newton_iteration(lcs_newton* h)
     const lcs_scene_desc& d = h->d;
     int rc;
     for (int attempt = 0; attempt < 8; ++attempt) {
-        if (attempt) h->retries++;
+        if (attempt) {
+            h->retries++;
+            h->filter_ok = false;  // the CCD lists of the undone iteration do not describe this iterate
+        }
+        const bool filter = !h->plain && h->filter_ok;
+        if (filter) {
+            k_save_ccd_counts<<<1, 1, 0, h->s>>>(h->st, h->prev_ccd);
+            lcs_count_launch();
+        }
         mark(h, kPhMaterial);
         k_reset_status<<<1, 32, 0, h->s>>>(h->st);
         lcs_count_launch();
@@ -756,17 +808,23 @@ int newton_iteration(lcs_newton* h)
         }
         // update_contact_set (newton_solver.cpp:4093-4104)
         mark(h, kPhDcdBroad);
-        if ((rc = broad_phase(h, h->x, h->x, &h->st->cnt[0], &h->st->cnt[1]))) return rc;
+        uint2* dvf = h->plain ? h->bp_vf : h->dcd_vf;
+        uint2* dee = h->plain ? h->bp_ee : h->dcd_ee;
+        if (filter) {
+            if ((rc = dcd_by_filter(h))) return rc;
+        } else if ((rc = broad_phase(h, h->x, h->x, dvf, dee, &h->st->cnt[0], &h->st->cnt[1], nullptr))) {
+            return rc;
+        }
         if (h->plain) {
             if ((rc = host_readback(h))) return rc;  // download_broadphase_collision_count
             if (grow(h)) { if ((rc = alloc_contact(h))) return rc; continue; }
         }
         mark(h, kPhDcdNarrow);
         const float* X = reinterpret_cast<const float*>(h->x);
-        if ((rc = lcs_dcd_vf(reinterpret_cast<uint32_t*>(h->bp_vf), &h->st->cnt[0], h->cap_vf, X, reinterpret_cast<const uint32_t*>(h->faces), h->body, h->vert_area,
+        if ((rc = lcs_dcd_vf(reinterpret_cast<uint32_t*>(dvf), &h->st->cnt[0], h->cap_vf, X, reinterpret_cast<const uint32_t*>(h->faces), h->body, h->vert_area,
                              h->face_area, h->dhat, h->offset, d.kappa, h->pairs, h->cap_pairs, &h->st->cnt[2], h->s)))
             return rc;
-        if ((rc = lcs_dcd_ee(reinterpret_cast<uint32_t*>(h->bp_ee), &h->st->cnt[1], h->cap_ee, X, reinterpret_cast<const uint32_t*>(h->edges), h->body, h->edge_area, h->dhat,
+        if ((rc = lcs_dcd_ee(reinterpret_cast<uint32_t*>(dee), &h->st->cnt[1], h->cap_ee, X, reinterpret_cast<const uint32_t*>(h->edges), h->body, h->edge_area, h->dhat,
                              h->offset, d.kappa, h->pairs, h->cap_pairs, &h->st->cnt[2], h->s)))
             return rc;
         if (h->plain) {
@@ -821,7 +879,9 @@ int newton_iteration(lcs_newton* h)
         else
             k_apply_unit<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->st);
         lcs_count_launch();
-        if ((rc = broad_phase(h, h->x_iter, h->x, &h->st->cnt[3], &h->st->cnt[4]))) return rc;
+        if ((rc = broad_phase(h, h->x_iter, h->x, h->bp_vf, h->bp_ee, &h->st->cnt[3], &h->st->cnt[4],
+                              h->plain ? nullptr : &h->st->cnt[5])))
+            return rc;
         if (h->plain) {
             if ((rc = host_readback(h))) return rc;
             if (grow(h)) {
@@ -886,6 +946,8 @@ int newton_iteration(lcs_newton* h)
                 h->phase_launch_count[p] += 1;
             }
         }
+        // the next iteration may filter these CCD lists if no traversal ended early
+        h->filter_ok = !h->plain && h->h_st->cnt[5] == 0u;
         if (grow(h)) {  // an overflow anywhere: undo the step and run the iteration again
             k_copy4<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->x);
             lcs_count_launch();
@@ -976,6 +1038,7 @@ int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batc
     A(dalloc(h->b, V));
     A(dalloc(h->diag, 3 * V));
     A(dalloc(h->st, 1));
+    A(dalloc(h->prev_ccd, 2));
     if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->h_st), sizeof(Status));
     if (h->plain) {
         if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->h_x), 16 * V);
@@ -1182,7 +1245,7 @@ extern "C" int lcs_newton_destroy(lcs_newton* h)
     void* ptrs[] = {h->faces, h->edges, h->bend, h->Q, h->rest_len, h->vert_area, h->face_area, h->edge_area,
                     h->mass, h->dhat, h->offset, h->body, h->pinned, h->group, h->anim, h->rest, h->x, h->v,
                     h->x_step, h->x_iter, h->x_tilde, h->target, h->dx, h->b, h->diag, h->mat_rp, h->mat_col,
-                    h->spring_slots, h->bend_slots, h->mat_val, h->st, h->sell_ptr, h->sell_col};
+                    h->spring_slots, h->bend_slots, h->mat_val, h->st, h->sell_ptr, h->sell_col, h->prev_ccd};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_st) cudaFreeHost(h->h_st);
@@ -1210,6 +1273,7 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
     int rc;
     const auto t_host0 = std::chrono::steady_clock::now();
     h->retries = 0;
+    h->filter_ok = false;  // the trees are rebuilt below: no list of this step's trees yet
     h->time += d.dt;
     if (h->plain) {  // physics_step_GPU uploads x_step_start, x and v from the host every step
         const size_t bytes = 16 * (size_t)V;

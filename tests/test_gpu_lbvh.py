@@ -146,3 +146,41 @@ def test_single_leaf_tree_and_empty_queries():
     n = int(counts(cnt)[0])
     assert n == n_want
     np.testing.assert_array_equal(SC.sorted_pairs(host(pairs, np.uint32)[:n]), SC.sorted_pairs(want))
+
+
+@pytest.mark.parametrize("scene", ["cloth_sphere", "folded"])
+def test_filtered_swept_lists_equal_static_queries_on_the_sweep(scene):
+    """The fused Newton loop takes its DCD candidates from the previous CCD lists: filtering the swept
+    list (x0 -> x1) at any x = x0 + t (x1 - x0), 0 <= t <= 1, must give the static-box list at x."""
+    import ctypes as C
+    from luisacomputesimulator_b200 import _capi as A
+    from luisacomputesimulator_b200.collision import ptr, stream
+    sc, x0 = _scene(scene)
+    x1 = SC.random_motion(x0, 2e-3, seed=3)
+    xm = x0.copy()
+    xm[:, :3] = x0[:, :3] + np.float32(0.37) * (x1[:, :3] - x0[:, :3])
+    D = SceneOnDevice(sc)
+    lib = A.load()
+    for kind_name, is_ee in (("face", 0), ("edge", 1)):
+        t_o, bvh, _, ed = _build_both(sc, x0, kind_name)
+        elems = getattr(sc, KINDS[kind_name][1])
+        bvh.update_and_refit(D.offset, dev(x0), dev(x1), ed)
+        cap = 4 * max(sc.num_verts, elems.shape[0]) + 1024
+        swept = torch.zeros((cap, 2), dtype=torch.int32, device="cuda")
+        cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+        if is_ee:
+            bvh.broad_phase_query_from_edges(dev(x0), dev(x1), D.edges, cnt, swept, D.d_hat, D.offset)
+        else:
+            bvh.broad_phase_query_from_verts(dev(x0), dev(x1), cnt, swept, D.d_hat, D.offset)
+        out = torch.zeros((cap, 2), dtype=torch.int32, device="cuda")
+        ocnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+        A.check(lib.lcs_candidates_filter(is_ee, ptr(swept), ptr(cnt), cap, ptr(dev(xm)), ptr(ed), ptr(D.d_hat),
+                                          ptr(D.offset), ptr(out), cap, ptr(ocnt), stream()), "filter")
+        O.lbvh_refit(t_o, xm, xm, elems, sc.offset)
+        if is_ee:
+            want, n_want = O.lbvh_query_ee(t_o, xm, xm, sc.edges, sc.d_hat, sc.offset)
+        else:
+            want, n_want = O.lbvh_query_vf(t_o, xm, xm, sc.d_hat, sc.offset)
+        n = int(counts(ocnt)[0])
+        assert n == n_want and n <= int(counts(cnt)[0])
+        np.testing.assert_array_equal(SC.sorted_pairs(host(out, np.uint32)[:n]), SC.sorted_pairs(want))
