@@ -165,13 +165,14 @@ def test_filtered_swept_lists_equal_static_queries_on_the_sweep(scene):
         t_o, bvh, _, ed = _build_both(sc, x0, kind_name)
         elems = getattr(sc, KINDS[kind_name][1])
         bvh.update_and_refit(D.offset, dev(x0), dev(x1), ed)
-        cap = 4 * max(sc.num_verts, elems.shape[0]) + 1024
+        cap = 64 * max(sc.num_verts, elems.shape[0])
         swept = torch.zeros((cap, 2), dtype=torch.int32, device="cuda")
         cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
         if is_ee:
             bvh.broad_phase_query_from_edges(dev(x0), dev(x1), D.edges, cnt, swept, D.d_hat, D.offset)
         else:
             bvh.broad_phase_query_from_verts(dev(x0), dev(x1), cnt, swept, D.d_hat, D.offset)
+        assert int(counts(cnt)[0]) <= cap  # the whole swept list was written
         out = torch.zeros((cap, 2), dtype=torch.int32, device="cuda")
         ocnt = torch.zeros(1, dtype=torch.int32, device="cuda")
         A.check(lib.lcs_candidates_filter(is_ee, ptr(swept), ptr(cnt), cap, ptr(dev(xm)), ptr(ed), ptr(D.d_hat),
