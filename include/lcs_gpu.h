@@ -133,6 +133,16 @@ LCS_API int lcs_bvh_query_ee(const lcs_bvh* edge_tree, const float* x0, const fl
                      lcs_stream stream);
 
 /* LBVH::check_health (lbvh.cpp:1033-1036).  Synchronises `stream`. host out. */
+/* EE query over the tree's own edges that skips subtrees whose elements all have ids <= the query's
+ * (they only hold pairs the eid < adj rule drops); no counterpart in the reference.  Same result as
+ * lcs_bvh_query_ee unless bit 2 of *d_flags (device, ORed in) is set, meaning the skip could not be shown
+ * to leave the reference's early exits unchanged: then call lcs_bvh_query_ee.  Bit 1: a traversal ended
+ * early (full stack or 100000 steps), as in the reference. */
+LCS_API int lcs_bvh_query_ee_pruned(const lcs_bvh* edge_tree, const float* x0, const float* x1,
+                                    const uint32_t* edges, const float* d_hat, const float* thickness,
+                                    uint32_t* pairs, uint32_t capacity, uint32_t* d_count, uint32_t* d_flags,
+                                    lcs_stream stream);
+
 /* Candidate filter (no counterpart in the reference): the pairs of a VF (is_ee = 0, elems = faces)
  * or EE (is_ee = 1, elems = edges) candidate list whose boxes overlap at positions x, with the
  * boxes and the strict test of the queries above (query box +- thickness + d_hat of its first
