@@ -41,6 +41,9 @@ def args_():
     p.add_argument("--fp64", action="store_true", help="precision form")
     p.add_argument("--pcg", choices=["rows", "pipelined"], default="pipelined",
                    help="fused mode: row-resident PCG recurrences (classic: 3 grid syncs/iter; pipelined: 1)")
+    p.add_argument("--traversal", choices=["fast", "full"], default="fast",
+                   help="fast: DCD lists filtered from the previous CCD lists and pruned EE queries (same sets); "
+                        "full: a full traversal for every list")
     p.add_argument("--e2e-steps", type=int, default=10)
     p.add_argument("--cpu-iters", type=int, default=0, help="CPU baseline sample (0: auto, ~10-30 s)")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -212,7 +215,8 @@ def run_ours(a):
     lib = _capi.load()
     _capi.check(lib.lcs_device_check(local), "device check")
     sc = scenes.twisted_tube(a.n_around, a.n_along)
-    solver = NewtonSolver(sc, plain=(a.mode == "plain"), fp64=a.fp64, profile=True, pipelined=(a.pcg == "pipelined"))
+    solver = NewtonSolver(sc, plain=(a.mode == "plain"), fp64=a.fp64, profile=True, pipelined=(a.pcg == "pipelined"),
+                          full_traversal=(a.traversal == "full"))
     stream = torch.cuda.current_stream()
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
 
@@ -310,7 +314,7 @@ def run_ours(a):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms_total / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" + ("+f64 reductions" if a.fp64 else ""), "data": "synthetic (seeded tube mesh)",
-            "impl": "ours", "mode": a.mode, "pcg": solver.pcg_kind(),
+            "impl": "ours", "mode": a.mode, "pcg": solver.pcg_kind(), "traversal": a.traversal,
             "config": {**tube_config(a), "parallelism": f"replicas x{world}" if world > 1 else "single scene"},
             "e2e": None if a.e2e_steps == 0 else {
                 "value": e2e_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * 16 * V,

@@ -386,7 +386,9 @@ enum {
     LCS_NEWTON_PLAIN = 1,   /* the reference's dispatch structure (one-scene comparator) */
     LCS_NEWTON_FP64 = 2,    /* precision form: FP64 PCG reductions, ACCD step bound in FP64 */
     LCS_NEWTON_PROFILE = 4, /* per-phase CUDA-event timing (lcs_newton_profile) */
-    LCS_NEWTON_PCG_PIPELINED = 8 /* fused mode: pipelined row-resident PCG (LCS_PCG_PIPELINED) */
+    LCS_NEWTON_PCG_PIPELINED = 8, /* fused mode: pipelined row-resident PCG (LCS_PCG_PIPELINED) */
+    LCS_NEWTON_FULL_TRAVERSAL = 16 /* fused mode: every candidate list by a full unpruned traversal (no DCD
+                                      filtering of the previous CCD lists, no EE subtree pruning) */
 };
 
 typedef struct lcs_newton_stats {

@@ -127,7 +127,7 @@ SIGNATURES = {
     "lcs_newton_counts": (I32, [P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                 C.POINTER(C.c_uint32)]),
 }
-LCS_NEWTON_PLAIN, LCS_NEWTON_FP64, LCS_NEWTON_PROFILE, LCS_NEWTON_PCG_PIPELINED = 1, 2, 4, 8
+LCS_NEWTON_PLAIN, LCS_NEWTON_FP64, LCS_NEWTON_PROFILE, LCS_NEWTON_PCG_PIPELINED, LCS_NEWTON_FULL_TRAVERSAL = 1, 2, 4, 8, 16
 PHASES = ["build", "material", "dcd_broad", "dcd_narrow", "assembly", "pcg", "ccd_broad", "ccd_narrow", "apply"]
 
 _lib = None

@@ -440,6 +440,7 @@ struct lcs_newton {
     uint32_t* prev_ccd = nullptr;  // device: the CCD candidate counts of the previous iteration
     bool filter_ok = false;
     bool no_prune = false;         // this attempt re-runs an iteration whose pruned EE query was not provably exact
+    bool full_traversal = false;   // LCS_NEWTON_FULL_TRAVERSAL
     lcs_pair* pairs = nullptr;
     lcs_assembler* asmb = nullptr;
     lcs_pcg* pcg = nullptr;
@@ -708,7 +709,7 @@ int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint2* out_vf
         LCS_CUDA_TRY(cudaStreamWaitEvent(h->s2, h->fork, 0));
         if ((rc = lcs_bvh_update_refit(h->edge_tree, h->offset, X0, X1, ED, h->s2))) return rc;
         if ((rc = lcs_bvh_query_ee_capped(h->edge_tree, X0, X1, ED, h->E, h->dhat, h->offset, PE, h->cap_ee, cnt_ee,
-                                          &h->st->cnt[5], cap_bit, !h->no_prune, h->s2)))
+                                          &h->st->cnt[5], cap_bit, !h->no_prune && !h->full_traversal, h->s2)))
             return rc;
         if ((rc = lcs_bvh_update_refit(h->face_tree, h->offset, X0, X1, FA, h->s))) return rc;
         if ((rc = lcs_bvh_query_vf_capped(h->face_tree, X0, X1, h->V, h->dhat, h->offset, PV, h->cap_vf, cnt_vf,
@@ -734,7 +735,8 @@ int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint2* out_vf
         return rc;
     }
     return lcs_bvh_query_ee_capped(h->edge_tree, X0, X1, ED, h->E, h->dhat, h->offset, PE, h->cap_ee, cnt_ee,
-                                   h->plain ? nullptr : &h->st->cnt[5], cap_bit, !h->plain && !h->no_prune, h->s);
+                                   h->plain ? nullptr : &h->st->cnt[5], cap_bit,
+                                   !h->plain && !h->no_prune && !h->full_traversal, h->s);
 }
 
 // DCD candidates of iterate x from the previous iteration's CCD lists (swept from x_iter to x_iter + dx,
@@ -780,7 +782,7 @@ int newton_iteration(lcs_newton* h)
             h->retries++;
             h->filter_ok = false;  // the CCD lists of the undone iteration do not describe this iterate
         }
-        const bool filter = !h->plain && h->filter_ok;
+        const bool filter = !h->plain && !h->full_traversal && h->filter_ok;
         if (filter) {
             k_save_ccd_counts<<<1, 1, 0, h->s>>>(h->st, h->prev_ccd);
             lcs_count_launch();
@@ -995,6 +997,7 @@ int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batc
     h->fp64 = (flags & LCS_NEWTON_FP64) != 0;
     h->profile = (flags & LCS_NEWTON_PROFILE) != 0;
     h->pipelined = (flags & LCS_NEWTON_PCG_PIPELINED) != 0;
+    h->full_traversal = (flags & LCS_NEWTON_FULL_TRAVERSAL) != 0;
     h->batch = batch;
     h->V = d->n_verts;
     h->F = d->n_faces;

@@ -72,7 +72,7 @@ class NewtonSolver:
 
     def __init__(self, scene, plain=False, fp64=False, profile=False, nonlinear_iters=3, pcg_max_iter=100,
                  pcg_rel_tol=1e-4, pcg_abs_rz_tol=1e-10, pcg_check_every=25, damping=2.0, use_floor=False,
-                 floor_y=0.0, stream=None, pipelined=False):
+                 floor_y=0.0, stream=None, pipelined=False, full_traversal=False):
         self.lib = A.load()
         self.scene = scene
         sc = scene
@@ -82,7 +82,8 @@ class NewtonSolver:
                        pcg_check_every, damping, use_floor, floor_y)
         self.desc = d
         flags = (A.LCS_NEWTON_PLAIN if plain else 0) | (A.LCS_NEWTON_FP64 if fp64 else 0) | \
-            (A.LCS_NEWTON_PROFILE if profile else 0) | (A.LCS_NEWTON_PCG_PIPELINED if pipelined else 0)
+            (A.LCS_NEWTON_PROFILE if profile else 0) | (A.LCS_NEWTON_PCG_PIPELINED if pipelined else 0) | \
+            (A.LCS_NEWTON_FULL_TRAVERSAL if full_traversal else 0)
         s = C.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
         h = C.c_void_p()
         A.check(self.lib.lcs_newton_create(C.byref(d), flags, s, C.byref(h)), "lcs_newton_create")
