@@ -42,8 +42,8 @@ def args_():
     p.add_argument("--pcg", choices=["rows", "pipelined"], default="pipelined",
                    help="fused mode: row-resident PCG recurrences (classic: 3 grid syncs/iter; pipelined: 1)")
     p.add_argument("--traversal", choices=["fast", "full"], default="fast",
-                   help="fast: DCD lists filtered from the previous CCD lists and pruned EE queries (same sets); "
-                        "full: a full traversal for every list")
+                   help="fast: DCD lists filtered from the previous iteration's CCD lists (same sets); "
+                        "full: a traversal for every list")
     p.add_argument("--e2e-steps", type=int, default=10)
     p.add_argument("--cpu-iters", type=int, default=0, help="CPU baseline sample (0: auto, ~10-30 s)")
     p.add_argument("--no-cpu-baseline", action="store_true")

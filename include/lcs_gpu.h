@@ -133,16 +133,6 @@ LCS_API int lcs_bvh_query_ee(const lcs_bvh* edge_tree, const float* x0, const fl
                      lcs_stream stream);
 
 /* LBVH::check_health (lbvh.cpp:1033-1036).  Synchronises `stream`. host out. */
-/* EE query over the tree's own edges that skips subtrees whose elements all have ids <= the query's
- * (they only hold pairs the eid < adj rule drops); no counterpart in the reference.  Same result as
- * lcs_bvh_query_ee unless bit 2 of *d_flags (device, ORed in) is set, meaning the skip could not be shown
- * to leave the reference's early exits unchanged: then call lcs_bvh_query_ee.  Bit 1: a traversal ended
- * early (full stack or 100000 steps), as in the reference. */
-LCS_API int lcs_bvh_query_ee_pruned(const lcs_bvh* edge_tree, const float* x0, const float* x1,
-                                    const uint32_t* edges, const float* d_hat, const float* thickness,
-                                    uint32_t* pairs, uint32_t capacity, uint32_t* d_count, uint32_t* d_flags,
-                                    lcs_stream stream);
-
 /* Candidate filter (no counterpart in the reference): the pairs of a VF (is_ee = 0, elems = faces)
  * or EE (is_ee = 1, elems = edges) candidate list whose boxes overlap at positions x, with the
  * boxes and the strict test of the queries above (query box +- thickness + d_hat of its first
@@ -387,8 +377,8 @@ enum {
     LCS_NEWTON_FP64 = 2,    /* precision form: FP64 PCG reductions, ACCD step bound in FP64 */
     LCS_NEWTON_PROFILE = 4, /* per-phase CUDA-event timing (lcs_newton_profile) */
     LCS_NEWTON_PCG_PIPELINED = 8, /* fused mode: pipelined row-resident PCG (LCS_PCG_PIPELINED) */
-    LCS_NEWTON_FULL_TRAVERSAL = 16 /* fused mode: every candidate list by a full unpruned traversal (no DCD
-                                      filtering of the previous CCD lists, no EE subtree pruning) */
+    LCS_NEWTON_FULL_TRAVERSAL = 16 /* fused mode: every candidate list by a traversal (no DCD filtering of the
+                                      previous iteration's CCD lists) */
 };
 
 typedef struct lcs_newton_stats {

@@ -111,7 +111,6 @@ SIGNATURES = {
     "lcs_forest_query_ee": (I32, [P, P, P, P, P, P, P, U32, P, P]),
     "lcs_forest_health": (I32, [P, C.POINTER(C.c_int), P]),
     "lcs_forest_export_scene": (I32, [P, U32, P, P, P, P, P, P, P, P]),
-    "lcs_bvh_query_ee_pruned": (I32, [P, P, P, P, P, P, P, U32, P, P, P]),
     "lcs_candidates_filter": (I32, [I32, P, P, U32, P, P, P, P, P, U32, P, P]),
     "lcs_ccd_batch": (I32, [I32, P, P, U32, P, P, P, P, P, P, P, P, I32, P]),
     "lcs_pcg_solve_batch": (I32, [P, U32, P, P, P, P, C.POINTER(Bsr), C.POINTER(Bsr), P, P,

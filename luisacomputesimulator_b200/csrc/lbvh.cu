@@ -41,8 +41,6 @@ struct lcs_bvh {
     float4* wide = nullptr;          // 4 * max(ni, 1)
     uint32_t* counters = nullptr;    // max(ni, 1), refit arrival counters (self-resetting)
     uint32_t* healthy = nullptr;     // 1
-    uint32_t* height = nullptr;      // 1: edges on the longest root-to-leaf path (set by construct)
-    uint32_t* nlv = nullptr;         // max(ni, 1): leaves under each inner node
 };
 
 namespace {
@@ -143,7 +141,7 @@ __global__ void k_apply_sorted(const uint32_t* __restrict__ m30s, const uint32_t
 // traversal records' child codes and the child -> parent slot map
 __global__ void k_build_inner(const uint64_t* __restrict__ ms, const uint32_t* __restrict__ sgo, uint32_t n,
                               uint32_t* __restrict__ parent, uint2* __restrict__ children,
-                              uint32_t* __restrict__ slot, float4* __restrict__ wide, uint32_t* __restrict__ nlv)
+                              uint32_t* __restrict__ slot, float4* __restrict__ wide)
 {
     const int ni = (int)n - 1;
     for (int nid = blockIdx.x * blockDim.x + threadIdx.x; nid < ni; nid += gridDim.x * blockDim.x) {
@@ -192,34 +190,11 @@ __global__ void k_build_inner(const uint64_t* __restrict__ ms, const uint32_t* _
         children[nid] = make_uint2((uint32_t)cleft, (uint32_t)cright);
         slot[cleft] = 2u * (uint32_t)nid + 0u;
         slot[cright] = 2u * (uint32_t)nid + 1u;
-        nlv[nid] = (uint32_t)(b - a + 1);
         const uint32_t code_l = cleft < ni ? (uint32_t)cleft : (0x80000000u | sgo[cleft - ni]);
         const uint32_t code_r = cright < ni ? (uint32_t)cright : (0x80000000u | sgo[cright - ni]);
         wide[4 * nid + 0].w = __uint_as_float(code_l);
         wide[4 * nid + 2].w = __uint_as_float(code_r);
     }
-}
-
-// tree height (edges on the longest root-to-leaf path): each leaf walks to the root
-__global__ void k_height(const uint32_t* __restrict__ parent, uint32_t n, uint32_t* __restrict__ height)
-{
-    const uint32_t ni = n - 1;
-    uint32_t h = 0;
-    for (uint32_t lid = blockIdx.x * blockDim.x + threadIdx.x; lid < n; lid += gridDim.x * blockDim.x) {
-        uint32_t node = ni + lid, d = 0;
-        while (node != 0 && d < 512) {  // a broken link cannot loop forever
-            node = __ldg(&parent[node]);
-            if (node >= 2 * n) { d = 512; break; }
-            ++d;
-        }
-        h = h > d ? h : d;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const uint32_t t = __shfl_xor_sync(0xFFFFFFFFu, h, o);
-        h = h > t ? h : t;
-    }
-    if (lane_id() == 0 && h) atomicMax(height, h);
 }
 
 // fn_check_construction, lbvh.cpp:598-611
@@ -255,10 +230,10 @@ __global__ void k_leaves_refit(int kind, uint32_t n, const uint32_t* __restrict_
             v3 mn, mx;
             leaf_box(kind, e, thickness, x0, x1, elems, mn, mx);
             if (n == 1) {
-                store_slot(wide, 0, mn, mx, 0x80000000u | e, e);
-                store_slot(wide, 1, mn, mx, 0x80000000u | e, e);
+                store_slot(wide, 0, mn, mx, 0x80000000u | e);
+                store_slot(wide, 1, mn, mx, 0x80000000u | e);
             } else {
-                store_slot(wide, slot[ni + lid], mn, mx, 0x80000000u | e, e);
+                store_slot(wide, slot[ni + lid], mn, mx, 0x80000000u | e);
             }
         }
         if (!climb || n == 1) continue;
@@ -277,8 +252,7 @@ __global__ void k_leaves_refit(int kind, uint32_t n, const uint32_t* __restrict_
             v3 mn = mk3(fmn(a0.x, b0.x), fmn(a0.y, b0.y), fmn(a0.z, b0.z));
             v3 mx = mk3(fmx(a1.x, b1.x), fmx(a1.y, b1.y), fmx(a1.z, b1.z));
             if (p == 0) break;
-            const uint32_t ma = __float_as_uint(a1.w), mb = __float_as_uint(b1.w);
-            store_slot(wide, slot[p], mn, mx, p, ma > mb ? ma : mb);
+            store_slot(wide, slot[p], mn, mx, p);
             p = parent[p];
         }
     }
@@ -292,17 +266,8 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide, 
                                                const uint2* __restrict__ edges, uint32_t n_queries,
                                                const float* __restrict__ dhat, const float* __restrict__ thickness,
                                                uint2* __restrict__ pairs, uint32_t capacity, uint32_t* d_count,
-                                               const uint32_t* __restrict__ order, uint32_t* flags, uint32_t cap_bit,
-                                               const uint32_t* __restrict__ height, const uint32_t* __restrict__ nlv,
-                                               int prune)
+                                               const uint32_t* __restrict__ order, uint32_t* capped)
 {
-    // EE pruning: a subtree whose largest element id is <= q holds only pairs the eid < adj rule drops.
-    // Skipping it cannot change the candidate set as long as the reference traversal would not have
-    // ended early: never on a full stack when the tree height is <= 31 (the stack then holds at most one
-    // pending sibling per level plus two children), and not on the 100000-step limit while the pops
-    // made plus the inner nodes of the skipped subtrees stay below it; otherwise bit 2 of *flags asks
-    // the caller to run the query again without pruning.
-    const bool pr = EE && prune && height && nlv && __ldg(height) <= 31u;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_queries; t += gridDim.x * blockDim.x) {
         // queries in the order of `order` (the tree's Morton order when the queries are its own
         // leaves): neighbouring threads then walk nearly the same nodes
@@ -329,7 +294,7 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide, 
         }
         uint32_t stack[32];
         int sp = 0;
-        uint32_t loop = 0, skipped = 0;
+        uint32_t loop = 0;
         stack[sp++] = 0;
         while (sp > 0) {
             const uint32_t node = stack[--sp];
@@ -346,8 +311,6 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide, 
                     if (code & 0x80000000u) {
                         const uint32_t obj = code & 0x7FFFFFFFu;
                         if (!EE || q < obj) hit[nhit++] = obj;
-                    } else if (pr && __float_as_uint(mx.w) <= q) {
-                        skipped += __ldg(&nlv[code]) - 1u;  // inner nodes of the skipped subtree
                     } else if (sp < 32) {
                         stack[sp++] = code;
                     } else {
@@ -367,11 +330,10 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide, 
             for (uint32_t k = 0; k < nhit; ++k)
                 if (base + k < capacity) pairs[base + k] = make_uint2(q, hit[k]);
             if (stop || ++loop > 100000u) {  // the reference's early exits; reported so callers know the
-                if (flags && cap_bit) atomicOr(flags, cap_bit);  // list may lack pairs a full traversal finds
+                if (capped) atomicOr(capped, 1u);  // list may lack pairs a complete traversal would find
                 break;
             }
         }
-        if (pr && loop + skipped >= 100000u && flags) atomicOr(flags, 2u);
     }
 }
 
@@ -491,8 +453,6 @@ extern "C" int lcs_bvh_create(int kind, uint32_t n_leaves, lcs_bvh** out)
     A(alloc(h->wide, 4 * nw));
     A(alloc(h->counters, nw));
     A(alloc(h->healthy, 1));
-    A(alloc(h->height, 1));
-    A(alloc(h->nlv, h->ni ? h->ni : 1));
     if (e == cudaSuccess) e = cudaMemset(h->counters, 0, sizeof(uint32_t) * nw);
     if (e == cudaSuccess) e = cudaMemset(h->wide, 0, sizeof(float4) * 4 * nw);
     if (e == cudaSuccess) e = cudaMemset(h->slot, 0xFF, sizeof(uint32_t) * nn);
@@ -510,8 +470,7 @@ extern "C" int lcs_bvh_destroy(lcs_bvh* h)
 {
     if (!h) return LCS_OK;
     void* ptrs[] = {h->centers, h->block_aabb, h->gaabb, h->m30, h->keys, h->keys_alt, h->vals, h->vals_alt,
-                    h->hist, h->ms64, h->parent, h->children, h->slot, h->wide, h->counters, h->healthy,
-                    h->height, h->nlv};
+                    h->hist, h->ms64, h->parent, h->children, h->slot, h->wide, h->counters, h->healthy};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete h;
@@ -556,12 +515,9 @@ extern "C" int lcs_bvh_construct(lcs_bvh* h, lcs_stream stream)
     lcs_count_launch();
     if (h->ni > 0) {
         const int gi = grid_for(h->ni, 256);
-        k_build_inner<<<gi, 256, 0, s>>>(h->ms64, h->sgo, h->n, h->parent, h->children, h->slot, h->wide, h->nlv);
+        k_build_inner<<<gi, 256, 0, s>>>(h->ms64, h->sgo, h->n, h->parent, h->children, h->slot, h->wide);
         lcs_count_launch();
         k_check<<<gi, 256, 0, s>>>(h->children, h->parent, h->ni, h->healthy);
-        lcs_count_launch();
-        LCS_CUDA_TRY(cudaMemsetAsync(h->height, 0, sizeof(uint32_t), s));
-        k_height<<<grid_for(h->n, 256), 256, 0, s>>>(h->parent, h->n, h->height);
         lcs_count_launch();
     } else {
         cudaMemcpyAsync(h->slot, &kInvalid, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
@@ -596,12 +552,9 @@ int lcs_bvh_construct_host_sort(lcs_bvh* h, lcs_stream stream)
     lcs_count_launch();
     if (h->ni > 0) {
         const int gi = grid_for(h->ni, 256);
-        k_build_inner<<<gi, 256, 0, s>>>(h->ms64, h->sgo, h->n, h->parent, h->children, h->slot, h->wide, h->nlv);
+        k_build_inner<<<gi, 256, 0, s>>>(h->ms64, h->sgo, h->n, h->parent, h->children, h->slot, h->wide);
         lcs_count_launch();
         k_check<<<gi, 256, 0, s>>>(h->children, h->parent, h->ni, h->healthy);
-        lcs_count_launch();
-        LCS_CUDA_TRY(cudaMemsetAsync(h->height, 0, sizeof(uint32_t), s));
-        k_height<<<grid_for(h->n, 256), 256, 0, s>>>(h->parent, h->n, h->height);
         lcs_count_launch();
     }
     LCS_CUDA_TRY(cudaStreamSynchronize(s));  // host buffers go out of scope
@@ -646,21 +599,19 @@ extern "C" int lcs_bvh_query_vf(const lcs_bvh* t, const float* x0, const float* 
                                 const float* d_hat, const float* thickness, uint32_t* pairs, uint32_t capacity,
                                 uint32_t* d_count, lcs_stream stream)
 {
-    return lcs_bvh_query_vf_capped(t, x0, x1, n_verts, d_hat, thickness, pairs, capacity, d_count, nullptr, 0u,
-                                   stream);
+    return lcs_bvh_query_vf_capped(t, x0, x1, n_verts, d_hat, thickness, pairs, capacity, d_count, nullptr, stream);
 }
 
 int lcs_bvh_query_vf_capped(const lcs_bvh* t, const float* x0, const float* x1, uint32_t n_verts, const float* d_hat,
                             const float* thickness, uint32_t* pairs, uint32_t capacity, uint32_t* d_count,
-                            uint32_t* flags, uint32_t cap_bit, lcs_stream stream)
+                            uint32_t* capped, lcs_stream stream)
 {
     if (!t || t->kind != LCS_TREE_FACE || !x0 || !x1 || !d_hat || !thickness || !d_count || (capacity && !pairs))
         return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_vf: bad argument (needs a face tree)");
     if (t->n == 0 || n_verts == 0) return LCS_OK;
     k_query<false><<<grid_for(n_verts, 128, 16), 128, 0, (cudaStream_t)stream>>>(
         t->wide, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1), nullptr, n_verts,
-        d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count, nullptr, flags, cap_bit, nullptr, nullptr,
-        0);
+        d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count, nullptr, capped);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
@@ -671,12 +622,12 @@ extern "C" int lcs_bvh_query_ee(const lcs_bvh* t, const float* x0, const float* 
                                 uint32_t capacity, uint32_t* d_count, lcs_stream stream)
 {
     return lcs_bvh_query_ee_capped(t, x0, x1, edges, n_edges, d_hat, thickness, pairs, capacity, d_count, nullptr,
-                                   0u, 0, stream);
+                                   stream);
 }
 
 int lcs_bvh_query_ee_capped(const lcs_bvh* t, const float* x0, const float* x1, const uint32_t* edges, uint32_t n_edges,
                             const float* d_hat, const float* thickness, uint32_t* pairs, uint32_t capacity,
-                            uint32_t* d_count, uint32_t* flags, uint32_t cap_bit, int prune, lcs_stream stream)
+                            uint32_t* d_count, uint32_t* capped, lcs_stream stream)
 {
     if (!t || t->kind != LCS_TREE_EDGE || !x0 || !x1 || !edges || !d_hat || !thickness || !d_count ||
         (capacity && !pairs))
@@ -685,7 +636,7 @@ int lcs_bvh_query_ee_capped(const lcs_bvh* t, const float* x0, const float* x1, 
     k_query<true><<<grid_for(n_edges, 128, 16), 128, 0, (cudaStream_t)stream>>>(
         t->wide, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
         reinterpret_cast<const uint2*>(edges), n_edges, d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity,
-        d_count, n_edges == t->n ? t->sgo : nullptr, flags, cap_bit, t->height, t->nlv, prune && n_edges == t->n);
+        d_count, n_edges == t->n ? t->sgo : nullptr, capped);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
@@ -738,13 +689,4 @@ extern "C" int lcs_candidates_filter(int is_ee, const uint32_t* in_pairs, const 
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
-}
-
-extern "C" int lcs_bvh_query_ee_pruned(const lcs_bvh* t, const float* x0, const float* x1, const uint32_t* edges,
-                                       const float* d_hat, const float* thickness, uint32_t* pairs, uint32_t capacity,
-                                       uint32_t* d_count, uint32_t* d_flags, lcs_stream stream)
-{
-    if (!t || !d_flags) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_ee_pruned: bad argument");
-    return lcs_bvh_query_ee_capped(t, x0, x1, edges, t->n, d_hat, thickness, pairs, capacity, d_count, d_flags, 1u, 1,
-                                   stream);
 }

@@ -21,16 +21,14 @@ int64_t lcs_pcg_rows_capacity();
 // uploaded; lbvh.cpp:983-993) -- used by the plain one-scene comparator loop only.
 int lcs_bvh_construct_host_sort(lcs_bvh* h, lcs_stream stream);
 
-// lcs_bvh_query_vf / _ee that also OR cap_bit into *flags (device, may be NULL) when a traversal ends
-// early (full stack or the 100000-step limit), i.e. when the list may be incomplete.  prune (EE, the
-// tree's own edges as queries): skip subtrees whose elements all have ids <= the query's; ORs 2 into
-// *flags when it cannot show that the result equals the unpruned traversal (run it again unpruned).
+// lcs_bvh_query_vf / _ee that also OR 1 into *capped (device, may be NULL) when a traversal ends
+// early (full stack or the 100000-step limit), i.e. when the list may be incomplete.
 int lcs_bvh_query_vf_capped(const lcs_bvh* t, const float* x0, const float* x1, uint32_t n_verts, const float* d_hat,
                             const float* thickness, uint32_t* pairs, uint32_t capacity, uint32_t* d_count,
-                            uint32_t* flags, uint32_t cap_bit, lcs_stream stream);
+                            uint32_t* capped, lcs_stream stream);
 int lcs_bvh_query_ee_capped(const lcs_bvh* t, const float* x0, const float* x1, const uint32_t* edges, uint32_t n_edges,
                             const float* d_hat, const float* thickness, uint32_t* pairs, uint32_t capacity,
-                            uint32_t* d_count, uint32_t* flags, uint32_t cap_bit, int prune, lcs_stream stream);
+                            uint32_t* d_count, uint32_t* capped, lcs_stream stream);
 int lcs_forest_query_vf_capped(const lcs_forest* f, const float* x0, const float* x1, uint32_t n_verts,
                                const uint32_t* vert_scene, const float* d_hat, const float* thickness, uint32_t* pairs,
                                uint32_t capacity, uint32_t* d_count, uint32_t* capped, lcs_stream stream);

@@ -439,7 +439,6 @@ struct lcs_newton {
     uint2 *dcd_vf = nullptr, *dcd_ee = nullptr;
     uint32_t* prev_ccd = nullptr;  // device: the CCD candidate counts of the previous iteration
     bool filter_ok = false;
-    bool no_prune = false;         // this attempt re-runs an iteration whose pruned EE query was not provably exact
     bool full_traversal = false;   // LCS_NEWTON_FULL_TRAVERSAL
     lcs_pair* pairs = nullptr;
     lcs_assembler* asmb = nullptr;
@@ -675,10 +674,9 @@ int copy_x_to_host(lcs_newton* h, const float4* src)
     return LCS_OK;
 }
 
-// refit + queries of both trees; lists into out_vf / out_ee.  Status cnt[5]: cap_bit (1 for the CCD
-// queries, 0 for DCD) when a traversal ended early; 2 when a pruned EE query must be run again unpruned
+// refit + queries of both trees; lists into out_vf / out_ee; *capped |= 1 when a traversal ended early
 int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint2* out_vf, uint2* out_ee, uint32_t* cnt_vf,
-                uint32_t* cnt_ee, uint32_t cap_bit)
+                uint32_t* cnt_ee, uint32_t* capped)
 {
     const float* X0 = reinterpret_cast<const float*>(x0);
     const float* X1 = reinterpret_cast<const float*>(x1);
@@ -692,11 +690,11 @@ int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint2* out_vf
         LCS_CUDA_TRY(cudaStreamWaitEvent(h->s2, h->fork, 0));
         if ((rc = lcs_forest_update_refit(h->edge_forest, h->offset, X0, X1, ED, h->s2))) return rc;
         if ((rc = lcs_forest_query_ee_capped(h->edge_forest, X0, X1, ED, h->dhat, h->offset, PE, h->cap_ee, cnt_ee,
-                                             cap_bit ? &h->st->cnt[5] : nullptr, h->s2)))
+                                             capped, h->s2)))
             return rc;
         if ((rc = lcs_forest_update_refit(h->face_forest, h->offset, X0, X1, FA, h->s))) return rc;
         if ((rc = lcs_forest_query_vf_capped(h->face_forest, X0, X1, h->V, h->vscene, h->dhat, h->offset, PV, h->cap_vf,
-                                             cnt_vf, cap_bit ? &h->st->cnt[5] : nullptr, h->s)))
+                                             cnt_vf, capped, h->s)))
             return rc;
         LCS_CUDA_TRY(cudaEventRecord(h->join, h->s2));
         LCS_CUDA_TRY(cudaStreamWaitEvent(h->s, h->join, 0));
@@ -709,11 +707,11 @@ int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint2* out_vf
         LCS_CUDA_TRY(cudaStreamWaitEvent(h->s2, h->fork, 0));
         if ((rc = lcs_bvh_update_refit(h->edge_tree, h->offset, X0, X1, ED, h->s2))) return rc;
         if ((rc = lcs_bvh_query_ee_capped(h->edge_tree, X0, X1, ED, h->E, h->dhat, h->offset, PE, h->cap_ee, cnt_ee,
-                                          &h->st->cnt[5], cap_bit, !h->no_prune && !h->full_traversal, h->s2)))
+                                          capped, h->s2)))
             return rc;
         if ((rc = lcs_bvh_update_refit(h->face_tree, h->offset, X0, X1, FA, h->s))) return rc;
-        if ((rc = lcs_bvh_query_vf_capped(h->face_tree, X0, X1, h->V, h->dhat, h->offset, PV, h->cap_vf, cnt_vf,
-                                          &h->st->cnt[5], cap_bit, h->s)))
+        if ((rc = lcs_bvh_query_vf_capped(h->face_tree, X0, X1, h->V, h->dhat, h->offset, PV, h->cap_vf, cnt_vf, capped,
+                                          h->s)))
             return rc;
         LCS_CUDA_TRY(cudaEventRecord(h->join, h->s2));
         LCS_CUDA_TRY(cudaStreamWaitEvent(h->s, h->join, 0));
@@ -725,8 +723,7 @@ int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint2* out_vf
     } else if ((rc = lcs_bvh_update_refit(h->face_tree, h->offset, X0, X1, FA, h->s))) {
         return rc;
     }
-    if ((rc = lcs_bvh_query_vf_capped(h->face_tree, X0, X1, h->V, h->dhat, h->offset, PV, h->cap_vf, cnt_vf,
-                                      h->plain ? nullptr : &h->st->cnt[5], cap_bit, h->s)))
+    if ((rc = lcs_bvh_query_vf_capped(h->face_tree, X0, X1, h->V, h->dhat, h->offset, PV, h->cap_vf, cnt_vf, capped, h->s)))
         return rc;
     if (h->plain) {
         if ((rc = lcs_bvh_update_leaves(h->edge_tree, h->offset, X0, X1, ED, h->s))) return rc;
@@ -734,9 +731,8 @@ int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint2* out_vf
     } else if ((rc = lcs_bvh_update_refit(h->edge_tree, h->offset, X0, X1, ED, h->s))) {
         return rc;
     }
-    return lcs_bvh_query_ee_capped(h->edge_tree, X0, X1, ED, h->E, h->dhat, h->offset, PE, h->cap_ee, cnt_ee,
-                                   h->plain ? nullptr : &h->st->cnt[5], cap_bit,
-                                   !h->plain && !h->no_prune && !h->full_traversal, h->s);
+    return lcs_bvh_query_ee_capped(h->edge_tree, X0, X1, ED, h->E, h->dhat, h->offset, PE, h->cap_ee, cnt_ee, capped,
+                                   h->s);
 }
 
 // DCD candidates of iterate x from the previous iteration's CCD lists (swept from x_iter to x_iter + dx,
@@ -817,7 +813,7 @@ int newton_iteration(lcs_newton* h)
         uint2* dee = h->plain ? h->bp_ee : h->dcd_ee;
         if (filter) {
             if ((rc = dcd_by_filter(h))) return rc;
-        } else if ((rc = broad_phase(h, h->x, h->x, dvf, dee, &h->st->cnt[0], &h->st->cnt[1], 0u))) {
+        } else if ((rc = broad_phase(h, h->x, h->x, dvf, dee, &h->st->cnt[0], &h->st->cnt[1], nullptr))) {
             return rc;
         }
         if (h->plain) {
@@ -884,7 +880,8 @@ int newton_iteration(lcs_newton* h)
         else
             k_apply_unit<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->st);
         lcs_count_launch();
-        if ((rc = broad_phase(h, h->x_iter, h->x, h->bp_vf, h->bp_ee, &h->st->cnt[3], &h->st->cnt[4], 1u)))
+        if ((rc = broad_phase(h, h->x_iter, h->x, h->bp_vf, h->bp_ee, &h->st->cnt[3], &h->st->cnt[4],
+                              h->plain ? nullptr : &h->st->cnt[5])))
             return rc;
         if (h->plain) {
             if ((rc = host_readback(h))) return rc;
@@ -951,10 +948,8 @@ int newton_iteration(lcs_newton* h)
             }
         }
         // the next iteration may filter these CCD lists if no traversal ended early
-        h->filter_ok = !h->plain && (h->h_st->cnt[5] & 1u) == 0u;
-        const bool unprune = !h->plain && (h->h_st->cnt[5] & 2u) != 0u;
-        h->no_prune = unprune;
-        if (unprune || grow(h)) {  // an overflow anywhere, or a pruned query to redo: run the iteration again
+        h->filter_ok = !h->plain && h->h_st->cnt[5] == 0u;
+        if (grow(h)) {  // an overflow anywhere: undo the step and run the iteration again
             k_copy4<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->x);
             lcs_count_launch();
             if ((rc = alloc_contact(h))) return rc;

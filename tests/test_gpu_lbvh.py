@@ -185,29 +185,3 @@ def test_filtered_swept_lists_equal_static_queries_on_the_sweep(scene):
         n = int(counts(ocnt)[0])
         assert n == n_want and n <= int(counts(cnt)[0])
         np.testing.assert_array_equal(SC.sorted_pairs(host(out, np.uint32)[:n]), SC.sorted_pairs(want))
-
-
-@pytest.mark.parametrize("scene", ["cloth_sphere", "folded", "tube"])
-@pytest.mark.parametrize("swept", [False, True])
-def test_pruned_ee_query_equals_reference_set(scene, swept):
-    """EE queries that skip subtrees of smaller element ids give the reference's candidate set."""
-    from luisacomputesimulator_b200 import _capi as A
-    from luisacomputesimulator_b200.collision import ptr, stream
-    sc, x = _scene(scene)
-    x1 = SC.random_motion(x, 2e-3, seed=11) if swept else x
-    D = SceneOnDevice(sc)
-    t_o, bvh, xd, ed = _build_both(sc, x, "edge")
-    x1d = dev(x1)
-    O.lbvh_refit(t_o, x, x1, sc.edges, sc.offset)
-    bvh.update_and_refit(D.offset, xd, x1d, ed)
-    want, n_want = O.lbvh_query_ee(t_o, x, x1, sc.edges, sc.d_hat, sc.offset)
-    pairs = torch.zeros((n_want + 64, 2), dtype=torch.int32, device="cuda")
-    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
-    flags = torch.zeros(1, dtype=torch.int32, device="cuda")
-    lib = A.load()
-    A.check(lib.lcs_bvh_query_ee_pruned(bvh.h, ptr(xd), ptr(x1d), ptr(D.edges), ptr(D.d_hat), ptr(D.offset), ptr(pairs),
-                                        pairs.shape[0], ptr(cnt), ptr(flags), stream()), "pruned query")
-    assert int(counts(flags)[0]) == 0
-    n = int(counts(cnt)[0])
-    assert n == n_want
-    np.testing.assert_array_equal(SC.sorted_pairs(host(pairs, np.uint32)[:n]), SC.sorted_pairs(want))
