@@ -320,8 +320,9 @@ LCS_API int lcs_pcg_solve_noalloc(uint32_t n, const float* diag, const lcs_bsr* 
 /* Batched scenes (no counterpart in the reference): n_scenes independent systems, scene s owning
  * block rows [row_offsets[s], row_offsets[s+1]) of one BSR pair (row_offsets: device array of
  * n_scenes + 1; host_row_offsets: the same offsets in host memory), solved in one launch with one
- * thread-block cluster of `cluster` CTAs (1, 2, 4, 8 or 16; 0 picks the smallest size that gives
- * the largest scene at most 8 chunks of 256 rows per CTA) per scene.  Each scene has its own
+ * thread-block cluster of `cluster` CTAs (1, 2, 4, 8 or 16) per scene, or with `cluster` = 0 one
+ * cluster per scene of the smallest size that leaves it at most 8 chunks of 256 rows per CTA (one
+ * launch per size, side by side on streams forked from `stream`).  Each scene has its own
  * alpha, beta and stop decision (the rules of lcs_pcg_solve); its result does not depend on
  * `cluster` or on the other scenes.  active: device flags per scene (0: skip, x = 0) or NULL.
  * stats_per_scene: device array of n_scenes.  Asynchronous; the handle must hold at least

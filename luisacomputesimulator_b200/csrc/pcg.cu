@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <vector>
 
 #include <mutex>
 #include <new>
@@ -982,6 +983,7 @@ constexpr int kBatchThreads = 256;
 constexpr int kBatchLanes = 4;
 
 struct BatchArgs {
+    const uint32_t* scenes;  // cluster index -> scene id (null: the identity)
     const uint32_t* roff;    // S + 1
     const uint32_t* active;  // S (0: skip the scene, x = 0) or null
     const float4* diag;
@@ -1057,7 +1059,7 @@ __global__ void __launch_bounds__(kBatchThreads) k_pcg_batch(BatchArgs a)
     __shared__ double s_out[2];
     __shared__ double s_pq[kBatchThreads];
     const uint32_t C = cluster_ctas(), rank = cluster_rank();
-    const uint32_t s = blockIdx.x / C;
+    const uint32_t s = a.scenes ? a.scenes[blockIdx.x / C] : blockIdx.x / C;
     const uint32_t r0 = a.roff[s], r1 = a.roff[s + 1], nrows = r1 - r0;
     const uint32_t nchunks = (nrows + kBatchThreads - 1) / kBatchThreads;
     double* cp = a.cpart + 4 * (size_t)((r0 >> 8) + s);
@@ -1189,6 +1191,12 @@ struct lcs_pcg {
     int rows_capacity = -1;  // most rows the row-resident solve can hold co-resident (-1: not queried)
     double* cpart = nullptr;  // batched solve: per-chunk partial sums
     size_t cpart_cap = 0;     // chunks
+    // batched solve with per-scene cluster sizes: scene lists per size class, one stream per class
+    uint32_t* class_scenes = nullptr;
+    size_t class_cap = 0;
+    std::vector<uint32_t> class_host;
+    cudaStream_t class_stream[5] = {};
+    cudaEvent_t class_fork = nullptr, class_join[5] = {};
 };
 
 static constexpr int kRowLanes = 4;
@@ -1234,7 +1242,16 @@ extern "C" int lcs_pcg_create(uint32_t n, lcs_pcg** out)
 extern "C" int lcs_pcg_destroy(lcs_pcg* p)
 {
     if (!p) return LCS_OK;
-    void* ptrs[] = {p->r, p->z, p->p, p->q, p->minv, p->part, p->part_f, p->scal, p->bar, p->d_stats, p->cpart};
+    void* ptrs[] = {p->r, p->z, p->p, p->q, p->minv, p->part, p->part_f, p->scal, p->bar, p->d_stats, p->cpart,
+                    p->class_scenes};
+    for (int k = 0; k < 5; ++k) {
+        if (p->class_stream[k]) {
+            cudaStreamSynchronize(p->class_stream[k]);
+            cudaStreamDestroy(p->class_stream[k]);
+        }
+        if (p->class_join[k]) cudaEventDestroy(p->class_join[k]);
+    }
+    if (p->class_fork) cudaEventDestroy(p->class_fork);
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (p->h_scal) cudaFreeHost(p->h_scal);
@@ -1564,14 +1581,6 @@ extern "C" int lcs_pcg_solve_batch(lcs_pcg* P, uint32_t n_scenes, const uint32_t
         return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_batch: row count mismatch");
     if (cluster != 0 && cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8 && cluster != 16)
         return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_batch: cluster size must be 0 (auto), 1, 2, 4, 8 or 16");
-    if (cluster == 0) {  // auto: at most 8 chunks of 256 rows per CTA for the largest scene, up to 16 CTAs
-        if (!host_row_offsets) return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_batch: auto cluster needs host row offsets");
-        uint32_t most = 0;
-        for (uint32_t s = 0; s < n_scenes; ++s) most = std::max(most, host_row_offsets[s + 1] - host_row_offsets[s]);
-        const uint32_t chunks_most = (most + 255) / 256;
-        cluster = 1;
-        while (cluster < 16 && chunks_most > 8u * (uint32_t)cluster) cluster *= 2;
-    }
     lcs_pcg_opts o = opts ? *opts : lcs_pcg_opts{100, 1e-4f, 1e-10f, 1, 0};
     if (o.check_every <= 0) o.check_every = 1;
     const size_t chunks = (size_t)(*host_row_end >> 8) + n_scenes + 1;
@@ -1598,20 +1607,79 @@ extern "C" int lcs_pcg_solve_batch(lcs_pcg* P, uint32_t n_scenes, const uint32_t
     a.check_every = o.check_every;
     a.fp64 = (o.flags & LCS_PCG_FP64_DOTS) ? 1 : 0;
     a.stats = stats_per_scene;
-    if (cluster == 16) LCS_CUDA_TRY(cudaFuncSetAttribute(k_pcg_batch, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(n_scenes * (uint32_t)cluster);
-    cfg.blockDim = dim3(kBatchThreads);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = (cudaStream_t)stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = (unsigned)cluster;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    LCS_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_pcg_batch, a));
-    lcs_count_launch();
+    a.scenes = nullptr;
+    auto launch = [&](int C, uint32_t clusters, const uint32_t* scene_list, cudaStream_t st) -> cudaError_t {
+        if (C == 16) {
+            const cudaError_t e = cudaFuncSetAttribute(k_pcg_batch, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            if (e != cudaSuccess) return e;
+        }
+        BatchArgs b = a;
+        b.scenes = scene_list;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(clusters * (uint32_t)C);
+        cfg.blockDim = dim3(kBatchThreads);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)C;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, k_pcg_batch, b);
+    };
+    cudaStream_t s0 = (cudaStream_t)stream;
+    if (cluster != 0) {
+        LCS_CUDA_TRY(launch(cluster, n_scenes, nullptr, s0));
+        lcs_count_launch();
+        return LCS_OK;
+    }
+    // auto: every scene gets the smallest cluster (1..16 CTAs) that leaves it at most 8 chunks of 256 rows
+    // per CTA; one launch per cluster size, on forked streams so that the classes run side by side
+    std::vector<uint32_t> lists[5];
+    for (uint32_t sc = 0; sc < n_scenes; ++sc) {
+        const uint32_t chunks = (host_row_offsets[sc + 1] - host_row_offsets[sc] + 255) / 256;
+        int k = 0;
+        while (k < 4 && chunks > 8u << k) ++k;
+        lists[k].push_back(sc);
+    }
+    std::vector<uint32_t> flat;
+    size_t start[6] = {0};
+    for (int k = 0; k < 5; ++k) {
+        start[k] = flat.size();
+        flat.insert(flat.end(), lists[k].begin(), lists[k].end());
+    }
+    start[5] = flat.size();
+    if (flat.size() > P->class_cap) {
+        if (P->class_scenes) cudaFree(P->class_scenes);
+        P->class_scenes = nullptr;
+        P->class_cap = 0;
+        LCS_CUDA_TRY(cudaMalloc((void**)&P->class_scenes, 4 * flat.size()));
+        P->class_cap = flat.size();
+        P->class_host.clear();
+    }
+    if (P->class_host != flat) {  // scene lists change only with the scenes' sizes
+        LCS_CUDA_TRY(cudaMemcpyAsync(P->class_scenes, flat.data(), 4 * flat.size(), cudaMemcpyHostToDevice, s0));
+        LCS_CUDA_TRY(cudaStreamSynchronize(s0));
+        P->class_host = flat;
+    }
+    if (!P->class_fork) {
+        LCS_CUDA_TRY(cudaEventCreateWithFlags(&P->class_fork, cudaEventDisableTiming));
+        for (int k = 0; k < 5; ++k) {
+            LCS_CUDA_TRY(cudaStreamCreateWithFlags(&P->class_stream[k], cudaStreamNonBlocking));
+            LCS_CUDA_TRY(cudaEventCreateWithFlags(&P->class_join[k], cudaEventDisableTiming));
+        }
+    }
+    LCS_CUDA_TRY(cudaEventRecord(P->class_fork, s0));
+    for (int k = 0; k < 5; ++k) {
+        const uint32_t m = (uint32_t)(start[k + 1] - start[k]);
+        if (m == 0) continue;
+        LCS_CUDA_TRY(cudaStreamWaitEvent(P->class_stream[k], P->class_fork, 0));
+        LCS_CUDA_TRY(launch(1 << k, m, P->class_scenes + start[k], P->class_stream[k]));
+        lcs_count_launch();
+        LCS_CUDA_TRY(cudaEventRecord(P->class_join[k], P->class_stream[k]));
+        LCS_CUDA_TRY(cudaStreamWaitEvent(s0, P->class_join[k], 0));
+    }
     return LCS_OK;
 }

@@ -206,7 +206,7 @@ def _solve(systems_c, which, cluster):
     return host(x), offs, host(stats)
 
 
-@pytest.mark.parametrize("cluster", [1, 4, 16])
+@pytest.mark.parametrize("cluster", [0, 1, 4, 16])
 def test_batched_pcg_per_scene_matches_oracle_and_is_independent(systems, cluster):
     sysl, c = systems
     x, offs, stats = _solve(systems, [0, 1, 2], cluster)
