@@ -334,6 +334,61 @@ LCS_API int lcs_pcg_solve_batch(lcs_pcg* p, uint32_t n_scenes, const uint32_t* r
                                 lcs_stream stream);
 
 /* ------------------------------------------------------------------------------------------
+ * Cloth energies  (replaces the evaluate kernels of NewtonSolver::compile_evaluate,
+ * Solver/SimulationSolver/newton_solver.cpp:1002-1175, and the elastic energy of the line
+ * search, Solver/SimulationSolver/solver_interface.cpp:505-728)
+ *
+ * Per-element outputs use the reference's layouts: gradients one float4 per (element, local
+ * vertex); Hessians one float3x3 record (three float4 columns) per block, the N diagonal blocks
+ * first, then the off-diagonal blocks (i, j), i != j, in row-major order (row vertex i, column
+ * vertex j): N*N blocks per element.
+ * ------------------------------------------------------------------------------------------ */
+/* ConstitutiveStretchModelCloth / ConstitutiveBendingModelCloth (physical_material.h:11-23) */
+enum { LCS_STRETCH_SPRING = 0, LCS_STRETCH_BW98 = 1 };
+enum { LCS_BENDING_NONE = 0, LCS_BENDING_QUADRATIC = 1, LCS_BENDING_DIHEDRAL = 2 };
+
+/* fn_evaluate_spring (newton_solver.cpp:1002-1050): edges uint2, per-spring rest length and
+ * stiffness; 2 gradients and 4 blocks ((0,0) (1,1) (0,1) (1,0)) per spring. */
+LCS_API int lcs_eval_springs(const float* x, const uint32_t* edges, const float* rest_len, const float* stiffness,
+                             uint32_t n, float* gradients, float* hessians, lcs_stream stream);
+/* fn_evaluate_stretch_face (newton_solver.cpp:1052-1100): Baraff-Witkin stretch + shear with
+ * projected Hessians (stretch_energy.h:156-476).  faces uint4; dm_inv 4 floats per face (the rest
+ * Dm^-1 columns, StretchEnergy::get_Dm_inv); rest_area; mu_lambda 2 floats per face. */
+LCS_API int lcs_eval_stretch_faces(const float* x, const uint32_t* faces, const float* dm_inv, const float* rest_area,
+                                   const float* mu_lambda, uint32_t n, float* gradients, float* hessians,
+                                   lcs_stream stream);
+/* fn_evaluate_bending (newton_solver.cpp:1102-1175): dihedral angle of the hinge (s.x, s.y) with
+ * wings s.z, s.w; gradient k (theta - rest_angle) dtheta/dx, Gauss-Newton blocks k g_i g_j^T with
+ * k = stiffness * scaling * rest_hbar (init_sim_data.cpp:420-448). */
+LCS_API int lcs_eval_bending(const float* x, const uint32_t* stencils, const float* rest_angle, const float* rest_hbar,
+                             const float* stiffness, float scaling, uint32_t n, float* gradients, float* hessians,
+                             lcs_stream stream);
+
+/* The per-element arrays of a cloth system (device pointers), as SimulationData holds them. */
+typedef struct lcs_cloth_elements {
+    uint32_t n_verts, n_springs, n_stretch_faces, n_bending;
+    const float* mass;                 /* per vertex */
+    const uint8_t* is_fixed;           /* per vertex, or NULL */
+    const uint32_t* springs;           /* uint2 */
+    const float* spring_rest_len;
+    const float* spring_stiffness;
+    const uint32_t* stretch_faces;     /* uint4 */
+    const float* stretch_dm_inv;       /* 4 floats per face */
+    const float* stretch_area;
+    const float* stretch_mu_lambda;    /* 2 floats per face */
+    const uint32_t* bending_edges;     /* uint4 stencils */
+    const float* bending_rest_angle;
+    const float* bending_hbar;
+    const float* bending_stiffness;
+    float bending_scaling;             /* stiffness_bending_ui */
+} lcs_cloth_elements;
+/* SolverInterface::device_compute_elastic_energy without the ground term: writes 4 doubles
+ * (device) -- inertia (with the Dirichlet factor on fixed vertices), springs, stretch faces,
+ * bending -- each summed in FP64.  Asynchronous. */
+LCS_API int lcs_material_energy(const lcs_cloth_elements* m, const float* x, const float* x_tilde, float dt,
+                                float stiffness_dirichlet, double* energy, lcs_stream stream);
+
+/* ------------------------------------------------------------------------------------------
  * Newton loop  (replaces NewtonSolver::physics_step_GPU and its contact glue,
  * Solver/SimulationSolver/newton_solver.cpp:3174-3375, 3685-3884, 4051-4345)
  * ------------------------------------------------------------------------------------------ */
@@ -371,6 +426,22 @@ typedef struct lcs_scene_desc {
     float pcg_rel_tol;
     float pcg_abs_rz_tol;
     int32_t pcg_check_every;    /* host check cadence of the plain loop (reference: 25) */
+    /* cloth models (ClothMaterial, physical_material.h:53-62; element culling init_sim_data.cpp:205-270).
+     * stretch_model LCS_STRETCH_SPRING: springs on `edges` with rest_len and spring_k;
+     * LCS_STRETCH_BW98: the stretch faces below.  bending_model LCS_BENDING_DIHEDRAL: the stencils
+     * in `bending` with bending_rest_angle / bending_hbar, stiffness bending_k * bending_scaling * hbar;
+     * LCS_BENDING_QUADRATIC: the rest-relative quadratic form with bending_Q and bending_k (the
+     * reference's disabled branch, newton_solver.cpp:3013-3045); LCS_BENDING_NONE: no bending. */
+    int32_t stretch_model;
+    int32_t bending_model;
+    uint32_t n_stretch_faces;
+    const uint32_t* stretch_faces;   /* host uint4, faces with a free vertex */
+    const float* stretch_dm_inv;     /* host, 4 floats per stretch face (rest Dm^-1 columns) */
+    const float* stretch_area;       /* host, rest area per stretch face */
+    float stretch_mu, stretch_lambda;/* thickness-scaled Lame parameters (init_sim_data.cpp:388-397) */
+    const float* bending_rest_angle; /* host, per stencil */
+    const float* bending_hbar;       /* host, per stencil: (A0 + A1) / (3 |e|) */
+    float bending_scaling;           /* stiffness_bending_ui */
 } lcs_scene_desc;
 
 enum {

@@ -26,6 +26,8 @@ STATUS = {0: "LCS_OK", 1: "LCS_ERR_INVALID", 2: "LCS_ERR_CUDA", 3: "LCS_ERR_CAPA
 LCS_TREE_VERT, LCS_TREE_EDGE, LCS_TREE_FACE = 0, 1, 2
 LCS_CCD_FP64_FINAL, LCS_CCD_FP64 = 1, 2
 LCS_PCG_FP64_DOTS, LCS_PCG_PLAIN, LCS_PCG_NO_STATS, LCS_PCG_ROWS, LCS_PCG_PIPELINED = 1, 2, 4, 8, 16
+LCS_STRETCH_SPRING, LCS_STRETCH_BW98 = 0, 1
+LCS_BENDING_NONE, LCS_BENDING_QUADRATIC, LCS_BENDING_DIHEDRAL = 0, 1, 2
 
 
 class Bsr(C.Structure):
@@ -46,7 +48,18 @@ class SceneDesc(C.Structure):
                 ("bending_k", C.c_float), ("dirichlet", C.c_float), ("damping", C.c_float),
                 ("use_floor", C.c_int32), ("floor_y", C.c_float), ("nonlinear_iters", C.c_int32),
                 ("pcg_max_iter", C.c_int32), ("pcg_rel_tol", C.c_float), ("pcg_abs_rz_tol", C.c_float),
-                ("pcg_check_every", C.c_int32)]
+                ("pcg_check_every", C.c_int32), ("stretch_model", C.c_int32), ("bending_model", C.c_int32),
+                ("n_stretch_faces", C.c_uint32), ("stretch_faces", P), ("stretch_dm_inv", P), ("stretch_area", P),
+                ("stretch_mu", C.c_float), ("stretch_lambda", C.c_float), ("bending_rest_angle", P),
+                ("bending_hbar", P), ("bending_scaling", C.c_float)]
+
+
+class ClothElements(C.Structure):
+    _fields_ = [("n_verts", C.c_uint32), ("n_springs", C.c_uint32), ("n_stretch_faces", C.c_uint32),
+                ("n_bending", C.c_uint32), ("mass", P), ("is_fixed", P), ("springs", P), ("spring_rest_len", P),
+                ("spring_stiffness", P), ("stretch_faces", P), ("stretch_dm_inv", P), ("stretch_area", P),
+                ("stretch_mu_lambda", P), ("bending_edges", P), ("bending_rest_angle", P), ("bending_hbar", P),
+                ("bending_stiffness", P), ("bending_scaling", C.c_float)]
 
 
 class NewtonStats(C.Structure):
@@ -98,6 +111,10 @@ SIGNATURES = {
     "lcs_pcg_device_stats": (P, [P]),
     "lcs_pcg_solve_noalloc": (I32, [U32, P, C.POINTER(Bsr), C.POINTER(Bsr), P, P, C.POINTER(PcgOpts),
                                     C.POINTER(PcgStats), P]),
+    "lcs_eval_springs": (I32, [P, P, P, P, U32, P, P, P]),
+    "lcs_eval_stretch_faces": (I32, [P, P, P, P, P, U32, P, P, P]),
+    "lcs_eval_bending": (I32, [P, P, P, P, P, F32, U32, P, P, P]),
+    "lcs_material_energy": (I32, [C.POINTER(ClothElements), P, P, F32, F32, P, P]),
     "lcs_newton_create": (I32, [C.POINTER(SceneDesc), I32, P, C.POINTER(P)]),
     "lcs_newton_create_batch": (I32, [C.POINTER(SceneDesc), U32, I32, P, I32, C.POINTER(P)]),
     "lcs_newton_num_scenes": (U32, [P]),

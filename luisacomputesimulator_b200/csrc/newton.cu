@@ -29,6 +29,7 @@
 
 #include "lcs_common.cuh"
 #include "lcs_internal.h"
+#include "material.cuh"
 
 using namespace lcs;
 
@@ -239,6 +240,89 @@ __global__ void k_bending(uint32_t nb, const uint4* __restrict__ stencil, const 
     }
 }
 
+// one 16-byte vector atomic (sm_90 and later) per vertex record
+__device__ __forceinline__ void red4(float4* p, float x, float y, float z) { atomicAdd(p, make_float4(x, y, z, 0.0f)); }
+
+// adds the 3x3 block K (column-major [3 c + r]) into a diagonal record (three float4 columns)
+__device__ __forceinline__ void red_diag(float4* D, const float* K)
+{
+#pragma unroll
+    for (int c = 0; c < 3; ++c) red4(D + c, K[3 * c], K[3 * c + 1], K[3 * c + 2]);
+}
+// adds K (or its transpose) into an off-diagonal block whose component 3 c + r sits at O[cs (3 c + r)]
+__device__ __forceinline__ void red_off(float* O, uint32_t cs, const float* K, bool t)
+{
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < 3; ++r) atomicAdd(O + cs * (3 * c + r), t ? K[3 * r + c] : K[3 * c + r]);
+}
+
+// fn_evaluate_stretch_face + fn_material_energy_assembly_stretch_face (newton_solver.cpp:1052-1100,
+// 705-789): Baraff-Witkin stretch and shear added straight into b, the diagonal and the material
+// blocks; slots: the 6 off-diagonal blocks (0,1) (0,2) (1,0) (1,2) (2,0) (2,1) of each face
+__global__ void k_stretch_bw98(uint32_t nf, const uint4* __restrict__ faces, const float4* __restrict__ dm,
+                               const float* __restrict__ area, float mu, float lambda, const float4* __restrict__ x,
+                               float4* b, float4* diag, const uint32_t* __restrict__ slots, uint32_t cs, float* mat_val)
+{
+    for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x) {
+        const uint4 fc = faces[f];
+        Bw98Out o;
+        bw98_face(ld3(x, fc.x), ld3(x, fc.y), ld3(x, fc.z), dm[f], mu, lambda, area[f], o);
+        const uint32_t v[3] = {fc.x, fc.y, fc.z};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            red4(&b[v[a]], -o.g[a].x, -o.g[a].y, -o.g[a].z);
+            red_diag(diag + 3 * (size_t)v[a], o.K[a]);
+        }
+        const uint32_t* sl = slots + 6 * (size_t)f;
+        red_off(mat_val + sl[0], cs, o.K[3], false);  // (0,1)
+        red_off(mat_val + sl[1], cs, o.K[4], false);  // (0,2)
+        red_off(mat_val + sl[2], cs, o.K[3], true);   // (1,0)
+        red_off(mat_val + sl[3], cs, o.K[5], false);  // (1,2)
+        red_off(mat_val + sl[4], cs, o.K[4], true);   // (2,0)
+        red_off(mat_val + sl[5], cs, o.K[5], true);   // (2,1)
+    }
+}
+
+// fn_evaluate_bending + fn_material_energy_assembly_bending (newton_solver.cpp:1102-1175, 790-801):
+// dihedral-angle bending, Gauss-Newton blocks k g_i g_j^T; slots as k_bending
+__global__ void k_bending_dihedral(uint32_t nb, const uint4* __restrict__ stencil, const float* __restrict__ rest_angle,
+                                   const float* __restrict__ hbar, float k_area, const float4* __restrict__ x,
+                                   float4* b, float4* diag, const uint32_t* __restrict__ slots, uint32_t cs,
+                                   float* mat_val)
+{
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nb; s += gridDim.x * blockDim.x) {
+        const uint4 e = stencil[s];
+        const uint32_t v[4] = {e.x, e.y, e.z, e.w};
+        v3 g[4];
+        const float theta = dihedral_angle_grad(ld3(x, e.x), ld3(x, e.y), ld3(x, e.z), ld3(x, e.w), g);
+        const float stiff = k_area * hbar[s];
+        const float sd = stiff * (theta - rest_angle[s]);
+        int t = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            red4(&b[v[i]], -(sd * g[i].x), -(sd * g[i].y), -(sd * g[i].z));
+            const float gi[3] = {g[i].x, g[i].y, g[i].z};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float gj[3] = {g[j].x, g[j].y, g[j].z};
+                float K[9];
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int r = 0; r < 3; ++r) K[3 * c + r] = stiff * (gi[r] * gj[c]);
+                if (i == j) {
+                    red_diag(diag + 3 * (size_t)v[i], K);
+                } else {
+                    red_off(mat_val + slots[12 * (size_t)s + t], cs, K, false);
+                    ++t;
+                }
+            }
+        }
+    }
+}
+
 // fn_apply_dx (newton_solver.cpp:491-503) with alpha = 1, and the |dx|_inf of the small-step test
 __global__ void k_apply_unit(uint32_t n, const float4* __restrict__ x0, const float4* __restrict__ dx, float4* __restrict__ x,
                              Status* st)
@@ -413,6 +497,10 @@ struct lcs_newton {
     uint4* faces = nullptr;
     uint2* edges = nullptr;
     uint4* bend = nullptr;
+    uint4* sfaces = nullptr;        // BW98 stretch faces
+    float4* dm = nullptr;           // their rest Dm^-1
+    float *sarea = nullptr, *rest_angle = nullptr, *hbar = nullptr;
+    uint32_t Fs = 0;
     float *Q = nullptr, *rest_len = nullptr, *vert_area = nullptr, *face_area = nullptr, *edge_area = nullptr;
     float *mass = nullptr, *dhat = nullptr, *offset = nullptr;
     uint32_t* body = nullptr;
@@ -423,7 +511,7 @@ struct lcs_newton {
     float4 *target = nullptr, *dx = nullptr, *b = nullptr, *diag = nullptr;
     // material BSR
     uint32_t nnz_mat = 0;
-    uint32_t *mat_rp = nullptr, *mat_col = nullptr, *spring_slots = nullptr, *bend_slots = nullptr;
+    uint32_t *mat_rp = nullptr, *mat_col = nullptr, *spring_slots = nullptr, *bend_slots = nullptr, *face_slots = nullptr;
     float* mat_val = nullptr;
     bool sell = false;             // material matrix in SELL-32 for the row-resident PCG (fused mode)
     bool pipelined = false;        // pipelined row-resident PCG (one grid synchronisation per iteration)
@@ -521,8 +609,6 @@ int alloc_contact(lcs_newton* h)
     return e == cudaSuccess ? LCS_OK : lcs_fail(LCS_ERR_CUDA, "lcs_newton: contact buffer allocation failed");
 }
 
-// material off-diagonal pattern: springs (both directions) + every ordered pair of each
-// bending stencil; slots of each contribution found by binary search in the sorted rows
 // runs f(begin, end) over [0, n) on the host's cores
 template <typename F>
 void parallel_ranges(size_t n, F f)
@@ -542,18 +628,28 @@ void parallel_ranges(size_t n, F f)
     for (auto& th : pool) th.join();
 }
 
+// material off-diagonal pattern from the element contributions; the slot of each contribution
+// is its column's position in its sorted, de-duplicated row
 int build_material_pattern(lcs_newton* h, const lcs_scene_desc* d)
 {
-    // contributions: key k < 2E is spring k/2 (a->c, then c->a); the rest are the ordered pairs
-    // (i, j), i != j, of each bending stencil, 12 per stencil
-    const size_t KE = 2 * (size_t)h->E, K = KE + 12 * (size_t)h->B;
+    // contributions, in three ranges: spring k/2 (a->c, then c->a) when the stretch model is the
+    // spring model; the ordered pairs (i, j), i != j, of each stretch face (6 per face) for BW98;
+    // the ordered pairs of each bending stencil (12 per stencil) unless bending is off
+    const size_t KS = h->d.stretch_model == LCS_STRETCH_SPRING ? 2 * (size_t)h->E : 0;
+    const size_t KF = h->d.stretch_model == LCS_STRETCH_BW98 ? 6 * (size_t)h->Fs : 0;
+    const size_t KB = h->d.bending_model != LCS_BENDING_NONE ? 12 * (size_t)h->B : 0;
+    const size_t K = KS + KF + KB;
     auto key_rc = [&](size_t k, uint32_t& r, uint32_t& c) {
-        if (k < KE) {
+        if (k < KS) {
             const uint32_t* e = d->edges + 2 * (k >> 1);
             r = e[k & 1];
             c = e[(k & 1) ^ 1];
+        } else if (k < KS + KF) {
+            const size_t q = k - KS, f = q / 6, m = q % 6, i = m / 2, jj = m % 2, j = jj < i ? jj : jj + 1;
+            r = d->stretch_faces[4 * f + i];
+            c = d->stretch_faces[4 * f + j];
         } else {
-            const size_t q = k - KE, st = q / 12, m = q % 12, i = m / 3, jj = m % 3, j = jj < i ? jj : jj + 1;
+            const size_t q = k - KS - KF, st = q / 12, m = q % 12, i = m / 3, jj = m % 3, j = jj < i ? jj : jj + 1;
             r = d->bending[4 * st + i];
             c = d->bending[4 * st + j];
         }
@@ -629,16 +725,18 @@ int build_material_pattern(lcs_newton* h, const lcs_scene_desc* d)
         for (size_t j = 0; j < nnz; ++j) base[j] = (uint32_t)(9 * j);
         h->sell_vals = 9ull * nnz;
     }
-    std::vector<uint32_t> ss(KE ? KE : 1), bs(K - KE ? K - KE : 1);
+    std::vector<uint32_t> ss(KS ? KS : 1), fs(KF ? KF : 1), bs(KB ? KB : 1);
     parallel_ranges(K, [&](size_t kb, size_t ke) {
         for (size_t k = kb; k < ke; ++k) {
             const uint32_t v = base[slot_of(k)];
-            if (k < KE) ss[k] = v;
-            else bs[k - KE] = v;
+            if (k < KS) ss[k] = v;
+            else if (k < KS + KF) fs[k - KS] = v;
+            else bs[k - KS - KF] = v;
         }
     });
     if (upload(h->mat_rp, rp.data(), rp.size()) != cudaSuccess || upload(h->mat_col, col.data(), col.size()) != cudaSuccess ||
         upload(h->spring_slots, ss.data(), ss.size()) != cudaSuccess ||
+        upload(h->face_slots, fs.data(), fs.size()) != cudaSuccess ||
         upload(h->bend_slots, bs.data(), bs.size()) != cudaSuccess || dalloc(h->mat_val, h->sell_vals) != cudaSuccess)
         return lcs_fail(LCS_ERR_CUDA, "lcs_newton: material pattern upload failed");
     if (h->sell && (upload(h->sell_ptr, sell_ptr.data(), sell_ptr.size()) != cudaSuccess ||
@@ -797,14 +895,26 @@ int newton_iteration(lcs_newton* h)
                                           h->diag, d.use_floor, d.floor_y, d.kappa, h->vert_area, h->dhat, h->offset);
         lcs_count_launch();
         LCS_CUDA_TRY(cudaMemsetAsync(h->mat_val, 0, sizeof(float) * h->sell_vals, h->s));
-        if (h->E) {
+        const uint32_t cs = h->sell ? 128u : 1u;
+        if (h->E && d.stretch_model == LCS_STRETCH_SPRING) {
             k_springs<<<G(h->E), 256, 0, h->s>>>(h->E, h->edges, h->rest_len, d.spring_k, h->x, h->b, h->diag,
-                                                 h->spring_slots, h->sell ? 128u : 1u, h->mat_val);
+                                                 h->spring_slots, cs, h->mat_val);
             lcs_count_launch();
         }
-        if (h->B) {
+        if (h->Fs && d.stretch_model == LCS_STRETCH_BW98) {
+            k_stretch_bw98<<<G(h->Fs), 256, 0, h->s>>>(h->Fs, h->sfaces, h->dm, h->sarea, d.stretch_mu,
+                                                       d.stretch_lambda, h->x, h->b, h->diag, h->face_slots, cs,
+                                                       h->mat_val);
+            lcs_count_launch();
+        }
+        if (h->B && d.bending_model == LCS_BENDING_DIHEDRAL) {
+            k_bending_dihedral<<<G(h->B), 256, 0, h->s>>>(h->B, h->bend, h->rest_angle, h->hbar,
+                                                          d.bending_k * d.bending_scaling, h->x, h->b, h->diag,
+                                                          h->bend_slots, cs, h->mat_val);
+            lcs_count_launch();
+        } else if (h->B && d.bending_model == LCS_BENDING_QUADRATIC) {
             k_bending<<<G(h->B), 256, 0, h->s>>>(h->B, h->bend, h->Q, d.bending_k, h->x, h->rest, h->b, h->diag,
-                                                 h->bend_slots, h->sell ? 128u : 1u, h->mat_val);
+                                                 h->bend_slots, cs, h->mat_val);
             lcs_count_launch();
         }
         // update_contact_set (newton_solver.cpp:4093-4104)
@@ -970,6 +1080,25 @@ int newton_iteration(lcs_newton* h)
 
 namespace {
 int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batch, lcs_newton** out);
+
+// the element arrays the selected cloth models need
+int check_models(const lcs_scene_desc& d)
+{
+    if (d.stretch_model != LCS_STRETCH_SPRING && d.stretch_model != LCS_STRETCH_BW98)
+        return lcs_fail(LCS_ERR_INVALID, "lcs_newton: unknown stretch model");
+    if (d.bending_model != LCS_BENDING_NONE && d.bending_model != LCS_BENDING_QUADRATIC &&
+        d.bending_model != LCS_BENDING_DIHEDRAL)
+        return lcs_fail(LCS_ERR_INVALID, "lcs_newton: unknown bending model");
+    if (d.stretch_model == LCS_STRETCH_BW98 && d.n_stretch_faces &&
+        (!d.stretch_faces || !d.stretch_dm_inv || !d.stretch_area))
+        return lcs_fail(LCS_ERR_INVALID, "lcs_newton: BW98 stretch needs stretch_faces, stretch_dm_inv, stretch_area");
+    if (d.n_bending && !d.bending) return lcs_fail(LCS_ERR_INVALID, "lcs_newton: bending stencils missing");
+    if (d.n_bending && d.bending_model == LCS_BENDING_QUADRATIC && !d.bending_Q)
+        return lcs_fail(LCS_ERR_INVALID, "lcs_newton: quadratic bending needs bending_Q");
+    if (d.n_bending && d.bending_model == LCS_BENDING_DIHEDRAL && (!d.bending_rest_angle || !d.bending_hbar))
+        return lcs_fail(LCS_ERR_INVALID, "lcs_newton: dihedral bending needs bending_rest_angle and bending_hbar");
+    return LCS_OK;
+}
 }
 
 extern "C" int lcs_newton_create(const lcs_scene_desc* d, int flags, lcs_stream stream, lcs_newton** out)
@@ -981,9 +1110,9 @@ namespace {
 int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batch, lcs_newton** out)
 {
     if (!d || !out || !d->x || !d->faces || !d->edges || !d->mass || !d->d_hat || !d->offset || !d->vert_area ||
-        !d->face_area || !d->edge_area || d->n_verts == 0 || (d->n_bending && (!d->bending || !d->bending_Q)) ||
-        (d->n_edges && !d->rest_len))
+        !d->face_area || !d->edge_area || d->n_verts == 0 || (d->n_edges && !d->rest_len))
         return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create: incomplete scene description");
+    if (int rc = check_models(*d)) return rc;
     lcs_newton* h = new (std::nothrow) lcs_newton();
     if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create: out of host memory");
     h->d = *d;
@@ -1010,7 +1139,17 @@ int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batc
     A(upload(h->faces, reinterpret_cast<const uint4*>(d->faces), h->F));
     A(upload(h->edges, reinterpret_cast<const uint2*>(d->edges), h->E));
     A(upload(h->bend, reinterpret_cast<const uint4*>(d->bending), h->B));
-    A(upload(h->Q, d->bending_Q, 16 * (size_t)h->B));
+    if (d->bending_model == LCS_BENDING_QUADRATIC) A(upload(h->Q, d->bending_Q, 16 * (size_t)h->B));
+    if (d->bending_model == LCS_BENDING_DIHEDRAL) {
+        A(upload(h->rest_angle, d->bending_rest_angle, h->B));
+        A(upload(h->hbar, d->bending_hbar, h->B));
+    }
+    if (d->stretch_model == LCS_STRETCH_BW98) {
+        h->Fs = d->n_stretch_faces;
+        A(upload(h->sfaces, reinterpret_cast<const uint4*>(d->stretch_faces), h->Fs));
+        A(upload(h->dm, reinterpret_cast<const float4*>(d->stretch_dm_inv), h->Fs));
+        A(upload(h->sarea, d->stretch_area, h->Fs));
+    }
     A(upload(h->rest_len, d->rest_len, h->E));
     A(upload(h->vert_area, d->vert_area, V));
     A(upload(h->face_area, d->face_area, h->F));
@@ -1096,14 +1235,19 @@ extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_s
         return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: cluster size must be 0 (auto), 1, 2, 4, 8 or 16");
     const lcs_scene_desc& d0 = descs[0];
     // concatenate the scenes: indices shifted by the vertex offset, animation groups renumbered
-    std::vector<uint32_t> voff(n_scenes + 1, 0), foff(n_scenes + 1, 0), eoff(n_scenes + 1, 0), boff(n_scenes + 1, 0);
+    std::vector<uint32_t> voff(n_scenes + 1, 0), foff(n_scenes + 1, 0), eoff(n_scenes + 1, 0), boff(n_scenes + 1, 0),
+        soff(n_scenes + 1, 0);
     uint32_t groups = 0;
     for (uint32_t s = 0; s < n_scenes; ++s) {
         const lcs_scene_desc& d = descs[s];
         if (!d.x || !d.faces || !d.edges || !d.mass || !d.d_hat || !d.offset || !d.vert_area || !d.face_area ||
-            !d.edge_area || d.n_verts == 0 || d.n_faces < 2 || d.n_edges < 2 ||
-            (d.n_bending && (!d.bending || !d.bending_Q)) || !d.rest_len)
+            !d.edge_area || d.n_verts == 0 || d.n_faces < 2 || d.n_edges < 2 || !d.rest_len)
             return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: incomplete scene description");
+        if (int rc = check_models(d)) return rc;
+        if (d.stretch_model != d0.stretch_model || d.bending_model != d0.bending_model ||
+            d.stretch_mu != d0.stretch_mu || d.stretch_lambda != d0.stretch_lambda ||
+            d.bending_scaling != d0.bending_scaling)
+            return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: scenes must share the cloth models and parameters");
         if (d.dt != d0.dt || d.gravity[0] != d0.gravity[0] || d.gravity[1] != d0.gravity[1] ||
             d.gravity[2] != d0.gravity[2] || d.kappa != d0.kappa || d.spring_k != d0.spring_k ||
             d.bending_k != d0.bending_k || d.dirichlet != d0.dirichlet || d.damping != d0.damping ||
@@ -1115,11 +1259,15 @@ extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_s
         foff[s + 1] = foff[s] + d.n_faces;
         eoff[s + 1] = eoff[s] + d.n_edges;
         boff[s + 1] = boff[s] + d.n_bending;
+        soff[s + 1] = soff[s] + (d.stretch_model == LCS_STRETCH_BW98 ? d.n_stretch_faces : 0);
         groups += d.anim_group ? d.n_anim : 0;
     }
     if (groups > 127) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: more than 127 animation groups");
-    const uint32_t V = voff[n_scenes], F = foff[n_scenes], E = eoff[n_scenes], B = boff[n_scenes];
-    std::vector<float> x(4 * (size_t)V), v(4 * (size_t)V, 0.0f), Q(16 * (size_t)B), rest_len(E), vert_area(V),
+    const uint32_t V = voff[n_scenes], F = foff[n_scenes], E = eoff[n_scenes], B = boff[n_scenes], Fs = soff[n_scenes];
+    const bool quad = d0.bending_model == LCS_BENDING_QUADRATIC, dih = d0.bending_model == LCS_BENDING_DIHEDRAL;
+    std::vector<uint32_t> sfaces(4 * (size_t)Fs);
+    std::vector<float> dm(4 * (size_t)Fs), sarea(Fs), rest_angle(dih ? B : 0), hbar(dih ? B : 0);
+    std::vector<float> x(4 * (size_t)V), v(4 * (size_t)V, 0.0f), Q(quad ? 16 * (size_t)B : 0), rest_len(E), vert_area(V),
         face_area(F), edge_area(E), mass(V), dhat(V), offset(V), anim(8 * (size_t)std::max(groups, 1u), 0.0f);
     std::vector<uint32_t> faces(4 * (size_t)F), edges(2 * (size_t)E), bend(4 * (size_t)B), body(V, kInvalid);
     std::vector<uint8_t> pinned(V, 0);
@@ -1134,7 +1282,18 @@ extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_s
             faces[4 * (size_t)foff[s] + k] = (k % 4 == 3) ? d.faces[k] : d.faces[k] + vo;
         for (size_t k = 0; k < 2 * (size_t)d.n_edges; ++k) edges[2 * (size_t)eoff[s] + k] = d.edges[k] + vo;
         for (size_t k = 0; k < 4 * (size_t)d.n_bending; ++k) bend[4 * (size_t)boff[s] + k] = d.bending[k] + vo;
-        if (d.n_bending) std::memcpy(&Q[16 * (size_t)boff[s]], d.bending_Q, 64 * (size_t)d.n_bending);
+        if (d.n_bending && quad) std::memcpy(&Q[16 * (size_t)boff[s]], d.bending_Q, 64 * (size_t)d.n_bending);
+        if (d.n_bending && dih) {
+            std::memcpy(&rest_angle[boff[s]], d.bending_rest_angle, 4 * (size_t)d.n_bending);
+            std::memcpy(&hbar[boff[s]], d.bending_hbar, 4 * (size_t)d.n_bending);
+        }
+        const uint32_t ns = soff[s + 1] - soff[s];
+        for (size_t k = 0; k < 4 * (size_t)ns; ++k)
+            sfaces[4 * (size_t)soff[s] + k] = (k % 4 == 3) ? d.stretch_faces[k] : d.stretch_faces[k] + vo;
+        if (ns) {
+            std::memcpy(&dm[4 * (size_t)soff[s]], d.stretch_dm_inv, 16 * (size_t)ns);
+            std::memcpy(&sarea[soff[s]], d.stretch_area, 4 * (size_t)ns);
+        }
         std::memcpy(&rest_len[eoff[s]], d.rest_len, 4 * (size_t)d.n_edges);
         std::memcpy(&vert_area[vo], d.vert_area, 4 * (size_t)d.n_verts);
         std::memcpy(&face_area[foff[s]], d.face_area, 4 * (size_t)d.n_faces);
@@ -1155,6 +1314,8 @@ extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_s
     D.n_verts = V; D.n_faces = F; D.n_edges = E; D.n_bending = B;
     D.x = x.data(); D.v = v.data(); D.faces = faces.data(); D.edges = edges.data(); D.bending = bend.data();
     D.bending_Q = Q.data(); D.rest_len = rest_len.data(); D.vert_area = vert_area.data();
+    D.n_stretch_faces = Fs; D.stretch_faces = sfaces.data(); D.stretch_dm_inv = dm.data(); D.stretch_area = sarea.data();
+    D.bending_rest_angle = rest_angle.data(); D.bending_hbar = hbar.data();
     D.face_area = face_area.data(); D.edge_area = edge_area.data(); D.mass = mass.data(); D.d_hat = dhat.data();
     D.offset = offset.data(); D.body = body.data(); D.pinned = pinned.data();
     D.anim_group = groups ? group.data() : nullptr; D.n_anim = groups; D.anim = groups ? anim.data() : nullptr;
@@ -1244,7 +1405,8 @@ extern "C" int lcs_newton_destroy(lcs_newton* h)
         if (h->h_bsc) cudaFreeHost(h->h_bsc);
         if (h->h_bpcg) cudaFreeHost(h->h_bpcg);
     }
-    void* ptrs[] = {h->faces, h->edges, h->bend, h->Q, h->rest_len, h->vert_area, h->face_area, h->edge_area,
+    void* ptrs[] = {h->faces, h->edges, h->bend, h->sfaces, h->dm, h->sarea, h->rest_angle, h->hbar, h->face_slots,
+                    h->Q, h->rest_len, h->vert_area, h->face_area, h->edge_area,
                     h->mass, h->dhat, h->offset, h->body, h->pinned, h->group, h->anim, h->rest, h->x, h->v,
                     h->x_step, h->x_iter, h->x_tilde, h->target, h->dx, h->b, h->diag, h->mat_rp, h->mat_col,
                     h->spring_slots, h->bend_slots, h->mat_val, h->st, h->sell_ptr, h->sell_col, h->prev_ccd};

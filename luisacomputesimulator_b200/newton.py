@@ -59,6 +59,15 @@ def scene_desc(sc, keep, nonlinear_iters=3, pcg_max_iter=100, pcg_rel_tol=1e-4, 
     d.use_floor, d.floor_y = int(use_floor), floor_y
     d.nonlinear_iters, d.pcg_max_iter = nonlinear_iters, pcg_max_iter
     d.pcg_rel_tol, d.pcg_abs_rz_tol, d.pcg_check_every = pcg_rel_tol, pcg_abs_rz_tol, pcg_check_every
+    d.stretch_model, d.bending_model = sc.stretch_model, sc.bending_model
+    d.n_stretch_faces = sc.stretch_faces.shape[0]
+    d.stretch_faces = arr(sc.stretch_faces, np.uint32)
+    d.stretch_dm_inv = arr(sc.stretch_dm_inv, np.float32)
+    d.stretch_area = arr(sc.stretch_area, np.float32)
+    d.stretch_mu, d.stretch_lambda = sc.stretch_mu, sc.stretch_lambda
+    d.bending_rest_angle = arr(sc.bending_rest_angle, np.float32)
+    d.bending_hbar = arr(sc.bending_hbar, np.float32)
+    d.bending_scaling = sc.bending_scaling
     return d
 
 

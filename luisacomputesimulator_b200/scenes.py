@@ -14,7 +14,15 @@ reference's initialisers derive it:
   smallest rest edge length / triangle altitude of the mesh
   (Solver/Initializer/init_collision_data.cpp:67-171);
 * pinned vertices and their animated targets (Solver/Initializer/init_mesh_data.cpp:116-170,
-  Solver/SimulationSolver/solver_interface.cpp:130-162).
+  Solver/SimulationSolver/solver_interface.cpp:130-162);
+* the cloth material of ClothMaterial's defaults (Solver/SimulationCore/physical_material.h:53-62):
+  Baraff-Witkin stretch faces with rest Dm^-1 (StretchEnergy::get_Dm_inv, Solver/Energy/stretch_energy.h:424-438),
+  rest area and mu = lambda = E / (2 (1 + nu)) resp. E nu / ((1 + nu)(1 - 2 nu)) scaled by the thickness
+  (E = 1e5, nu = 0.25, thickness 2e-3: 80 each; Solver/Initializer/init_sim_data.cpp:370-397), and
+  dihedral bending with the rest angle and h_bar = (A0 + A1) / (3 |e|) per stencil
+  (init_sim_data.cpp:400-448).  Elements whose vertices are all pinned are dropped
+  (init_sim_data.cpp:205-270).  The material thickness only scales the stiffnesses; the contact
+  thickness of a mesh part is separate (0 in the benchmark configurations).
 """
 from __future__ import annotations
 
@@ -59,6 +67,17 @@ class Scene:
     bending_k: float = 5e-3
     dirichlet: float = 1e9
     anims: list = dataclasses.field(default_factory=list)  # (vertex ids, center, axis, omega)
+    # cloth material (ConstitutiveStretchModelCloth / ConstitutiveBendingModelCloth values)
+    stretch_model: int = 1                # 0 spring, 1 BW98
+    bending_model: int = 2                # 0 none, 1 quadratic, 2 dihedral
+    stretch_faces: np.ndarray = None      # (Fs, 4) uint32
+    stretch_dm_inv: np.ndarray = None     # (Fs, 4) float32: rest Dm^-1 columns
+    stretch_area: np.ndarray = None       # (Fs,) float32
+    stretch_mu: float = 80.0
+    stretch_lambda: float = 80.0
+    bending_rest_angle: np.ndarray = None  # (B,) float32
+    bending_hbar: np.ndarray = None        # (B,) float32
+    bending_scaling: float = 1.0           # stiffness_bending_ui
 
     @property
     def num_verts(self):
@@ -218,6 +237,52 @@ def _bending_Q(x, bend):
     return Q.astype(np.float32)
 
 
+def lame(youngs_modulus=1e5, poisson_ratio=0.25, thickness=2e-3):
+    """StretchEnergy::convert_prop (stretch_energy.h:418-423) scaled by the thickness, as float32."""
+    mu = youngs_modulus / (2.0 * (1.0 + poisson_ratio))
+    lam = youngs_modulus * poisson_ratio / ((1.0 + poisson_ratio) * (1.0 - 2.0 * poisson_ratio))
+    return float(np.float32(np.float32(thickness) * mu)), float(np.float32(np.float32(thickness) * lam))
+
+
+def _dm_inv(x, faces):
+    """StretchEnergy::get_Dm_inv per face: the 2D rest edge matrix in the triangle's own frame,
+    inverted; 4 floats per face = its columns."""
+    x = x.astype(np.float64)
+    x0, x1, x2 = x[faces[:, 0]], x[faces[:, 1]], x[faces[:, 2]]
+    r1, r2 = x1 - x0, x2 - x0
+    n = np.cross(r1, r2)
+    a1 = r1 / np.linalg.norm(r1, axis=1)[:, None]
+    a2 = np.cross(n, a1)
+    a2 = a2 / np.linalg.norm(a2, axis=1)[:, None]
+    uv = [np.stack([np.einsum("ij,ij->i", a1, p), np.einsum("ij,ij->i", a2, p)], 1) for p in (x0, x1, x2)]
+    d0, d1 = uv[1] - uv[0], uv[2] - uv[0]          # columns of Dm
+    a, b, c, d = d0[:, 0], d0[:, 1], d1[:, 0], d1[:, 1]
+    det = a * d - c * b
+    return np.stack([d / det, -b / det, -c / det, a / det], 1).astype(np.float32)
+
+
+def dihedral_angle(p0, p1, p2, p3):
+    """Signed dihedral angle of hinge (p0, p1) with wings p2, p3 (face_dihedral_angle(p2, p1, p0, p3),
+    bending_energy.h:222-231), float32."""
+    f = np.float32
+    n1 = np.cross(p1 - p2, p0 - p2).astype(f)
+    n2 = np.cross(p0 - p3, p1 - p3).astype(f)
+    c = np.einsum("ij,ij->i", n1, n2) / np.sqrt(np.einsum("ij,ij->i", n1, n1) * np.einsum("ij,ij->i", n2, n2))
+    ang = np.arccos(np.clip(c, f(-1), f(1))).astype(f)
+    return (np.sign(np.einsum("ij,ij->i", np.cross(n2, n1), p1 - p0)) * ang).astype(f)
+
+
+def _dihedral_rest(x, bend):
+    """Rest angle and h_bar = (A0 + A1) / (3 |e|) per stencil (init_sim_data.cpp:420-436)."""
+    x = x.astype(np.float32)
+    p = [x[bend[:, k]] for k in range(4)]
+    ang = dihedral_angle(*p)
+    a0 = np.linalg.norm(np.cross(p[1] - p[0], p[2] - p[0]), axis=1) * np.float32(0.5)
+    a1 = np.linalg.norm(np.cross(p[1] - p[0], p[3] - p[0]), axis=1) * np.float32(0.5)
+    l0 = np.linalg.norm(p[0] - p[1], axis=1)
+    return ang.astype(np.float32), ((a0 + a1) / (np.float32(3.0) * l0)).astype(np.float32)
+
+
 def _min_rest_dist(x, faces, edges):
     x = x.astype(np.float32)
     lens = np.linalg.norm(x[edges[:, 0]] - x[edges[:, 1]], axis=1)
@@ -232,7 +297,8 @@ def _min_rest_dist(x, faces, edges):
     return best
 
 
-def assemble(name, parts, dt, gravity, kappa, spring_k=1e4, bending_k=5e-3, bodies=None):
+def assemble(name, parts, dt, gravity, kappa, spring_k=None, bending_k=5e-3, bodies=None, stretch_model=1,
+             bending_model=2):
     """Merge mesh parts into one Scene (vertex/face order = part order)."""
     xs, fs, pins, vmesh, anims = [], [], [], [], []
     off = 0
@@ -285,11 +351,23 @@ def assemble(name, parts, dt, gravity, kappa, spring_k=1e4, bending_k=5e-3, bodi
     f4[:, :3] = faces
     body = np.full(V, 0xFFFFFFFF, np.uint32) if bodies is None else bodies.astype(np.uint32)
     rest_len = np.linalg.norm(x3[edges[:, 0]] - x3[edges[:, 1]], axis=1).astype(np.float32)
-    return Scene(name=name, x=x4, faces=f4, edges=edges.astype(np.uint32), bending=bending,
+    pinned = np.concatenate(pins).astype(np.uint8)
+    # elements with a free vertex (init_sim_data.cpp:205-270)
+    free = pinned == 0
+    bending = bending[free[bending].any(axis=1)] if len(bending) else bending
+    sf = faces[free[faces].any(axis=1)]
+    sf4 = np.zeros((sf.shape[0], 4), np.uint32)
+    sf4[:, :3] = sf
+    mu, lam = lame()
+    rest_angle, hbar = _dihedral_rest(x3, bending) if len(bending) else (np.zeros(0, np.float32),) * 2
+    return Scene(name=name, x=x4, faces=f4, edges=edges.astype(np.uint32), bending=bending.astype(np.uint32),
                  vert_area=vert_area.astype(np.float32), face_area=face_area, edge_area=edge_area.astype(np.float32),
-                 mass=mass, pinned=np.concatenate(pins).astype(np.uint8), d_hat=d_hat, offset=offset, body=body,
+                 mass=mass, pinned=pinned, d_hat=d_hat, offset=offset, body=body,
                  rest_len=rest_len, bending_Q=_bending_Q(x3, bending), dt=dt, gravity=tuple(gravity), kappa=kappa,
-                 spring_k=spring_k, bending_k=bending_k, anims=anims)
+                 spring_k=mu if spring_k is None else spring_k, bending_k=bending_k, anims=anims,
+                 stretch_model=stretch_model, bending_model=bending_model, stretch_faces=sf4,
+                 stretch_dm_inv=_dm_inv(x3, sf), stretch_area=_face_area(x3, sf), stretch_mu=mu, stretch_lambda=lam,
+                 bending_rest_angle=rest_angle, bending_hbar=hbar)
 
 
 def cloth_on_sphere(n=64, spacing=0.01, seed=0, subdiv=4, radius=0.2, drop=0.05):

@@ -133,6 +133,30 @@ void orc_material_fill(uint32_t V, uint32_t E, uint32_t B, const float* x4, cons
                        const uint32_t* spring_slots, const uint32_t* bend_slots, uint32_t nnz,
                        float* b4, float* diag12, float* val9);
 
+/* ---------------- cloth energies (lcs_oracle_material.c) ---------------- */
+void orc_bw98_face(const float* x0, const float* x1, const float* x2, const float* dm, float mu, float lambda,
+                   float area, float* g9, float* K54);
+float orc_dihedral(const float* p0, const float* p1, const float* p2, const float* p3, float* g12);
+void orc_eval_stretch_faces(uint32_t n, const float* x4, const uint32_t* faces4, const float* dm4, const float* area,
+                            const float* mu_lambda2, float* grad4, float* hess12);
+void orc_eval_bending(uint32_t n, const float* x4, const uint32_t* st4, const float* rest_angle, const float* hbar,
+                      const float* stiffness, float scaling, float* grad4, float* hess12);
+void orc_eval_springs(uint32_t n, const float* x4, const uint32_t* edges2, const float* rest_len,
+                      const float* stiffness, float* grad4, float* hess12);
+void orc_material_energy(uint32_t V, const float* x4, const float* xt4, const float* mass, const uint8_t* fixed,
+                         float dt, float dirichlet, uint32_t E, const uint32_t* springs2, const float* rest_len,
+                         const float* spring_k, uint32_t Fs, const uint32_t* faces4, const float* dm4,
+                         const float* area, const float* mu_lambda2, uint32_t B, const uint32_t* st4,
+                         const float* rest_angle, const float* hbar, const float* bend_k, float scaling, double* out);
+void orc_material_fill2(uint32_t V, const float* x4, const float* rest4, const float* xt4, const float* mass,
+                        const uint8_t* pinned, float dt, float dirichlet, int stretch_model, int bending_model,
+                        uint32_t E, const uint32_t* edges, const float* rest_len, float spring_k, uint32_t Fs,
+                        const uint32_t* sfaces4, const float* dm4, const float* sarea, float mu, float lambda,
+                        uint32_t B, const uint32_t* stencil, const float* Q16, const float* rest_angle,
+                        const float* hbar, float bending_k, float bending_scaling, const uint32_t* spring_slots,
+                        const uint32_t* face_slots, const uint32_t* bend_slots, uint32_t nnz, float* b4,
+                        float* diag12, float* val9);
+
 #ifdef __cplusplus
 }
 #endif

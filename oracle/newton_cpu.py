@@ -3,7 +3,7 @@
 TEST INFRASTRUCTURE ONLY: the timed CPU baseline of bench.py (``cpu_baseline`` and the
 ``--impl reference`` arm) and a checker for the GPU Newton loop.  It follows the loop body of
 NewtonSolver::physics_step_GPU (Solver/SimulationSolver/newton_solver.cpp:4186-4284):
-inertia + springs + quadratic bending, contact set (LBVH build / refit / VF + EE queries,
+inertia + the cloth material (BW98 stretch and dihedral bending by default), contact set (LBVH build / refit / VF + EE queries,
 barrier DCD), contact assembly, Jacobi-PCG, CCD line search, apply.
 """
 from __future__ import annotations
@@ -15,105 +15,56 @@ import numpy as np
 from oracle import oracle as O
 
 
-def material_system(sc, x, x_tilde, dt):
-    """Inertia (+ Dirichlet pinning), springs and rest-relative quadratic bending:
-    b = -grad, diag (V, 3, 4) column-major float4 columns, off-diagonal BSR."""
-    V = sc.num_verts
-    xv = x[:, :3].astype(np.float64)
-    h2 = 1.0 / (dt * dt)
-    m = sc.mass.astype(np.float64)
-    scale = np.where(sc.pinned.astype(bool), 1.0 + sc.dirichlet, 1.0)
-    b = -(m * h2 * scale)[:, None] * (xv - x_tilde[:, :3])
-    D = np.zeros((V, 3, 3))
-    D[:, 0, 0] = D[:, 1, 1] = D[:, 2, 2] = m * h2 * scale
-    # springs (newton_solver.cpp:1003-1045)
-    e = sc.edges.astype(np.int64)
-    d = xv[e[:, 0]] - xv[e[:, 1]]
-    l = np.maximum(np.linalg.norm(d, axis=1), 1.19209290e-7)
-    L = sc.rest_len.astype(np.float64)
-    k = sc.spring_k
-    g = (k * (l - L) / l)[:, None] * d
-    np.add.at(b, e[:, 0], -g)
-    np.add.at(b, e[:, 1], g)
-    xxT = d[:, :, None] * d[:, None, :] / (l * l)[:, None, None]
-    H = k * xxT + (k * np.maximum(1 - L / l, 0))[:, None, None] * (np.eye(3)[None] - xxT)
-    np.add.at(D, e[:, 0], H)
-    np.add.at(D, e[:, 1], H)
-    rows = [e[:, 0], e[:, 1]]
-    cols = [e[:, 1], e[:, 0]]
-    blocks = [-H, -H]
-    # quadratic bending relative to rest (init_sim_data.cpp:455-480)
-    st = sc.bending.astype(np.int64)
-    Q = sc.bending_Q.astype(np.float64) * sc.bending_k
-    u = xv[st] - sc.x[st][:, :, :3].astype(np.float64)  # (B, 4, 3)
-    gb = np.einsum("bij,bjk->bik", Q, u)
-    for i in range(4):
-        np.add.at(b, st[:, i], -gb[:, i])
-        np.add.at(D, st[:, i], Q[:, i, i][:, None, None] * np.eye(3)[None])
-        for j in range(4):
-            if i != j:
-                rows.append(st[:, i])
-                cols.append(st[:, j])
-                blocks.append(Q[:, i, j][:, None, None] * np.eye(3)[None])
-    rows = np.concatenate(rows)
-    cols = np.concatenate(cols)
-    blocks = np.concatenate(blocks)
-    key = rows * V + cols
-    uk, inv = np.unique(key, return_inverse=True)
-    val = np.zeros((len(uk), 3, 3))
-    np.add.at(val, inv, blocks)
-    rp = np.zeros(V + 1, np.int64)
-    np.add.at(rp, (uk // V) + 1, 1)
-    rp = np.cumsum(rp).astype(np.uint32)
-    val9 = np.ascontiguousarray(np.transpose(val, (0, 2, 1)).reshape(-1, 9), np.float32)
-    diag = np.zeros((V, 3, 4), np.float32)
-    diag[:, :, :3] = np.transpose(D, (0, 2, 1))
-    b4 = np.zeros((V, 4), np.float32)
-    b4[:, :3] = b
-    return b4, diag, (rp, (uk % V).astype(np.uint32), val9)
-
-
 class MaterialPattern:
-    """Fixed off-diagonal block pattern of springs + bending stencils (set-up, not timed)."""
+    """Fixed off-diagonal block pattern of the material elements (set-up, not timed): springs (both
+    directions) for the spring model, the 6 ordered vertex pairs of each stretch face for BW98, the 12
+    ordered pairs of each bending stencil unless bending is off; slots = block index of each contribution."""
 
     def __init__(self, sc):
         V = sc.num_verts
-        e = sc.edges.astype(np.int64)
-        st = sc.bending.astype(np.int64)
-        rows = [e[:, 0], e[:, 1]]
-        cols = [e[:, 1], e[:, 0]]
+        e = sc.edges.astype(np.int64) if sc.stretch_model == 0 else np.zeros((0, 2), np.int64)
+        f = sc.stretch_faces[:, :3].astype(np.int64) if sc.stretch_model == 1 else np.zeros((0, 3), np.int64)
+        st = sc.bending.astype(np.int64) if sc.bending_model != 0 else np.zeros((0, 4), np.int64)
         sk = np.stack([e[:, 0] * V + e[:, 1], e[:, 1] * V + e[:, 0]], 1).reshape(-1)
-        bk = []
-        for i in range(4):
-            for j in range(4):
-                if i != j:
-                    bk.append(st[:, i] * V + st[:, j])
-        bk = np.stack(bk, 1).reshape(-1) if len(st) else np.zeros(0, np.int64)
-        uk = np.unique(np.concatenate([sk, bk]))
+        fk = np.stack([f[:, i] * V + f[:, j] for i in range(3) for j in range(3) if i != j], 1).reshape(-1)
+        bk = np.stack([st[:, i] * V + st[:, j] for i in range(4) for j in range(4) if i != j], 1).reshape(-1)
+        uk = np.unique(np.concatenate([sk, fk, bk]))
         self.nnz = len(uk)
         rp = np.zeros(V + 1, np.int64)
         np.add.at(rp, (uk // V) + 1, 1)
         self.rp = np.cumsum(rp).astype(np.uint32)
         self.col = (uk % V).astype(np.uint32)
         self.spring_slots = np.searchsorted(uk, sk).astype(np.uint32)
+        self.face_slots = np.searchsorted(uk, fk).astype(np.uint32)
         self.bend_slots = np.searchsorted(uk, bk).astype(np.uint32)
-        del rows, cols
 
 
 def material_fill(sc, pat, x, x_tilde, dt):
-    """orc_material_fill: the C restatement of the material producers on the fixed pattern."""
+    """orc_material_fill2: inertia (+ Dirichlet pinning) and the scene's stretch and bending models,
+    b = -grad, diagonal (V, 3, 4) float4 columns, off-diagonal BSR on the fixed pattern."""
     V = sc.num_verts
     b = np.zeros((V, 4), np.float32)
     diag = np.zeros((V, 3, 4), np.float32)
-    val = np.zeros((pat.nnz, 9), np.float32)
+    val = np.zeros((max(pat.nnz, 1), 9), np.float32)
     c = np.ascontiguousarray
-    O.lib().orc_material_fill(V, sc.edges.shape[0], sc.bending.shape[0], O._p(O.f4(x)), O._p(c(sc.x, np.float32)),
-                              O._p(O.f4(x_tilde)), O._p(c(sc.mass, np.float32)), O._p(c(sc.pinned, np.uint8)),
-                              float(dt), float(sc.dirichlet), O._p(c(sc.edges, np.uint32)),
-                              O._p(c(sc.rest_len, np.float32)), float(sc.spring_k), O._p(c(sc.bending, np.uint32)),
-                              O._p(c(sc.bending_Q.reshape(-1, 16), np.float32)), float(sc.bending_k),
-                              O._p(pat.spring_slots), O._p(pat.bend_slots), pat.nnz, O._p(b), O._p(diag), O._p(val))
-    return b, diag, (pat.rp, pat.col, val)
+    one = lambda a: a if a.size else np.zeros(1, a.dtype)  # noqa: E731
+    O.lib().orc_material_fill2(
+        V, O._p(O.f4(x)), O._p(c(sc.x, np.float32)), O._p(O.f4(x_tilde)), O._p(c(sc.mass, np.float32)),
+        O._p(c(sc.pinned, np.uint8)), float(dt), float(sc.dirichlet), int(sc.stretch_model), int(sc.bending_model),
+        sc.edges.shape[0], O._p(c(sc.edges, np.uint32)), O._p(c(sc.rest_len, np.float32)), float(sc.spring_k),
+        sc.stretch_faces.shape[0], O._p(one(c(sc.stretch_faces, np.uint32))),
+        O._p(one(c(sc.stretch_dm_inv, np.float32))), O._p(one(c(sc.stretch_area, np.float32))), float(sc.stretch_mu),
+        float(sc.stretch_lambda), sc.bending.shape[0], O._p(one(c(sc.bending, np.uint32))),
+        O._p(one(c(sc.bending_Q.reshape(-1, 16), np.float32))), O._p(one(c(sc.bending_rest_angle, np.float32))),
+        O._p(one(c(sc.bending_hbar, np.float32))), float(sc.bending_k), float(sc.bending_scaling),
+        O._p(one(pat.spring_slots)), O._p(one(pat.face_slots)), O._p(one(pat.bend_slots)), pat.nnz, O._p(b),
+        O._p(diag), O._p(val))
+    return b, diag, (pat.rp, pat.col, val[: pat.nnz])
+
+
+def material_system(sc, x, x_tilde, dt):
+    """material_fill on a freshly built pattern."""
+    return material_fill(sc, MaterialPattern(sc), x, x_tilde, dt)
 
 
 def newton_iteration(sc, x, x_tilde, dt, timings=None, pattern=None):

@@ -82,6 +82,15 @@ def _declare(L):
         "orc_material_fill": (None, [U32, U32, U32, P, P, P, P, P, F32, F32, P, P, F32, P, P, F32, P, P, U32, P, P,
                                      P]),
         "orc_min_distance": (F32, [P, U32, P, U32, P, P, P]),
+        "orc_bw98_face": (None, [P, P, P, P, F32, F32, F32, P, P]),
+        "orc_dihedral": (F32, [P, P, P, P, P]),
+        "orc_eval_stretch_faces": (None, [U32, P, P, P, P, P, P, P]),
+        "orc_eval_bending": (None, [U32, P, P, P, P, P, F32, P, P]),
+        "orc_eval_springs": (None, [U32, P, P, P, P, P, P]),
+        "orc_material_energy": (None, [U32, P, P, P, P, F32, F32, U32, P, P, P, U32, P, P, P, P, U32, P, P, P, P, F32,
+                                       P]),
+        "orc_material_fill2": (None, [U32, P, P, P, P, P, F32, F32, I32, I32, U32, P, P, F32, U32, P, P, P, F32, F32,
+                                      U32, P, P, P, P, F32, F32, P, P, P, U32, P, P, P]),
         "orc_pcg": (I32, [U32, P, P, P, P, P, P, P, P, P, I32, F32, F32, I32, I32, C.POINTER(PcgStats)]),
     }
     for name, (res, args) in sig.items():
@@ -349,3 +358,74 @@ def min_distance(sc, x, radius=5e-3):
     ee = np.ascontiguousarray(ee, np.uint32)
     return lib().orc_min_distance(_p(vf), vf.shape[0], _p(ee), ee.shape[0], _p(x), _p(u4(sc.faces)),
                                   _p(np.ascontiguousarray(sc.edges, np.uint32)))
+
+
+# --------------------------------------------------------------------------- cloth energies
+def eval_stretch_faces(x, faces4, dm4, area, mu_lambda):
+    """orc_eval_stretch_faces: per face 3 gradients (float4) and 9 Hessian blocks (3 float4 columns)."""
+    n = faces4.shape[0]
+    g = np.zeros((n, 3, 4), np.float32)
+    h = np.zeros((n, 9, 3, 4), np.float32)
+    c = np.ascontiguousarray
+    lib().orc_eval_stretch_faces(n, _p(f4(x)), _p(u4(faces4)), _p(c(dm4, np.float32)), _p(c(area, np.float32)),
+                                 _p(c(mu_lambda, np.float32)), _p(g), _p(h))
+    return g, h
+
+
+def eval_bending(x, stencils, rest_angle, hbar, stiffness, scaling):
+    """orc_eval_bending: per stencil 4 gradients and 16 Hessian blocks."""
+    n = stencils.shape[0]
+    g = np.zeros((n, 4, 4), np.float32)
+    h = np.zeros((n, 16, 3, 4), np.float32)
+    c = np.ascontiguousarray
+    lib().orc_eval_bending(n, _p(f4(x)), _p(c(stencils, np.uint32)), _p(c(rest_angle, np.float32)),
+                           _p(c(hbar, np.float32)), _p(c(stiffness, np.float32)), float(scaling), _p(g), _p(h))
+    return g, h
+
+
+def eval_springs(x, edges, rest_len, stiffness):
+    n = edges.shape[0]
+    g = np.zeros((n, 2, 4), np.float32)
+    h = np.zeros((n, 4, 3, 4), np.float32)
+    c = np.ascontiguousarray
+    lib().orc_eval_springs(n, _p(f4(x)), _p(c(edges, np.uint32)), _p(c(rest_len, np.float32)),
+                           _p(c(stiffness, np.float32)), _p(g), _p(h))
+    return g, h
+
+
+def bw98_face(x0, x1, x2, dm, mu, lam, area):
+    """orc_bw98_face on one triangle: gradient (3, 3) and blocks (6, 9) [(0,0) (1,1) (2,2) (0,1) (0,2) (1,2)]."""
+    f = lambda a: np.ascontiguousarray(a, np.float32)  # noqa: E731
+    g = np.zeros(9, np.float32)
+    K = np.zeros(54, np.float32)
+    lib().orc_bw98_face(_p(f(x0)), _p(f(x1)), _p(f(x2)), _p(f(dm)), float(mu), float(lam), float(area), _p(g), _p(K))
+    return g.reshape(3, 3), K.reshape(6, 9)
+
+
+def dihedral(p0, p1, p2, p3):
+    f = lambda a: np.ascontiguousarray(a, np.float32)  # noqa: E731
+    g = np.zeros(12, np.float32)
+    th = lib().orc_dihedral(_p(f(p0)), _p(f(p1)), _p(f(p2)), _p(f(p3)), _p(g))
+    return th, g.reshape(4, 3)
+
+
+def material_energy(sc, x, x_tilde, dt):
+    """orc_material_energy of a scene: [inertia, springs, stretch faces, bending] in double."""
+    c = np.ascontiguousarray
+    out = np.zeros(4, np.float64)
+    spring = sc.stretch_model == 0
+    bw = sc.stretch_model == 1
+    dih = sc.bending_model == 2
+    E = sc.edges.shape[0] if spring else 0
+    Fs = sc.stretch_faces.shape[0] if bw else 0
+    B = sc.bending.shape[0] if dih else 0
+    ml = np.tile(np.float32([sc.stretch_mu, sc.stretch_lambda]), (max(Fs, 1), 1))
+    lib().orc_material_energy(sc.num_verts, _p(f4(x)), _p(f4(x_tilde)), _p(c(sc.mass, np.float32)),
+                              _p(c(sc.pinned, np.uint8)), float(dt), float(sc.dirichlet), E,
+                              _p(c(sc.edges, np.uint32)), _p(c(sc.rest_len, np.float32)),
+                              _p(np.full(max(E, 1), sc.spring_k, np.float32)), Fs, _p(c(sc.stretch_faces, np.uint32)),
+                              _p(c(sc.stretch_dm_inv, np.float32)), _p(c(sc.stretch_area, np.float32)), _p(ml), B,
+                              _p(c(sc.bending, np.uint32)), _p(c(sc.bending_rest_angle, np.float32)),
+                              _p(c(sc.bending_hbar, np.float32)), _p(np.full(max(B, 1), sc.bending_k, np.float32)),
+                              float(sc.bending_scaling), _p(out))
+    return out
