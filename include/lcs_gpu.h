@@ -44,7 +44,8 @@ typedef enum lcs_status {
     LCS_ERR_NAN = 5,            /* NaN / Inf met (PCG rz, barrier stiffness) */
     LCS_ERR_CCD_NOCONVERGE = 6, /* an ACCD pair hit the 10000-iteration cap (toi 0.001) */
     LCS_ERR_TIMEOUT = 7,        /* a bounded device-side wait gave up */
-    LCS_ERR_NO_DEVICE = 8       /* no CUDA device / not an sm_100 device */
+    LCS_ERR_NO_DEVICE = 8,      /* no CUDA device / not an sm_100 device */
+    LCS_ERR_LINESEARCH = 9      /* the energy line search found no decrease above step length 1e-4 */
 } lcs_status;
 
 enum { LCS_TREE_VERT = 0, LCS_TREE_EDGE = 1, LCS_TREE_FACE = 2 };
@@ -449,8 +450,13 @@ enum {
     LCS_NEWTON_FP64 = 2,    /* precision form: FP64 PCG reductions, ACCD step bound in FP64 */
     LCS_NEWTON_PROFILE = 4, /* per-phase CUDA-event timing (lcs_newton_profile) */
     LCS_NEWTON_PCG_PIPELINED = 8, /* fused mode: pipelined row-resident PCG (LCS_PCG_PIPELINED) */
-    LCS_NEWTON_FULL_TRAVERSAL = 16 /* fused mode: every candidate list by a traversal (no DCD filtering of the
+    LCS_NEWTON_FULL_TRAVERSAL = 16, /* fused mode: every candidate list by a traversal (no DCD filtering of the
                                       previous iteration's CCD lists) */
+    LCS_NEWTON_ENERGY_LINESEARCH = 32 /* use_energy_linesearch (scene_params.h:41): after the CCD bound, halve the
+                                         step until the energy (inertia, cloth, barrier of the iteration-start
+                                         pairs; FP64 sums) decreases (newton_solver.cpp:3790-3834).  Single scenes;
+                                         the fused loop evaluates 7 step lengths per launch and decides on the
+                                         device, the plain loop one per host round trip as the reference does. */
 };
 
 typedef struct lcs_newton_stats {
@@ -462,6 +468,8 @@ typedef struct lcs_newton_stats {
     int32_t status;
     int32_t retries;  /* iterations re-run after a buffer grew */
     float host_ms;    /* host wall time of the step */
+    float last_alpha; /* step length of the last iteration (the CCD bound, or the line search's choice) */
+    int32_t ls_halvings; /* step halvings of the energy line search in this step */
 } lcs_newton_stats;
 
 typedef struct lcs_newton lcs_newton;
@@ -485,6 +493,9 @@ LCS_API int lcs_newton_scene_stats(const lcs_newton* h, uint32_t scene, lcs_newt
 /* one scene's x, v (float4 per vertex) to host memory; synchronises the solver's stream */
 LCS_API int lcs_newton_download_scene(const lcs_newton* h, uint32_t scene, float* x_out, float* v_out);
 LCS_API int lcs_newton_destroy(lcs_newton* h);
+/* The last Newton iteration's start positions (sa_x_iter_start), direction (sa_cgX) and the step's
+ * inertial target (sa_x_tilde), float4 per vertex, to host memory (any may be NULL); synchronises. */
+LCS_API int lcs_newton_last_iterate(const lcs_newton* h, float* x_iter_out, float* dx_out, float* x_tilde_out);
 /* NewtonSolver::physics_step_GPU (newton_solver.cpp:4051-4345) on the device-resident state. */
 LCS_API int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats);
 /* The same step with host positions / velocities in and out (float4 per vertex, any may be NULL). */

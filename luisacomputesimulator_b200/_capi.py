@@ -22,7 +22,8 @@ class LcsError(RuntimeError):
 
 
 STATUS = {0: "LCS_OK", 1: "LCS_ERR_INVALID", 2: "LCS_ERR_CUDA", 3: "LCS_ERR_CAPACITY", 4: "LCS_ERR_UNHEALTHY_BVH",
-          5: "LCS_ERR_NAN", 6: "LCS_ERR_CCD_NOCONVERGE", 7: "LCS_ERR_TIMEOUT", 8: "LCS_ERR_NO_DEVICE"}
+          5: "LCS_ERR_NAN", 6: "LCS_ERR_CCD_NOCONVERGE", 7: "LCS_ERR_TIMEOUT", 8: "LCS_ERR_NO_DEVICE",
+          9: "LCS_ERR_LINESEARCH"}
 LCS_TREE_VERT, LCS_TREE_EDGE, LCS_TREE_FACE = 0, 1, 2
 LCS_CCD_FP64_FINAL, LCS_CCD_FP64 = 1, 2
 LCS_PCG_FP64_DOTS, LCS_PCG_PLAIN, LCS_PCG_NO_STATS, LCS_PCG_ROWS, LCS_PCG_PIPELINED = 1, 2, 4, 8, 16
@@ -67,7 +68,7 @@ class NewtonStats(C.Structure):
                 ("last_rel_residual", C.c_float), ("vf_candidates", C.c_uint32), ("ee_candidates", C.c_uint32),
                 ("contact_pairs", C.c_uint32), ("ccd_vf_candidates", C.c_uint32),
                 ("ccd_ee_candidates", C.c_uint32), ("status", C.c_int32), ("retries", C.c_int32),
-                ("host_ms", C.c_float)]
+                ("host_ms", C.c_float), ("last_alpha", C.c_float), ("ls_halvings", C.c_int32)]
 
 
 class PcgStats(C.Structure):
@@ -133,6 +134,7 @@ SIGNATURES = {
     "lcs_pcg_solve_batch": (I32, [P, U32, P, P, P, P, C.POINTER(Bsr), C.POINTER(Bsr), P, P,
                                   C.POINTER(PcgOpts), P, I32, P]),
     "lcs_newton_destroy": (I32, [P]),
+    "lcs_newton_last_iterate": (I32, [P, P, P, P]),
     "lcs_newton_step": (I32, [P, C.POINTER(NewtonStats)]),
     "lcs_newton_step_host": (I32, [P, P, P, P, P, C.POINTER(NewtonStats)]),
     "lcs_newton_state": (I32, [P, C.POINTER(P), C.POINTER(P)]),
@@ -144,6 +146,7 @@ SIGNATURES = {
                                 C.POINTER(C.c_uint32)]),
 }
 LCS_NEWTON_PLAIN, LCS_NEWTON_FP64, LCS_NEWTON_PROFILE, LCS_NEWTON_PCG_PIPELINED, LCS_NEWTON_FULL_TRAVERSAL = 1, 2, 4, 8, 16
+LCS_NEWTON_ENERGY_LINESEARCH = 32
 PHASES = ["build", "material", "dcd_broad", "dcd_narrow", "assembly", "pcg", "ccd_broad", "ccd_narrow", "apply"]
 
 _lib = None

@@ -18,12 +18,6 @@ using namespace lcs;
 
 namespace {
 
-__device__ __forceinline__ uint32_t pair_count(const uint32_t* d_count, uint32_t cap)
-{
-    uint32_t n = *d_count;
-    return n < cap ? n : cap;
-}
-
 // float atomic min valid for either sign
 __device__ __forceinline__ void atomic_min_float(float* addr, float v)
 {
@@ -210,40 +204,6 @@ __global__ void __launch_bounds__(256) k_dcd_ee(const uint2* __restrict__ pairs,
         const uint32_t s = warp_append(d_out_count, emit);
         if (emit && s < out_cap) write_pair(out, s, l.x, l.y, r.x, r.y | 0x80000000u, nrm, k1, k2, stiff, c0, c2);
     }
-}
-
-struct PairView {
-    uint32_t v[4];
-    float w[4];
-    v3 n;
-    float k1, k2, stiff;
-    int type;  // 0 none, 1 VF, 2 EE
-};
-
-// CollisionPairTemplate::get_weight, collision_data.h:308-324
-__device__ __forceinline__ PairView load_pair(const lcs_pair* pairs, uint32_t k)
-{
-    const uint4* r = reinterpret_cast<const uint4*>(pairs + k);
-    const uint4 id = __ldg(r);
-    const float4 a = __ldg(reinterpret_cast<const float4*>(r) + 1);
-    const float4 b = __ldg(reinterpret_cast<const float4*>(r) + 2);
-    PairView P;
-    P.v[0] = id.x & 0x7FFFFFFFu; P.v[1] = id.y & 0x7FFFFFFFu; P.v[2] = id.z & 0x7FFFFFFFu; P.v[3] = id.w & 0x7FFFFFFFu;
-    P.n = mk3(a.x, a.y, a.z);
-    P.stiff = a.w;
-    P.k1 = b.x;
-    P.k2 = b.y;
-    if (id.z >> 31) {
-        P.type = 1;
-        P.w[0] = 1.0f; P.w[1] = -b.z; P.w[2] = -b.w; P.w[3] = b.z + b.w - 1.0f;
-    } else if (id.w >> 31) {
-        P.type = 2;
-        P.w[0] = b.z; P.w[1] = 1.0f - b.z; P.w[2] = -b.w; P.w[3] = b.w - 1.0f;
-    } else {
-        P.type = 0;
-        P.w[0] = P.w[1] = P.w[2] = P.w[3] = 0.0f;
-    }
-    return P;
 }
 
 // fn_perPair_assemble_gradient_hessian (soft bodies), narrow_phase.cpp:2550-2676

@@ -29,6 +29,7 @@
 
 #include "lcs_common.cuh"
 #include "lcs_internal.h"
+#include "lcs_geom.cuh"
 #include "material.cuh"
 
 using namespace lcs;
@@ -43,7 +44,10 @@ struct Status {
     int32_t pcg_iters;
     float pcg_rel;
     int32_t pcg_status;
-    float pad[4];
+    float alpha;      // step length applied: the CCD bound, or the energy line search's choice
+    int32_t ls_iters; // halvings of the accepted step length (energy line search)
+    int32_t ls_state; // energy line search: 0 not run, 1 decided, 2 undecided after this round, 3 failed
+    float pad;
 };
 
 struct Anim {
@@ -341,9 +345,9 @@ __global__ void k_apply_unit(uint32_t n, const float4* __restrict__ x0, const fl
 // apply_final_dx with alpha = the CCD step bound, and the Dirichlet check (newton_solver.cpp:3741-3752, 3858-3882)
 __global__ void k_apply_final(uint32_t n, const float4* __restrict__ x0, const float4* __restrict__ dx,
                               float4* __restrict__ x, const uint8_t* __restrict__ pinned,
-                              const float4* __restrict__ x_tilde, Status* st)
+                              const float4* __restrict__ x_tilde, Status* st, int use_ls_alpha)
 {
-    const float alpha = st->toi;
+    const float alpha = use_ls_alpha ? st->alpha : st->toi;
     float m = 0.0f;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 a = x0[i], d = dx[i];
@@ -406,6 +410,193 @@ __global__ void k_pcg_to_status(const lcs_pcg_stats* ps, Status* st)
     st->pcg_iters = ps->iterations;
     st->pcg_rel = ps->rel_residual;
     st->pcg_status = ps->status;
+}
+
+// ---- energy line search (line_search with use_energy_linesearch, newton_solver.cpp:3790-3834)
+// The reference evaluates the energy at alpha = 0 and then at toi, toi / 2, ... one step length at
+// a time with a host round trip each, and takes the first with E < E(0) + Epsilon; a step length
+// below 1e-4 is an error.  Here one launch evaluates E at alpha = 0 and at kLsSlots - 1 successive
+// halvings together (every element loads its vertices once), and a one-thread kernel picks the
+// step on the device, so the usual case costs no host synchronisation.
+constexpr int kLsSlots = 8;
+
+struct LsArgs {
+    uint32_t V, E, Fs, B, P;  // vertices, springs, stretch faces, bending stencils, pair capacity
+    const float4 *x0, *dx, *xt, *rest;
+    const float* mass;
+    const uint8_t* pinned;
+    float h2inv, dirichlet;
+    const uint2* edges;
+    const float* rest_len;
+    float spring_k;
+    const uint4* sfaces;
+    const float4* dm;
+    const float* sarea;
+    float mu, lambda;
+    const uint4* bend;
+    const float *rest_angle, *hbar, *Q;
+    float kb;         // dihedral: bending_k * scaling; quadratic: bending_k
+    int bending_model;
+    const lcs_pair* pairs;
+    const uint32_t* pair_count;
+    const float *dhat, *offset;
+};
+
+__device__ __forceinline__ float ls_alpha(float toi, int j)
+{
+    float a = toi;
+    for (int k = 0; k < j; ++k) a /= 2.0f;
+    return a;
+}
+
+__device__ __forceinline__ v3 ls_pos(const LsArgs& a, uint32_t v, float alpha)
+{
+    const float4 p = a.x0[v], d = a.dx[v];
+    return mk3(p.x + alpha * d.x, p.y + alpha * d.y, p.z + alpha * d.z);
+}
+
+// E(alpha_k) for slot 0 (alpha = 0) and slots k >= 1 (alpha = toi / 2^(j0 + k - 1)): inertia with the
+// Dirichlet factor, the stretch and bending models, and the barrier energy of the iteration-start pairs
+// (fn_calc_energy_*, solver_interface.cpp:505-728; compute_contact_energy_from_iter_start_list)
+template <int NS>
+__global__ void __launch_bounds__(256) k_ls_energy(LsArgs a, int j0, const Status* __restrict__ st, double* E)
+{
+    const uint32_t npairs = a.P ? pair_count(a.pair_count, a.P) : 0;
+    const uint32_t n = max(max(max(a.V, a.E), max(a.Fs, a.B)), npairs);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t n_round = (n + stride - 1) / stride * stride;
+    const float toi = st->toi;
+    float al[NS];
+    al[0] = 0.0f;
+#pragma unroll
+    for (int k = 1; k < NS; ++k) al[k] = ls_alpha(toi, j0 + k - 1);
+    double e[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) e[k] = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += stride) {
+        if (i < a.V) {
+            const float4 t = a.xt[i];
+            const float m = a.mass[i];
+            const bool fixed = a.pinned && a.pinned[i];
+#pragma unroll
+            for (int k = 0; k < NS; ++k) {
+                const v3 d = ls_pos(a, i, al[k]) - mk3(t.x, t.y, t.z);
+                float en = a.h2inv * dot3(d, d) * m / 2.0f;
+                if (fixed) en = a.dirichlet * en;
+                e[k] += (double)en;
+            }
+        }
+        if (i < a.E) {
+            const uint2 ed = a.edges[i];
+#pragma unroll
+            for (int k = 0; k < NS; ++k) {
+                const v3 d = ls_pos(a, ed.y, al[k]) - ls_pos(a, ed.x, al[k]);
+                const float C = sqrtf(dot3(d, d)) - a.rest_len[i];
+                e[k] += (double)(0.5f * a.spring_k * C * C);
+            }
+        }
+        if (i < a.Fs) {
+            const uint4 fc = a.sfaces[i];
+            const float4 dm = a.dm[i];
+            const float ar = a.sarea[i];
+#pragma unroll
+            for (int k = 0; k < NS; ++k) {
+                const v3 x0 = ls_pos(a, fc.x, al[k]), e1 = ls_pos(a, fc.y, al[k]) - x0, e2 = ls_pos(a, fc.z, al[k]) - x0;
+                const v3 Fu = mk3(__fmaf_rn(e2.x, dm.y, e1.x * dm.x), __fmaf_rn(e2.y, dm.y, e1.y * dm.x),
+                                  __fmaf_rn(e2.z, dm.y, e1.z * dm.x));
+                const v3 Fv = mk3(__fmaf_rn(e2.x, dm.w, e1.x * dm.z), __fmaf_rn(e2.y, dm.w, e1.y * dm.z),
+                                  __fmaf_rn(e2.z, dm.w, e1.z * dm.z));
+                const float su = sqrtf(dot3(Fu, Fu)) - 1.0f, sv = sqrtf(dot3(Fv, Fv)) - 1.0f, i6 = dot3(Fu, Fv);
+                e[k] += (double)(ar * (0.5f * a.mu * (su * su + sv * sv) + 0.5f * a.lambda * (i6 * i6)));
+            }
+        }
+        if (i < a.B) {
+            const uint4 st4 = a.bend[i];
+            const uint32_t v[4] = {st4.x, st4.y, st4.z, st4.w};
+            if (a.bending_model == LCS_BENDING_DIHEDRAL) {
+                const float stiff = a.kb * a.hbar[i], ra = a.rest_angle[i];
+#pragma unroll
+                for (int k = 0; k < NS; ++k) {
+                    v3 g[4];
+                    const float d = dihedral_angle_grad(ls_pos(a, v[0], al[k]), ls_pos(a, v[1], al[k]),
+                                                        ls_pos(a, v[2], al[k]), ls_pos(a, v[3], al[k]), g) - ra;
+                    e[k] += (double)(0.5f * stiff * d * d);
+                }
+            } else {  // quadratic: E = k/2 sum_ij Q_ij (x_i - X_i).(x_j - X_j)
+                const float* q = a.Q + 16 * (size_t)i;
+#pragma unroll 1
+                for (int k = 0; k < NS; ++k) {
+                    v3 u[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float4 r = a.rest[v[j]];
+                        u[j] = ls_pos(a, v[j], al[k]) - mk3(r.x, r.y, r.z);
+                    }
+                    float en = 0.0f;
+#pragma unroll
+                    for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+                        for (int jj = 0; jj < 4; ++jj) en += q[4 * ii + jj] * dot3(u[ii], u[jj]);
+                    e[k] += (double)(0.5f * a.kb * en);
+                }
+            }
+        }
+        if (i < npairs) {
+            const PairView P = load_pair(a.pairs, i);
+            if (P.type) {
+                const float dh = 0.5f * (a.dhat[P.v[0]] + a.dhat[P.v[2]]);
+                const float th = a.offset[P.v[0]] + a.offset[P.v[2]];
+#pragma unroll
+                for (int k = 0; k < NS; ++k) {
+                    const v3 diff = ((P.w[0] * ls_pos(a, P.v[0], al[k]) + P.w[1] * ls_pos(a, P.v[1], al[k])) +
+                                     P.w[2] * ls_pos(a, P.v[2], al[k])) + P.w[3] * ls_pos(a, P.v[3], al[k]);
+                    const float d = sqrtf(dot3(diff, diff));
+                    if (d < th + dh) e[k] += (double)(P.stiff * barrier_e(d - th, dh));
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        double v = e[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+        if (lane_id() == 0 && v != 0.0) atomicAdd(E + k, v);
+    }
+}
+
+// the first slot k >= 1 with E_k < E_0 + Epsilon (newton_solver.cpp:3810-3834); small steps skip the
+// search (newton_solver.cpp:3774-3788); step lengths below 1e-4 are a failure
+__global__ void k_ls_pick(const double* __restrict__ E, int j0, float small_step, Status* st)
+{
+    const float toi = st->toi;
+    st->dirichlet = 0.0f;  // the apply that follows measures it again
+    if (st->max_dx < small_step) {
+        st->alpha = toi;
+        st->ls_iters = 0;
+        st->ls_state = 1;
+        return;
+    }
+    const double limit = E[0] + (double)1.19209290E-7f;
+    for (int k = 1; k < kLsSlots; ++k) {
+        const int j = j0 + k - 1;
+        const float alpha = ls_alpha(toi, j);
+        if (j > 0 && alpha < 1e-4f) {
+            st->alpha = alpha;
+            st->ls_iters = j;
+            st->ls_state = 3;
+            return;
+        }
+        if (E[k] < limit) {
+            st->alpha = alpha;
+            st->ls_iters = j;
+            st->ls_state = 1;
+            return;
+        }
+    }
+    st->alpha = ls_alpha(toi, j0 + kLsSlots - 2);
+    st->ls_iters = j0 + kLsSlots - 2;
+    st->ls_state = 2;
 }
 
 // ---- batched scenes: per-scene step bound, small-step and Dirichlet tests
@@ -528,6 +719,11 @@ struct lcs_newton {
     uint32_t* prev_ccd = nullptr;  // device: the CCD candidate counts of the previous iteration
     bool filter_ok = false;
     bool full_traversal = false;   // LCS_NEWTON_FULL_TRAVERSAL
+    bool energy_ls = false;        // LCS_NEWTON_ENERGY_LINESEARCH
+    double *ls_E = nullptr, *h_ls_E = nullptr;  // energies of one line-search round (device, pinned host)
+    float* h_alpha = nullptr;      // pinned: the plain loop's chosen step length
+    int32_t ls_halvings = 0;       // this step
+    float last_alpha = 1.0f;
     lcs_pair* pairs = nullptr;
     lcs_assembler* asmb = nullptr;
     lcs_pcg* pcg = nullptr;
@@ -745,7 +941,7 @@ int build_material_pattern(lcs_newton* h, const lcs_scene_desc* d)
     return LCS_OK;
 }
 
-inline int G(uint64_t n) { return grid_for(n, 256); }
+inline int grid256(uint64_t n) { return grid_for(n, 256); }
 
 void mark(lcs_newton* h, int phase)
 {
@@ -865,6 +1061,96 @@ bool grow(lcs_newton* h)
     return g;
 }
 
+LsArgs ls_args(const lcs_newton* h)
+{
+    const lcs_scene_desc& d = h->d;
+    LsArgs a{};
+    a.V = h->V;
+    a.x0 = h->x_iter;
+    a.dx = h->dx;
+    a.xt = h->x_tilde;
+    a.rest = h->rest;
+    a.mass = h->mass;
+    a.pinned = h->pinned;
+    a.h2inv = 1.0f / (d.dt * d.dt);
+    a.dirichlet = d.dirichlet;
+    if (d.stretch_model == LCS_STRETCH_SPRING) {
+        a.E = h->E;
+        a.edges = h->edges;
+        a.rest_len = h->rest_len;
+        a.spring_k = d.spring_k;
+    } else {
+        a.Fs = h->Fs;
+        a.sfaces = h->sfaces;
+        a.dm = h->dm;
+        a.sarea = h->sarea;
+        a.mu = d.stretch_mu;
+        a.lambda = d.stretch_lambda;
+    }
+    if (d.bending_model != LCS_BENDING_NONE) {
+        a.B = h->B;
+        a.bend = h->bend;
+        a.rest_angle = h->rest_angle;
+        a.hbar = h->hbar;
+        a.Q = h->Q;
+        a.kb = d.bending_model == LCS_BENDING_DIHEDRAL ? d.bending_k * d.bending_scaling : d.bending_k;
+        a.bending_model = d.bending_model;
+    }
+    a.P = h->cap_pairs;
+    a.pairs = h->pairs;
+    a.pair_count = &h->st->cnt[2];
+    a.dhat = h->dhat;
+    a.offset = h->offset;
+    return a;
+}
+
+int ls_grid(const lcs_newton* h)
+{
+    const uint32_t n = std::max(std::max(std::max(h->V, h->Fs), std::max(h->E, h->B)), h->cap_pairs);
+    return grid_for(n, 256, 4);
+}
+
+// one round of the fused energy line search on the device: E at alpha = 0 and kLsSlots - 1 halvings
+// starting at toi / 2^j0, then the pick (st->alpha, st->ls_state)
+int ls_round(lcs_newton* h, int j0)
+{
+    LCS_CUDA_TRY(cudaMemsetAsync(h->ls_E, 0, sizeof(double) * kLsSlots, h->s));
+    k_ls_energy<kLsSlots><<<ls_grid(h), 256, 0, h->s>>>(ls_args(h), j0, h->st, h->ls_E);
+    lcs_count_launch();
+    k_ls_pick<<<1, 1, 0, h->s>>>(h->ls_E, j0, 1e-2f * h->d.dt, h->st);
+    lcs_count_launch();
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+// the reference's sequence for the plain loop: one step length per energy evaluation, each read
+// back to the host (newton_solver.cpp:3790-3834); toi and max |dx| are on the host already
+int plain_line_search(lcs_newton* h)
+{
+    const Status& s = *h->h_st;
+    float alpha = s.toi;
+    int j = 0;
+    if (!(s.max_dx < 1e-2f * h->d.dt)) {
+        const LsArgs a = ls_args(h);
+        for (int count = 0; count < 20; ++count) {
+            LCS_CUDA_TRY(cudaMemsetAsync(h->ls_E, 0, sizeof(double) * 2, h->s));
+            k_ls_energy<2><<<ls_grid(h), 256, 0, h->s>>>(a, j, h->st, h->ls_E);
+            lcs_count_launch();
+            LCS_LAUNCH_CHECK();
+            LCS_CUDA_TRY(cudaMemcpyAsync(h->h_ls_E, h->ls_E, sizeof(double) * 2, cudaMemcpyDeviceToHost, h->s));
+            LCS_CUDA_TRY(cudaStreamSynchronize(h->s));
+            if (h->h_ls_E[1] < h->h_ls_E[0] + (double)1.19209290E-7f) break;
+            alpha /= 2.0f;
+            ++j;
+            if (alpha < 1e-4f) return lcs_fail(LCS_ERR_LINESEARCH, "lcs_newton: energy line search failed (step below 1e-4)");
+        }
+    }
+    *h->h_alpha = alpha;
+    LCS_CUDA_TRY(cudaMemcpyAsync(&h->st->alpha, h->h_alpha, sizeof(float), cudaMemcpyHostToDevice, h->s));
+    h->ls_halvings += j;
+    return LCS_OK;
+}
+
 // one Newton iteration (the body of the loop in physics_step_GPU); returns LCS_OK or an error
 int newton_iteration(lcs_newton* h)
 {
@@ -891,29 +1177,29 @@ int newton_iteration(lcs_newton* h)
         if (h->plain) {  // x_iter_start copied to the host for host_apply_dx (newton_solver.cpp:4196-4198)
             if ((rc = copy_x_to_host(h, h->x))) return rc;
         }
-        k_inertia<<<G(V), 256, 0, h->s>>>(V, d.dt, d.dirichlet, h->mass, h->pinned, h->x, h->x_tilde, h->x_iter, h->b,
+        k_inertia<<<grid256(V), 256, 0, h->s>>>(V, d.dt, d.dirichlet, h->mass, h->pinned, h->x, h->x_tilde, h->x_iter, h->b,
                                           h->diag, d.use_floor, d.floor_y, d.kappa, h->vert_area, h->dhat, h->offset);
         lcs_count_launch();
         LCS_CUDA_TRY(cudaMemsetAsync(h->mat_val, 0, sizeof(float) * h->sell_vals, h->s));
         const uint32_t cs = h->sell ? 128u : 1u;
         if (h->E && d.stretch_model == LCS_STRETCH_SPRING) {
-            k_springs<<<G(h->E), 256, 0, h->s>>>(h->E, h->edges, h->rest_len, d.spring_k, h->x, h->b, h->diag,
+            k_springs<<<grid256(h->E), 256, 0, h->s>>>(h->E, h->edges, h->rest_len, d.spring_k, h->x, h->b, h->diag,
                                                  h->spring_slots, cs, h->mat_val);
             lcs_count_launch();
         }
         if (h->Fs && d.stretch_model == LCS_STRETCH_BW98) {
-            k_stretch_bw98<<<G(h->Fs), 256, 0, h->s>>>(h->Fs, h->sfaces, h->dm, h->sarea, d.stretch_mu,
+            k_stretch_bw98<<<grid256(h->Fs), 256, 0, h->s>>>(h->Fs, h->sfaces, h->dm, h->sarea, d.stretch_mu,
                                                        d.stretch_lambda, h->x, h->b, h->diag, h->face_slots, cs,
                                                        h->mat_val);
             lcs_count_launch();
         }
         if (h->B && d.bending_model == LCS_BENDING_DIHEDRAL) {
-            k_bending_dihedral<<<G(h->B), 256, 0, h->s>>>(h->B, h->bend, h->rest_angle, h->hbar,
+            k_bending_dihedral<<<grid256(h->B), 256, 0, h->s>>>(h->B, h->bend, h->rest_angle, h->hbar,
                                                           d.bending_k * d.bending_scaling, h->x, h->b, h->diag,
                                                           h->bend_slots, cs, h->mat_val);
             lcs_count_launch();
         } else if (h->B && d.bending_model == LCS_BENDING_QUADRATIC) {
-            k_bending<<<G(h->B), 256, 0, h->s>>>(h->B, h->bend, h->Q, d.bending_k, h->x, h->rest, h->b, h->diag,
+            k_bending<<<grid256(h->B), 256, 0, h->s>>>(h->B, h->bend, h->Q, d.bending_k, h->x, h->rest, h->b, h->diag,
                                                  h->bend_slots, cs, h->mat_val);
             lcs_count_launch();
         }
@@ -986,9 +1272,9 @@ int newton_iteration(lcs_newton* h)
         // line_search (newton_solver.cpp:3685-3884): CCD step bound
         mark(h, kPhCcdBroad);
         if (h->batch)
-            k_b_apply_unit<<<G(V), 256, 0, h->s>>>(V, h->vscene, h->S, h->x_iter, h->dx, h->x, h->bsc);
+            k_b_apply_unit<<<grid256(V), 256, 0, h->s>>>(V, h->vscene, h->S, h->x_iter, h->dx, h->x, h->bsc);
         else
-            k_apply_unit<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->st);
+            k_apply_unit<<<grid256(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->st);
         lcs_count_launch();
         if ((rc = broad_phase(h, h->x_iter, h->x, h->bp_vf, h->bp_ee, &h->st->cnt[3], &h->st->cnt[4],
                               h->plain ? nullptr : &h->st->cnt[5])))
@@ -996,7 +1282,7 @@ int newton_iteration(lcs_newton* h)
         if (h->plain) {
             if ((rc = host_readback(h))) return rc;
             if (grow(h)) {
-                k_copy4<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->x);
+                k_copy4<<<grid256(V), 256, 0, h->s>>>(V, h->x_iter, h->x);
                 lcs_count_launch();
                 if ((rc = alloc_contact(h))) return rc;
                 continue;
@@ -1006,7 +1292,7 @@ int newton_iteration(lcs_newton* h)
         const float* XI = reinterpret_cast<const float*>(h->x_iter);
         const int ccd_flags = h->fp64 ? LCS_CCD_FP64 : 0;
         if (d.use_floor) {
-            k_floor_ccd<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->x, h->offset, h->pinned, d.floor_y, h->st);
+            k_floor_ccd<<<grid256(V), 256, 0, h->s>>>(V, h->x_iter, h->x, h->offset, h->pinned, d.floor_y, h->st);
             lcs_count_launch();
         }
         // fused mode: the EE step bound runs beside the VF one (both only lower the same minimum)
@@ -1039,12 +1325,16 @@ int newton_iteration(lcs_newton* h)
         }
         if (h->plain)
             if ((rc = host_readback(h))) return rc;  // ccd_get_toi
+        if (h->energy_ls) {
+            if ((rc = h->plain ? plain_line_search(h) : ls_round(h, 0))) return rc;
+        }
         mark(h, kPhApply);
         if (h->batch)
-            k_b_apply_final<<<G(V), 256, 0, h->s>>>(V, h->vscene, h->S, h->x_iter, h->dx, h->x, h->pinned, h->x_tilde,
+            k_b_apply_final<<<grid256(V), 256, 0, h->s>>>(V, h->vscene, h->S, h->x_iter, h->dx, h->x, h->pinned, h->x_tilde,
                                                     h->bsc);
         else
-            k_apply_final<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->pinned, h->x_tilde, h->st);
+            k_apply_final<<<grid256(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->pinned, h->x_tilde, h->st,
+                                                  h->energy_ls);
         lcs_count_launch();
         LCS_LAUNCH_CHECK();
         mark(h, kPhases);
@@ -1060,7 +1350,7 @@ int newton_iteration(lcs_newton* h)
         // the next iteration may filter these CCD lists if no traversal ended early
         h->filter_ok = !h->plain && h->h_st->cnt[5] == 0u;
         if (grow(h)) {  // an overflow anywhere: undo the step and run the iteration again
-            k_copy4<<<G(V), 256, 0, h->s>>>(V, h->x_iter, h->x);
+            k_copy4<<<grid256(V), 256, 0, h->s>>>(V, h->x_iter, h->x);
             lcs_count_launch();
             if ((rc = alloc_contact(h))) return rc;
             continue;
@@ -1071,6 +1361,19 @@ int newton_iteration(lcs_newton* h)
         } else if (h->h_st->pcg_status == LCS_ERR_NAN) {
             return lcs_fail(LCS_ERR_NAN, "lcs_newton: NaN/Inf in PCG");
         }
+        if (h->energy_ls && !h->plain) {
+            // rare: no step length of the first round lowered the energy; continue with the next halvings
+            for (int round = 1; h->h_st->ls_state == 2; ++round) {
+                if ((rc = ls_round(h, round * (kLsSlots - 1)))) return rc;
+                k_apply_final<<<grid256(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->pinned, h->x_tilde, h->st, 1);
+                lcs_count_launch();
+                if ((rc = host_readback(h))) return rc;
+            }
+            if (h->h_st->ls_state == 3)
+                return lcs_fail(LCS_ERR_LINESEARCH, "lcs_newton: energy line search failed (step below 1e-4)");
+            h->ls_halvings += h->h_st->ls_iters;
+        }
+        h->last_alpha = h->energy_ls ? h->h_st->alpha : h->h_st->toi;
         return LCS_OK;
     }
     return lcs_fail(LCS_ERR_CAPACITY, "lcs_newton: buffers kept overflowing");
@@ -1122,6 +1425,7 @@ int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batc
     h->profile = (flags & LCS_NEWTON_PROFILE) != 0;
     h->pipelined = (flags & LCS_NEWTON_PCG_PIPELINED) != 0;
     h->full_traversal = (flags & LCS_NEWTON_FULL_TRAVERSAL) != 0;
+    h->energy_ls = (flags & LCS_NEWTON_ENERGY_LINESEARCH) != 0;
     h->batch = batch;
     h->V = d->n_verts;
     h->F = d->n_faces;
@@ -1181,6 +1485,11 @@ int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batc
     A(dalloc(h->st, 1));
     A(dalloc(h->prev_ccd, 2));
     if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->h_st), sizeof(Status));
+    if (h->energy_ls) {
+        A(dalloc(h->ls_E, kLsSlots));
+        if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->h_ls_E), sizeof(double) * kLsSlots);
+        if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->h_alpha), sizeof(float));
+    }
     if (h->plain) {
         if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->h_x), 16 * V);
         if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&h->h_v), 16 * V);
@@ -1230,6 +1539,8 @@ extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_s
 {
     if (!descs || !out || n_scenes == 0) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: bad argument");
     if (flags & LCS_NEWTON_PLAIN) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: the batch runs fused only");
+    if (flags & LCS_NEWTON_ENERGY_LINESEARCH)
+        return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: the energy line search runs on single scenes only");
     if (pcg_cluster != 0 && pcg_cluster != 1 && pcg_cluster != 2 && pcg_cluster != 4 && pcg_cluster != 8 &&
         pcg_cluster != 16)
         return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: cluster size must be 0 (auto), 1, 2, 4, 8 or 16");
@@ -1387,6 +1698,17 @@ extern "C" int lcs_newton_download_scene(const lcs_newton* h, uint32_t scene, fl
     return LCS_OK;
 }
 
+extern "C" int lcs_newton_last_iterate(const lcs_newton* h, float* x_iter_out, float* dx_out, float* x_tilde_out)
+{
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_last_iterate: null handle");
+    const size_t bytes = 16 * (size_t)h->V;
+    if (x_iter_out) LCS_CUDA_TRY(cudaMemcpyAsync(x_iter_out, h->x_iter, bytes, cudaMemcpyDeviceToHost, h->s));
+    if (dx_out) LCS_CUDA_TRY(cudaMemcpyAsync(dx_out, h->dx, bytes, cudaMemcpyDeviceToHost, h->s));
+    if (x_tilde_out) LCS_CUDA_TRY(cudaMemcpyAsync(x_tilde_out, h->x_tilde, bytes, cudaMemcpyDeviceToHost, h->s));
+    LCS_CUDA_TRY(cudaStreamSynchronize(h->s));
+    return LCS_OK;
+}
+
 extern "C" int lcs_newton_destroy(lcs_newton* h)
 {
     if (!h) return LCS_OK;
@@ -1413,6 +1735,9 @@ extern "C" int lcs_newton_destroy(lcs_newton* h)
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_st) cudaFreeHost(h->h_st);
+    if (h->ls_E) cudaFree(h->ls_E);
+    if (h->h_ls_E) cudaFreeHost(h->h_ls_E);
+    if (h->h_alpha) cudaFreeHost(h->h_alpha);
     if (h->h_x) cudaFreeHost(h->h_x);
     if (h->h_v) cudaFreeHost(h->h_v);
     if (h->h_x_iter) cudaFreeHost(h->h_x_iter);
@@ -1447,9 +1772,9 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
         LCS_CUDA_TRY(cudaStreamSynchronize(h->s));
     }
     mark(h, kPhBuild);
-    k_targets<<<G(V), 256, 0, h->s>>>(V, h->rest, h->group, h->anim, (float)h->time, h->target);
+    k_targets<<<grid256(V), 256, 0, h->s>>>(V, h->rest, h->group, h->anim, (float)h->time, h->target);
     lcs_count_launch();
-    k_predict<<<G(V), 256, 0, h->s>>>(V, d.dt, d.gravity[0], d.gravity[1], d.gravity[2], h->pinned, h->target, h->x,
+    k_predict<<<grid256(V), 256, 0, h->s>>>(V, d.dt, d.gravity[0], d.gravity[1], d.gravity[2], h->pinned, h->target, h->x,
                                       h->v, h->x_step, h->x_tilde);
     lcs_count_launch();
     // Init LBVH once per step (newton_solver.cpp:4152-4161)
@@ -1505,7 +1830,7 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
             }
             LCS_CUDA_TRY(cudaMemcpyAsync(h->active, h->h_active, 4 * (size_t)S, cudaMemcpyHostToDevice, h->s));
         }
-        k_update_velocity<<<G(V), 256, 0, h->s>>>(V, d.dt, d.damping, h->x, h->x_step, h->v);
+        k_update_velocity<<<grid256(V), 256, 0, h->s>>>(V, d.dt, d.damping, h->x, h->x_step, h->v);
         lcs_count_launch();
         LCS_LAUNCH_CHECK();
         h->total_newton += iter;
@@ -1529,6 +1854,7 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
     }
     bool global_converged = false, dirichlet_converged = false;
     int iter = 0, pcg_total = 0;
+    h->ls_halvings = 0;
     float last_toi = 1.0f, last_rel = 0.0f;
     for (iter = 0; iter < 100; ++iter) {
         if (global_converged || (iter >= d.nonlinear_iters && dirichlet_converged)) break;
@@ -1540,7 +1866,7 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
         global_converged = s.max_dx < 1e-2f * d.dt;
         dirichlet_converged = s.dirichlet < 1e-3f;
     }
-    k_update_velocity<<<G(V), 256, 0, h->s>>>(V, d.dt, d.damping, h->x, h->x_step, h->v);
+    k_update_velocity<<<grid256(V), 256, 0, h->s>>>(V, d.dt, d.damping, h->x, h->x_step, h->v);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     if (h->plain) {  // x, v copied back to the host at the end of the step
@@ -1557,6 +1883,8 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
         stats->pcg_iters = pcg_total;
         stats->last_toi = last_toi;
         stats->last_rel_residual = last_rel;
+        stats->last_alpha = h->last_alpha;
+        stats->ls_halvings = h->ls_halvings;
         stats->vf_candidates = s.cnt[0];
         stats->ee_candidates = s.cnt[1];
         stats->contact_pairs = s.cnt[2];

@@ -76,12 +76,13 @@ class NewtonSolver:
 
     plain=True selects the reference's dispatch structure (the one-scene comparator);
     fp64=True the precision form; profile=True per-phase CUDA-event timing;
-    pipelined=True the pipelined row-resident PCG (fused mode).
+    pipelined=True the pipelined row-resident PCG (fused mode); energy_linesearch=True the
+    reference's use_energy_linesearch (step halving until the energy decreases).
     """
 
     def __init__(self, scene, plain=False, fp64=False, profile=False, nonlinear_iters=3, pcg_max_iter=100,
                  pcg_rel_tol=1e-4, pcg_abs_rz_tol=1e-10, pcg_check_every=25, damping=2.0, use_floor=False,
-                 floor_y=0.0, stream=None, pipelined=False, full_traversal=False):
+                 floor_y=0.0, stream=None, pipelined=False, full_traversal=False, energy_linesearch=False):
         self.lib = A.load()
         self.scene = scene
         sc = scene
@@ -92,7 +93,8 @@ class NewtonSolver:
         self.desc = d
         flags = (A.LCS_NEWTON_PLAIN if plain else 0) | (A.LCS_NEWTON_FP64 if fp64 else 0) | \
             (A.LCS_NEWTON_PROFILE if profile else 0) | (A.LCS_NEWTON_PCG_PIPELINED if pipelined else 0) | \
-            (A.LCS_NEWTON_FULL_TRAVERSAL if full_traversal else 0)
+            (A.LCS_NEWTON_FULL_TRAVERSAL if full_traversal else 0) | \
+            (A.LCS_NEWTON_ENERGY_LINESEARCH if energy_linesearch else 0)
         s = C.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
         h = C.c_void_p()
         A.check(self.lib.lcs_newton_create(C.byref(d), flags, s, C.byref(h)), "lcs_newton_create")
@@ -132,6 +134,13 @@ class NewtonSolver:
         out = np.zeros((self.scene.num_verts, 4), np.float32)
         A.check(self.lib.lcs_newton_download(self.h, None, out.ctypes.data_as(C.c_void_p)), "lcs_newton_download")
         return out
+
+    def last_iterate(self):
+        """(x at the start of the last Newton iteration, its direction dx, x_tilde), float32 (V, 4) each."""
+        out = [np.zeros((self.scene.num_verts, 4), np.float32) for _ in range(3)]
+        A.check(self.lib.lcs_newton_last_iterate(self.h, *[o.ctypes.data_as(C.c_void_p) for o in out]),
+                "lcs_newton_last_iterate")
+        return tuple(out)
 
     def profile(self):
         ms = (C.c_double * 9)()
