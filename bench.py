@@ -132,11 +132,11 @@ def measured_peak():
 
 
 def committed_traffic():
-    """DRAM bytes per PCG iteration of the row-resident solve from the committed ncu capture (or None)."""
+    """DRAM bytes per launch of the row-resident PCG solve from the committed ncu capture (or None)."""
     path = os.path.join(ROOT, "profiles", "k_pcg_pipe_tube88k_traffic.txt")
     try:
         for ln in open(path):
-            if ln.startswith("bytes_per_iteration="):
+            if ln.startswith("bytes_per_launch="):
                 return float(ln.split("=")[1])
     except Exception:
         return None
@@ -323,7 +323,7 @@ def run_ours(a):
             "roofline": {"bound": "hbm", "kernel": pcg_kernel_name,
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind,
-                         "traffic": None if traffic is None else traffic * it_per_launch,
+                         "traffic": traffic,
                          "algorithmic_bytes_per_launch": bytes_per_launch,
                          "pcg_iters_per_launch": it_per_launch, "avg_launch_ms": pcg_ms / max(pcg_launches, 1)},
             "cpu_baseline": cpu,
