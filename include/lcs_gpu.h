@@ -273,9 +273,10 @@ enum {
     LCS_PCG_NO_STATS = 4,  /* fused path: do not synchronise to fill *stats */
     LCS_PCG_ROWS = 8,      /* row-resident persistent solve (one thread per block row, state in registers);
                               falls back to the persistent solve when the rows exceed one thread each */
-    LCS_PCG_PIPELINED = 16 /* with LCS_PCG_ROWS: pipelined recurrences (Ghysels-Vanroose), one grid-wide
-                              synchronisation per iteration instead of three; the same Krylov iterates in
-                              exact arithmetic, different rounding */
+    LCS_PCG_SINGLE_REDUCTION = 16 /* with LCS_PCG_ROWS: the single-reduction (Chronopoulos-Gear) form of the
+                              same PCG, r.u and (A u).u summed in one grid reduction: two grid-wide
+                              synchronisations per iteration instead of three; the same Krylov iterates in
+                              exact arithmetic, rounding as stable as the classic form */
 };
 
 typedef struct lcs_pcg_opts {
@@ -449,7 +450,7 @@ enum {
     LCS_NEWTON_PLAIN = 1,   /* the reference's dispatch structure (one-scene comparator) */
     LCS_NEWTON_FP64 = 2,    /* precision form: FP64 PCG reductions, ACCD step bound in FP64 */
     LCS_NEWTON_PROFILE = 4, /* per-phase CUDA-event timing (lcs_newton_profile) */
-    LCS_NEWTON_PCG_PIPELINED = 8, /* fused mode: pipelined row-resident PCG (LCS_PCG_PIPELINED) */
+    LCS_NEWTON_PCG_SINGLE_REDUCTION = 8, /* fused mode: single-reduction row-resident PCG (LCS_PCG_SINGLE_REDUCTION) */
     LCS_NEWTON_FULL_TRAVERSAL = 16, /* fused mode: every candidate list by a traversal (no DCD filtering of the
                                       previous iteration's CCD lists) */
     LCS_NEWTON_ENERGY_LINESEARCH = 32 /* use_energy_linesearch (scene_params.h:41): after the CCD bound, halve the
@@ -513,7 +514,7 @@ LCS_API int lcs_newton_reset_profile(lcs_newton* h);
 LCS_API int lcs_newton_counts(const lcs_newton* h, uint32_t* nnz_material, uint32_t* cap_vf, uint32_t* cap_ee,
                               uint32_t* cap_pairs);
 /* Which PCG the Newton loop runs: 0 plain kernels, 1 persistent CSR solve, 2 row-resident,
- * 3 pipelined row-resident (-1: null handle).  No counterpart in the reference. */
+ * 3 single-reduction row-resident (-1: null handle).  No counterpart in the reference. */
 LCS_API int lcs_newton_pcg_kind(const lcs_newton* h);
 
 #ifdef __cplusplus

@@ -26,7 +26,7 @@ STATUS = {0: "LCS_OK", 1: "LCS_ERR_INVALID", 2: "LCS_ERR_CUDA", 3: "LCS_ERR_CAPA
           9: "LCS_ERR_LINESEARCH"}
 LCS_TREE_VERT, LCS_TREE_EDGE, LCS_TREE_FACE = 0, 1, 2
 LCS_CCD_FP64_FINAL, LCS_CCD_FP64 = 1, 2
-LCS_PCG_FP64_DOTS, LCS_PCG_PLAIN, LCS_PCG_NO_STATS, LCS_PCG_ROWS, LCS_PCG_PIPELINED = 1, 2, 4, 8, 16
+LCS_PCG_FP64_DOTS, LCS_PCG_PLAIN, LCS_PCG_NO_STATS, LCS_PCG_ROWS, LCS_PCG_SINGLE_REDUCTION = 1, 2, 4, 8, 16
 LCS_STRETCH_SPRING, LCS_STRETCH_BW98 = 0, 1
 LCS_BENDING_NONE, LCS_BENDING_QUADRATIC, LCS_BENDING_DIHEDRAL = 0, 1, 2
 
@@ -145,7 +145,8 @@ SIGNATURES = {
     "lcs_newton_counts": (I32, [P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                 C.POINTER(C.c_uint32)]),
 }
-LCS_NEWTON_PLAIN, LCS_NEWTON_FP64, LCS_NEWTON_PROFILE, LCS_NEWTON_PCG_PIPELINED, LCS_NEWTON_FULL_TRAVERSAL = 1, 2, 4, 8, 16
+LCS_NEWTON_PLAIN, LCS_NEWTON_FP64, LCS_NEWTON_PROFILE, LCS_NEWTON_PCG_SINGLE_REDUCTION, LCS_NEWTON_FULL_TRAVERSAL = \
+    1, 2, 4, 8, 16
 LCS_NEWTON_ENERGY_LINESEARCH = 32
 PHASES = ["build", "material", "dcd_broad", "dcd_narrow", "assembly", "pcg", "ccd_broad", "ccd_narrow", "apply"]
 

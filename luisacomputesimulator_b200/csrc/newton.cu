@@ -705,7 +705,7 @@ struct lcs_newton {
     uint32_t *mat_rp = nullptr, *mat_col = nullptr, *spring_slots = nullptr, *bend_slots = nullptr, *face_slots = nullptr;
     float* mat_val = nullptr;
     bool sell = false;             // material matrix in SELL-32 for the row-resident PCG (fused mode)
-    bool pipelined = false;        // pipelined row-resident PCG (one grid synchronisation per iteration)
+    bool cg1 = false;              // single-reduction row-resident PCG (two grid synchronisations per iteration)
     size_t sell_vals = 0;          // floats in mat_val
     uint32_t *sell_ptr = nullptr, *sell_col = nullptr;
     // contact
@@ -1246,7 +1246,7 @@ int newton_iteration(lcs_newton* h)
         lcs_assembler_bsr(h->asmb, &Bc, &d_nnzb);
         lcs_pcg_opts o{d.pcg_max_iter, d.pcg_rel_tol, d.pcg_abs_rz_tol, h->plain ? d.pcg_check_every : 1,
                        (h->fp64 ? LCS_PCG_FP64_DOTS : 0) | (h->plain ? LCS_PCG_PLAIN : LCS_PCG_NO_STATS) |
-                           (h->pipelined ? LCS_PCG_PIPELINED : 0)};
+                           (h->cg1 ? LCS_PCG_SINGLE_REDUCTION : 0)};
         lcs_pcg_stats ps;
         if (h->batch)
             rc = lcs_pcg_solve_batch(h->pcg, h->S, h->voff_d, h->h_voff.data(), h->active,
@@ -1423,7 +1423,7 @@ int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batc
     h->plain = (flags & LCS_NEWTON_PLAIN) != 0;
     h->fp64 = (flags & LCS_NEWTON_FP64) != 0;
     h->profile = (flags & LCS_NEWTON_PROFILE) != 0;
-    h->pipelined = (flags & LCS_NEWTON_PCG_PIPELINED) != 0;
+    h->cg1 = (flags & LCS_NEWTON_PCG_SINGLE_REDUCTION) != 0;
     h->full_traversal = (flags & LCS_NEWTON_FULL_TRAVERSAL) != 0;
     h->energy_ls = (flags & LCS_NEWTON_ENERGY_LINESEARCH) != 0;
     h->batch = batch;
@@ -1960,7 +1960,7 @@ extern "C" int lcs_newton_pcg_kind(const lcs_newton* h)
     if (!h) return -1;
     if (h->plain) return 0;
     if (!h->sell) return 1;
-    return h->pipelined ? 3 : 2;
+    return h->cg1 ? 3 : 2;
 }
 
 extern "C" int lcs_newton_counts(const lcs_newton* h, uint32_t* nnz_material, uint32_t* cap_vf, uint32_t* cap_ee,

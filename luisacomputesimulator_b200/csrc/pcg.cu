@@ -678,15 +678,13 @@ __global__ void __launch_bounds__(BS) k_pcg_rows(RowArgs a)
 
 constexpr int kRowThreads = 256;
 
-// ---------------------------------------------------------------- pipelined row-resident solve
-// Pipelined PCG (Ghysels & Vanroose, "Hiding global synchronization latency in the
-// preconditioned conjugate gradient algorithm", Parallel Computing 40, 2014): the same Krylov
-// iterates as CG in exact arithmetic, rearranged so that the three dot products of an
-// iteration (r.u, w.u, r.r) and the exchange of the next SpMV input m = M w share ONE grid-wide
-// synchronisation.  With the block-Jacobi preconditioner M is row-local, so every vector but m
-// stays in the registers of the thread that owns the row.  m and the partial sums are double
-// buffered across iterations (a block that runs ahead must not overwrite what a slower block
-// still reads).  Stop rules as in device_solve: r.z (= r.u) and |r| checked before the update.
+// ---------------------------------------------------------------- single-reduction row-resident solve
+// Grid barrier, partial sums and their prefetch for the row-resident kernels.  The single-reduction
+// form (Chronopoulos & Gear, "s-step iterative methods for symmetric linear systems", J. Comput.
+// Appl. Math. 25, 1989) computes the same Krylov iterates as CG in exact arithmetic with the dot
+// products of an iteration (r.u, w.u, r.r) in one grid-wide reduction.  With the block-Jacobi
+// preconditioner M is row-local, so every vector but u stays with the thread that owns the row.
+// Stop rules as in device_solve: r.z (= r.u) and |r| checked before the update.
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
 {
@@ -851,20 +849,27 @@ __device__ __forceinline__ void grid_reduce3(Fetch3 f, double& o0, double& o1, d
     __syncthreads();
 }
 
+// Single-reduction row-resident solve (the Chronopoulos-Gear form of the same preconditioned CG):
+// with w = A u and u = M^-1 r kept per row, gamma = r.u and delta = w.u are summed in ONE grid
+// reduction, alpha = gamma / (delta - beta gamma / alpha_old), and p, s = A p, x, r follow by
+// recurrence.  Two grid synchronisations per iteration (the reduction, and the publication of u
+// before w = A u) instead of the three of k_pcg_rows; the only extra recurrence (s) keeps the
+// rounding behaviour of the classic method, unlike fully pipelined forms, whose extra recurrences
+// (A M^-1 w ...) drift apart in FP32 on stiff systems.
 template <int BS>
-__global__ void __launch_bounds__(BS, 3) k_pcg_pipe(RowArgs a, float4* pg2)
+__global__ void __launch_bounds__(BS, 3) k_pcg_cg1(RowArgs a)
 {
     __shared__ int s_fail;
-    // x, p, s, q, z of this block's rows: each read and written once per iteration, so they live in
-    // shared memory (private slot per thread, no synchronisation) and leave registers to the SpMV
-    __shared__ float4 sv[5][BS];
-    __shared__ float4 sminv[3][BS];  // inverse diagonal block, column-major (read once per iteration)
+    // x, p, s of this block's rows: each read and written once per iteration, so they live in shared
+    // memory (private slot per thread, no synchronisation) and leave registers to the SpMV
+    __shared__ float4 sv[3][BS];
+    __shared__ float4 sminv[3][BS];  // inverse diagonal block, column-major
     __shared__ __align__(16) double spart[kPipeMaxBlocks][4];  // every block's partial sums
     if (threadIdx.x == 0) s_fail = 0;
     unsigned gen_seen = threadIdx.x == 0 ? ld_acquire(a.bar_gen) : 0u;
     const uint32_t t = threadIdx.x;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) sv[k][t] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int k = 0; k < 3; ++k) sv[k][t] = make_float4(0.f, 0.f, 0.f, 0.f);
     const uint32_t i = blockIdx.x * BS + t;
     const bool own = i < a.n;
     const uint32_t row = own ? i : a.n - 1;
@@ -890,10 +895,11 @@ __global__ void __launch_bounds__(BS, 3) k_pcg_pipe(RowArgs a, float4* pg2)
     }
     float u0, u1, u2, w0, w1, w2;
     LCS_MINV(r0, r1, r2, u0, u1, u2)
-    // w = A u (one extra synchronisation before the loop)
-    if (own) __stcg(&pg2[i], make_float4(u0, u1, u2, 0.0f));
+    // u is published before every w = A u; the reduction barrier between a SpMV and the next
+    // publication guarantees every block has finished reading, so one buffer suffices
+    if (own) __stcg(&a.pg[i], make_float4(u0, u1, u2, 0.0f));
     if (!pipe_barrier(a.bar_count, a.bar_gen, gen_seen, a.stats, &s_fail)) return;
-    row_matvec(a, i, row, own, slice, lane, pg2, u0, u1, u2, w0, w1, w2);
+    row_matvec(a, i, row, own, slice, lane, a.pg, u0, u1, u2, w0, w1, w2);
     float gamma_old = 0.0f, alpha_old = 0.0f, norm_r0 = 0.0f, norm_r = 0.0f, gamma = 0.0f;
     int iter = 0, status = 0;
     for (iter = 0; iter < a.max_iter; ++iter) {
@@ -910,16 +916,8 @@ __global__ void __launch_bounds__(BS, 3) k_pcg_pipe(RowArgs a, float4* pg2)
         if (!own) dg = dd = dr = 0.0;
         double* part = a.part + 4 * (size_t)gridDim.x * (iter & 1);
         block_partial3<BS>(dg, dd, dr, &part[4 * blockIdx.x]);
-        float mm0, mm1, mm2;
-        LCS_MINV(w0, w1, w2, mm0, mm1, mm2)
-        float4* mbuf = (iter & 1) ? pg2 : a.pg;
-        if (own) __stcg(&mbuf[i], make_float4(mm0, mm1, mm2, 0.0f));
         if (!pipe_barrier(a.bar_count, a.bar_gen, gen_seen, a.stats, &s_fail)) return;
-        // the partial-sum loads are in flight while this row computes n = A m (which needs no
-        // scalar of this iteration)
         grid_prefetch3<BS>(part, spart);
-        float n0, n1, n2;
-        row_matvec(a, i, row, own, slice, lane, mbuf, mm0, mm1, mm2, n0, n1, n2);
         double sg, sd, sr;
         grid_collect3<BS>(spart, sg, sd, sr);
         gamma = (float)sg;
@@ -931,10 +929,8 @@ __global__ void __launch_bounds__(BS, 3) k_pcg_pipe(RowArgs a, float4* pg2)
             if (gamma < a.abs_rz_tol) break;
             if (a.rel_tol > 0.0f && norm_r <= a.rel_tol * norm_r0) break;
         }
-        // alpha = gamma / (p.Ap) with p.Ap = delta - beta gamma / alpha_old.  That difference can
-        // cancel to below pcg_epsilon near convergence; a zero step there would leave the search
-        // directions inconsistent and the recurrences diverge, so the iteration restarts from
-        // the current residual instead (beta = 0, p = u), as on the first iteration.
+        // p.Ap = delta - beta gamma / alpha_old can cancel to below pcg_epsilon near convergence;
+        // the iteration then restarts from the current residual (beta = 0, p = u), as on the first
         float beta = 0.0f, alpha = 0.0f;
         bool restart = iter == 0 || alpha_old == 0.0f;
         if (!restart) {
@@ -947,16 +943,16 @@ __global__ void __launch_bounds__(BS, 3) k_pcg_pipe(RowArgs a, float4* pg2)
             beta = 0.0f;
             alpha = safe_div(gamma, delta);
         }
-        float4 z = sv[4][t], q = sv[3][t], sd4 = sv[2][t], p = sv[1][t], x = sv[0][t];
-        z = make_float4(n0 + beta * z.x, n1 + beta * z.y, n2 + beta * z.z, 0.f);
-        q = make_float4(mm0 + beta * q.x, mm1 + beta * q.y, mm2 + beta * q.z, 0.f);
-        sd4 = make_float4(w0 + beta * sd4.x, w1 + beta * sd4.y, w2 + beta * sd4.z, 0.f);
+        float4 sd4 = sv[2][t], p = sv[1][t], x = sv[0][t];
         p = make_float4(u0 + beta * p.x, u1 + beta * p.y, u2 + beta * p.z, 0.f);
+        sd4 = make_float4(w0 + beta * sd4.x, w1 + beta * sd4.y, w2 + beta * sd4.z, 0.f);
         x = make_float4(x.x + alpha * p.x, x.y + alpha * p.y, x.z + alpha * p.z, 0.f);
-        sv[4][t] = z; sv[3][t] = q; sv[2][t] = sd4; sv[1][t] = p; sv[0][t] = x;
+        sv[2][t] = sd4; sv[1][t] = p; sv[0][t] = x;
         r0 -= alpha * sd4.x; r1 -= alpha * sd4.y; r2 -= alpha * sd4.z;
-        u0 -= alpha * q.x; u1 -= alpha * q.y; u2 -= alpha * q.z;
-        w0 -= alpha * z.x; w1 -= alpha * z.y; w2 -= alpha * z.z;
+        LCS_MINV(r0, r1, r2, u0, u1, u2)
+        if (own) __stcg(&a.pg[i], make_float4(u0, u1, u2, 0.0f));
+        if (!pipe_barrier(a.bar_count, a.bar_gen, gen_seen, a.stats, &s_fail)) return;
+        row_matvec(a, i, row, own, slice, lane, a.pg, u0, u1, u2, w0, w1, w2);
         gamma_old = gamma;
         alpha_old = alpha;
     }
@@ -1215,7 +1211,7 @@ extern "C" int lcs_pcg_create(uint32_t n, lcs_pcg** out)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_fused<kRowLanes>, kFusedThreads, 0);
     if (per_sm > 1) per_sm = 1;
     p->fused_grid = sms * (per_sm > 0 ? per_sm : 1);
-    // fused: 3 doubles per block; row-resident: 4 per block, twice (pipelined) for up to kRowMaxBlocks
+    // fused: 3 doubles per block; row-resident: 4 per block, twice (alternate iterations) for up to kRowMaxBlocks
     const int parts = 8 * kRowMaxBlocks / 3 + 1 + (p->fused_grid > kPlainBlocks ? p->fused_grid : kPlainBlocks);
     cudaError_t e = cudaSuccess;
     auto A = [&](void** q, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(q, bytes); };
@@ -1336,7 +1332,7 @@ static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* 
 {
     if (P->rows_capacity < 0) P->rows_capacity = (int)lcs_pcg_rows_capacity();
     if ((int64_t)P->n > P->rows_capacity) return LCS_ERR_CAPACITY;
-    const bool pipe = (o.flags & LCS_PCG_PIPELINED) != 0;
+    const bool pipe = (o.flags & LCS_PCG_SINGLE_REDUCTION) != 0;
     if (pipe && (P->n + kRowThreads - 1) / kRowThreads > (uint32_t)kPipeMaxBlocks) return LCS_ERR_CAPACITY;
     RowArgs a;
     a.n = P->n;
@@ -1362,11 +1358,9 @@ static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* 
     LCS_CUDA_TRY(cudaMemsetAsync(P->bar, 0, sizeof(unsigned), s));
     void* args[] = {&a};
     const int grid = (int)((P->n + kRowThreads - 1) / kRowThreads);
-    float4* pg2 = P->q;  // second buffer of the exchanged vector (pipelined form)
-    void* pargs[] = {&a, &pg2};
     if (pipe)
-        LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_pipe<kRowThreads>, dim3(grid), dim3(kRowThreads),
-                                                 pargs, 0, s));
+        LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_cg1<kRowThreads>, dim3(grid), dim3(kRowThreads),
+                                                 args, 0, s));
     else
         LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_rows<kRowThreads>, dim3(grid), dim3(kRowThreads),
                                                  args, 0, s));
@@ -1386,7 +1380,7 @@ int64_t lcs_pcg_rows_capacity()
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_rows<kRowThreads>, kRowThreads, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_pcg_pipe<kRowThreads>, kRowThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_pcg_cg1<kRowThreads>, kRowThreads, 0);
     if (per_sm2 < per_sm) per_sm = per_sm2;
     int64_t blocks = (int64_t)sms * per_sm;
     if (blocks > kRowMaxBlocks) blocks = kRowMaxBlocks;  // partial-sum space

@@ -46,10 +46,11 @@ class ConjugateGradientSolver:
             self.h = None
 
     def device_solve(self, diag, A_bsr, B_bsr, b, x, max_iter=100, rel_tol=1e-4, abs_rz_tol=1e-10, check_every=25,
-                     fp64_dots=False, plain=False, rows=False, pipelined=False):
+                     fp64_dots=False, plain=False, rows=False, single_reduction=False):
         o = A.PcgOpts(max_iter, rel_tol, abs_rz_tol, check_every,
                       (A.LCS_PCG_FP64_DOTS if fp64_dots else 0) | (A.LCS_PCG_PLAIN if plain else 0) |
-                      (A.LCS_PCG_ROWS if rows or pipelined else 0) | (A.LCS_PCG_PIPELINED if pipelined else 0))
+                      (A.LCS_PCG_ROWS if rows or single_reduction else 0) |
+                      (A.LCS_PCG_SINGLE_REDUCTION if single_reduction else 0))
         st = A.PcgStats()
         A.check(self.lib.lcs_pcg_solve(self.h, ptr(diag), C.byref(A_bsr) if A_bsr is not None else None,
                                        C.byref(B_bsr) if B_bsr is not None else None, ptr(b), ptr(x), C.byref(o),

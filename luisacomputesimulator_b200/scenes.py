@@ -39,7 +39,8 @@ class MeshPart:
     pinned: np.ndarray     # (n,) bool
     thickness: float = 0.0
     d_hat: float = 1e-3
-    density: float = 1e3   # kg per m^2 of rest area (MaterialBase::density)
+    density: float = 1e3   # kg / m^3 (MaterialBase::density)
+    material_thickness: float = 2e-3  # ClothMaterial::thickness: shell volume = area x thickness
     rotate: tuple | None = None  # pinned-vertex animation: (axis_point(3), axis(3), ang_vel, mask)
 
 
@@ -343,8 +344,13 @@ def assemble(name, parts, dt, gravity, kappa, spring_k=None, bending_k=5e-3, bod
                 sd = safe - so
         d_hat[vm] = sd
         offset[vm] = so
-        area_m = vert_area[vm].sum()
-        mass[vm] = (vert_area[vm] / area_m * area_m * part.density).astype(np.float32)
+        # vertex mass = vertex volume / body volume x body mass, shell volumes = area x thickness
+        # (init_mesh_data.cpp:826-845, 884-898, 946-990)
+        th = np.float32(part.material_thickness)
+        vert_vol = (vert_area[vm] * th).astype(np.float32)
+        body_vol = float(np.sum(face_area[sel_f].astype(np.float64) * th))
+        body_mass = np.float32(body_vol * part.density)
+        mass[vm] = (vert_vol / np.float32(body_vol) * body_mass).astype(np.float32)
     x4 = np.zeros((V, 4), np.float32)
     x4[:, :3] = x3
     f4 = np.zeros((faces.shape[0], 4), np.uint32)

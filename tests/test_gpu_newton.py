@@ -45,11 +45,11 @@ def test_one_newton_iteration_matches_cpu_restatement():
     assert abs(st.last_toi - toi) <= 1e-3 * toi + 1e-6
 
 
-@pytest.mark.parametrize("fp64,pipelined", [(False, False), (True, False), (False, True)])
-def test_drop_stays_intersection_free(fp64, pipelined):
+@pytest.mark.parametrize("fp64,cg1", [(False, False), (True, False), (False, True)])
+def test_drop_stays_intersection_free(fp64, cg1):
     sc = S.cloth_on_sphere(n=32)
-    gpu = NewtonSolver(sc, fp64=fp64, pipelined=pipelined)
-    assert gpu.pcg_kind() == ("pipelined" if pipelined else "rows")
+    gpu = NewtonSolver(sc, fp64=fp64, single_reduction=cg1)
+    assert gpu.pcg_kind() == ("cg1" if cg1 else "rows")
     d0 = O.min_distance(sc, sc.x)
     for k in range(40):
         st = gpu.step()
@@ -63,11 +63,11 @@ def test_drop_stays_intersection_free(fp64, pipelined):
     assert O.min_distance(sc, x) > 0.0 and d0 > 0.0
 
 
-@pytest.mark.parametrize("pipelined", [False, True])
-def test_plain_and_fused_agree_on_a_step(pipelined):
+@pytest.mark.parametrize("cg1", [False, True])
+def test_plain_and_fused_agree_on_a_step(cg1):
     sc = touching_scene()
     a = NewtonSolver(sc, plain=True, pcg_check_every=1)
-    b = NewtonSolver(sc, plain=False, pipelined=pipelined)
+    b = NewtonSolver(sc, plain=False, single_reduction=cg1)
     sa, sb = a.step(), b.step()
     assert sa.newton_iters == sb.newton_iters
     xa, xb = a.positions(), b.positions()
@@ -77,9 +77,9 @@ def test_plain_and_fused_agree_on_a_step(pipelined):
 
 def test_twisted_tube_steps_small():
     # a reduced tube (60 x 60) through the full step path, every mode
-    for plain, pipelined in ((False, False), (False, True), (True, False)):
+    for plain, cg1 in ((False, False), (False, True), (True, False)):
         sc = S.twisted_tube(60, 60)
-        gpu = NewtonSolver(sc, plain=plain, pipelined=pipelined)
+        gpu = NewtonSolver(sc, plain=plain, single_reduction=cg1)
         for _ in range(5):
             st = gpu.step()
             assert 1 <= st.newton_iters <= 100  # the small-step rule may end the loop early

@@ -83,7 +83,7 @@ def test_spmv_matches_oracle(system):
     np.testing.assert_allclose(got[:, :3], want[:, :3], rtol=1e-5, atol=1e-6 * scale)
 
 
-@pytest.mark.parametrize("mode", ["plain", "fused", "rows", "pipelined"])
+@pytest.mark.parametrize("mode", ["plain", "fused", "rows", "cg1"])
 @pytest.mark.parametrize("fp64", [False, True])
 def test_pcg_matches_oracle(system, mode, fp64):
     sc, diag, A, B, b = system
@@ -93,21 +93,21 @@ def test_pcg_matches_oracle(system, mode, fp64):
     x = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
     st = solver.device_solve(dev(diag), _dev_bsr(n, A), _dev_bsr(n, B), dev(b), x, max_iter=500, rel_tol=1e-4,
                              check_every=25 if plain else 1, fp64_dots=fp64, plain=plain, rows=mode == "rows",
-                             pipelined=mode == "pipelined")
+                             single_reduction=mode == "cg1")
     ox, ost = O.pcg(diag, A, B, b, max_iter=500, rel_tol=1e-4, check_every=25 if plain else 1, fp64_dots=fp64)
     assert st["status"] == 0 and ost["status"] == 0
     assert st["rel_residual"] <= 1e-4
     # same recurrences, different summation order: iteration counts within a few percent (the
-    # pipelined recurrences round differently and may take a few more)
-    slack = ost["iterations"] // (10 if mode == "pipelined" else 20) + 1
+    # single-reduction recurrences round differently and may take a few more)
+    slack = ost["iterations"] // (10 if mode == "cg1" else 20) + 1
     assert abs(st["iterations"] - ost["iterations"]) <= max(3, slack)
     # true residual of the GPU solution, in FP64 on the host
     xr = host(x)
     r = b[:, :3].astype(np.float64) - O.bsr_spmv(diag, A, B, xr)[:, :3].astype(np.float64)
     assert np.linalg.norm(r) <= 2e-4 * np.linalg.norm(b[:, :3])
-    # the pipelined recurrences round differently: both solutions meet the 1e-4 residual rule
+    # the single-reduction recurrences round differently: both solutions meet the 1e-4 residual rule
     # above, and on this system that leaves differences up to about 4e-3 of the largest entry
-    tol = 5e-3 if mode == "pipelined" else 2e-3
+    tol = 5e-3 if mode == "cg1" else 2e-3
     np.testing.assert_allclose(xr[:, :3], ox[:, :3], rtol=0, atol=tol * np.abs(ox).max())
 
 
