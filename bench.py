@@ -134,7 +134,7 @@ def measured_peak():
 
 def committed_traffic():
     """DRAM bytes per launch of the row-resident PCG solve from the committed ncu capture (or None)."""
-    path = os.path.join(ROOT, "profiles", "k_pcg_pipe_tube88k_traffic.txt")
+    path = os.path.join(ROOT, "profiles", "k_pcg_cg1_tube88k_traffic.txt")
     try:
         for ln in open(path):
             if ln.startswith("bytes_per_launch="):

@@ -233,6 +233,18 @@ LCS_API int lcs_dcd_ee(const uint32_t* pairs, const uint32_t* d_count, uint32_t 
 LCS_API int lcs_contact_grad_diag(const lcs_pair* pairs, const uint32_t* d_count, uint32_t capacity,
                           float* b, float* diag, lcs_stream stream);
 
+/* Affine bodies (ABD).  A body's 12 DOFs q = [p, a0, a1, a2] are four DOF-slot rows of the system
+ * (vertex ids body_dof[b] .. body_dof[b] + 3); its mesh vertices move by x = p + A x_bar. */
+typedef struct lcs_abd_view {
+    const uint32_t* body;      /* per vertex: affine-body id, 0xFFFFFFFF = soft */
+    const float* model_x;      /* float4 per vertex: body-frame rest position x_bar of rigid vertices */
+    const uint32_t* body_dof;  /* per body: vertex id of its first DOF slot */
+} lcs_abd_view;
+/* lcs_contact_grad_diag with the ABD remap (collision_data.h:198-268, narrow_phase.cpp:2598-2676): a rigid
+ * side of a pair adds to its body's four DOF slots with weights sum_i w_i (1, x_bar_i). */
+LCS_API int lcs_contact_grad_diag_abd(const lcs_pair* pairs, const uint32_t* d_count, uint32_t capacity, float* b,
+                                      float* diag, const lcs_abd_view* abd, lcs_stream stream);
+
 /* NarrowPhasesDetector::compute_contact_energy_from_iter_start_list + download_energy
  * (narrow_phase.cpp:2968-3070, 123-130): sum of kappa * area * barrier over the pairs at
  * positions x, accumulated in FP64 into *d_energy (device double, caller resets). */
@@ -249,6 +261,11 @@ LCS_API int lcs_assembler_create(uint32_t n_rows, uint32_t pair_capacity, lcs_as
 LCS_API int lcs_assembler_destroy(lcs_assembler* a);
 LCS_API int lcs_contact_offdiag_bsr(lcs_assembler* a, const lcs_pair* pairs, const uint32_t* d_count,
                             uint32_t capacity, lcs_stream stream);
+/* An assembler sized for pairs with rigid sides (up to 8 generalised DOFs, 56 blocks per pair), and the
+ * off-diagonal blocks with the ABD remap (fn_assemble_triplet_sorted, narrow_phase.cpp:1760-1880). */
+LCS_API int lcs_assembler_create_abd(uint32_t n_rows, uint32_t pair_capacity, lcs_assembler** out);
+LCS_API int lcs_contact_offdiag_bsr_abd(lcs_assembler* a, const lcs_pair* pairs, const uint32_t* d_count,
+                                        uint32_t capacity, const lcs_abd_view* abd, lcs_stream stream);
 /* Device pointers of the assembled BSR; *d_nnzb is a device uint32. */
 LCS_API int lcs_assembler_bsr(const lcs_assembler* a, lcs_bsr* out, const uint32_t** d_nnzb);
 /* NarrowPhasesDetector::download_contact_triplet (narrow_phase.cpp:207-233): copies the BSR

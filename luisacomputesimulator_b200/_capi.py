@@ -55,6 +55,10 @@ class SceneDesc(C.Structure):
                 ("bending_hbar", P), ("bending_scaling", C.c_float)]
 
 
+class AbdView(C.Structure):
+    _fields_ = [("body", P), ("model_x", P), ("body_dof", P)]
+
+
 class ClothElements(C.Structure):
     _fields_ = [("n_verts", C.c_uint32), ("n_springs", C.c_uint32), ("n_stretch_faces", C.c_uint32),
                 ("n_bending", C.c_uint32), ("mass", P), ("is_fixed", P), ("springs", P), ("spring_rest_len", P),
@@ -99,6 +103,9 @@ SIGNATURES = {
     "lcs_dcd_vf": (I32, [P, P, U32, P, P, P, P, P, P, P, F32, P, U32, P, P]),
     "lcs_dcd_ee": (I32, [P, P, U32, P, P, P, P, P, P, F32, P, U32, P, P]),
     "lcs_contact_grad_diag": (I32, [P, P, U32, P, P, P]),
+    "lcs_contact_grad_diag_abd": (I32, [P, P, U32, P, P, C.POINTER(AbdView), P]),
+    "lcs_assembler_create_abd": (I32, [U32, U32, C.POINTER(P)]),
+    "lcs_contact_offdiag_bsr_abd": (I32, [P, P, P, U32, C.POINTER(AbdView), P]),
     "lcs_contact_energy": (I32, [P, P, U32, P, P, P, P, P]),
     "lcs_assembler_create": (I32, [U32, U32, C.POINTER(P)]),
     "lcs_assembler_destroy": (I32, [P]),

@@ -288,9 +288,14 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide, 
                 mx = max3(a, b);
                 v0 = q;
             }
-            const float r = __ldg(&thickness[v0]) + __ldg(&dhat[v0]);
+            const float dh = __ldg(&dhat[v0]);
+            const float r = __ldg(&thickness[v0]) + dh;
             box[0] = mn.x - r; box[1] = mn.y - r; box[2] = mn.z - r;
             box[3] = mx.x + r; box[4] = mx.y + r; box[5] = mx.z + r;
+            if (!EE && dh < 0.0f) {  // a vertex with a negative d_hat (affine-body DOF slot) queries nothing
+                box[0] = box[1] = box[2] = __int_as_float(0x7f800000);
+                box[3] = box[4] = box[5] = __int_as_float(0xff800000);
+            }
         }
         uint32_t stack[32];
         int sp = 0;

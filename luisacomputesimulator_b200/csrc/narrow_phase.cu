@@ -13,6 +13,7 @@
 #include "lcs_internal.h"
 #include "radix_sort.cuh"
 #include "scan.cuh"
+#include "abd.cuh"
 
 using namespace lcs;
 
@@ -206,24 +207,39 @@ __global__ void __launch_bounds__(256) k_dcd_ee(const uint2* __restrict__ pairs,
     }
 }
 
-// fn_perPair_assemble_gradient_hessian (soft bodies), narrow_phase.cpp:2550-2676
+// fn_perPair_assemble_gradient_hessian, narrow_phase.cpp:2550-2676: b += k1 w n and D += k2 w^2 n n^T for
+// every generalised DOF of the pair (soft vertices, or a rigid side's four DOF slots)
+template <bool ABD>
 __global__ void __launch_bounds__(256) k_grad_diag(const lcs_pair* __restrict__ pairs, const uint32_t* d_count,
-                                                   uint32_t cap, float* b, float* diag)
+                                                   uint32_t cap, float* b, float* diag, AbdView abd)
 {
     const uint32_t n = pair_count(d_count, cap);
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const PairView P = load_pair(pairs, k);
         if (!P.type) continue;
         const float nn[3] = {P.n.x, P.n.y, P.n.z};
+        uint32_t dof[8];
+        float gw[8];
+        int nd = 4;
+        if (ABD) {
+            nd = pair_dofs(P, abd, dof, gw);
+        } else {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const float g = P.k1 * P.w[i];
-            float* bv = b + 4 * (size_t)P.v[i];
+            for (int i = 0; i < 4; ++i) {
+                dof[i] = P.v[i];
+                gw[i] = P.w[i];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            if (i >= nd) break;
+            const float g = P.k1 * gw[i];
+            float* bv = b + 4 * (size_t)dof[i];
             atomicAdd(bv + 0, g * P.n.x);
             atomicAdd(bv + 1, g * P.n.y);
             atomicAdd(bv + 2, g * P.n.z);
-            const float h = P.k2 * P.w[i] * P.w[i];
-            float* dv = diag + 12 * (size_t)P.v[i];
+            const float h = P.k2 * gw[i] * gw[i];
+            float* dv = diag + 12 * (size_t)dof[i];
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -263,26 +279,48 @@ __global__ void __launch_bounds__(256) k_energy(const lcs_pair* __restrict__ pai
 }
 
 // ---------------------------------------------------------------- off-diagonal blocks (BSR)
-// key = row << bits | col; value = pair * 16 + i * 4 + j.  12 directed (i, j) per pair.
+// key = row << bits | col; value = pair * 16 + i * 4 + j: 12 directed (i, j) per pair.  With affine
+// bodies the pair's generalised DOFs (up to 8) give up to 56 directed pairs, value = pair * 64 + i * 8 + j,
+// unused entries sorting last like non-contact ones.
+template <bool ABD>
 __global__ void k_trip_keys(const lcs_pair* __restrict__ pairs, const uint32_t* d_count, uint32_t cap, int bits,
                             uint32_t n_rows, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
-                            uint32_t* d_ntrip)
+                            uint32_t* d_ntrip, AbdView abd)
 {
+    constexpr uint32_t T = ABD ? 56u : 12u;
     const uint32_t n = pair_count(d_count, cap);
-    if (blockIdx.x == 0 && threadIdx.x == 0) *d_ntrip = 12u * n;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d_ntrip = T * n;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const PairView P = load_pair(pairs, k);
-        int t = 0;
+        if (!ABD) {
+            int t = 0;
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+            for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if (i != j) {
-                    const uint64_t row = P.type ? P.v[i] : n_rows;  // non-contact entries sort last, dropped
-                    keys[12 * (size_t)k + t] = (row << bits) | (uint64_t)P.v[j];
-                    vals[12 * (size_t)k + t] = 16u * k + 4u * i + j;
-                    ++t;
-                }
+                for (int j = 0; j < 4; ++j)
+                    if (i != j) {
+                        const uint64_t row = P.type ? P.v[i] : n_rows;  // non-contact entries sort last, dropped
+                        keys[12 * (size_t)k + t] = (row << bits) | (uint64_t)P.v[j];
+                        vals[12 * (size_t)k + t] = 16u * k + 4u * i + j;
+                        ++t;
+                    }
+        } else {
+            uint32_t dof[8];
+            float gw[8];
+            const int nd = P.type ? pair_dofs(P, abd, dof, gw) : 0;
+            uint32_t t = 0;
+            for (int i = 0; i < nd; ++i)
+                for (int j = 0; j < nd; ++j)
+                    if (i != j) {
+                        keys[T * (size_t)k + t] = ((uint64_t)dof[i] << bits) | (uint64_t)dof[j];
+                        vals[T * (size_t)k + t] = 64u * k + 8u * i + j;
+                        ++t;
+                    }
+            for (; t < T; ++t) {
+                keys[T * (size_t)k + t] = (uint64_t)n_rows << bits;
+                vals[T * (size_t)k + t] = 64u * k;
+            }
+        }
     }
 }
 
@@ -298,11 +336,12 @@ __global__ void k_heads(const uint64_t* __restrict__ keys, const uint32_t* d_n, 
 
 // segmented sum in sorted (key, pair, i, j) order -- the oracle's order, so values match bitwise
 // (fn_assemble_triplet_sorted, narrow_phase.cpp:1760-1880)
+template <bool ABD>
 __global__ void k_segments(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals,
                            const uint32_t* __restrict__ flags, const uint32_t* __restrict__ excl,
                            const uint32_t* d_n, uint32_t cap, int bits, uint32_t n_rows,
                            const lcs_pair* __restrict__ pairs, uint32_t* __restrict__ col, uint32_t* __restrict__ brow,
-                           float* __restrict__ val, uint32_t* d_nnzb)
+                           float* __restrict__ val, uint32_t* d_nnzb, AbdView abd)
 {
     const uint32_t n = pair_count(d_n, cap);
     const uint64_t cmask = (1ull << bits) - 1ull;
@@ -318,8 +357,18 @@ __global__ void k_segments(const uint64_t* __restrict__ keys, const uint32_t* __
         for (int q = 0; q < 9; ++q) acc[q] = 0.0f;
         for (uint32_t t = s; t < n && keys[t] == key; ++t) {
             const uint32_t v = vals[t];
-            const PairView P = load_pair(pairs, v >> 4);
-            const float sw = P.w[(v >> 2) & 3u] * P.w[v & 3u];
+            float sw;
+            PairView P;
+            if (ABD) {
+                P = load_pair(pairs, v >> 6);
+                uint32_t dof[8];
+                float gw[8];
+                pair_dofs(P, abd, dof, gw);
+                sw = gw[(v >> 3) & 7u] * gw[v & 7u];
+            } else {
+                P = load_pair(pairs, v >> 4);
+                sw = P.w[(v >> 2) & 3u] * P.w[v & 3u];
+            }
             const float nn[3] = {P.n.x, P.n.y, P.n.z};
 #pragma unroll
             for (int c = 0; c < 3; ++c)
@@ -350,6 +399,7 @@ __global__ void k_row_ptr(const uint32_t* __restrict__ brow, const uint32_t* d_n
 
 struct lcs_assembler {
     uint32_t n_rows = 0, pair_cap = 0, trip_cap = 0;
+    bool abd = false;  // sized for pairs with affine-body sides (56 directed DOF pairs each)
     int bits = 1;
     uint64_t *keys = nullptr, *keys_alt = nullptr;
     uint32_t *vals = nullptr, *vals_alt = nullptr, *hist = nullptr;
@@ -359,14 +409,16 @@ struct lcs_assembler {
     float* val = nullptr;
 };
 
-extern "C" int lcs_assembler_create(uint32_t n_rows, uint32_t pair_capacity, lcs_assembler** out)
+namespace {
+int assembler_create(uint32_t n_rows, uint32_t pair_capacity, bool abd, lcs_assembler** out)
 {
     if (!out || n_rows == 0) return lcs_fail(LCS_ERR_INVALID, "lcs_assembler_create: bad argument");
     lcs_assembler* a = new (std::nothrow) lcs_assembler();
     if (!a) return lcs_fail(LCS_ERR_INVALID, "lcs_assembler_create: out of host memory");
     a->n_rows = n_rows;
+    a->abd = abd;
     a->pair_cap = pair_capacity ? pair_capacity : 1;
-    a->trip_cap = 12u * a->pair_cap;
+    a->trip_cap = (abd ? 56u : 12u) * a->pair_cap;
     int bits = 1;
     while ((1ull << bits) <= (uint64_t)n_rows) ++bits;  // rows up to n_rows (the drop marker) fit
     a->bits = bits;
@@ -396,6 +448,17 @@ extern "C" int lcs_assembler_create(uint32_t n_rows, uint32_t pair_capacity, lcs
     *out = a;
     return LCS_OK;
 }
+}  // namespace
+
+extern "C" int lcs_assembler_create(uint32_t n_rows, uint32_t pair_capacity, lcs_assembler** out)
+{
+    return assembler_create(n_rows, pair_capacity, false, out);
+}
+
+extern "C" int lcs_assembler_create_abd(uint32_t n_rows, uint32_t pair_capacity, lcs_assembler** out)
+{
+    return assembler_create(n_rows, pair_capacity, true, out);
+}
 
 extern "C" int lcs_assembler_destroy(lcs_assembler* a)
 {
@@ -408,15 +471,29 @@ extern "C" int lcs_assembler_destroy(lcs_assembler* a)
     return LCS_OK;
 }
 
-extern "C" int lcs_contact_offdiag_bsr(lcs_assembler* a, const lcs_pair* pairs, const uint32_t* d_count,
-                                       uint32_t capacity, lcs_stream stream)
+namespace {
+AbdView abd_view(const lcs_abd_view* v)
+{
+    return v ? AbdView{v->body, reinterpret_cast<const float4*>(v->model_x), v->body_dof} : AbdView{nullptr, nullptr, nullptr};
+}
+
+int offdiag_bsr(lcs_assembler* a, const lcs_pair* pairs, const uint32_t* d_count, uint32_t capacity,
+                const lcs_abd_view* abdv, lcs_stream stream)
 {
     if (!a || !pairs || !d_count) return lcs_fail(LCS_ERR_INVALID, "lcs_contact_offdiag_bsr: bad argument");
     if (capacity > a->pair_cap) return lcs_fail(LCS_ERR_CAPACITY, "lcs_contact_offdiag_bsr: capacity above the assembler's");
+    const bool abd = abdv != nullptr;
+    if (abd && (!a->abd || !abdv->body || !abdv->model_x || !abdv->body_dof))
+        return lcs_fail(LCS_ERR_INVALID, "lcs_contact_offdiag_bsr_abd: assembler not created for affine bodies, or view incomplete");
+    const AbdView av = abd_view(abdv);
     cudaStream_t s = (cudaStream_t)stream;
-    const uint32_t tcap = 12u * capacity;
-    k_trip_keys<<<grid_for(capacity, 256), 256, 0, s>>>(pairs, d_count, capacity, a->bits, a->n_rows, a->keys,
-                                                        a->vals, a->d_ntrip);
+    const uint32_t tcap = (abd ? 56u : 12u) * capacity;
+    if (abd)
+        k_trip_keys<true><<<grid_for(capacity, 256), 256, 0, s>>>(pairs, d_count, capacity, a->bits, a->n_rows,
+                                                                  a->keys, a->vals, a->d_ntrip, av);
+    else
+        k_trip_keys<false><<<grid_for(capacity, 256), 256, 0, s>>>(pairs, d_count, capacity, a->bits, a->n_rows,
+                                                                   a->keys, a->vals, a->d_ntrip, av);
     lcs_count_launch();
     const bool alt = rs::sort_pairs<uint64_t>(a->keys, a->vals, a->keys_alt, a->vals_alt, a->d_ntrip, 0, tcap, 0,
                                               2 * a->bits, a->hist, s);
@@ -426,13 +503,49 @@ extern "C" int lcs_contact_offdiag_bsr(lcs_assembler* a, const lcs_pair* pairs, 
     k_heads<<<g, 256, 0, s>>>(keys, a->d_ntrip, tcap, a->bits, a->n_rows, a->flags);
     lcs_count_launch();
     scan::exclusive_u32(a->flags, a->excl, a->d_ntrip, tcap, a->scan_tmp, s);
-    k_segments<<<g, 256, 0, s>>>(keys, vals, a->flags, a->excl, a->d_ntrip, tcap, a->bits, a->n_rows, pairs, a->col,
-                                 a->brow, a->val, a->d_nnzb);
+    if (abd)
+        k_segments<true><<<g, 256, 0, s>>>(keys, vals, a->flags, a->excl, a->d_ntrip, tcap, a->bits, a->n_rows, pairs,
+                                           a->col, a->brow, a->val, a->d_nnzb, av);
+    else
+        k_segments<false><<<g, 256, 0, s>>>(keys, vals, a->flags, a->excl, a->d_ntrip, tcap, a->bits, a->n_rows,
+                                            pairs, a->col, a->brow, a->val, a->d_nnzb, av);
     lcs_count_launch();
     k_row_ptr<<<grid_for(a->n_rows + 1, 256), 256, 0, s>>>(a->brow, a->d_nnzb, a->n_rows, a->row_ptr);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
+}
+
+int grad_diag(const lcs_pair* pairs, const uint32_t* d_count, uint32_t capacity, float* b, float* diag,
+              const lcs_abd_view* abdv, lcs_stream stream)
+{
+    if (!d_count || !b || !diag || (capacity && !pairs)) return lcs_fail(LCS_ERR_INVALID, "lcs_contact_grad_diag: bad argument");
+    if (abdv && (!abdv->body || !abdv->model_x || !abdv->body_dof))
+        return lcs_fail(LCS_ERR_INVALID, "lcs_contact_grad_diag_abd: incomplete view");
+    if (capacity == 0) return LCS_OK;
+    if (abdv)
+        k_grad_diag<true><<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(pairs, d_count, capacity, b, diag,
+                                                                                     abd_view(abdv));
+    else
+        k_grad_diag<false><<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(pairs, d_count, capacity, b,
+                                                                                      diag, abd_view(nullptr));
+    lcs_count_launch();
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+}  // namespace
+
+extern "C" int lcs_contact_offdiag_bsr(lcs_assembler* a, const lcs_pair* pairs, const uint32_t* d_count,
+                                       uint32_t capacity, lcs_stream stream)
+{
+    return offdiag_bsr(a, pairs, d_count, capacity, nullptr, stream);
+}
+
+extern "C" int lcs_contact_offdiag_bsr_abd(lcs_assembler* a, const lcs_pair* pairs, const uint32_t* d_count,
+                                           uint32_t capacity, const lcs_abd_view* abd, lcs_stream stream)
+{
+    if (!abd) return lcs_fail(LCS_ERR_INVALID, "lcs_contact_offdiag_bsr_abd: null view");
+    return offdiag_bsr(a, pairs, d_count, capacity, abd, stream);
 }
 
 extern "C" int lcs_assembler_bsr(const lcs_assembler* a, lcs_bsr* out, const uint32_t** d_nnzb)
@@ -549,12 +662,14 @@ extern "C" int lcs_dcd_ee(const uint32_t* pairs, const uint32_t* d_count, uint32
 extern "C" int lcs_contact_grad_diag(const lcs_pair* pairs, const uint32_t* d_count, uint32_t capacity, float* b,
                                      float* diag, lcs_stream stream)
 {
-    if (!d_count || !b || !diag || (capacity && !pairs)) return lcs_fail(LCS_ERR_INVALID, "lcs_contact_grad_diag: bad argument");
-    if (capacity == 0) return LCS_OK;
-    k_grad_diag<<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(pairs, d_count, capacity, b, diag);
-    lcs_count_launch();
-    LCS_LAUNCH_CHECK();
-    return LCS_OK;
+    return grad_diag(pairs, d_count, capacity, b, diag, nullptr, stream);
+}
+
+extern "C" int lcs_contact_grad_diag_abd(const lcs_pair* pairs, const uint32_t* d_count, uint32_t capacity, float* b,
+                                         float* diag, const lcs_abd_view* abd, lcs_stream stream)
+{
+    if (!abd) return lcs_fail(LCS_ERR_INVALID, "lcs_contact_grad_diag_abd: null view");
+    return grad_diag(pairs, d_count, capacity, b, diag, abd, stream);
 }
 
 extern "C" int lcs_contact_energy(const lcs_pair* pairs, const uint32_t* d_count, uint32_t capacity, const float* x,

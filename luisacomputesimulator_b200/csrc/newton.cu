@@ -31,6 +31,7 @@
 #include "lcs_internal.h"
 #include "lcs_geom.cuh"
 #include "material.cuh"
+#include "abd.cuh"
 
 using namespace lcs;
 
@@ -53,6 +54,40 @@ struct Status {
 struct Anim {
     float cx, cy, cz, ax, ay, az, omega, pad;
 };
+
+// affine bodies on the device (body == nullptr: none).  slot[v] = j for the j-th DOF slot of a body
+// (holding p, a0, a1, a2), -1 otherwise; a vertex with a body id and slot -1 is a rigid mesh vertex.
+struct AbdDev {
+    const uint32_t* body;
+    const int8_t* slot;
+    const float4* model_x;
+    const uint32_t* body_dof;
+    const uint8_t* fixed;  // per body
+};
+
+__device__ __forceinline__ bool is_rigid(const AbdDev& a, uint32_t i)
+{
+    return a.body && a.body[i] != kInvalid && a.slot[i] < 0;
+}
+
+// x0 + alpha dx for vertex i; a rigid vertex follows its body: p + A x_bar with q = q0 + alpha dq
+__device__ __forceinline__ float4 stepped(const AbdDev& a, uint32_t i, const float4* __restrict__ x0,
+                                          const float4* __restrict__ dx, float alpha)
+{
+    if (is_rigid(a, i)) {
+        const uint32_t d = a.body_dof[a.body[i]];
+        v3 q[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float4 p = x0[d + j], e = dx[d + j];
+            q[j] = mk3(p.x + alpha * e.x, p.y + alpha * e.y, p.z + alpha * e.z);
+        }
+        const v3 r = affine_apply(q[0], q[1], q[2], q[3], a.model_x[i]);
+        return make_float4(r.x, r.y, r.z, 0.0f);
+    }
+    const float4 p = x0[i], e = dx[i];
+    return make_float4(p.x + alpha * e.x, p.y + alpha * e.y, p.z + alpha * e.z, 0.0f);
+}
 
 __device__ __forceinline__ void atomic_max_pos(float* a, float v) { atomicMax(reinterpret_cast<int*>(a), __float_as_int(v)); }
 
@@ -92,13 +127,21 @@ __global__ void k_targets(uint32_t n, const float4* __restrict__ rest, const int
 // newton_solver.cpp:576-604): pinned vertices get v = (target - x) / dt
 __global__ void k_predict(uint32_t n, float dt, float gx, float gy, float gz, const uint8_t* __restrict__ pinned,
                           const float4* __restrict__ target, const float4* __restrict__ x, float4* __restrict__ v,
-                          float4* __restrict__ x_step_start, float4* __restrict__ x_tilde)
+                          float4* __restrict__ x_step_start, float4* __restrict__ x_tilde, AbdDev abd)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 xp = x[i];
         float4 vp = v[i];
         float3 vpred;
-        if (pinned && pinned[i]) {
+        const int slot = abd.body ? abd.slot[i] : -1;
+        if (slot >= 0) {
+            // fn_abd_predict_position (newton_solver.cpp:640-676): gravity on the translation only, none
+            // for a fixed body
+            const bool acc = slot == 0 && !abd.fixed[abd.body[i]];
+            vpred = acc ? make_float3(vp.x + dt * gx, vp.y + dt * gy, vp.z + dt * gz) : make_float3(vp.x, vp.y, vp.z);
+        } else if (is_rigid(abd, i)) {
+            vpred = make_float3(0.0f, 0.0f, 0.0f);  // x_tilde of rigid vertices: k_abd_rigid_tilde
+        } else if (pinned && pinned[i]) {
             const float4 tg = target[i];
             vp = make_float4((tg.x - xp.x) / dt, (tg.y - xp.y) / dt, (tg.z - xp.z) / dt, 0.0f);
             v[i] = vp;
@@ -118,10 +161,21 @@ __global__ void k_inertia(uint32_t n, float h, float dirichlet, const float* __r
                           const float4* __restrict__ x_tilde, float4* __restrict__ x_iter_start, float4* __restrict__ b,
                           float4* __restrict__ diag, int use_floor, float floor_y, float kappa,
                           const float* __restrict__ vert_area, const float* __restrict__ dhat,
-                          const float* __restrict__ offset)
+                          const float* __restrict__ offset, AbdDev abd)
 {
     const float h2inv = 1.0f / (h * h);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (abd.body && abd.body[i] != kInvalid) {
+            // a rigid mesh vertex's row is inert (identity, zero right-hand side); a DOF slot's row is
+            // written by k_abd_body
+            const float one = abd.slot[i] < 0 ? 1.0f : 0.0f;
+            x_iter_start[i] = x[i];
+            b[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            diag[3 * i + 0] = make_float4(one, 0.0f, 0.0f, 0.0f);
+            diag[3 * i + 1] = make_float4(0.0f, one, 0.0f, 0.0f);
+            diag[3 * i + 2] = make_float4(0.0f, 0.0f, one, 0.0f);
+            continue;
+        }
         const float4 xk = x[i], xt = x_tilde[i];
         const float m = mass[i];
         const float s = -m * h2inv;
@@ -244,6 +298,170 @@ __global__ void k_bending(uint32_t nb, const uint4* __restrict__ stencil, const 
     }
 }
 
+// ---- affine bodies
+// x_tilde of rigid mesh vertices from their body's predicted q (used by the Dirichlet check)
+__global__ void k_abd_rigid_tilde(uint32_t n, AbdDev abd, float4* __restrict__ x_tilde)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (!is_rigid(abd, i)) continue;
+        const uint32_t d = abd.body_dof[abd.body[i]];
+        const v3 r = affine_apply(ld3(x_tilde, d), ld3(x_tilde, d + 1), ld3(x_tilde, d + 2), ld3(x_tilde, d + 3),
+                                  abd.model_x[i]);
+        x_tilde[i] = make_float4(r.x, r.y, r.z, 0.0f);
+    }
+}
+
+// fn_evaluate_abd_inertia + fn_evaluate_abd_orthogonality + fn_material_energy_assembly_affine_body
+// (newton_solver.cpp:1176-1330, 705-814): per body, b = -grad and the 4 x 4 blocks of
+//   inertia       alpha h^-2 M (x) I, grad_i = alpha h^-2 sum_j M_ij (q_j - q~_j), alpha = 1 (+ dirichlet if fixed)
+//   orthogonality kappa V sum_ij (a_i.a_j - delta_ij)^2 on A = [a0 a1 a2] (the reference's gradient and
+//                 Hessian blocks: 4 s (sum_j (a_i.a_j) a_j - a_i); 4 s (a_i a_i^T + (a_i.a_i - 1) I +
+//                 sum_k a_k a_k^T) on the diagonal, 4 s (a_j a_i^T + (a_i.a_j) I) at (i, j), i < j)
+// written into the body's DOF slot rows; off-diagonal blocks (i, j), i != j, row-major in `slots`.
+__global__ void k_abd_body(uint32_t nb, const uint32_t* __restrict__ body_dof, const float* __restrict__ mass16,
+                           const float* __restrict__ volume, const float* __restrict__ kappa,
+                           const uint8_t* __restrict__ fixed, float h2inv, float dirichlet,
+                           const float4* __restrict__ x, const float4* __restrict__ x_tilde, float4* b, float4* diag,
+                           const uint32_t* __restrict__ slots, uint32_t cs, float* mat_val)
+{
+    for (uint32_t bi = blockIdx.x * blockDim.x + threadIdx.x; bi < nb; bi += gridDim.x * blockDim.x) {
+        const uint32_t d = body_dof[bi];
+        v3 q[4], dq[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            q[j] = ld3(x, d + j);
+            dq[j] = q[j] - ld3(x_tilde, d + j);
+        }
+        const float* M = mass16 + 16 * (size_t)bi;
+        const float c = (fixed[bi] ? 1.0f + dirichlet : 1.0f) * h2inv;
+        float H[4][4][9];  // block (i, j), column-major 3 x 3
+        v3 G[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            v3 g = mk3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float m = M[4 * i + j];
+                g = mk3(g.x + m * dq[j].x, g.y + m * dq[j].y, g.z + m * dq[j].z);
+                const float hm = c * m;
+#pragma unroll
+                for (int k = 0; k < 9; ++k) H[i][j][k] = (k % 4 == 0) ? hm : 0.0f;
+            }
+            G[i] = c * g;
+        }
+        const float s4 = 4.0f * (kappa[bi] * volume[bi]);
+        const v3 A[3] = {q[1], q[2], q[3]};
+#pragma unroll
+        for (int ii = 0; ii < 3; ++ii) {
+            v3 og = neg3(A[ii]);
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) og = og + dot3(A[ii], A[jj]) * A[jj];
+            G[1 + ii] = G[1 + ii] + s4 * og;
+        }
+#pragma unroll
+        for (int ii = 0; ii < 3; ++ii)
+#pragma unroll
+            for (int jj = ii; jj < 3; ++jj) {
+                const float ai[3] = {A[ii].x, A[ii].y, A[ii].z}, aj[3] = {A[jj].x, A[jj].y, A[jj].z};
+                float h[9];
+                if (ii == jj) {
+                    const float dd = dot3(A[ii], A[ii]) - 1.0f;
+#pragma unroll
+                    for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+                        for (int r = 0; r < 3; ++r) {
+                            float e = ai[r] * ai[cc] + (r == cc ? dd : 0.0f);
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+                                const float ak[3] = {A[k].x, A[k].y, A[k].z};
+                                e = e + ak[r] * ak[cc];
+                            }
+                            h[3 * cc + r] = e;
+                        }
+                } else {
+                    const float dd = dot3(A[ii], A[jj]);
+#pragma unroll
+                    for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+                        for (int r = 0; r < 3; ++r) h[3 * cc + r] = aj[r] * ai[cc] + (r == cc ? dd : 0.0f);
+                }
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+                    for (int r = 0; r < 3; ++r) {
+                        H[1 + ii][1 + jj][3 * cc + r] = H[1 + ii][1 + jj][3 * cc + r] + s4 * h[3 * cc + r];
+                        if (ii != jj)
+                            H[1 + jj][1 + ii][3 * r + cc] = H[1 + jj][1 + ii][3 * r + cc] + s4 * h[3 * cc + r];
+                    }
+            }
+        int t = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            b[d + i] = make_float4(-G[i].x, -G[i].y, -G[i].z, 0.0f);
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc)
+                diag[3 * (size_t)(d + i) + cc] = make_float4(H[i][i][3 * cc], H[i][i][3 * cc + 1], H[i][i][3 * cc + 2], 0.0f);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (i == j) continue;
+                float* O = mat_val + slots[12 * (size_t)bi + t];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) O[cs * k] = H[i][j][k];
+                ++t;
+            }
+        }
+    }
+}
+
+// fn_evaluate_abd_ground_collision (newton_solver.cpp:1333-1410): the floor barrier of a rigid mesh
+// vertex, added to its body's DOF slots with weights (1, x_bar)
+__global__ void k_abd_floor(uint32_t n, AbdDev abd, const uint8_t* __restrict__ pinned, const float4* __restrict__ x,
+                            float floor_y, float kappa, const float* __restrict__ vert_area,
+                            const float* __restrict__ dhat, const float* __restrict__ offset, float4* b, float4* diag,
+                            const uint32_t* __restrict__ slots, uint32_t cs, float* mat_val)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (!is_rigid(abd, i) || (pinned && pinned[i])) continue;
+        const float dh = dhat[i], th = offset[i], dist = x[i].y - floor_y;
+        if (!(dist - th < dh)) continue;
+        const float stiff = kappa * vert_area[i];
+        const float dd = dist - th;
+        const float k1 = stiff * ((dh - dd) * (2.0f * logf(dd / dh) - dh / dd + 1.0f));
+        const float qq = dh / dd;
+        const float k2 = stiff * ((qq + 2.0f) * qq - 2.0f * logf(dd / dh) - 3.0f);
+        const uint32_t bi = abd.body[i], d = abd.body_dof[bi];
+        const float4 m = abd.model_x[i];
+        const float w[4] = {1.0f, m.x, m.y, m.z};
+        int t = 0;
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii) {
+            atomicAdd(&b[d + ii].y, -(w[ii] * k1));
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) {
+                const float hv = w[ii] * w[jj] * k2;  // only the (y, y) entry of n n^T
+                if (ii == jj) {
+                    atomicAdd(&diag[3 * (size_t)(d + ii) + 1].y, hv);
+                } else {
+                    atomicAdd(mat_val + slots[12 * (size_t)bi + t] + cs * 4, hv);
+                    ++t;
+                }
+            }
+        }
+    }
+}
+
+// after the solve: the rigid mesh vertices' increment J(x_bar) dq, so that the CCD bound, the line
+// search and the small-step test see them move
+__global__ void k_abd_expand(uint32_t n, AbdDev abd, float4* dx)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (!is_rigid(abd, i)) continue;
+        const uint32_t d = abd.body_dof[abd.body[i]];
+        const v3 r = affine_apply(ld3(dx, d), ld3(dx, d + 1), ld3(dx, d + 2), ld3(dx, d + 3), abd.model_x[i]);
+        dx[i] = make_float4(r.x, r.y, r.z, 0.0f);
+    }
+}
+
 // one 16-byte vector atomic (sm_90 and later) per vertex record
 __device__ __forceinline__ void red4(float4* p, float x, float y, float z) { atomicAdd(p, make_float4(x, y, z, 0.0f)); }
 
@@ -329,13 +547,15 @@ __global__ void k_bending_dihedral(uint32_t nb, const uint4* __restrict__ stenci
 
 // fn_apply_dx (newton_solver.cpp:491-503) with alpha = 1, and the |dx|_inf of the small-step test
 __global__ void k_apply_unit(uint32_t n, const float4* __restrict__ x0, const float4* __restrict__ dx, float4* __restrict__ x,
-                             Status* st)
+                             Status* st, AbdDev abd)
 {
     float m = 0.0f;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 a = x0[i], d = dx[i];
-        x[i] = make_float4(a.x + d.x, a.y + d.y, a.z + d.z, 0.0f);
-        m = fmaxf(m, sqrtf(d.x * d.x + d.y * d.y + d.z * d.z));
+        x[i] = stepped(abd, i, x0, dx, 1.0f);
+        if (!is_rigid(abd, i)) {  // the solve's unknowns: soft vertices and DOF slots (sa_cgX)
+            const float4 d = dx[i];
+            m = fmaxf(m, sqrtf(d.x * d.x + d.y * d.y + d.z * d.z));
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
@@ -345,13 +565,12 @@ __global__ void k_apply_unit(uint32_t n, const float4* __restrict__ x0, const fl
 // apply_final_dx with alpha = the CCD step bound, and the Dirichlet check (newton_solver.cpp:3741-3752, 3858-3882)
 __global__ void k_apply_final(uint32_t n, const float4* __restrict__ x0, const float4* __restrict__ dx,
                               float4* __restrict__ x, const uint8_t* __restrict__ pinned,
-                              const float4* __restrict__ x_tilde, Status* st, int use_ls_alpha)
+                              const float4* __restrict__ x_tilde, Status* st, int use_ls_alpha, AbdDev abd)
 {
     const float alpha = use_ls_alpha ? st->alpha : st->toi;
     float m = 0.0f;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 a = x0[i], d = dx[i];
-        const float4 r = make_float4(a.x + alpha * d.x, a.y + alpha * d.y, a.z + alpha * d.z, 0.0f);
+        const float4 r = stepped(abd, i, x0, dx, alpha);
         x[i] = r;
         if (pinned && pinned[i]) {
             const float4 t = x_tilde[i];
@@ -627,24 +846,24 @@ __device__ __forceinline__ void scene_max(float* slots, uint32_t s, float m)
 
 __global__ void k_b_apply_unit(uint32_t n, const uint32_t* __restrict__ vscene, uint32_t S,
                                const float4* __restrict__ x0, const float4* __restrict__ dx, float4* __restrict__ x,
-                               float* bsc)
+                               float* bsc, AbdDev abd)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 a = x0[i], d = dx[i];
-        x[i] = make_float4(a.x + d.x, a.y + d.y, a.z + d.z, 0.0f);
-        scene_max(bsc + S, vscene[i], sqrtf(d.x * d.x + d.y * d.y + d.z * d.z));
+        x[i] = stepped(abd, i, x0, dx, 1.0f);
+        const float4 d = dx[i];
+        scene_max(bsc + S, vscene[i], is_rigid(abd, i) ? 0.0f : sqrtf(d.x * d.x + d.y * d.y + d.z * d.z));
     }
 }
 
 __global__ void k_b_apply_final(uint32_t n, const uint32_t* __restrict__ vscene, uint32_t S,
                                 const float4* __restrict__ x0, const float4* __restrict__ dx, float4* __restrict__ x,
-                                const uint8_t* __restrict__ pinned, const float4* __restrict__ x_tilde, float* bsc)
+                                const uint8_t* __restrict__ pinned, const float4* __restrict__ x_tilde, float* bsc,
+                                AbdDev abd)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t s = vscene[i];
         const float alpha = bsc[s];
-        const float4 a = x0[i], d = dx[i];
-        const float4 r = make_float4(a.x + alpha * d.x, a.y + alpha * d.y, a.z + alpha * d.z, 0.0f);
+        const float4 r = stepped(abd, i, x0, dx, alpha);
         x[i] = r;
         float m = 0.0f;
         if (pinned && pinned[i]) {

@@ -42,6 +42,8 @@ class MeshPart:
     density: float = 1e3   # kg / m^3 (MaterialBase::density)
     material_thickness: float = 2e-3  # ClothMaterial::thickness: shell volume = area x thickness
     rotate: tuple | None = None  # pinned-vertex animation: (axis_point(3), axis(3), ang_vel, mask)
+    rigid: bool = False    # an affine body (RigidMaterial): 12 DOFs q = [p, a0, a1, a2], x = p + A x_bar
+    rigid_stiffness: float = 1e6  # RigidMaterial::stiffness (orthogonality kappa)
 
 
 @dataclasses.dataclass
@@ -79,6 +81,18 @@ class Scene:
     bending_rest_angle: np.ndarray = None  # (B,) float32
     bending_hbar: np.ndarray = None        # (B,) float32
     bending_scaling: float = 1.0           # stiffness_bending_ui
+    # affine bodies: the 4 DOF slots of body b are vertices body_dof[b] .. body_dof[b] + 3 holding
+    # p, a0, a1, a2 (not part of any face, edge or contact query: d_hat < 0); rigid vertices carry
+    # their body id in `body` and their body-frame position in model_x
+    body_dof: np.ndarray = None            # (NB,) uint32
+    body_mass: np.ndarray = None           # (NB, 4, 4) float32: [M, MI^T; MI, I] (init_sim_data.cpp:640-703)
+    body_volume: np.ndarray = None         # (NB,) float32
+    body_kappa: np.ndarray = None          # (NB,) float32
+    model_x: np.ndarray = None             # (V, 4) float32
+
+    @property
+    def num_bodies(self):
+        return 0 if self.body_dof is None else int(self.body_dof.shape[0])
 
     @property
     def num_verts(self):
@@ -298,9 +312,9 @@ def _min_rest_dist(x, faces, edges):
     return best
 
 
-def assemble(name, parts, dt, gravity, kappa, spring_k=None, bending_k=5e-3, bodies=None, stretch_model=1,
-             bending_model=2):
-    """Merge mesh parts into one Scene (vertex/face order = part order)."""
+def assemble(name, parts, dt, gravity, kappa, spring_k=None, bending_k=5e-3, stretch_model=1, bending_model=2):
+    """Merge mesh parts into one Scene (vertex/face order = part order; the DOF slots of rigid parts,
+    four per body, follow all mesh vertices)."""
     xs, fs, pins, vmesh, anims = [], [], [], [], []
     off = 0
     for m, part in enumerate(parts):
@@ -355,13 +369,63 @@ def assemble(name, parts, dt, gravity, kappa, spring_k=None, bending_k=5e-3, bod
     x4[:, :3] = x3
     f4 = np.zeros((faces.shape[0], 4), np.uint32)
     f4[:, :3] = faces
-    body = np.full(V, 0xFFFFFFFF, np.uint32) if bodies is None else bodies.astype(np.uint32)
+    body = np.full(V, 0xFFFFFFFF, np.uint32)
     rest_len = np.linalg.norm(x3[edges[:, 0]] - x3[edges[:, 1]], axis=1).astype(np.float32)
     pinned = np.concatenate(pins).astype(np.uint8)
-    # elements with a free vertex (init_sim_data.cpp:205-270)
-    free = pinned == 0
-    bending = bending[free[bending].any(axis=1)] if len(bending) else bending
-    sf = faces[free[faces].any(axis=1)]
+    # cloth elements: of cloth parts, with a free vertex (init_sim_data.cpp:205-270)
+    rigid_v = np.zeros(V, bool)
+    for m, part in enumerate(parts):
+        if part.rigid:
+            rigid_v[vmesh == m] = True
+    free = (pinned == 0) & ~rigid_v
+    bending = bending[free[bending].any(axis=1) & ~rigid_v[bending].any(axis=1)] if len(bending) else bending
+    sf = faces[free[faces].any(axis=1) & ~rigid_v[faces].any(axis=1)]
+    # affine bodies (init_sim_data.cpp:520-757): q = [p, a0, a1, a2] with p the part's centroid and A = I
+    # at rest, x_bar = x - p; mass matrix from the vertex masses, diagonal clamped to >= Epsilon; volume
+    # = area x thickness (shell); four DOF slots appended per body
+    rig = [m for m, part in enumerate(parts) if part.rigid]
+    NB = len(rig)
+    model_x = np.zeros((V + 4 * NB, 4), np.float32)
+    body_dof = np.zeros(NB, np.uint32)
+    body_mass = np.zeros((NB, 4, 4), np.float32)
+    body_volume = np.zeros(NB, np.float32)
+    body_kappa = np.zeros(NB, np.float32)
+    slot_x = np.zeros((4 * NB, 3), np.float32)
+    foff_m = np.concatenate([[0], np.cumsum([p.faces.shape[0] for p in parts])])
+    for b, m in enumerate(rig):
+        vm = np.nonzero(vmesh == m)[0]
+        body[vm] = b
+        pc = x3[vm].astype(np.float64).mean(axis=0).astype(np.float32)
+        xb = (x3[vm] - pc).astype(np.float32)
+        model_x[vm, :3] = xb
+        mv = mass[vm].astype(np.float64)
+        Mb = mv.sum()
+        MI = (mv[:, None] * xb).sum(0)
+        Ib = (mv[:, None, None] * xb[:, :, None] * xb[:, None, :]).sum(0)
+        Mm = np.zeros((4, 4))
+        Mm[0, 0] = Mb
+        Mm[0, 1:] = Mm[1:, 0] = MI
+        Mm[1:, 1:] = Ib
+        Mm[np.arange(4), np.arange(4)] = np.maximum(Mm[np.arange(4), np.arange(4)], 1.19209290e-7)
+        body_mass[b] = Mm.astype(np.float32)
+        body_volume[b] = np.float32(face_area[foff_m[m]:foff_m[m + 1]].astype(np.float64).sum() *
+                                    parts[m].material_thickness)
+        body_kappa[b] = parts[m].rigid_stiffness
+        body_dof[b] = V + 4 * b
+        slot_x[4 * b] = pc
+        slot_x[4 * b + 1:4 * b + 4] = np.eye(3, dtype=np.float32)
+    if NB:
+        Vt = V + 4 * NB
+        x3 = np.concatenate([x3, slot_x])
+        x4 = np.zeros((Vt, 4), np.float32)
+        x4[:, :3] = x3
+        slot_body = np.repeat(np.arange(NB, dtype=np.uint32), 4)
+        body = np.concatenate([body, slot_body])
+        vert_area = np.concatenate([vert_area, np.zeros(4 * NB)])
+        mass = np.concatenate([mass, np.zeros(4 * NB, np.float32)])
+        pinned = np.concatenate([pinned, np.zeros(4 * NB, np.uint8)])
+        d_hat = np.concatenate([d_hat, np.full(4 * NB, -1.0, np.float32)])  # no contact queries
+        offset = np.concatenate([offset, np.zeros(4 * NB, np.float32)])
     sf4 = np.zeros((sf.shape[0], 4), np.uint32)
     sf4[:, :3] = sf
     mu, lam = lame()
@@ -373,7 +437,10 @@ def assemble(name, parts, dt, gravity, kappa, spring_k=None, bending_k=5e-3, bod
                  spring_k=mu if spring_k is None else spring_k, bending_k=bending_k, anims=anims,
                  stretch_model=stretch_model, bending_model=bending_model, stretch_faces=sf4,
                  stretch_dm_inv=_dm_inv(x3, sf), stretch_area=_face_area(x3, sf), stretch_mu=mu, stretch_lambda=lam,
-                 bending_rest_angle=rest_angle, bending_hbar=hbar)
+                 bending_rest_angle=rest_angle, bending_hbar=hbar,
+                 body_dof=body_dof if NB else None, body_mass=body_mass if NB else None,
+                 body_volume=body_volume if NB else None, body_kappa=body_kappa if NB else None,
+                 model_x=model_x if NB else None)
 
 
 def cloth_on_sphere(n=64, spacing=0.01, seed=0, subdiv=4, radius=0.2, drop=0.05):

@@ -438,6 +438,7 @@ uint32_t orc_lbvh_query_vf(uint32_t n_leaves, const float* node_aabb8, const uin
 #pragma omp for schedule(dynamic, 256)
         for (long long vl = 0; vl < (long long)n_verts; ++vl) {
             uint32_t v = (uint32_t)vl;
+            if (dhat[v] < 0.0f) continue; /* affine-body DOF slot: no queries */
             v3_f a = ld3(x0, v), c = ld3(x1, v);
             float r = thickness[v] + dhat[v];
             float q[8] = {fminf_(a.x, c.x) - r, fminf_(a.y, c.y) - r, fminf_(a.z, c.z) - r, 0,
