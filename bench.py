@@ -53,7 +53,9 @@ def args_():
     p.add_argument("--workload", choices=["tube", "batch", "serve"], default="tube",
                    help="tube: the headline Newton iters/s line; batch: batched drape solves/s (256 scenes); "
                         "serve: Poisson drape requests, p50/p99 latency and solves/s")
-    p.add_argument("--n-scenes", type=int, default=256, help="batch workload: scenes")
+    p.add_argument("--n-scenes", type=int, default=256, help="batch workload: cloth-on-sphere scenes")
+    p.add_argument("--n-box-scenes", type=int, default=16,
+                   help="batch workload: cloth scenes coupled with an affine rigid box (12 DOFs, 8 vertices)")
     p.add_argument("--solve-steps", type=int, default=20, help="time steps of one drape solve")
     p.add_argument("--plain-sample", type=int, default=32, help="requests/scenes timed through the plain loop")
     p.add_argument("--requests", type=int, default=64, help="serve workload: requests")
@@ -388,12 +390,14 @@ def run_batch(a):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     lib = _capi.load()
     _capi.check(lib.lcs_device_check(local), "device check")
-    sizes = _log_uniform_sizes(a.n_scenes, 1000, 32000, seed=0)
+    sizes = list(_log_uniform_sizes(a.n_scenes, 1000, 32000, seed=0))
+    sizes += list(_log_uniform_sizes(a.n_box_scenes, 1000, 32000, seed=1)) if a.n_box_scenes else []
     n_all = len(sizes)
     V_all = int(sum(sizes))
     # whole scenes per rank (independent problems: no collective on the data path)
     mine = partition(sizes, world)[rank]
-    scs = [scenes.random_cloth_scene(sizes[k], k, "sphere") for k in mine]
+    scs = [scenes.random_cloth_scene(sizes[k], k, "sphere") if k < a.n_scenes else
+           scenes.cloth_box_scene(sizes[k], k) for k in mine]
     V = sum(sc.num_verts for sc in scs)
     warm = NewtonBatch(scs[:4])  # warm-up: first-call set-up paths
     for _ in range(max(a.warmup, 1)):
@@ -439,14 +443,16 @@ def run_batch(a):
     fused_t = [_plain_service(scs[i], a.solve_steps, plain=False) for i in sample] or [float("nan")]
     value = done_all / t_max
     line = {
-        "metric": f"batched drape solves/s ({n_all} cloth-on-sphere scenes, 1K-32K verts, {a.solve_steps} steps)",
+        "metric": f"batched drape solves/s ({a.n_scenes} cloth-on-sphere + {a.n_box_scenes} cloth-box scenes, 1K-32K "
+                  f"verts, {a.solve_steps} steps)",
         "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.solve_steps, "warmup": max(a.warmup, 1),
         "ms_per_step": 1e3 * t_max / a.solve_steps, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded cloth grids over icospheres)", "impl": "ours",
-        "config": {"workload": f"C4 batching: {n_all} scenes, {V_all} vertices in all (cloth), sizes log-uniform "
-                               "[1K, 32K] (seed 0), scene k seeded k, dt 1/60, kappa 1e7, 3 Newton/step, PCG <=100 it "
-                               "rel 1e-4; the 16 affine-box scenes are not run (affine bodies not built)",
+        "config": {"workload": f"C4 batching: {a.n_scenes} cloth-on-sphere scenes (cloth sizes log-uniform [1K, 32K], "
+                               f"seed 0) + {a.n_box_scenes} scenes of a cloth (sizes seed 1) over a sphere with an "
+                               f"affine rigid box (8 verts, 12 DOFs) dropped on it; {V_all} cloth vertices in all, "
+                               "scene k seeded k, dt 1/60, kappa 1e7, 3 Newton/step, PCG <=100 it rel 1e-4",
                    "scenes": n_all, "verts_rank0": V, "pcg_cluster": "auto",
                    "parallelism": f"whole scenes over {world} GPUs" if world > 1 else "one batch"},
         "e2e": {"value": done_all / e2e_max, "unit": "solves/s", "h2d_bytes_per_step": None,

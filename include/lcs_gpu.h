@@ -461,6 +461,15 @@ typedef struct lcs_scene_desc {
     const float* bending_rest_angle; /* host, per stencil */
     const float* bending_hbar;       /* host, per stencil: (A0 + A1) / (3 |e|) */
     float bending_scaling;           /* stiffness_bending_ui */
+    /* affine bodies (ABD; init_sim_data.cpp:520-757).  Body b's DOFs q = [p, a0, a1, a2] are the four
+     * vertex records body_dof[b] .. body_dof[b] + 3 of x / v (slots in no face or edge, d_hat < 0 so that
+     * they query nothing); its mesh vertices carry `body` = b and their body-frame positions in model_x. */
+    uint32_t n_bodies;
+    const uint32_t* body_dof;        /* host, per body */
+    const float* body_mass;          /* host, 16 floats per body: the 4 x 4 mass matrix [M, MI^T; MI, I] */
+    const float* body_volume;        /* host, per body */
+    const float* body_kappa;         /* host, per body: RigidMaterial stiffness (orthogonality) */
+    const float* model_x;            /* host float4 per vertex (rigid vertices; others ignored) */
 } lcs_scene_desc;
 
 enum {

@@ -271,23 +271,45 @@ class NarrowPhasesDetector:
                 "dcd_ee")
 
     # -- assembly (narrow_phase.cpp:1264-2362, 2550-2843)
-    def device_perPair_evaluate_gradient_hessian(self, b, diag):
-        A.check(self.lib.lcs_contact_grad_diag(ptr(self.narrow_phase_list), ptr(self.count_view(2)), self.cap_pairs,
-                                               ptr(b), ptr(diag), stream()), "grad_diag")
+    def device_perPair_evaluate_gradient_hessian(self, b, diag, abd=None):
+        """abd: (body, model_x, body_dof) device tensors to remap rigid sides onto affine-body DOF slots."""
+        if abd is None:
+            A.check(self.lib.lcs_contact_grad_diag(ptr(self.narrow_phase_list), ptr(self.count_view(2)),
+                                                   self.cap_pairs, ptr(b), ptr(diag), stream()), "grad_diag")
+        else:
+            v = abd_view(abd)
+            A.check(self.lib.lcs_contact_grad_diag_abd(ptr(self.narrow_phase_list), ptr(self.count_view(2)),
+                                                       self.cap_pairs, ptr(b), ptr(diag), C.byref(v), stream()),
+                    "grad_diag_abd")
 
-    def device_assemble_contact_triplet(self):
+    def device_assemble_contact_triplet(self, abd=None):
         """Off-diagonal contact blocks as BSR; returns (lcs_bsr struct, nnzb device pointer)."""
         if self.assembler is None:
             h = C.c_void_p()
-            A.check(self.lib.lcs_assembler_create(self.nv, self.cap_pairs, C.byref(h)), "assembler_create")
+            create = self.lib.lcs_assembler_create_abd if abd is not None else self.lib.lcs_assembler_create
+            A.check(create(self.nv, self.cap_pairs, C.byref(h)), "assembler_create")
             self.assembler = _Assembler(self.lib, h)
-        A.check(self.lib.lcs_contact_offdiag_bsr(self.assembler.h, ptr(self.narrow_phase_list),
-                                                 ptr(self.count_view(2)), self.cap_pairs, stream()), "offdiag_bsr")
+        if abd is None:
+            A.check(self.lib.lcs_contact_offdiag_bsr(self.assembler.h, ptr(self.narrow_phase_list),
+                                                     ptr(self.count_view(2)), self.cap_pairs, stream()), "offdiag_bsr")
+        else:
+            v = abd_view(abd)
+            A.check(self.lib.lcs_contact_offdiag_bsr_abd(self.assembler.h, ptr(self.narrow_phase_list),
+                                                         ptr(self.count_view(2)), self.cap_pairs, C.byref(v),
+                                                         stream()), "offdiag_bsr_abd")
         return self.assembler.bsr()
 
     def compute_contact_energy(self, x, d_hat, offset):
         A.check(self.lib.lcs_contact_energy(ptr(self.narrow_phase_list), ptr(self.count_view(2)), self.cap_pairs,
                                             ptr(x), ptr(d_hat), ptr(offset), ptr(self.energy), stream()), "energy")
+
+
+def abd_view(abd):
+    """lcs_abd_view of (body, model_x, body_dof) device tensors."""
+    body, model_x, body_dof = abd
+    v = A.AbdView()
+    v.body, v.model_x, v.body_dof = ptr(body), ptr(model_x), ptr(body_dof)
+    return v
 
 
 class _Assembler:

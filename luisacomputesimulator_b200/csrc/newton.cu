@@ -659,6 +659,9 @@ struct LsArgs {
     const lcs_pair* pairs;
     const uint32_t* pair_count;
     const float *dhat, *offset;
+    AbdDev abd;
+    uint32_t NB;
+    const float *bmass, *bvol, *bkappa;
 };
 
 __device__ __forceinline__ float ls_alpha(float toi, int j)
@@ -681,7 +684,7 @@ template <int NS>
 __global__ void __launch_bounds__(256) k_ls_energy(LsArgs a, int j0, const Status* __restrict__ st, double* E)
 {
     const uint32_t npairs = a.P ? pair_count(a.pair_count, a.P) : 0;
-    const uint32_t n = max(max(max(a.V, a.E), max(a.Fs, a.B)), npairs);
+    const uint32_t n = max(max(max(a.V, a.E), max(a.Fs, a.B)), max(npairs, a.NB));
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t n_round = (n + stride - 1) / stride * stride;
     const float toi = st->toi;
@@ -693,7 +696,7 @@ __global__ void __launch_bounds__(256) k_ls_energy(LsArgs a, int j0, const Statu
 #pragma unroll
     for (int k = 0; k < NS; ++k) e[k] = 0.0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += stride) {
-        if (i < a.V) {
+        if (i < a.V && !(a.abd.body && a.abd.body[i] != kInvalid)) {  // bodies: the per-body terms below
             const float4 t = a.xt[i];
             const float m = a.mass[i];
             const bool fixed = a.pinned && a.pinned[i];
@@ -758,6 +761,37 @@ __global__ void __launch_bounds__(256) k_ls_energy(LsArgs a, int j0, const Statu
                         for (int jj = 0; jj < 4; ++jj) en += q[4 * ii + jj] * dot3(u[ii], u[jj]);
                     e[k] += (double)(0.5f * a.kb * en);
                 }
+            }
+        }
+        if (i < a.NB) {  // fn_calc_energy_abd_inertia / _abd_ortho (solver_interface.cpp:631-728)
+            const uint32_t d = a.abd.body_dof[i];
+            const float* M = a.bmass + 16 * (size_t)i;
+            const bool fixed = a.abd.fixed[i] != 0;
+            const float kv = a.bkappa[i] * a.bvol[i];
+#pragma unroll 1
+            for (int k = 0; k < NS; ++k) {
+                v3 q[4], dq[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    q[j] = ls_pos(a, d + j, al[k]);
+                    const float4 t = a.xt[d + j];
+                    dq[j] = q[j] - mk3(t.x, t.y, t.z);
+                }
+                float ei = 0.0f;
+#pragma unroll
+                for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+                    for (int jj = 0; jj < 4; ++jj) ei += a.h2inv * dot3(dq[ii], dq[jj]) * M[4 * ii + jj] / 2.0f;
+                if (fixed) ei = a.dirichlet * ei;
+                float eo = 0.0f;
+#pragma unroll
+                for (int ii = 0; ii < 3; ++ii)
+#pragma unroll
+                    for (int jj = 0; jj < 3; ++jj) {
+                        const float tt = dot3(q[1 + ii], q[1 + jj]) - (ii == jj ? 1.0f : 0.0f);
+                        eo += tt * tt;
+                    }
+                e[k] += (double)ei + (double)(eo * kv);
             }
         }
         if (i < npairs) {
@@ -907,6 +941,14 @@ struct lcs_newton {
     uint4* faces = nullptr;
     uint2* edges = nullptr;
     uint4* bend = nullptr;
+    // affine bodies
+    uint32_t NB = 0;
+    uint32_t* body_dof = nullptr;
+    float *bmass = nullptr, *bvol = nullptr, *bkappa = nullptr;
+    uint8_t* bfixed = nullptr;
+    float4* model_x = nullptr;
+    int8_t* slot = nullptr;
+    uint32_t* body_slots = nullptr;  // material-matrix slots of each body's 12 off-diagonal blocks
     uint4* sfaces = nullptr;        // BW98 stretch faces
     float4* dm = nullptr;           // their rest Dm^-1
     float *sarea = nullptr, *rest_angle = nullptr, *hbar = nullptr;
@@ -973,6 +1015,11 @@ struct lcs_newton {
 
 namespace {
 
+AbdDev abd_of(const lcs_newton* h)
+{
+    return h->NB ? AbdDev{h->body, h->slot, h->model_x, h->body_dof, h->bfixed} : AbdDev{nullptr, nullptr, nullptr, nullptr, nullptr};
+}
+
 void free_contact(lcs_newton* h)
 {
     if (h->bp_vf) cudaFree(h->bp_vf);
@@ -1019,7 +1066,9 @@ int alloc_contact(lcs_newton* h)
         h->asmb = nullptr;
         e = dalloc(h->pairs, h->cap_pairs);
         h->alloc_pairs = h->cap_pairs;
-        if (e == cudaSuccess) return lcs_assembler_create(h->V, h->cap_pairs, &h->asmb);
+        if (e == cudaSuccess)
+            return h->NB ? lcs_assembler_create_abd(h->V, h->cap_pairs, &h->asmb)
+                         : lcs_assembler_create(h->V, h->cap_pairs, &h->asmb);
     }
     return e == cudaSuccess ? LCS_OK : lcs_fail(LCS_ERR_CUDA, "lcs_newton: contact buffer allocation failed");
 }
@@ -1053,7 +1102,8 @@ int build_material_pattern(lcs_newton* h, const lcs_scene_desc* d)
     const size_t KS = h->d.stretch_model == LCS_STRETCH_SPRING ? 2 * (size_t)h->E : 0;
     const size_t KF = h->d.stretch_model == LCS_STRETCH_BW98 ? 6 * (size_t)h->Fs : 0;
     const size_t KB = h->d.bending_model != LCS_BENDING_NONE ? 12 * (size_t)h->B : 0;
-    const size_t K = KS + KF + KB;
+    const size_t KA = 12 * (size_t)h->NB;  // the 12 off-diagonal blocks among each body's DOF slots
+    const size_t K = KS + KF + KB + KA;
     auto key_rc = [&](size_t k, uint32_t& r, uint32_t& c) {
         if (k < KS) {
             const uint32_t* e = d->edges + 2 * (k >> 1);
@@ -1063,10 +1113,14 @@ int build_material_pattern(lcs_newton* h, const lcs_scene_desc* d)
             const size_t q = k - KS, f = q / 6, m = q % 6, i = m / 2, jj = m % 2, j = jj < i ? jj : jj + 1;
             r = d->stretch_faces[4 * f + i];
             c = d->stretch_faces[4 * f + j];
-        } else {
+        } else if (k < KS + KF + KB) {
             const size_t q = k - KS - KF, st = q / 12, m = q % 12, i = m / 3, jj = m % 3, j = jj < i ? jj : jj + 1;
             r = d->bending[4 * st + i];
             c = d->bending[4 * st + j];
+        } else {
+            const size_t q = k - KS - KF - KB, bi = q / 12, m = q % 12, i = m / 3, jj = m % 3, j = jj < i ? jj : jj + 1;
+            r = d->body_dof[bi] + (uint32_t)i;
+            c = d->body_dof[bi] + (uint32_t)j;
         }
     };
     // bucket the columns by row (counting sort), then sort and de-duplicate each row
@@ -1140,19 +1194,21 @@ int build_material_pattern(lcs_newton* h, const lcs_scene_desc* d)
         for (size_t j = 0; j < nnz; ++j) base[j] = (uint32_t)(9 * j);
         h->sell_vals = 9ull * nnz;
     }
-    std::vector<uint32_t> ss(KS ? KS : 1), fs(KF ? KF : 1), bs(KB ? KB : 1);
+    std::vector<uint32_t> ss(KS ? KS : 1), fs(KF ? KF : 1), bs(KB ? KB : 1), as(KA ? KA : 1);
     parallel_ranges(K, [&](size_t kb, size_t ke) {
         for (size_t k = kb; k < ke; ++k) {
             const uint32_t v = base[slot_of(k)];
             if (k < KS) ss[k] = v;
             else if (k < KS + KF) fs[k - KS] = v;
-            else bs[k - KS - KF] = v;
+            else if (k < KS + KF + KB) bs[k - KS - KF] = v;
+            else as[k - KS - KF - KB] = v;
         }
     });
     if (upload(h->mat_rp, rp.data(), rp.size()) != cudaSuccess || upload(h->mat_col, col.data(), col.size()) != cudaSuccess ||
         upload(h->spring_slots, ss.data(), ss.size()) != cudaSuccess ||
         upload(h->face_slots, fs.data(), fs.size()) != cudaSuccess ||
-        upload(h->bend_slots, bs.data(), bs.size()) != cudaSuccess || dalloc(h->mat_val, h->sell_vals) != cudaSuccess)
+        upload(h->bend_slots, bs.data(), bs.size()) != cudaSuccess ||
+        upload(h->body_slots, as.data(), as.size()) != cudaSuccess || dalloc(h->mat_val, h->sell_vals) != cudaSuccess)
         return lcs_fail(LCS_ERR_CUDA, "lcs_newton: material pattern upload failed");
     if (h->sell && (upload(h->sell_ptr, sell_ptr.data(), sell_ptr.size()) != cudaSuccess ||
                     upload(h->sell_col, sell_col.data(), sell_col.size()) != cudaSuccess))
@@ -1320,12 +1376,17 @@ LsArgs ls_args(const lcs_newton* h)
     a.pair_count = &h->st->cnt[2];
     a.dhat = h->dhat;
     a.offset = h->offset;
+    a.abd = abd_of(h);
+    a.NB = h->NB;
+    a.bmass = h->bmass;
+    a.bvol = h->bvol;
+    a.bkappa = h->bkappa;
     return a;
 }
 
 int ls_grid(const lcs_newton* h)
 {
-    const uint32_t n = std::max(std::max(std::max(h->V, h->Fs), std::max(h->E, h->B)), h->cap_pairs);
+    const uint32_t n = std::max(std::max(std::max(h->V, h->Fs), std::max(h->E, h->B)), std::max(h->cap_pairs, h->NB));
     return grid_for(n, 256, 4);
 }
 
@@ -1397,7 +1458,7 @@ int newton_iteration(lcs_newton* h)
             if ((rc = copy_x_to_host(h, h->x))) return rc;
         }
         k_inertia<<<grid256(V), 256, 0, h->s>>>(V, d.dt, d.dirichlet, h->mass, h->pinned, h->x, h->x_tilde, h->x_iter, h->b,
-                                          h->diag, d.use_floor, d.floor_y, d.kappa, h->vert_area, h->dhat, h->offset);
+                                          h->diag, d.use_floor, d.floor_y, d.kappa, h->vert_area, h->dhat, h->offset, abd_of(h));
         lcs_count_launch();
         LCS_CUDA_TRY(cudaMemsetAsync(h->mat_val, 0, sizeof(float) * h->sell_vals, h->s));
         const uint32_t cs = h->sell ? 128u : 1u;
@@ -1421,6 +1482,18 @@ int newton_iteration(lcs_newton* h)
             k_bending<<<grid256(h->B), 256, 0, h->s>>>(h->B, h->bend, h->Q, d.bending_k, h->x, h->rest, h->b, h->diag,
                                                  h->bend_slots, cs, h->mat_val);
             lcs_count_launch();
+        }
+        if (h->NB) {
+            k_abd_body<<<grid256(h->NB), 256, 0, h->s>>>(h->NB, h->body_dof, h->bmass, h->bvol, h->bkappa, h->bfixed,
+                                                         1.0f / (d.dt * d.dt), d.dirichlet, h->x, h->x_tilde, h->b,
+                                                         h->diag, h->body_slots, cs, h->mat_val);
+            lcs_count_launch();
+            if (d.use_floor) {
+                k_abd_floor<<<grid256(V), 256, 0, h->s>>>(V, abd_of(h), h->pinned, h->x, d.floor_y, d.kappa,
+                                                          h->vert_area, h->dhat, h->offset, h->b, h->diag,
+                                                          h->body_slots, cs, h->mat_val);
+                lcs_count_launch();
+            }
         }
         // update_contact_set (newton_solver.cpp:4093-4104)
         mark(h, kPhDcdBroad);
@@ -1449,10 +1522,18 @@ int newton_iteration(lcs_newton* h)
         }
         // evaluate_contact (newton_solver.cpp:4105-4120)
         mark(h, kPhAssembly);
-        if ((rc = lcs_contact_grad_diag(h->pairs, &h->st->cnt[2], h->cap_pairs, reinterpret_cast<float*>(h->b),
-                                        reinterpret_cast<float*>(h->diag), h->s)))
-            return rc;
-        if ((rc = lcs_contact_offdiag_bsr(h->asmb, h->pairs, &h->st->cnt[2], h->cap_pairs, h->s))) return rc;
+        if (h->NB) {  // pairs with a rigid side go to the body's DOF slots (ABD remap)
+            const lcs_abd_view av{h->body, reinterpret_cast<const float*>(h->model_x), h->body_dof};
+            if ((rc = lcs_contact_grad_diag_abd(h->pairs, &h->st->cnt[2], h->cap_pairs, reinterpret_cast<float*>(h->b),
+                                                reinterpret_cast<float*>(h->diag), &av, h->s)))
+                return rc;
+            if ((rc = lcs_contact_offdiag_bsr_abd(h->asmb, h->pairs, &h->st->cnt[2], h->cap_pairs, &av, h->s))) return rc;
+        } else {
+            if ((rc = lcs_contact_grad_diag(h->pairs, &h->st->cnt[2], h->cap_pairs, reinterpret_cast<float*>(h->b),
+                                            reinterpret_cast<float*>(h->diag), h->s)))
+                return rc;
+            if ((rc = lcs_contact_offdiag_bsr(h->asmb, h->pairs, &h->st->cnt[2], h->cap_pairs, h->s))) return rc;
+        }
         if (h->plain) {  // prescan + construct adjacency + the two-level triplet sort read back counts 4 times
             for (int k = 0; k < 4; ++k)
                 if ((rc = host_readback(h))) return rc;
@@ -1485,15 +1566,19 @@ int newton_iteration(lcs_newton* h)
             k_pcg_to_status<<<1, 1, 0, h->s>>>(lcs_pcg_device_stats(h->pcg), h->st);
             lcs_count_launch();
         }
+        if (h->NB) {
+            k_abd_expand<<<grid256(V), 256, 0, h->s>>>(V, abd_of(h), h->dx);
+            lcs_count_launch();
+        }
         if (h->plain) {  // device_solve copies cgX to the host at its end (precond_cg.cpp:757-758)
             if ((rc = copy_x_to_host(h, h->dx))) return rc;
         }
         // line_search (newton_solver.cpp:3685-3884): CCD step bound
         mark(h, kPhCcdBroad);
         if (h->batch)
-            k_b_apply_unit<<<grid256(V), 256, 0, h->s>>>(V, h->vscene, h->S, h->x_iter, h->dx, h->x, h->bsc);
+            k_b_apply_unit<<<grid256(V), 256, 0, h->s>>>(V, h->vscene, h->S, h->x_iter, h->dx, h->x, h->bsc, abd_of(h));
         else
-            k_apply_unit<<<grid256(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->st);
+            k_apply_unit<<<grid256(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->st, abd_of(h));
         lcs_count_launch();
         if ((rc = broad_phase(h, h->x_iter, h->x, h->bp_vf, h->bp_ee, &h->st->cnt[3], &h->st->cnt[4],
                               h->plain ? nullptr : &h->st->cnt[5])))
@@ -1550,10 +1635,10 @@ int newton_iteration(lcs_newton* h)
         mark(h, kPhApply);
         if (h->batch)
             k_b_apply_final<<<grid256(V), 256, 0, h->s>>>(V, h->vscene, h->S, h->x_iter, h->dx, h->x, h->pinned, h->x_tilde,
-                                                    h->bsc);
+                                                    h->bsc, abd_of(h));
         else
             k_apply_final<<<grid256(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->pinned, h->x_tilde, h->st,
-                                                  h->energy_ls);
+                                                  h->energy_ls, abd_of(h));
         lcs_count_launch();
         LCS_LAUNCH_CHECK();
         mark(h, kPhases);
@@ -1584,7 +1669,8 @@ int newton_iteration(lcs_newton* h)
             // rare: no step length of the first round lowered the energy; continue with the next halvings
             for (int round = 1; h->h_st->ls_state == 2; ++round) {
                 if ((rc = ls_round(h, round * (kLsSlots - 1)))) return rc;
-                k_apply_final<<<grid256(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->pinned, h->x_tilde, h->st, 1);
+                k_apply_final<<<grid256(V), 256, 0, h->s>>>(V, h->x_iter, h->dx, h->x, h->pinned, h->x_tilde, h->st, 1,
+                                                            abd_of(h));
                 lcs_count_launch();
                 if ((rc = host_readback(h))) return rc;
             }
@@ -1619,6 +1705,21 @@ int check_models(const lcs_scene_desc& d)
         return lcs_fail(LCS_ERR_INVALID, "lcs_newton: quadratic bending needs bending_Q");
     if (d.n_bending && d.bending_model == LCS_BENDING_DIHEDRAL && (!d.bending_rest_angle || !d.bending_hbar))
         return lcs_fail(LCS_ERR_INVALID, "lcs_newton: dihedral bending needs bending_rest_angle and bending_hbar");
+    if (d.n_bodies) {
+        if (!d.body || !d.body_dof || !d.body_mass || !d.body_volume || !d.body_kappa || !d.model_x || !d.d_hat)
+            return lcs_fail(LCS_ERR_INVALID, "lcs_newton: affine bodies need body, body_dof, body_mass, body_volume, "
+                                             "body_kappa and model_x");
+        for (uint32_t bi = 0; bi < d.n_bodies; ++bi) {
+            const uint32_t s0 = d.body_dof[bi];
+            if ((uint64_t)s0 + 4 > d.n_verts) return lcs_fail(LCS_ERR_INVALID, "lcs_newton: body_dof out of range");
+            for (uint32_t j = 0; j < 4; ++j)
+                if (d.body[s0 + j] != bi || !(d.d_hat[s0 + j] < 0.0f))
+                    return lcs_fail(LCS_ERR_INVALID, "lcs_newton: a DOF slot must carry its body id and a negative d_hat");
+        }
+        for (uint32_t v = 0; v < d.n_verts; ++v)
+            if (d.body[v] != kInvalid && d.body[v] >= d.n_bodies)
+                return lcs_fail(LCS_ERR_INVALID, "lcs_newton: body id out of range");
+    }
     return LCS_OK;
 }
 }
@@ -1666,6 +1767,22 @@ int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batc
     if (d->bending_model == LCS_BENDING_DIHEDRAL) {
         A(upload(h->rest_angle, d->bending_rest_angle, h->B));
         A(upload(h->hbar, d->bending_hbar, h->B));
+    }
+    if (d->n_bodies) {
+        h->NB = d->n_bodies;
+        std::vector<int8_t> slot(V, -1);
+        std::vector<uint8_t> fixed(h->NB, 0);
+        for (uint32_t bi = 0; bi < h->NB; ++bi)
+            for (uint32_t j = 0; j < 4; ++j) slot[d->body_dof[bi] + j] = (int8_t)j;
+        for (size_t v = 0; v < V; ++v)
+            if (d->body[v] != kInvalid && slot[v] < 0 && d->pinned && d->pinned[v]) fixed[d->body[v]] = 1;
+        A(upload(h->body_dof, d->body_dof, h->NB));
+        A(upload(h->bmass, d->body_mass, 16 * (size_t)h->NB));
+        A(upload(h->bvol, d->body_volume, h->NB));
+        A(upload(h->bkappa, d->body_kappa, h->NB));
+        A(upload(h->bfixed, fixed.data(), h->NB));
+        A(upload(h->model_x, reinterpret_cast<const float4*>(d->model_x), V));
+        A(upload(h->slot, slot.data(), V));
     }
     if (d->stretch_model == LCS_STRETCH_BW98) {
         h->Fs = d->n_stretch_faces;
@@ -1766,7 +1883,7 @@ extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_s
     const lcs_scene_desc& d0 = descs[0];
     // concatenate the scenes: indices shifted by the vertex offset, animation groups renumbered
     std::vector<uint32_t> voff(n_scenes + 1, 0), foff(n_scenes + 1, 0), eoff(n_scenes + 1, 0), boff(n_scenes + 1, 0),
-        soff(n_scenes + 1, 0);
+        soff(n_scenes + 1, 0), aoff(n_scenes + 1, 0);
     uint32_t groups = 0;
     for (uint32_t s = 0; s < n_scenes; ++s) {
         const lcs_scene_desc& d = descs[s];
@@ -1790,6 +1907,7 @@ extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_s
         eoff[s + 1] = eoff[s] + d.n_edges;
         boff[s + 1] = boff[s] + d.n_bending;
         soff[s + 1] = soff[s] + (d.stretch_model == LCS_STRETCH_BW98 ? d.n_stretch_faces : 0);
+        aoff[s + 1] = aoff[s] + d.n_bodies;
         groups += d.anim_group ? d.n_anim : 0;
     }
     if (groups > 127) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: more than 127 animation groups");
@@ -1797,6 +1915,9 @@ extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_s
     const bool quad = d0.bending_model == LCS_BENDING_QUADRATIC, dih = d0.bending_model == LCS_BENDING_DIHEDRAL;
     std::vector<uint32_t> sfaces(4 * (size_t)Fs);
     std::vector<float> dm(4 * (size_t)Fs), sarea(Fs), rest_angle(dih ? B : 0), hbar(dih ? B : 0);
+    const uint32_t NBt = aoff[n_scenes];
+    std::vector<uint32_t> body_dof(NBt);
+    std::vector<float> bmass(16 * (size_t)NBt), bvol(NBt), bkappa(NBt), model_x(NBt ? 4 * (size_t)V : 0, 0.0f);
     std::vector<float> x(4 * (size_t)V), v(4 * (size_t)V, 0.0f), Q(quad ? 16 * (size_t)B : 0), rest_len(E), vert_area(V),
         face_area(F), edge_area(E), mass(V), dhat(V), offset(V), anim(8 * (size_t)std::max(groups, 1u), 0.0f);
     std::vector<uint32_t> faces(4 * (size_t)F), edges(2 * (size_t)E), bend(4 * (size_t)B), body(V, kInvalid);
@@ -1831,7 +1952,16 @@ extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_s
         std::memcpy(&mass[vo], d.mass, 4 * (size_t)d.n_verts);
         std::memcpy(&dhat[vo], d.d_hat, 4 * (size_t)d.n_verts);
         std::memcpy(&offset[vo], d.offset, 4 * (size_t)d.n_verts);
-        if (d.body) std::memcpy(&body[vo], d.body, 4 * (size_t)d.n_verts);
+        if (d.body)
+            for (uint32_t k = 0; k < d.n_verts; ++k)
+                body[vo + k] = d.body[k] == kInvalid ? kInvalid : d.body[k] + aoff[s];
+        for (uint32_t k = 0; k < d.n_bodies; ++k) {
+            body_dof[aoff[s] + k] = d.body_dof[k] + vo;
+            std::memcpy(&bmass[16 * (size_t)(aoff[s] + k)], d.body_mass + 16 * (size_t)k, 64);
+            bvol[aoff[s] + k] = d.body_volume[k];
+            bkappa[aoff[s] + k] = d.body_kappa[k];
+        }
+        if (d.n_bodies) std::memcpy(&model_x[4 * (size_t)vo], d.model_x, 16 * (size_t)d.n_verts);
         if (d.pinned) std::memcpy(&pinned[vo], d.pinned, d.n_verts);
         if (d.anim_group && d.n_anim) {
             for (uint32_t k = 0; k < d.n_verts; ++k)
@@ -1846,6 +1976,8 @@ extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_s
     D.bending_Q = Q.data(); D.rest_len = rest_len.data(); D.vert_area = vert_area.data();
     D.n_stretch_faces = Fs; D.stretch_faces = sfaces.data(); D.stretch_dm_inv = dm.data(); D.stretch_area = sarea.data();
     D.bending_rest_angle = rest_angle.data(); D.bending_hbar = hbar.data();
+    D.n_bodies = NBt; D.body_dof = body_dof.data(); D.body_mass = bmass.data(); D.body_volume = bvol.data();
+    D.body_kappa = bkappa.data(); D.model_x = NBt ? model_x.data() : nullptr;
     D.face_area = face_area.data(); D.edge_area = edge_area.data(); D.mass = mass.data(); D.d_hat = dhat.data();
     D.offset = offset.data(); D.body = body.data(); D.pinned = pinned.data();
     D.anim_group = groups ? group.data() : nullptr; D.n_anim = groups; D.anim = groups ? anim.data() : nullptr;
@@ -1947,6 +2079,7 @@ extern "C" int lcs_newton_destroy(lcs_newton* h)
         if (h->h_bpcg) cudaFreeHost(h->h_bpcg);
     }
     void* ptrs[] = {h->faces, h->edges, h->bend, h->sfaces, h->dm, h->sarea, h->rest_angle, h->hbar, h->face_slots,
+                    h->body_dof, h->bmass, h->bvol, h->bkappa, h->bfixed, h->model_x, h->slot, h->body_slots,
                     h->Q, h->rest_len, h->vert_area, h->face_area, h->edge_area,
                     h->mass, h->dhat, h->offset, h->body, h->pinned, h->group, h->anim, h->rest, h->x, h->v,
                     h->x_step, h->x_iter, h->x_tilde, h->target, h->dx, h->b, h->diag, h->mat_rp, h->mat_col,
@@ -1994,8 +2127,12 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
     k_targets<<<grid256(V), 256, 0, h->s>>>(V, h->rest, h->group, h->anim, (float)h->time, h->target);
     lcs_count_launch();
     k_predict<<<grid256(V), 256, 0, h->s>>>(V, d.dt, d.gravity[0], d.gravity[1], d.gravity[2], h->pinned, h->target, h->x,
-                                      h->v, h->x_step, h->x_tilde);
+                                      h->v, h->x_step, h->x_tilde, abd_of(h));
     lcs_count_launch();
+    if (h->NB) {
+        k_abd_rigid_tilde<<<grid256(V), 256, 0, h->s>>>(V, abd_of(h), h->x_tilde);
+        lcs_count_launch();
+    }
     // Init LBVH once per step (newton_solver.cpp:4152-4161)
     const float* XS = reinterpret_cast<const float*>(h->x_step);
     if (!h->batch) {

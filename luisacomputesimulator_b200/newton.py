@@ -68,6 +68,13 @@ def scene_desc(sc, keep, nonlinear_iters=3, pcg_max_iter=100, pcg_rel_tol=1e-4, 
     d.bending_rest_angle = arr(sc.bending_rest_angle, np.float32)
     d.bending_hbar = arr(sc.bending_hbar, np.float32)
     d.bending_scaling = sc.bending_scaling
+    d.n_bodies = sc.num_bodies
+    if sc.num_bodies:
+        d.body_dof = arr(sc.body_dof, np.uint32)
+        d.body_mass = arr(sc.body_mass.reshape(-1, 16), np.float32)
+        d.body_volume = arr(sc.body_volume, np.float32)
+        d.body_kappa = arr(sc.body_kappa, np.float32)
+        d.model_x = arr(sc.model_x, np.float32)
     return d
 
 

@@ -480,3 +480,21 @@ def random_cloth_scene(n_verts, seed, collider="sphere"):
     return assemble(f"cloth{side}_{collider}_{seed}",
                     [MeshPart(cx, cf, np.zeros(cx.shape[0], bool)), MeshPart(sx, sf, np.ones(sx.shape[0], bool))],
                     dt=1.0 / 60.0, gravity=(0, -9.8, 0), kappa=1e7)
+
+
+def cloth_box_scene(n_verts, seed, box=0.08, gap=2e-3, collider=True):
+    """A square cloth of ~n_verts over a seeded sphere (pinned) with an affine rigid box (8 vertices,
+    12 DOFs, RigidMaterial) resting `gap` above the cloth's centre: the coupled scenes of the batching
+    configuration."""
+    side = max(4, int(round(math.sqrt(n_verts))))
+    rng = np.random.default_rng(seed)
+    spacing = 0.6 / side
+    cy = 0.25
+    cx, cf = cloth_grid(side, side, spacing, origin=(0.0, cy, 0.0), jitter=1e-4, seed=seed)
+    parts = [MeshPart(cx, cf, np.zeros(cx.shape[0], bool))]
+    if collider:
+        sx, sf = icosphere(3, 0.2 * float(rng.uniform(0.8, 1.2)))
+        parts.append(MeshPart(sx, sf, np.ones(sx.shape[0], bool)))
+    bx, bf = box_mesh((box, box, box), (0.0, float(cx[:, 1].max()) + gap + box / 2.0, 0.0))
+    parts.append(MeshPart(bx, bf, np.zeros(8, bool), rigid=True))
+    return assemble(f"cloth{side}_box_{seed}", parts, dt=1.0 / 60.0, gravity=(0, -9.8, 0), kappa=1e7)

@@ -952,6 +952,122 @@ uint32_t orc_contact_offdiag_bsr(const orc_pair* pairs, uint32_t n, uint32_t n_r
     return nb;
 }
 
+/*
+ * Affine bodies: the generalised DOFs of a pair (get_active_indices, collision_data.h:198-268, and
+ * add_to_rigid_body, narrow_phase.cpp:2612-2629).  Each side (VF: vertex 0 | face 1..3; EE: edge 0,1 | edge
+ * 2,3) is soft -- its vertices and weights -- or rigid -- its body's four DOF slots body_dof[b] + j with
+ * weights sum_i w_i (1, x_bar_i), the body being that of vertex 0 (left) or vertex 2 (right).
+ */
+static int pair_dofs_abd(const orc_pair* p, const uint32_t* body, const float* model_x4, const uint32_t* body_dof,
+                         uint32_t dof[8], float gw[8])
+{
+    uint32_t v[4];
+    float w[4];
+    if (!pair_weights(p, v, w)) return 0;
+    const int split = (p->idx[2] >> 31) ? 1 : 2;
+    int n = 0;
+    for (int side = 0; side < 2; ++side) {
+        const int s0 = side ? split : 0, s1 = side ? 4 : split;
+        const uint32_t b = body[v[side ? 2 : 0]];
+        if (b == 0xFFFFFFFFu) {
+            for (int i = s0; i < s1; ++i) {
+                dof[n] = v[i];
+                gw[n] = w[i];
+                ++n;
+            }
+        } else {
+            float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
+            for (int i = s0; i < s1; ++i) {
+                const float* m = model_x4 + 4 * (size_t)v[i];
+                a0 += w[i];
+                a1 += w[i] * m[0];
+                a2 += w[i] * m[1];
+                a3 += w[i] * m[2];
+            }
+            const float aw[4] = {a0, a1, a2, a3};
+            for (int j = 0; j < 4; ++j) {
+                dof[n] = body_dof[b] + (uint32_t)j;
+                gw[n] = aw[j];
+                ++n;
+            }
+        }
+    }
+    return n;
+}
+
+void orc_contact_grad_diag_abd(const orc_pair* pairs, uint32_t n, const uint32_t* body, const float* model_x4,
+                               const uint32_t* body_dof, float* b4, float* diag12)
+{
+    for (uint32_t k = 0; k < n; ++k) {
+        uint32_t dof[8];
+        float gw[8];
+        const int nd = pair_dofs_abd(&pairs[k], body, model_x4, body_dof, dof, gw);
+        float nx = pairs[k].vec1[0], ny = pairs[k].vec1[1], nz = pairs[k].vec1[2];
+        float k1 = pairs[k].vec2[0], k2 = pairs[k].vec2[1];
+        float nn[3] = {nx, ny, nz};
+        for (int i = 0; i < nd; ++i) {
+            float g = k1 * gw[i];
+            b4[4 * (size_t)dof[i] + 0] += g * nx;
+            b4[4 * (size_t)dof[i] + 1] += g * ny;
+            b4[4 * (size_t)dof[i] + 2] += g * nz;
+            float h = k2 * gw[i] * gw[i];
+            for (int c = 0; c < 3; ++c)
+                for (int r = 0; r < 3; ++r) diag12[12 * (size_t)dof[i] + 4 * c + r] += h * (nn[r] * nn[c]);
+        }
+    }
+}
+
+/* orc_contact_offdiag_bsr over the generalised DOFs (every ordered pair of a pair's DOFs) */
+uint32_t orc_contact_offdiag_bsr_abd(const orc_pair* pairs, uint32_t n, uint32_t n_rows, const uint32_t* body,
+                                     const float* model_x4, const uint32_t* body_dof, uint32_t* row_ptr, uint32_t* col,
+                                     float* val9, uint32_t cap)
+{
+    trip* t = (trip*)malloc(sizeof(trip) * 56 * (size_t)(n ? n : 1));
+    size_t nt = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        uint32_t dof[8];
+        float gw[8];
+        const int nd = pair_dofs_abd(&pairs[k], body, model_x4, body_dof, dof, gw);
+        for (int i = 0; i < nd; ++i)
+            for (int j = 0; j < nd; ++j)
+                if (i != j) {
+                    t[nt].key = ((uint64_t)dof[i] << 32) | dof[j];
+                    t[nt].pair = k;
+                    t[nt].i = (uint8_t)i;
+                    t[nt].j = (uint8_t)j;
+                    nt++;
+                }
+    }
+    qsort(t, nt, sizeof(trip), cmp_trip);
+    uint32_t nb = 0;
+    for (uint32_t r = 0; r <= n_rows; ++r) row_ptr[r] = 0;
+    for (size_t s = 0; s < nt; ++s) {
+        if (s == 0 || t[s].key != t[s - 1].key) {
+            uint32_t row = (uint32_t)(t[s].key >> 32);
+            if (nb < cap) {
+                col[nb] = (uint32_t)(t[s].key & 0xFFFFFFFFu);
+                for (int q = 0; q < 9; ++q) val9[9 * (size_t)nb + q] = 0.0f;
+            }
+            if (row < n_rows) row_ptr[row + 1]++;
+            nb++;
+        }
+        if (nb - 1 < cap) {
+            const orc_pair* p = &pairs[t[s].pair];
+            uint32_t dof[8];
+            float gw[8];
+            pair_dofs_abd(p, body, model_x4, body_dof, dof, gw);
+            float k2 = p->vec2[1];
+            float nn[3] = {p->vec1[0], p->vec1[1], p->vec1[2]};
+            float sw = gw[t[s].i] * gw[t[s].j];
+            for (int c = 0; c < 3; ++c)
+                for (int r = 0; r < 3; ++r) val9[9 * (size_t)(nb - 1) + 3 * c + r] += sw * (k2 * (nn[r] * nn[c]));
+        }
+    }
+    for (uint32_t r = 0; r < n_rows; ++r) row_ptr[r + 1] += row_ptr[r];
+    free(t);
+    return nb;
+}
+
 /* fn_compute_repulsion_energy (barrier), narrow_phase.cpp:2968-3044 */
 double orc_contact_energy(const orc_pair* pairs, uint32_t n, const float* x, const float* dhat_v,
                           const float* offset, int fp64_sum)

@@ -157,6 +157,16 @@ void orc_material_fill2(uint32_t V, const float* x4, const float* rest4, const f
                         const uint32_t* face_slots, const uint32_t* bend_slots, uint32_t nnz, float* b4,
                         float* diag12, float* val9);
 
+/* ---------------- affine bodies ---------------- */
+void orc_contact_grad_diag_abd(const orc_pair* pairs, uint32_t n, const uint32_t* body, const float* model_x4,
+                               const uint32_t* body_dof, float* b4, float* diag12);
+uint32_t orc_contact_offdiag_bsr_abd(const orc_pair* pairs, uint32_t n, uint32_t n_rows, const uint32_t* body,
+                                     const float* model_x4, const uint32_t* body_dof, uint32_t* row_ptr, uint32_t* col,
+                                     float* val9, uint32_t cap);
+void orc_abd_fill(uint32_t NB, const uint32_t* body_dof, const float* mass16, const float* volume, const float* kappa,
+                  const uint8_t* fixed, const float* x4, const float* xt4, float dt, float dirichlet,
+                  const uint32_t* body_slots, float* b4, float* diag12, float* val9);
+
 #ifdef __cplusplus
 }
 #endif

@@ -359,3 +359,95 @@ void orc_material_fill2(uint32_t V, const float* x4, const float* rest4, const f
         }
     }
 }
+
+/*
+ * Affine bodies (newton_solver.cpp:1176-1330): per body, b = -grad and the 4 x 4 blocks of inertia
+ * (alpha h^-2 M, alpha = 1 + dirichlet for a fixed body) and orthogonality (kappa V sum_ij (a_i.a_j -
+ * delta_ij)^2, the reference's gradient and Hessian blocks), written into the DOF slot rows: b and the
+ * diagonal stored, off-diagonal blocks (i, j), i != j row-major, at block index body_slots[12 b + t].
+ * The operation order follows the CUDA kernel k_abd_body.
+ */
+void orc_abd_fill(uint32_t NB, const uint32_t* body_dof, const float* mass16, const float* volume, const float* kappa,
+                  const uint8_t* fixed, const float* x4, const float* xt4, float dt, float dirichlet,
+                  const uint32_t* body_slots, float* b4, float* diag12, float* val9)
+{
+    const float h2inv = 1.0f / (dt * dt);
+    for (uint32_t bi = 0; bi < NB; ++bi) {
+        const uint32_t d = body_dof[bi];
+        m3 q[4], dq[4];
+        for (int j = 0; j < 4; ++j) {
+            q[j] = mld(x4, d + j);
+            dq[j] = msub(q[j], mld(xt4, d + j));
+        }
+        const float* M = mass16 + 16 * (size_t)bi;
+        const float c = (fixed[bi] ? 1.0f + dirichlet : 1.0f) * h2inv;
+        float H[4][4][9];
+        m3 G[4];
+        for (int i = 0; i < 4; ++i) {
+            m3 g = M3(0.0f, 0.0f, 0.0f);
+            for (int j = 0; j < 4; ++j) {
+                const float m = M[4 * i + j];
+                g = M3(g.x + m * dq[j].x, g.y + m * dq[j].y, g.z + m * dq[j].z);
+                const float hm = c * m;
+                for (int k = 0; k < 9; ++k) H[i][j][k] = (k % 4 == 0) ? hm : 0.0f;
+            }
+            G[i] = mscl(c, g);
+        }
+        const float s4 = 4.0f * (kappa[bi] * volume[bi]);
+        const m3 A[3] = {q[1], q[2], q[3]};
+        for (int ii = 0; ii < 3; ++ii) {
+            m3 og = M3(-A[ii].x, -A[ii].y, -A[ii].z);
+            for (int jj = 0; jj < 3; ++jj) {
+                const float dd = mdot(A[ii], A[jj]);
+                og = M3(og.x + dd * A[jj].x, og.y + dd * A[jj].y, og.z + dd * A[jj].z);
+            }
+            G[1 + ii] = M3(G[1 + ii].x + s4 * og.x, G[1 + ii].y + s4 * og.y, G[1 + ii].z + s4 * og.z);
+        }
+        for (int ii = 0; ii < 3; ++ii)
+            for (int jj = ii; jj < 3; ++jj) {
+                const float ai[3] = {A[ii].x, A[ii].y, A[ii].z}, aj[3] = {A[jj].x, A[jj].y, A[jj].z};
+                float h[9];
+                if (ii == jj) {
+                    const float dd = mdot(A[ii], A[ii]) - 1.0f;
+                    for (int cc = 0; cc < 3; ++cc)
+                        for (int r = 0; r < 3; ++r) {
+                            float e = ai[r] * ai[cc] + (r == cc ? dd : 0.0f);
+                            for (int k = 0; k < 3; ++k) {
+                                const float ak[3] = {A[k].x, A[k].y, A[k].z};
+                                e = e + ak[r] * ak[cc];
+                            }
+                            h[3 * cc + r] = e;
+                        }
+                } else {
+                    const float dd = mdot(A[ii], A[jj]);
+                    for (int cc = 0; cc < 3; ++cc)
+                        for (int r = 0; r < 3; ++r) h[3 * cc + r] = aj[r] * ai[cc] + (r == cc ? dd : 0.0f);
+                }
+                for (int cc = 0; cc < 3; ++cc)
+                    for (int r = 0; r < 3; ++r) {
+                        H[1 + ii][1 + jj][3 * cc + r] = H[1 + ii][1 + jj][3 * cc + r] + s4 * h[3 * cc + r];
+                        if (ii != jj)
+                            H[1 + jj][1 + ii][3 * r + cc] = H[1 + jj][1 + ii][3 * r + cc] + s4 * h[3 * cc + r];
+                    }
+            }
+        int t = 0;
+        for (int i = 0; i < 4; ++i) {
+            float* bv = b4 + 4 * (size_t)(d + i);
+            bv[0] = -G[i].x;
+            bv[1] = -G[i].y;
+            bv[2] = -G[i].z;
+            bv[3] = 0.0f;
+            float* dv = diag12 + 12 * (size_t)(d + i);
+            for (int cc = 0; cc < 3; ++cc) {
+                for (int r = 0; r < 3; ++r) dv[4 * cc + r] = H[i][i][3 * cc + r];
+                dv[4 * cc + 3] = 0.0f;
+            }
+            for (int j = 0; j < 4; ++j) {
+                if (i == j) continue;
+                float* O = val9 + 9 * (size_t)body_slots[12 * (size_t)bi + t];
+                for (int k = 0; k < 9; ++k) O[k] = H[i][j][k];
+                ++t;
+            }
+        }
+    }
+}

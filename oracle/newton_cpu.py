@@ -25,10 +25,12 @@ class MaterialPattern:
         e = sc.edges.astype(np.int64) if sc.stretch_model == 0 else np.zeros((0, 2), np.int64)
         f = sc.stretch_faces[:, :3].astype(np.int64) if sc.stretch_model == 1 else np.zeros((0, 3), np.int64)
         st = sc.bending.astype(np.int64) if sc.bending_model != 0 else np.zeros((0, 4), np.int64)
+        dof = (sc.body_dof.astype(np.int64)[:, None] + np.arange(4)[None]) if sc.num_bodies else np.zeros((0, 4), np.int64)
         sk = np.stack([e[:, 0] * V + e[:, 1], e[:, 1] * V + e[:, 0]], 1).reshape(-1)
         fk = np.stack([f[:, i] * V + f[:, j] for i in range(3) for j in range(3) if i != j], 1).reshape(-1)
         bk = np.stack([st[:, i] * V + st[:, j] for i in range(4) for j in range(4) if i != j], 1).reshape(-1)
-        uk = np.unique(np.concatenate([sk, fk, bk]))
+        ak = np.stack([dof[:, i] * V + dof[:, j] for i in range(4) for j in range(4) if i != j], 1).reshape(-1)
+        uk = np.unique(np.concatenate([sk, fk, bk, ak]))
         self.nnz = len(uk)
         rp = np.zeros(V + 1, np.int64)
         np.add.at(rp, (uk // V) + 1, 1)
@@ -37,6 +39,7 @@ class MaterialPattern:
         self.spring_slots = np.searchsorted(uk, sk).astype(np.uint32)
         self.face_slots = np.searchsorted(uk, fk).astype(np.uint32)
         self.bend_slots = np.searchsorted(uk, bk).astype(np.uint32)
+        self.body_slots = np.searchsorted(uk, ak).astype(np.uint32)
 
 
 def material_fill(sc, pat, x, x_tilde, dt):
@@ -59,7 +62,59 @@ def material_fill(sc, pat, x, x_tilde, dt):
         O._p(one(c(sc.bending_hbar, np.float32))), float(sc.bending_k), float(sc.bending_scaling),
         O._p(one(pat.spring_slots)), O._p(one(pat.face_slots)), O._p(one(pat.bend_slots)), pat.nnz, O._p(b),
         O._p(diag), O._p(val))
+    if sc.num_bodies:  # rigid mesh rows inert, DOF slot rows from the bodies (orc_abd_fill)
+        rigid, slot = rigid_mask(sc)
+        b[rigid | slot] = 0.0
+        diag[rigid | slot] = 0.0
+        diag[rigid, 0, 0] = diag[rigid, 1, 1] = diag[rigid, 2, 2] = 1.0
+        O.lib().orc_abd_fill(sc.num_bodies, O._p(c(sc.body_dof, np.uint32)),
+                             O._p(c(sc.body_mass.reshape(-1, 16), np.float32)), O._p(c(sc.body_volume, np.float32)),
+                             O._p(c(sc.body_kappa, np.float32)), O._p(body_fixed(sc)), O._p(O.f4(x)),
+                             O._p(O.f4(x_tilde)), float(dt), float(sc.dirichlet), O._p(pat.body_slots), O._p(b),
+                             O._p(diag), O._p(val))
     return b, diag, (pat.rp, pat.col, val[: pat.nnz])
+
+
+def rigid_mask(sc):
+    """(rigid mesh vertices, DOF slots) as boolean masks."""
+    slot = np.zeros(sc.num_verts, bool)
+    if sc.num_bodies:
+        slot[(sc.body_dof.astype(np.int64)[:, None] + np.arange(4)[None]).ravel()] = True
+    rigid = (sc.body != 0xFFFFFFFF) & ~slot
+    return rigid, slot
+
+
+def body_fixed(sc):
+    rigid, _ = rigid_mask(sc)
+    fixed = np.zeros(sc.num_bodies, np.uint8)
+    sel = rigid & (sc.pinned != 0)
+    fixed[sc.body[sel]] = 1
+    return fixed
+
+
+def affine_step(sc, x0, dx, alpha, out):
+    """Rigid mesh vertices of out = p + A x_bar with q = q0 + alpha dq (the device's operation order)."""
+    rigid, _ = rigid_mask(sc)
+    if not rigid.any():
+        return out
+    f = np.float32
+    a = f(alpha)
+    d = sc.body_dof.astype(np.int64)[sc.body[rigid].astype(np.int64)]
+    q = [x0[d + j, :3] + a * dx[d + j, :3] for j in range(4)]
+    m = sc.model_x[rigid, :3]
+    out[rigid, :3] = ((q[1] * m[:, 0:1] + q[2] * m[:, 1:2]) + q[3] * m[:, 2:3]) + q[0]
+    return out
+
+
+def affine_expand(sc, dx):
+    """dx of rigid mesh vertices = J(x_bar) dq (k_abd_expand)."""
+    rigid, _ = rigid_mask(sc)
+    if rigid.any():
+        d = sc.body_dof.astype(np.int64)[sc.body[rigid].astype(np.int64)]
+        q = [dx[d + j, :3] for j in range(4)]
+        m = sc.model_x[rigid, :3]
+        dx[rigid, :3] = ((q[1] * m[:, 0:1] + q[2] * m[:, 1:2]) + q[3] * m[:, 2:3]) + q[0]
+    return dx
 
 
 def material_system(sc, x, x_tilde, dt):
@@ -86,13 +141,19 @@ def newton_iteration(sc, x, x_tilde, dt, timings=None, pattern=None):
     pairs = np.concatenate([
         O.dcd_vf(vf, x, sc.faces, sc.body, sc.vert_area, sc.face_area, sc.d_hat, sc.offset, sc.kappa),
         O.dcd_ee(ee, x, sc.edges, sc.body, sc.edge_area, sc.d_hat, sc.offset, sc.kappa)])
-    b, diag = O.contact_grad_diag(pairs, sc.num_verts, b, diag)
-    B = O.contact_offdiag_bsr(pairs, sc.num_verts)
+    if sc.num_bodies:
+        b, diag = O.contact_grad_diag_abd(pairs, sc, b, diag)
+        B = O.contact_offdiag_bsr_abd(pairs, sc)
+    else:
+        b, diag = O.contact_grad_diag(pairs, sc.num_verts, b, diag)
+        B = O.contact_offdiag_bsr(pairs, sc.num_verts)
     c3 = time.perf_counter()
     dx, st = O.pcg(diag, A, B, b, max_iter=100, rel_tol=1e-4, abs_rz_tol=1e-10, check_every=25)
     c4 = time.perf_counter()
+    dx = affine_expand(sc, dx)
     x1 = x.copy()
     x1[:, :3] += dx[:, :3]
+    x1 = affine_step(sc, x, dx, 1.0, x1)
     O.lbvh_refit(tf, x, x1, sc.faces, sc.offset)
     O.lbvh_refit(te, x, x1, sc.edges, sc.offset)
     cvf, _ = O.lbvh_query_vf(tf, x, x1, sc.d_hat, sc.offset)
@@ -102,6 +163,7 @@ def newton_iteration(sc, x, x_tilde, dt, timings=None, pattern=None):
     toi = min(g1, g2)
     out = x.copy()
     out[:, :3] += np.float32(toi) * dx[:, :3]
+    out = affine_step(sc, x, dx, toi, out)
     c5 = time.perf_counter()
     for k, v in dict(material=c1 - c0, dcd_broad=c2 - c1, dcd_narrow_assembly=c3 - c2, pcg=c4 - c3,
                      ccd=c5 - c4).items():

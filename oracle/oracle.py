@@ -89,6 +89,9 @@ def _declare(L):
         "orc_eval_springs": (None, [U32, P, P, P, P, P, P]),
         "orc_material_energy": (None, [U32, P, P, P, P, F32, F32, U32, P, P, P, U32, P, P, P, P, U32, P, P, P, P, F32,
                                        P]),
+        "orc_contact_grad_diag_abd": (None, [P, U32, P, P, P, P, P]),
+        "orc_contact_offdiag_bsr_abd": (U32, [P, U32, U32, P, P, P, P, P, P, U32]),
+        "orc_abd_fill": (None, [U32, P, P, P, P, P, P, P, F32, F32, P, P, P, P]),
         "orc_material_fill2": (None, [U32, P, P, P, P, P, F32, F32, I32, I32, U32, P, P, F32, U32, P, P, P, F32, F32,
                                       U32, P, P, P, P, F32, F32, P, P, P, U32, P, P, P]),
         "orc_pcg": (I32, [U32, P, P, P, P, P, P, P, P, P, I32, F32, F32, I32, I32, C.POINTER(PcgStats)]),
@@ -307,6 +310,33 @@ def contact_offdiag_bsr(pairs, n_rows):
     return rp, col[:nb], val[:nb]
 
 
+def _abd_args(sc):
+    return (np.ascontiguousarray(sc.body, np.uint32), f4(sc.model_x), np.ascontiguousarray(sc.body_dof, np.uint32))
+
+
+def contact_grad_diag_abd(pairs, sc, b, diag):
+    """contact_grad_diag with the affine-body remap (a rigid side adds to its body's DOF slots)."""
+    pairs = np.ascontiguousarray(pairs, PAIR_DTYPE)
+    b = np.ascontiguousarray(b, np.float32).copy()
+    diag = np.ascontiguousarray(diag, np.float32).copy()
+    body, mx, dof = _abd_args(sc)
+    lib().orc_contact_grad_diag_abd(_p(pairs), pairs.shape[0], _p(body), _p(mx), _p(dof), _p(b), _p(diag))
+    return b, diag
+
+
+def contact_offdiag_bsr_abd(pairs, sc):
+    pairs = np.ascontiguousarray(pairs, PAIR_DTYPE)
+    n_rows = sc.num_verts
+    cap = 56 * max(pairs.shape[0], 1)
+    rp = np.zeros(n_rows + 1, np.uint32)
+    col = np.zeros(cap, np.uint32)
+    val = np.zeros((cap, 9), np.float32)
+    body, mx, dof = _abd_args(sc)
+    nb = lib().orc_contact_offdiag_bsr_abd(_p(pairs), pairs.shape[0], n_rows, _p(body), _p(mx), _p(dof), _p(rp),
+                                           _p(col), _p(val), cap)
+    return rp, col[:nb], val[:nb]
+
+
 def contact_energy(pairs, x, dhat, offset, fp64=True):
     pairs = np.ascontiguousarray(pairs, PAIR_DTYPE)
     return lib().orc_contact_energy(_p(pairs), pairs.shape[0], _p(f4(x)), _p(_v(dhat)), _p(_v(offset)), int(fp64))
@@ -347,6 +377,7 @@ def min_distance(sc, x, radius=5e-3):
     intersection (device_post_dist_check, newton_solver.cpp:3364-3375)."""
     x = f4(x)
     r = np.full(sc.num_verts, radius, np.float32)
+    r[np.asarray(sc.d_hat) < 0] = -1.0  # affine-body DOF slots query nothing
     z = np.zeros(sc.num_verts, np.float32)
     tf = lbvh_build(TREE_FACE, x, sc.faces, sc.num_verts)
     lbvh_refit(tf, x, x, sc.faces, z)
