@@ -430,7 +430,9 @@ typedef struct lcs_scene_desc {
     const uint8_t* pinned;      /* host, or NULL */
     const int8_t* anim_group;   /* host, per vertex animation group of pinned vertices (-1 none) */
     uint32_t n_anim;
-    const float* anim;          /* host, 8 floats per group: centre xyz, axis xyz, rad/s, pad */
+    const float* anim;          /* host, 16 floats per group (FixedPointAnimationInfo): centre xyz, unit axis xyz,
+                                   rad/s, mode (bits: 1 rotate, 2 scale, 4 translate), translation velocity xyz,
+                                   scale rate xyz, 2 pad */
     float dt;
     float gravity[3];
     float kappa;                /* stiffness_collision */
@@ -470,6 +472,11 @@ typedef struct lcs_scene_desc {
     const float* body_volume;        /* host, per body */
     const float* body_kappa;         /* host, per body: RigidMaterial stiffness (orthogonality) */
     const float* model_x;            /* host float4 per vertex (rigid vertices; others ignored) */
+    /* per-element material parameters (SimulationData's sa_stretch_faces_mu_lambda,
+     * sa_bending_edges_stiffness, sa_stretch_spring_stiffness), or NULL for the scalars above */
+    const float* stretch_mu_lambda;  /* host, 2 floats per stretch face */
+    const float* bending_stiffness;  /* host, per stencil (area_bending_stiffness of its mesh) */
+    const float* spring_stiffness;   /* host, per edge */
 } lcs_scene_desc;
 
 enum {

@@ -53,7 +53,8 @@ class SceneDesc(C.Structure):
                 ("n_stretch_faces", C.c_uint32), ("stretch_faces", P), ("stretch_dm_inv", P), ("stretch_area", P),
                 ("stretch_mu", C.c_float), ("stretch_lambda", C.c_float), ("bending_rest_angle", P),
                 ("bending_hbar", P), ("bending_scaling", C.c_float), ("n_bodies", C.c_uint32), ("body_dof", P),
-                ("body_mass", P), ("body_volume", P), ("body_kappa", P), ("model_x", P)]
+                ("body_mass", P), ("body_volume", P), ("body_kappa", P), ("model_x", P),
+                ("stretch_mu_lambda", P), ("bending_stiffness", P), ("spring_stiffness", P)]
 
 
 class AbdView(C.Structure):

@@ -51,8 +51,12 @@ struct Status {
     float pad;
 };
 
+// animation of a group of pinned vertices (FixedPointAnimationInfo::fn_affine_position,
+// Solver/Initializer/init_mesh_data.h:61-92): mode bit 1 scale by (s t), bit 0 rotate about the axis
+// through the centre by omega t, bit 2 translate by (tr t), in that order
 struct Anim {
-    float cx, cy, cz, ax, ay, az, omega, pad;
+    float cx, cy, cz, ax, ay, az, omega, mode;
+    float tx, ty, tz, sx, sy, sz, pad0, pad1;
 };
 
 // affine bodies on the device (body == nullptr: none).  slot[v] = j for the j-th DOF slot of a body
@@ -101,14 +105,22 @@ __global__ void k_reset_status(Status* s)
     }
 }
 
-// targets of animated pinned vertices: rotation of the rest position about an axis
+// targets of animated pinned vertices at time t (WorldData::get_fixed_point_target_positions,
+// init_mesh_data.cpp:272-297)
 __global__ void k_targets(uint32_t n, const float4* __restrict__ rest, const int8_t* __restrict__ group,
                           const Anim* __restrict__ anim, float t, float4* __restrict__ target)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 p = rest[i];
         const int g = group ? group[i] : -1;
-        if (g >= 0) {
+        const int mode = g >= 0 ? (int)anim[g].mode : 0;
+        if (g >= 0 && (mode & 2)) {
+            const Anim A = anim[g];
+            p.x = (A.sx * t) * p.x;
+            p.y = (A.sy * t) * p.y;
+            p.z = (A.sz * t) * p.z;
+        }
+        if (g >= 0 && (mode & 1)) {
             const Anim A = anim[g];
             const float ang = A.omega * t;
             const float c = cosf(ang), s = sinf(ang);
@@ -118,6 +130,12 @@ __global__ void k_targets(uint32_t n, const float4* __restrict__ rest, const int
             p.x = A.cx + px * c + kx * s + A.ax * d * (1.0f - c);
             p.y = A.cy + py * c + ky * s + A.ay * d * (1.0f - c);
             p.z = A.cz + pz * c + kz * s + A.az * d * (1.0f - c);
+        }
+        if (g >= 0 && (mode & 4)) {
+            const Anim A = anim[g];
+            p.x = p.x + A.tx * t;
+            p.y = p.y + A.ty * t;
+            p.z = p.z + A.tz * t;
         }
         target[i] = p;
     }
@@ -216,11 +234,12 @@ __device__ __forceinline__ void atomic_add3(float4* p, float x, float y, float z
 }
 
 // fn_evaluate_spring + its assembly (newton_solver.cpp:1003-1045): projected spring Hessian
-__global__ void k_springs(uint32_t ne, const uint2* __restrict__ edges, const float* __restrict__ rest_len, float k,
-                          const float4* __restrict__ x, float4* b, float4* diag, const uint32_t* __restrict__ slots,
-                          uint32_t cs, float* mat_val)
+__global__ void k_springs(uint32_t ne, const uint2* __restrict__ edges, const float* __restrict__ rest_len,
+                          const float* __restrict__ kper, float k_scalar, const float4* __restrict__ x, float4* b,
+                          float4* diag, const uint32_t* __restrict__ slots, uint32_t cs, float* mat_val)
 {
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+        const float k = kper ? kper[e] : k_scalar;
         const uint2 ed = edges[e];
         const float4 p0 = x[ed.x], p1 = x[ed.y];
         const float dx = p0.x - p1.x, dy = p0.y - p1.y, dz = p0.z - p1.z;
@@ -484,13 +503,15 @@ __device__ __forceinline__ void red_off(float* O, uint32_t cs, const float* K, b
 // 705-789): Baraff-Witkin stretch and shear added straight into b, the diagonal and the material
 // blocks; slots: the 6 off-diagonal blocks (0,1) (0,2) (1,0) (1,2) (2,0) (2,1) of each face
 __global__ void k_stretch_bw98(uint32_t nf, const uint4* __restrict__ faces, const float4* __restrict__ dm,
-                               const float* __restrict__ area, float mu, float lambda, const float4* __restrict__ x,
-                               float4* b, float4* diag, const uint32_t* __restrict__ slots, uint32_t cs, float* mat_val)
+                               const float* __restrict__ area, const float2* __restrict__ ml, float mu, float lambda,
+                               const float4* __restrict__ x, float4* b, float4* diag, const uint32_t* __restrict__ slots,
+                               uint32_t cs, float* mat_val)
 {
     for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x) {
         const uint4 fc = faces[f];
+        const float2 m = ml ? ml[f] : make_float2(mu, lambda);
         Bw98Out o;
-        bw98_face(ld3(x, fc.x), ld3(x, fc.y), ld3(x, fc.z), dm[f], mu, lambda, area[f], o);
+        bw98_face(ld3(x, fc.x), ld3(x, fc.y), ld3(x, fc.z), dm[f], m.x, m.y, area[f], o);
         const uint32_t v[3] = {fc.x, fc.y, fc.z};
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
@@ -510,16 +531,16 @@ __global__ void k_stretch_bw98(uint32_t nf, const uint4* __restrict__ faces, con
 // fn_evaluate_bending + fn_material_energy_assembly_bending (newton_solver.cpp:1102-1175, 790-801):
 // dihedral-angle bending, Gauss-Newton blocks k g_i g_j^T; slots as k_bending
 __global__ void k_bending_dihedral(uint32_t nb, const uint4* __restrict__ stencil, const float* __restrict__ rest_angle,
-                                   const float* __restrict__ hbar, float k_area, const float4* __restrict__ x,
-                                   float4* b, float4* diag, const uint32_t* __restrict__ slots, uint32_t cs,
-                                   float* mat_val)
+                                   const float* __restrict__ hbar, const float* __restrict__ kper, float k,
+                                   float scaling, const float4* __restrict__ x, float4* b, float4* diag,
+                                   const uint32_t* __restrict__ slots, uint32_t cs, float* mat_val)
 {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nb; s += gridDim.x * blockDim.x) {
         const uint4 e = stencil[s];
         const uint32_t v[4] = {e.x, e.y, e.z, e.w};
         v3 g[4];
         const float theta = dihedral_angle_grad(ld3(x, e.x), ld3(x, e.y), ld3(x, e.z), ld3(x, e.w), g);
-        const float stiff = k_area * hbar[s];
+        const float stiff = ((kper ? kper[s] : k) * scaling) * hbar[s];
         const float sd = stiff * (theta - rest_angle[s]);
         int t = 0;
 #pragma unroll
@@ -648,6 +669,10 @@ struct LsArgs {
     const uint2* edges;
     const float* rest_len;
     float spring_k;
+    const float* spring_kper;
+    const float2* ml;
+    const float* bend_kper;
+    float bend_scaling;
     const uint4* sfaces;
     const float4* dm;
     const float* sarea;
@@ -714,13 +739,14 @@ __global__ void __launch_bounds__(256) k_ls_energy(LsArgs a, int j0, const Statu
             for (int k = 0; k < NS; ++k) {
                 const v3 d = ls_pos(a, ed.y, al[k]) - ls_pos(a, ed.x, al[k]);
                 const float C = sqrtf(dot3(d, d)) - a.rest_len[i];
-                e[k] += (double)(0.5f * a.spring_k * C * C);
+                e[k] += (double)(0.5f * (a.spring_kper ? a.spring_kper[i] : a.spring_k) * C * C);
             }
         }
         if (i < a.Fs) {
             const uint4 fc = a.sfaces[i];
             const float4 dm = a.dm[i];
             const float ar = a.sarea[i];
+            const float2 ml = a.ml ? a.ml[i] : make_float2(a.mu, a.lambda);
 #pragma unroll
             for (int k = 0; k < NS; ++k) {
                 const v3 x0 = ls_pos(a, fc.x, al[k]), e1 = ls_pos(a, fc.y, al[k]) - x0, e2 = ls_pos(a, fc.z, al[k]) - x0;
@@ -729,20 +755,21 @@ __global__ void __launch_bounds__(256) k_ls_energy(LsArgs a, int j0, const Statu
                 const v3 Fv = mk3(__fmaf_rn(e2.x, dm.w, e1.x * dm.z), __fmaf_rn(e2.y, dm.w, e1.y * dm.z),
                                   __fmaf_rn(e2.z, dm.w, e1.z * dm.z));
                 const float su = sqrtf(dot3(Fu, Fu)) - 1.0f, sv = sqrtf(dot3(Fv, Fv)) - 1.0f, i6 = dot3(Fu, Fv);
-                e[k] += (double)(ar * (0.5f * a.mu * (su * su + sv * sv) + 0.5f * a.lambda * (i6 * i6)));
+                e[k] += (double)(ar * (0.5f * ml.x * (su * su + sv * sv) + 0.5f * ml.y * (i6 * i6)));
             }
         }
         if (i < a.B) {
             const uint4 st4 = a.bend[i];
             const uint32_t v[4] = {st4.x, st4.y, st4.z, st4.w};
             if (a.bending_model == LCS_BENDING_DIHEDRAL) {
-                const float stiff = a.kb * a.hbar[i], ra = a.rest_angle[i];
+                const float kb = a.bend_kper ? a.bend_kper[i] : a.kb, hb = a.hbar[i];
+                const float ra = a.rest_angle[i];
 #pragma unroll
                 for (int k = 0; k < NS; ++k) {
                     v3 g[4];
                     const float d = dihedral_angle_grad(ls_pos(a, v[0], al[k]), ls_pos(a, v[1], al[k]),
                                                         ls_pos(a, v[2], al[k]), ls_pos(a, v[3], al[k]), g) - ra;
-                    e[k] += (double)(0.5f * stiff * d * d);
+                    e[k] += (double)(0.5f * kb * a.bend_scaling * hb * d * d);
                 }
             } else {  // quadratic: E = k/2 sum_ij Q_ij (x_i - X_i).(x_j - X_j)
                 const float* q = a.Q + 16 * (size_t)i;
@@ -949,6 +976,8 @@ struct lcs_newton {
     float4* model_x = nullptr;
     int8_t* slot = nullptr;
     uint32_t* body_slots = nullptr;  // material-matrix slots of each body's 12 off-diagonal blocks
+    float2* ml = nullptr;           // per-face mu, lambda (or null: the scalars)
+    float *bend_kper = nullptr, *spring_kper = nullptr;  // per-stencil / per-edge stiffness (or null)
     uint4* sfaces = nullptr;        // BW98 stretch faces
     float4* dm = nullptr;           // their rest Dm^-1
     float *sarea = nullptr, *rest_angle = nullptr, *hbar = nullptr;
@@ -1354,7 +1383,9 @@ LsArgs ls_args(const lcs_newton* h)
         a.edges = h->edges;
         a.rest_len = h->rest_len;
         a.spring_k = d.spring_k;
+        a.spring_kper = h->spring_kper;
     } else {
+        a.ml = h->ml;
         a.Fs = h->Fs;
         a.sfaces = h->sfaces;
         a.dm = h->dm;
@@ -1368,7 +1399,9 @@ LsArgs ls_args(const lcs_newton* h)
         a.rest_angle = h->rest_angle;
         a.hbar = h->hbar;
         a.Q = h->Q;
-        a.kb = d.bending_model == LCS_BENDING_DIHEDRAL ? d.bending_k * d.bending_scaling : d.bending_k;
+        a.kb = d.bending_k;
+        a.bend_kper = h->bend_kper;
+        a.bend_scaling = d.bending_scaling;
         a.bending_model = d.bending_model;
     }
     a.P = h->cap_pairs;
@@ -1463,20 +1496,20 @@ int newton_iteration(lcs_newton* h)
         LCS_CUDA_TRY(cudaMemsetAsync(h->mat_val, 0, sizeof(float) * h->sell_vals, h->s));
         const uint32_t cs = h->sell ? 128u : 1u;
         if (h->E && d.stretch_model == LCS_STRETCH_SPRING) {
-            k_springs<<<grid256(h->E), 256, 0, h->s>>>(h->E, h->edges, h->rest_len, d.spring_k, h->x, h->b, h->diag,
-                                                 h->spring_slots, cs, h->mat_val);
+            k_springs<<<grid256(h->E), 256, 0, h->s>>>(h->E, h->edges, h->rest_len, h->spring_kper, d.spring_k, h->x,
+                                                       h->b, h->diag, h->spring_slots, cs, h->mat_val);
             lcs_count_launch();
         }
         if (h->Fs && d.stretch_model == LCS_STRETCH_BW98) {
-            k_stretch_bw98<<<grid256(h->Fs), 256, 0, h->s>>>(h->Fs, h->sfaces, h->dm, h->sarea, d.stretch_mu,
-                                                       d.stretch_lambda, h->x, h->b, h->diag, h->face_slots, cs,
-                                                       h->mat_val);
+            k_stretch_bw98<<<grid256(h->Fs), 256, 0, h->s>>>(h->Fs, h->sfaces, h->dm, h->sarea, h->ml, d.stretch_mu,
+                                                             d.stretch_lambda, h->x, h->b, h->diag, h->face_slots, cs,
+                                                             h->mat_val);
             lcs_count_launch();
         }
         if (h->B && d.bending_model == LCS_BENDING_DIHEDRAL) {
-            k_bending_dihedral<<<grid256(h->B), 256, 0, h->s>>>(h->B, h->bend, h->rest_angle, h->hbar,
-                                                          d.bending_k * d.bending_scaling, h->x, h->b, h->diag,
-                                                          h->bend_slots, cs, h->mat_val);
+            k_bending_dihedral<<<grid256(h->B), 256, 0, h->s>>>(h->B, h->bend, h->rest_angle, h->hbar, h->bend_kper,
+                                                                d.bending_k, d.bending_scaling, h->x, h->b, h->diag,
+                                                                h->bend_slots, cs, h->mat_val);
             lcs_count_launch();
         } else if (h->B && d.bending_model == LCS_BENDING_QUADRATIC) {
             k_bending<<<grid256(h->B), 256, 0, h->s>>>(h->B, h->bend, h->Q, d.bending_k, h->x, h->rest, h->b, h->diag,
@@ -1784,6 +1817,10 @@ int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batc
         A(upload(h->model_x, reinterpret_cast<const float4*>(d->model_x), V));
         A(upload(h->slot, slot.data(), V));
     }
+    if (d->stretch_model == LCS_STRETCH_BW98 && d->stretch_mu_lambda)
+        A(upload(h->ml, reinterpret_cast<const float2*>(d->stretch_mu_lambda), d->n_stretch_faces));
+    if (d->bending_model == LCS_BENDING_DIHEDRAL && d->bending_stiffness) A(upload(h->bend_kper, d->bending_stiffness, h->B));
+    if (d->stretch_model == LCS_STRETCH_SPRING && d->spring_stiffness) A(upload(h->spring_kper, d->spring_stiffness, h->E));
     if (d->stretch_model == LCS_STRETCH_BW98) {
         h->Fs = d->n_stretch_faces;
         A(upload(h->sfaces, reinterpret_cast<const uint4*>(d->stretch_faces), h->Fs));
@@ -1916,10 +1953,13 @@ extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_s
     std::vector<uint32_t> sfaces(4 * (size_t)Fs);
     std::vector<float> dm(4 * (size_t)Fs), sarea(Fs), rest_angle(dih ? B : 0), hbar(dih ? B : 0);
     const uint32_t NBt = aoff[n_scenes];
+    const bool has_ml = d0.stretch_mu_lambda != nullptr, has_bk = d0.bending_stiffness != nullptr,
+               has_sk = d0.spring_stiffness != nullptr;
+    std::vector<float> mlv(has_ml ? 2 * (size_t)Fs : 0), bkv(has_bk ? B : 0), skv(has_sk ? E : 0);
     std::vector<uint32_t> body_dof(NBt);
     std::vector<float> bmass(16 * (size_t)NBt), bvol(NBt), bkappa(NBt), model_x(NBt ? 4 * (size_t)V : 0, 0.0f);
     std::vector<float> x(4 * (size_t)V), v(4 * (size_t)V, 0.0f), Q(quad ? 16 * (size_t)B : 0), rest_len(E), vert_area(V),
-        face_area(F), edge_area(E), mass(V), dhat(V), offset(V), anim(8 * (size_t)std::max(groups, 1u), 0.0f);
+        face_area(F), edge_area(E), mass(V), dhat(V), offset(V), anim(16 * (size_t)std::max(groups, 1u), 0.0f);
     std::vector<uint32_t> faces(4 * (size_t)F), edges(2 * (size_t)E), bend(4 * (size_t)B), body(V, kInvalid);
     std::vector<uint8_t> pinned(V, 0);
     std::vector<int8_t> group(V, -1);
@@ -1962,11 +2002,17 @@ extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_s
             bkappa[aoff[s] + k] = d.body_kappa[k];
         }
         if (d.n_bodies) std::memcpy(&model_x[4 * (size_t)vo], d.model_x, 16 * (size_t)d.n_verts);
+        if ((d.stretch_mu_lambda != nullptr) != has_ml || (d.bending_stiffness != nullptr) != has_bk ||
+            (d.spring_stiffness != nullptr) != has_sk)
+            return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create_batch: per-element material arrays given for some scenes only");
+        if (has_ml && ns) std::memcpy(&mlv[2 * (size_t)soff[s]], d.stretch_mu_lambda, 8 * (size_t)ns);
+        if (has_bk && d.n_bending) std::memcpy(&bkv[boff[s]], d.bending_stiffness, 4 * (size_t)d.n_bending);
+        if (has_sk) std::memcpy(&skv[eoff[s]], d.spring_stiffness, 4 * (size_t)d.n_edges);
         if (d.pinned) std::memcpy(&pinned[vo], d.pinned, d.n_verts);
         if (d.anim_group && d.n_anim) {
             for (uint32_t k = 0; k < d.n_verts; ++k)
                 group[vo + k] = d.anim_group[k] >= 0 ? (int8_t)(d.anim_group[k] + (int)g0) : (int8_t)-1;
-            std::memcpy(&anim[8 * (size_t)g0], d.anim, 32 * (size_t)d.n_anim);
+            std::memcpy(&anim[16 * (size_t)g0], d.anim, 64 * (size_t)d.n_anim);
             g0 += d.n_anim;
         }
     }
@@ -1978,6 +2024,8 @@ extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_s
     D.bending_rest_angle = rest_angle.data(); D.bending_hbar = hbar.data();
     D.n_bodies = NBt; D.body_dof = body_dof.data(); D.body_mass = bmass.data(); D.body_volume = bvol.data();
     D.body_kappa = bkappa.data(); D.model_x = NBt ? model_x.data() : nullptr;
+    D.stretch_mu_lambda = has_ml ? mlv.data() : nullptr; D.bending_stiffness = has_bk ? bkv.data() : nullptr;
+    D.spring_stiffness = has_sk ? skv.data() : nullptr;
     D.face_area = face_area.data(); D.edge_area = edge_area.data(); D.mass = mass.data(); D.d_hat = dhat.data();
     D.offset = offset.data(); D.body = body.data(); D.pinned = pinned.data();
     D.anim_group = groups ? group.data() : nullptr; D.n_anim = groups; D.anim = groups ? anim.data() : nullptr;
@@ -2080,6 +2128,7 @@ extern "C" int lcs_newton_destroy(lcs_newton* h)
     }
     void* ptrs[] = {h->faces, h->edges, h->bend, h->sfaces, h->dm, h->sarea, h->rest_angle, h->hbar, h->face_slots,
                     h->body_dof, h->bmass, h->bvol, h->bkappa, h->bfixed, h->model_x, h->slot, h->body_slots,
+                    h->ml, h->bend_kper, h->spring_kper,
                     h->Q, h->rest_len, h->vert_area, h->face_area, h->edge_area,
                     h->mass, h->dhat, h->offset, h->body, h->pinned, h->group, h->anim, h->rest, h->x, h->v,
                     h->x_step, h->x_iter, h->x_tilde, h->target, h->dx, h->b, h->diag, h->mat_rp, h->mat_col,

@@ -41,14 +41,21 @@ def scene_desc(sc, keep, nonlinear_iters=3, pcg_max_iter=100, pcg_rel_tol=1e-4, 
     d.body = arr(sc.body, np.uint32)
     d.pinned = arr(sc.pinned, np.uint8)
     groups = np.full(sc.num_verts, -1, np.int8)
-    anim = np.zeros((max(len(sc.anims), 1), 8), np.float32)
-    for gi, (vids, center, axis, omega) in enumerate(sc.anims):
+    anim = np.zeros((max(len(sc.anims), 1), 16), np.float32)
+    for gi, an in enumerate(sc.anims):
+        vids, center, axis, omega = an[:4]
+        translate, scale, mode = (an[4], an[5], an[6]) if len(an) > 4 else (None, None, 1)
         groups[vids] = gi
         ax = np.asarray(axis, np.float64)
-        ax = ax / np.linalg.norm(ax)
+        n_ax = np.linalg.norm(ax)
         anim[gi, :3] = center
-        anim[gi, 3:6] = ax
+        anim[gi, 3:6] = ax / n_ax if n_ax > 0 else 0.0
         anim[gi, 6] = omega
+        anim[gi, 7] = mode
+        if translate is not None:
+            anim[gi, 8:11] = translate
+        if scale is not None:
+            anim[gi, 11:14] = scale
     d.anim_group = arr(groups, np.int8)
     d.n_anim = len(sc.anims)
     d.anim = arr(anim, np.float32)
@@ -68,6 +75,12 @@ def scene_desc(sc, keep, nonlinear_iters=3, pcg_max_iter=100, pcg_rel_tol=1e-4, 
     d.bending_rest_angle = arr(sc.bending_rest_angle, np.float32)
     d.bending_hbar = arr(sc.bending_hbar, np.float32)
     d.bending_scaling = sc.bending_scaling
+    if sc.stretch_mu_lambda is not None:
+        d.stretch_mu_lambda = arr(sc.stretch_mu_lambda, np.float32)
+    if sc.bending_stiffness is not None:
+        d.bending_stiffness = arr(sc.bending_stiffness, np.float32)
+    if sc.spring_stiffness is not None:
+        d.spring_stiffness = arr(sc.spring_stiffness, np.float32)
     d.n_bodies = sc.num_bodies
     if sc.num_bodies:
         d.body_dof = arr(sc.body_dof, np.uint32)

@@ -44,6 +44,10 @@ class MeshPart:
     rotate: tuple | None = None  # pinned-vertex animation: (axis_point(3), axis(3), ang_vel, mask)
     rigid: bool = False    # an affine body (RigidMaterial): 12 DOFs q = [p, a0, a1, a2], x = p + A x_bar
     rigid_stiffness: float = 1e6  # RigidMaterial::stiffness (orthogonality kappa)
+    total_mass: float | None = None  # MaterialBase::mass: the part's mass when given (else volume x density)
+    youngs_modulus: float | None = None      # ClothMaterial (None: the scene's lame_params)
+    poisson_ratio: float | None = None
+    area_bending_stiffness: float | None = None
 
 
 @dataclasses.dataclass
@@ -89,6 +93,10 @@ class Scene:
     body_volume: np.ndarray = None         # (NB,) float32
     body_kappa: np.ndarray = None          # (NB,) float32
     model_x: np.ndarray = None             # (V, 4) float32
+    # per-element material parameters (one value per scene unless the parts' materials differ)
+    stretch_mu_lambda: np.ndarray = None   # (Fs, 2) float32
+    bending_stiffness: np.ndarray = None   # (B,) float32
+    spring_stiffness: np.ndarray = None    # (E,) float32
 
     @property
     def num_bodies(self):
@@ -99,11 +107,20 @@ class Scene:
         return self.x.shape[0]
 
     def targets(self, t):
-        """Positions of the pinned vertices at time t (others: rest position)."""
+        """Positions of the pinned vertices at time t (others: rest position): scale, rotation, translation
+        (FixedPointAnimationInfo::fn_affine_position, init_mesh_data.h:61-92)."""
         out = self.x[:, :3].astype(np.float64).copy()
-        for vids, center, axis, omega in self.anims:
-            p = self.x[vids, :3].astype(np.float64) - center
-            out[vids] = _rotate(p, axis, omega * t) + center
+        for an in self.anims:
+            vids, center, axis, omega = an[:4]
+            translate, scale, mode = (an[4], an[5], an[6]) if len(an) > 4 else (None, None, 1)
+            p = out[vids]
+            if mode & 2:
+                p = np.asarray(scale, np.float64) * t * p
+            if mode & 1:
+                p = _rotate(p - center, axis, omega * t) + center
+            if mode & 4:
+                p = p + np.asarray(translate, np.float64) * t
+            out[vids] = p
         return out.astype(np.float32)
 
 
@@ -312,7 +329,8 @@ def _min_rest_dist(x, faces, edges):
     return best
 
 
-def assemble(name, parts, dt, gravity, kappa, spring_k=None, bending_k=5e-3, stretch_model=1, bending_model=2):
+def assemble(name, parts, dt, gravity, kappa, spring_k=None, bending_k=5e-3, stretch_model=1, bending_model=2,
+             lame_params=(1e5, 0.25, 2e-3)):
     """Merge mesh parts into one Scene (vertex/face order = part order; the DOF slots of rigid parts,
     four per body, follow all mesh vertices)."""
     xs, fs, pins, vmesh, anims = [], [], [], [], []
@@ -363,7 +381,7 @@ def assemble(name, parts, dt, gravity, kappa, spring_k=None, bending_k=5e-3, str
         th = np.float32(part.material_thickness)
         vert_vol = (vert_area[vm] * th).astype(np.float32)
         body_vol = float(np.sum(face_area[sel_f].astype(np.float64) * th))
-        body_mass = np.float32(body_vol * part.density)
+        body_mass = np.float32(part.total_mass if part.total_mass else body_vol * part.density)
         mass[vm] = (vert_vol / np.float32(body_vol) * body_mass).astype(np.float32)
     x4 = np.zeros((V, 4), np.float32)
     x4[:, :3] = x3
@@ -428,8 +446,23 @@ def assemble(name, parts, dt, gravity, kappa, spring_k=None, bending_k=5e-3, str
         offset = np.concatenate([offset, np.zeros(4 * NB, np.float32)])
     sf4 = np.zeros((sf.shape[0], 4), np.uint32)
     sf4[:, :3] = sf
-    mu, lam = lame()
+    mu, lam = lame(*lame_params)
     rest_angle, hbar = _dihedral_rest(x3, bending) if len(bending) else (np.zeros(0, np.float32),) * 2
+    # per-element materials: each element takes its part's (mesh of its first vertex)
+    part_ml = np.zeros((len(parts), 2), np.float32)
+    part_kb = np.zeros(len(parts), np.float32)
+    for m, part in enumerate(parts):
+        E_, nu_, th_ = lame_params
+        if part.youngs_modulus is not None:
+            E_ = part.youngs_modulus
+        if part.poisson_ratio is not None:
+            nu_ = part.poisson_ratio
+        part_ml[m] = lame(E_, nu_, part.material_thickness if part.youngs_modulus is not None else th_)
+        part_kb[m] = bending_k if part.area_bending_stiffness is None else part.area_bending_stiffness
+    vm_all = np.concatenate([vmesh, np.zeros(4 * NB, vmesh.dtype)]) if NB else vmesh
+    stretch_ml = part_ml[vm_all[sf[:, 0]]] if len(sf) else np.zeros((0, 2), np.float32)
+    bend_k = part_kb[vm_all[bending[:, 0]]] if len(bending) else np.zeros(0, np.float32)
+    spring_k_e = part_ml[vm_all[edges[:, 0]], 0] if len(edges) else np.zeros(0, np.float32)
     return Scene(name=name, x=x4, faces=f4, edges=edges.astype(np.uint32), bending=bending.astype(np.uint32),
                  vert_area=vert_area.astype(np.float32), face_area=face_area, edge_area=edge_area.astype(np.float32),
                  mass=mass, pinned=pinned, d_hat=d_hat, offset=offset, body=body,
@@ -440,7 +473,9 @@ def assemble(name, parts, dt, gravity, kappa, spring_k=None, bending_k=5e-3, str
                  bending_rest_angle=rest_angle, bending_hbar=hbar,
                  body_dof=body_dof if NB else None, body_mass=body_mass if NB else None,
                  body_volume=body_volume if NB else None, body_kappa=body_kappa if NB else None,
-                 model_x=model_x if NB else None)
+                 model_x=model_x if NB else None, stretch_mu_lambda=stretch_ml.astype(np.float32),
+                 bending_stiffness=bend_k.astype(np.float32),
+                 spring_stiffness=(spring_k_e if spring_k is None else np.full(len(edges), spring_k)).astype(np.float32))
 
 
 def cloth_on_sphere(n=64, spacing=0.01, seed=0, subdiv=4, radius=0.2, drop=0.05):

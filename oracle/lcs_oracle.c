@@ -1231,7 +1231,8 @@ int orc_pcg(uint32_t n, const float* diag12, const uint32_t* rp_a, const uint32_
  * ========================================================================================= */
 void orc_material_fill(uint32_t V, uint32_t E, uint32_t B, const float* x4, const float* rest4,
                        const float* xt4, const float* mass, const uint8_t* pinned, float dt,
-                       float dirichlet, const uint32_t* edges, const float* rest_len, float spring_k,
+                       float dirichlet, const uint32_t* edges, const float* rest_len, float spring_k_scalar,
+                       const float* spring_kper,
                        const uint32_t* stencil, const float* Q16, float bending_k,
                        const uint32_t* spring_slots, const uint32_t* bend_slots, uint32_t nnz,
                        float* b4, float* diag12, float* val9)
@@ -1256,6 +1257,7 @@ void orc_material_fill(uint32_t V, uint32_t E, uint32_t B, const float* x4, cons
         diag12[12 * i + 10] = hd;
     }
     for (uint32_t e = 0; e < E; ++e) {
+        const float spring_k = spring_kper ? spring_kper[e] : spring_k_scalar;
         uint32_t a = edges[2 * e], c = edges[2 * e + 1];
         float d[3] = {x4[4 * a] - x4[4 * c], x4[4 * a + 1] - x4[4 * c + 1], x4[4 * a + 2] - x4[4 * c + 2]};
         float l = sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);

@@ -129,7 +129,7 @@ float orc_min_distance(const uint32_t* vf, uint32_t n_vf, const uint32_t* ee, ui
 void orc_material_fill(uint32_t V, uint32_t E, uint32_t B, const float* x4, const float* rest4,
                        const float* xt4, const float* mass, const uint8_t* pinned, float dt,
                        float dirichlet, const uint32_t* edges, const float* rest_len, float spring_k,
-                       const uint32_t* stencil, const float* Q16, float bending_k,
+                       const float* spring_kper, const uint32_t* stencil, const float* Q16, float bending_k,
                        const uint32_t* spring_slots, const uint32_t* bend_slots, uint32_t nnz,
                        float* b4, float* diag12, float* val9);
 
@@ -155,7 +155,8 @@ void orc_material_fill2(uint32_t V, const float* x4, const float* rest4, const f
                         uint32_t B, const uint32_t* stencil, const float* Q16, const float* rest_angle,
                         const float* hbar, float bending_k, float bending_scaling, const uint32_t* spring_slots,
                         const uint32_t* face_slots, const uint32_t* bend_slots, uint32_t nnz, float* b4,
-                        float* diag12, float* val9);
+                        float* diag12, float* val9, const float* ml2, const float* bend_kper,
+                        const float* spring_kper);
 
 /* ---------------- affine bodies ---------------- */
 void orc_contact_grad_diag_abd(const orc_pair* pairs, uint32_t n, const uint32_t* body, const float* model_x4,

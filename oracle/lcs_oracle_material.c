@@ -291,12 +291,13 @@ void orc_material_fill2(uint32_t V, const float* x4, const float* rest4, const f
                         uint32_t B, const uint32_t* stencil, const float* Q16, const float* rest_angle,
                         const float* hbar, float bending_k, float bending_scaling, const uint32_t* spring_slots,
                         const uint32_t* face_slots, const uint32_t* bend_slots, uint32_t nnz, float* b4,
-                        float* diag12, float* val9)
+                        float* diag12, float* val9, const float* ml2, const float* bend_kper,
+                        const float* spring_kper)
 {
-    /* inertia, and the spring / quadratic models when selected */
+    /* inertia, and the spring / quadratic models when selected; per-element parameters when given */
     orc_material_fill(V, stretch_model == 0 ? E : 0, bending_model == 1 ? B : 0, x4, rest4, xt4, mass, pinned, dt,
-                      dirichlet, edges, rest_len, spring_k, stencil, Q16, bending_k, spring_slots, bend_slots, nnz, b4,
-                      diag12, val9);
+                      dirichlet, edges, rest_len, spring_k, spring_kper, stencil, Q16, bending_k, spring_slots,
+                      bend_slots, nnz, b4, diag12, val9);
     if (stretch_model == 1) {
         static const int src[6] = {3, 4, 3, 5, 4, 5}, tr[6] = {0, 0, 1, 0, 1, 1};  /* (0,1) (0,2) (1,0) (1,2) (2,0) (2,1) */
 #pragma omp parallel for schedule(static)
@@ -304,8 +305,8 @@ void orc_material_fill2(uint32_t V, const float* x4, const float* rest4, const f
             const size_t f = (size_t)fl;
             const uint32_t* v = sfaces4 + 4 * f;
             float g[9], K[54];
-            orc_bw98_face(x4 + 4 * (size_t)v[0], x4 + 4 * (size_t)v[1], x4 + 4 * (size_t)v[2], dm4 + 4 * f, mu,
-                          lambda, sarea[f], g, K);
+            orc_bw98_face(x4 + 4 * (size_t)v[0], x4 + 4 * (size_t)v[1], x4 + 4 * (size_t)v[2], dm4 + 4 * f,
+                          ml2 ? ml2[2 * f] : mu, ml2 ? ml2[2 * f + 1] : lambda, sarea[f], g, K);
             for (int a = 0; a < 3; ++a) {
                 for (int k = 0; k < 3; ++k) {
 #pragma omp atomic
@@ -329,7 +330,7 @@ void orc_material_fill2(uint32_t V, const float* x4, const float* rest4, const f
         }
     }
     if (bending_model == 2) {
-        const float kb = bending_k * bending_scaling;
+
 #pragma omp parallel for schedule(static)
         for (long long sl = 0; sl < (long long)B; ++sl) {
             const size_t s = (size_t)sl;
@@ -337,7 +338,7 @@ void orc_material_fill2(uint32_t V, const float* x4, const float* rest4, const f
             float g[12];
             const float th = orc_dihedral(x4 + 4 * (size_t)v[0], x4 + 4 * (size_t)v[1], x4 + 4 * (size_t)v[2],
                                           x4 + 4 * (size_t)v[3], g);
-            const float stiff = kb * hbar[s];
+            const float stiff = ((bend_kper ? bend_kper[s] : bending_k) * bending_scaling) * hbar[s];
             const float sd = stiff * (th - rest_angle[s]);
             int t = 0;
             for (int i = 0; i < 4; ++i) {

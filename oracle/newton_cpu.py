@@ -51,6 +51,7 @@ def material_fill(sc, pat, x, x_tilde, dt):
     val = np.zeros((max(pat.nnz, 1), 9), np.float32)
     c = np.ascontiguousarray
     one = lambda a: a if a.size else np.zeros(1, a.dtype)  # noqa: E731
+    per = [_opt(sc.stretch_mu_lambda), _opt(sc.bending_stiffness), _opt(sc.spring_stiffness)]  # kept alive
     O.lib().orc_material_fill2(
         V, O._p(O.f4(x)), O._p(c(sc.x, np.float32)), O._p(O.f4(x_tilde)), O._p(c(sc.mass, np.float32)),
         O._p(c(sc.pinned, np.uint8)), float(dt), float(sc.dirichlet), int(sc.stretch_model), int(sc.bending_model),
@@ -61,7 +62,7 @@ def material_fill(sc, pat, x, x_tilde, dt):
         O._p(one(c(sc.bending_Q.reshape(-1, 16), np.float32))), O._p(one(c(sc.bending_rest_angle, np.float32))),
         O._p(one(c(sc.bending_hbar, np.float32))), float(sc.bending_k), float(sc.bending_scaling),
         O._p(one(pat.spring_slots)), O._p(one(pat.face_slots)), O._p(one(pat.bend_slots)), pat.nnz, O._p(b),
-        O._p(diag), O._p(val))
+        O._p(diag), O._p(val), *[None if a is None else O._p(a) for a in per])
     if sc.num_bodies:  # rigid mesh rows inert, DOF slot rows from the bodies (orc_abd_fill)
         rigid, slot = rigid_mask(sc)
         b[rigid | slot] = 0.0
@@ -115,6 +116,11 @@ def affine_expand(sc, dx):
         m = sc.model_x[rigid, :3]
         dx[rigid, :3] = ((q[1] * m[:, 0:1] + q[2] * m[:, 1:2]) + q[3] * m[:, 2:3]) + q[0]
     return dx
+
+
+def _opt(a):
+    """an optional per-element array (None or empty: the scalar), contiguous float32"""
+    return None if a is None or len(a) == 0 else np.ascontiguousarray(a, np.float32)
 
 
 def material_system(sc, x, x_tilde, dt):

@@ -79,8 +79,8 @@ def _declare(L):
         "orc_contact_offdiag_bsr": (U32, [P, U32, U32, P, P, P, U32]),
         "orc_contact_energy": (C.c_double, [P, U32, P, P, P, I32]),
         "orc_bsr_spmv": (None, [U32, P, P, P, P, P, P, P, P, P]),
-        "orc_material_fill": (None, [U32, U32, U32, P, P, P, P, P, F32, F32, P, P, F32, P, P, F32, P, P, U32, P, P,
-                                     P]),
+        "orc_material_fill": (None, [U32, U32, U32, P, P, P, P, P, F32, F32, P, P, F32, P, P, P, F32, P, P, U32, P,
+                                     P, P]),
         "orc_min_distance": (F32, [P, U32, P, U32, P, P, P]),
         "orc_bw98_face": (None, [P, P, P, P, F32, F32, F32, P, P]),
         "orc_dihedral": (F32, [P, P, P, P, P]),
@@ -93,7 +93,7 @@ def _declare(L):
         "orc_contact_offdiag_bsr_abd": (U32, [P, U32, U32, P, P, P, P, P, P, U32]),
         "orc_abd_fill": (None, [U32, P, P, P, P, P, P, P, F32, F32, P, P, P, P]),
         "orc_material_fill2": (None, [U32, P, P, P, P, P, F32, F32, I32, I32, U32, P, P, F32, U32, P, P, P, F32, F32,
-                                      U32, P, P, P, P, F32, F32, P, P, P, U32, P, P, P]),
+                                      U32, P, P, P, P, F32, F32, P, P, P, U32, P, P, P, P, P, P]),
         "orc_pcg": (I32, [U32, P, P, P, P, P, P, P, P, P, I32, F32, F32, I32, I32, C.POINTER(PcgStats)]),
     }
     for name, (res, args) in sig.items():
@@ -450,13 +450,17 @@ def material_energy(sc, x, x_tilde, dt):
     E = sc.edges.shape[0] if spring else 0
     Fs = sc.stretch_faces.shape[0] if bw else 0
     B = sc.bending.shape[0] if dih else 0
-    ml = np.tile(np.float32([sc.stretch_mu, sc.stretch_lambda]), (max(Fs, 1), 1))
+    ml = np.ascontiguousarray(sc.stretch_mu_lambda, np.float32) if sc.stretch_mu_lambda is not None and Fs else \
+        np.tile(np.float32([sc.stretch_mu, sc.stretch_lambda]), (max(Fs, 1), 1))
     lib().orc_material_energy(sc.num_verts, _p(f4(x)), _p(f4(x_tilde)), _p(c(sc.mass, np.float32)),
                               _p(c(sc.pinned, np.uint8)), float(dt), float(sc.dirichlet), E,
                               _p(c(sc.edges, np.uint32)), _p(c(sc.rest_len, np.float32)),
-                              _p(np.full(max(E, 1), sc.spring_k, np.float32)), Fs, _p(c(sc.stretch_faces, np.uint32)),
+                              _p(c(sc.spring_stiffness, np.float32) if sc.spring_stiffness is not None and E else
+                                 np.full(max(E, 1), sc.spring_k, np.float32)), Fs, _p(c(sc.stretch_faces, np.uint32)),
                               _p(c(sc.stretch_dm_inv, np.float32)), _p(c(sc.stretch_area, np.float32)), _p(ml), B,
                               _p(c(sc.bending, np.uint32)), _p(c(sc.bending_rest_angle, np.float32)),
-                              _p(c(sc.bending_hbar, np.float32)), _p(np.full(max(B, 1), sc.bending_k, np.float32)),
+                              _p(c(sc.bending_hbar, np.float32)),
+                              _p(c(sc.bending_stiffness, np.float32) if sc.bending_stiffness is not None and B else
+                                 np.full(max(B, 1), sc.bending_k, np.float32)),
                               float(sc.bending_scaling), _p(out))
     return out

@@ -47,40 +47,70 @@ def _velocity(sc, speed):
     return v
 
 
+def _oracle_halvings(sc, gpu, st):
+    """The reference's decision for the last iteration, from the GPU's iterate: None on a tie."""
+    x_it, dx, xt = gpu.last_iterate()
+    pairs = _oracle_pairs(sc, x_it)
+    toi = np.float32(st.last_toi)
+    if np.linalg.norm(dx[:, :3], axis=1).max() < 1e-2 * sc.dt:  # small step: no search
+        return 0, x_it, dx
+    E0 = _energy(sc, pairs, x_it, xt)
+    alpha = toi
+    for j in range(21):
+        xa = x_it.copy()
+        xa[:, :3] = x_it[:, :3] + alpha * dx[:, :3]
+        Ej = _energy(sc, pairs, xa, xt)
+        if abs(Ej - (E0 + EPS)) <= 1e-7 * abs(E0):
+            return None, x_it, dx
+        if Ej < E0 + EPS:
+            return j, x_it, dx
+        alpha = np.float32(alpha / np.float32(2.0))
+    raise AssertionError("no decrease within 20 halvings")
+
+
+def _check_step(sc, gpu, st):
+    want, x_it, dx = _oracle_halvings(sc, gpu, st)
+    if want is None:
+        return None
+    toi = np.float32(st.last_toi)
+    assert st.ls_halvings == want
+    assert np.float32(st.last_alpha) == np.float32(toi / np.float32(2.0 ** want))
+    np.testing.assert_array_equal(gpu.positions()[:, :3], x_it[:, :3] + np.float32(st.last_alpha) * dx[:, :3])
+    return want
+
+
 @pytest.mark.parametrize("speed", [0.0, 0.5, 2.0, 6.0])
 def test_line_search_takes_the_oracle_step(speed):
     sc = _scene()
     gpu = NewtonSolver(sc, energy_linesearch=True, nonlinear_iters=1)
-    x0 = sc.x.copy()
-    st = gpu.step_host(x_in=x0, v_in=_velocity(sc, speed))
+    st = gpu.step_host(x_in=sc.x.copy(), v_in=_velocity(sc, speed))
     assert st.status == 0 and st.newton_iters >= 1
-    x_it, dx, xt = gpu.last_iterate()
     if st.newton_iters > 1:
         pytest.skip("more than one Newton iteration: the read-back holds the last one only")
-    pairs = _oracle_pairs(sc, x_it)
-    toi = np.float32(st.last_toi)
-    small = np.linalg.norm(dx[:, :3], axis=1).max() < 1e-2 * sc.dt
-    E0 = _energy(sc, pairs, x_it, xt)
-    alpha, j, want = toi, 0, None
-    if small:
-        want = 0
-    else:
-        while j <= 20:
-            xa = x_it.copy()
-            xa[:, :3] = x_it[:, :3] + alpha * dx[:, :3]
-            Ej = _energy(sc, pairs, xa, xt)
-            if abs(Ej - (E0 + EPS)) <= 1e-7 * abs(E0):
-                pytest.skip(f"E(toi/2^{j}) is within rounding of the acceptance threshold")
-            if Ej < E0 + EPS:
-                want = j
-                break
-            alpha = np.float32(alpha / np.float32(2.0))
-            j += 1
-    print(f"\nspeed {speed}: toi {float(toi):.4g}, halvings device {st.ls_halvings}, oracle {want}")
-    assert want is not None
-    assert st.ls_halvings == want
-    assert np.float32(st.last_alpha) == np.float32(toi / np.float32(2.0 ** want))
-    np.testing.assert_array_equal(gpu.positions()[:, :3], x_it[:, :3] + np.float32(st.last_alpha) * dx[:, :3])
+    want = _check_step(sc, gpu, st)
+    print(f"\nspeed {speed}: toi {st.last_toi:.4g}, halvings device {st.ls_halvings}, oracle {want}")
+
+
+def test_line_search_halves_like_the_oracle_on_a_stiff_fold():
+    """A folded cloth with 10^4 x the default bending stiffness: the Gauss-Newton bending Hessian
+    underestimates the curvature and full steps raise the energy, so the search halves."""
+    sc, x = SC.folded_cloth(n=32, gap=4e-4)
+    sc.bending_k = 50.0
+    gpu = NewtonSolver(sc, energy_linesearch=True, nonlinear_iters=1)
+    st = gpu.step_host(x_in=x)
+    halved, checked = 0, 0
+    for k in range(12):
+        if k:
+            st = gpu.step()
+        assert st.status == 0
+        if st.newton_iters != 1:
+            continue
+        want = _check_step(sc, gpu, st)
+        if want is not None:
+            checked += 1
+            halved += want > 0
+    print(f"\nstiff fold: {checked} steps checked, {halved} with halvings")
+    assert checked >= 6 and halved >= 1
 
 
 def test_fused_and_plain_line_search_agree():
