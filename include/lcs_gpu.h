@@ -538,6 +538,10 @@ LCS_API int lcs_newton_step_host(lcs_newton* h, const float* x_in, const float* 
 /* Copies the positions / velocities (float4 per vertex) to host buffers; either may be NULL.
  * Synchronises the solver's stream. */
 LCS_API int lcs_newton_download(const lcs_newton* h, float* x_out, float* v_out);
+/* Replaces the positions / velocities (float4 per vertex; either may be NULL) with host buffers, as
+ * SolverInterface::load_saved_state_from_host (solver_interface.cpp:275-412) does before the next frame.
+ * Synchronises the solver's stream. */
+LCS_API int lcs_newton_upload(lcs_newton* h, const float* x_in, const float* v_in);
 /* Device pointers of the solver's positions and velocities (float4 per vertex). */
 LCS_API int lcs_newton_state(const lcs_newton* h, float** d_x, float** d_v);
 /* Accumulated per-phase GPU time (LCS_NEWTON_PROFILE): build, material, DCD broad, DCD narrow,

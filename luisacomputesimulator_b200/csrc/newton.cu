@@ -2332,6 +2332,22 @@ extern "C" int lcs_newton_download(const lcs_newton* h, float* x_out, float* v_o
     return LCS_OK;
 }
 
+// SolverInterface::load_saved_state_from_host (solver_interface.cpp:275-412) followed by the upload of the
+// frame state: the next step starts from these positions / velocities.
+extern "C" int lcs_newton_upload(lcs_newton* h, const float* x_in, const float* v_in)
+{
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_upload: null handle");
+    const size_t bytes = 16 * (size_t)h->V;
+    if (x_in) LCS_CUDA_TRY(cudaMemcpyAsync(h->x, x_in, bytes, cudaMemcpyHostToDevice, h->s));
+    if (v_in) LCS_CUDA_TRY(cudaMemcpyAsync(h->v, v_in, bytes, cudaMemcpyHostToDevice, h->s));
+    if (h->plain) {
+        if (x_in) std::memcpy(h->h_x, x_in, bytes);
+        if (v_in) std::memcpy(h->h_v, v_in, bytes);
+    }
+    LCS_CUDA_TRY(cudaStreamSynchronize(h->s));
+    return LCS_OK;
+}
+
 extern "C" int lcs_newton_state(const lcs_newton* h, float** d_x, float** d_v)
 {
     if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_state: null handle");

@@ -155,6 +155,27 @@ class NewtonSolver:
         A.check(self.lib.lcs_newton_download(self.h, None, out.ctypes.data_as(C.c_void_p)), "lcs_newton_download")
         return out
 
+    def upload(self, x=None, v=None):
+        """Replace the device positions / velocities, float32 (V, 4) each (either may be None)."""
+        p = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)  # noqa: E731
+        xa, va = p(x), p(v)
+        for a in (xa, va):
+            if a is not None and a.shape != (self.scene.num_verts, 4):
+                raise ValueError(f"state of shape {a.shape}, expected ({self.scene.num_verts}, 4)")
+        q = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        A.check(self.lib.lcs_newton_upload(self.h, q(xa), q(va)), "lcs_newton_upload")
+
+    def save_current_frame_state_to_host(self, path):
+        """The reference's frame state file (positions, velocities, body q and q velocities) for this state."""
+        from . import scene_io
+        scene_io.save_state(path, self.scene, self.positions(), self.velocities())
+
+    def load_saved_state_from_host(self, path):
+        """Load a frame state file written by the reference or by save_current_frame_state_to_host."""
+        from . import scene_io
+        x, v = scene_io.load_state(path, self.scene, self.positions())
+        self.upload(x, v)
+
     def last_iterate(self):
         """(x at the start of the last Newton iteration, its direction dx, x_tilde), float32 (V, 4) each."""
         out = [np.zeros((self.scene.num_verts, 4), np.float32) for _ in range(3)]

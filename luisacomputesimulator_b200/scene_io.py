@@ -15,6 +15,10 @@
 
 Edges, bending stencils, areas, masses, contact offsets and affine bodies are then derived by
 ``scenes.assemble`` exactly as for the synthetic scenes.
+
+* ``save_state`` / ``load_state``: the frame state files of SolverInterface
+  (Solver/SimulationSolver/solver_interface.cpp:206-412); ``write_obj``: the frame's meshes as
+  ``save_mesh_to_obj`` writes them (:413-485).
 """
 from __future__ import annotations
 
@@ -199,3 +203,72 @@ def _model(v, bending=False):
     if isinstance(v, str):
         return names.get(v, 2 if bending else 1)
     return int(v)
+
+
+def _mesh_verts(sc):
+    return sc.num_verts - 4 * sc.num_bodies
+
+
+def save_state(path, sc, x, v):
+    """A frame state file as SolverInterface::save_current_frame_state_to_host writes it
+    (solver_interface.cpp:206-273): sections ``o position`` and ``o velocity`` (one ``v x y z`` line per mesh
+    vertex) and ``o q`` and ``o qv`` (four lines per affine body: p, a0, a1, a2 and their velocities).
+    Values are written with 9 significant digits, so a float32 state reads back bit for bit."""
+    V, NB = _mesh_verts(sc), sc.num_bodies
+    x, v = np.asarray(x, np.float32), np.asarray(v, np.float32)
+    slots = np.concatenate([np.arange(int(d), int(d) + 4) for d in sc.body_dof]) if NB else np.zeros(0, np.int64)
+
+    def block(a):
+        return "".join(f"v {r[0]:.9g} {r[1]:.9g} {r[2]:.9g}\n" for r in a[:, :3].tolist())
+    with open(path, "w") as fh:
+        fh.write("o position\n" + block(x[:V]) + "o velocity\n" + block(v[:V]) +
+                 "o q\n" + block(x[slots]) + "o qv\n" + block(v[slots]))
+
+
+def load_state(path, sc, like=None):
+    """(positions, velocities) float32 (V, 4) of the scene from a frame state file
+    (SolverInterface::load_saved_state_from_host, solver_interface.cpp:275-412).  ``like`` supplies the
+    fourth lane (and is the starting copy); the body q and q velocities of the ``o q`` / ``o qv`` sections go
+    to the bodies' DOF slots.  A section with more or fewer lines than the scene has vertices (bodies x 4)
+    raises ValueError; a missing file raises FileNotFoundError."""
+    V, NB = _mesh_verts(sc), sc.num_bodies
+    sec = {"position": [], "velocity": [], "q": [], "qv": []}
+    cur = None
+    with open(path) as fh:
+        for line in fh:
+            tok = line.split()
+            if not tok:
+                continue
+            if tok[0] == "o":
+                cur = tok[1] if len(tok) > 1 and tok[1] in sec else None
+                continue
+            if tok[0] == "v" and cur is not None:
+                sec[cur].append((float(tok[1]), float(tok[2]), float(tok[3])))
+    want = {"position": V, "velocity": V, "q": 4 * NB, "qv": 4 * NB}
+    for k, n in want.items():
+        if len(sec[k]) != n:
+            raise ValueError(f"{path}: section {k!r} holds {len(sec[k])} vertices, the scene has {n}")
+    x = np.zeros((sc.num_verts, 4), np.float32) if like is None else np.array(like, np.float32, copy=True)
+    v = np.zeros((sc.num_verts, 4), np.float32)
+    x[:V, :3] = np.asarray(sec["position"], np.float32).reshape(-1, 3)
+    v[:V, :3] = np.asarray(sec["velocity"], np.float32).reshape(-1, 3)
+    if NB:
+        slots = np.concatenate([np.arange(int(d), int(d) + 4) for d in sc.body_dof])
+        x[slots, :3] = np.asarray(sec["q"], np.float32).reshape(-1, 3)
+        v[slots, :3] = np.asarray(sec["qv"], np.float32).reshape(-1, 3)
+    return x, v
+
+
+def write_obj(path, sc, x):
+    """The frame's meshes as SolverInterface::save_mesh_to_obj writes them (solver_interface.cpp:413-485):
+    one ``o mesh_<k>`` object per mesh part with its vertices, faces indexed 1-based over the whole file."""
+    x = np.asarray(x, np.float32)
+    pv = sc.part_verts if sc.part_verts is not None else np.array([0, _mesh_verts(sc)])
+    pf = sc.part_faces if sc.part_faces is not None else np.array([0, sc.faces.shape[0]])
+    out = ["# simulated result\n"]
+    for k in range(len(pv) - 1):
+        out.append(f"o mesh_{k}\n")
+        out.extend(f"v {r[0]:.9g} {r[1]:.9g} {r[2]:.9g}\n" for r in x[pv[k]:pv[k + 1], :3].tolist())
+        out.extend(f"f {a + 1} {b + 1} {c + 1}\n" for a, b, c in sc.faces[pf[k]:pf[k + 1], :3].tolist())
+    with open(path, "w") as fh:
+        fh.write("".join(out))

@@ -97,6 +97,9 @@ class Scene:
     stretch_mu_lambda: np.ndarray = None   # (Fs, 2) float32
     bending_stiffness: np.ndarray = None   # (B,) float32
     spring_stiffness: np.ndarray = None    # (E,) float32
+    # mesh parts in order: vertex and face offsets (num_parts + 1 each; the DOF slots follow the last part)
+    part_verts: np.ndarray = None
+    part_faces: np.ndarray = None
 
     @property
     def num_bodies(self):
@@ -475,7 +478,9 @@ def assemble(name, parts, dt, gravity, kappa, spring_k=None, bending_k=5e-3, str
                  body_volume=body_volume if NB else None, body_kappa=body_kappa if NB else None,
                  model_x=model_x if NB else None, stretch_mu_lambda=stretch_ml.astype(np.float32),
                  bending_stiffness=bend_k.astype(np.float32),
-                 spring_stiffness=(spring_k_e if spring_k is None else np.full(len(edges), spring_k)).astype(np.float32))
+                 spring_stiffness=(spring_k_e if spring_k is None else np.full(len(edges), spring_k)).astype(np.float32),
+                 part_verts=np.concatenate([[0], np.cumsum([p.x.shape[0] for p in parts])]).astype(np.int64),
+                 part_faces=np.concatenate([[0], np.cumsum([p.faces.shape[0] for p in parts])]).astype(np.int64))
 
 
 def cloth_on_sphere(n=64, spacing=0.01, seed=0, subdiv=4, radius=0.2, drop=0.05):

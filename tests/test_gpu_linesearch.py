@@ -96,6 +96,7 @@ def test_line_search_halves_like_the_oracle_on_a_stiff_fold():
     underestimates the curvature and full steps raise the energy, so the search halves."""
     sc, x = SC.folded_cloth(n=32, gap=4e-4)
     sc.bending_k = 50.0
+    sc.bending_stiffness[:] = 50.0  # the per-stencil stiffness takes precedence over the scalar
     gpu = NewtonSolver(sc, energy_linesearch=True, nonlinear_iters=1)
     st = gpu.step_host(x_in=x)
     halved, checked = 0, 0

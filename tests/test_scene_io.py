@@ -90,3 +90,49 @@ def test_reference_scene_files_load():
         if os.path.basename(f) == "cloth_rigid_coupling_drop.json":
             assert sc.num_bodies == 1 and sc.pinned.sum() == 4
     assert loaded >= 12
+
+
+def _two_part_scene(tmp_path):
+    _grid_obj(tmp_path / "grid.obj")
+    scene = {"shells": [{"model_name": "grid.obj", "translation": [0, 1, 0]},
+                        {"model_name": "grid.obj", "translation": [0.2, 1.1, 0.2], "scale": 0.1, "shell_type": "Rigid"}]}
+    (tmp_path / "s.json").write_text(json.dumps(scene))
+    return scene_io.load_scene_json(str(tmp_path / "s.json"), [str(tmp_path)])[0]
+
+
+def test_state_file_round_trip_with_bodies(tmp_path):
+    sc = _two_part_scene(tmp_path)
+    rng = np.random.default_rng(3)
+    x = sc.x.copy()
+    x[:, :3] += rng.normal(0, 0.1, (sc.num_verts, 3)).astype(np.float32)
+    v = np.zeros_like(x)
+    v[:, :3] = rng.normal(0, 1, (sc.num_verts, 3)).astype(np.float32)
+    p = tmp_path / "frame_3.state"
+    scene_io.save_state(str(p), sc, x, v)
+    text = p.read_text().splitlines()
+    assert text[0] == "o position" and text.count("o q") == 1 and text.count("o qv") == 1
+    assert len(text) == 4 + 2 * 50 + 2 * 4  # 50 mesh vertices, one body's four slots
+    x2, v2 = scene_io.load_state(str(p), sc, like=sc.x)
+    np.testing.assert_array_equal(x2[:, :3], x[:, :3])
+    np.testing.assert_array_equal(v2[:, :3], v[:, :3])
+    # the reference's 6-digit output reads too; a scene of another size is refused
+    short = "\n".join(ln if not ln.startswith("v ") else "v " + " ".join(f"{float(t):g}" for t in ln.split()[1:])
+                      for ln in text)
+    (tmp_path / "short.state").write_text(short + "\n")
+    x3, _ = scene_io.load_state(str(tmp_path / "short.state"), sc)
+    np.testing.assert_allclose(x3[:, :3], x[:, :3], rtol=1e-5, atol=1e-6)
+    (tmp_path / "bad.state").write_text("\n".join(text[:-1]) + "\n")
+    with pytest.raises(ValueError):
+        scene_io.load_state(str(tmp_path / "bad.state"), sc)
+    with pytest.raises(FileNotFoundError):
+        scene_io.load_state(str(tmp_path / "missing.state"), sc)
+
+
+def test_frame_obj_round_trip(tmp_path):
+    sc = _two_part_scene(tmp_path)
+    p = tmp_path / "frame_0.obj"
+    scene_io.write_obj(str(p), sc, sc.x)
+    assert p.read_text().count("o mesh_") == 2
+    x, f = scene_io.read_obj(str(p))
+    np.testing.assert_array_equal(x, sc.x[:50, :3])
+    np.testing.assert_array_equal(f, sc.faces[:, :3])
