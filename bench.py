@@ -39,9 +39,11 @@ def args_():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--mode", choices=["fused", "plain"], default="fused")
     p.add_argument("--fp64", action="store_true", help="precision form")
-    p.add_argument("--pcg", choices=["rows", "cg1"], default="cg1",
+    p.add_argument("--pcg", choices=["rows", "cg1", "cg1-global"], default="cg1",
                    help="fused mode: row-resident PCG (classic recurrences: 3 grid syncs/iter; cg1: the "
-                        "single-reduction form, 2)")
+                        "single-reduction form, slice-resident where the rows fit -- one block per SM with its "
+                        "leading matrix groups in shared memory; cg1-global: the single-reduction form reading "
+                        "the matrix from L2 every iteration)")
     p.add_argument("--traversal", choices=["fast", "full"], default="fast",
                    help="fast: DCD lists filtered from the previous iteration's CCD lists (same sets); "
                         "full: a traversal for every list")
@@ -218,8 +220,8 @@ def run_ours(a):
     lib = _capi.load()
     _capi.check(lib.lcs_device_check(local), "device check")
     sc = scenes.twisted_tube(a.n_around, a.n_along)
-    solver = NewtonSolver(sc, plain=(a.mode == "plain"), fp64=a.fp64, profile=True, single_reduction=(a.pcg == "cg1"),
-                          full_traversal=(a.traversal == "full"))
+    solver = NewtonSolver(sc, plain=(a.mode == "plain"), fp64=a.fp64, profile=True, single_reduction=(a.pcg != "rows"),
+                          global_matrix=(a.pcg == "cg1-global"), full_traversal=(a.traversal == "full"))
     stream = torch.cuda.current_stream()
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
 
@@ -290,8 +292,9 @@ def run_ours(a):
     if rank == 0:
         value = newton_all / t_s
         solver_uses_rows = solver.uses_row_pcg()
-        pcg_kernel_name = ("k_pcg_cg1 (single-reduction row-resident Jacobi-PCG)" if a.pcg == "cg1" else
-                           "k_pcg_rows (row-resident Jacobi-PCG)") if solver_uses_rows else \
+        pcg_kernel_name = {"cg1-res": "k_pcg_res (single-reduction slice-resident Jacobi-PCG)",
+                           "cg1": "k_pcg_cg1 (single-reduction row-resident Jacobi-PCG)",
+                           "rows": "k_pcg_rows (row-resident Jacobi-PCG)"}[solver.pcg_kind()] if solver_uses_rows else \
             ("k_pcg_fused (persistent Jacobi-PCG solve)" if a.mode == "fused" else "plain PCG kernels")
         # roofline of the dominant kernel: the persistent PCG solve (one launch per Newton iteration)
         pcg_ms, pcg_launches = prof["pcg"]

@@ -486,11 +486,15 @@ enum {
     LCS_NEWTON_PCG_SINGLE_REDUCTION = 8, /* fused mode: single-reduction row-resident PCG (LCS_PCG_SINGLE_REDUCTION) */
     LCS_NEWTON_FULL_TRAVERSAL = 16, /* fused mode: every candidate list by a traversal (no DCD filtering of the
                                       previous iteration's CCD lists) */
-    LCS_NEWTON_ENERGY_LINESEARCH = 32 /* use_energy_linesearch (scene_params.h:41): after the CCD bound, halve the
+    LCS_NEWTON_ENERGY_LINESEARCH = 32, /* use_energy_linesearch (scene_params.h:41): after the CCD bound, halve the
                                          step until the energy (inertia, cloth, barrier of the iteration-start
                                          pairs; FP64 sums) decreases (newton_solver.cpp:3790-3834).  Single scenes;
                                          the fused loop evaluates 7 step lengths per launch and decides on the
                                          device, the plain loop one per host round trip as the reference does. */
+    LCS_NEWTON_PCG_GLOBAL_MATRIX = 64 /* with LCS_NEWTON_PCG_SINGLE_REDUCTION: read the material matrix from
+                                         global memory every iteration (the grid of 256-row blocks) instead of
+                                         the slice-resident solve (one block per SM, its rows' leading matrix
+                                         groups held in shared memory), which is used where the rows fit */
 };
 
 typedef struct lcs_newton_stats {
@@ -551,7 +555,7 @@ LCS_API int lcs_newton_reset_profile(lcs_newton* h);
 LCS_API int lcs_newton_counts(const lcs_newton* h, uint32_t* nnz_material, uint32_t* cap_vf, uint32_t* cap_ee,
                               uint32_t* cap_pairs);
 /* Which PCG the Newton loop runs: 0 plain kernels, 1 persistent CSR solve, 2 row-resident,
- * 3 single-reduction row-resident (-1: null handle).  No counterpart in the reference. */
+ * 3 single-reduction row-resident, 4 single-reduction slice-resident (-1: null handle).  No counterpart in the reference. */
 LCS_API int lcs_newton_pcg_kind(const lcs_newton* h);
 
 #ifdef __cplusplus

@@ -158,6 +158,7 @@ SIGNATURES = {
 LCS_NEWTON_PLAIN, LCS_NEWTON_FP64, LCS_NEWTON_PROFILE, LCS_NEWTON_PCG_SINGLE_REDUCTION, LCS_NEWTON_FULL_TRAVERSAL = \
     1, 2, 4, 8, 16
 LCS_NEWTON_ENERGY_LINESEARCH = 32
+LCS_NEWTON_PCG_GLOBAL_MATRIX = 64
 PHASES = ["build", "material", "dcd_broad", "dcd_narrow", "assembly", "pcg", "ccd_broad", "ccd_narrow", "apply"]
 
 _lib = None

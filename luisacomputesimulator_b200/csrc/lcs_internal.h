@@ -11,11 +11,25 @@ int lcs_fail(int code, const char* msg);
 // Row-resident PCG solve with the material matrix in SELL-32 (slices of 32 rows; slot k of a
 // slice at col[32 * k + lane], value component c at val[(9 * k + c) * 32 + lane], k counted from
 // slice_ptr[slice]) and the contact blocks in CSR.  LCS_ERR_CAPACITY if the rows do not fit.
+// c_ptr / c_col / c_val / c_ok (optional): the contact blocks B again in the same SELL-32 layout
+// (lcs_contact_to_sell); the solve reads them instead of B's CSR while *c_ok is set on the device.
 int lcs_pcg_solve_sell(lcs_pcg* P, const float* diag, const uint32_t* slice_ptr, const uint32_t* col,
                        const float* val, const lcs_bsr* B, const float* b, float* x, const lcs_pcg_opts* opts,
-                       lcs_pcg_stats* stats, lcs_stream stream);
+                       lcs_pcg_stats* stats, lcs_stream stream, const uint32_t* c_ptr = nullptr,
+                       const uint32_t* c_col = nullptr, const float* c_val = nullptr, const int* c_ok = nullptr);
+// The CSR matrix B (n block rows) rewritten as SELL-32 with 4-slot groups (the layout lcs_pcg_solve_sell
+// takes for the material matrix): width (ceil(n / 32) words of scratch), ptr (ceil(n / 32) + 1 slot
+// offsets), col (32 words per slot), val (288 floats per slot).  *ok (device) is set to 0 when the
+// slots would exceed cap_slots, and nothing else is written then.
+int lcs_contact_to_sell(uint32_t n, const lcs_bsr* B, uint32_t* width, uint32_t* ptr, uint32_t* col, float* val,
+                        uint32_t cap_slots, int* ok, lcs_stream stream);
 // Most block rows the row-resident solve holds on the current device (one thread per row).
 int64_t lcs_pcg_rows_capacity();
+// lcs_pcg_opts flag: keep the SELL matrix in global memory (k_pcg_cg1) where the slice-resident
+// single-reduction solve (one block per SM, matrix groups in shared memory) would apply.
+constexpr int LCS_PCG_INTERNAL_NO_RESIDENT = 1 << 16;
+// 1 if single-reduction SELL solves of this handle run slice-resident (k_pcg_res), else 0.
+int lcs_pcg_resident(lcs_pcg* P);
 
 // construct_tree with the reference's host sort (Morton codes downloaded, sorted on the CPU,
 // uploaded; lbvh.cpp:983-993) -- used by the plain one-scene comparator loop only.

@@ -998,6 +998,11 @@ struct lcs_newton {
     bool cg1 = false;              // single-reduction row-resident PCG (two grid synchronisations per iteration)
     size_t sell_vals = 0;          // floats in mat_val
     uint32_t *sell_ptr = nullptr, *sell_col = nullptr;
+    // the contact blocks rewritten as SELL-32 before each solve (fused single-scene mode)
+    uint32_t *cs_width = nullptr, *cs_ptr = nullptr, *cs_col = nullptr;
+    float* cs_val = nullptr;
+    int* cs_ok = nullptr;
+    uint32_t cs_cap = 0;  // slots
     // contact
     lcs_bvh *face_tree = nullptr, *edge_tree = nullptr;
     uint32_t cap_vf = 0, cap_ee = 0, cap_pairs = 0;
@@ -1010,6 +1015,7 @@ struct lcs_newton {
     bool filter_ok = false;
     bool full_traversal = false;   // LCS_NEWTON_FULL_TRAVERSAL
     bool energy_ls = false;        // LCS_NEWTON_ENERGY_LINESEARCH
+    bool global_matrix = false;    // LCS_NEWTON_PCG_GLOBAL_MATRIX
     double *ls_E = nullptr, *h_ls_E = nullptr;  // energies of one line-search round (device, pinned host)
     float* h_alpha = nullptr;      // pinned: the plain loop's chosen step length
     int32_t ls_halvings = 0;       // this step
@@ -1057,6 +1063,12 @@ void free_contact(lcs_newton* h)
     if (h->dcd_ee) cudaFree(h->dcd_ee);
     if (h->pairs) cudaFree(h->pairs);
     if (h->asmb) lcs_assembler_destroy(h->asmb);
+    for (void* q : {(void*)h->cs_width, (void*)h->cs_ptr, (void*)h->cs_col, (void*)h->cs_val, (void*)h->cs_ok})
+        if (q) cudaFree(q);
+    h->cs_width = h->cs_ptr = h->cs_col = nullptr;
+    h->cs_val = nullptr;
+    h->cs_ok = nullptr;
+    h->cs_cap = 0;
     h->bp_vf = nullptr;
     h->bp_ee = nullptr;
     h->dcd_vf = nullptr;
@@ -1095,6 +1107,22 @@ int alloc_contact(lcs_newton* h)
         h->asmb = nullptr;
         e = dalloc(h->pairs, h->cap_pairs);
         h->alloc_pairs = h->cap_pairs;
+        if (e == cudaSuccess && h->sell) {
+            // SELL copy of the contact blocks: twice the assembler's block capacity plus a padded
+            // group per slice; a step whose slices need more uses the CSR form
+            for (void* q : {(void*)h->cs_col, (void*)h->cs_val})
+                if (q) cudaFree(q);
+            h->cs_col = nullptr;
+            h->cs_val = nullptr;
+            const uint64_t S = (h->V + 31) / 32;
+            const uint64_t blocks = (uint64_t)(h->NB ? 56 : 12) * h->cap_pairs;
+            h->cs_cap = (uint32_t)std::min<uint64_t>((2 * blocks + 31) / 32 + 4 * S, 0x7FFFFFFFu);
+            if (!h->cs_width) e = dalloc(h->cs_width, S);
+            if (e == cudaSuccess && !h->cs_ptr) e = dalloc(h->cs_ptr, S + 1);
+            if (e == cudaSuccess && !h->cs_ok) e = dalloc(h->cs_ok, 1);
+            if (e == cudaSuccess) e = dalloc(h->cs_col, 32ull * h->cs_cap);
+            if (e == cudaSuccess) e = dalloc(h->cs_val, 288ull * h->cs_cap);
+        }
         if (e == cudaSuccess)
             return h->NB ? lcs_assembler_create_abd(h->V, h->cap_pairs, &h->asmb)
                          : lcs_assembler_create(h->V, h->cap_pairs, &h->asmb);
@@ -1579,17 +1607,24 @@ int newton_iteration(lcs_newton* h)
         lcs_assembler_bsr(h->asmb, &Bc, &d_nnzb);
         lcs_pcg_opts o{d.pcg_max_iter, d.pcg_rel_tol, d.pcg_abs_rz_tol, h->plain ? d.pcg_check_every : 1,
                        (h->fp64 ? LCS_PCG_FP64_DOTS : 0) | (h->plain ? LCS_PCG_PLAIN : LCS_PCG_NO_STATS) |
-                           (h->cg1 ? LCS_PCG_SINGLE_REDUCTION : 0)};
+                           (h->cg1 ? LCS_PCG_SINGLE_REDUCTION : 0) |
+                           (h->global_matrix ? LCS_PCG_INTERNAL_NO_RESIDENT : 0)};
         lcs_pcg_stats ps;
         if (h->batch)
             rc = lcs_pcg_solve_batch(h->pcg, h->S, h->voff_d, h->h_voff.data(), h->active,
                                      reinterpret_cast<const float*>(h->diag), h->nnz_mat ? &A : nullptr, &Bc,
                                      reinterpret_cast<const float*>(h->b), reinterpret_cast<float*>(h->dx), &o, h->bpcg,
                                      h->cluster, h->s);
-        else if (h->sell)
+        else if (h->sell) {
+            const bool cs = h->cs_val != nullptr;
+            if (cs && (rc = lcs_contact_to_sell(h->V, &Bc, h->cs_width, h->cs_ptr, h->cs_col, h->cs_val, h->cs_cap,
+                                                h->cs_ok, h->s)))
+                return rc;
             rc = lcs_pcg_solve_sell(h->pcg, reinterpret_cast<const float*>(h->diag), h->sell_ptr, h->sell_col,
                                     h->mat_val, &Bc, reinterpret_cast<const float*>(h->b),
-                                    reinterpret_cast<float*>(h->dx), &o, nullptr, h->s);
+                                    reinterpret_cast<float*>(h->dx), &o, nullptr, h->s, cs ? h->cs_ptr : nullptr,
+                                    h->cs_col, h->cs_val, h->cs_ok);
+        }
         else
             rc = lcs_pcg_solve(h->pcg, reinterpret_cast<const float*>(h->diag), h->nnz_mat ? &A : nullptr, &Bc,
                                reinterpret_cast<const float*>(h->b), reinterpret_cast<float*>(h->dx), &o,
@@ -1779,6 +1814,7 @@ int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batc
     h->cg1 = (flags & LCS_NEWTON_PCG_SINGLE_REDUCTION) != 0;
     h->full_traversal = (flags & LCS_NEWTON_FULL_TRAVERSAL) != 0;
     h->energy_ls = (flags & LCS_NEWTON_ENERGY_LINESEARCH) != 0;
+    h->global_matrix = (flags & LCS_NEWTON_PCG_GLOBAL_MATRIX) != 0;
     h->batch = batch;
     h->V = d->n_verts;
     h->F = d->n_faces;
@@ -2381,7 +2417,8 @@ extern "C" int lcs_newton_pcg_kind(const lcs_newton* h)
     if (!h) return -1;
     if (h->plain) return 0;
     if (!h->sell) return 1;
-    return h->cg1 ? 3 : 2;
+    if (!h->cg1) return 2;
+    return !h->global_matrix && lcs_pcg_resident(h->pcg) ? 4 : 3;
 }
 
 extern "C" int lcs_newton_counts(const lcs_newton* h, uint32_t* nnz_material, uint32_t* cap_vf, uint32_t* cap_ee,

@@ -428,6 +428,11 @@ struct RowArgs {
     const uint32_t* m_col; // CSR col | SELL col[(g * 32 + lane) * 4 + j], slot 4g + j (see row_matvec)
     const float* m_val;    // CSR 9 floats per block | SELL val[((g * 9 + c) * 32 + lane) * 4 + j]
     Bsr B;                 // contact blocks (CSR)
+    int b_vec;             // B.val is 16-B aligned: contact values by 16-B loads
+    const uint32_t* c_ptr; // the contact blocks again in SELL-32 (layout of m_*), or null
+    const uint32_t* c_col;
+    const float* c_val;
+    const int* c_ok;       // device flag: the SELL copy is complete (else the CSR form is used)
     const float4* b;
     float4* x;
     float4* pg;            // p of every row, exchanged through L2
@@ -527,6 +532,127 @@ __device__ __forceinline__ void acc_block(const float* m, int stride, float4 v, 
     q2 += __fmaf_rn(m[8 * stride], v.z, __fmaf_rn(m[5 * stride], v.y, m[2 * stride] * v.x));
 }
 
+// The 9 floats of contact block k in two steps, so that the loads of the next chunk can be issued
+// before the current one is used: fetch_block9 issues three aligned 16-B loads covering the block
+// (block k starts (k mod 4) floats into the 16-B word at 9k / 4) when the value array is 16-B aligned,
+// else nine scalar loads (also for the array's last block, whose covering words may run past its end);
+// block9 picks the 9 floats out.
+struct Raw9 {
+    float4 a, b, c;
+    uint32_t sh;
+};
+
+__device__ __forceinline__ Raw9 fetch_block9(const float* val, uint32_t k, bool scalar)
+{
+    Raw9 r;
+    if (scalar) {
+        const float* m = val + 9 * (size_t)k;
+        r.a = make_float4(__ldcg(m), __ldcg(m + 1), __ldcg(m + 2), __ldcg(m + 3));
+        r.b = make_float4(__ldcg(m + 4), __ldcg(m + 5), __ldcg(m + 6), __ldcg(m + 7));
+        r.c = make_float4(__ldcg(m + 8), 0.f, 0.f, 0.f);
+        r.sh = 0;
+    } else {
+        const float4* v4 = reinterpret_cast<const float4*>(val) + ((9 * (size_t)k) >> 2);
+        r.a = __ldcg(v4);
+        r.b = __ldcg(v4 + 1);
+        r.c = __ldcg(v4 + 2);
+        r.sh = k & 3u;
+    }
+    return r;
+}
+
+__device__ __forceinline__ void block9(const Raw9& r, float m[9])
+{
+    const float w[12] = {r.a.x, r.a.y, r.a.z, r.a.w, r.b.x, r.b.y, r.b.z, r.b.w, r.c.x, r.c.y, r.c.z, r.c.w};
+#pragma unroll
+    for (int j = 0; j < 9; ++j) m[j] = r.sh == 0 ? w[j] : r.sh == 1 ? w[j + 1] : r.sh == 2 ? w[j + 2] : w[j + 3];
+}
+
+// Contact blocks of a warp's 32 consecutive rows r0 .. r0 + 31 (rows >= n have none), added to the
+// calling lane's row accumulators (o0, o1, o2).  The rows' blocks form one CSR range, taken 32 blocks at
+// a time with one block per lane (column, gather, values: neighbouring lanes read neighbouring blocks),
+// summed per row by a segmented scan over the lanes and handed to the lane owning the row.  Columns are
+// loaded two chunks ahead, gathers and values one chunk ahead of the chunk being summed.  Rows next to a prescribed
+// boundary or inside a fold carry dozens of contact blocks; walking them one row per lane made every
+// load of the warp touch 32 different lines.  Every lane of the warp must call this.
+// Summation order: per chunk of 32 blocks a fixed tree, chunks in CSR order.
+template <class LdU>
+__device__ __forceinline__ void contact_warp(const Bsr& B, uint32_t r0, uint32_t n, bool vec, LdU ld_u, float& o0,
+                                             float& o1, float& o2)
+{
+    const uint32_t lane = lane_id();
+    const uint32_t total = __ldcg(&B.rp[n]);
+    const uint32_t rp_l = __ldcg(&B.rp[min(r0 + lane, n)]);
+    const uint32_t rend = __ldcg(&B.rp[min(r0 + 32u, n)]);
+    const uint32_t rp_down = __shfl_down_sync(0xFFFFFFFFu, rp_l, 1);  // every lane takes part in each shuffle
+    const uint32_t rp_next = lane < 31u ? rp_down : rend;
+    const uint32_t kbeg = __shfl_sync(0xFFFFFFFFu, rp_l, 0);
+    // software pipeline over the chunks: columns two chunks ahead, gathers and values one chunk ahead
+    const uint32_t k0 = kbeg + lane;
+    uint32_t col_a = k0 + 32u < rend ? __ldcg(&B.col[k0 + 32u]) : 0u;
+    float4 u_cur = make_float4(0.f, 0.f, 0.f, 0.f);
+    Raw9 raw{};
+    if (k0 < rend) {
+        u_cur = ld_u(__ldcg(&B.col[k0]));
+        raw = fetch_block9(B.val, k0, !vec || k0 + 1u >= total);
+    }
+    for (uint32_t kc = kbeg; kc < rend; kc += 32u) {
+        const uint32_t k = kc + lane;
+        const bool act = k < rend;
+        const uint32_t col_b = k + 64u < rend ? __ldcg(&B.col[k + 64u]) : 0u;
+        float4 u_next = make_float4(0.f, 0.f, 0.f, 0.f);
+        Raw9 raw_n{};
+        if (k + 32u < rend) {
+            u_next = ld_u(col_a);
+            raw_n = fetch_block9(B.val, k + 32u, !vec || k + 33u >= total);
+        }
+        float y0 = 0.f, y1 = 0.f, y2 = 0.f;
+        if (act) {
+            const float4 v = u_cur;
+            float m[9];
+            block9(raw, m);
+            y0 = __fmaf_rn(m[6], v.z, __fmaf_rn(m[3], v.y, m[0] * v.x));
+            y1 = __fmaf_rn(m[7], v.z, __fmaf_rn(m[4], v.y, m[1] * v.x));
+            y2 = __fmaf_rn(m[8], v.z, __fmaf_rn(m[5], v.y, m[2] * v.x));
+        }
+        // row (lane index) of block k: the last lane whose row starts at or before k
+        uint32_t seg = 0;
+#pragma unroll
+        for (uint32_t st = 16; st > 0; st >>= 1) {
+            const uint32_t cand = seg + st;
+            const uint32_t v = __shfl_sync(0xFFFFFFFFu, rp_l, cand < 32u ? cand : 31u);
+            if (cand < 32u && v <= k) seg = cand;
+        }
+        if (!act) seg = 32u + lane;  // past the range: a segment of its own
+        // inclusive segmented scan: the last lane of each row's run holds the run's sum
+#pragma unroll
+        for (uint32_t d = 1; d < 32u; d <<= 1) {
+            const float a0 = __shfl_up_sync(0xFFFFFFFFu, y0, d), a1 = __shfl_up_sync(0xFFFFFFFFu, y1, d),
+                        a2 = __shfl_up_sync(0xFFFFFFFFu, y2, d);
+            const uint32_t sg = __shfl_up_sync(0xFFFFFFFFu, seg, d);
+            if (lane >= d && sg == seg) {
+                y0 += a0;
+                y1 += a1;
+                y2 += a2;
+            }
+        }
+        // this lane's row: its blocks in the chunk end at hi - 1
+        const uint32_t lo = max(rp_l, kc), hi = min(min(rp_next, kc + 32u), rend);
+        const bool mine = hi > lo;
+        const uint32_t src = mine ? hi - 1u - kc : lane;
+        const float s0 = __shfl_sync(0xFFFFFFFFu, y0, src), s1 = __shfl_sync(0xFFFFFFFFu, y1, src),
+                    s2 = __shfl_sync(0xFFFFFFFFu, y2, src);
+        if (mine) {
+            o0 += s0;
+            o1 += s1;
+            o2 += s2;
+        }
+        col_a = col_b;
+        u_cur = u_next;
+        raw = raw_n;
+    }
+}
+
 // streamed read-only 16-B load that does not displace L1 lines (matrix values: read once per iteration)
 __device__ __forceinline__ float4 ld_stream4(const float4* p)
 {
@@ -548,6 +674,35 @@ __device__ __forceinline__ float comp(const float4& v, int j) { return j == 0 ? 
 // each group with one 512-B coalesced uint4 load and nine 512-B float4 loads, 2.5 load instructions per
 // block instead of 10.  Padding slots hold zero blocks against the row itself.  The blocks are summed in
 // slot order, the order of the CSR row.
+// Groups [g0, g1) of a SELL-32 matrix (4-slot groups: columns col[(g * 32 + lane) * 4 + j], value
+// component c at val[((g * 9 + c) * 32 + lane) * 4 + j]) against u, added to the lane's row sums in slot
+// order.  Values are streamed past L1.
+template <class LdU>
+__device__ __forceinline__ void sell_range(const uint32_t* col, const float* val, uint32_t g0, uint32_t g1,
+                                           uint32_t lane, LdU ld_u, float& o0, float& o1, float& o2)
+{
+    const uint4* C4 = reinterpret_cast<const uint4*>(col);
+    const float4* V4 = reinterpret_cast<const float4*>(val);
+    for (uint32_t g = g0; g < g1; ++g) {
+        const uint4 jc = __ldg(&C4[(size_t)g * 32 + lane]);
+        const float4 pv[4] = {ld_u(jc.x), ld_u(jc.y), ld_u(jc.z), ld_u(jc.w)};
+        const float4* vg = V4 + (size_t)g * 9 * 32 + lane;
+        // one output component at a time (block row r uses components r, r + 3, r + 6): three value
+        // vectors live at once instead of nine
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            const float4 ma = ld_stream4(vg + 32 * r), mb = ld_stream4(vg + 32 * (r + 3)), mc = ld_stream4(vg + 32 * (r + 6));
+            float o = r == 0 ? o0 : r == 1 ? o1 : o2;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                o += __fmaf_rn(comp(mc, j), pv[j].z, __fmaf_rn(comp(mb, j), pv[j].y, comp(ma, j) * pv[j].x));
+            if (r == 0) o0 = o;
+            else if (r == 1) o1 = o;
+            else o2 = o;
+        }
+    }
+}
+
 __device__ __forceinline__ void row_matvec(const RowArgs& a, uint32_t i, uint32_t row, bool own, uint32_t slice,
                                           uint32_t lane, const float4* src, float v0, float v1, float v2, float& q0,
                                           float& q1, float& q2)
@@ -557,38 +712,21 @@ __device__ __forceinline__ void row_matvec(const RowArgs& a, uint32_t i, uint32_
     q1 = __fmaf_rn(c2.y, v2, __fmaf_rn(c1.y, v1, c0.y * v0));
     q2 = __fmaf_rn(c2.z, v2, __fmaf_rn(c1.z, v1, c0.z * v0));
     float o0 = 0.f, o1 = 0.f, o2 = 0.f;
+    const auto ld_src = [&](uint32_t col) { return __ldcg(&src[col]); };
     if (a.sell && slice * 32 < a.n) {  // threads past the last slice have no slot range
-        const uint32_t g0 = __ldg(&a.m_ptr[slice]) >> 2, g1 = __ldg(&a.m_ptr[slice + 1]) >> 2;
-        const uint4* C4 = reinterpret_cast<const uint4*>(a.m_col);
-        const float4* V4 = reinterpret_cast<const float4*>(a.m_val);
-        for (uint32_t g = g0; g < g1; ++g) {
-            const uint4 jc = __ldg(&C4[(size_t)g * 32 + lane]);
-            const float4 pv[4] = {__ldcg(&src[jc.x]), __ldcg(&src[jc.y]), __ldcg(&src[jc.z]), __ldcg(&src[jc.w])};
-            const float4* vg = V4 + (size_t)g * 9 * 32 + lane;
-            // one output component at a time (block row r uses components r, r + 3, r + 6): three
-            // value vectors live at once instead of nine
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                const float4 ma = ld_stream4(vg + 32 * r), mb = ld_stream4(vg + 32 * (r + 3)),
-                             mc = ld_stream4(vg + 32 * (r + 6));
-                float o = r == 0 ? o0 : r == 1 ? o1 : o2;
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    o += __fmaf_rn(comp(mc, j), pv[j].z, __fmaf_rn(comp(mb, j), pv[j].y, comp(ma, j) * pv[j].x));
-                if (r == 0) o0 = o;
-                else if (r == 1) o1 = o;
-                else o2 = o;
-            }
-        }
+        sell_range(a.m_col, a.m_val, __ldg(&a.m_ptr[slice]) >> 2, __ldg(&a.m_ptr[slice + 1]) >> 2, lane, ld_src, o0,
+                   o1, o2);
     } else if (a.m_ptr && own) {
         const uint32_t end = __ldg(&a.m_ptr[i + 1]);
         for (uint32_t k = __ldg(&a.m_ptr[i]); k < end; ++k)
             acc_block(a.m_val + 9 * (size_t)k, 1, __ldcg(&src[__ldg(&a.m_col[k])]), o0, o1, o2);
     }
-    if (a.B.rp && own) {
-        const uint32_t end = __ldcg(&a.B.rp[i + 1]);
-        for (uint32_t k = __ldcg(&a.B.rp[i]); k < end; ++k)
-            acc_block(a.B.val + 9 * (size_t)k, 1, __ldcg(&src[__ldcg(&a.B.col[k])]), o0, o1, o2);
+    if (a.c_ptr && *a.c_ok) {
+        if (slice * 32 < a.n)
+            sell_range(a.c_col, a.c_val, __ldcg(&a.c_ptr[slice]) >> 2, __ldcg(&a.c_ptr[slice + 1]) >> 2, lane, ld_src,
+                       o0, o1, o2);
+    } else if (a.B.rp) {
+        contact_warp(a.B, i - lane, a.n, a.b_vec != 0, ld_src, o0, o1, o2);
     }
     q0 += o0;
     q1 += o1;
@@ -966,6 +1104,287 @@ __global__ void __launch_bounds__(BS, 3) k_pcg_cg1(RowArgs a)
     }
 }
 
+// ------------------------------------------------------------ slice-resident single-reduction solve
+// The same single-reduction PCG as k_pcg_cg1 for a SELL-32 material matrix, laid out for one block per
+// SM: block c owns the contiguous slices [c S / P, (c + 1) S / P) (S slices, P blocks), so every SM
+// holds the same number of rows (within one slice).  Per solve the block copies the first `gres` 4-slot
+// groups of each of its slices (values and columns) into shared memory, where they stay for all
+// iterations; the remaining groups, the diagonal and the contact blocks are read from L2 as before.
+// u of the block's own rows is kept in shared memory too, so only columns owned by other blocks are
+// gathered from L2.
+//
+// Synchronisation: the dot-product reduction is a grid barrier; the publication of u before w = A u
+// is not -- each block waits only for the blocks whose rows its own rows reference (a bit mask built
+// once per solve from the material and contact columns), through per-block flags holding the
+// iteration each block last published.  A block overwrites u only after the next reduction barrier,
+// which every reader of the previous u has passed, so one u buffer suffices (as in k_pcg_cg1).
+// Summation orders are those of k_pcg_cg1: the diagonal, the material slots in slot order, the
+// contact blocks in CSR order; the dot products in a fixed order over warps and blocks.
+constexpr int kResThreads = 640;                           // at most 20 slices (640 rows) per block
+constexpr int kResGroupBytes = 9 * 32 * 16 + 32 * 16;      // values + columns of one group of a slice
+constexpr int kResMaxBlocks = 512;
+constexpr int kResDepWords = kResMaxBlocks / 32;
+
+struct ResArgs {
+    RowArgs a;
+    unsigned* flags;     // per block: the last iteration tag whose u the block published
+    uint32_t n_slices;
+    uint32_t max_slices; // slices of the largest block (shared-memory stride)
+    int gres;            // resident groups per slice
+};
+
+__device__ __forceinline__ uint32_t res_owner(uint32_t slice, uint32_t S, uint32_t P)
+{
+    return (uint32_t)((((uint64_t)slice + 1) * P - 1) / S);
+}
+
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// publish this block's u (stores already issued by every thread), then wait for the blocks in `dep`:
+// thread b waits for block b, so all waits run at once.  Flags are kResFlagStride words apart (one
+// 32-B sector each), so the polls of different blocks do not share a sector.
+constexpr int kResFlagStride = 8;
+
+__device__ __forceinline__ bool res_publish_wait(unsigned* flags, unsigned tag, const unsigned* dep,
+                                                 lcs_pcg_stats* stats, volatile int* s_fail)
+{
+    __syncthreads();
+    const uint32_t t = threadIdx.x;
+    if (t == 0) {
+        __threadfence();
+        st_release(flags + kResFlagStride * blockIdx.x, tag);
+    }
+    if (t < gridDim.x && ((dep[t >> 5] >> (t & 31u)) & 1u)) {
+        const unsigned* f = flags + kResFlagStride * t;
+        unsigned it = 0;
+        while ((int)(ld_acquire(f) - tag) < 0) {
+            if (++it > kBarrierSpinLimit) {
+                *s_fail = 1;
+                stats->status = LCS_ERR_TIMEOUT;
+                break;
+            }
+        }
+    }
+    __syncthreads();
+    return *s_fail == 0;
+}
+
+template <int BT>
+__global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
+{
+    const RowArgs& a = ra.a;
+    extern __shared__ __align__(16) unsigned char res_smem[];
+    __shared__ int s_fail;
+    __shared__ unsigned s_dep[kResDepWords];
+    const uint32_t P = gridDim.x, S = ra.n_slices, c = blockIdx.x;
+    const uint32_t s_lo = (uint32_t)(((uint64_t)c * S) / P), s_hi = (uint32_t)(((uint64_t)(c + 1) * S) / P);
+    const uint32_t nsl = s_hi - s_lo, row0 = 32u * s_lo;
+    const uint32_t nloc = min(32u * s_hi, a.n) - row0;
+    const int G = ra.gres;
+    float4* su = reinterpret_cast<float4*>(res_smem);                      // BT
+    double(*spart)[4] = reinterpret_cast<double(*)[4]>(su + BT);            // P
+    float4* sval = reinterpret_cast<float4*>(spart + P);                   // [max_slices * G][9][32]
+    uint4* scol = reinterpret_cast<uint4*>(sval + (size_t)ra.max_slices * G * 9 * 32);  // [max_slices * G][32]
+    const uint32_t t = threadIdx.x, ls = t >> 5, lane = t & 31u;
+    const uint32_t i = row0 + t;
+    const bool own = ls < nsl && i < a.n;
+    const uint32_t row = own ? i : row0;
+    const uint32_t slice = s_lo + ls;
+    if (t == 0) s_fail = 0;
+    for (int w = t; w < kResDepWords; w += BT) s_dep[w] = 0u;
+    unsigned gen_seen = t == 0 ? ld_acquire(a.bar_gen) : 0u;
+    const uint4* C4 = reinterpret_cast<const uint4*>(a.m_col);
+    const float4* V4 = reinterpret_cast<const float4*>(a.m_val);
+    uint32_t g0 = 0, g1 = 0;
+    if (ls < nsl) {
+        g0 = __ldg(&a.m_ptr[slice]) >> 2;
+        g1 = __ldg(&a.m_ptr[slice + 1]) >> 2;
+        // this warp's slice: resident groups to shared memory
+        const uint32_t nres = min((uint32_t)G, g1 - g0);
+        for (uint32_t j = 0; j < nres; ++j) {
+            const float4* src = V4 + (size_t)(g0 + j) * 9 * 32;
+            float4* dst = sval + ((size_t)ls * G + j) * 9 * 32;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) dst[32 * k + lane] = ld_stream4(src + 32 * k + lane);
+            scol[((size_t)ls * G + j) * 32 + lane] = __ldg(&C4[(size_t)(g0 + j) * 32 + lane]);
+        }
+    }
+    __syncthreads();  // s_dep cleared
+    // the blocks this block's rows read u from: a window of 32 blocks around c by warp vote, others
+    // (distant contacts) one shared-memory OR each
+    {
+        unsigned near = 0u;
+        auto note = [&](uint32_t col) {
+            const uint32_t oc = res_owner(col >> 5, S, P);
+            if (oc == c) return;
+            const int d = (int)oc - (int)c + 16;
+            if (d >= 0 && d < 32) near |= 1u << d;
+            else atomicOr(&s_dep[oc >> 5], 1u << (oc & 31u));
+        };
+        if (ls < nsl) {
+            for (uint32_t g = g0; g < g1; ++g) {
+                const uint4 jc = __ldg(&C4[(size_t)g * 32 + lane]);
+                if (own) { note(jc.x); note(jc.y); note(jc.z); note(jc.w); }
+            }
+        }
+        if (a.B.rp && own) {
+            const uint32_t end = __ldcg(&a.B.rp[i + 1]);
+            for (uint32_t k = __ldcg(&a.B.rp[i]); k < end; ++k) note(__ldcg(&a.B.col[k]));
+        }
+        near = __reduce_or_sync(0xFFFFFFFFu, near);
+        if (lane == 0) {
+            while (near) {
+                const int d = __ffs(near) - 1;
+                near &= near - 1u;
+                const uint32_t oc = c + (uint32_t)d - 16u;
+                atomicOr(&s_dep[oc >> 5], 1u << (oc & 31u));
+            }
+        }
+    }
+    // u = M^-1 b; the inverse diagonal block stays in registers
+    float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+    float m0, m1, m2, m3, m4, m5, m6, m7, m8;
+    {
+        const float4 bv = a.b[row];
+        if (own) { r0 = bv.x; r1 = bv.y; r2 = bv.z; }
+        const float4 c0 = a.diag[3 * row], c1 = a.diag[3 * row + 1], c2 = a.diag[3 * row + 2];
+        const float aa = c0.x, bb = c1.x, cc = c2.x, d = c0.y, e = c1.y, f = c2.y, g = c0.z, h = c1.z, k = c2.z;
+        const float A = e * k - f * h, B = f * g - d * k, C = d * h - e * g;
+        const float id = 1.0f / (aa * A + bb * B + cc * C);
+        m0 = A * id; m1 = B * id; m2 = C * id;
+        m3 = (cc * h - bb * k) * id; m4 = (aa * k - cc * g) * id; m5 = (bb * g - aa * h) * id;
+        m6 = (bb * f - cc * e) * id; m7 = (cc * d - aa * f) * id; m8 = (aa * e - bb * d) * id;
+    }
+    const bool c_sell = a.c_ptr && *a.c_ok;
+    auto ld_u = [&](uint32_t col) -> float4 {
+        const uint32_t lc = col - row0;
+        return lc < nloc ? su[lc] : __ldcg(&a.pg[col]);
+    };
+    // w = A u for the lane's row (k_pcg_cg1's row_matvec with the resident groups and local u); called by
+    // every lane of the block's slices, lanes past n compute a discarded value
+    auto matvec = [&](float v0, float v1, float v2, float& q0, float& q1, float& q2) {
+        const float4 c0 = __ldg(&a.diag[3 * row]), c1 = __ldg(&a.diag[3 * row + 1]), c2 = __ldg(&a.diag[3 * row + 2]);
+        q0 = __fmaf_rn(c2.x, v2, __fmaf_rn(c1.x, v1, c0.x * v0));
+        q1 = __fmaf_rn(c2.y, v2, __fmaf_rn(c1.y, v1, c0.y * v0));
+        q2 = __fmaf_rn(c2.z, v2, __fmaf_rn(c1.z, v1, c0.z * v0));
+        float o0 = 0.f, o1 = 0.f, o2 = 0.f;
+        for (uint32_t g = g0; g < g1; ++g) {
+            const uint32_t j = g - g0;
+            const bool res = j < (uint32_t)G;
+            const uint4 jc = res ? scol[((size_t)ls * G + j) * 32 + lane] : __ldg(&C4[(size_t)g * 32 + lane]);
+            const float4 pv[4] = {ld_u(jc.x), ld_u(jc.y), ld_u(jc.z), ld_u(jc.w)};
+            const float4* vg = res ? sval + ((size_t)ls * G + j) * 9 * 32 + lane : V4 + (size_t)g * 9 * 32 + lane;
+#pragma unroll
+            for (int rr = 0; rr < 3; ++rr) {
+                float4 ma, mb, mc;
+                if (res) {
+                    ma = vg[32 * rr]; mb = vg[32 * (rr + 3)]; mc = vg[32 * (rr + 6)];
+                } else {
+                    ma = ld_stream4(vg + 32 * rr); mb = ld_stream4(vg + 32 * (rr + 3)); mc = ld_stream4(vg + 32 * (rr + 6));
+                }
+                float o = rr == 0 ? o0 : rr == 1 ? o1 : o2;
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj)
+                    o += __fmaf_rn(comp(mc, jj), pv[jj].z, __fmaf_rn(comp(mb, jj), pv[jj].y, comp(ma, jj) * pv[jj].x));
+                if (rr == 0) o0 = o;
+                else if (rr == 1) o1 = o;
+                else o2 = o;
+            }
+        }
+        if (c_sell)
+            sell_range(a.c_col, a.c_val, __ldcg(&a.c_ptr[slice]) >> 2, __ldcg(&a.c_ptr[slice + 1]) >> 2, lane, ld_u, o0,
+                       o1, o2);
+        else if (a.B.rp)
+            contact_warp(a.B, row0 + 32u * ls, a.n, a.b_vec != 0, ld_u, o0, o1, o2);
+        q0 += o0;
+        q1 += o1;
+        q2 += o2;
+    };
+#define LCS_MINV(v0, v1, v2, o0, o1, o2)                          \
+    {                                                              \
+        o0 = __fmaf_rn(m6, v2, __fmaf_rn(m3, v1, m0 * v0));        \
+        o1 = __fmaf_rn(m7, v2, __fmaf_rn(m4, v1, m1 * v0));        \
+        o2 = __fmaf_rn(m8, v2, __fmaf_rn(m5, v1, m2 * v0));        \
+    }
+    float u0, u1, u2, w0 = 0.f, w1 = 0.f, w2 = 0.f;
+    LCS_MINV(r0, r1, r2, u0, u1, u2)
+    unsigned tag = 1u;
+    if (own) {
+        su[t] = make_float4(u0, u1, u2, 0.0f);
+        __stcg(&a.pg[i], make_float4(u0, u1, u2, 0.0f));
+    }
+    if (!res_publish_wait(ra.flags, tag, s_dep, a.stats, &s_fail)) return;
+    if (ls < nsl) matvec(u0, u1, u2, w0, w1, w2);  // whole warps (the contact product is warp-wide)
+    float x0 = 0.f, x1 = 0.f, x2 = 0.f, p0 = 0.f, p1 = 0.f, p2 = 0.f, sd0 = 0.f, sd1 = 0.f, sd2 = 0.f;
+    float gamma_old = 0.0f, alpha_old = 0.0f, norm_r0 = 0.0f, norm_r = 0.0f, gamma = 0.0f;
+    int iter = 0, status = 0;
+    for (iter = 0; iter < a.max_iter; ++iter) {
+        double dg, dd, dr;
+        if (a.fp64) {
+            dg = (double)r0 * u0 + (double)r1 * u1 + (double)r2 * u2;
+            dd = (double)w0 * u0 + (double)w1 * u1 + (double)w2 * u2;
+            dr = (double)r0 * r0 + (double)r1 * r1 + (double)r2 * r2;
+        } else {
+            dg = __fmaf_rn(r2, u2, __fmaf_rn(r1, u1, r0 * u0));
+            dd = __fmaf_rn(w2, u2, __fmaf_rn(w1, u1, w0 * u0));
+            dr = __fmaf_rn(r2, r2, __fmaf_rn(r1, r1, r0 * r0));
+        }
+        if (!own) dg = dd = dr = 0.0;
+        double* part = a.part + 4 * (size_t)P * (iter & 1);
+        block_partial3<BT>(dg, dd, dr, &part[4 * c]);
+        if (!pipe_barrier(a.bar_count, a.bar_gen, gen_seen, a.stats, &s_fail)) return;
+        grid_prefetch3<BT>(part, spart);
+        double sg, sdd, sr;
+        grid_collect3<BT>(spart, sg, sdd, sr);
+        gamma = (float)sg;
+        const float delta = (float)sdd;
+        norm_r = sqrtf((float)sr);
+        if (iter == 0) norm_r0 = norm_r;
+        if (iter % a.check_every == 0) {
+            if (isnan(gamma) || isinf(gamma)) { status = LCS_ERR_NAN; break; }
+            if (gamma < a.abs_rz_tol) break;
+            if (a.rel_tol > 0.0f && norm_r <= a.rel_tol * norm_r0) break;
+        }
+        float beta = 0.0f, alpha = 0.0f;
+        bool restart = iter == 0 || alpha_old == 0.0f;
+        if (!restart) {
+            beta = safe_div(gamma, gamma_old);
+            const float den = delta - beta * gamma / alpha_old;
+            restart = !(den >= kPcgEps);
+            if (!restart) alpha = gamma / den;
+        }
+        if (restart) {
+            beta = 0.0f;
+            alpha = safe_div(gamma, delta);
+        }
+        p0 = u0 + beta * p0; p1 = u1 + beta * p1; p2 = u2 + beta * p2;
+        sd0 = w0 + beta * sd0; sd1 = w1 + beta * sd1; sd2 = w2 + beta * sd2;
+        x0 = x0 + alpha * p0; x1 = x1 + alpha * p1; x2 = x2 + alpha * p2;
+        r0 -= alpha * sd0; r1 -= alpha * sd1; r2 -= alpha * sd2;
+        LCS_MINV(r0, r1, r2, u0, u1, u2)
+        ++tag;
+        if (own) {
+            su[t] = make_float4(u0, u1, u2, 0.0f);
+            __stcg(&a.pg[i], make_float4(u0, u1, u2, 0.0f));
+        }
+        if (!res_publish_wait(ra.flags, tag, s_dep, a.stats, &s_fail)) return;
+        if (ls < nsl) matvec(u0, u1, u2, w0, w1, w2);
+        gamma_old = gamma;
+        alpha_old = alpha;
+    }
+#undef LCS_MINV
+    if (own) a.x[i] = make_float4(x0, x1, x2, 0.0f);
+    if (c == 0 && t == 0) {
+        a.stats->iterations = iter;
+        a.stats->rel_residual = norm_r0 > 0.0f ? norm_r / norm_r0 : 0.0f;
+        a.stats->dot_rz = gamma;
+        if (a.stats->status == LCS_OK) a.stats->status = status;
+    }
+}
+
 // ------------------------------------------------------------------------ batched scenes
 // Many independent systems (one per scene, rows [roff[s], roff[s+1])) solved in one launch: one
 // thread-block cluster per scene, synchronised by the hardware cluster barrier, with the scene's
@@ -1182,6 +1601,10 @@ struct lcs_pcg {
     float* scal = nullptr;       // plain-mode scalars
     float* h_scal = nullptr;     // pinned host copy
     unsigned* bar = nullptr;     // [count, gen]
+    unsigned* flags = nullptr;   // slice-resident solve: per-block publication tags (kResMaxBlocks)
+    int res_gres = -2;           // slice-resident solve: resident groups per slice (-2: not set up)
+    uint32_t res_blocks = 0, res_slices = 0, res_max_slices = 0;
+    size_t res_smem = 0;
     lcs_pcg_stats* d_stats = nullptr;
     int fused_grid = 0;
     int rows_capacity = -1;  // most rows the row-resident solve can hold co-resident (-1: not queried)
@@ -1198,6 +1621,7 @@ struct lcs_pcg {
 static constexpr int kRowLanes = 4;
 static constexpr int kPlainBlocks = 256;
 static constexpr int kRowMaxBlocks = 1024;
+static constexpr int kPcgNoResident = LCS_PCG_INTERNAL_NO_RESIDENT;
 
 extern "C" int lcs_pcg_create(uint32_t n, lcs_pcg** out)
 {
@@ -1224,6 +1648,7 @@ extern "C" int lcs_pcg_create(uint32_t n, lcs_pcg** out)
     A((void**)&p->part_f, 3 * sizeof(float) * parts);
     A((void**)&p->scal, 16 * sizeof(float));
     A((void**)&p->bar, 2 * sizeof(unsigned));
+    A((void**)&p->flags, kResFlagStride * kResMaxBlocks * sizeof(unsigned));
     A((void**)&p->d_stats, sizeof(lcs_pcg_stats));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&p->h_scal, 16 * sizeof(float));
     if (e == cudaSuccess) e = cudaMemset(p->bar, 0, 2 * sizeof(unsigned));
@@ -1238,8 +1663,8 @@ extern "C" int lcs_pcg_create(uint32_t n, lcs_pcg** out)
 extern "C" int lcs_pcg_destroy(lcs_pcg* p)
 {
     if (!p) return LCS_OK;
-    void* ptrs[] = {p->r, p->z, p->p, p->q, p->minv, p->part, p->part_f, p->scal, p->bar, p->d_stats, p->cpart,
-                    p->class_scenes};
+    void* ptrs[] = {p->r, p->z, p->p, p->q, p->minv, p->part, p->part_f, p->scal, p->bar, p->flags, p->d_stats,
+                    p->cpart, p->class_scenes};
     for (int k = 0; k < 5; ++k) {
         if (p->class_stream[k]) {
             cudaStreamSynchronize(p->class_stream[k]);
@@ -1325,10 +1750,151 @@ static int plain_solve(lcs_pcg* P, const float4* diag, Bsr A, Bsr B, const float
     return status == LCS_OK ? LCS_OK : lcs_fail(status, "lcs_pcg_solve: NaN/Inf in r.z");
 }
 
+// Launch shape of the slice-resident solve for P->n rows: one block per SM (fewer when there are fewer
+// slices), at most kResThreads / 32 slices per block, and as many resident groups per slice as the
+// shared memory left after u and the partial sums holds.  LCS_ERR_CAPACITY when it does not apply.
+static int res_setup(lcs_pcg* P)
+{
+    if (P->res_gres >= 0) return LCS_OK;
+    if (P->res_gres == -1) return LCS_ERR_CAPACITY;
+    P->res_gres = -1;
+    int dev = 0, sms = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return LCS_ERR_CAPACITY;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const uint32_t S = (P->n + 31) / 32;
+    uint32_t blocks = (uint32_t)sms < S ? (uint32_t)sms : S;
+    if (blocks > (uint32_t)kResMaxBlocks) blocks = kResMaxBlocks;
+    if (blocks > (uint32_t)kResThreads) blocks = kResThreads;  // one waiting thread per block
+    if (blocks == 0) return LCS_ERR_CAPACITY;
+    const uint32_t max_slices = (S + blocks - 1) / blocks;
+    if (max_slices > (uint32_t)(kResThreads / 32)) return LCS_ERR_CAPACITY;
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, k_pcg_res<kResThreads>) != cudaSuccess) return LCS_ERR_CAPACITY;
+    const size_t base = 16 * (size_t)kResThreads + 32 * (size_t)blocks;
+    const size_t avail = (size_t)optin > fa.sharedSizeBytes + base ? (size_t)optin - fa.sharedSizeBytes - base : 0;
+    size_t gres = avail / ((size_t)max_slices * kResGroupBytes);
+    if (gres > 8) gres = 8;
+    const size_t dyn = base + gres * max_slices * kResGroupBytes;
+    if (cudaFuncSetAttribute(k_pcg_res<kResThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return LCS_ERR_CAPACITY;
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_res<kResThreads>, kResThreads, dyn);
+    if (per_sm < 1 || (int64_t)per_sm * sms < (int64_t)blocks) return LCS_ERR_CAPACITY;
+    P->res_blocks = blocks;
+    P->res_slices = S;
+    P->res_max_slices = max_slices;
+    P->res_smem = dyn;
+    P->res_gres = (int)gres;
+    return LCS_OK;
+}
+
+// ------------------------------------------------ contact blocks as SELL-32 (once per Newton iteration)
+// The contact CSR rewritten in the material matrix's SELL-32 layout, so that the row-resident solves
+// read a row's contact blocks like its material blocks: coalesced 16-B loads, slot order = CSR order
+// (the same sums as the CSR walk).  k_csell_width: slots per slice (the slice's longest row, rounded up
+// to 4); k_csell_scan: slice offsets and the fit flag; k_csell_fill: columns and values at their SELL
+// positions, padding slots as zero blocks against the row itself.
+__global__ void k_csell_width(uint32_t n, const uint32_t* __restrict__ rp, uint32_t* __restrict__ width)
+{
+    const uint32_t S = (n + 31) / 32, lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < S; s += warps) {
+        const uint32_t r = 32 * s + lane;
+        const uint32_t len = r < n ? __ldcg(&rp[r + 1]) - __ldcg(&rp[r]) : 0u;
+        const uint32_t w = __reduce_max_sync(0xFFFFFFFFu, len);
+        if (lane == 0) width[s] = (w + 3u) & ~3u;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_csell_scan(uint32_t S, const uint32_t* __restrict__ width,
+                                                     uint32_t* __restrict__ ptr, uint32_t cap_slots, int* ok)
+{
+    __shared__ uint32_t ws[32];
+    __shared__ uint32_t carry;
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    if (t == 0) carry = 0u;
+    __syncthreads();
+    for (uint32_t base = 0; base < S; base += 1024u) {
+        const uint32_t s = base + t;
+        const uint32_t v = s < S ? width[s] : 0u;
+        uint32_t incl = v;
+#pragma unroll
+        for (uint32_t o = 1; o < 32u; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += x;
+        }
+        if (lane == 31u) ws[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = ws[lane];
+#pragma unroll
+            for (uint32_t o = 1; o < 32u; o <<= 1) {
+                const uint32_t x = __shfl_up_sync(0xFFFFFFFFu, w, o);
+                if (lane >= o) w += x;
+            }
+            ws[lane] = w;
+        }
+        __syncthreads();
+        const uint32_t pre = carry + (warp ? ws[warp - 1] : 0u);
+        if (s < S) ptr[s] = pre + incl - v;
+        __syncthreads();
+        if (t == 0) carry += ws[31];
+        __syncthreads();
+    }
+    if (t == 0) {
+        ptr[S] = carry;
+        *ok = carry <= cap_slots ? 1 : 0;
+    }
+}
+
+__global__ void k_csell_fill(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ col,
+                             const float* __restrict__ val, const uint32_t* __restrict__ ptr, const int* __restrict__ ok,
+                             uint32_t* __restrict__ scol, float* __restrict__ sval)
+{
+    if (!*ok) return;
+    const uint32_t rows = 32u * ((n + 31) / 32);
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+        const uint32_t s = r >> 5, lane = r & 31u;
+        const uint32_t p0 = ptr[s], w = ptr[s + 1] - p0;
+        const uint32_t k0 = r < n ? rp[r] : 0u, len = r < n ? rp[r + 1] - k0 : 0u;
+        const uint32_t pad = r < n ? r : n - 1;
+        for (uint32_t j = 0; j < w; ++j) {
+            const size_t slot = (size_t)p0 + j, g = slot >> 2, jj = slot & 3u;
+            const bool real = j < len;
+            scol[(g * 32 + lane) * 4 + jj] = real ? col[k0 + j] : pad;
+#pragma unroll
+            for (int c = 0; c < 9; ++c)
+                sval[((g * 9 + c) * 32 + lane) * 4 + jj] = real ? val[9 * ((size_t)k0 + j) + c] : 0.0f;
+        }
+    }
+}
+
+int lcs_contact_to_sell(uint32_t n, const lcs_bsr* B, uint32_t* width, uint32_t* ptr, uint32_t* col, float* val,
+                        uint32_t cap_slots, int* ok, lcs_stream stream)
+{
+    if (!B || !B->row_ptr || !width || !ptr || !col || !val || !ok || n == 0)
+        return lcs_fail(LCS_ERR_INVALID, "lcs_contact_to_sell: bad argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint32_t S = (n + 31) / 32;
+    k_csell_width<<<grid_for((uint64_t)S * 32, 256), 256, 0, s>>>(n, B->row_ptr, width);
+    k_csell_scan<<<1, 1024, 0, s>>>(S, width, ptr, cap_slots, ok);
+    k_csell_fill<<<grid_for((uint64_t)S * 32, 256), 256, 0, s>>>(n, B->row_ptr, B->col, B->val, ptr, ok, col, val);
+    for (int k = 0; k < 3; ++k) lcs_count_launch();
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+int lcs_pcg_resident(lcs_pcg* P) { return P && res_setup(P) == LCS_OK ? 1 : 0; }
+
 // row-resident solve; LCS_ERR_CAPACITY when one thread per row does not fit co-resident
 static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* m_ptr, const uint32_t* m_col,
                       const float* m_val, Bsr B, const float4* b, float4* x, const lcs_pcg_opts& o,
-                      lcs_pcg_stats* stats, cudaStream_t s)
+                      lcs_pcg_stats* stats, cudaStream_t s, const uint32_t* c_ptr = nullptr,
+                      const uint32_t* c_col = nullptr, const float* c_val = nullptr, const int* c_ok = nullptr)
 {
     if (P->rows_capacity < 0) P->rows_capacity = (int)lcs_pcg_rows_capacity();
     if ((int64_t)P->n > P->rows_capacity) return LCS_ERR_CAPACITY;
@@ -1342,6 +1908,12 @@ static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* 
     a.m_col = m_col;
     a.m_val = m_val;
     a.B = B;
+    a.b_vec = B.val && (reinterpret_cast<uintptr_t>(B.val) & 15u) == 0;
+    const bool cs = sell && c_ptr && c_col && c_val && c_ok;
+    a.c_ptr = cs ? c_ptr : nullptr;
+    a.c_col = cs ? c_col : nullptr;
+    a.c_val = cs ? c_val : nullptr;
+    a.c_ok = cs ? c_ok : nullptr;
     a.b = b;
     a.x = x;
     a.pg = P->p;
@@ -1358,7 +1930,13 @@ static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* 
     LCS_CUDA_TRY(cudaMemsetAsync(P->bar, 0, sizeof(unsigned), s));
     void* args[] = {&a};
     const int grid = (int)((P->n + kRowThreads - 1) / kRowThreads);
-    if (pipe)
+    if (pipe && sell && !(o.flags & kPcgNoResident) && res_setup(P) == LCS_OK) {
+        ResArgs ra{a, P->flags, P->res_slices, P->res_max_slices, P->res_gres};
+        void* rargs[] = {&ra};
+        LCS_CUDA_TRY(cudaMemsetAsync(P->flags, 0, sizeof(unsigned) * kResFlagStride * P->res_blocks, s));
+        LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_res<kResThreads>, dim3(P->res_blocks),
+                                                 dim3(kResThreads), rargs, P->res_smem, s));
+    } else if (pipe)
         LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_cg1<kRowThreads>, dim3(grid), dim3(kRowThreads),
                                                  args, 0, s));
     else
@@ -1389,12 +1967,13 @@ int64_t lcs_pcg_rows_capacity()
 
 int lcs_pcg_solve_sell(lcs_pcg* P, const float* diag, const uint32_t* slice_ptr, const uint32_t* col,
                        const float* val, const lcs_bsr* B, const float* b, float* x, const lcs_pcg_opts* opts,
-                       lcs_pcg_stats* stats, lcs_stream stream)
+                       lcs_pcg_stats* stats, lcs_stream stream, const uint32_t* c_ptr, const uint32_t* c_col,
+                       const float* c_val, const int* c_ok)
 {
     if (!P || !diag || !b || !x || !opts) return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_sell: bad argument");
     return rows_solve(P, reinterpret_cast<const float4*>(diag), 1, slice_ptr, col, val, to_bsr(B),
                       reinterpret_cast<const float4*>(b), reinterpret_cast<float4*>(x), *opts, stats,
-                      (cudaStream_t)stream);
+                      (cudaStream_t)stream, c_ptr, c_col, c_val, c_ok);
 }
 
 extern "C" int lcs_pcg_solve(lcs_pcg* P, const float* diag, const lcs_bsr* A, const lcs_bsr* B, const float* b,

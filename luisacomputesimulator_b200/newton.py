@@ -96,13 +96,15 @@ class NewtonSolver:
 
     plain=True selects the reference's dispatch structure (the one-scene comparator);
     fp64=True the precision form; profile=True per-phase CUDA-event timing;
-    single_reduction=True the single-reduction row-resident PCG (fused mode); energy_linesearch=True the
+    single_reduction=True the single-reduction row-resident PCG (fused mode; slice-resident where the rows fit,
+    unless global_matrix=True); energy_linesearch=True the
     reference's use_energy_linesearch (step halving until the energy decreases).
     """
 
     def __init__(self, scene, plain=False, fp64=False, profile=False, nonlinear_iters=3, pcg_max_iter=100,
                  pcg_rel_tol=1e-4, pcg_abs_rz_tol=1e-10, pcg_check_every=25, damping=2.0, use_floor=False,
-                 floor_y=0.0, stream=None, single_reduction=False, full_traversal=False, energy_linesearch=False):
+                 floor_y=0.0, stream=None, single_reduction=False, full_traversal=False, energy_linesearch=False,
+                 global_matrix=False):
         self.lib = A.load()
         self.scene = scene
         sc = scene
@@ -114,7 +116,8 @@ class NewtonSolver:
         flags = (A.LCS_NEWTON_PLAIN if plain else 0) | (A.LCS_NEWTON_FP64 if fp64 else 0) | \
             (A.LCS_NEWTON_PROFILE if profile else 0) | (A.LCS_NEWTON_PCG_SINGLE_REDUCTION if single_reduction else 0) | \
             (A.LCS_NEWTON_FULL_TRAVERSAL if full_traversal else 0) | \
-            (A.LCS_NEWTON_ENERGY_LINESEARCH if energy_linesearch else 0)
+            (A.LCS_NEWTON_ENERGY_LINESEARCH if energy_linesearch else 0) | \
+            (A.LCS_NEWTON_PCG_GLOBAL_MATRIX if global_matrix else 0)
         s = C.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
         h = C.c_void_p()
         A.check(self.lib.lcs_newton_create(C.byref(d), flags, s, C.byref(h)), "lcs_newton_create")
@@ -193,11 +196,12 @@ class NewtonSolver:
         A.check(self.lib.lcs_newton_reset_profile(self.h), "lcs_newton_reset_profile")
 
     def pcg_kind(self):
-        """'plain', 'fused' (persistent CSR solve), 'rows' or 'cg1' (row-resident: classic, single-reduction)."""
-        return ["plain", "fused", "rows", "cg1"][self.lib.lcs_newton_pcg_kind(self.h)]
+        """'plain', 'fused' (persistent CSR solve), 'rows', 'cg1' (row-resident: classic, single-reduction) or
+        'cg1-res' (single-reduction, slice-resident: one block per SM with its matrix groups in shared memory)."""
+        return ["plain", "fused", "rows", "cg1", "cg1-res"][self.lib.lcs_newton_pcg_kind(self.h)]
 
     def uses_row_pcg(self):
-        return self.pcg_kind() in ("rows", "cg1")
+        return self.pcg_kind() in ("rows", "cg1", "cg1-res")
 
     def counts(self):
         v = [C.c_uint32() for _ in range(4)]

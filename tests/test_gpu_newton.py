@@ -45,11 +45,14 @@ def test_one_newton_iteration_matches_cpu_restatement():
     assert abs(st.last_toi - toi) <= 1e-3 * toi + 1e-6
 
 
-@pytest.mark.parametrize("fp64,cg1", [(False, False), (True, False), (False, True)])
-def test_drop_stays_intersection_free(fp64, cg1):
+@pytest.mark.parametrize("fp64,cg1,gm", [(False, False, False), (True, False, False), (False, True, False),
+                                         (False, True, True)])
+def test_drop_stays_intersection_free(fp64, cg1, gm):
+    # cloth rows first, sphere rows after: the contacts couple rows of distant blocks of the
+    # slice-resident solve (its dependency mask beyond the neighbouring blocks)
     sc = S.cloth_on_sphere(n=32)
-    gpu = NewtonSolver(sc, fp64=fp64, single_reduction=cg1)
-    assert gpu.pcg_kind() == ("cg1" if cg1 else "rows")
+    gpu = NewtonSolver(sc, fp64=fp64, single_reduction=cg1, global_matrix=gm)
+    assert gpu.pcg_kind() == (("cg1" if gm else "cg1-res") if cg1 else "rows")
     d0 = O.min_distance(sc, sc.x)
     for k in range(40):
         st = gpu.step()
@@ -86,3 +89,22 @@ def test_twisted_tube_steps_small():
         x = gpu.positions()
         assert np.isfinite(x).all()
         assert O.min_distance(sc, x) > 0.0
+
+
+def test_slice_resident_pcg_matches_the_global_form_on_the_tube():
+    """The 88,800-row tube at a twisted, self-touching state: one step with the slice-resident solve
+    (one block per SM, leading matrix groups in shared memory, neighbour-only publication waits) and
+    one with the 256-row-block form that reads the matrix from L2.  Same summation order per row, so
+    the steps agree to rounding of the grid-wide dot products."""
+    sc, x = SC.twisted_tube_state(angle=1.2)
+    out = {}
+    for gm in (False, True):
+        gpu = NewtonSolver(sc, single_reduction=True, global_matrix=gm)
+        assert gpu.pcg_kind() == ("cg1" if gm else "cg1-res")
+        st = gpu.step_host(x_in=x.copy())
+        assert st.status == 0
+        out[gm] = (gpu.positions(), st.pcg_iters, st.newton_iters)
+    (xa, ia, na), (xb, ib, nb) = out[False], out[True]
+    assert na == nb and abs(ia - ib) <= 2 * na
+    scale = np.abs(xb[:, :3] - x[:, :3]).max()
+    np.testing.assert_allclose(xa[:, :3], xb[:, :3], rtol=0, atol=1e-3 * scale + 1e-7)
