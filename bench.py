@@ -136,9 +136,9 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def committed_traffic():
-    """DRAM bytes per launch of the row-resident PCG solve from the committed ncu capture (or None)."""
-    path = os.path.join(ROOT, "profiles", "k_pcg_cg1_tube88k_traffic.txt")
+def committed_traffic(kernel):
+    """DRAM bytes per launch of the tube's PCG kernel from the committed ncu capture (or None)."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_tube88k_traffic.txt")
     try:
         for ln in open(path):
             if ln.startswith("bytes_per_launch="):
@@ -309,7 +309,7 @@ def run_ours(a):
         bytes_per_launch = it_per_launch * bytes_per_iter + 160.0 * V
         achieved = bytes_per_launch / (pcg_ms / max(pcg_launches, 1) / 1e3) / 1e9
         peak, peak_kind = measured_peak()
-        traffic = committed_traffic()
+        traffic = committed_traffic(pcg_kernel_name.split()[0])
         cpu = None
         if not a.no_cpu_baseline and world == 1:
             v_cpu, n_cpu, el_cpu, cores, _ = cpu_sample(a, a.cpu_iters)
