@@ -133,6 +133,16 @@ LCS_API int lcs_bvh_query_ee(const lcs_bvh* edge_tree, const float* x0, const fl
                      const float* thickness, uint32_t* pairs, uint32_t capacity, uint32_t* d_count,
                      lcs_stream stream);
 
+/* The candidate set of lcs_bvh_query_ee over every edge of the tree with thickness 0 and the same
+ * d_hat for every edge's first vertex (no counterpart in the reference; what the Newton loop uses
+ * when its scene satisfies that): each pair is met once, from the leaf with the lower Morton
+ * position, and decided by the reference's test in the reference's direction, so the list holds the
+ * same (eid, adj_eid) pairs, eid < adj_eid, in another order.  The edge tree must have been refitted
+ * by this library (its node records carry the subtrees' last sorted positions). */
+LCS_API int lcs_bvh_query_ee_sym(const lcs_bvh* edge_tree, const float* x0, const float* x1, const uint32_t* edges,
+                                 float d_hat, uint32_t* pairs, uint32_t capacity, uint32_t* d_count,
+                                 lcs_stream stream);
+
 /* LBVH::check_health (lbvh.cpp:1033-1036).  Synchronises `stream`. host out. */
 /* Candidate filter (no counterpart in the reference): the pairs of a VF (is_ee = 0, elems = faces)
  * or EE (is_ee = 1, elems = edges) candidate list whose boxes overlap at positions x, with the

@@ -97,6 +97,7 @@ SIGNATURES = {
     "lcs_bvh_update_refit": (I32, [P, P, P, P, P, P]),
     "lcs_bvh_query_vf": (I32, [P, P, P, U32, P, P, P, U32, P, P]),
     "lcs_bvh_query_ee": (I32, [P, P, P, P, U32, P, P, P, U32, P, P]),
+    "lcs_bvh_query_ee_sym": (I32, [P, P, P, P, C.c_float, P, U32, P, P]),
     "lcs_bvh_health": (I32, [P, C.POINTER(C.c_int), P]),
     "lcs_bvh_export": (I32, [P, P, P, P, P, P, P, P, P, P]),
     "lcs_bvh_num_leaves": (U32, [P]),

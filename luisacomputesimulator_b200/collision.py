@@ -151,6 +151,12 @@ class LBVH:
                                           ptr(thickness), ptr(pairs), pairs.shape[0], ptr(count), stream()),
                 "query_ee")
 
+    def broad_phase_query_from_edges_sym(self, x0, x1, edges, count, pairs, d_hat):
+        """The set of broad_phase_query_from_edges for thickness 0 and one d_hat (a float) on every edge,
+        each pair met once (no counterpart in the reference)."""
+        A.check(self.lib.lcs_bvh_query_ee_sym(self.h, ptr(x0), ptr(x1), ptr(edges), float(d_hat), ptr(pairs),
+                                              pairs.shape[0], ptr(count), stream()), "query_ee_sym")
+
     def export(self):
         """The tree in the reference's LbvhData layout (CUDA tensors)."""
         n = self.n

@@ -233,7 +233,7 @@ __global__ void k_leaves_refit(int kind, uint32_t n, const uint32_t* __restrict_
                 store_slot(wide, 0, mn, mx, 0x80000000u | e);
                 store_slot(wide, 1, mn, mx, 0x80000000u | e);
             } else {
-                store_slot(wide, slot[ni + lid], mn, mx, 0x80000000u | e);
+                store_slot(wide, slot[ni + lid], mn, mx, 0x80000000u | e, lid);
             }
         }
         if (!climb || n == 1) continue;
@@ -252,7 +252,8 @@ __global__ void k_leaves_refit(int kind, uint32_t n, const uint32_t* __restrict_
             v3 mn = mk3(fmn(a0.x, b0.x), fmn(a0.y, b0.y), fmn(a0.z, b0.z));
             v3 mx = mk3(fmx(a1.x, b1.x), fmx(a1.y, b1.y), fmx(a1.z, b1.z));
             if (p == 0) break;
-            store_slot(wide, slot[p], mn, mx, p);
+            const uint32_t la = __float_as_uint(a1.w), lb = __float_as_uint(b1.w);
+            store_slot(wide, slot[p], mn, mx, p, la > lb ? la : lb);
             p = parent[p];
         }
     }
@@ -336,6 +337,85 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide, 
                 if (base + k < capacity) pairs[base + k] = make_uint2(q, hit[k]);
             if (stop || ++loop > 100000u) {  // the reference's early exits; reported so callers know the
                 if (capped) atomicOr(capped, 1u);  // list may lack pairs a complete traversal would find
+                break;
+            }
+        }
+    }
+}
+
+// EE candidates with every pair found once: the set query_template2 / fn_query_from_edges_v2 produce
+// ({(a, b): a < b, query box of a overlaps leaf box of b}) when every edge's first vertex has thickness 0
+// and the same d_hat r.  The query of the leaf at sorted position i visits only slots whose largest
+// sorted position (`last`) exceeds i, so each pair of leaves is met from the lower position alone, with a
+// culling box a few ulps wider than the query box; at a leaf the reference's own test decides, in the
+// reference's direction: for q < e the query box of q against the leaf box of e, for e < q the query box
+// of e (e's leaf box widened by r, exact since its thickness is 0) against the leaf box of q (q's own box).
+// Pairs are written (smaller id, larger id) as the reference writes them.  Leaves of other queries are
+// pruned by position, not by id, so a traversal visits about half the nodes of k_query<true>.
+__global__ void __launch_bounds__(128) k_query_ee_sym(const float4* __restrict__ wide, const uint32_t* __restrict__ sgo,
+                                                      uint32_t n_leaves, const float4* __restrict__ x0,
+                                                      const float4* __restrict__ x1, const uint2* __restrict__ edges,
+                                                      float r, uint2* __restrict__ pairs, uint32_t capacity,
+                                                      uint32_t* d_count, uint32_t* capped)
+{
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_leaves; t += gridDim.x * blockDim.x) {
+        const uint32_t q = __ldg(&sgo[t]);
+        const uint2 ed = __ldg(&edges[q]);
+        const v3 s0 = ld3(x0, ed.x), s1 = ld3(x0, ed.y), e0 = ld3(x1, ed.x), e1 = ld3(x1, ed.y);
+        const v3 mn = min3(min3(s0, s1), min3(e0, e1)), mx = max3(max3(s0, s1), max3(e0, e1));
+        const float4 own_mn = make_float4(mn.x, mn.y, mn.z, 0.f), own_mx = make_float4(mx.x, mx.y, mx.z, 0.f);
+        const float box[6] = {mn.x - r, mn.y - r, mn.z - r, mx.x + r, mx.y + r, mx.z + r};
+        float cull[6];
+        {
+            const float mgx = (fabsf(mn.x) + fabsf(mx.x) + r) * 9.5367431640625e-07f;  // 2^-20
+            const float mgy = (fabsf(mn.y) + fabsf(mx.y) + r) * 9.5367431640625e-07f;
+            const float mgz = (fabsf(mn.z) + fabsf(mx.z) + r) * 9.5367431640625e-07f;
+            cull[0] = box[0] - mgx; cull[1] = box[1] - mgy; cull[2] = box[2] - mgz;
+            cull[3] = box[3] + mgx; cull[4] = box[4] + mgy; cull[5] = box[5] + mgz;
+        }
+        uint32_t stack[32];
+        int sp = 0;
+        uint32_t loop = 0;
+        stack[sp++] = 0;
+        while (sp > 0) {
+            const uint32_t node = stack[--sp];
+            const float4* rec = wide + 4 * node;
+            const float4 a0 = __ldg(rec + 0), a1 = __ldg(rec + 1), b0 = __ldg(rec + 2), b1 = __ldg(rec + 3);
+            bool stop = false;
+            uint2 hit[2];
+            uint32_t nhit = 0;
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const float4 cmn = side ? b0 : a0, cmx = side ? b1 : a1;
+                if (!stop && __float_as_uint(cmx.w) > t && overlap(cmn, cmx, cull)) {
+                    const uint32_t code = __float_as_uint(cmn.w);
+                    if (code & 0x80000000u) {
+                        const uint32_t e = code & 0x7FFFFFFFu;
+                        if (q < e) {
+                            if (overlap(cmn, cmx, box)) hit[nhit++] = make_uint2(q, e);
+                        } else {
+                            const float qe[6] = {cmn.x - r, cmn.y - r, cmn.z - r, cmx.x + r, cmx.y + r, cmx.z + r};
+                            if (overlap(own_mn, own_mx, qe)) hit[nhit++] = make_uint2(e, q);
+                        }
+                    } else if (sp < 32) {
+                        stack[sp++] = code;
+                    } else {
+                        stop = true;
+                    }
+                }
+            }
+            const uint32_t active = __activemask();
+            const uint32_t lt = (1u << lane_id()) - 1u;
+            const uint32_t one = __ballot_sync(active, nhit >= 1), two = __ballot_sync(active, nhit == 2);
+            const uint32_t total = __popc(one) + __popc(two);
+            const uint32_t leader = __ffs(active) - 1;
+            uint32_t base = 0;
+            if (lane_id() == leader && total) base = atomicAdd(d_count, total);
+            base = __shfl_sync(active, base, leader) + __popc(one & lt) + __popc(two & lt);
+            for (uint32_t k = 0; k < nhit; ++k)
+                if (base + k < capacity) pairs[base + k] = hit[k];
+            if (stop || ++loop > 100000u) {
+                if (capped) atomicOr(capped, 1u);
                 break;
             }
         }
@@ -642,6 +722,29 @@ int lcs_bvh_query_ee_capped(const lcs_bvh* t, const float* x0, const float* x1, 
         t->wide, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
         reinterpret_cast<const uint2*>(edges), n_edges, d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity,
         d_count, n_edges == t->n ? t->sgo : nullptr, capped);
+    lcs_count_launch();
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+extern "C" int lcs_bvh_query_ee_sym(const lcs_bvh* t, const float* x0, const float* x1, const uint32_t* edges,
+                                    float d_hat, uint32_t* pairs, uint32_t capacity, uint32_t* d_count,
+                                    lcs_stream stream)
+{
+    return lcs_bvh_query_ee_sym_capped(t, x0, x1, edges, d_hat, pairs, capacity, d_count, nullptr, stream);
+}
+
+int lcs_bvh_query_ee_sym_capped(const lcs_bvh* t, const float* x0, const float* x1, const uint32_t* edges,
+                                float d_hat, uint32_t* pairs, uint32_t capacity, uint32_t* d_count, uint32_t* capped,
+                                lcs_stream stream)
+{
+    if (!t || t->kind != LCS_TREE_EDGE || !x0 || !x1 || !edges || !d_count || (capacity && !pairs) ||
+        !(d_hat >= 0.0f))
+        return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_ee_sym: bad argument (needs an edge tree, d_hat >= 0)");
+    if (t->n == 0) return LCS_OK;
+    k_query_ee_sym<<<grid_for(t->n, 128, 16), 128, 0, (cudaStream_t)stream>>>(
+        t->wide, t->sgo, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
+        reinterpret_cast<const uint2*>(edges), d_hat, reinterpret_cast<uint2*>(pairs), capacity, d_count, capped);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;

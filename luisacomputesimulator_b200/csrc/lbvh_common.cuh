@@ -78,11 +78,13 @@ __device__ __forceinline__ void leaf_box(int kind, uint32_t e, const float* __re
     mx = mk3(mx.x + th, mx.y + th, mx.z + th);
 }
 
-__device__ __forceinline__ void store_slot(float4* wide, uint32_t s, v3 mn, v3 mx, uint32_t code)
+// slot s of the node records: {min.xyz | code}{max.xyz | last}, `last` being the largest sorted leaf
+// position under the slot (the pruning key of the once-per-pair EE traversal)
+__device__ __forceinline__ void store_slot(float4* wide, uint32_t s, v3 mn, v3 mx, uint32_t code, uint32_t last = 0u)
 {
     float4* r = wide + 4 * (s >> 1) + 2 * (s & 1u);
     __stcg(r, make_float4(mn.x, mn.y, mn.z, __uint_as_float(code)));
-    __stcg(r + 1, make_float4(mx.x, mx.y, mx.z, 0.0f));
+    __stcg(r + 1, make_float4(mx.x, mx.y, mx.z, __uint_as_float(last)));
 }
 
 // the strict overlap test of AABB::is_overlap_aabb (aabb.h:95-100); q = {min xyz, max xyz}

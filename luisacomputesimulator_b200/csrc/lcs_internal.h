@@ -43,6 +43,9 @@ int lcs_bvh_query_vf_capped(const lcs_bvh* t, const float* x0, const float* x1, 
 int lcs_bvh_query_ee_capped(const lcs_bvh* t, const float* x0, const float* x1, const uint32_t* edges, uint32_t n_edges,
                             const float* d_hat, const float* thickness, uint32_t* pairs, uint32_t capacity,
                             uint32_t* d_count, uint32_t* capped, lcs_stream stream);
+int lcs_bvh_query_ee_sym_capped(const lcs_bvh* t, const float* x0, const float* x1, const uint32_t* edges,
+                                float d_hat, uint32_t* pairs, uint32_t capacity, uint32_t* d_count, uint32_t* capped,
+                                lcs_stream stream);
 int lcs_forest_query_vf_capped(const lcs_forest* f, const float* x0, const float* x1, uint32_t n_verts,
                                const uint32_t* vert_scene, const float* d_hat, const float* thickness, uint32_t* pairs,
                                uint32_t capacity, uint32_t* d_count, uint32_t* capped, lcs_stream stream);

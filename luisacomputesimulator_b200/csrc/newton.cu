@@ -1014,6 +1014,8 @@ struct lcs_newton {
     uint32_t* prev_ccd = nullptr;  // device: the CCD candidate counts of the previous iteration
     bool filter_ok = false;
     bool full_traversal = false;   // LCS_NEWTON_FULL_TRAVERSAL
+    bool ee_sym = false;           // every edge's first vertex: thickness 0, the same d_hat (ee_dhat)
+    float ee_dhat = 0.0f;
     bool energy_ls = false;        // LCS_NEWTON_ENERGY_LINESEARCH
     bool global_matrix = false;    // LCS_NEWTON_PCG_GLOBAL_MATRIX
     double *ls_E = nullptr, *h_ls_E = nullptr;  // energies of one line-search round (device, pinned host)
@@ -1301,6 +1303,15 @@ int copy_x_to_host(lcs_newton* h, const float4* src)
 }
 
 // refit + queries of both trees; lists into out_vf / out_ee; *capped |= 1 when a traversal ended early
+// EE candidates of the edge tree (fused mode: the once-per-pair traversal where it applies)
+int query_ee(lcs_newton* h, const float* X0, const float* X1, const uint32_t* ED, uint32_t* PE, uint32_t* cnt_ee,
+             uint32_t* capped, cudaStream_t s)
+{
+    if (h->ee_sym && !h->plain && !h->full_traversal)
+        return lcs_bvh_query_ee_sym_capped(h->edge_tree, X0, X1, ED, h->ee_dhat, PE, h->cap_ee, cnt_ee, capped, s);
+    return lcs_bvh_query_ee_capped(h->edge_tree, X0, X1, ED, h->E, h->dhat, h->offset, PE, h->cap_ee, cnt_ee, capped, s);
+}
+
 int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint2* out_vf, uint2* out_ee, uint32_t* cnt_vf,
                 uint32_t* cnt_ee, uint32_t* capped)
 {
@@ -1332,9 +1343,7 @@ int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint2* out_vf
         LCS_CUDA_TRY(cudaEventRecord(h->fork, h->s));
         LCS_CUDA_TRY(cudaStreamWaitEvent(h->s2, h->fork, 0));
         if ((rc = lcs_bvh_update_refit(h->edge_tree, h->offset, X0, X1, ED, h->s2))) return rc;
-        if ((rc = lcs_bvh_query_ee_capped(h->edge_tree, X0, X1, ED, h->E, h->dhat, h->offset, PE, h->cap_ee, cnt_ee,
-                                          capped, h->s2)))
-            return rc;
+        if ((rc = query_ee(h, X0, X1, ED, PE, cnt_ee, capped, h->s2))) return rc;
         if ((rc = lcs_bvh_update_refit(h->face_tree, h->offset, X0, X1, FA, h->s))) return rc;
         if ((rc = lcs_bvh_query_vf_capped(h->face_tree, X0, X1, h->V, h->dhat, h->offset, PV, h->cap_vf, cnt_vf, capped,
                                           h->s)))
@@ -1357,8 +1366,7 @@ int broad_phase(lcs_newton* h, const float4* x0, const float4* x1, uint2* out_vf
     } else if ((rc = lcs_bvh_update_refit(h->edge_tree, h->offset, X0, X1, ED, h->s))) {
         return rc;
     }
-    return lcs_bvh_query_ee_capped(h->edge_tree, X0, X1, ED, h->E, h->dhat, h->offset, PE, h->cap_ee, cnt_ee, capped,
-                                   h->s);
+    return query_ee(h, X0, X1, ED, PE, cnt_ee, capped, h->s);
 }
 
 // DCD candidates of iterate x from the previous iteration's CCD lists (swept from x_iter to x_iter + dx,
@@ -1870,6 +1878,17 @@ int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batc
     A(upload(h->mass, d->mass, V));
     A(upload(h->dhat, d->d_hat, V));
     A(upload(h->offset, d->offset, V));
+    // the once-per-pair EE traversal applies when the EE queries' boxes are symmetric
+    if (h->E > 0) {
+        const float D = d->d_hat[d->edges[0]];
+        bool sym = D >= 0.0f;
+        for (uint32_t e = 0; e < h->E && sym; ++e) {
+            const uint32_t v0 = d->edges[2 * e];
+            sym = d->offset[v0] == 0.0f && d->d_hat[v0] == D;
+        }
+        h->ee_sym = sym;
+        h->ee_dhat = D;
+    }
     {
         std::vector<uint32_t> body(V, kInvalid);
         if (d->body) std::memcpy(body.data(), d->body, 4 * V);

@@ -185,3 +185,61 @@ def test_filtered_swept_lists_equal_static_queries_on_the_sweep(scene):
         n = int(counts(ocnt)[0])
         assert n == n_want and n <= int(counts(cnt)[0])
         np.testing.assert_array_equal(SC.sorted_pairs(host(out, np.uint32)[:n]), SC.sorted_pairs(want))
+
+
+@pytest.mark.parametrize("scene", ["cloth_sphere", "folded", "tube"])
+@pytest.mark.parametrize("swept", [False, True])
+def test_once_per_pair_ee_query_matches_the_reference_set(scene, swept):
+    """lcs_bvh_query_ee_sym (each pair met once, from the lower Morton position) returns the oracle's
+    EE set bit for bit on scenes with thickness 0 and one d_hat -- the Newton loop's configuration."""
+    sc, x = _scene(scene)
+    sc.offset = np.zeros_like(sc.offset)
+    sc.d_hat = np.full_like(sc.d_hat, sc.d_hat[sc.edges[0, 0]])
+    x1 = SC.random_motion(x, 2e-3, seed=13) if swept else x
+    D = SceneOnDevice(sc)
+    xd, x1d = dev(x), dev(x1)
+    t_o, bvh, _, ed = _build_both(sc, x, "edge")
+    O.lbvh_refit(t_o, x, x1, sc.edges, sc.offset)
+    bvh.update_and_refit(D.offset, xd, x1d, ed)
+    want, n_want = O.lbvh_query_ee(t_o, x, x1, sc.edges, sc.d_hat, sc.offset)
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    pairs = torch.zeros((n_want + 64, 2), dtype=torch.int32, device="cuda")
+    bvh.broad_phase_query_from_edges_sym(xd, x1d, D.edges, cnt, pairs, float(sc.d_hat[0]))
+    n = int(counts(cnt)[0])
+    assert n == n_want
+    np.testing.assert_array_equal(SC.sorted_pairs(host(pairs, np.uint32)[:n]), SC.sorted_pairs(want))
+
+
+def test_once_per_pair_ee_query_on_boxes_at_the_threshold():
+    """A grid whose edge boxes sit at distance d_hat from each other on every axis (spacing = edge length
+    + d_hat, scaled so the sums round): the strict test decides at the last ulp, from either side."""
+    rng = np.random.default_rng(5)
+    n = 40
+    d = np.float32(1e-3)
+    seg = []
+    for i in range(n):
+        for j in range(n):
+            p = np.array([i * 3e-3, j * 3e-3, 0.0], np.float32)
+            seg.append((p, p + np.array([2e-3, 0, 0], np.float32)))
+            seg.append((p + np.array([0, 1e-3, 0], np.float32),
+                        p + np.array([0, 1e-3, 0], np.float32) + np.float32(1e-3) * rng.normal(size=3).astype(np.float32)))
+    x = np.zeros((2 * len(seg), 4), np.float32)
+    for k, (a, b) in enumerate(seg):
+        x[2 * k, :3], x[2 * k + 1, :3] = a, b
+    edges = np.arange(2 * len(seg), dtype=np.uint32).reshape(-1, 2)
+    V = x.shape[0]
+    dh, off = np.full(V, d, np.float32), np.zeros(V, np.float32)
+    t_o = O.lbvh_build(O.TREE_EDGE, x, edges, V)
+    O.lbvh_refit(t_o, x, x, edges, off)
+    want, n_want = O.lbvh_query_ee(t_o, x, x, edges, dh, off)
+    bvh = LBVH(O.TREE_EDGE, edges.shape[0])
+    xd, ed = dev(x), dev(edges)
+    bvh.reduce_edge_tree_aabb(xd, ed)
+    bvh.construct_tree()
+    bvh.update_and_refit(dev(off), xd, xd, ed)
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    pairs = torch.zeros((n_want + 64, 2), dtype=torch.int32, device="cuda")
+    bvh.broad_phase_query_from_edges_sym(xd, xd, ed, cnt, pairs, float(d))
+    m = int(counts(cnt)[0])
+    assert m == n_want and n_want > 0
+    np.testing.assert_array_equal(SC.sorted_pairs(host(pairs, np.uint32)[:m]), SC.sorted_pairs(want))
