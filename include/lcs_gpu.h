@@ -556,8 +556,13 @@ LCS_API int lcs_newton_download(const lcs_newton* h, float* x_out, float* v_out)
  * SolverInterface::load_saved_state_from_host (solver_interface.cpp:275-412) does before the next frame.
  * Synchronises the solver's stream. */
 LCS_API int lcs_newton_upload(lcs_newton* h, const float* x_in, const float* v_in);
-/* Device pointers of the solver's positions and velocities (float4 per vertex). */
+/* Device pointers of the solver's positions and velocities (float4 per vertex).  Positions written
+ * through this pointer must be announced with lcs_newton_invalidate(h), so that the next step does not
+ * reuse candidate lists of the old positions. */
 LCS_API int lcs_newton_state(const lcs_newton* h, float** d_x, float** d_v);
+/* The positions changed outside the solver (through lcs_newton_state): the next step traverses the
+ * trees for its first DCD lists instead of filtering the previous step's CCD lists. */
+LCS_API int lcs_newton_invalidate(lcs_newton* h);
 /* Accumulated per-phase GPU time (LCS_NEWTON_PROFILE): build, material, DCD broad, DCD narrow,
  * assembly, PCG, CCD broad, CCD narrow, apply -- and how many times each ran. */
 LCS_API int lcs_newton_profile(const lcs_newton* h, double* phase_ms, int32_t* launches, int n);

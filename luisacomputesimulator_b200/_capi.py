@@ -150,6 +150,7 @@ SIGNATURES = {
     "lcs_newton_state": (I32, [P, C.POINTER(P), C.POINTER(P)]),
     "lcs_newton_download": (I32, [P, P, P]),
     "lcs_newton_upload": (I32, [P, P, P]),
+    "lcs_newton_invalidate": (I32, [P]),
     "lcs_newton_profile": (I32, [P, C.POINTER(C.c_double), C.POINTER(C.c_int32), I32]),
     "lcs_newton_reset_profile": (I32, [P]),
     "lcs_newton_pcg_kind": (I32, [P]),

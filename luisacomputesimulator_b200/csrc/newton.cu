@@ -1013,6 +1013,7 @@ struct lcs_newton {
     uint2 *dcd_vf = nullptr, *dcd_ee = nullptr;
     uint32_t* prev_ccd = nullptr;  // device: the CCD candidate counts of the previous iteration
     bool filter_ok = false;
+    bool carry_filter = false;     // the last CCD lists of the previous step describe the current positions
     bool full_traversal = false;   // LCS_NEWTON_FULL_TRAVERSAL
     bool ee_sym = false;           // every edge's first vertex: thickness 0, the same d_hat (ee_dhat)
     float ee_dhat = 0.0f;
@@ -1728,7 +1729,9 @@ int newton_iteration(lcs_newton* h)
             }
         }
         // the next iteration may filter these CCD lists if no traversal ended early
-        h->filter_ok = !h->plain && h->h_st->cnt[5] == 0u;
+        // (not with affine bodies: their vertices are placed by p + A x_bar of the stepped q, which may round
+        // outside the swept box of x_iter + t dx by an ulp)
+        h->filter_ok = !h->plain && !h->NB && h->h_st->cnt[5] == 0u;
         if (grow(h)) {  // an overflow anywhere: undo the step and run the iteration again
             k_copy4<<<grid256(V), 256, 0, h->s>>>(V, h->x_iter, h->x);
             lcs_count_launch();
@@ -2218,7 +2221,12 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
     int rc;
     const auto t_host0 = std::chrono::steady_clock::now();
     h->retries = 0;
-    h->filter_ok = false;  // the trees are rebuilt below: no list of this step's trees yet
+    // the positions at the start of this step are the last iterate of the previous one, x_iter + t dx with
+    // 0 <= t <= 1, inside that iteration's swept boxes: its CCD lists (element pairs, independent of the
+    // trees rebuilt below) filter to this iteration's DCD lists as within a step.  Not across a batch
+    // (finished scenes drop out of the last iterations' lists) or after the state was replaced.
+    h->filter_ok = h->carry_filter && !h->batch;
+    h->carry_filter = false;
     h->time += d.dt;
     if (h->plain) {  // physics_step_GPU uploads x_step_start, x and v from the host every step
         const size_t bytes = 16 * (size_t)V;
@@ -2326,6 +2334,7 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
         global_converged = s.max_dx < 1e-2f * d.dt;
         dirichlet_converged = s.dirichlet < 1e-3f;
     }
+    h->carry_filter = h->filter_ok && !h->full_traversal;
     k_update_velocity<<<grid256(V), 256, 0, h->s>>>(V, d.dt, d.damping, h->x, h->x_step, h->v);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
@@ -2363,6 +2372,7 @@ extern "C" int lcs_newton_step_host(lcs_newton* h, const float* x_in, const floa
 {
     if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_step_host: null handle");
     const size_t bytes = 16 * (size_t)h->V;
+    if (x_in) h->carry_filter = false;  // new positions: no CCD list describes them
     if (x_in) LCS_CUDA_TRY(cudaMemcpyAsync(h->x, x_in, bytes, cudaMemcpyHostToDevice, h->s));
     if (v_in) LCS_CUDA_TRY(cudaMemcpyAsync(h->v, v_in, bytes, cudaMemcpyHostToDevice, h->s));
     if (h->plain) {
@@ -2393,6 +2403,7 @@ extern "C" int lcs_newton_upload(lcs_newton* h, const float* x_in, const float* 
 {
     if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_upload: null handle");
     const size_t bytes = 16 * (size_t)h->V;
+    if (x_in) h->carry_filter = false;
     if (x_in) LCS_CUDA_TRY(cudaMemcpyAsync(h->x, x_in, bytes, cudaMemcpyHostToDevice, h->s));
     if (v_in) LCS_CUDA_TRY(cudaMemcpyAsync(h->v, v_in, bytes, cudaMemcpyHostToDevice, h->s));
     if (h->plain) {
@@ -2400,6 +2411,13 @@ extern "C" int lcs_newton_upload(lcs_newton* h, const float* x_in, const float* 
         if (v_in) std::memcpy(h->h_v, v_in, bytes);
     }
     LCS_CUDA_TRY(cudaStreamSynchronize(h->s));
+    return LCS_OK;
+}
+
+extern "C" int lcs_newton_invalidate(lcs_newton* h)
+{
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_invalidate: null handle");
+    h->carry_filter = false;
     return LCS_OK;
 }
 

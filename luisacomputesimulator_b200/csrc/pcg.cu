@@ -1153,10 +1153,7 @@ __device__ __forceinline__ bool res_publish_wait(unsigned* flags, unsigned tag, 
 {
     __syncthreads();
     const uint32_t t = threadIdx.x;
-    if (t == 0) {
-        __threadfence();
-        st_release(flags + kResFlagStride * blockIdx.x, tag);
-    }
+    if (t == 0) st_release(flags + kResFlagStride * blockIdx.x, tag);  // releases the block's u, ordered by the barrier
     if (t < gridDim.x && ((dep[t >> 5] >> (t & 31u)) & 1u)) {
         const unsigned* f = flags + kResFlagStride * t;
         unsigned it = 0;

@@ -142,6 +142,10 @@ class NewtonSolver:
                 "lcs_newton_step_host")
         return self.stats
 
+    def invalidate(self):
+        """Announce positions written through state_ptrs() (the next step re-traverses for its DCD lists)."""
+        A.check(self.lib.lcs_newton_invalidate(self.h), "lcs_newton_invalidate")
+
     def state_ptrs(self):
         x, v = C.c_void_p(), C.c_void_p()
         A.check(self.lib.lcs_newton_state(self.h, C.byref(x), C.byref(v)), "lcs_newton_state")

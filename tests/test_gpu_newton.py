@@ -108,3 +108,32 @@ def test_slice_resident_pcg_matches_the_global_form_on_the_tube():
     assert na == nb and abs(ia - ib) <= 2 * na
     scale = np.abs(xb[:, :3] - x[:, :3]).max()
     np.testing.assert_allclose(xa[:, :3], xb[:, :3], rtol=0, atol=1e-3 * scale + 1e-7)
+
+
+def test_first_iteration_dcd_lists_filtered_across_steps_equal_a_traversal():
+    """From the second step on, the first Newton iteration's DCD lists are the previous step's last CCD lists
+    filtered at the step-start positions.  With one Newton iteration per step, every step's reported DCD
+    candidate and pair counts are those of its first iteration: they must equal the oracle's static query and
+    barrier pairs at the positions the step started from."""
+    sc, x = SC.folded_cloth(n=32, gap=4e-4)
+    gpu = NewtonSolver(sc, single_reduction=True, nonlinear_iters=1)
+    st = gpu.step_host(x_in=x)
+    checked = 0
+    for _ in range(8):
+        x0 = gpu.positions()
+        st = gpu.step()
+        assert st.status == 0
+        if st.newton_iters != 1:
+            continue
+        tf = O.lbvh_build(O.TREE_FACE, x0, sc.faces, sc.num_verts)
+        te = O.lbvh_build(O.TREE_EDGE, x0, sc.edges, sc.num_verts)
+        O.lbvh_refit(tf, x0, x0, sc.faces, sc.offset)
+        O.lbvh_refit(te, x0, x0, sc.edges, sc.offset)
+        vf, n_vf = O.lbvh_query_vf(tf, x0, x0, sc.d_hat, sc.offset)
+        ee, n_ee = O.lbvh_query_ee(te, x0, x0, sc.edges, sc.d_hat, sc.offset)
+        pairs = len(O.dcd_vf(vf, x0, sc.faces, sc.body, sc.vert_area, sc.face_area, sc.d_hat, sc.offset, sc.kappa)) + \
+            len(O.dcd_ee(ee, x0, sc.edges, sc.body, sc.edge_area, sc.d_hat, sc.offset, sc.kappa))
+        assert (st.vf_candidates, st.ee_candidates) == (n_vf, n_ee)
+        assert st.contact_pairs == pairs
+        checked += 1
+    assert checked >= 4
