@@ -1127,15 +1127,93 @@ constexpr int kResDepWords = kResMaxBlocks / 32;
 
 struct ResArgs {
     RowArgs a;
+    const uint32_t* part;   // P + 1: block c owns slices [part[c], part[c + 1])
+    const uint32_t* owner;  // S: the block owning each slice
     unsigned* flags;     // per block: the last iteration tag whose u the block published
     uint32_t n_slices;
     uint32_t max_slices; // slices of the largest block (shared-memory stride)
     int gres;            // resident groups per slice
 };
 
-__device__ __forceinline__ uint32_t res_owner(uint32_t slice, uint32_t S, uint32_t P)
+// Slices to blocks by cost, before each solve: a slice costs its material groups, its contact groups
+// (when the contact blocks are in SELL form) and kResSliceBase for the diagonal and the vectors; block c
+// takes the slices whose cost prefix reaches c / P of the total, with at most `cap` slices per block and
+// at least one, and every later block still able to take the rest.  One block of 1024 threads: the
+// prefix by block scans, the ideal cuts by one binary search per block, the clamping in one thread.
+constexpr uint32_t kResSliceBase = 2;
+
+__global__ void __launch_bounds__(1024) k_res_partition(uint32_t S, uint32_t P, uint32_t cap, const uint32_t* __restrict__ m_ptr,
+                                                        const uint32_t* __restrict__ c_ptr, const int* __restrict__ c_ok,
+                                                        uint32_t* __restrict__ prefix, uint32_t* __restrict__ part,
+                                                        uint32_t* __restrict__ owner)
 {
-    return (uint32_t)((((uint64_t)slice + 1) * P - 1) / S);
+    __shared__ uint32_t ws[32];
+    __shared__ uint32_t carry;
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    const bool cs = c_ptr && c_ok && *c_ok;
+    if (t == 0) carry = 0u;
+    __syncthreads();
+    // prefix[s] = cost of slices [0, s)
+    for (uint32_t base = 0; base < S; base += 1024u) {
+        const uint32_t sl = base + t;
+        uint32_t v = 0u;
+        if (sl < S) {
+            v = ((m_ptr[sl + 1] - m_ptr[sl]) >> 2) + kResSliceBase;
+            if (cs) v += (c_ptr[sl + 1] - c_ptr[sl]) >> 2;
+        }
+        uint32_t incl = v;
+#pragma unroll
+        for (uint32_t o = 1; o < 32u; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += x;
+        }
+        if (lane == 31u) ws[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = ws[lane];
+#pragma unroll
+            for (uint32_t o = 1; o < 32u; o <<= 1) {
+                const uint32_t x = __shfl_up_sync(0xFFFFFFFFu, w, o);
+                if (lane >= o) w += x;
+            }
+            ws[lane] = w;
+        }
+        __syncthreads();
+        if (sl < S) prefix[sl] = carry + (warp ? ws[warp - 1] : 0u) + incl - v;
+        __syncthreads();
+        if (t == 0) carry += ws[31];
+        __syncthreads();
+    }
+    if (t == 0) prefix[S] = carry;
+    __syncthreads();
+    const uint64_t total = carry;
+    // ideal cut of block c: the first slice whose prefix reaches c / P of the total
+    for (uint32_t c = t; c <= P; c += 1024u) {
+        const uint64_t target = total * c / P;
+        uint32_t lo = 0, hi = S;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if ((uint64_t)prefix[mid] < target) lo = mid + 1;
+            else hi = mid;
+        }
+        part[c] = lo;
+    }
+    __syncthreads();
+    if (t == 0) {
+        uint32_t prev = 0u;
+        part[0] = 0u;
+        for (uint32_t c = 1; c < P; ++c) {
+            const uint32_t lo = max(prev + 1u, S > cap * (P - c) ? S - cap * (P - c) : 0u);
+            const uint32_t hi = min(prev + cap, S - (P - c));
+            const uint32_t b = min(max(part[c], lo), hi);
+            part[c] = b;
+            prev = b;
+        }
+        part[P] = S;
+    }
+    __syncthreads();
+    for (uint32_t c = warp; c < P; c += 32u)
+        for (uint32_t sl = part[c] + lane; sl < part[c + 1]; sl += 32u) owner[sl] = c;
 }
 
 __device__ __forceinline__ void st_release(unsigned* p, unsigned v)
@@ -1177,7 +1255,7 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
     __shared__ int s_fail;
     __shared__ unsigned s_dep[kResDepWords];
     const uint32_t P = gridDim.x, S = ra.n_slices, c = blockIdx.x;
-    const uint32_t s_lo = (uint32_t)(((uint64_t)c * S) / P), s_hi = (uint32_t)(((uint64_t)(c + 1) * S) / P);
+    const uint32_t s_lo = __ldcg(&ra.part[c]), s_hi = __ldcg(&ra.part[c + 1]);
     const uint32_t nsl = s_hi - s_lo, row0 = 32u * s_lo;
     const uint32_t nloc = min(32u * s_hi, a.n) - row0;
     const int G = ra.gres;
@@ -1215,7 +1293,7 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
     {
         unsigned near = 0u;
         auto note = [&](uint32_t col) {
-            const uint32_t oc = res_owner(col >> 5, S, P);
+            const uint32_t oc = __ldcg(&ra.owner[col >> 5]);
             if (oc == c) return;
             const int d = (int)oc - (int)c + 16;
             if (d >= 0 && d < 32) near |= 1u << d;
@@ -1601,6 +1679,7 @@ struct lcs_pcg {
     unsigned* flags = nullptr;   // slice-resident solve: per-block publication tags (kResMaxBlocks)
     int res_gres = -2;           // slice-resident solve: resident groups per slice (-2: not set up)
     uint32_t res_blocks = 0, res_slices = 0, res_max_slices = 0;
+    uint32_t *res_prefix = nullptr, *res_part = nullptr, *res_owner = nullptr;  // slice partition (per solve)
     size_t res_smem = 0;
     lcs_pcg_stats* d_stats = nullptr;
     int fused_grid = 0;
@@ -1661,7 +1740,7 @@ extern "C" int lcs_pcg_destroy(lcs_pcg* p)
 {
     if (!p) return LCS_OK;
     void* ptrs[] = {p->r, p->z, p->p, p->q, p->minv, p->part, p->part_f, p->scal, p->bar, p->flags, p->d_stats,
-                    p->cpart, p->class_scenes};
+                    p->cpart, p->class_scenes, p->res_prefix, p->res_part, p->res_owner};
     for (int k = 0; k < 5; ++k) {
         if (p->class_stream[k]) {
             cudaStreamSynchronize(p->class_stream[k]);
@@ -1764,8 +1843,9 @@ static int res_setup(lcs_pcg* P)
     if (blocks > (uint32_t)kResMaxBlocks) blocks = kResMaxBlocks;
     if (blocks > (uint32_t)kResThreads) blocks = kResThreads;  // one waiting thread per block
     if (blocks == 0) return LCS_ERR_CAPACITY;
-    const uint32_t max_slices = (S + blocks - 1) / blocks;
-    if (max_slices > (uint32_t)(kResThreads / 32)) return LCS_ERR_CAPACITY;
+    if ((S + blocks - 1) / blocks > (uint32_t)(kResThreads / 32)) return LCS_ERR_CAPACITY;
+    // room for a full block of slices, so that the per-solve partition can balance cost
+    const uint32_t max_slices = S < (uint32_t)(kResThreads / 32) ? S : (uint32_t)(kResThreads / 32);
     cudaFuncAttributes fa;
     if (cudaFuncGetAttributes(&fa, k_pcg_res<kResThreads>) != cudaSuccess) return LCS_ERR_CAPACITY;
     const size_t base = 16 * (size_t)kResThreads + 32 * (size_t)blocks;
@@ -1781,6 +1861,12 @@ static int res_setup(lcs_pcg* P)
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_res<kResThreads>, kResThreads, dyn);
     if (per_sm < 1 || (int64_t)per_sm * sms < (int64_t)blocks) return LCS_ERR_CAPACITY;
+    if (cudaMalloc((void**)&P->res_prefix, sizeof(uint32_t) * (S + 1)) != cudaSuccess ||
+        cudaMalloc((void**)&P->res_part, sizeof(uint32_t) * (blocks + 1)) != cudaSuccess ||
+        cudaMalloc((void**)&P->res_owner, sizeof(uint32_t) * S) != cudaSuccess) {
+        cudaGetLastError();
+        return LCS_ERR_CAPACITY;
+    }
     P->res_blocks = blocks;
     P->res_slices = S;
     P->res_max_slices = max_slices;
@@ -1928,7 +2014,10 @@ static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* 
     void* args[] = {&a};
     const int grid = (int)((P->n + kRowThreads - 1) / kRowThreads);
     if (pipe && sell && !(o.flags & kPcgNoResident) && res_setup(P) == LCS_OK) {
-        ResArgs ra{a, P->flags, P->res_slices, P->res_max_slices, P->res_gres};
+        k_res_partition<<<1, 1024, 0, s>>>(P->res_slices, P->res_blocks, P->res_max_slices, m_ptr, a.c_ptr, a.c_ok,
+                                           P->res_prefix, P->res_part, P->res_owner);
+        lcs_count_launch();
+        ResArgs ra{a, P->res_part, P->res_owner, P->flags, P->res_slices, P->res_max_slices, P->res_gres};
         void* rargs[] = {&ra};
         LCS_CUDA_TRY(cudaMemsetAsync(P->flags, 0, sizeof(unsigned) * kResFlagStride * P->res_blocks, s));
         LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_res<kResThreads>, dim3(P->res_blocks),
