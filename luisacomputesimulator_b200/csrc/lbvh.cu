@@ -39,6 +39,8 @@ struct lcs_bvh {
     uint2* children = nullptr;       // 2n - 1, reference layout
     uint32_t* slot = nullptr;        // 2n - 1, 2 * parent + side
     float4* wide = nullptr;          // 4 * max(ni, 1)
+    float4* wide4 = nullptr;         // 8 * max(ni, 1): 4-child records of the even-depth inner nodes
+    uint8_t* even = nullptr;         // max(ni, 1): inner node at even depth (root: depth 0)
     uint32_t* counters = nullptr;    // max(ni, 1), refit arrival counters (self-resetting)
     uint32_t* healthy = nullptr;     // 1
 };
@@ -197,6 +199,75 @@ __global__ void k_build_inner(const uint64_t* __restrict__ ms, const uint32_t* _
     }
 }
 
+// 4-wide traversal records.  The binary tree stays the reference's (topology, refit and export are
+// bit-exact against it); after each refit every inner node b at even depth gets a record of its four
+// grandchild slots (a leaf child keeps its own slot): {min.xyz | code}{max.xyz | last} x 4, 128 B, empty
+// slots as inverted boxes that no strict overlap test passes.  A traversal then takes one dependent
+// 128-B fetch where the binary walk took two 64-B ones.  k_depth_parity marks the even-depth inner nodes
+// after each build (a climb to the root per node, at most 256 levels).
+__global__ void k_depth_parity(const uint32_t* __restrict__ parent, uint32_t ni, uint8_t* __restrict__ even)
+{
+    for (uint32_t nid = blockIdx.x * blockDim.x + threadIdx.x; nid < ni; nid += gridDim.x * blockDim.x) {
+        uint32_t p = nid, d = 0;
+        while (p != 0u && p < ni && d < 256u) {
+            p = parent[p];
+            ++d;
+        }
+        even[nid] = (d & 1u) == 0u ? 1 : 0;
+    }
+}
+
+__global__ void k_collapse4(const float4* __restrict__ wide, const uint8_t* __restrict__ even, uint32_t ni,
+                            float4* __restrict__ wide4)
+{
+    const uint32_t nodes = ni ? ni : 1u;
+    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nodes; b += gridDim.x * blockDim.x) {
+        if (ni && !even[b]) continue;
+        float4 out[8];
+        int k = 0;
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const float4 mn = __ldcg(wide + 4 * b + 2 * side), mx = __ldcg(wide + 4 * b + 2 * side + 1);
+            const uint32_t code = __float_as_uint(mn.w);
+            if (ni == 0u || (code & 0x80000000u)) {
+                out[k++] = mn;
+                out[k++] = mx;
+            } else {
+                const float4* c = wide + 4 * code;
+                out[k++] = __ldcg(c);
+                out[k++] = __ldcg(c + 1);
+                out[k++] = __ldcg(c + 2);
+                out[k++] = __ldcg(c + 3);
+            }
+        }
+        const float inf = __int_as_float(0x7f800000);
+        for (; k < 8; k += 2) {
+            out[k] = make_float4(inf, inf, inf, __uint_as_float(0x80000000u));
+            out[k + 1] = make_float4(-inf, -inf, -inf, __uint_as_float(0u));
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) __stcg(wide4 + 8 * b + j, out[j]);
+    }
+}
+
+// pairs of this traversal step (up to 4 per thread) appended with one atomic per warp: the counts' bits
+// are balloted, so every lane's offset is a sum of popcounts
+__device__ __forceinline__ void emit_pairs(const uint2* hit, uint32_t nhit, uint2* pairs, uint32_t capacity,
+                                           uint32_t* d_count)
+{
+    const uint32_t active = __activemask();
+    const uint32_t lt = (1u << lane_id()) - 1u;
+    const uint32_t b0 = __ballot_sync(active, nhit & 1u), b1 = __ballot_sync(active, nhit & 2u),
+                   b2 = __ballot_sync(active, nhit & 4u);
+    const uint32_t total = __popc(b0) + 2u * __popc(b1) + 4u * __popc(b2);
+    const uint32_t leader = __ffs(active) - 1;
+    uint32_t base = 0;
+    if (lane_id() == leader && total) base = atomicAdd(d_count, total);
+    base = __shfl_sync(active, base, leader) + __popc(b0 & lt) + 2u * __popc(b1 & lt) + 4u * __popc(b2 & lt);
+    for (uint32_t k = 0; k < nhit; ++k)
+        if (base + k < capacity) pairs[base + k] = hit[k];
+}
+
 // fn_check_construction, lbvh.cpp:598-611
 __global__ void k_check(const uint2* __restrict__ children, const uint32_t* __restrict__ parent, uint32_t ni,
                         uint32_t* __restrict__ healthy)
@@ -261,8 +332,10 @@ __global__ void k_leaves_refit(int kind, uint32_t n, const uint32_t* __restrict_
 
 // query_template2 (lbvh.cpp:293-360) for fn_query_from_verts_v2 (EE = false, lbvh.cpp:776-808)
 // and fn_query_from_edges_v2 (EE = true, lbvh.cpp:810-846)
+constexpr int kStack4 = 64;  // entries of the 4-wide traversal stack
+
 template <bool EE>
-__global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide, uint32_t n_leaves,
+__global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide4, uint32_t n_leaves,
                                                const float4* __restrict__ x0, const float4* __restrict__ x1,
                                                const uint2* __restrict__ edges, uint32_t n_queries,
                                                const float* __restrict__ dhat, const float* __restrict__ thickness,
@@ -298,43 +371,35 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide, 
                 box[3] = box[4] = box[5] = __int_as_float(0xff800000);
             }
         }
-        uint32_t stack[32];
+        uint32_t stack[kStack4];
         int sp = 0;
         uint32_t loop = 0;
         stack[sp++] = 0;
         while (sp > 0) {
             const uint32_t node = stack[--sp];
-            const float4* r = wide + 4 * node;
-            const float4 a0 = __ldg(r + 0), a1 = __ldg(r + 1), b0 = __ldg(r + 2), b1 = __ldg(r + 3);
+            const float4* r = wide4 + 8 * node;
+            float4 rec[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) rec[j] = __ldg(r + j);
             bool stop = false;
-            uint32_t hit[2];
+            uint2 hit[4];
             uint32_t nhit = 0;
 #pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                const float4 mn = side ? b0 : a0, mx = side ? b1 : a1;
+            for (int k = 0; k < 4; ++k) {
+                const float4 mn = rec[2 * k], mx = rec[2 * k + 1];
                 if (!stop && overlap(mn, mx, box)) {
                     const uint32_t code = __float_as_uint(mn.w);
                     if (code & 0x80000000u) {
                         const uint32_t obj = code & 0x7FFFFFFFu;
-                        if (!EE || q < obj) hit[nhit++] = obj;
-                    } else if (sp < 32) {
+                        if (!EE || q < obj) hit[nhit++] = make_uint2(q, obj);
+                    } else if (sp < kStack4) {
                         stack[sp++] = code;
                     } else {
                         stop = true;  // a full stack ends the whole traversal (lbvh.cpp:344-351)
                     }
                 }
             }
-            // one warp-aggregated reservation for the (up to two) pairs of this step
-            const uint32_t active = __activemask();
-            const uint32_t lt = (1u << lane_id()) - 1u;
-            const uint32_t one = __ballot_sync(active, nhit >= 1), two = __ballot_sync(active, nhit == 2);
-            const uint32_t total = __popc(one) + __popc(two);
-            const uint32_t leader = __ffs(active) - 1;
-            uint32_t base = 0;
-            if (lane_id() == leader && total) base = atomicAdd(d_count, total);
-            base = __shfl_sync(active, base, leader) + __popc(one & lt) + __popc(two & lt);
-            for (uint32_t k = 0; k < nhit; ++k)
-                if (base + k < capacity) pairs[base + k] = make_uint2(q, hit[k]);
+            emit_pairs(hit, nhit, pairs, capacity, d_count);
             if (stop || ++loop > 100000u) {  // the reference's early exits; reported so callers know the
                 if (capped) atomicOr(capped, 1u);  // list may lack pairs a complete traversal would find
                 break;
@@ -352,7 +417,7 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide, 
 // of e (e's leaf box widened by r, exact since its thickness is 0) against the leaf box of q (q's own box).
 // Pairs are written (smaller id, larger id) as the reference writes them.  Leaves of other queries are
 // pruned by position, not by id, so a traversal visits about half the nodes of k_query<true>.
-__global__ void __launch_bounds__(128) k_query_ee_sym(const float4* __restrict__ wide, const uint32_t* __restrict__ sgo,
+__global__ void __launch_bounds__(128) k_query_ee_sym(const float4* __restrict__ wide4, const uint32_t* __restrict__ sgo,
                                                       uint32_t n_leaves, const float4* __restrict__ x0,
                                                       const float4* __restrict__ x1, const uint2* __restrict__ edges,
                                                       float r, uint2* __restrict__ pairs, uint32_t capacity,
@@ -373,20 +438,22 @@ __global__ void __launch_bounds__(128) k_query_ee_sym(const float4* __restrict__
             cull[0] = box[0] - mgx; cull[1] = box[1] - mgy; cull[2] = box[2] - mgz;
             cull[3] = box[3] + mgx; cull[4] = box[4] + mgy; cull[5] = box[5] + mgz;
         }
-        uint32_t stack[32];
+        uint32_t stack[kStack4];
         int sp = 0;
         uint32_t loop = 0;
         stack[sp++] = 0;
         while (sp > 0) {
             const uint32_t node = stack[--sp];
-            const float4* rec = wide + 4 * node;
-            const float4 a0 = __ldg(rec + 0), a1 = __ldg(rec + 1), b0 = __ldg(rec + 2), b1 = __ldg(rec + 3);
+            const float4* node_rec = wide4 + 8 * node;
+            float4 rec[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) rec[j] = __ldg(node_rec + j);
             bool stop = false;
-            uint2 hit[2];
+            uint2 hit[4];
             uint32_t nhit = 0;
 #pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                const float4 cmn = side ? b0 : a0, cmx = side ? b1 : a1;
+            for (int k = 0; k < 4; ++k) {
+                const float4 cmn = rec[2 * k], cmx = rec[2 * k + 1];
                 if (!stop && __float_as_uint(cmx.w) > t && overlap(cmn, cmx, cull)) {
                     const uint32_t code = __float_as_uint(cmn.w);
                     if (code & 0x80000000u) {
@@ -397,23 +464,14 @@ __global__ void __launch_bounds__(128) k_query_ee_sym(const float4* __restrict__
                             const float qe[6] = {cmn.x - r, cmn.y - r, cmn.z - r, cmx.x + r, cmx.y + r, cmx.z + r};
                             if (overlap(own_mn, own_mx, qe)) hit[nhit++] = make_uint2(e, q);
                         }
-                    } else if (sp < 32) {
+                    } else if (sp < kStack4) {
                         stack[sp++] = code;
                     } else {
                         stop = true;
                     }
                 }
             }
-            const uint32_t active = __activemask();
-            const uint32_t lt = (1u << lane_id()) - 1u;
-            const uint32_t one = __ballot_sync(active, nhit >= 1), two = __ballot_sync(active, nhit == 2);
-            const uint32_t total = __popc(one) + __popc(two);
-            const uint32_t leader = __ffs(active) - 1;
-            uint32_t base = 0;
-            if (lane_id() == leader && total) base = atomicAdd(d_count, total);
-            base = __shfl_sync(active, base, leader) + __popc(one & lt) + __popc(two & lt);
-            for (uint32_t k = 0; k < nhit; ++k)
-                if (base + k < capacity) pairs[base + k] = hit[k];
+            emit_pairs(hit, nhit, pairs, capacity, d_count);
             if (stop || ++loop > 100000u) {
                 if (capped) atomicOr(capped, 1u);
                 break;
@@ -536,10 +594,14 @@ extern "C" int lcs_bvh_create(int kind, uint32_t n_leaves, lcs_bvh** out)
     A(alloc(h->children, nn));
     A(alloc(h->slot, nn));
     A(alloc(h->wide, 4 * nw));
+    A(alloc(h->wide4, 8 * nw));
+    A(alloc(h->even, nw));
     A(alloc(h->counters, nw));
     A(alloc(h->healthy, 1));
     if (e == cudaSuccess) e = cudaMemset(h->counters, 0, sizeof(uint32_t) * nw);
     if (e == cudaSuccess) e = cudaMemset(h->wide, 0, sizeof(float4) * 4 * nw);
+    if (e == cudaSuccess) e = cudaMemset(h->wide4, 0, sizeof(float4) * 8 * nw);
+    if (e == cudaSuccess) e = cudaMemset(h->even, 1, nw);
     if (e == cudaSuccess) e = cudaMemset(h->slot, 0xFF, sizeof(uint32_t) * nn);
     if (e != cudaSuccess) {
         lcs_bvh_destroy(h);
@@ -555,7 +617,8 @@ extern "C" int lcs_bvh_destroy(lcs_bvh* h)
 {
     if (!h) return LCS_OK;
     void* ptrs[] = {h->centers, h->block_aabb, h->gaabb, h->m30, h->keys, h->keys_alt, h->vals, h->vals_alt,
-                    h->hist, h->ms64, h->parent, h->children, h->slot, h->wide, h->counters, h->healthy};
+                    h->hist, h->ms64, h->parent, h->children, h->slot, h->wide, h->wide4, h->even, h->counters,
+                    h->healthy};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete h;
@@ -604,6 +667,8 @@ extern "C" int lcs_bvh_construct(lcs_bvh* h, lcs_stream stream)
         lcs_count_launch();
         k_check<<<gi, 256, 0, s>>>(h->children, h->parent, h->ni, h->healthy);
         lcs_count_launch();
+        k_depth_parity<<<gi, 256, 0, s>>>(h->parent, h->ni, h->even);
+        lcs_count_launch();
     } else {
         cudaMemcpyAsync(h->slot, &kInvalid, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
     }
@@ -641,6 +706,8 @@ int lcs_bvh_construct_host_sort(lcs_bvh* h, lcs_stream stream)
         lcs_count_launch();
         k_check<<<gi, 256, 0, s>>>(h->children, h->parent, h->ni, h->healthy);
         lcs_count_launch();
+        k_depth_parity<<<gi, 256, 0, s>>>(h->parent, h->ni, h->even);
+        lcs_count_launch();
     }
     LCS_CUDA_TRY(cudaStreamSynchronize(s));  // host buffers go out of scope
     LCS_LAUNCH_CHECK();
@@ -659,6 +726,10 @@ static int leaves_refit(lcs_bvh* h, const float* thickness, const float* x0, con
                                                        reinterpret_cast<const float4*>(x1), elems, h->wide,
                                                        h->counters, h->healthy, write_leaf, climb);
     lcs_count_launch();
+    if (climb || h->ni == 0) {
+        k_collapse4<<<grid_for(h->ni ? h->ni : 1, 256), 256, 0, s>>>(h->wide, h->even, h->ni, h->wide4);
+        lcs_count_launch();
+    }
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }
@@ -695,7 +766,7 @@ int lcs_bvh_query_vf_capped(const lcs_bvh* t, const float* x0, const float* x1, 
         return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_vf: bad argument (needs a face tree)");
     if (t->n == 0 || n_verts == 0) return LCS_OK;
     k_query<false><<<grid_for(n_verts, 128, 16), 128, 0, (cudaStream_t)stream>>>(
-        t->wide, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1), nullptr, n_verts,
+        t->wide4, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1), nullptr, n_verts,
         d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count, nullptr, capped);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
@@ -719,7 +790,7 @@ int lcs_bvh_query_ee_capped(const lcs_bvh* t, const float* x0, const float* x1, 
         return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_ee: bad argument (needs an edge tree)");
     if (t->n == 0 || n_edges == 0) return LCS_OK;
     k_query<true><<<grid_for(n_edges, 128, 16), 128, 0, (cudaStream_t)stream>>>(
-        t->wide, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
+        t->wide4, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
         reinterpret_cast<const uint2*>(edges), n_edges, d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity,
         d_count, n_edges == t->n ? t->sgo : nullptr, capped);
     lcs_count_launch();
@@ -743,7 +814,7 @@ int lcs_bvh_query_ee_sym_capped(const lcs_bvh* t, const float* x0, const float* 
         return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_ee_sym: bad argument (needs an edge tree, d_hat >= 0)");
     if (t->n == 0) return LCS_OK;
     k_query_ee_sym<<<grid_for(t->n, 128, 16), 128, 0, (cudaStream_t)stream>>>(
-        t->wide, t->sgo, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
+        t->wide4, t->sgo, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
         reinterpret_cast<const uint2*>(edges), d_hat, reinterpret_cast<uint2*>(pairs), capacity, d_count, capped);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();

@@ -1254,7 +1254,7 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
     extern __shared__ __align__(16) unsigned char res_smem[];
     __shared__ int s_fail;
     __shared__ unsigned s_dep[kResDepWords];
-    const uint32_t P = gridDim.x, S = ra.n_slices, c = blockIdx.x;
+    const uint32_t P = gridDim.x, c = blockIdx.x;
     const uint32_t s_lo = __ldcg(&ra.part[c]), s_hi = __ldcg(&ra.part[c + 1]);
     const uint32_t nsl = s_hi - s_lo, row0 = 32u * s_lo;
     const uint32_t nloc = min(32u * s_hi, a.n) - row0;
