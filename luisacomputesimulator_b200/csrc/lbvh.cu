@@ -200,9 +200,10 @@ __global__ void k_build_inner(const uint64_t* __restrict__ ms, const uint32_t* _
 }
 
 // 4-wide traversal records.  The binary tree stays the reference's (topology, refit and export are
-// bit-exact against it); after each refit every inner node b at even depth gets a record of its four
-// grandchild slots (a leaf child keeps its own slot): {min.xyz | code}{max.xyz | last} x 4, 128 B, empty
-// slots as inverted boxes that no strict overlap test passes.  A traversal then takes one dependent
+// bit-exact against it); during each refit every inner node b at even depth gets a record of its four
+// grandchild slots (a leaf child keeps its own slot), written by the thread that completes b in the
+// bottom-up walk: {min.xyz | code}{max.xyz | last} x 4, 128 B, empty slots as inverted boxes that no strict
+// overlap test passes.  A traversal then takes one dependent
 // 128-B fetch where the binary walk took two 64-B ones.  k_depth_parity marks the even-depth inner nodes
 // after each build (a climb to the root per node, at most 256 levels).
 __global__ void k_depth_parity(const uint32_t* __restrict__ parent, uint32_t ni, uint8_t* __restrict__ even)
@@ -217,36 +218,34 @@ __global__ void k_depth_parity(const uint32_t* __restrict__ parent, uint32_t ni,
     }
 }
 
-__global__ void k_collapse4(const float4* __restrict__ wide, const uint8_t* __restrict__ even, uint32_t ni,
-                            float4* __restrict__ wide4)
+// the 4-wide record of inner node b from the binary records (leaf_only: a one-leaf tree, whose two slots
+// are both the leaf)
+__device__ __forceinline__ void collapse_node(const float4* wide, uint32_t b, bool leaf_only, float4* wide4)
 {
-    const uint32_t nodes = ni ? ni : 1u;
-    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nodes; b += gridDim.x * blockDim.x) {
-        if (ni && !even[b]) continue;
-        float4 out[8];
-        int k = 0;
+    float4* out = wide4 + 8 * b;
+    int k = 0;
 #pragma unroll
-        for (int side = 0; side < 2; ++side) {
-            const float4 mn = __ldcg(wide + 4 * b + 2 * side), mx = __ldcg(wide + 4 * b + 2 * side + 1);
-            const uint32_t code = __float_as_uint(mn.w);
-            if (ni == 0u || (code & 0x80000000u)) {
-                out[k++] = mn;
-                out[k++] = mx;
-            } else {
-                const float4* c = wide + 4 * code;
-                out[k++] = __ldcg(c);
-                out[k++] = __ldcg(c + 1);
-                out[k++] = __ldcg(c + 2);
-                out[k++] = __ldcg(c + 3);
-            }
+    for (int side = 0; side < 2; ++side) {
+        const float4 mn = __ldcg(wide + 4 * b + 2 * side), mx = __ldcg(wide + 4 * b + 2 * side + 1);
+        const uint32_t code = __float_as_uint(mn.w);
+        if (leaf_only || (code & 0x80000000u)) {
+            __stcg(out + k, mn);
+            __stcg(out + k + 1, mx);
+            k += 2;
+        } else {
+            const float4* c = wide + 4 * code;
+            const float4 c0 = __ldcg(c), c1 = __ldcg(c + 1), c2 = __ldcg(c + 2), c3 = __ldcg(c + 3);
+            __stcg(out + k, c0);
+            __stcg(out + k + 1, c1);
+            __stcg(out + k + 2, c2);
+            __stcg(out + k + 3, c3);
+            k += 4;
         }
-        const float inf = __int_as_float(0x7f800000);
-        for (; k < 8; k += 2) {
-            out[k] = make_float4(inf, inf, inf, __uint_as_float(0x80000000u));
-            out[k + 1] = make_float4(-inf, -inf, -inf, __uint_as_float(0u));
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) __stcg(wide4 + 8 * b + j, out[j]);
+    }
+    const float inf = __int_as_float(0x7f800000);
+    for (; k < 8; k += 2) {
+        __stcg(out + k, make_float4(inf, inf, inf, __uint_as_float(0x80000000u)));
+        __stcg(out + k + 1, make_float4(-inf, -inf, -inf, __uint_as_float(0u)));
     }
 }
 
@@ -288,11 +287,14 @@ __device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v
 // fn_update_*_tree_leave_aabb_v2 (lbvh.cpp:617-683) and, when `climb`, fn_refit_tree_aabb
 // (lbvh.cpp:702-754): the second child to arrive at a parent unions the two slot boxes and
 // carries on upwards; arrival counters reset themselves, so no init pass is needed.
+__device__ __forceinline__ void collapse_node(const float4* wide, uint32_t b, bool leaf_only, float4* wide4);
+
 __global__ void k_leaves_refit(int kind, uint32_t n, const uint32_t* __restrict__ sgo,
                                const uint32_t* __restrict__ slot, const uint32_t* __restrict__ parent,
                                const float* __restrict__ thickness, const float4* __restrict__ x0,
                                const float4* __restrict__ x1, const uint32_t* __restrict__ elems, float4* wide,
-                               uint32_t* counters, uint32_t* healthy, int write_leaf, int climb)
+                               uint32_t* counters, uint32_t* healthy, int write_leaf, int climb,
+                               const uint8_t* __restrict__ even, float4* __restrict__ wide4)
 {
     const uint32_t ni = n - 1;
     for (uint32_t lid = blockIdx.x * blockDim.x + threadIdx.x; lid < n; lid += gridDim.x * blockDim.x) {
@@ -303,6 +305,7 @@ __global__ void k_leaves_refit(int kind, uint32_t n, const uint32_t* __restrict_
             if (n == 1) {
                 store_slot(wide, 0, mn, mx, 0x80000000u | e);
                 store_slot(wide, 1, mn, mx, 0x80000000u | e);
+                collapse_node(wide, 0, true, wide4);
             } else {
                 store_slot(wide, slot[ni + lid], mn, mx, 0x80000000u | e, lid);
             }
@@ -322,6 +325,8 @@ __global__ void k_leaves_refit(int kind, uint32_t n, const uint32_t* __restrict_
             float4 a0 = __ldcg(r + 0), a1 = __ldcg(r + 1), b0 = __ldcg(r + 2), b1 = __ldcg(r + 3);
             v3 mn = mk3(fmn(a0.x, b0.x), fmn(a0.y, b0.y), fmn(a0.z, b0.z));
             v3 mx = mk3(fmx(a1.x, b1.x), fmx(a1.y, b1.y), fmx(a1.z, b1.z));
+            // p's 4-wide record: its children's records are final (their last writers arrived before us)
+            if (even[p]) collapse_node(wide, p, false, wide4);
             if (p == 0) break;
             const uint32_t la = __float_as_uint(a1.w), lb = __float_as_uint(b1.w);
             store_slot(wide, slot[p], mn, mx, p, la > lb ? la : lb);
@@ -724,12 +729,9 @@ static int leaves_refit(lcs_bvh* h, const float* thickness, const float* x0, con
     k_leaves_refit<<<grid_for(h->n, 256), 256, 0, s>>>(h->kind, h->n, h->sgo, h->slot, h->parent, thickness,
                                                        reinterpret_cast<const float4*>(x0),
                                                        reinterpret_cast<const float4*>(x1), elems, h->wide,
-                                                       h->counters, h->healthy, write_leaf, climb);
+                                                       h->counters, h->healthy, write_leaf, climb, h->even,
+                                                       h->wide4);
     lcs_count_launch();
-    if (climb || h->ni == 0) {
-        k_collapse4<<<grid_for(h->ni ? h->ni : 1, 256), 256, 0, s>>>(h->wide, h->even, h->ni, h->wide4);
-        lcs_count_launch();
-    }
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }
