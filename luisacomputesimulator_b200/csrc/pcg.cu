@@ -1334,6 +1334,9 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
         m6 = (bb * f - cc * e) * id; m7 = (cc * d - aa * f) * id; m8 = (aa * e - bb * d) * id;
     }
     const bool c_sell = a.c_ptr && *a.c_ok;
+    // the slice's contact groups (fixed for the solve)
+    const uint32_t cg0 = c_sell && ls < nsl ? __ldcg(&a.c_ptr[slice]) >> 2 : 0u;
+    const uint32_t cg1 = c_sell && ls < nsl ? __ldcg(&a.c_ptr[slice + 1]) >> 2 : 0u;
     auto ld_u = [&](uint32_t col) -> float4 {
         const uint32_t lc = col - row0;
         return lc < nloc ? su[lc] : __ldcg(&a.pg[col]);
@@ -1369,9 +1372,7 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
                 else o2 = o;
             }
         }
-        if (c_sell)
-            sell_range(a.c_col, a.c_val, __ldcg(&a.c_ptr[slice]) >> 2, __ldcg(&a.c_ptr[slice + 1]) >> 2, lane, ld_u, o0,
-                       o1, o2);
+        if (c_sell) sell_range(a.c_col, a.c_val, cg0, cg1, lane, ld_u, o0, o1, o2);
         else if (a.B.rp)
             contact_warp(a.B, row0 + 32u * ls, a.n, a.b_vec != 0, ld_u, o0, o1, o2);
         q0 += o0;
