@@ -428,6 +428,7 @@ def run_batch(a):
     xs = [batch.positions(k) for k in range(len(scs))]
     t_e2e = time.perf_counter() - t_e2e
     assert all(np.isfinite(x).all() for x in xs)
+    tuned_chunks, tuned_ms = batch.pcg_tuning()
     del batch
     ms = e0.elapsed_time(e1)
     done_all, t_max = combine(len(scs), ms / 1e3, device="cuda")  # sum of solves, max of device time
@@ -457,6 +458,8 @@ def run_batch(a):
                                f"affine rigid box (8 verts, 12 DOFs) dropped on it; {V_all} cloth vertices in all, "
                                "scene k seeded k, dt 1/60, kappa 1e7, 3 Newton/step, PCG <=100 it rel 1e-4",
                    "scenes": n_all, "verts_rank0": V, "pcg_cluster": "auto",
+                   "pcg_autotune": {"chunks_per_cta": tuned_chunks, "tuned_solve_ms": tuned_ms,
+                                    "candidates": [2, 4, 8, 16]},
                    "parallelism": f"whole scenes over {world} GPUs" if world > 1 else "one batch"},
         "e2e": {"value": done_all / e2e_max, "unit": "solves/s", "h2d_bytes_per_step": None,
                 "d2h_bytes_per_step": 16 * V, "includes": "batch creation (host upload), all steps, read-back"},

@@ -350,8 +350,11 @@ LCS_API int lcs_pcg_solve_noalloc(uint32_t n, const float* diag, const lcs_bsr* 
  * block rows [row_offsets[s], row_offsets[s+1]) of one BSR pair (row_offsets: device array of
  * n_scenes + 1; host_row_offsets: the same offsets in host memory), solved in one launch with one
  * thread-block cluster of `cluster` CTAs (1, 2, 4, 8 or 16) per scene, or with `cluster` = 0 one
- * cluster per scene of the smallest size that leaves it at most 8 chunks of 256 rows per CTA (one
- * launch per size, side by side on streams forked from `stream`).  Each scene has its own
+ * cluster per scene of the smallest size that leaves it at most T chunks of 256 rows per CTA (one
+ * launch per size, side by side on streams forked from `stream`).  T is tuned by the first such call
+ * on the handle: it solves the system once for each T in {2, 4, 8, 16}, times each on `stream`
+ * (synchronising it) and keeps the fastest for later calls (lcs_pcg_batch_tuning reports it).
+ * Each scene has its own
  * alpha, beta and stop decision (the rules of lcs_pcg_solve); its result does not depend on
  * `cluster` or on the other scenes.  active: device flags per scene (0: skip, x = 0) or NULL.
  * stats_per_scene: device array of n_scenes.  Asynchronous; the handle must hold at least
@@ -361,6 +364,9 @@ LCS_API int lcs_pcg_solve_batch(lcs_pcg* p, uint32_t n_scenes, const uint32_t* r
                                 const lcs_bsr* A, const lcs_bsr* B, const float* b, float* x,
                                 const lcs_pcg_opts* opts, lcs_pcg_stats* stats_per_scene, int cluster,
                                 lcs_stream stream);
+/* The chunks-per-CTA target the batched solve tuned (0 before the first cluster = 0 call) and its
+ * measured solve time in ms. */
+LCS_API int lcs_pcg_batch_tuning(const lcs_pcg* p, uint32_t* chunks_per_cta, float* solve_ms);
 
 /* ------------------------------------------------------------------------------------------
  * Cloth energies  (replaces the evaluate kernels of NewtonSolver::compile_evaluate,
@@ -572,6 +578,9 @@ LCS_API int lcs_newton_counts(const lcs_newton* h, uint32_t* nnz_material, uint3
 /* Which PCG the Newton loop runs: 0 plain kernels, 1 persistent CSR solve, 2 row-resident,
  * 3 single-reduction row-resident, 4 single-reduction slice-resident (-1: null handle).  No counterpart in the reference. */
 LCS_API int lcs_newton_pcg_kind(const lcs_newton* h);
+/* A batch's tuned PCG shape (lcs_pcg_batch_tuning of its solver): chunks of 256 rows per CTA and the
+ * tuned solve's time in ms; 0 before the first step of a batch created with pcg_cluster 0. */
+LCS_API int lcs_newton_batch_tuning(const lcs_newton* h, uint32_t* chunks_per_cta, float* solve_ms);
 
 #ifdef __cplusplus
 }

@@ -143,6 +143,7 @@ SIGNATURES = {
     "lcs_ccd_batch": (I32, [I32, P, P, U32, P, P, P, P, P, P, P, P, I32, P]),
     "lcs_pcg_solve_batch": (I32, [P, U32, P, P, P, P, C.POINTER(Bsr), C.POINTER(Bsr), P, P,
                                   C.POINTER(PcgOpts), P, I32, P]),
+    "lcs_pcg_batch_tuning": (I32, [P, C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
     "lcs_newton_destroy": (I32, [P]),
     "lcs_newton_last_iterate": (I32, [P, P, P, P]),
     "lcs_newton_step": (I32, [P, C.POINTER(NewtonStats)]),
@@ -154,6 +155,7 @@ SIGNATURES = {
     "lcs_newton_profile": (I32, [P, C.POINTER(C.c_double), C.POINTER(C.c_int32), I32]),
     "lcs_newton_reset_profile": (I32, [P]),
     "lcs_newton_pcg_kind": (I32, [P]),
+    "lcs_newton_batch_tuning": (I32, [P, C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
     "lcs_newton_counts": (I32, [P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                 C.POINTER(C.c_uint32)]),
 }

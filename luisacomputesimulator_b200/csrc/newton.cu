@@ -2449,6 +2449,12 @@ extern "C" int lcs_newton_reset_profile(lcs_newton* h)
     return LCS_OK;
 }
 
+extern "C" int lcs_newton_batch_tuning(const lcs_newton* h, uint32_t* chunks_per_cta, float* solve_ms)
+{
+    if (!h || !h->pcg) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_batch_tuning: bad handle");
+    return lcs_pcg_batch_tuning(h->pcg, chunks_per_cta, solve_ms);
+}
+
 extern "C" int lcs_newton_pcg_kind(const lcs_newton* h)
 {
     if (!h) return -1;

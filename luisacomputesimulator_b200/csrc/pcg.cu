@@ -1682,6 +1682,8 @@ struct lcs_pcg {
     uint32_t res_blocks = 0, res_slices = 0, res_max_slices = 0;
     uint32_t *res_prefix = nullptr, *res_part = nullptr, *res_owner = nullptr;  // slice partition (per solve)
     size_t res_smem = 0;
+    uint32_t tuned_target = 0;   // batched solves: chunks of 256 rows per CTA picking each scene's cluster (0: untuned)
+    float tuned_ms = 0.0f;       // the tuned configuration's solve time
     lcs_pcg_stats* d_stats = nullptr;
     int fused_grid = 0;
     int rows_capacity = -1;  // most rows the row-resident solve can hold co-resident (-1: not queried)
@@ -2229,6 +2231,18 @@ extern "C" int lcs_pcg_solve_noalloc(uint32_t n, const float* diag, const lcs_bs
     return LCS_OK;
 }
 
+template <class Launch>
+static int solve_batch_auto(lcs_pcg* P, uint32_t n_scenes, const uint32_t* host_row_offsets, Launch& launch,
+                            cudaStream_t s0);
+
+extern "C" int lcs_pcg_batch_tuning(const lcs_pcg* p, uint32_t* chunks_per_cta, float* solve_ms)
+{
+    if (!p) return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_batch_tuning: null handle");
+    if (chunks_per_cta) *chunks_per_cta = p->tuned_target;
+    if (solve_ms) *solve_ms = p->tuned_ms;
+    return LCS_OK;
+}
+
 extern "C" int lcs_pcg_solve_batch(lcs_pcg* P, uint32_t n_scenes, const uint32_t* row_offsets, const uint32_t* host_row_offsets,
                                    const uint32_t* active, const float* diag, const lcs_bsr* A, const lcs_bsr* B,
                                    const float* b, float* x, const lcs_pcg_opts* opts, lcs_pcg_stats* stats_per_scene,
@@ -2295,13 +2309,49 @@ extern "C" int lcs_pcg_solve_batch(lcs_pcg* P, uint32_t n_scenes, const uint32_t
         lcs_count_launch();
         return LCS_OK;
     }
-    // auto: every scene gets the smallest cluster (1..16 CTAs) that leaves it at most 8 chunks of 256 rows
-    // per CTA; one launch per cluster size, on forked streams so that the classes run side by side
+    // auto: every scene gets the smallest cluster (1..16 CTAs) that leaves it at most `target` chunks of 256
+    // rows per CTA; one launch per cluster size, on forked streams so that the classes run side by side.
+    // The target is tuned on the first solve of the handle: the same system is solved with each candidate
+    // (2, 4, 8, 16 chunks per CTA; a scene's solution does not depend on its cluster size) and the fastest
+    // is kept.
+    if (P->tuned_target == 0) {
+        P->tuned_target = 8;  // the untimed default while tuning (and if a timing fails)
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
+            float best = 0.0f;
+            uint32_t best_target = 8;
+            for (uint32_t target : {2u, 4u, 8u, 16u}) {
+                P->tuned_target = target;
+                LCS_CUDA_TRY(cudaEventRecord(e0, s0));
+                const int rc = solve_batch_auto(P, n_scenes, host_row_offsets, launch, s0);
+                if (rc != LCS_OK) return rc;
+                LCS_CUDA_TRY(cudaEventRecord(e1, s0));
+                LCS_CUDA_TRY(cudaEventSynchronize(e1));
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (best == 0.0f || ms < best) {
+                    best = ms;
+                    best_target = target;
+                }
+            }
+            P->tuned_target = best_target;
+            P->tuned_ms = best;
+        }
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    }
+    return solve_batch_auto(P, n_scenes, host_row_offsets, launch, s0);
+}
+
+template <class Launch>
+static int solve_batch_auto(lcs_pcg* P, uint32_t n_scenes, const uint32_t* host_row_offsets, Launch& launch,
+                            cudaStream_t s0)
+{
     std::vector<uint32_t> lists[5];
     for (uint32_t sc = 0; sc < n_scenes; ++sc) {
         const uint32_t chunks = (host_row_offsets[sc + 1] - host_row_offsets[sc] + 255) / 256;
         int k = 0;
-        while (k < 4 && chunks > 8u << k) ++k;
+        while (k < 4 && chunks > P->tuned_target << k) ++k;
         lists[k].push_back(sc);
     }
     std::vector<uint32_t> flat;

@@ -243,6 +243,12 @@ class NewtonBatch:
         A.check(self.lib.lcs_newton_step(self.h, C.byref(self.stats)), "lcs_newton_step")
         return self.stats
 
+    def pcg_tuning(self):
+        """(chunks of 256 rows per CTA, solve ms) picked by the batched PCG's autotuner (0 before tuning)."""
+        t, ms = C.c_uint32(), C.c_float()
+        A.check(self.lib.lcs_newton_batch_tuning(self.h, C.byref(t), C.byref(ms)), "lcs_newton_batch_tuning")
+        return int(t.value), float(ms.value)
+
     def scene_stats(self, k):
         st = A.NewtonStats()
         A.check(self.lib.lcs_newton_scene_stats(self.h, k, C.byref(st)), "lcs_newton_scene_stats")
