@@ -964,6 +964,9 @@ struct lcs_newton {
     // fused mode: the edge-tree lane of the broad phase runs on s2, forked from and joined back to s
     cudaStream_t s2 = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
+    // fused mode: the material producers run on s3 beside the DCD broad and narrow phases
+    cudaStream_t s3 = nullptr;
+    cudaEvent_t fork_m = nullptr, join_m = nullptr;
     // mesh
     uint4* faces = nullptr;
     uint2* edges = nullptr;
@@ -1527,39 +1530,46 @@ int newton_iteration(lcs_newton* h)
         if (h->plain) {  // x_iter_start copied to the host for host_apply_dx (newton_solver.cpp:4196-4198)
             if ((rc = copy_x_to_host(h, h->x))) return rc;
         }
-        k_inertia<<<grid256(V), 256, 0, h->s>>>(V, d.dt, d.dirichlet, h->mass, h->pinned, h->x, h->x_tilde, h->x_iter, h->b,
+        // the material producers (inertia, elastic energies, bodies) touch b, the diagonal and the material
+        // blocks only: beside the DCD broad and narrow phases on s3 (fused mode), joined before assembly
+        cudaStream_t ms = h->s3 ? h->s3 : h->s;
+        if (ms != h->s) {
+            LCS_CUDA_TRY(cudaEventRecord(h->fork_m, h->s));
+            LCS_CUDA_TRY(cudaStreamWaitEvent(ms, h->fork_m, 0));
+        }
+        k_inertia<<<grid256(V), 256, 0, ms>>>(V, d.dt, d.dirichlet, h->mass, h->pinned, h->x, h->x_tilde, h->x_iter, h->b,
                                           h->diag, d.use_floor, d.floor_y, d.kappa, h->vert_area, h->dhat, h->offset, abd_of(h));
         lcs_count_launch();
-        LCS_CUDA_TRY(cudaMemsetAsync(h->mat_val, 0, sizeof(float) * h->sell_vals, h->s));
+        LCS_CUDA_TRY(cudaMemsetAsync(h->mat_val, 0, sizeof(float) * h->sell_vals, ms));
         const uint32_t cs = h->sell ? 128u : 1u;
         if (h->E && d.stretch_model == LCS_STRETCH_SPRING) {
-            k_springs<<<grid256(h->E), 256, 0, h->s>>>(h->E, h->edges, h->rest_len, h->spring_kper, d.spring_k, h->x,
+            k_springs<<<grid256(h->E), 256, 0, ms>>>(h->E, h->edges, h->rest_len, h->spring_kper, d.spring_k, h->x,
                                                        h->b, h->diag, h->spring_slots, cs, h->mat_val);
             lcs_count_launch();
         }
         if (h->Fs && d.stretch_model == LCS_STRETCH_BW98) {
-            k_stretch_bw98<<<grid256(h->Fs), 256, 0, h->s>>>(h->Fs, h->sfaces, h->dm, h->sarea, h->ml, d.stretch_mu,
+            k_stretch_bw98<<<grid256(h->Fs), 256, 0, ms>>>(h->Fs, h->sfaces, h->dm, h->sarea, h->ml, d.stretch_mu,
                                                              d.stretch_lambda, h->x, h->b, h->diag, h->face_slots, cs,
                                                              h->mat_val);
             lcs_count_launch();
         }
         if (h->B && d.bending_model == LCS_BENDING_DIHEDRAL) {
-            k_bending_dihedral<<<grid256(h->B), 256, 0, h->s>>>(h->B, h->bend, h->rest_angle, h->hbar, h->bend_kper,
+            k_bending_dihedral<<<grid256(h->B), 256, 0, ms>>>(h->B, h->bend, h->rest_angle, h->hbar, h->bend_kper,
                                                                 d.bending_k, d.bending_scaling, h->x, h->b, h->diag,
                                                                 h->bend_slots, cs, h->mat_val);
             lcs_count_launch();
         } else if (h->B && d.bending_model == LCS_BENDING_QUADRATIC) {
-            k_bending<<<grid256(h->B), 256, 0, h->s>>>(h->B, h->bend, h->Q, d.bending_k, h->x, h->rest, h->b, h->diag,
+            k_bending<<<grid256(h->B), 256, 0, ms>>>(h->B, h->bend, h->Q, d.bending_k, h->x, h->rest, h->b, h->diag,
                                                  h->bend_slots, cs, h->mat_val);
             lcs_count_launch();
         }
         if (h->NB) {
-            k_abd_body<<<grid256(h->NB), 256, 0, h->s>>>(h->NB, h->body_dof, h->bmass, h->bvol, h->bkappa, h->bfixed,
+            k_abd_body<<<grid256(h->NB), 256, 0, ms>>>(h->NB, h->body_dof, h->bmass, h->bvol, h->bkappa, h->bfixed,
                                                          1.0f / (d.dt * d.dt), d.dirichlet, h->x, h->x_tilde, h->b,
                                                          h->diag, h->body_slots, cs, h->mat_val);
             lcs_count_launch();
             if (d.use_floor) {
-                k_abd_floor<<<grid256(V), 256, 0, h->s>>>(V, abd_of(h), h->pinned, h->x, d.floor_y, d.kappa,
+                k_abd_floor<<<grid256(V), 256, 0, ms>>>(V, abd_of(h), h->pinned, h->x, d.floor_y, d.kappa,
                                                           h->vert_area, h->dhat, h->offset, h->b, h->diag,
                                                           h->body_slots, cs, h->mat_val);
                 lcs_count_launch();
@@ -1589,6 +1599,10 @@ int newton_iteration(lcs_newton* h)
         if (h->plain) {
             if ((rc = host_readback(h))) return rc;  // download_narrowphase_collision_count
             if (grow(h)) { if ((rc = alloc_contact(h))) return rc; continue; }
+        }
+        if (ms != h->s) {
+            LCS_CUDA_TRY(cudaEventRecord(h->join_m, ms));
+            LCS_CUDA_TRY(cudaStreamWaitEvent(h->s, h->join_m, 0));
         }
         // evaluate_contact (newton_solver.cpp:4105-4120)
         mark(h, kPhAssembly);
@@ -1956,7 +1970,10 @@ int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batc
         for (auto& ev : h->ev) cudaEventCreate(&ev);
     if (!h->plain && (cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking) != cudaSuccess ||
                       cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming) != cudaSuccess ||
-                      cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming) != cudaSuccess)) {
+                      cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming) != cudaSuccess ||
+                      cudaStreamCreateWithFlags(&h->s3, cudaStreamNonBlocking) != cudaSuccess ||
+                      cudaEventCreateWithFlags(&h->fork_m, cudaEventDisableTiming) != cudaSuccess ||
+                      cudaEventCreateWithFlags(&h->join_m, cudaEventDisableTiming) != cudaSuccess)) {
         lcs_newton_destroy(h);
         return lcs_fail(LCS_ERR_CUDA, "lcs_newton_create: stream/event creation failed");
     }
@@ -2208,6 +2225,12 @@ extern "C" int lcs_newton_destroy(lcs_newton* h)
     }
     if (h->fork) cudaEventDestroy(h->fork);
     if (h->join) cudaEventDestroy(h->join);
+    if (h->s3) {
+        cudaStreamSynchronize(h->s3);
+        cudaStreamDestroy(h->s3);
+    }
+    if (h->fork_m) cudaEventDestroy(h->fork_m);
+    if (h->join_m) cudaEventDestroy(h->join_m);
     if (h->own_stream) cudaStreamDestroy(h->s);
     delete h;
     return LCS_OK;
