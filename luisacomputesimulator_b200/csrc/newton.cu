@@ -2270,9 +2270,16 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
     }
     // Init LBVH once per step (newton_solver.cpp:4152-4161)
     const float* XS = reinterpret_cast<const float*>(h->x_step);
+    // fused single scene: the edge tree is built on s2 beside the face tree (independent sorts and builds)
+    const bool two = !h->batch && !h->plain && h->s2;
+    cudaStream_t es = two ? h->s2 : h->s;
+    if (two) {
+        LCS_CUDA_TRY(cudaEventRecord(h->fork, h->s));
+        LCS_CUDA_TRY(cudaStreamWaitEvent(es, h->fork, 0));
+    }
     if (!h->batch) {
         if ((rc = lcs_bvh_reduce_aabb(h->face_tree, XS, reinterpret_cast<const uint32_t*>(h->faces), V, h->s))) return rc;
-        if ((rc = lcs_bvh_reduce_aabb(h->edge_tree, XS, reinterpret_cast<const uint32_t*>(h->edges), V, h->s))) return rc;
+        if ((rc = lcs_bvh_reduce_aabb(h->edge_tree, XS, reinterpret_cast<const uint32_t*>(h->edges), V, es))) return rc;
     }
     if (h->batch) {
         if ((rc = lcs_forest_build(h->face_forest, XS, reinterpret_cast<const uint32_t*>(h->faces), h->s))) return rc;
@@ -2282,7 +2289,11 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
         if ((rc = lcs_bvh_construct_host_sort(h->edge_tree, h->s))) return rc;
     } else {
         if ((rc = lcs_bvh_construct(h->face_tree, h->s))) return rc;
-        if ((rc = lcs_bvh_construct(h->edge_tree, h->s))) return rc;
+        if ((rc = lcs_bvh_construct(h->edge_tree, es))) return rc;
+    }
+    if (two) {
+        LCS_CUDA_TRY(cudaEventRecord(h->join, es));
+        LCS_CUDA_TRY(cudaStreamWaitEvent(h->s, h->join, 0));
     }
     if (h->profile) {
         mark(h, kPhMaterial);
