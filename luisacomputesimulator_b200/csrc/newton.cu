@@ -1590,12 +1590,26 @@ int newton_iteration(lcs_newton* h)
         }
         mark(h, kPhDcdNarrow);
         const float* X = reinterpret_cast<const float*>(h->x);
+        // fused: the EE pairs on s2 beside the VF pairs (both append through the pair counter)
+        const bool dlanes = !h->plain && h->s2;
+        if (dlanes) {
+            LCS_CUDA_TRY(cudaEventRecord(h->fork, h->s));
+            LCS_CUDA_TRY(cudaStreamWaitEvent(h->s2, h->fork, 0));
+        }
+        auto dcd_ee = [&](cudaStream_t st) {
+            return lcs_dcd_ee(reinterpret_cast<uint32_t*>(dee), &h->st->cnt[1], h->cap_ee, X,
+                              reinterpret_cast<const uint32_t*>(h->edges), h->body, h->edge_area, h->dhat, h->offset,
+                              d.kappa, h->pairs, h->cap_pairs, &h->st->cnt[2], st);
+        };
+        if (dlanes && (rc = dcd_ee(h->s2))) return rc;
         if ((rc = lcs_dcd_vf(reinterpret_cast<uint32_t*>(dvf), &h->st->cnt[0], h->cap_vf, X, reinterpret_cast<const uint32_t*>(h->faces), h->body, h->vert_area,
                              h->face_area, h->dhat, h->offset, d.kappa, h->pairs, h->cap_pairs, &h->st->cnt[2], h->s)))
             return rc;
-        if ((rc = lcs_dcd_ee(reinterpret_cast<uint32_t*>(dee), &h->st->cnt[1], h->cap_ee, X, reinterpret_cast<const uint32_t*>(h->edges), h->body, h->edge_area, h->dhat,
-                             h->offset, d.kappa, h->pairs, h->cap_pairs, &h->st->cnt[2], h->s)))
-            return rc;
+        if (!dlanes && (rc = dcd_ee(h->s))) return rc;  // the reference's order: VF pairs, then EE pairs
+        if (dlanes) {
+            LCS_CUDA_TRY(cudaEventRecord(h->join, h->s2));
+            LCS_CUDA_TRY(cudaStreamWaitEvent(h->s, h->join, 0));
+        }
         if (h->plain) {
             if ((rc = host_readback(h))) return rc;  // download_narrowphase_collision_count
             if (grow(h)) { if ((rc = alloc_contact(h))) return rc; continue; }
@@ -1606,17 +1620,27 @@ int newton_iteration(lcs_newton* h)
         }
         // evaluate_contact (newton_solver.cpp:4105-4120)
         mark(h, kPhAssembly);
+        // fused: gradient and diagonal on s2 beside the off-diagonal assembly (disjoint outputs)
+        cudaStream_t gs = dlanes ? h->s2 : h->s;
+        if (dlanes) {
+            LCS_CUDA_TRY(cudaEventRecord(h->fork, h->s));
+            LCS_CUDA_TRY(cudaStreamWaitEvent(gs, h->fork, 0));
+        }
         if (h->NB) {  // pairs with a rigid side go to the body's DOF slots (ABD remap)
             const lcs_abd_view av{h->body, reinterpret_cast<const float*>(h->model_x), h->body_dof};
             if ((rc = lcs_contact_grad_diag_abd(h->pairs, &h->st->cnt[2], h->cap_pairs, reinterpret_cast<float*>(h->b),
-                                                reinterpret_cast<float*>(h->diag), &av, h->s)))
+                                                reinterpret_cast<float*>(h->diag), &av, gs)))
                 return rc;
             if ((rc = lcs_contact_offdiag_bsr_abd(h->asmb, h->pairs, &h->st->cnt[2], h->cap_pairs, &av, h->s))) return rc;
         } else {
             if ((rc = lcs_contact_grad_diag(h->pairs, &h->st->cnt[2], h->cap_pairs, reinterpret_cast<float*>(h->b),
-                                            reinterpret_cast<float*>(h->diag), h->s)))
+                                            reinterpret_cast<float*>(h->diag), gs)))
                 return rc;
             if ((rc = lcs_contact_offdiag_bsr(h->asmb, h->pairs, &h->st->cnt[2], h->cap_pairs, h->s))) return rc;
+        }
+        if (dlanes) {
+            LCS_CUDA_TRY(cudaEventRecord(h->join, gs));
+            LCS_CUDA_TRY(cudaStreamWaitEvent(h->s, h->join, 0));
         }
         if (h->plain) {  // prescan + construct adjacency + the two-level triplet sort read back counts 4 times
             for (int k = 0; k < 4; ++k)
