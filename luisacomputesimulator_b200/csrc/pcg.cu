@@ -1141,19 +1141,20 @@ struct ResArgs {
 // at least one, and every later block still able to take the rest.  One block of 1024 threads: the
 // prefix by block scans, the ideal cuts by one binary search per block, the clamping in one thread.
 constexpr uint32_t kResSliceBase = 2;
+constexpr uint32_t kResMaxSlices = kResMaxBlocks * (kResThreads / 32);  // the partition's shared prefix
 
 __global__ void __launch_bounds__(1024) k_res_partition(uint32_t S, uint32_t P, uint32_t cap, const uint32_t* __restrict__ m_ptr,
                                                         const uint32_t* __restrict__ c_ptr, const int* __restrict__ c_ok,
-                                                        uint32_t* __restrict__ prefix, uint32_t* __restrict__ part,
-                                                        uint32_t* __restrict__ owner)
+                                                        uint32_t* __restrict__ part, uint32_t* __restrict__ owner)
 {
+    __shared__ uint32_t prefix[kResMaxSlices + 1];  // cost of slices [0, s)
+    __shared__ uint32_t cut[kResMaxBlocks + 1];
     __shared__ uint32_t ws[32];
     __shared__ uint32_t carry;
     const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
     const bool cs = c_ptr && c_ok && *c_ok;
     if (t == 0) carry = 0u;
     __syncthreads();
-    // prefix[s] = cost of slices [0, s)
     for (uint32_t base = 0; base < S; base += 1024u) {
         const uint32_t sl = base + t;
         uint32_t v = 0u;
@@ -1196,24 +1197,25 @@ __global__ void __launch_bounds__(1024) k_res_partition(uint32_t S, uint32_t P, 
             if ((uint64_t)prefix[mid] < target) lo = mid + 1;
             else hi = mid;
         }
-        part[c] = lo;
+        cut[c] = lo;
     }
     __syncthreads();
     if (t == 0) {
         uint32_t prev = 0u;
-        part[0] = 0u;
+        cut[0] = 0u;
         for (uint32_t c = 1; c < P; ++c) {
             const uint32_t lo = max(prev + 1u, S > cap * (P - c) ? S - cap * (P - c) : 0u);
             const uint32_t hi = min(prev + cap, S - (P - c));
-            const uint32_t b = min(max(part[c], lo), hi);
-            part[c] = b;
+            const uint32_t b = min(max(cut[c], lo), hi);
+            cut[c] = b;
             prev = b;
         }
-        part[P] = S;
+        cut[P] = S;
     }
     __syncthreads();
+    for (uint32_t c = t; c <= P; c += 1024u) part[c] = cut[c];
     for (uint32_t c = warp; c < P; c += 32u)
-        for (uint32_t sl = part[c] + lane; sl < part[c + 1]; sl += 32u) owner[sl] = c;
+        for (uint32_t sl = cut[c] + lane; sl < cut[c + 1]; sl += 32u) owner[sl] = c;
 }
 
 __device__ __forceinline__ void st_release(unsigned* p, unsigned v)
@@ -1680,7 +1682,7 @@ struct lcs_pcg {
     unsigned* flags = nullptr;   // slice-resident solve: per-block publication tags (kResMaxBlocks)
     int res_gres = -2;           // slice-resident solve: resident groups per slice (-2: not set up)
     uint32_t res_blocks = 0, res_slices = 0, res_max_slices = 0;
-    uint32_t *res_prefix = nullptr, *res_part = nullptr, *res_owner = nullptr;  // slice partition (per solve)
+    uint32_t *res_part = nullptr, *res_owner = nullptr;  // slice partition (per solve)
     size_t res_smem = 0;
     uint32_t tuned_target = 0;   // batched solves: chunks of 256 rows per CTA picking each scene's cluster (0: untuned)
     float tuned_ms = 0.0f;       // the tuned configuration's solve time
@@ -1743,7 +1745,7 @@ extern "C" int lcs_pcg_destroy(lcs_pcg* p)
 {
     if (!p) return LCS_OK;
     void* ptrs[] = {p->r, p->z, p->p, p->q, p->minv, p->part, p->part_f, p->scal, p->bar, p->flags, p->d_stats,
-                    p->cpart, p->class_scenes, p->res_prefix, p->res_part, p->res_owner};
+                    p->cpart, p->class_scenes, p->res_part, p->res_owner};
     for (int k = 0; k < 5; ++k) {
         if (p->class_stream[k]) {
             cudaStreamSynchronize(p->class_stream[k]);
@@ -1864,8 +1866,7 @@ static int res_setup(lcs_pcg* P)
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_res<kResThreads>, kResThreads, dyn);
     if (per_sm < 1 || (int64_t)per_sm * sms < (int64_t)blocks) return LCS_ERR_CAPACITY;
-    if (cudaMalloc((void**)&P->res_prefix, sizeof(uint32_t) * (S + 1)) != cudaSuccess ||
-        cudaMalloc((void**)&P->res_part, sizeof(uint32_t) * (blocks + 1)) != cudaSuccess ||
+    if (cudaMalloc((void**)&P->res_part, sizeof(uint32_t) * (blocks + 1)) != cudaSuccess ||
         cudaMalloc((void**)&P->res_owner, sizeof(uint32_t) * S) != cudaSuccess) {
         cudaGetLastError();
         return LCS_ERR_CAPACITY;
@@ -2018,7 +2019,7 @@ static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* 
     const int grid = (int)((P->n + kRowThreads - 1) / kRowThreads);
     if (pipe && sell && !(o.flags & kPcgNoResident) && res_setup(P) == LCS_OK) {
         k_res_partition<<<1, 1024, 0, s>>>(P->res_slices, P->res_blocks, P->res_max_slices, m_ptr, a.c_ptr, a.c_ok,
-                                           P->res_prefix, P->res_part, P->res_owner);
+                                           P->res_part, P->res_owner);
         lcs_count_launch();
         ResArgs ra{a, P->res_part, P->res_owner, P->flags, P->res_slices, P->res_max_slices, P->res_gres};
         void* rargs[] = {&ra};
