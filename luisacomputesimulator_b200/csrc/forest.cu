@@ -274,10 +274,11 @@ __global__ void __launch_bounds__(128) k_f_query(const float4* __restrict__ wide
                                                  uint32_t n_queries, const float* __restrict__ dhat,
                                                  const float* __restrict__ thickness, uint2* __restrict__ pairs,
                                                  uint32_t capacity, uint32_t* d_count, const uint32_t* __restrict__ order,
-                                                 uint32_t* capped)
+                                                 uint32_t* capped, const uint8_t* __restrict__ only)
 {
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_queries; t += gridDim.x * blockDim.x) {
         const uint32_t q = order ? __ldg(&order[t]) : t;
+        if (only && !only[EE ? __ldg(&edges[q]).x : q]) continue;  // queries of the masked scenes only
         float box[6];
         {
             v3 mn, mx;
@@ -549,7 +550,8 @@ extern "C" int lcs_forest_query_vf(const lcs_forest* face_forest, const float* x
 
 int lcs_forest_query_vf_capped(const lcs_forest* face_forest, const float* x0, const float* x1, uint32_t n_verts,
                                const uint32_t* vert_scene, const float* d_hat, const float* thickness, uint32_t* pairs,
-                               uint32_t capacity, uint32_t* d_count, uint32_t* capped, lcs_stream stream)
+                               uint32_t capacity, uint32_t* d_count, uint32_t* capped, lcs_stream stream,
+                               const uint8_t* only)
 {
     const lcs_forest* f = face_forest;
     if (!f || f->kind != LCS_TREE_FACE || !x0 || !x1 || !vert_scene || !d_hat || !thickness || !d_count ||
@@ -558,7 +560,7 @@ int lcs_forest_query_vf_capped(const lcs_forest* face_forest, const float* x0, c
     if (n_verts == 0) return LCS_OK;
     k_f_query<false><<<grid_for(n_verts, 128, 16), 128, 0, (cudaStream_t)stream>>>(
         f->wide, f->ioff, vert_scene, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1), nullptr,
-        n_verts, d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count, nullptr, capped);
+        n_verts, d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count, nullptr, capped, only);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
@@ -574,7 +576,7 @@ extern "C" int lcs_forest_query_ee(const lcs_forest* edge_forest, const float* x
 
 int lcs_forest_query_ee_capped(const lcs_forest* edge_forest, const float* x0, const float* x1, const uint32_t* edges,
                                const float* d_hat, const float* thickness, uint32_t* pairs, uint32_t capacity,
-                               uint32_t* d_count, uint32_t* capped, lcs_stream stream)
+                               uint32_t* d_count, uint32_t* capped, lcs_stream stream, const uint8_t* only)
 {
     const lcs_forest* f = edge_forest;
     if (!f || f->kind != LCS_TREE_EDGE || !x0 || !x1 || !edges || !d_hat || !thickness || !d_count ||
@@ -583,7 +585,7 @@ int lcs_forest_query_ee_capped(const lcs_forest* edge_forest, const float* x0, c
     k_f_query<true><<<grid_for(f->N, 128, 16), 128, 0, (cudaStream_t)stream>>>(
         f->wide, f->ioff, f->escene, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
         reinterpret_cast<const uint2*>(edges), f->N, d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity,
-        d_count, f->sgo, capped);
+        d_count, f->sgo, capped, only);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;

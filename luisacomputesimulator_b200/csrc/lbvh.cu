@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(256) k_filter(const uint2* __restrict__ in, co
                                                 uint32_t in_cap, const float4* __restrict__ x,
                                                 const uint32_t* __restrict__ elems, const float* __restrict__ dhat,
                                                 const float* __restrict__ thickness, uint2* __restrict__ out,
-                                                uint32_t out_cap, uint32_t* out_count)
+                                                uint32_t out_cap, uint32_t* out_count, const uint8_t* __restrict__ skip)
 {
     uint32_t n = *in_count;
     n = n < in_cap ? n : in_cap;
@@ -516,7 +516,8 @@ __global__ void __launch_bounds__(256) k_filter(const uint2* __restrict__ in, co
                 const float q[6] = {mn.x - r, mn.y - r, mn.z - r, mx.x + r, mx.y + r, mx.z + r};
                 v3 lm, lx;
                 leaf_box(LCS_TREE_EDGE, pr.y, thickness, x, x, elems, lm, lx);
-                keep = overlap(make_float4(lm.x, lm.y, lm.z, 0.f), make_float4(lx.x, lx.y, lx.z, 0.f), q);
+                keep = overlap(make_float4(lm.x, lm.y, lm.z, 0.f), make_float4(lx.x, lx.y, lx.z, 0.f), q) &&
+                       !(skip && skip[v0]);
             } else {
                 qa = ld3(x, pr.x);
                 const v3 mn = min3(qa, qa), mx = max3(qa, qa);
@@ -525,7 +526,8 @@ __global__ void __launch_bounds__(256) k_filter(const uint2* __restrict__ in, co
                 const float q[6] = {mn.x - r, mn.y - r, mn.z - r, mx.x + r, mx.y + r, mx.z + r};
                 v3 lm, lx;
                 leaf_box(LCS_TREE_FACE, pr.y, thickness, x, x, elems, lm, lx);
-                keep = overlap(make_float4(lm.x, lm.y, lm.z, 0.f), make_float4(lx.x, lx.y, lx.z, 0.f), q);
+                keep = overlap(make_float4(lm.x, lm.y, lm.z, 0.f), make_float4(lx.x, lx.y, lx.z, 0.f), q) &&
+                       !(skip && skip[v0]);
             }
         }
         const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, keep);
@@ -855,9 +857,10 @@ extern "C" int lcs_bvh_export(const lcs_bvh* h, uint32_t* parent, uint32_t* chil
     return LCS_OK;
 }
 
-extern "C" int lcs_candidates_filter(int is_ee, const uint32_t* in_pairs, const uint32_t* in_count, uint32_t in_capacity,
-                                     const float* x, const uint32_t* elems, const float* d_hat, const float* thickness,
-                                     uint32_t* out_pairs, uint32_t out_capacity, uint32_t* out_count, lcs_stream stream)
+int lcs_candidates_filter_masked(int is_ee, const uint32_t* in_pairs, const uint32_t* in_count, uint32_t in_capacity,
+                                 const float* x, const uint32_t* elems, const float* d_hat, const float* thickness,
+                                 uint32_t* out_pairs, uint32_t out_capacity, uint32_t* out_count, lcs_stream stream,
+                                 const uint8_t* skip)
 {
     if (!in_count || !x || !elems || !d_hat || !thickness || !out_count || (in_capacity && !in_pairs) ||
         (out_capacity && !out_pairs))
@@ -866,8 +869,17 @@ extern "C" int lcs_candidates_filter(int is_ee, const uint32_t* in_pairs, const 
     auto kern = is_ee ? k_filter<true> : k_filter<false>;
     kern<<<grid_for(in_capacity, 256), 256, 0, (cudaStream_t)stream>>>(
         reinterpret_cast<const uint2*>(in_pairs), in_count, in_capacity, reinterpret_cast<const float4*>(x), elems,
-        d_hat, thickness, reinterpret_cast<uint2*>(out_pairs), out_capacity, out_count);
+        d_hat, thickness, reinterpret_cast<uint2*>(out_pairs), out_capacity, out_count, skip);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }
+
+extern "C" int lcs_candidates_filter(int is_ee, const uint32_t* in_pairs, const uint32_t* in_count, uint32_t in_capacity,
+                                     const float* x, const uint32_t* elems, const float* d_hat, const float* thickness,
+                                     uint32_t* out_pairs, uint32_t out_capacity, uint32_t* out_count, lcs_stream stream)
+{
+    return lcs_candidates_filter_masked(is_ee, in_pairs, in_count, in_capacity, x, elems, d_hat, thickness, out_pairs,
+                                        out_capacity, out_count, stream, nullptr);
+}
+

@@ -46,9 +46,17 @@ int lcs_bvh_query_ee_capped(const lcs_bvh* t, const float* x0, const float* x1, 
 int lcs_bvh_query_ee_sym_capped(const lcs_bvh* t, const float* x0, const float* x1, const uint32_t* edges,
                                 float d_hat, uint32_t* pairs, uint32_t capacity, uint32_t* d_count, uint32_t* capped,
                                 lcs_stream stream);
+// only (optional): a per-vertex mask; queries whose (first) vertex is not set are skipped.
 int lcs_forest_query_vf_capped(const lcs_forest* f, const float* x0, const float* x1, uint32_t n_verts,
                                const uint32_t* vert_scene, const float* d_hat, const float* thickness, uint32_t* pairs,
-                               uint32_t capacity, uint32_t* d_count, uint32_t* capped, lcs_stream stream);
+                               uint32_t capacity, uint32_t* d_count, uint32_t* capped, lcs_stream stream,
+                               const uint8_t* only = nullptr);
 int lcs_forest_query_ee_capped(const lcs_forest* f, const float* x0, const float* x1, const uint32_t* edges,
                                const float* d_hat, const float* thickness, uint32_t* pairs, uint32_t capacity,
-                               uint32_t* d_count, uint32_t* capped, lcs_stream stream);
+                               uint32_t* d_count, uint32_t* capped, lcs_stream stream, const uint8_t* only = nullptr);
+// lcs_candidates_filter that also drops the pairs whose query vertex (VF: the vertex; EE: the first vertex
+// of the query edge) is set in `skip` (optional).
+int lcs_candidates_filter_masked(int is_ee, const uint32_t* in_pairs, const uint32_t* in_count, uint32_t in_capacity,
+                                 const float* x, const uint32_t* elems, const float* d_hat, const float* thickness,
+                                 uint32_t* out_pairs, uint32_t out_capacity, uint32_t* out_count, lcs_stream stream,
+                                 const uint8_t* skip);

@@ -1038,6 +1038,7 @@ struct lcs_newton {
     int cluster = 4;
     std::vector<uint32_t> h_voff, h_foff, h_eoff;
     uint32_t *vscene = nullptr, *voff_d = nullptr, *active = nullptr, *h_active = nullptr;
+    uint8_t* rigid_scene_v = nullptr;  // batch with affine bodies: 1 for the vertices of scenes that hold one
     lcs_forest *face_forest = nullptr, *edge_forest = nullptr;
     float* bsc = nullptr;           // device: toi[S], max_dx[S], dirichlet[S]
     float* h_bsc = nullptr;         // pinned mirror
@@ -1394,6 +1395,40 @@ int dcd_by_filter(lcs_newton* h)
     return LCS_OK;
 }
 
+// A batch with affine bodies: its scenes without bodies filter the previous CCD lists (exact, as above),
+// its scenes with bodies -- whose rigid vertices are placed by p + A x_bar and may round outside the swept
+// boxes -- are traversed again with static boxes; both append to the same DCD lists.
+int dcd_mixed(lcs_newton* h)
+{
+    const float* X = reinterpret_cast<const float*>(h->x);
+    const uint32_t* ED = reinterpret_cast<const uint32_t*>(h->edges);
+    const uint32_t* FA = reinterpret_cast<const uint32_t*>(h->faces);
+    int rc;
+    LCS_CUDA_TRY(cudaEventRecord(h->fork, h->s));
+    LCS_CUDA_TRY(cudaStreamWaitEvent(h->s2, h->fork, 0));
+    if ((rc = lcs_candidates_filter_masked(1, reinterpret_cast<const uint32_t*>(h->bp_ee), h->prev_ccd + 1, h->cap_ee, X,
+                                           ED, h->dhat, h->offset, reinterpret_cast<uint32_t*>(h->dcd_ee), h->cap_ee,
+                                           &h->st->cnt[1], h->s2, h->rigid_scene_v)))
+        return rc;
+    if ((rc = lcs_forest_update_refit(h->edge_forest, h->offset, X, X, ED, h->s2))) return rc;
+    if ((rc = lcs_forest_query_ee_capped(h->edge_forest, X, X, ED, h->dhat, h->offset,
+                                         reinterpret_cast<uint32_t*>(h->dcd_ee), h->cap_ee, &h->st->cnt[1], nullptr,
+                                         h->s2, h->rigid_scene_v)))
+        return rc;
+    if ((rc = lcs_candidates_filter_masked(0, reinterpret_cast<const uint32_t*>(h->bp_vf), h->prev_ccd, h->cap_vf, X, FA,
+                                           h->dhat, h->offset, reinterpret_cast<uint32_t*>(h->dcd_vf), h->cap_vf,
+                                           &h->st->cnt[0], h->s, h->rigid_scene_v)))
+        return rc;
+    if ((rc = lcs_forest_update_refit(h->face_forest, h->offset, X, X, FA, h->s))) return rc;
+    if ((rc = lcs_forest_query_vf_capped(h->face_forest, X, X, h->V, h->vscene, h->dhat, h->offset,
+                                         reinterpret_cast<uint32_t*>(h->dcd_vf), h->cap_vf, &h->st->cnt[0], nullptr,
+                                         h->s, h->rigid_scene_v)))
+        return rc;
+    LCS_CUDA_TRY(cudaEventRecord(h->join, h->s2));
+    LCS_CUDA_TRY(cudaStreamWaitEvent(h->s, h->join, 0));
+    return LCS_OK;
+}
+
 bool grow(lcs_newton* h)
 {
     const Status& s = *h->h_st;
@@ -1580,7 +1615,7 @@ int newton_iteration(lcs_newton* h)
         uint2* dvf = h->plain ? h->bp_vf : h->dcd_vf;
         uint2* dee = h->plain ? h->bp_ee : h->dcd_ee;
         if (filter) {
-            if ((rc = dcd_by_filter(h))) return rc;
+            if ((rc = h->rigid_scene_v ? dcd_mixed(h) : dcd_by_filter(h))) return rc;
         } else if ((rc = broad_phase(h, h->x, h->x, dvf, dee, &h->st->cnt[0], &h->st->cnt[1], nullptr))) {
             return rc;
         }
@@ -1769,7 +1804,8 @@ int newton_iteration(lcs_newton* h)
         // the next iteration may filter these CCD lists if no traversal ended early
         // (not with affine bodies: their vertices are placed by p + A x_bar of the stepped q, which may round
         // outside the swept box of x_iter + t dx by an ulp)
-        h->filter_ok = !h->plain && !h->NB && h->h_st->cnt[5] == 0u;
+        // (a batch with bodies filters its other scenes and traverses those, dcd_mixed)
+        h->filter_ok = !h->plain && (!h->NB || h->batch) && h->h_st->cnt[5] == 0u;
         if (grow(h)) {  // an overflow anywhere: undo the step and run the iteration again
             k_copy4<<<grid256(V), 256, 0, h->s>>>(V, h->x_iter, h->x);
             lcs_count_launch();
@@ -2146,6 +2182,16 @@ extern "C" int lcs_newton_create_batch(const lcs_scene_desc* descs, uint32_t n_s
     cudaError_t e = cudaSuccess;
     auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
     A(upload(h->vscene, vscene.data(), V));
+    {
+        bool any = false;
+        std::vector<uint8_t> rsv(V, 0);
+        for (uint32_t s = 0; s < n_scenes; ++s)
+            if (descs[s].n_bodies > 0) {
+                any = true;
+                std::fill(rsv.begin() + voff[s], rsv.begin() + voff[s + 1], (uint8_t)1);
+            }
+        if (any) A(upload(h->rigid_scene_v, rsv.data(), V));
+    }
     A(upload(h->voff_d, voff.data(), n_scenes + 1));
     A(dalloc(h->active, n_scenes));
     A(dalloc(h->bsc, 3 * (size_t)n_scenes));
@@ -2218,7 +2264,7 @@ extern "C" int lcs_newton_destroy(lcs_newton* h)
     lcs_forest_destroy(h->edge_forest);
     lcs_pcg_destroy(h->pcg);
     {
-        void* bp[] = {h->vscene, h->voff_d, h->active, h->bsc, h->bpcg};
+        void* bp[] = {h->vscene, h->voff_d, h->active, h->bsc, h->bpcg, h->rigid_scene_v};
         for (void* p : bp)
             if (p) cudaFree(p);
         if (h->h_active) cudaFreeHost(h->h_active);

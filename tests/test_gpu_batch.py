@@ -273,3 +273,40 @@ def test_batched_newton_agrees_with_single_scene_solver():
         xm, xs = mix.positions(k), singles[k].positions()
         scale = np.abs(xs[:, :3] - sc.x[:, :3]).max()
         np.testing.assert_allclose(xm[:, :3], xs[:, :3], rtol=0, atol=5e-3 * scale + 1e-7)
+
+
+def _static_counts(sc, x):
+    tf = O.lbvh_build(O.TREE_FACE, x, sc.faces, sc.num_verts)
+    te = O.lbvh_build(O.TREE_EDGE, x, sc.edges, sc.num_verts)
+    O.lbvh_refit(tf, x, x, sc.faces, sc.offset)
+    O.lbvh_refit(te, x, x, sc.edges, sc.offset)
+    return O.lbvh_query_vf(tf, x, x, sc.d_hat, sc.offset)[1], O.lbvh_query_ee(te, x, x, sc.edges, sc.d_hat, sc.offset)[1]
+
+
+def test_batch_with_a_body_filters_soft_scenes_and_traverses_the_rigid_one():
+    """A batch holding an affine body: from the second Newton iteration of a step on, the soft scene's DCD lists
+    come from filtering the previous CCD lists and the rigid scene's from a traversal of its trees.  The last
+    iteration's candidate counts, summed over the scenes, equal the oracle's static queries at the positions that
+    iteration started from."""
+    import ctypes as C
+    scs = [S.random_cloth_scene(900, 2), S.cloth_box_scene(600, 5)]
+    batch = NewtonBatch(scs, nonlinear_iters=3)
+    V = sum(sc.num_verts for sc in scs)
+    offs = np.cumsum([0] + [sc.num_verts for sc in scs])
+    checked = 0
+    for _ in range(4):
+        st = batch.step()
+        assert st.status == 0
+        if st.newton_iters < 2:
+            continue
+        x_iter = np.zeros((V, 4), np.float32)
+        batch.lib.lcs_newton_last_iterate(batch.h, x_iter.ctypes.data_as(C.c_void_p), None, None)
+        vf = ee = 0
+        for k, sc in enumerate(scs):
+            a, b = _static_counts(sc, x_iter[offs[k]:offs[k + 1]].copy())
+            vf, ee = vf + a, ee + b
+        assert (st.vf_candidates, st.ee_candidates) == (vf, ee)
+        checked += 1
+    assert checked >= 2
+    for k, sc in enumerate(scs):
+        assert O.min_distance(sc, batch.positions(k)) > 0.0
