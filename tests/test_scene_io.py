@@ -11,7 +11,7 @@ import pytest
 
 from luisacomputesimulator_b200 import scene_io, scenes as S
 
-REF = "/root/reference/Resources"
+REF = os.path.join(os.environ.get("REFERENCE_ROOT", "/root/reference"), "Resources")  # read only when present
 
 
 def _grid_obj(path, n=5, quads=True):
