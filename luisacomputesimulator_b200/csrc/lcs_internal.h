@@ -60,3 +60,15 @@ int lcs_candidates_filter_masked(int is_ee, const uint32_t* in_pairs, const uint
                                  const float* x, const uint32_t* elems, const float* d_hat, const float* thickness,
                                  uint32_t* out_pairs, uint32_t out_capacity, uint32_t* out_count, lcs_stream stream,
                                  const uint8_t* skip);
+
+// DCD pairs straight from the previous iteration's CCD candidate list: the candidates whose static boxes
+// overlap at x (the test of lcs_candidates_filter, counted into *d_cand_count) go through the DCD test of
+// lcs_dcd_vf / lcs_dcd_ee; the same pairs and counts as filter + DCD without writing the candidate list.
+int lcs_dcd_vf_filtered(const uint32_t* ccd_pairs, const uint32_t* d_ccd_count, uint32_t capacity, const float* x,
+                        const uint32_t* faces, const uint32_t* body, const float* vert_area, const float* face_area,
+                        const float* d_hat, const float* offset, float kappa, lcs_pair* out, uint32_t out_capacity,
+                        uint32_t* d_out_count, uint32_t* d_cand_count, lcs_stream stream);
+int lcs_dcd_ee_filtered(const uint32_t* ccd_pairs, const uint32_t* d_ccd_count, uint32_t capacity, const float* x,
+                        const uint32_t* edges, const uint32_t* body, const float* edge_area, const float* d_hat,
+                        const float* offset, float kappa, lcs_pair* out, uint32_t out_capacity, uint32_t* d_out_count,
+                        uint32_t* d_cand_count, lcs_stream stream);

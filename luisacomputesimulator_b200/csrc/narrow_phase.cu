@@ -10,6 +10,7 @@
 
 #include "lcs_common.cuh"
 #include "lcs_geom.cuh"
+#include "lbvh_common.cuh"
 #include "lcs_internal.h"
 #include "radix_sort.cuh"
 #include "scan.cuh"
@@ -107,13 +108,44 @@ __device__ __forceinline__ void write_pair(lcs_pair* out, uint32_t s, uint32_t i
     reinterpret_cast<float4*>(o)[2] = make_float4(k1, k2, b0, b1);
 }
 
+// The candidate test of lcs_candidates_filter: a swept-box candidate whose static boxes overlap at x (the
+// query box +- thickness + d_hat of its first vertex, the leaf box +- thickness of its element's first
+// vertex, strict).  With FILTER the DCD kernels below take the previous iteration's CCD list and count the
+// candidates passing it into d_cand_count themselves -- the DCD list lcs_candidates_filter would write is the
+// same set, so the pairs and counts are those of filter + DCD.
+template <bool EE>
+__device__ __forceinline__ bool static_candidate(uint2 pr, const float4* __restrict__ x, const uint32_t* __restrict__ elems,
+                                                 const float* __restrict__ dhat, const float* __restrict__ thickness)
+{
+    v3 mn, mx;
+    uint32_t v0;
+    if (EE) {
+        const uint2 ed = __ldg(reinterpret_cast<const uint2*>(elems) + pr.x);
+        const v3 s0 = ld3(x, ed.x), s1 = ld3(x, ed.y);
+        mn = min3(min3(s0, s1), min3(s0, s1));
+        mx = max3(max3(s0, s1), max3(s0, s1));
+        v0 = ed.x;
+    } else {
+        const v3 qa = ld3(x, pr.x);
+        mn = min3(qa, qa);
+        mx = max3(qa, qa);
+        v0 = pr.x;
+    }
+    const float r = __ldg(&thickness[v0]) + __ldg(&dhat[v0]);
+    const float q[6] = {mn.x - r, mn.y - r, mn.z - r, mx.x + r, mx.y + r, mx.z + r};
+    v3 lm, lx;
+    leaf_box(EE ? LCS_TREE_EDGE : LCS_TREE_FACE, pr.y, thickness, x, x, elems, lm, lx);
+    return overlap(make_float4(lm.x, lm.y, lm.z, 0.f), make_float4(lx.x, lx.y, lx.z, 0.f), q);
+}
+
 // fn_narrow_phase_vf_dcd_query (barrier energy), narrow_phase.cpp:771-933
+template <bool FILTER>
 __global__ void __launch_bounds__(256) k_dcd_vf(const uint2* __restrict__ pairs, const uint32_t* d_count, uint32_t cap,
                                                 const float4* __restrict__ x, const uint4* __restrict__ faces,
                                                 const uint32_t* __restrict__ body, const float* __restrict__ vert_area,
                                                 const float* __restrict__ face_area, const float* __restrict__ dhat,
                                                 const float* __restrict__ offset, float kappa, lcs_pair* out,
-                                                uint32_t out_cap, uint32_t* d_out_count)
+                                                uint32_t out_cap, uint32_t* d_out_count, uint32_t* d_cand_count)
 {
     const uint32_t n = pair_count(d_count, cap);
     const uint32_t n_round = (n + 31u) & ~31u;  // whole warps iterate together for the append
@@ -123,13 +155,16 @@ __global__ void __launch_bounds__(256) k_dcd_vf(const uint2* __restrict__ pairs,
         uint4 f = make_uint4(0, 0, 0, 0);
         v3 nrm = mk3(0, 0, 0);
         float k1 = 0, k2 = 0, stiff = 0, c0 = 0, c1 = 0;
+        bool cand = false;
         if (p < n) {
             const uint2 pr = __ldg(&pairs[p]);
+            cand = !FILTER || static_candidate<false>(pr, x, reinterpret_cast<const uint32_t*>(faces), dhat, offset);
             vid = pr.x;
             fid = pr.y;
             f = __ldg(&faces[fid]);
             const uint32_t bv = __ldg(&body[vid]);
-            const bool skip = vid == f.x || vid == f.y || vid == f.z || (bv != kInvalid && bv == __ldg(&body[f.x]));
+            const bool skip = !cand || vid == f.x || vid == f.y || vid == f.z ||
+                              (bv != kInvalid && bv == __ldg(&body[f.x]));
             if (!skip) {
                 const v3 pp = ld3(x, vid), t0 = ld3(x, f.x), t1 = ld3(x, f.y), t2 = ld3(x, f.z);
                 float c[3];
@@ -152,17 +187,20 @@ __global__ void __launch_bounds__(256) k_dcd_vf(const uint2* __restrict__ pairs,
                 }
             }
         }
+        if (FILTER) warp_append(d_cand_count, cand);
         const uint32_t s = warp_append(d_out_count, emit);
         if (emit && s < out_cap) write_pair(out, s, vid, f.x, f.y | 0x80000000u, f.z, nrm, k1, k2, stiff, c0, c1);
     }
 }
 
 // fn_narrow_phase_ee_dcd_query (barrier energy), narrow_phase.cpp:935-1098
+template <bool FILTER>
 __global__ void __launch_bounds__(256) k_dcd_ee(const uint2* __restrict__ pairs, const uint32_t* d_count, uint32_t cap,
                                                 const float4* __restrict__ x, const uint2* __restrict__ edges,
                                                 const uint32_t* __restrict__ body, const float* __restrict__ edge_area,
                                                 const float* __restrict__ dhat, const float* __restrict__ offset,
-                                                float kappa, lcs_pair* out, uint32_t out_cap, uint32_t* d_out_count)
+                                                float kappa, lcs_pair* out, uint32_t out_cap, uint32_t* d_out_count,
+                                                uint32_t* d_cand_count)
 {
     const uint32_t n = pair_count(d_count, cap);
     const uint32_t n_round = (n + 31u) & ~31u;
@@ -171,13 +209,15 @@ __global__ void __launch_bounds__(256) k_dcd_ee(const uint2* __restrict__ pairs,
         uint2 l = make_uint2(0, 0), r = make_uint2(0, 0);
         v3 nrm = mk3(0, 0, 0);
         float k1 = 0, k2 = 0, stiff = 0, c0 = 0, c2 = 0;
+        bool cand = false;
         if (p < n) {
             const uint2 pr = __ldg(&pairs[p]);
+            cand = !FILTER || static_candidate<true>(pr, x, reinterpret_cast<const uint32_t*>(edges), dhat, offset);
             l = __ldg(&edges[pr.x]);
             r = __ldg(&edges[pr.y]);
             const uint32_t bl = __ldg(&body[l.x]);
-            const bool skip =
-                l.x == r.x || l.x == r.y || l.y == r.x || l.y == r.y || (bl != kInvalid && bl == __ldg(&body[r.x]));
+            const bool skip = !cand || l.x == r.x || l.x == r.y || l.y == r.x || l.y == r.y ||
+                              (bl != kInvalid && bl == __ldg(&body[r.x]));
             if (!skip) {
                 const v3 ea0 = ld3(x, l.x), ea1 = ld3(x, l.y), eb0 = ld3(x, r.x), eb1 = ld3(x, r.y);
                 float c[4];
@@ -202,6 +242,7 @@ __global__ void __launch_bounds__(256) k_dcd_ee(const uint2* __restrict__ pairs,
                 }
             }
         }
+        if (FILTER) warp_append(d_cand_count, cand);
         const uint32_t s = warp_append(d_out_count, emit);
         if (emit && s < out_cap) write_pair(out, s, l.x, l.y, r.x, r.y | 0x80000000u, nrm, k1, k2, stiff, c0, c2);
     }
@@ -633,10 +674,10 @@ extern "C" int lcs_dcd_vf(const uint32_t* pairs, const uint32_t* d_count, uint32
         (capacity && !pairs) || (out_capacity && !out))
         return lcs_fail(LCS_ERR_INVALID, "lcs_dcd_vf: bad argument");
     if (capacity == 0) return LCS_OK;
-    k_dcd_vf<<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
+    k_dcd_vf<false><<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
         reinterpret_cast<const uint2*>(pairs), d_count, capacity, reinterpret_cast<const float4*>(x),
         reinterpret_cast<const uint4*>(faces), body, vert_area, face_area, d_hat, offset, kappa, out, out_capacity,
-        d_out_count);
+        d_out_count, nullptr);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
@@ -651,9 +692,40 @@ extern "C" int lcs_dcd_ee(const uint32_t* pairs, const uint32_t* d_count, uint32
         (capacity && !pairs) || (out_capacity && !out))
         return lcs_fail(LCS_ERR_INVALID, "lcs_dcd_ee: bad argument");
     if (capacity == 0) return LCS_OK;
-    k_dcd_ee<<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
+    k_dcd_ee<false><<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
         reinterpret_cast<const uint2*>(pairs), d_count, capacity, reinterpret_cast<const float4*>(x),
-        reinterpret_cast<const uint2*>(edges), body, edge_area, d_hat, offset, kappa, out, out_capacity, d_out_count);
+        reinterpret_cast<const uint2*>(edges), body, edge_area, d_hat, offset, kappa, out, out_capacity, d_out_count,
+        nullptr);
+    lcs_count_launch();
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+int lcs_dcd_vf_filtered(const uint32_t* ccd_pairs, const uint32_t* d_ccd_count, uint32_t capacity, const float* x,
+                        const uint32_t* faces, const uint32_t* body, const float* vert_area, const float* face_area,
+                        const float* d_hat, const float* offset, float kappa, lcs_pair* out, uint32_t out_capacity,
+                        uint32_t* d_out_count, uint32_t* d_cand_count, lcs_stream stream)
+{
+    if (capacity == 0) return LCS_OK;
+    k_dcd_vf<true><<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
+        reinterpret_cast<const uint2*>(ccd_pairs), d_ccd_count, capacity, reinterpret_cast<const float4*>(x),
+        reinterpret_cast<const uint4*>(faces), body, vert_area, face_area, d_hat, offset, kappa, out, out_capacity,
+        d_out_count, d_cand_count);
+    lcs_count_launch();
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+int lcs_dcd_ee_filtered(const uint32_t* ccd_pairs, const uint32_t* d_ccd_count, uint32_t capacity, const float* x,
+                        const uint32_t* edges, const uint32_t* body, const float* edge_area, const float* d_hat,
+                        const float* offset, float kappa, lcs_pair* out, uint32_t out_capacity, uint32_t* d_out_count,
+                        uint32_t* d_cand_count, lcs_stream stream)
+{
+    if (capacity == 0) return LCS_OK;
+    k_dcd_ee<true><<<grid_for(capacity, 256), 256, 0, (cudaStream_t)stream>>>(
+        reinterpret_cast<const uint2*>(ccd_pairs), d_ccd_count, capacity, reinterpret_cast<const float4*>(x),
+        reinterpret_cast<const uint2*>(edges), body, edge_area, d_hat, offset, kappa, out, out_capacity, d_out_count,
+        d_cand_count);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;

@@ -1614,7 +1614,11 @@ int newton_iteration(lcs_newton* h)
         mark(h, kPhDcdBroad);
         uint2* dvf = h->plain ? h->bp_vf : h->dcd_vf;
         uint2* dee = h->plain ? h->bp_ee : h->dcd_ee;
-        if (filter) {
+        // a single scene filters inside the DCD kernels (no candidate list in between)
+        const bool fused_dcd = filter && !h->batch;
+        if (fused_dcd) {
+            // lcs_dcd_*_filtered below read the previous CCD lists directly
+        } else if (filter) {
             if ((rc = h->rigid_scene_v ? dcd_mixed(h) : dcd_by_filter(h))) return rc;
         } else if ((rc = broad_phase(h, h->x, h->x, dvf, dee, &h->st->cnt[0], &h->st->cnt[1], nullptr))) {
             return rc;
@@ -1632,14 +1636,26 @@ int newton_iteration(lcs_newton* h)
             LCS_CUDA_TRY(cudaStreamWaitEvent(h->s2, h->fork, 0));
         }
         auto dcd_ee = [&](cudaStream_t st) {
+            if (fused_dcd)
+                return lcs_dcd_ee_filtered(reinterpret_cast<const uint32_t*>(h->bp_ee), h->prev_ccd + 1, h->cap_ee, X,
+                                           reinterpret_cast<const uint32_t*>(h->edges), h->body, h->edge_area, h->dhat,
+                                           h->offset, d.kappa, h->pairs, h->cap_pairs, &h->st->cnt[2],
+                                           &h->st->cnt[1], st);
             return lcs_dcd_ee(reinterpret_cast<uint32_t*>(dee), &h->st->cnt[1], h->cap_ee, X,
                               reinterpret_cast<const uint32_t*>(h->edges), h->body, h->edge_area, h->dhat, h->offset,
                               d.kappa, h->pairs, h->cap_pairs, &h->st->cnt[2], st);
         };
         if (dlanes && (rc = dcd_ee(h->s2))) return rc;
-        if ((rc = lcs_dcd_vf(reinterpret_cast<uint32_t*>(dvf), &h->st->cnt[0], h->cap_vf, X, reinterpret_cast<const uint32_t*>(h->faces), h->body, h->vert_area,
-                             h->face_area, h->dhat, h->offset, d.kappa, h->pairs, h->cap_pairs, &h->st->cnt[2], h->s)))
-            return rc;
+        if (fused_dcd)
+            rc = lcs_dcd_vf_filtered(reinterpret_cast<const uint32_t*>(h->bp_vf), h->prev_ccd, h->cap_vf, X,
+                                     reinterpret_cast<const uint32_t*>(h->faces), h->body, h->vert_area, h->face_area,
+                                     h->dhat, h->offset, d.kappa, h->pairs, h->cap_pairs, &h->st->cnt[2],
+                                     &h->st->cnt[0], h->s);
+        else
+            rc = lcs_dcd_vf(reinterpret_cast<uint32_t*>(dvf), &h->st->cnt[0], h->cap_vf, X,
+                            reinterpret_cast<const uint32_t*>(h->faces), h->body, h->vert_area, h->face_area, h->dhat,
+                            h->offset, d.kappa, h->pairs, h->cap_pairs, &h->st->cnt[2], h->s);
+        if (rc) return rc;
         if (!dlanes && (rc = dcd_ee(h->s))) return rc;  // the reference's order: VF pairs, then EE pairs
         if (dlanes) {
             LCS_CUDA_TRY(cudaEventRecord(h->join, h->s2));
