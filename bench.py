@@ -1,16 +1,19 @@
 #!/usr/bin/env python
 """Newton iterations/s on the 88,800-vertex twisted cloth tube.
 
-Workload: a 300 x 296 periodic tube (88,800 vertices, 177,000 faces, 265,800 edges), radius
-0.15 m, length 0.6 m, the two end rings pinned and rotated at -/+2 rad/s about the tube axis;
-dt = 1/100 s, d_hat = 1e-3 m, thickness 0, kappa = 1e9, 3 Newton iterations per step,
-Jacobi-PCG up to 100 iterations / relative residual 1e-4, CCD line search.  Synthetic, seeded
-geometry (no mesh file).  A bench step is one time step; the metric counts the Newton
-iterations those steps ran.  State stays on the GPU; the working set (~150 MB: BVHs,
-candidate lists, block matrix) is larger than L2 and L2 is also flushed between steps.
+Workload: a 300 x 296 periodic tube (88,800 vertices, 177,000 faces, 265,800 edges), radius 0.15 m,
+length 0.6 m, the two end rings pinned and rotated at -/+2 rad/s about the tube axis; dt = 1/100 s,
+d_hat = 1e-3 m, thickness 0, kappa = 1e9, 3 Newton iterations per step, Jacobi-PCG with at most
+100 iterations (stop at r.z < 1e-10 or |r| <= 1e-4 |r0|), CCD line search.  Synthetic, seeded geometry
+(no mesh file).  Every bench step is the same time step: the one after the state the run from rest
+reaches after FRAME steps (tests/golden/tube88k_state.npz, made on the CPU by the restatement of the
+Newton loop), loaded before the step outside the timed region.  The metric counts the Newton
+iterations those steps ran.  The working set (~150 MB: BVHs, candidate lists, block matrix) is larger
+than L2 and L2 is also flushed between steps.
 
---impl reference runs the CPU restatement of the same Newton iteration (the oracle, OpenMP on
-all host cores) on the tube at the state the 60-step run reaches (end rings at -/+1.2 rad).
+--impl reference runs the CPU restatement of the same time step (the oracle, OpenMP on all host cores)
+from the same state, with the same PCG stop rule.  --workload c1 is the small configuration: a 64 x 64
+cloth dropped onto a pinned 2,562-vertex icosphere, 10 steps from rest, timed as whole 10-step runs.
 """
 from __future__ import annotations
 
@@ -27,6 +30,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Newton iters/s at 88K-vert cloth"
+METRIC_C1 = "Newton iters/s, 64x64 cloth on a pinned icosphere (C1)"
 UNIT = "newton_iters/s"
 L2_BYTES = 126 * 1024 * 1024
 
@@ -48,13 +52,15 @@ def args_():
                    help="fast: DCD lists filtered from the previous iteration's CCD lists (same sets); "
                         "full: a traversal for every list")
     p.add_argument("--e2e-steps", type=int, default=10)
-    p.add_argument("--cpu-iters", type=int, default=0, help="CPU baseline sample (0: auto, ~10-30 s)")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--n-around", type=int, default=300)
-    p.add_argument("--n-along", type=int, default=296)
-    p.add_argument("--workload", choices=["tube", "batch", "serve"], default="tube",
-                   help="tube: the headline Newton iters/s line; batch: batched drape solves/s (256 scenes); "
-                        "serve: Poisson drape requests, p50/p99 latency and solves/s")
+    p.add_argument("--no-converged", action="store_true",
+                   help="tube: skip the second measurement with the PCG run to |r| <= 1e-4 |r0|")
+    p.add_argument("--converged-cap", type=int, default=2000,
+                   help="tube: PCG iteration cap of the converged measurement")
+    p.add_argument("--workload", choices=["tube", "c1", "batch", "serve"], default="tube",
+                   help="tube: the headline Newton iters/s line; c1: the small cloth-on-icosphere configuration; "
+                        "batch: batched drape solves/s (256 scenes); serve: Poisson drape requests, p50/p99 latency "
+                        "and solves/s")
     p.add_argument("--n-scenes", type=int, default=256, help="batch workload: cloth-on-sphere scenes")
     p.add_argument("--n-box-scenes", type=int, default=16,
                    help="batch workload: cloth scenes coupled with an affine rigid box (12 DOFs, 8 vertices)")
@@ -75,11 +81,36 @@ def dist_env():
     return rank, world, local
 
 
-def tube_config(a):
-    return {"workload": f"twisted tube {a.n_around}x{a.n_along} ({a.n_around * a.n_along} verts), 60-step run, "
-                        "rings -/+2 rad/s, dt 1/100, d_hat 1e-3, kappa 1e9, 3 Newton/step, PCG <=100 it rel 1e-4",
-            "verts": a.n_around * a.n_along, "dt": 0.01, "d_hat": 1e-3, "kappa": 1e9, "newton_per_step": 3,
-            "pcg": "Jacobi, max 100 iterations, rel 1e-4", "l2": "flushed between steps (256 MB write)"}
+PCG_RULE = "Jacobi-PCG, stop at r.z < 1e-10 or |r| <= 1e-4 |r0| (checked every iteration), at most {cap} iterations"
+
+
+def tube_config(frame, cap=100):
+    """The tube workload's config; both arms print the same dict."""
+    return {"workload": f"twisted tube 300x296 (88800 verts): the time step after step {frame} of the run from rest "
+                        "(rings -/+2 rad/s), the same state in every timed step and in both arms; dt 1/100, d_hat 1e-3, "
+                        f"kappa 1e9, 3 Newton/step, {PCG_RULE.format(cap=cap)}",
+            "verts": 88800, "frame": frame, "dt": 0.01, "d_hat": 1e-3, "kappa": 1e9, "newton_per_step": 3,
+            "pcg": PCG_RULE.format(cap=cap), "state": "tests/golden/tube88k_state.npz (CPU restatement run from rest)",
+            "l2": "flushed between steps (256 MB write)"}
+
+
+def c1_config():
+    return {"workload": "C1: 64x64 cloth (1 cm spacing, jitter seed 0) dropped from 5 cm onto a pinned 2562-vertex "
+                        "icosphere (r 0.2 m), 10 steps from rest per bench step; dt 1/60, d_hat 1e-3, kappa 1e7, "
+                        f"3 Newton/step, {PCG_RULE.format(cap=100)}",
+            "verts": 6658, "dt": 1.0 / 60.0, "d_hat": 1e-3, "kappa": 1e7, "newton_per_step": 3, "sim_steps": 10,
+            "pcg": PCG_RULE.format(cap=100), "l2": "working set (< 10 MB) fits L2; flushed between bench steps"}
+
+
+def _residual_summary(recs):
+    import numpy as np
+    rel = np.array([r["rel_residual"] for r in recs], np.float64)
+    it = np.array([r["pcg_iters"] for r in recs], np.float64)
+    if not len(rel):
+        return None
+    return {"solves": int(len(rel)), "rel_residual_p50": float(np.median(rel)), "rel_residual_max": float(rel.max()),
+            "pcg_iters_p50": float(np.median(it)), "pcg_iters_max": int(it.max()),
+            "converged_1e-4": int((rel <= 1e-4).sum())}
 
 
 # --------------------------------------------------------------------------- clocks sampling
@@ -148,61 +179,121 @@ def committed_traffic(kernel):
     return None
 
 
-# ------------------------------------------------------------------------------ CPU baseline
-def cpu_sample(a, iters=0, budget_s=20.0):
-    """Newton iterations/s of the oracle (CPU restatement) on the tube state of the 60-step run."""
-    import numpy as np
-
+# ------------------------------------------------------------------------------ CPU arm
+def cpu_tube_steps(budget_s=20.0, max_steps=0, warmup=1, cap=100):
+    """Newton iterations/s of the CPU restatement (oracle, OpenMP on all host cores) over whole time steps from
+    the tube state, every step from the same state; returns (value, summary)."""
     from oracle import newton_cpu as N
     from tests import scenarios as SC
-    sc, x = SC.twisted_tube_state(angle=1.2, n_around=a.n_around, n_along=a.n_along)
+    sc, x, v, frame = SC.tube_state()
     pat = N.MaterialPattern(sc)
-    xt = x.copy()
-    done, t0 = 0, time.perf_counter()
+    run = lambda: N.time_step(sc, x, v, frame, pattern=pat, pcg_max_iter=cap, pcg_check_every=1)  # noqa: E731
+    for _ in range(warmup):
+        run()
+    recs, el, steps = [], 0.0, 0
     while True:
-        x, toi, st, cnt = N.newton_iteration(sc, x, xt, sc.dt, pattern=pat)
-        done += 1
-        el = time.perf_counter() - t0
-        if (iters and done >= iters) or (not iters and (el > budget_s or done >= 20)):
+        t0 = time.perf_counter()
+        _, _, r = run()
+        el += time.perf_counter() - t0
+        recs += r
+        steps += 1
+        if (max_steps and steps >= max_steps) or (not max_steps and el > budget_s):
             break
-    cores = os.cpu_count()
-    return done / el, done, el, cores, np.float32(toi)
+    first = recs[0]
+    return len(recs) / el, {"steps": steps, "newton_iters": len(recs), "seconds": el, "frame": frame,
+                            "first_iteration": {k: first[k] for k in ("vf", "ee", "pairs")},
+                            "residuals": _residual_summary(recs)}
+
+
+def cpu_c1_runs(budget_s=15.0, max_runs=0, warmup=1):
+    """Newton iterations/s of the CPU restatement over whole 10-step C1 runs from rest."""
+    import numpy as np
+
+    from luisacomputesimulator_b200 import scenes
+    from oracle import newton_cpu as N
+    sc = scenes.cloth_on_sphere(n=64)
+    pat = N.MaterialPattern(sc)
+
+    def run():
+        x, v, out = sc.x.copy(), np.zeros_like(sc.x), []
+        for f in range(10):
+            x, v, r = N.time_step(sc, x, v, f, pattern=pat, pcg_check_every=1)
+            out += r
+        return out
+    for _ in range(warmup):
+        run()
+    recs, el, runs = [], 0.0, 0
+    while True:
+        t0 = time.perf_counter()
+        recs += run()
+        el += time.perf_counter() - t0
+        runs += 1
+        if (max_runs and runs >= max_runs) or (not max_runs and el > budget_s):
+            break
+    return len(recs) / el, {"runs": runs, "newton_iters": len(recs), "seconds": el,
+                            "residuals": _residual_summary(recs)}
 
 
 def run_reference(a):
+    """The reference arm: the CPU restatement of the reference's kernels on all host cores, the same workload,
+    metric and config as the GPU arm; each bench step is a bounded sample (whole time steps)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    import numpy as np
-
-    from oracle import newton_cpu as N
-    from tests import scenarios as SC
-    sc, x = SC.twisted_tube_state(angle=1.2, n_around=a.n_around, n_along=a.n_along)
-    pat = N.MaterialPattern(sc)
-    xt = x.copy()
-    for _ in range(a.warmup):
-        N.newton_iteration(sc, x, xt, sc.dt, pattern=pat)
-    # one bench step = one Newton iteration of the CPU restatement (a bounded sample of the
-    # 3-iteration time step); cap the timed count so the run ends within a few minutes
-    steps = min(a.steps, 40)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        x, toi, st, cnt = N.newton_iteration(sc, x, xt, sc.dt, pattern=pat)
-    el = time.perf_counter() - t0
-    v = steps / el
     cores = os.cpu_count()
-    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": steps, "warmup": a.warmup,
-            "ms_per_step": 1e3 * el / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic", "impl": "reference", "config": tube_config(a),
+    if a.workload == "c1":
+        v, info = cpu_c1_runs(budget_s=30.0, max_runs=min(a.steps, 20), warmup=min(a.warmup, 1))
+        cfg, metric = c1_config(), METRIC_C1
+        sample = f"{info['runs']} whole 10-step C1 runs ({info['newton_iters']} Newton iterations, {info['seconds']:.1f} s)"
+    else:
+        v, info = cpu_tube_steps(budget_s=30.0, max_steps=min(a.steps, 12), warmup=min(a.warmup, 1))
+        cfg, metric = tube_config(info["frame"]), METRIC
+        sample = (f"{info['steps']} time steps from the tube state ({info['newton_iters']} Newton iterations, "
+                  f"{info['seconds']:.1f} s)")
+    line = {"metric": metric, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": info.get("steps", info.get("runs")),
+            "warmup": min(a.warmup, 1), "ms_per_step": 1e3 * info["seconds"] / max(info.get("steps", info.get("runs")), 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference", "config": cfg,
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{steps} Newton iterations of the CPU restatement (oracle, OpenMP) on the "
-                                       "tube at its 60-step state; one bench step = one Newton iteration"},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                             "sample": sample + " of the CPU restatement of the reference's kernels (oracle, OpenMP, "
+                                                "all host cores); the reference's LuisaCompute build is unavailable"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "residuals": info["residuals"]}
+    if "first_iteration" in info:
+        line["first_iteration"] = info["first_iteration"]
+    if a.workload != "c1" and not a.no_converged:
+        vc, ic = cpu_tube_steps(budget_s=20.0, max_steps=2, warmup=0, cap=a.converged_cap)
+        line["converged_1e-4"] = {"value": vc, "unit": UNIT, "pcg": PCG_RULE.format(cap=a.converged_cap),
+                                  "steps": ic["steps"], "residuals": ic["residuals"]}
     print(json.dumps(line), flush=True)
-    _ = np
 
 
 # --------------------------------------------------------------------------------- our arm
+def _timed_tube_steps(solver, x4, v4, frame, steps, flush, stream, records=None):
+    """`steps` time steps, each from (x4, v4) at `frame` (loaded outside the timed region, L2 flushed), each timed
+    with CUDA events on the solver's stream; returns (device ms, Newton iterations, PCG iterations, per-step)."""
+    import torch
+    ms_total, newton, pcg, per = 0.0, 0, 0, []
+    for _ in range(steps):
+        solver.upload(x4, v4)
+        solver.set_frame(frame)
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = solver.step()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        per.append((ms, st.newton_iters, st.retries, st.host_ms))
+        ms_total += ms
+        newton += st.newton_iters
+        pcg += st.pcg_iters
+        if records is not None:
+            records += solver.iteration_log()
+    return ms_total, newton, pcg, per
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -214,70 +305,70 @@ def run_ours(a):
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    from luisacomputesimulator_b200 import _capi, scenes
+    from luisacomputesimulator_b200 import _capi
     from luisacomputesimulator_b200.newton import NewtonSolver
+    from tests import scenarios as SC
 
     lib = _capi.load()
     _capi.check(lib.lcs_device_check(local), "device check")
-    sc = scenes.twisted_tube(a.n_around, a.n_along)
-    solver = NewtonSolver(sc, plain=(a.mode == "plain"), fp64=a.fp64, profile=True, single_reduction=(a.pcg != "rows"),
-                          global_matrix=(a.pcg == "cg1-global"), full_traversal=(a.traversal == "full"))
+    sc, x4, v4, frame = SC.tube_state()
+    mk = lambda cap: NewtonSolver(sc, plain=(a.mode == "plain"), fp64=a.fp64, profile=True,  # noqa: E731
+                                  single_reduction=(a.pcg != "rows"), global_matrix=(a.pcg == "cg1-global"),
+                                  full_traversal=(a.traversal == "full"), pcg_max_iter=cap)
+    solver = mk(100)
     stream = torch.cuda.current_stream()
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
 
-    for _ in range(a.warmup):
-        solver.step()
+    _timed_tube_steps(solver, x4, v4, frame, a.warmup, flush, stream)
     torch.cuda.synchronize()
     solver.reset_profile()
     if world > 1:
         torch.distributed.barrier()
 
-    newton, pcg, ms_total = 0, 0, 0.0
-    per_step = []
+    recs = []
     launches0 = lib.lcs_launch_count()
     with Clocks(local) as clk:
-        for _ in range(a.steps):
-            flush.fill_(1.0)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            st = solver.step()
-            e1.record(stream)
-            e1.synchronize()
-            ms = e0.elapsed_time(e1)
-            per_step.append((ms, st.newton_iters, st.retries, st.host_ms))
-            ms_total += ms
-            newton += st.newton_iters
-            pcg += st.pcg_iters
+        ms_total, newton, pcg, per_step = _timed_tube_steps(solver, x4, v4, frame, a.steps, flush, stream, recs)
     launches = lib.lcs_launch_count() - launches0
     torch.cuda.synchronize()
     clocks = clk.summary()
     prof = solver.profile()
-    last = dict(vf=st.vf_candidates, ee=st.ee_candidates, pairs=st.contact_pairs, ccd_vf=st.ccd_vf_candidates,
-                ccd_ee=st.ccd_ee_candidates, last_toi=st.last_toi, last_rel_residual=st.last_rel_residual)
     cnt = solver.counts()
+    first = recs[0]
 
-    # end to end through the public host-buffer call (x, v in from pinned host, x, v out)
+    # end to end through the public host-buffer call: x, v in from pinned host memory, x, v out; every step
+    # from the same state (wall clock around the call, which synchronises)
     V = sc.num_verts
-    hx = torch.empty((V, 4), dtype=torch.float32).pin_memory()
-    hv = torch.empty((V, 4), dtype=torch.float32).pin_memory()
-    hx.numpy()[:] = solver.positions()
-    hv.numpy()[:] = solver.velocities()
-    e2e_ms, e2e_newton = 0.0, 0
-    for _ in range(a.e2e_steps):
+    hx_in = torch.empty((V, 4), dtype=torch.float32).pin_memory()
+    hv_in = torch.empty((V, 4), dtype=torch.float32).pin_memory()
+    hx_out = torch.empty((V, 4), dtype=torch.float32).pin_memory()
+    hv_out = torch.empty((V, 4), dtype=torch.float32).pin_memory()
+    hx_in.numpy()[:] = x4
+    hv_in.numpy()[:] = v4
+    e2e_s, e2e_newton = 0.0, 0
+    for k in range(a.e2e_steps + 1):
+        solver.set_frame(frame)
         flush.fill_(1.0)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        s2 = solver.step_host(hx.numpy(), hv.numpy(), hx.numpy(), hv.numpy())
-        e1.record(stream)
-        e1.synchronize()
-        e2e_ms += e0.elapsed_time(e1)
-        e2e_newton += s2.newton_iters
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s2 = solver.step_host(hx_in.numpy(), hv_in.numpy(), hx_out.numpy(), hv_out.numpy())
+        el = time.perf_counter() - t0
+        if k:  # the first call is a warm-up
+            e2e_s += el
+            e2e_newton += s2.newton_iters
+
+    conv = None
+    if not a.no_converged:  # the same steps with the PCG run to |r| <= 1e-4 |r0| (cap raised)
+        del solver
+        solver = mk(a.converged_cap)
+        _timed_tube_steps(solver, x4, v4, frame, 2, flush, stream)
+        crecs = []
+        cms, cnewton, cpcg, _ = _timed_tube_steps(solver, x4, v4, frame, min(a.steps, 10), flush, stream, crecs)
+        conv = {"value": cnewton / (cms / 1e3), "unit": UNIT, "pcg": PCG_RULE.format(cap=a.converged_cap),
+                "steps": min(a.steps, 10), "ms_per_step": cms / min(a.steps, 10), "residuals": _residual_summary(crecs)}
 
     # max over ranks of the time, sum of the work
     t_s = ms_total / 1e3
-    e2e_s = e2e_ms / 1e3
     if world > 1:
         import torch.distributed as dist
         tt = torch.tensor([t_s, e2e_s], device="cuda", dtype=torch.float64)
@@ -291,40 +382,43 @@ def run_ours(a):
 
     if rank == 0:
         value = newton_all / t_s
-        solver_uses_rows = solver.uses_row_pcg()
+        solver_uses_rows = a.mode == "fused" and solver.uses_row_pcg()
+        kind = solver.pcg_kind()
         pcg_kernel_name = {"cg1-res": "k_pcg_res (single-reduction slice-resident Jacobi-PCG)",
                            "cg1": "k_pcg_cg1 (single-reduction row-resident Jacobi-PCG)",
-                           "rows": "k_pcg_rows (row-resident Jacobi-PCG)"}[solver.pcg_kind()] if solver_uses_rows else \
+                           "rows": "k_pcg_rows (row-resident Jacobi-PCG)"}[kind] if solver_uses_rows else \
             ("k_pcg_fused (persistent Jacobi-PCG solve)" if a.mode == "fused" else "plain PCG kernels")
         # roofline of the dominant kernel: the persistent PCG solve (one launch per Newton iteration)
         pcg_ms, pcg_launches = prof["pcg"]
-        nnz = cnt["nnz_material"] + 12 * last["pairs"]
+        nnz = cnt["nnz_material"] + 12 * int(np.mean([r["contact_pairs"] for r in recs]))
         it_per_launch = pcg / max(pcg_launches, 1)
-        # algorithmic bytes of one PCG iteration: every matrix block once (36 B values + 4 B
-        # column), the diagonal blocks (48 B/row) and the exchanged direction written and read
-        # once (32 B/row) when the row state stays in registers (row-resident kernels); the
-        # CSR-vector kernel also streams r, z, p, q, x (312 B/row in all)
-        rows_kind = a.mode == "fused" and solver_uses_rows
-        bytes_per_iter = 40.0 * nnz + (80.0 if rows_kind else 312.0) * V
+        # algorithmic bytes of one PCG iteration: every matrix block once (36 B values + 4 B column), the
+        # diagonal blocks (48 B/row) and the exchanged direction written and read once (32 B/row) when the row
+        # state stays in registers (row-resident kernels); the CSR-vector kernel also streams r, z, p, q, x
+        # (312 B/row in all)
+        bytes_per_iter = 40.0 * nnz + (80.0 if solver_uses_rows else 312.0) * V
         bytes_per_launch = it_per_launch * bytes_per_iter + 160.0 * V
         achieved = bytes_per_launch / (pcg_ms / max(pcg_launches, 1) / 1e3) / 1e9
         peak, peak_kind = measured_peak()
         traffic = committed_traffic(pcg_kernel_name.split()[0])
         cpu = None
         if not a.no_cpu_baseline and world == 1:
-            v_cpu, n_cpu, el_cpu, cores, _ = cpu_sample(a, a.cpu_iters)
-            cpu = {"value": v_cpu, "unit": UNIT, "cores": cores, "kind": "port",
-                   "sample": f"{n_cpu} Newton iterations ({el_cpu:.1f} s) of the CPU restatement (oracle, OpenMP, "
-                             "all host cores) on the tube at its 60-step state"}
+            v_cpu, info = cpu_tube_steps(budget_s=15.0, warmup=0)
+            cpu = {"value": v_cpu, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"{info['steps']} time steps ({info['newton_iters']} Newton iterations, "
+                             f"{info['seconds']:.1f} s) of the CPU restatement (oracle, OpenMP, all host cores) from "
+                             "the same tube state"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms_total / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" + ("+f64 reductions" if a.fp64 else ""), "data": "synthetic (seeded tube mesh)",
-            "impl": "ours", "mode": a.mode, "pcg": solver.pcg_kind(), "traversal": a.traversal,
-            "config": {**tube_config(a), "parallelism": f"replicas x{world}" if world > 1 else "single scene"},
+            "impl": "ours", "mode": a.mode, "pcg_kernel": kind, "traversal": a.traversal,
+            "config": tube_config(frame),
+            "parallelism": f"replicas x{world}" if world > 1 else "single scene",
             "e2e": None if a.e2e_steps == 0 else {
                 "value": e2e_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * 16 * V,
-                "d2h_bytes_per_step": 2 * 16 * V, "steps": a.e2e_steps},
+                "d2h_bytes_per_step": 2 * 16 * V, "steps": a.e2e_steps,
+                "timing": "wall clock around lcs_newton_step_host (copies in, step, copies out, synchronise)"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": pcg_kernel_name,
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -335,17 +429,101 @@ def run_ours(a):
             "cpu_baseline": cpu,
             "clocks": clocks,
             "newton_iters": newton, "pcg_iters": pcg,
+            "residuals": _residual_summary(recs),
+            "first_iteration": {"vf": first["vf_candidates"], "ee": first["ee_candidates"],
+                                "pairs": first["contact_pairs"]},
+            "converged_1e-4": conv,
             "step_ms": {"min": min(p[0] for p in per_step), "median": statistics.median(p[0] for p in per_step),
                         "max": max(p[0] for p in per_step), "retries": sum(p[2] for p in per_step),
                         "host_ms_median": statistics.median(p[3] for p in per_step)},
             "phase_ms": {k: round(v[0], 3) for k, v in prof.items()},
-            "last_step": last,
+            "iterations_of_a_step": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in r.items()}
+                                     for r in recs[:per_step[0][1]]],
         }
         print(json.dumps(line), flush=True)
+    del solver
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
-    _ = np
+
+
+def run_c1(a):
+    """C1 as configured: whole 10-step runs of the 64x64 cloth onto the pinned icosphere, from rest."""
+    import numpy as np
+    import torch
+    from luisacomputesimulator_b200 import _capi, scenes
+    from luisacomputesimulator_b200.newton import NewtonSolver
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    lib = _capi.load()
+    _capi.check(lib.lcs_device_check(local), "device check")
+    sc = scenes.cloth_on_sphere(n=64)
+    solver = NewtonSolver(sc, single_reduction=True)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+    x0, v0 = sc.x.copy(), np.zeros_like(sc.x)
+
+    def run(records=None):
+        solver.upload(x0, v0)
+        solver.set_frame(0)
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        n = 0
+        for _ in range(10):
+            n += solver.step().newton_iters
+            if records is not None:
+                records += solver.iteration_log()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), n
+
+    for _ in range(a.warmup):
+        run()
+    recs, ms, newton = [], 0.0, 0
+    launches0 = lib.lcs_launch_count()
+    with Clocks(local) as clk:
+        for _ in range(a.steps):
+            m, n = run(recs)
+            ms += m
+            newton += n
+    launches = lib.lcs_launch_count() - launches0
+    clocks = clk.summary()
+    # end to end: host state in, ten steps through lcs_newton_step_host, state out each step
+    V = sc.num_verts
+    hx = torch.empty((V, 4), dtype=torch.float32).pin_memory()
+    hv = torch.empty((V, 4), dtype=torch.float32).pin_memory()
+    e2e_s, e2e_n = 0.0, 0
+    for k in range(min(a.steps, 5) + 1):
+        hx.numpy()[:] = x0
+        hv.numpy()[:] = v0
+        solver.set_frame(0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        n = 0
+        for _ in range(10):
+            n += solver.step_host(hx.numpy(), hv.numpy(), hx.numpy(), hv.numpy()).newton_iters
+        el = time.perf_counter() - t0
+        if k:
+            e2e_s += el
+            e2e_n += n
+    if rank == 0:
+        cpu = None
+        if not a.no_cpu_baseline:
+            v_cpu, info = cpu_c1_runs(budget_s=10.0, warmup=0)
+            cpu = {"value": v_cpu, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"{info['runs']} whole 10-step C1 runs ({info['newton_iters']} Newton iterations, "
+                             f"{info['seconds']:.1f} s) of the CPU restatement (oracle, OpenMP, all host cores)"}
+        line = {"metric": METRIC_C1, "value": newton / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded cloth grid, icosphere)", "impl": "ours",
+                "config": c1_config(),
+                "e2e": {"value": e2e_n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 10 * 2 * 16 * V,
+                        "d2h_bytes_per_step": 10 * 2 * 16 * V, "steps": min(a.steps, 5),
+                        "timing": "wall clock around ten lcs_newton_step_host calls"},
+                "gpu_launches": int(launches), "cpu_baseline": cpu, "clocks": clocks, "newton_iters": newton,
+                "residuals": _residual_summary(recs)}
+        print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------------------------- batching / serving
@@ -560,6 +738,8 @@ def main():
         return run_serve(a)
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "c1":
+        run_c1(a)
     else:
         run_ours(a)
 

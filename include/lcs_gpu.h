@@ -156,6 +156,23 @@ LCS_API int lcs_candidates_filter(int is_ee, const uint32_t* in_pairs, const uin
                                   uint32_t* out_count, lcs_stream stream);
 
 LCS_API int lcs_bvh_health(lcs_bvh* h, int* healthy, lcs_stream stream);
+/* fn_check_construction (lbvh.cpp:598-611), which lcs_bvh_construct runs after every build, run again on the
+ * tree as it is now: the healthy flag is set, then cleared when an inner node's child does not name it as
+ * its parent (or names a node outside the tree).  Read the flag with lcs_bvh_health. */
+LCS_API int lcs_bvh_check_construction(lcs_bvh* h, lcs_stream stream);
+
+/* Device buffers of the tree in the reference's LbvhData layout (lbvh.h:79-152: sa_parrent, sa_children,
+ * sa_morton_sorted, sa_sorted_get_original, sa_is_healthy), valid until the handle is destroyed.  A caller
+ * that writes into them must run lcs_bvh_check_construction before any refit or query. */
+typedef struct lcs_bvh_data_view {
+    uint32_t n_leaves;
+    uint32_t* parent;              /* 2 n - 1 */
+    uint32_t* children;            /* 2 (2 n - 1): uint2 per node */
+    uint64_t* morton_sorted;       /* n */
+    uint32_t* sorted_get_original; /* n */
+    uint32_t* is_healthy;          /* 1 */
+} lcs_bvh_data_view;
+LCS_API int lcs_bvh_data(const lcs_bvh* h, lcs_bvh_data_view* out);
 
 /* Copies the tree out in the reference's LbvhData layout (lbvh.h:79-152), for tests and
  * interop; any pointer may be NULL.  node_aabb: 8 floats per node {min.xyz, 0, max.xyz, 0};
@@ -331,17 +348,31 @@ LCS_API int lcs_pcg_solve(lcs_pcg* p, const float* diag, const lcs_bsr* A, const
                   const float* b, float* x, const lcs_pcg_opts* opts, lcs_pcg_stats* stats,
                   lcs_stream stream);
 LCS_API const lcs_pcg_stats* lcs_pcg_device_stats(const lcs_pcg* p);
+/* Test hook for failure detection (no counterpart in the reference, whose bounded wait is wait_for_write,
+ * lbvh.cpp:62-82): runs the slice-resident solve's reduction barrier (which = 0) or its neighbour-flag wait
+ * (which = 1) on `blocks` (2..32) co-resident blocks, each waiting for all others, with block missing_block
+ * (-1: none) never arriving or publishing.  Every wait gives up after spin_limit polls (1..2^24; the solves use
+ * 2^24).  Returns LCS_ERR_TIMEOUT when a wait ran out, LCS_OK when all completed.  No block waits forever and
+ * the context stays usable. */
+LCS_API int lcs_debug_pcg_wait(int32_t which, int32_t missing_block, uint32_t blocks, uint32_t spin_limit,
+                               lcs_stream stream);
 
 /* Allocation-free variant of lcs_pcg_solve (fused solve only); it has no counterpart in the
  * reference.  For callers that cannot allocate device memory while they run: cudaMalloc and
  * cudaFree synchronise the whole device, which a fixed-latency loop cannot afford, and a host
  * that gives all device memory to its own pool allocator leaves none to allocate.  Needs no
- * handle: the working vectors live in one static device array the library reserves when it is
- * loaded (7.3 MB per GPU, kept until the process exits).  At most 65,536 block rows (larger
- * systems: LCS_ERR_CAPACITY).  Calls on one device share that array, so calls whose work
- * overlaps on the GPU race and must be ordered by the caller.  The first call on each device
- * does a one-time set-up (it looks up the array's device address); make it before any stream
- * capture.  LCS_PCG_PLAIN is rejected. */
+ * handle: the working vectors live in one static device array (7.3 MB per GPU).  Under CUDA's
+ * default lazy module loading that array is reserved on a device the first time the library's
+ * PCG module is used there -- the first call of this function or the first launch of any PCG
+ * solve -- and kept until the process exits; make one call on each device before a pool takes
+ * its memory (if the memory is gone, the set-up fails with LCS_ERR_CAPACITY).  At most 65,536
+ * block rows (larger systems: LCS_ERR_CAPACITY).  Calls on one device share that array, so
+ * calls whose work overlaps on the GPU race and must be ordered by the caller.  The first call
+ * on each device does a one-time set-up (it looks up the array's device address and caches it
+ * for the process); make it before any stream capture, and do not call this function on a
+ * device after cudaDeviceReset.  opts NULL: the defaults of lcs_pcg_solve (100 iterations,
+ * rel 1e-4, r.z 1e-10, checked every 25).  LCS_PCG_PLAIN, LCS_PCG_ROWS and
+ * LCS_PCG_SINGLE_REDUCTION are rejected (LCS_ERR_INVALID). */
 LCS_API int lcs_pcg_solve_noalloc(uint32_t n, const float* diag, const lcs_bsr* A, const lcs_bsr* B,
                                   const float* b, float* x, const lcs_pcg_opts* opts, lcs_pcg_stats* stats,
                                   lcs_stream stream);
@@ -526,6 +557,17 @@ typedef struct lcs_newton_stats {
     int32_t ls_halvings; /* step halvings of the energy line search in this step */
 } lcs_newton_stats;
 
+/* One Newton iteration of the last step: the figures NewtonSolver::line_search logs per iteration
+ * (newton_solver.cpp:3770-3780; PCG iterations and error, precond_cg.cpp:763-768) and the iteration's
+ * direction norm (the small-step test, newton_solver.cpp:3784-3800). */
+typedef struct lcs_newton_iter_record {
+    int32_t pcg_iters;
+    float rel_residual; /* |r| / |r0| where the solve stopped */
+    float toi;          /* CCD step bound */
+    float max_dx;       /* max over the solve's unknowns of |dx| */
+    uint32_t vf_candidates, ee_candidates, contact_pairs, ccd_vf_candidates, ccd_ee_candidates;
+} lcs_newton_iter_record;
+
 typedef struct lcs_newton lcs_newton;
 /* NewtonSolver::init_solver (newton_solver.h:31-51): uploads the scene, builds the material
  * block pattern, allocates the contact buffers (CollisionData sizing, collision_data.h:445-485).
@@ -553,6 +595,9 @@ LCS_API int lcs_newton_last_iterate(const lcs_newton* h, float* x_iter_out, floa
 /* NewtonSolver::physics_step_GPU (newton_solver.cpp:4051-4345) on the device-resident state. */
 LCS_API int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats);
 /* The same step with host positions / velocities in and out (float4 per vertex, any may be NULL). */
+/* Per-iteration records of the last single-scene step (at most cap are written; *n_out = the number of
+ * iterations the step ran).  A batch reports none (*n_out = 0). */
+LCS_API int lcs_newton_iteration_log(const lcs_newton* h, lcs_newton_iter_record* out, int32_t cap, int32_t* n_out);
 LCS_API int lcs_newton_step_host(lcs_newton* h, const float* x_in, const float* v_in, float* x_out, float* v_out,
                                  lcs_newton_stats* stats);
 /* Copies the positions / velocities (float4 per vertex) to host buffers; either may be NULL.
@@ -569,6 +614,12 @@ LCS_API int lcs_newton_state(const lcs_newton* h, float** d_x, float** d_v);
 /* The positions changed outside the solver (through lcs_newton_state): the next step traverses the
  * trees for its first DCD lists instead of filtering the previous step's CCD lists. */
 LCS_API int lcs_newton_invalidate(lcs_newton* h);
+/* Sets the frame counter (scene_params.h:79 current_frame, advanced once per step by app_simulation.cpp:134):
+ * the next step animates the pinned vertices to time (frame + 1) * dt.  Used with lcs_newton_upload to
+ * resume from a saved frame state. */
+LCS_API int lcs_newton_set_frame(lcs_newton* h, uint32_t frame);
+/* The number of steps taken since creation or the last lcs_newton_set_frame plus the frame set there. */
+LCS_API int lcs_newton_get_frame(const lcs_newton* h, uint32_t* frame_out);
 /* Accumulated per-phase GPU time (LCS_NEWTON_PROFILE): build, material, DCD broad, DCD narrow,
  * assembly, PCG, CCD broad, CCD narrow, apply -- and how many times each ran. */
 LCS_API int lcs_newton_profile(const lcs_newton* h, double* phase_ms, int32_t* launches, int n);

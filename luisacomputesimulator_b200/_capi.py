@@ -77,6 +77,17 @@ class NewtonStats(C.Structure):
                 ("host_ms", C.c_float), ("last_alpha", C.c_float), ("ls_halvings", C.c_int32)]
 
 
+class BvhDataView(C.Structure):
+    _fields_ = [("n_leaves", C.c_uint32), ("parent", P), ("children", P), ("morton_sorted", P),
+                ("sorted_get_original", P), ("is_healthy", P)]
+
+
+class IterRecord(C.Structure):
+    _fields_ = [("pcg_iters", C.c_int32), ("rel_residual", C.c_float), ("toi", C.c_float), ("max_dx", C.c_float),
+                ("vf_candidates", C.c_uint32), ("ee_candidates", C.c_uint32), ("contact_pairs", C.c_uint32),
+                ("ccd_vf_candidates", C.c_uint32), ("ccd_ee_candidates", C.c_uint32)]
+
+
 class PcgStats(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("rel_residual", C.c_float), ("dot_rz", C.c_float),
                 ("status", C.c_int32)]
@@ -90,6 +101,9 @@ SIGNATURES = {
     "lcs_launch_count": (C.c_uint64, []),
     "lcs_bvh_create": (I32, [I32, U32, C.POINTER(P)]),
     "lcs_bvh_destroy": (I32, [P]),
+    "lcs_debug_pcg_wait": (I32, [I32, I32, U32, U32, P]),
+    "lcs_bvh_check_construction": (I32, [P, P]),
+    "lcs_bvh_data": (I32, [P, P]),
     "lcs_bvh_reduce_aabb": (I32, [P, P, P, U32, P]),
     "lcs_bvh_construct": (I32, [P, P]),
     "lcs_bvh_update_leaves": (I32, [P, P, P, P, P, P]),
@@ -152,6 +166,9 @@ SIGNATURES = {
     "lcs_newton_download": (I32, [P, P, P]),
     "lcs_newton_upload": (I32, [P, P, P]),
     "lcs_newton_invalidate": (I32, [P]),
+    "lcs_newton_set_frame": (I32, [P, U32]),
+    "lcs_newton_iteration_log": (I32, [P, P, I32, P]),
+    "lcs_newton_get_frame": (I32, [P, P]),
     "lcs_newton_profile": (I32, [P, C.POINTER(C.c_double), C.POINTER(C.c_int32), I32]),
     "lcs_newton_reset_profile": (I32, [P]),
     "lcs_newton_pcg_kind": (I32, [P]),

@@ -21,6 +21,14 @@ def ptr(t):
     return None if t is None else C.c_void_p(t.data_ptr())
 
 
+class _CudaArray:
+    """A device buffer of the library seen through __cuda_array_interface__ (no copy)."""
+
+    def __init__(self, ptr_, shape, typestr):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr_), False),
+                                         "version": 3, "strides": None}
+
+
 def stream():
     return C.c_void_p(torch.cuda.current_stream().cuda_stream)
 
@@ -139,6 +147,22 @@ class LBVH:
         ok = C.c_int(0)
         A.check(self.lib.lcs_bvh_health(self.h, C.byref(ok), stream()), "check_health")
         return bool(ok.value)
+
+    def check_construction(self):
+        """fn_check_construction (lbvh.cpp:598-611) on the tree as it is now; read the result with check_health."""
+        A.check(self.lib.lcs_bvh_check_construction(self.h, stream()), "check_construction")
+
+    def device_data(self):
+        """The tree's device buffers (LbvhData layout) as int32 / int64 CUDA tensor views of the unsigned data:
+        parent (2n-1,), children (2n-1, 2), morton_sorted (n,), sorted_get_original (n,).  Writing into them is
+        the caller's business; run check_construction before any refit or query."""
+        v = A.BvhDataView()
+        A.check(self.lib.lcs_bvh_data(self.h, C.byref(v)), "lcs_bvh_data")
+        n = int(v.n_leaves)
+        view = lambda p, shape, typestr: torch.as_tensor(_CudaArray(p, shape, typestr), device="cuda")  # noqa: E731
+        return {"parent": view(v.parent, (2 * n - 1,), "<i4"), "children": view(v.children, (2 * n - 1, 2), "<i4"),
+                "morton_sorted": view(v.morton_sorted, (n,), "<i8"),
+                "sorted_get_original": view(v.sorted_get_original, (n,), "<i4")}
 
     # -- queries (lbvh.cpp:1146-1192)
     def broad_phase_query_from_verts(self, x0, x1, count, pairs, d_hat, thickness):

@@ -271,11 +271,15 @@ __device__ __forceinline__ void emit_pairs(const uint2* hit, uint32_t nhit, uint
 __global__ void k_check(const uint2* __restrict__ children, const uint32_t* __restrict__ parent, uint32_t ni,
                         uint32_t* __restrict__ healthy)
 {
+    const uint32_t nodes = 2 * ni + 1;
     for (uint32_t nid = blockIdx.x * blockDim.x + threadIdx.x; nid < ni; nid += gridDim.x * blockDim.x) {
         uint2 c = children[nid];
-        if (parent[c.x] != nid || parent[c.y] != nid) *healthy = 0u;
+        // a child index outside the tree is unhealthy too (and is not followed)
+        if (c.x >= nodes || c.y >= nodes || parent[c.x] != nid || parent[c.y] != nid) *healthy = 0u;
     }
 }
+
+__global__ void k_set_healthy(uint32_t* healthy) { *healthy = 1u; }
 
 __device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v)
 {
@@ -833,6 +837,32 @@ extern "C" int lcs_bvh_health(lcs_bvh* h, int* healthy, lcs_stream stream)
     LCS_CUDA_TRY(cudaMemcpyAsync(&v, h->healthy, sizeof(uint32_t), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     LCS_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
     *healthy = (int)v;
+    return LCS_OK;
+}
+
+// fn_check_construction (lbvh.cpp:598-611) on the tree as it is now
+extern "C" int lcs_bvh_check_construction(lcs_bvh* h, lcs_stream stream)
+{
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_check_construction: null handle");
+    if (h->ni == 0) return LCS_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    k_set_healthy<<<1, 1, 0, s>>>(h->healthy);
+    lcs_count_launch();
+    k_check<<<grid_for(h->ni, 256), 256, 0, s>>>(h->children, h->parent, h->ni, h->healthy);
+    lcs_count_launch();
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+extern "C" int lcs_bvh_data(const lcs_bvh* h, lcs_bvh_data_view* out)
+{
+    if (!h || !out) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_data: null argument");
+    out->n_leaves = h->n;
+    out->parent = h->parent;
+    out->children = reinterpret_cast<uint32_t*>(h->children);
+    out->morton_sorted = h->ms64;
+    out->sorted_get_original = h->sgo;
+    out->is_healthy = h->healthy;
     return LCS_OK;
 }
 

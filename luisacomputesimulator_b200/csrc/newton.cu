@@ -1044,10 +1044,12 @@ struct lcs_newton {
     float* h_bsc = nullptr;         // pinned mirror
     lcs_pcg_stats *bpcg = nullptr, *h_bpcg = nullptr;
     std::vector<int32_t> sc_iters, sc_pcg;  // this step, per scene
+    std::vector<lcs_newton_iter_record> iter_log;  // this step's Newton iterations (single scene)
     std::vector<float> sc_toi, sc_rel;
     std::vector<uint8_t> sc_done;
     // bookkeeping
     double time = 0.0;
+    uint32_t frame = 0;
     int64_t total_newton = 0, total_pcg = 0;
     int32_t retries = 0;  // iterations re-run after growth, this step
     cudaEvent_t ev[kPhases + 1] = {};
@@ -2337,6 +2339,7 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
     h->filter_ok = h->carry_filter && !h->batch;
     h->carry_filter = false;
     h->time += d.dt;
+    h->frame += 1;
     if (h->plain) {  // physics_step_GPU uploads x_step_start, x and v from the host every step
         const size_t bytes = 16 * (size_t)V;
         LCS_CUDA_TRY(cudaMemcpyAsync(h->x_step, h->h_x, bytes, cudaMemcpyHostToDevice, h->s));
@@ -2443,11 +2446,14 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
     bool global_converged = false, dirichlet_converged = false;
     int iter = 0, pcg_total = 0;
     h->ls_halvings = 0;
+    h->iter_log.clear();
     float last_toi = 1.0f, last_rel = 0.0f;
     for (iter = 0; iter < 100; ++iter) {
         if (global_converged || (iter >= d.nonlinear_iters && dirichlet_converged)) break;
         if ((rc = newton_iteration(h))) return rc;
         const Status& s = *h->h_st;
+        h->iter_log.push_back(lcs_newton_iter_record{s.pcg_iters, s.pcg_rel, s.toi, s.max_dx, s.cnt[0], s.cnt[1],
+                                                     s.cnt[2], s.cnt[3], s.cnt[4]});
         pcg_total += s.pcg_iters;
         last_toi = s.toi;
         last_rel = s.pcg_rel;
@@ -2484,6 +2490,16 @@ extern "C" int lcs_newton_step(lcs_newton* h, lcs_newton_stats* stats)
         stats->host_ms =
             std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_host0).count();
     }
+    return LCS_OK;
+}
+
+extern "C" int lcs_newton_iteration_log(const lcs_newton* h, lcs_newton_iter_record* out, int32_t cap,
+                                        int32_t* n_out)
+{
+    if (!h || !n_out || (cap > 0 && !out)) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_iteration_log: null argument");
+    const int32_t n = (int32_t)h->iter_log.size();
+    for (int32_t k = 0; k < n && k < cap; ++k) out[k] = h->iter_log[k];
+    *n_out = n;
     return LCS_OK;
 }
 
@@ -2538,6 +2554,21 @@ extern "C" int lcs_newton_invalidate(lcs_newton* h)
 {
     if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_invalidate: null handle");
     h->carry_filter = false;
+    return LCS_OK;
+}
+
+extern "C" int lcs_newton_set_frame(lcs_newton* h, uint32_t frame)
+{
+    if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_set_frame: null handle");
+    h->frame = frame;
+    h->time = (double)frame * (double)h->d.dt;
+    return LCS_OK;
+}
+
+extern "C" int lcs_newton_get_frame(const lcs_newton* h, uint32_t* frame_out)
+{
+    if (!h || !frame_out) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_get_frame: null argument");
+    *frame_out = h->frame;
     return LCS_OK;
 }
 

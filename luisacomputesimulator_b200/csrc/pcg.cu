@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <vector>
 
 #include <mutex>
@@ -846,7 +847,7 @@ __device__ __forceinline__ void red_add_release(unsigned* p, unsigned v)
 // (read once at kernel start: no block can pass the first barrier before every block has arrived, so
 // all read the same value), which saves a round trip per barrier.  Bounded spin -> LCS_ERR_TIMEOUT.
 __device__ __forceinline__ bool pipe_barrier(unsigned* count, unsigned* gen, unsigned& gen_seen, lcs_pcg_stats* stats,
-                                             volatile int* s_fail)
+                                             volatile int* s_fail, unsigned spin_limit = kBarrierSpinLimit)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -856,7 +857,7 @@ __device__ __forceinline__ bool pipe_barrier(unsigned* count, unsigned* gen, uns
         } else {
             unsigned it = 0;
             while (ld_acquire(gen) == gen_seen) {
-                if (++it > kBarrierSpinLimit) {
+                if (++it > spin_limit) {
                     *s_fail = 1;
                     stats->status = LCS_ERR_TIMEOUT;
                     break;
@@ -1229,7 +1230,8 @@ __device__ __forceinline__ void st_release(unsigned* p, unsigned v)
 constexpr int kResFlagStride = 8;
 
 __device__ __forceinline__ bool res_publish_wait(unsigned* flags, unsigned tag, const unsigned* dep,
-                                                 lcs_pcg_stats* stats, volatile int* s_fail)
+                                                 lcs_pcg_stats* stats, volatile int* s_fail,
+                                                 unsigned spin_limit = kBarrierSpinLimit)
 {
     __syncthreads();
     const uint32_t t = threadIdx.x;
@@ -1238,7 +1240,7 @@ __device__ __forceinline__ bool res_publish_wait(unsigned* flags, unsigned tag, 
         const unsigned* f = flags + kResFlagStride * t;
         unsigned it = 0;
         while ((int)(ld_acquire(f) - tag) < 0) {
-            if (++it > kBarrierSpinLimit) {
+            if (++it > spin_limit) {
                 *s_fail = 1;
                 stats->status = LCS_ERR_TIMEOUT;
                 break;
@@ -1247,6 +1249,32 @@ __device__ __forceinline__ bool res_publish_wait(unsigned* flags, unsigned tag, 
     }
     __syncthreads();
     return *s_fail == 0;
+}
+
+// The two bounded waits of the slice-resident solve (the reduction barrier and the neighbour-flag wait)
+// with a wait that nothing satisfies: block `missing` neither arrives nor publishes, so every other block
+// must give up after spin_limit polls and report LCS_ERR_TIMEOUT (missing < 0: every block takes part and
+// the waits complete).  Each block waits for every other one.
+__global__ void k_wait_probe(int which, int missing, unsigned spin_limit, unsigned* count, unsigned* gen,
+                             unsigned* flags, lcs_pcg_stats* stats)
+{
+    __shared__ int s_fail;
+    __shared__ unsigned s_dep[kResDepWords];
+    if (threadIdx.x == 0) s_fail = 0;
+    for (uint32_t w = threadIdx.x; w < (uint32_t)kResDepWords; w += blockDim.x) {
+        unsigned m = 0u;
+        for (uint32_t b = 32 * w; b < 32 * w + 32 && b < gridDim.x; ++b)
+            if (b != blockIdx.x) m |= 1u << (b & 31u);
+        s_dep[w] = m;
+    }
+    __syncthreads();
+    if ((int)blockIdx.x == missing) return;
+    if (which == 0) {
+        unsigned gen_seen = threadIdx.x == 0 ? ld_acquire(gen) : 0u;
+        pipe_barrier(count, gen, gen_seen, stats, &s_fail, spin_limit);
+    } else {
+        res_publish_wait(flags, 1u, s_dep, stats, &s_fail, spin_limit);
+    }
 }
 
 template <int BT>
@@ -1704,6 +1732,49 @@ static constexpr int kPlainBlocks = 256;
 static constexpr int kRowMaxBlocks = 1024;
 static constexpr int kPcgNoResident = LCS_PCG_INTERNAL_NO_RESIDENT;
 
+extern "C" int lcs_debug_pcg_wait(int32_t which, int32_t missing_block, uint32_t blocks, uint32_t spin_limit,
+                                  lcs_stream stream)
+{
+    if (which != 0 && which != 1) return lcs_fail(LCS_ERR_INVALID, "lcs_debug_pcg_wait: which must be 0 or 1");
+    if (blocks < 2 || blocks > 32 || blocks > (uint32_t)kResMaxBlocks)
+        return lcs_fail(LCS_ERR_INVALID, "lcs_debug_pcg_wait: blocks must be in [2, 32]");
+    if (spin_limit == 0 || spin_limit > kBarrierSpinLimit)
+        return lcs_fail(LCS_ERR_INVALID, "lcs_debug_pcg_wait: spin_limit must be in [1, 2^24]");
+    if (missing_block >= (int32_t)blocks) return lcs_fail(LCS_ERR_INVALID, "lcs_debug_pcg_wait: no such block");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned* words = nullptr;  // count, gen, flags (kResFlagStride per block)
+    lcs_pcg_stats* st = nullptr;
+    const size_t n_words = 2 + (size_t)kResFlagStride * blocks;
+    LCS_CUDA_TRY(cudaMalloc(&words, 4 * n_words));
+    if (cudaMalloc(&st, sizeof(lcs_pcg_stats)) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(words);
+        return lcs_fail(LCS_ERR_CUDA, "lcs_debug_pcg_wait: cudaMalloc failed");
+    }
+    lcs_pcg_stats h{};
+    int rc = LCS_OK;
+    if (cudaMemsetAsync(words, 0, 4 * n_words, s) != cudaSuccess || cudaMemsetAsync(st, 0, sizeof(h), s) != cudaSuccess)
+        rc = LCS_ERR_CUDA;
+    unsigned* count = words;
+    unsigned* gen = words + 1;
+    unsigned* flags = words + 2;
+    void* args[] = {&which, &missing_block, &spin_limit, &count, &gen, &flags, &st};
+    if (rc == LCS_OK &&
+        cudaLaunchCooperativeKernel((const void*)k_wait_probe, dim3(blocks), dim3(128), args, 0, s) != cudaSuccess)
+        rc = LCS_ERR_CUDA;
+    if (rc == LCS_OK) lcs_count_launch();
+    if (rc == LCS_OK && (cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                         cudaStreamSynchronize(s) != cudaSuccess))
+        rc = LCS_ERR_CUDA;
+    const cudaError_t err = cudaGetLastError();
+    cudaFree(words);
+    cudaFree(st);
+    if (rc != LCS_OK) return lcs_fail(rc, cudaGetErrorString(err));
+    if (h.status == LCS_ERR_TIMEOUT)
+        return lcs_fail(LCS_ERR_TIMEOUT, "lcs_debug_pcg_wait: a bounded wait ran out (LCS_ERR_TIMEOUT)");
+    return h.status;
+}
+
 extern "C" int lcs_pcg_create(uint32_t n, lcs_pcg** out)
 {
     if (!out || n == 0) return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_create: bad argument");
@@ -2124,9 +2195,17 @@ extern "C" int lcs_pcg_solve(lcs_pcg* P, const float* diag, const lcs_bsr* A, co
 // the whole device, which a fixed-latency simulation loop cannot afford, and a host framework
 // that hands the whole GPU to its own pool allocator leaves nothing for a library to
 // cudaMalloc.  lcs_pcg_solve_noalloc runs the same persistent solve as lcs_pcg_solve, but its
-// working vectors live in one file-scope device array, g_pcg_scratch, reserved when the
-// library is loaded (7.3 MB on every GPU that loads it, held until the process exits), so it
-// needs no handle and allocates nothing.
+// working vectors live in one file-scope device array, g_pcg_scratch (7.3 MB), so it needs no
+// handle and allocates nothing itself.
+//
+// When the array's memory is taken: the device memory of a module's __device__ variables is
+// reserved when that module is loaded on a device.  Under CUDA's default lazy module loading
+// (CUDA_MODULE_LOADING=LAZY) that happens on the first use of this file's module on that device:
+// the first call of this entry point (its set-up takes the array's address) or the first launch
+// of any PCG kernel of the library, whichever comes first.  It is held until the process exits.
+// A caller that hands the device's memory to its own pool must therefore make one call (or use
+// any PCG entry point) on each device before the pool takes the memory; if the memory is gone
+// by then, the set-up reports LCS_ERR_CAPACITY.
 //
 // Limits and sharing rules:
 //  * at most kNoAllocMaxRows (65,536) block rows; larger systems are rejected with
@@ -2135,8 +2214,10 @@ extern "C" int lcs_pcg_solve(lcs_pcg* P, const float* diag, const lcs_bsr* A, co
 //    two calls whose work overlaps on the GPU (different streams, or different host threads)
 //    race on it and give wrong results, so the caller must order them;
 //  * the first call on each device resolves the array's device address with
-//    cudaGetSymbolAddress (host code cannot use the symbol itself as a pointer) and caches it;
-//    make that first call before any stream capture.
+//    cudaGetSymbolAddress (host code cannot use the symbol itself as a pointer) and caches it
+//    for the life of the process; make that first call before any stream capture.  The cache
+//    does not survive cudaDeviceReset (the address belongs to the old context): do not call
+//    this entry point on a device after resetting it.
 // ------------------------------------------------------------------------------------------
 constexpr uint32_t kNoAllocMaxRows = 65536;
 constexpr uint32_t kNoAllocMaxBlocks = 1024;
@@ -2168,9 +2249,10 @@ extern "C" int lcs_pcg_solve_noalloc(uint32_t n, const float* diag, const lcs_bs
         return lcs_fail(LCS_ERR_CAPACITY, "lcs_pcg_solve_noalloc: more than 65536 block rows (static scratch limit)");
     if ((A && A->n_rows != n) || (B && B->n_rows != n))
         return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_noalloc: row count mismatch");
-    lcs_pcg_opts o = opts ? *opts : lcs_pcg_opts{100, 1e-4f, 1e-10f, 1, 0};
-    if (o.flags & LCS_PCG_PLAIN)
-        return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_noalloc: only the fused solve is allocation-free");
+    lcs_pcg_opts o = opts ? *opts : lcs_pcg_opts{100, 1e-4f, 1e-10f, 25, 0};  // the defaults of lcs_pcg_solve
+    if (o.flags & (LCS_PCG_PLAIN | LCS_PCG_ROWS | LCS_PCG_SINGLE_REDUCTION))
+        return lcs_fail(LCS_ERR_INVALID, "lcs_pcg_solve_noalloc: only the fused solve is allocation-free "
+                                         "(LCS_PCG_PLAIN, LCS_PCG_ROWS and LCS_PCG_SINGLE_REDUCTION are rejected)");
     if (o.check_every <= 0) o.check_every = 1;
     int dev = 0;
     LCS_CUDA_TRY(cudaGetDevice(&dev));
@@ -2180,8 +2262,16 @@ extern "C" int lcs_pcg_solve_noalloc(uint32_t n, const float* diag, const lcs_bs
         std::lock_guard<std::mutex> lock(g_noalloc_mutex);
         if (!g_noalloc[dev].base) {  // one-time set-up on this device, with it current
             void* p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_pcg_scratch) != cudaSuccess || !p)
-                return lcs_fail(LCS_ERR_CUDA, "lcs_pcg_solve_noalloc: cudaGetSymbolAddress failed");
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_pcg_scratch);
+            if (e != cudaSuccess || !p) {
+                cudaGetLastError();  // do not leave the error for an unrelated later check to find
+                static thread_local char msg[256];
+                const bool oom = e == cudaErrorMemoryAllocation;
+                std::snprintf(msg, sizeof(msg), "lcs_pcg_solve_noalloc: set-up could not reserve the %zu-byte static "
+                              "scratch on device %d (cudaGetSymbolAddress: %s)%s", kNaBytes, dev,
+                              cudaGetErrorString(e), oom ? "; make the first call before a pool takes the memory" : "");
+                return lcs_fail(oom ? LCS_ERR_CAPACITY : LCS_ERR_CUDA, msg);
+            }
             int sms = 0, per_sm = 0;
             LCS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
             LCS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_fused<kRowLanes>, kFusedThreads, 0));

@@ -172,6 +172,24 @@ class NewtonSolver:
         q = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
         A.check(self.lib.lcs_newton_upload(self.h, q(xa), q(va)), "lcs_newton_upload")
 
+    def iteration_log(self):
+        """Per-iteration records of the last step: dicts of pcg_iters, rel_residual, toi, max_dx and the
+        DCD / CCD candidate and contact pair counts."""
+        cap = 128
+        recs = (A.IterRecord * cap)()
+        n = C.c_int32()
+        A.check(self.lib.lcs_newton_iteration_log(self.h, recs, cap, C.byref(n)), "lcs_newton_iteration_log")
+        return [{f: getattr(recs[k], f) for f, _ in A.IterRecord._fields_} for k in range(min(n.value, cap))]
+
+    def set_frame(self, frame):
+        """Frame counter (the reference's current_frame): the next step animates the pins to (frame + 1) dt."""
+        A.check(self.lib.lcs_newton_set_frame(self.h, int(frame)), "lcs_newton_set_frame")
+
+    def frame(self):
+        f = C.c_uint32()
+        A.check(self.lib.lcs_newton_get_frame(self.h, C.byref(f)), "lcs_newton_get_frame")
+        return int(f.value)
+
     def save_current_frame_state_to_host(self, path):
         """The reference's frame state file (positions, velocities, body q and q velocities) for this state."""
         from . import scene_io

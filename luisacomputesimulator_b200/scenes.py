@@ -127,6 +127,22 @@ class Scene:
         return out.astype(np.float32)
 
 
+def scaled_offset_d_hat(thickness, d_hat, min_rest_dist, rigid):
+    """Contact offset and d_hat of one mesh (init_collision_data.cpp:106-146, in float32 as there): offset =
+    thickness / 2; when offset + d_hat reaches the safe distance 0.9 x the mesh's smallest rest edge length /
+    triangle altitude, the offset is cut to half the safe distance and d_hat to what is left.  A rigid body's
+    safe distance is 1e8, which exempts it."""
+    f = np.float32
+    safe = f(1e8) if rigid else f(0.9) * f(min_rest_dist)
+    so, sd = f(0.5) * f(thickness), f(d_hat)
+    if not (so + sd < safe):
+        if so > f(0.5) * safe:
+            so = f(0.5) * safe
+        if sd > safe - so:
+            sd = safe - so
+    return float(so), float(sd)
+
+
 def _rotate(p, axis, ang):
     axis = np.asarray(axis, np.float64)
     axis = axis / np.linalg.norm(axis)
@@ -370,13 +386,7 @@ def assemble(name, parts, dt, gravity, kappa, spring_k=None, bending_k=5e-3, str
         vm = vmesh == m
         fe = faces[sel_f]
         emask = vm[edges[:, 0]]
-        safe = 0.9 * _min_rest_dist(x3, fe, edges[emask])
-        so, sd = 0.5 * part.thickness, part.d_hat
-        if not (so + sd < safe):
-            if so > 0.5 * safe:
-                so = 0.5 * safe
-            if sd > safe - so:
-                sd = safe - so
+        so, sd = scaled_offset_d_hat(part.thickness, part.d_hat, _min_rest_dist(x3, fe, edges[emask]), part.rigid)
         d_hat[vm] = sd
         offset[vm] = so
         # vertex mass = vertex volume / body volume x body mass, shell volumes = area x thickness

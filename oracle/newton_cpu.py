@@ -128,8 +128,14 @@ def material_system(sc, x, x_tilde, dt):
     return material_fill(sc, MaterialPattern(sc), x, x_tilde, dt)
 
 
-def newton_iteration(sc, x, x_tilde, dt, timings=None, pattern=None):
-    """One CPU Newton iteration from positions x; returns (new x, toi, pcg stats, counts)."""
+def newton_iteration(sc, x, x_tilde, dt, timings=None, pattern=None, pcg_max_iter=100, pcg_rel_tol=1e-4,
+                     pcg_check_every=25, info=None):
+    """One CPU Newton iteration from positions x; returns (new x, toi, pcg stats, counts).
+
+    The PCG stops at pcg_max_iter iterations, or when r.z < 1e-10 or |r| <= pcg_rel_tol |r0| at an
+    iteration that is a multiple of pcg_check_every (the reference checks r.z every 25 iterations,
+    precond_cg.cpp:681-755).  ``info`` (a dict), when given, receives the direction ``dx`` and the
+    iterate ``x_iter`` the step bound was taken on."""
     t = {} if timings is None else timings
     c0 = time.perf_counter()
     if pattern is None:
@@ -154,7 +160,8 @@ def newton_iteration(sc, x, x_tilde, dt, timings=None, pattern=None):
         b, diag = O.contact_grad_diag(pairs, sc.num_verts, b, diag)
         B = O.contact_offdiag_bsr(pairs, sc.num_verts)
     c3 = time.perf_counter()
-    dx, st = O.pcg(diag, A, B, b, max_iter=100, rel_tol=1e-4, abs_rz_tol=1e-10, check_every=25)
+    dx, st = O.pcg(diag, A, B, b, max_iter=pcg_max_iter, rel_tol=pcg_rel_tol, abs_rz_tol=1e-10,
+                   check_every=pcg_check_every)
     c4 = time.perf_counter()
     dx = affine_expand(sc, dx)
     x1 = x.copy()
@@ -174,4 +181,118 @@ def newton_iteration(sc, x, x_tilde, dt, timings=None, pattern=None):
     for k, v in dict(material=c1 - c0, dcd_broad=c2 - c1, dcd_narrow_assembly=c3 - c2, pcg=c4 - c3,
                      ccd=c5 - c4).items():
         t[k] = t.get(k, 0.0) + v
+    if info is not None:
+        info.update(dx=dx, x_iter=x, ccd_vf=len(cvf), ccd_ee=len(cee))
     return out, toi, st, dict(vf=n_vf, ee=n_ee, pairs=len(pairs))
+
+
+# ------------------------------------------------------------------------------------ time step
+_F = np.float32
+
+
+def pinned_targets(sc, t):
+    """Targets of the animated pinned vertices at time t (float32), in the order of the device's
+    k_targets: scale, rotation about an axis through a centre (Rodrigues), translation
+    (WorldData::get_fixed_point_target_positions, Solver/Initializer/init_mesh_data.cpp:272-297).
+    cos/sin are numpy's float32 functions, which may differ from CUDA's cosf/sinf in the last bit."""
+    p = sc.x[:, :3].astype(np.float32).copy()
+    t = _F(t)
+    for an in sc.anims:
+        vids, center, axis, omega = an[:4]
+        translate, scale, mode = (an[4], an[5], an[6]) if len(an) > 4 else (None, None, 1)
+        q = p[vids]
+        if mode & 2:
+            q = (np.asarray(scale, np.float32) * t) * q
+        if mode & 1:
+            ax = np.asarray(axis, np.float64)
+            n = np.linalg.norm(ax)
+            ax = (ax / n if n > 0 else ax).astype(np.float32)
+            c3 = np.asarray(center, np.float32)
+            ang = _F(omega) * t
+            c, s = np.cos(ang, dtype=np.float32), np.sin(ang, dtype=np.float32)
+            px, py, pz = q[:, 0] - c3[0], q[:, 1] - c3[1], q[:, 2] - c3[2]
+            d = (ax[0] * px + ax[1] * py) + ax[2] * pz
+            kx, ky, kz = ax[1] * pz - ax[2] * py, ax[2] * px - ax[0] * pz, ax[0] * py - ax[1] * px
+            omc = _F(1.0) - c
+            q = np.stack([((c3[0] + px * c) + kx * s) + (ax[0] * d) * omc,
+                          ((c3[1] + py * c) + ky * s) + (ax[1] * d) * omc,
+                          ((c3[2] + pz * c) + kz * s) + (ax[2] * d) * omc], 1).astype(np.float32)
+        if mode & 4:
+            q = q + np.asarray(translate, np.float32) * t
+        p[vids] = q
+    return p
+
+
+def step_time(frame, dt):
+    """The time the step after `frame` steps animates to: the device keeps a double clock advanced by the
+    float dt at the start of every step and passes it to the targets as a float."""
+    return np.float32(frame * float(np.float32(dt)) + float(np.float32(dt)))
+
+
+def predict(sc, x, v, t):
+    """fn_predict_position (Solver/SimulationSolver/newton_solver.cpp:576-604) with the pinned vertices'
+    velocity set towards their targets (physics_step_prev_operation, solver_interface.cpp:130-162):
+    returns (x_tilde, v) as float32 (V, 4)."""
+    dt = _F(sc.dt)
+    g = np.asarray(sc.gravity, np.float32)
+    v = v.astype(np.float32).copy()
+    pin = sc.pinned.astype(bool)
+    tg = pinned_targets(sc, t)
+    v[pin, :3] = (tg[pin] - x[pin, :3]) / dt
+    vp = v[:, :3] + dt * g
+    vp[pin] = v[pin, :3]
+    xt = x.astype(np.float32).copy()
+    xt[:, :3] = x[:, :3] + dt * vp
+    xt[:, 3] = 0.0
+    return xt, v
+
+
+def floor_ccd(x0, x1, offset, pinned, floor_y):
+    """fn_gound_collision_ccd (Solver/SimulationSolver/newton_solver.cpp:952-1000): every free vertex whose
+    end position minus its offset lies below the floor bounds the step by
+    (y0 - offset - floor_y) / (y0 - y1) / 1.25 (accd::line_search_max_t); the minimum of those, 1 when none."""
+    f = np.float32
+    off = np.asarray(offset, f)
+    y0, y1 = x0[:, 1].astype(f), x1[:, 1].astype(f)
+    sel = ~np.asarray(pinned, bool) & ((y1 - off) < f(floor_y))
+    if not sel.any():
+        return 1.0
+    toi = ((y0[sel] - off[sel]) - f(floor_y)) / (y0[sel] - y1[sel]) / f(1.25)
+    return float(toi.min())
+
+
+def time_step(sc, x, v, frame, pattern=None, nonlinear_iters=3, pcg_max_iter=100, pcg_rel_tol=1e-4,
+              pcg_check_every=25, damping=2.0, log=None):
+    """One time step of NewtonSolver::physics_step_GPU (newton_solver.cpp:4152-4297) for soft scenes
+    without a floor: predict, Newton iterations until the direction is small (max |dx| < 1e-2 dt) or,
+    after `nonlinear_iters` iterations, the pinned vertices are within 1e-3 of their targets
+    (line_search, newton_solver.cpp:3784-3880), then the damped velocity update
+    (fn_update_velocity, newton_solver.cpp:606-633).  Returns (x, v, per-iteration records)."""
+    if sc.num_bodies:
+        raise ValueError("time_step: affine bodies are not restated here")
+    pat = pattern if pattern is not None else MaterialPattern(sc)
+    dt = _F(sc.dt)
+    x = x.astype(np.float32).copy()
+    x_step = x.copy()
+    xt, v = predict(sc, x, v, step_time(frame, sc.dt))
+    pin = sc.pinned.astype(bool)
+    recs = [] if log is None else log
+    glob = dirich = False
+    for it in range(100):
+        if glob or (it >= nonlinear_iters and dirich):
+            break
+        info = {}
+        x, toi, st, cnt = newton_iteration(sc, x, xt, dt, pattern=pat, pcg_max_iter=pcg_max_iter,
+                                           pcg_rel_tol=pcg_rel_tol, pcg_check_every=pcg_check_every, info=info)
+        d = info["dx"][:, :3]
+        max_dx = float(np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]).max(initial=0.0))
+        e = x[pin, :3] - xt[pin, :3]
+        dirichlet = float(np.sqrt((e[:, 0] * e[:, 0] + e[:, 1] * e[:, 1]) + e[:, 2] * e[:, 2]).max(initial=0.0))
+        glob = max_dx < float(_F(1e-2) * dt)
+        dirich = dirichlet < 1e-3
+        recs.append(dict(toi=float(toi), pcg_iters=st["iterations"], rel_residual=st["rel_residual"],
+                         max_dx=max_dx, dirichlet=dirichlet, ccd_vf=info["ccd_vf"], ccd_ee=info["ccd_ee"], **cnt))
+    f = np.exp(_F(-damping) * dt, dtype=np.float32)
+    v = np.zeros_like(x)
+    v[:, :3] = (x[:, :3] - x_step[:, :3]) / dt * f
+    return x, v, recs

@@ -1,7 +1,7 @@
 """Extracts the reference's own known answers for the contact path into
 reference_known_answers.json.
 
-Run where the reference sources are mounted (REFERENCE_ROOT, default /root/reference); the
+Run where the reference sources are mounted, with REFERENCE_ROOT naming the reference project's root; the
 committed JSON is what the tests read, so they run without the reference.  Sources read:
   Solver/CollisionDetector/lbvh.cpp         LBVH::unit_test answers (Morton codes) and the
                                             expected ranges / splits / children / parents
@@ -15,7 +15,7 @@ import os
 import re
 import sys
 
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("REFERENCE_ROOT", "")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_known_answers.json")
 
 
@@ -34,6 +34,8 @@ def _vec3(src, name):
 
 
 def main():
+    if not REF or not os.path.isdir(REF):
+        sys.exit("set REFERENCE_ROOT to the reference project's root")
     lbvh = _read("Solver/CollisionDetector/lbvh.cpp")
     m32 = re.search(r"answer_morton32\s*=\s*\{([^}]*)\}", lbvh)
     m64 = re.search(r"answer_morton64\s*=\s*\{([^}]*)\}", lbvh)

@@ -1,6 +1,8 @@
 """Seeded contact configurations for the parity tests (positions only; meshes from scenes.py)."""
 from __future__ import annotations
 
+import os
+
 import numpy as np
 
 from luisacomputesimulator_b200 import scenes as S
@@ -48,6 +50,21 @@ def twisted_tube_state(angle=1.2, n_around=300, n_along=296):
     x[:, 1] = (c * y - s * z).astype(np.float32)
     x[:, 2] = (s * y + c * z).astype(np.float32)
     return sc, x
+
+
+TUBE_STATE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "tube88k_state.npz")
+
+
+def tube_state(path=TUBE_STATE):
+    """Config-2 tube (300 x 296) at the state its run from rest reaches after `frame` steps, stepped by the
+    CPU restatement (tests/golden/make_tube_state.py): (scene, x (V, 4), v (V, 4), frame), float32."""
+    z = np.load(path)
+    sc = S.twisted_tube(300, 296)
+    x = sc.x.copy()
+    x[:, :3] = z["x"]
+    v = np.zeros_like(x)
+    v[:, :3] = z["v"]
+    return sc, x, v, int(z["frame"])
 
 
 def sorted_pairs(p):

@@ -137,3 +137,72 @@ def test_first_iteration_dcd_lists_filtered_across_steps_equal_a_traversal():
         assert st.contact_pairs == pairs
         checked += 1
     assert checked >= 4
+
+
+@pytest.mark.parametrize("plain", [True, False])
+def test_c1_ten_steps_follow_the_cpu_restatement(plain):
+    """Config 1 as configured (64 x 64 cloth dropped from 5 cm onto the pinned 2,562-vertex icosphere, dt 1/60,
+    10 steps from rest).  Every GPU step is compared with the CPU restatement's time step from the same state
+    (the GPU's state before the step): the first iteration's DCD candidates and contact pairs are equal (same
+    positions), the Newton iteration counts are equal, and the new positions agree within 2 % of the step's motion
+    (the PCG solves run to 1e-4 or to the 100-iteration cap, where FP32 rounding of different summation orders
+    separates the iterates); the cloth stays intersection-free."""
+    sc = S.cloth_on_sphere(n=64)
+    gpu = NewtonSolver(sc, plain=plain, single_reduction=not plain)
+    pat = N.MaterialPattern(sc)
+    worst = 0.0
+    touched = 0
+    for k in range(10):
+        xk, vk = gpu.positions(), gpu.velocities()
+        st = gpu.step()
+        assert st.status == 0
+        log = gpu.iteration_log()
+        xg = gpu.positions()
+        xo, vo, recs = N.time_step(sc, xk, vk, k, pattern=pat, pcg_check_every=25 if plain else 1)
+        assert (log[0]["vf_candidates"], log[0]["ee_candidates"], log[0]["contact_pairs"]) == \
+            (recs[0]["vf"], recs[0]["ee"], recs[0]["pairs"])
+        assert len(log) == len(recs)
+        touched += log[0]["contact_pairs"] > 0
+        motion = float(np.abs(xo[:, :3] - xk[:, :3]).max())
+        dev_ = float(np.abs(xg[:, :3] - xo[:, :3]).max()) / motion
+        worst = max(worst, dev_)
+        assert dev_ <= 2e-2, (k, dev_)
+        if k % 5 == 4:
+            assert O.min_distance(sc, xg) > 0.0
+    print(f"C1 ({'plain' if plain else 'fused'}): largest deviation {worst:.2e} of the step's motion; "
+          f"{touched} steps with contact pairs")
+    assert touched >= 2  # the cloth reached the sphere
+
+
+def test_floor_ccd_bounds_the_step_like_the_reference():
+    """fn_gound_collision_ccd: a cloth falling fast onto the floor (floor on, y = 0).  The step bound of the GPU's
+    iteration equals the reference rule evaluated by the oracle on the GPU's own iterate and direction."""
+    cx, cf = S.cloth_grid(32, 32, 0.01, origin=(0.0, 0.01, 0.0), jitter=1e-4, seed=3)
+    sc = S.assemble("cloth_over_floor", [S.MeshPart(cx, cf, np.zeros(cx.shape[0], bool))], dt=1 / 60,
+                    gravity=(0, -9.8, 0), kappa=1e7)
+    v = np.zeros_like(sc.x)
+    v[:, 1] = -2.0
+    for plain in (False, True):
+        gpu = NewtonSolver(sc, plain=plain, single_reduction=not plain, use_floor=True, floor_y=0.0,
+                           nonlinear_iters=1)
+        gpu.upload(sc.x, v)
+        st = gpu.step()
+        assert st.status == 0
+        x_iter, dx, _ = gpu.last_iterate()
+        x1 = x_iter.copy()
+        x1[:, :3] = x_iter[:, :3] + dx[:, :3]
+        floor = N.floor_ccd(x_iter, x1, sc.offset, sc.pinned, 0.0)
+        assert floor < 1.0  # the unconstrained direction goes through the floor
+        tf = O.lbvh_build(O.TREE_FACE, x_iter, sc.faces, sc.num_verts)
+        te = O.lbvh_build(O.TREE_EDGE, x_iter, sc.edges, sc.num_verts)
+        O.lbvh_refit(tf, x_iter, x1, sc.faces, sc.offset)
+        O.lbvh_refit(te, x_iter, x1, sc.edges, sc.offset)
+        cvf, _ = O.lbvh_query_vf(tf, x_iter, x1, sc.d_hat, sc.offset)
+        cee, _ = O.lbvh_query_ee(te, x_iter, x1, sc.edges, sc.d_hat, sc.offset)
+        g1, _ = O.ccd_vf(cvf, x_iter, x1, sc.faces, sc.body, sc.offset, per_pair=False)
+        g2, _ = O.ccd_ee(cee, x_iter, x1, sc.edges, sc.body, sc.offset, per_pair=False)
+        want = min(floor, g1, g2)
+        got = gpu.iteration_log()[-1]["toi"]
+        assert got <= want and abs(got - want) <= 1e-6 * want, (plain, got, want)
+        x = gpu.positions()
+        assert (x[:, 1] - sc.offset > 0.0).all()  # nothing below the floor

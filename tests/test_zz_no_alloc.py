@@ -57,3 +57,43 @@ def test_noalloc_rejects_systems_above_its_limit():
                            A.PcgOpts(10, 1e-4, 1e-10, 1, 0))
     assert rc == 3  # LCS_ERR_CAPACITY
     assert b"65536" in A.load().lcs_last_error()
+
+
+def test_noalloc_call_allocates_no_device_memory():
+    sc, diag_h, Ah, Bh, b_h = contact_system()
+    n = sc.num_verts
+    diag, b = dev(diag_h), dev(b_h)
+    Ab = make_bsr(n, dev(Ah[0]), dev(Ah[1]), dev(Ah[2]))
+    Bb = make_bsr(n, dev(Bh[0]), dev(Bh[1]), dev(Bh[2]))
+    x = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    opts = A.PcgOpts(300, 1e-4, 1e-10, 1, 0)
+    assert _solve_noalloc(n, diag, Ab, Bb, b, x, opts)[0] == 0  # set-up call
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        assert _solve_noalloc(n, diag, Ab, Bb, b, x, opts)[0] == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
+def test_noalloc_defaults_and_rejected_flags_follow_the_regular_solve():
+    sc, diag_h, Ah, Bh, b_h = contact_system()
+    n = sc.num_verts
+    diag, b = dev(diag_h), dev(b_h)
+    Ab = make_bsr(n, dev(Ah[0]), dev(Ah[1]), dev(Ah[2]))
+    Bb = make_bsr(n, dev(Bh[0]), dev(Bh[1]), dev(Bh[2]))
+    lib = A.load()
+    # opts NULL: the regular solve's defaults (100 iterations, checks every 25)
+    x0 = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    x1 = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    s0, s1 = A.PcgStats(), A.PcgStats()
+    solver = ConjugateGradientSolver(n)
+    assert lib.lcs_pcg_solve(solver.h, ptr(diag), C.byref(Ab), C.byref(Bb), ptr(b), ptr(x0), None, C.byref(s0),
+                             stream()) == 0
+    assert lib.lcs_pcg_solve_noalloc(n, ptr(diag), C.byref(Ab), C.byref(Bb), ptr(b), ptr(x1), None, C.byref(s1),
+                                     stream()) == 0
+    assert s1.iterations == s0.iterations and s1.iterations % 25 == 0
+    for flag in (A.LCS_PCG_PLAIN, A.LCS_PCG_ROWS, A.LCS_PCG_SINGLE_REDUCTION):
+        rc, _ = _solve_noalloc(n, diag, Ab, Bb, b, x1, A.PcgOpts(100, 1e-4, 1e-10, 1, flag))
+        assert rc == 1  # LCS_ERR_INVALID
