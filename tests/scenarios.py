@@ -52,6 +52,33 @@ def twisted_tube_state(angle=1.2, n_around=300, n_along=296):
     return sc, x
 
 
+def deep_tree_elements(kind, dup_top=8):
+    """Elements whose sorted Morton codes make an LBVH with inner nodes deeper than 32 levels, where the
+    reference's 32-entry traversal stack can fill up: for every bit k of the 30-bit code, two elements whose
+    code has every bit but k set (each such pair becomes an inner node to the left of all larger codes, so a
+    traversal keeps one pending node per level), `dup_top` elements at the all-ones code and one at code 0.
+    The elements at code 0 and at the top reach the corners 0 and 1024 of the global box, so a centre
+    quantises to the integer part of its coordinates.  kind "face": degenerate triangles, kind "edge":
+    degenerate edges.  Returns (x (V, 4) float32, elements (n, 4 | 2) uint32)."""
+    m = 3 if kind == "face" else 2
+    elems = []
+    for k in range(30):
+        axis, bit = 2 - k % 3, k // 3  # Morton bit 3 j + 2 is x bit j, 3 j + 1 is y bit j, 3 j is z bit j
+        c = np.full(3, 1023.5)
+        c[axis] -= 2 ** bit
+        elems += [[c - 0.25, c + 0.25, c][:m]] * 2
+    top = np.full(3, 1023.5)
+    elems.append([top - 0.5, top + 0.5, top][:m])  # reaches 1024
+    elems += [[top - 0.25, top + 0.25, top][:m]] * (dup_top - 1)
+    elems.append([np.zeros(3), np.ones(3), np.full(3, 0.5)][:m])  # reaches 0
+    x = np.zeros((len(elems) * m, 4), np.float32)
+    x[:, :3] = np.asarray([v for e in elems for v in e], np.float64).astype(np.float32)
+    el = np.arange(len(elems) * m, dtype=np.uint32).reshape(-1, m)
+    if kind == "face":  # faces are stored as uint4 (the layout of Buffer<uint3>)
+        el = np.concatenate([el, np.zeros((len(el), 1), np.uint32)], 1)
+    return x, el
+
+
 TUBE_STATE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "tube88k_state.npz")
 
 

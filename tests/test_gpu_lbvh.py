@@ -23,6 +23,9 @@ def _scene(name):
         return SC.folded_cloth(n=48, gap=4e-4)
     if name == "tube":
         return SC.twisted_tube_state(angle=1.2)
+    if name == "tube_state":  # the benchmarked state: 56 steps of the run from rest
+        sc, x, _, _ = SC.tube_state()
+        return sc, x
     raise KeyError(name)
 
 
@@ -80,7 +83,7 @@ def test_refit_bit_exact(scene, kind_name, fused):
     np.testing.assert_array_equal(got[:, 4:7], t_o.node_aabb[:, 4:7])
 
 
-@pytest.mark.parametrize("scene", ["cloth_sphere", "folded", "tube"])
+@pytest.mark.parametrize("scene", ["cloth_sphere", "folded", "tube", "tube_state"])
 @pytest.mark.parametrize("swept", [False, True])
 def test_candidate_sets_bit_exact(scene, swept):
     sc, x = _scene(scene)
@@ -187,7 +190,7 @@ def test_filtered_swept_lists_equal_static_queries_on_the_sweep(scene):
         np.testing.assert_array_equal(SC.sorted_pairs(host(out, np.uint32)[:n]), SC.sorted_pairs(want))
 
 
-@pytest.mark.parametrize("scene", ["cloth_sphere", "folded", "tube"])
+@pytest.mark.parametrize("scene", ["cloth_sphere", "folded", "tube", "tube_state"])
 @pytest.mark.parametrize("swept", [False, True])
 def test_once_per_pair_ee_query_matches_the_reference_set(scene, swept):
     """lcs_bvh_query_ee_sym (each pair met once, from the lower Morton position) returns the oracle's
@@ -243,3 +246,81 @@ def test_once_per_pair_ee_query_on_boxes_at_the_threshold():
     m = int(counts(cnt)[0])
     assert m == n_want and n_want > 0
     np.testing.assert_array_equal(SC.sorted_pairs(host(pairs, np.uint32)[:m]), SC.sorted_pairs(want))
+
+
+def _deep_tree(kind_name):
+    x, el = SC.deep_tree_elements(kind_name)
+    V = x.shape[0]
+    kind = KINDS[kind_name][0]
+    t_o = O.lbvh_build(kind, x, el, V)
+    bvh = LBVH(kind, el.shape[0])
+    xd, ed = dev(x), dev(el)
+    if kind == O.TREE_FACE:
+        bvh.reduce_face_tree_aabb(xd, ed)
+    else:
+        bvh.reduce_edge_tree_aabb(xd, ed)
+    bvh.construct_tree()
+    z = np.zeros(V, np.float32)
+    O.lbvh_refit(t_o, x, x, el, z)
+    bvh.update_and_refit(dev(z), xd, xd, ed)
+    return x, el, t_o, bvh, xd, ed
+
+
+def _brute_force_count(x, el, r, ee):
+    """Size of the complete candidate set (strict box overlap, no early exit)."""
+    m = 2 if ee else 3
+    lo, hi = x[el[:, :m], :3].min(1), x[el[:, :m], :3].max(1)
+    if ee:  # edge i's query box: its box widened by r of its first vertex; pairs i < j
+        rq = r[el[:, 0]][:, None]
+        qlo, qhi = lo - rq, hi + rq
+    else:  # vertex v's query box: the point widened by r[v]
+        qlo, qhi = x[:, :3] - r[:, None], x[:, :3] + r[:, None]
+    ov = (lo[None] < qhi[:, None]).all(2) & (hi[None] > qlo[:, None]).all(2)
+    if ee:
+        i, j = np.nonzero(ov)
+        return int((i < j).sum())
+    return int(ov.sum())
+
+
+@pytest.mark.parametrize("kind_name", ["face", "edge"])
+def test_deep_tree_traversal_ends_early_like_the_reference(kind_name):
+    """A tree with inner nodes at depth >= 32, where the reference's 32-entry stack fills: every query whose
+    walk meets a full stack ends there, keeping only the pairs found before (lbvh.cpp:293-360).  Per-vertex
+    query radii mix queries that end early with queries that finish.  The GPU sets equal the oracle's, which
+    are smaller than the complete sets; the early exit is reported."""
+    x, el, t_o, bvh, xd, ed = _deep_tree(kind_name)
+    V = x.shape[0]
+    r = np.random.default_rng(7).uniform(200.0, 800.0, V).astype(np.float32)
+    z = np.zeros(V, np.float32)
+    ee = kind_name == "edge"
+    if ee:
+        want, n_want = O.lbvh_query_ee(t_o, x, x, el, r, z)
+    else:
+        want, n_want = O.lbvh_query_vf(t_o, x, x, r, z)
+    assert 0 < n_want < _brute_force_count(x, el, r, ee)  # the reference's early exit removed pairs
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    pairs = torch.zeros((n_want + 64, 2), dtype=torch.int32, device="cuda")
+    if ee:
+        bvh.broad_phase_query_from_edges(xd, xd, ed, cnt, pairs, dev(r), dev(z))
+    else:
+        bvh.broad_phase_query_from_verts(xd, xd, cnt, pairs, dev(r), dev(z))
+    n = int(counts(cnt)[0])
+    assert n == n_want
+    np.testing.assert_array_equal(SC.sorted_pairs(host(pairs, np.uint32)[:n]), SC.sorted_pairs(want))
+
+
+def test_deep_tree_once_per_pair_query_falls_back_to_the_reference_walk():
+    """The once-per-pair EE form relies on the set being symmetric, which the reference's early exit breaks:
+    on a deep tree lcs_bvh_query_ee_sym runs the reference's full EE walk and returns its set."""
+    x, el, t_o, bvh, xd, ed = _deep_tree("edge")
+    V = x.shape[0]
+    z = np.zeros(V, np.float32)
+    for rad in (300.0, 520.0, 600.0):
+        r = np.full(V, rad, np.float32)
+        want, n_want = O.lbvh_query_ee(t_o, x, x, el, r, z)
+        cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+        pairs = torch.zeros((max(n_want, 1) + 64, 2), dtype=torch.int32, device="cuda")
+        bvh.broad_phase_query_from_edges_sym(xd, xd, ed, cnt, pairs, rad)
+        n = int(counts(cnt)[0])
+        assert n == n_want, (rad, n, n_want)
+        np.testing.assert_array_equal(SC.sorted_pairs(host(pairs, np.uint32)[:n]), SC.sorted_pairs(want))

@@ -93,11 +93,8 @@ def test_bending_matches_oracle(lib, amp):
     print(f"\nbending Hessian blocks bit-identical: {100 * exact:.1f} %")
 
 
-def test_material_energy_fp64(lib):
-    sc = S.cloth_on_sphere(n=24)
-    x = _deformed(sc, 3, 2e-3)
-    xt = sc.x.copy()
-    want = O.material_energy(sc, x, xt, sc.dt)
+def _cloth_elements(sc, x, xt):
+    """lcs_cloth_elements of a scene's BW98 stretch faces and dihedral stencils (device copies in `keep`)."""
     Fs, B = sc.stretch_faces.shape[0], sc.bending.shape[0]
     keep = dict(x=dev(x), xt=dev(xt), mass=dev(sc.mass), fixed=dev(sc.pinned), f=dev(sc.stretch_faces),
                 dm=dev(sc.stretch_dm_inv), ar=dev(sc.stretch_area),
@@ -110,6 +107,15 @@ def test_material_energy_fp64(lib):
     m.stretch_mu_lambda = _ptr(keep["ml"])
     m.bending_edges, m.bending_rest_angle, m.bending_hbar = _ptr(keep["st"]), _ptr(keep["ra"]), _ptr(keep["hb"])
     m.bending_stiffness, m.bending_scaling = _ptr(keep["kb"]), sc.bending_scaling
+    return m, keep
+
+
+def test_material_energy_fp64(lib):
+    sc = S.cloth_on_sphere(n=24)
+    x = _deformed(sc, 3, 2e-3)
+    xt = sc.x.copy()
+    want = O.material_energy(sc, x, xt, sc.dt)
+    m, keep = _cloth_elements(sc, x, xt)
     out = torch.zeros(4, dtype=torch.float64, device="cuda")
     A.check(lib.lcs_material_energy(C.byref(m), _ptr(keep["x"]), _ptr(keep["xt"]), sc.dt, sc.dirichlet, _ptr(out),
                                     None), "lcs_material_energy")

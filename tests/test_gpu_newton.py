@@ -144,9 +144,9 @@ def test_c1_ten_steps_follow_the_cpu_restatement(plain):
     """Config 1 as configured (64 x 64 cloth dropped from 5 cm onto the pinned 2,562-vertex icosphere, dt 1/60,
     10 steps from rest).  Every GPU step is compared with the CPU restatement's time step from the same state
     (the GPU's state before the step): the first iteration's DCD candidates and contact pairs are equal (same
-    positions), the Newton iteration counts are equal, and the new positions agree within 2 % of the step's motion
-    (the PCG solves run to 1e-4 or to the 100-iteration cap, where FP32 rounding of different summation orders
-    separates the iterates); the cloth stays intersection-free."""
+    positions), the Newton iteration counts are equal, and the new positions agree within 1e-3 of the step's
+    motion (the PCG solves run to 1e-4 or to the 100-iteration cap, where FP32 rounding of different summation
+    orders separates the iterates; measured up to 1.6e-4); the cloth stays intersection-free."""
     sc = S.cloth_on_sphere(n=64)
     gpu = NewtonSolver(sc, plain=plain, single_reduction=not plain)
     pat = N.MaterialPattern(sc)
@@ -166,7 +166,7 @@ def test_c1_ten_steps_follow_the_cpu_restatement(plain):
         motion = float(np.abs(xo[:, :3] - xk[:, :3]).max())
         dev_ = float(np.abs(xg[:, :3] - xo[:, :3]).max()) / motion
         worst = max(worst, dev_)
-        assert dev_ <= 2e-2, (k, dev_)
+        assert dev_ <= 1e-3, (k, dev_)
         if k % 5 == 4:
             assert O.min_distance(sc, xg) > 0.0
     print(f"C1 ({'plain' if plain else 'fused'}): largest deviation {worst:.2e} of the step's motion; "

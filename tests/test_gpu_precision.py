@@ -6,7 +6,10 @@ algorithm on the same (FP32) inputs, with the errors printed (`pytest -s`) and b
   that rounding alone separates the runs.
 * Contact energy: the GPU's FP64 accumulation and a float32 accumulation of the same per-pair energies
   against a float64 evaluation and sum.
-* ACCD step bound: see test_gpu_narrow.py (the FP64 form equals the all-FP64 oracle bit for bit)."""
+* ACCD step bound: see test_gpu_narrow.py (the FP64 form equals the all-FP64 oracle bit for bit).
+
+The same on the 88,800-vertex tube at the benchmarked state (config 3): the system of the last Newton iteration
+of the benchmarked step, its contact pairs and elastic energy, and its CCD candidates and step bound."""
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -96,3 +99,122 @@ def test_contact_energy_error_against_fp64():
           f"FP32 accumulation {rel_32:.3e}")
     assert rel_gpu <= 1e-5
     assert isinstance(det, NarrowPhasesDetector)
+
+
+# ----------------------------------------------------------------------------------------------- tube (config 3)
+@pytest.fixture(scope="module")
+def tube_iterate():
+    from luisacomputesimulator_b200.newton import NewtonSolver
+    from oracle import newton_cpu as N
+    from tests import scenarios as SC
+    from tests.test_gpu_tube import _oracle_contact_set
+    sc, x, v, frame = SC.tube_state()
+    gpu = NewtonSolver(sc, single_reduction=True)
+    gpu.upload(x, v)
+    gpu.set_frame(frame)
+    assert gpu.step().status == 0
+    x_iter, dx, x_tilde = gpu.last_iterate()
+    _, _, pairs = _oracle_contact_set(sc, x_iter)
+    b, diag, Am = N.material_fill(sc, N.MaterialPattern(sc), x_iter, x_tilde, sc.dt)
+    b, diag = O.contact_grad_diag(pairs, sc.num_verts, b, diag)
+    Bm = O.contact_offdiag_bsr(pairs, sc.num_verts)
+    return dict(sc=sc, x_iter=x_iter, dx=dx, x_tilde=x_tilde, pairs=pairs, b=b, diag=diag, A=Am, B=Bm)
+
+
+@pytest.mark.parametrize("iters", [25, 100])
+def test_tube_pcg_error_against_fp64(tube_iterate, iters):
+    """K iterations of the production solve (single reduction, slice-resident) with FP32 and with FP64 dot
+    products against K iterations of the same PCG in float64 on the tube's 88,800-row system."""
+    t = tube_iterate
+    sc, diag, A, B, b = t["sc"], t["diag"], t["A"], t["B"], t["b"]
+    n = sc.num_verts
+    M = _csr64(diag, A, B, n)
+    x64 = _pcg64(M, diag, b, iters)
+    b64 = np.asarray(b, np.float64)[:, :3].reshape(-1)
+    res = lambda y: float(np.linalg.norm(b64 - M @ y.reshape(-1)) / np.linalg.norm(b64))  # noqa: E731
+    err, rr = {}, {}
+    for fp64 in (False, True):
+        solver = ConjugateGradientSolver(n)
+        x = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+        bsr = lambda m: make_bsr(n, dev(m[0]), dev(m[1]), dev(m[2]))  # noqa: E731
+        st = solver.device_solve(dev(diag), bsr(A), bsr(B), dev(b), x, max_iter=iters, rel_tol=0.0,
+                                 abs_rz_tol=-1.0, check_every=1, fp64_dots=fp64, single_reduction=True)
+        assert st["iterations"] == iters
+        xs = host(x)[:, :3].astype(np.float64)
+        err[fp64] = float(np.linalg.norm(xs - x64) / np.linalg.norm(x64))
+        rr[fp64] = res(xs)
+    r64 = res(x64)
+    print(f"\ntube PCG {iters} iterations: rel error vs all-FP64 run: FP32 dots {err[False]:.3e}, FP64 dots "
+          f"{err[True]:.3e}; true rel residual: FP32 {rr[False]:.3e}, FP64 dots {rr[True]:.3e}, all-FP64 {r64:.3e}")
+    assert err[False] < 5e-2 and err[True] < 5e-2
+    assert rr[False] <= 1.5 * r64 + 1e-6 and rr[True] <= 1.5 * r64 + 1e-6
+
+
+def test_tube_energy_sums_against_fp64(tube_iterate):
+    """The line search's sums on the tube: the barrier energy of the contact pairs and the elastic + inertia
+    energy, accumulated in FP64 on the GPU, against the oracle's float64 sums (and the FP32 accumulation the
+    reference does)."""
+    import ctypes as C
+
+    from luisacomputesimulator_b200 import _capi as A
+    from luisacomputesimulator_b200.collision import ptr, stream
+    t = tube_iterate
+    sc, x, pairs = t["sc"], t["x_iter"], t["pairs"]
+    lib = A.load()
+    dp = dev(np.ascontiguousarray(pairs).view(np.uint32).reshape(len(pairs), -1))
+    cnt = dev(np.array([len(pairs)], np.uint32))
+    xd, dh, off = dev(x), dev(sc.d_hat), dev(sc.offset)  # kept alive across the call
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    A.check(lib.lcs_contact_energy(ptr(dp), ptr(cnt), len(pairs), ptr(xd), ptr(dh), ptr(off), ptr(out), stream()),
+            "lcs_contact_energy")
+    e_gpu = float(host(out)[0])
+    e64 = O.contact_energy(pairs, x, sc.d_hat, sc.offset, fp64=True)
+    e32 = O.contact_energy(pairs, x, sc.d_hat, sc.offset, fp64=False)
+    rel_gpu, rel_32 = abs(e_gpu - e64) / abs(e64), abs(e32 - e64) / abs(e64)
+    # elastic + inertia (BW98 stretch, dihedral bending, inertia with the Dirichlet term), FP64 sums
+    from tests.test_gpu_material import _cloth_elements
+    m, keep = _cloth_elements(sc, x, t["x_tilde"])
+    mo = torch.zeros(4, dtype=torch.float64, device="cuda")
+    A.check(lib.lcs_material_energy(C.byref(m), ptr(keep["x"]), ptr(keep["xt"]), sc.dt, sc.dirichlet, ptr(mo),
+                                    stream()), "lcs_material_energy")
+    got = host(mo)
+    want = O.material_energy(sc, x, t["x_tilde"], sc.dt)
+    rel_m = float(np.abs(got - want).max() / np.abs(want).max())
+    print(f"\ntube contact energy ({len(pairs)} pairs): rel error vs FP64 sum: GPU FP64 accumulation {rel_gpu:.3e}, "
+          f"FP32 accumulation {rel_32:.3e}; material energy terms {got}: rel error {rel_m:.3e}")
+    assert rel_gpu <= 1e-5 and rel_m <= 1e-5
+
+
+def test_tube_step_bound_against_fp64(tube_iterate):
+    """The CCD step bound of the last iteration (the GPU's own direction): the FP32 ACCD and the precision form
+    (whole iteration in FP64, TOI rounded toward zero) against the all-FP64 oracle ACCD on the tube's candidates."""
+    from luisacomputesimulator_b200.collision import NarrowPhasesDetector
+    from tests.gpu_util import SceneOnDevice
+    from tests.test_gpu_narrow import _load
+    t = tube_iterate
+    sc, x0, dx = t["sc"], t["x_iter"], t["dx"]
+    x1 = x0.copy()
+    x1[:, :3] = x0[:, :3] + dx[:, :3]
+    tf = O.lbvh_build(O.TREE_FACE, x0, sc.faces, sc.num_verts)
+    te = O.lbvh_build(O.TREE_EDGE, x0, sc.edges, sc.num_verts)
+    O.lbvh_refit(tf, x0, x1, sc.faces, sc.offset)
+    O.lbvh_refit(te, x0, x1, sc.edges, sc.offset)
+    vf, _ = O.lbvh_query_vf(tf, x0, x1, sc.d_hat, sc.offset)
+    ee, _ = O.lbvh_query_ee(te, x0, x1, sc.edges, sc.d_hat, sc.offset)
+    t64 = min(O.ccd_f64(False, vf, x0, x1, sc.faces, sc.body, sc.offset).min(initial=1.25),
+              O.ccd_f64(True, ee, x0, x1, sc.edges, sc.body, sc.offset).min(initial=1.25)) / 1.25
+    D = SceneOnDevice(sc)
+    got = {}
+    for fp64 in (False, True):  # the FP32 ACCD, the precision form (LCS_CCD_FP64)
+        det = NarrowPhasesDetector(sc.num_verts, sc.edges.shape[0])
+        _load(det, vf, ee)
+        det.reset_toi()
+        det.vf_ccd_query(dev(x0), dev(x1), D.faces, D.body, D.offset, fp64=fp64)
+        det.ee_ccd_query(dev(x0), dev(x1), D.edges, D.body, D.offset, fp64=fp64)
+        torch.cuda.synchronize()
+        got[fp64] = float(host(det.toi)[0])
+    e32, e64 = abs(got[False] - t64) / t64, abs(got[True] - t64) / t64
+    print(f"\ntube step bound ({len(vf)} VF + {len(ee)} EE candidates): all-FP64 {t64:.9g}; FP32 {got[False]:.9g} "
+          f"(rel {e32:.2e}), FP64 form {got[True]:.9g} (rel {e64:.2e})")
+    assert got[True] <= t64 and e64 <= 1e-6
+    assert e32 <= 1e-6
