@@ -607,6 +607,7 @@ def run_batch(a):
     t_e2e = time.perf_counter() - t_e2e
     assert all(np.isfinite(x).all() for x in xs)
     tuned_chunks, tuned_ms = batch.pcg_tuning()
+    q_vf, q_ee = batch.query_tuning()
     del batch
     ms = e0.elapsed_time(e1)
     done_all, t_max = combine(len(scs), ms / 1e3, device="cuda")  # sum of solves, max of device time
@@ -638,6 +639,8 @@ def run_batch(a):
                    "scenes": n_all, "verts_rank0": V, "pcg_cluster": "auto",
                    "pcg_autotune": {"chunks_per_cta": tuned_chunks, "tuned_solve_ms": tuned_ms,
                                     "candidates": [2, 4, 8, 16]},
+                   "traversal_autotune": {"vf_threads_per_block": q_vf, "ee_threads_per_block": q_ee,
+                                          "candidates": [64, 128, 256]},
                    "parallelism": f"whole scenes over {world} GPUs" if world > 1 else "one batch"},
         "e2e": {"value": done_all / e2e_max, "unit": "solves/s", "h2d_bytes_per_step": None,
                 "d2h_bytes_per_step": 16 * V, "includes": "batch creation (host upload), all steps, read-back"},

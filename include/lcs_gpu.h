@@ -211,6 +211,9 @@ LCS_API int lcs_forest_query_ee(const lcs_forest* edge_forest, const float* x0, 
                                 const uint32_t* edges, const float* d_hat, const float* thickness,
                                 uint32_t* pairs, uint32_t capacity, uint32_t* d_count, lcs_stream stream);
 LCS_API int lcs_forest_health(lcs_forest* f, int* healthy, lcs_stream stream);
+/* The queries' launch shape, tuned on a forest's first query (threads per block: 64, 128 or 256, each timed
+ * once on that query, the fastest kept) and the tuned query's time in ms; 0 before the first query. */
+LCS_API int lcs_forest_query_tuning(const lcs_forest* f, uint32_t* threads_per_block, float* query_ms);
 /* one scene's tree in the layout of lcs_bvh_export (local node and element ids) */
 LCS_API int lcs_forest_export_scene(const lcs_forest* f, uint32_t scene, uint32_t* parent, uint32_t* children,
                                     uint32_t* object_idx, uint64_t* morton_sorted,
@@ -632,6 +635,9 @@ LCS_API int lcs_newton_pcg_kind(const lcs_newton* h);
 /* A batch's tuned PCG shape (lcs_pcg_batch_tuning of its solver): chunks of 256 rows per CTA and the
  * tuned solve's time in ms; 0 before the first step of a batch created with pcg_cluster 0. */
 LCS_API int lcs_newton_batch_tuning(const lcs_newton* h, uint32_t* chunks_per_cta, float* solve_ms);
+/* A batch's tuned traversal shapes (lcs_forest_query_tuning of its face and edge forests): threads per block
+ * of the VF and EE queries; 0 before the first step. */
+LCS_API int lcs_newton_batch_query_tuning(const lcs_newton* h, uint32_t* vf_threads, uint32_t* ee_threads);
 
 #ifdef __cplusplus
 }

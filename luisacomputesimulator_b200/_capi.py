@@ -102,6 +102,8 @@ SIGNATURES = {
     "lcs_bvh_create": (I32, [I32, U32, C.POINTER(P)]),
     "lcs_bvh_destroy": (I32, [P]),
     "lcs_debug_pcg_wait": (I32, [I32, I32, U32, U32, P]),
+    "lcs_forest_query_tuning": (I32, [P, P, P]),
+    "lcs_newton_batch_query_tuning": (I32, [P, P, P]),
     "lcs_bvh_check_construction": (I32, [P, P]),
     "lcs_bvh_data": (I32, [P, P]),
     "lcs_bvh_reduce_aabb": (I32, [P, P, P, U32, P]),

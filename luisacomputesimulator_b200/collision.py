@@ -83,6 +83,12 @@ class Forest:
         A.check(self.lib.lcs_forest_health(self.h, C.byref(ok), stream()), "lcs_forest_health")
         return bool(ok.value)
 
+    def query_tuning(self):
+        """(threads per block, ms) of the traversal shape tuned on the first query (0 before it)."""
+        t, ms = C.c_uint32(), C.c_float()
+        A.check(self.lib.lcs_forest_query_tuning(self.h, C.byref(t), C.byref(ms)), "lcs_forest_query_tuning")
+        return int(t.value), float(ms.value)
+
     def export_scene(self, scene):
         """(parent, children, object_idx, morton_sorted, sorted_get_original, node_aabb, global_aabb) of one
         scene's tree in the layout of LBVH.export (local ids)."""

@@ -49,6 +49,9 @@ struct lcs_forest {
     float4* wide = nullptr;       // 4 NI
     uint32_t* counters = nullptr; // NI
     uint32_t* healthy = nullptr;
+    uint32_t* saved_count = nullptr;  // 1: the candidate count before a tuning query (restored between trials)
+    mutable uint32_t q_threads = 0;   // tuned threads per block of the queries (0: not tuned yet)
+    mutable float q_ms = 0.0f;        // the tuned configuration's query time
 };
 
 namespace {
@@ -268,7 +271,7 @@ __global__ void k_f_refit(int kind, uint32_t n, uint32_t NI, const uint32_t* __r
 
 // query_template2 from the root of the query's own scene (fn_query_from_verts_v2 / _edges_v2)
 template <bool EE>
-__global__ void __launch_bounds__(128) k_f_query(const float4* __restrict__ wide, const uint32_t* __restrict__ ioff,
+__global__ void __launch_bounds__(256) k_f_query(const float4* __restrict__ wide, const uint32_t* __restrict__ ioff,
                                                  const uint32_t* __restrict__ qscene, const float4* __restrict__ x0,
                                                  const float4* __restrict__ x1, const uint2* __restrict__ edges,
                                                  uint32_t n_queries, const float* __restrict__ dhat,
@@ -475,6 +478,7 @@ extern "C" int lcs_forest_create(int kind, uint32_t n_scenes, const uint32_t* el
     A(dalloc(f->wide, 4 * (size_t)f->NI));
     A(dalloc(f->counters, f->NI));
     A(dalloc(f->healthy, 1));
+    A(dalloc(f->saved_count, 1));
     if (e == cudaSuccess) e = cudaMemset(f->counters, 0, sizeof(uint32_t) * (size_t)f->NI);
     if (e == cudaSuccess) e = cudaMemset(f->wide, 0, sizeof(float4) * 4 * (size_t)f->NI);
     if (e != cudaSuccess) {
@@ -492,7 +496,7 @@ extern "C" int lcs_forest_destroy(lcs_forest* f)
     if (!f) return LCS_OK;
     void* ptrs[] = {f->eoff, f->ioff, f->boff, f->bcover, f->escene, f->iscene, f->bscene, f->centers,
                     f->block_aabb, f->gaabb, f->m30, f->keys, f->keys_alt, f->vals, f->vals_alt, f->hist,
-                    f->ms64, f->parent, f->children, f->slot, f->wide, f->counters, f->healthy};
+                    f->ms64, f->parent, f->children, f->slot, f->wide, f->counters, f->healthy, f->saved_count};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete f;
@@ -540,6 +544,77 @@ extern "C" int lcs_forest_update_refit(lcs_forest* f, const float* thickness, co
     return LCS_OK;
 }
 
+// The traversal's launch shape (threads per block: 64, 128 or 256; the grid covers every query, at most 2048
+// threads per SM) is tuned on the first query of a forest: the query runs once in each shape, timed with CUDA
+// events, with the candidate count restored before each run, so that the last run's pairs are the result
+// (every run writes the same set).  Later queries use the fastest shape.
+template <bool EE>
+static int f_query_tuned(const lcs_forest* f, uint32_t n_queries, const uint32_t* qscene, const float4* x0,
+                         const float4* x1, const uint2* edges, const float* d_hat, const float* thickness, uint2* pairs,
+                         uint32_t capacity, uint32_t* d_count, const uint32_t* order, uint32_t* capped,
+                         const uint8_t* only, cudaStream_t s)
+{
+    auto launch = [&](uint32_t threads) {
+        k_f_query<EE><<<grid_for(n_queries, (int)threads, (int)(2048u / threads)), threads, 0, s>>>(
+            f->wide, f->ioff, qscene, x0, x1, edges, n_queries, d_hat, thickness, pairs, capacity, d_count, order,
+            capped, only);
+        lcs_count_launch();
+    };
+    if (f->q_threads != 0) {
+        launch(f->q_threads);
+        LCS_LAUNCH_CHECK();
+        return LCS_OK;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        cudaGetLastError();
+        if (e0) cudaEventDestroy(e0);
+        f->q_threads = 128;  // untuned default
+        launch(f->q_threads);
+        LCS_LAUNCH_CHECK();
+        return LCS_OK;
+    }
+    int rc = LCS_OK;
+    float best = 0.0f;
+    uint32_t best_threads = 128;
+    if (cudaMemcpyAsync(f->saved_count, d_count, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        rc = LCS_ERR_CUDA;
+    for (uint32_t threads : {64u, 256u, 128u}) {
+        if (rc != LCS_OK) break;
+        if (cudaMemcpyAsync(d_count, f->saved_count, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+            cudaEventRecord(e0, s) != cudaSuccess) {
+            rc = LCS_ERR_CUDA;
+            break;
+        }
+        launch(threads);
+        float ms = 0.0f;
+        if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            rc = LCS_ERR_CUDA;
+            break;
+        }
+        if (best == 0.0f || ms < best) {
+            best = ms;
+            best_threads = threads;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != LCS_OK) return lcs_fail(rc, "lcs_forest_query: tuning the launch shape failed");
+    f->q_threads = best_threads;
+    f->q_ms = best;
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+extern "C" int lcs_forest_query_tuning(const lcs_forest* f, uint32_t* threads_per_block, float* query_ms)
+{
+    if (!f) return lcs_fail(LCS_ERR_INVALID, "lcs_forest_query_tuning: null handle");
+    if (threads_per_block) *threads_per_block = f->q_threads;
+    if (query_ms) *query_ms = f->q_ms;
+    return LCS_OK;
+}
+
 extern "C" int lcs_forest_query_vf(const lcs_forest* face_forest, const float* x0, const float* x1, uint32_t n_verts,
                                    const uint32_t* vert_scene, const float* d_hat, const float* thickness,
                                    uint32_t* pairs, uint32_t capacity, uint32_t* d_count, lcs_stream stream)
@@ -558,12 +633,10 @@ int lcs_forest_query_vf_capped(const lcs_forest* face_forest, const float* x0, c
         (capacity && !pairs))
         return lcs_fail(LCS_ERR_INVALID, "lcs_forest_query_vf: bad argument");
     if (n_verts == 0) return LCS_OK;
-    k_f_query<false><<<grid_for(n_verts, 128, 16), 128, 0, (cudaStream_t)stream>>>(
-        f->wide, f->ioff, vert_scene, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1), nullptr,
-        n_verts, d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count, nullptr, capped, only);
-    lcs_count_launch();
-    LCS_LAUNCH_CHECK();
-    return LCS_OK;
+    return f_query_tuned<false>(f, n_verts, vert_scene, reinterpret_cast<const float4*>(x0),
+                                reinterpret_cast<const float4*>(x1), nullptr, d_hat, thickness,
+                                reinterpret_cast<uint2*>(pairs), capacity, d_count, nullptr, capped, only,
+                                (cudaStream_t)stream);
 }
 
 extern "C" int lcs_forest_query_ee(const lcs_forest* edge_forest, const float* x0, const float* x1,
@@ -582,13 +655,10 @@ int lcs_forest_query_ee_capped(const lcs_forest* edge_forest, const float* x0, c
     if (!f || f->kind != LCS_TREE_EDGE || !x0 || !x1 || !edges || !d_hat || !thickness || !d_count ||
         (capacity && !pairs))
         return lcs_fail(LCS_ERR_INVALID, "lcs_forest_query_ee: bad argument");
-    k_f_query<true><<<grid_for(f->N, 128, 16), 128, 0, (cudaStream_t)stream>>>(
-        f->wide, f->ioff, f->escene, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
-        reinterpret_cast<const uint2*>(edges), f->N, d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity,
-        d_count, f->sgo, capped, only);
-    lcs_count_launch();
-    LCS_LAUNCH_CHECK();
-    return LCS_OK;
+    return f_query_tuned<true>(f, f->N, f->escene, reinterpret_cast<const float4*>(x0),
+                               reinterpret_cast<const float4*>(x1), reinterpret_cast<const uint2*>(edges), d_hat,
+                               thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count, f->sgo, capped, only,
+                               (cudaStream_t)stream);
 }
 
 extern "C" int lcs_forest_health(lcs_forest* f, int* healthy, lcs_stream stream)

@@ -44,7 +44,6 @@ struct lcs_bvh {
     uint32_t* counters = nullptr;    // max(ni, 1), refit arrival counters (self-resetting)
     uint32_t* healthy = nullptr;     // 1
     uint32_t* maxdepth = nullptr;    // 1: depth of the deepest inner node (root: 0), capped at 256
-    uint32_t* work = nullptr;        // 4: the persistent walks' query counters (k_query, k_query_ee_sym)
 };
 
 namespace {
@@ -360,83 +359,6 @@ constexpr int kStack4 = 64;  // entries of the 4-wide traversal stack
 // the other kind, so the choice costs no host synchronisation.
 constexpr uint32_t kRefStack = 32;
 
-// Persistent walks: a warp takes its queries from a grid-wide counter in chunks of 32 and hands them to its
-// lanes one at a time as their walks end, so the lanes stay busy until the queries run out instead of
-// idling until the longest of 32 fixed walks ends.  The counter (work[0]) resets itself: the last warp of
-// the grid to finish (counted in work[1]) zeroes both words for the next launch.  Two walks over the same
-// tree and counter must therefore not overlap on the GPU.
-constexpr uint32_t kQueryChunk = 32;
-constexpr uint32_t kNoQuery = 0xFFFFFFFFu;     // no query for the lane in this step (it asks again)
-constexpr uint32_t kQueriesDone = 0xFFFFFFFEu; // the queries have run out
-
-// a query index for each lane in `need`; cb / ce (the warp's current chunk) and dry are warp-uniform
-__device__ __forceinline__ uint32_t take_query(uint32_t* work, uint32_t n, bool need, uint32_t& cb, uint32_t& ce,
-                                               bool& dry)
-{
-    const uint32_t needm = __ballot_sync(0xFFFFFFFFu, need);
-    uint32_t got = kNoQuery;
-    if (needm) {
-        if (cb >= ce && !dry) {
-            uint32_t b = 0;
-            if (lane_id() == 0) b = atomicAdd(work, kQueryChunk);
-            b = __shfl_sync(0xFFFFFFFFu, b, 0);
-            cb = b;
-            ce = b < n ? min(b + kQueryChunk, n) : b;
-            dry = b >= n;
-        }
-        const uint32_t avail = ce > cb ? ce - cb : 0u;
-        const uint32_t k = (uint32_t)__popc(needm);
-        const uint32_t rank = (uint32_t)__popc(needm & ((1u << lane_id()) - 1u));
-        if (need) got = rank < avail ? cb + rank : (dry ? kQueriesDone : kNoQuery);
-        cb += k < avail ? k : avail;
-    }
-    return got;
-}
-
-// the last warp of the grid to finish resets the counter
-__device__ __forceinline__ void finish_queries(uint32_t* work)
-{
-    if (lane_id() == 0) {
-        __threadfence();
-        const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-        if (atomicAdd(work + 1, 1u) == warps - 1u) {
-            work[0] = 0u;
-            work[1] = 0u;
-        }
-    }
-}
-
-// the reference's query box of vertex q (VF) or edge q (EE): swept box +- (thickness + d_hat) of the
-// (first) vertex; a vertex with a negative d_hat (affine-body DOF slot) queries nothing
-template <bool EE>
-__device__ __forceinline__ void query_box(uint32_t q, const float4* __restrict__ x0, const float4* __restrict__ x1,
-                                          const uint2* __restrict__ edges, const float* __restrict__ dhat,
-                                          const float* __restrict__ thickness, float* box)
-{
-    v3 mn, mx;
-    uint32_t v0;
-    if (EE) {
-        const uint2 ed = __ldg(&edges[q]);
-        const v3 s0 = ld3(x0, ed.x), s1 = ld3(x0, ed.y), e0 = ld3(x1, ed.x), e1 = ld3(x1, ed.y);
-        mn = min3(min3(s0, s1), min3(e0, e1));
-        mx = max3(max3(s0, s1), max3(e0, e1));
-        v0 = ed.x;
-    } else {
-        const v3 a = ld3(x0, q), b = ld3(x1, q);
-        mn = min3(a, b);
-        mx = max3(a, b);
-        v0 = q;
-    }
-    const float dh = __ldg(&dhat[v0]);
-    const float r = __ldg(&thickness[v0]) + dh;
-    box[0] = mn.x - r; box[1] = mn.y - r; box[2] = mn.z - r;
-    box[3] = mx.x + r; box[4] = mx.y + r; box[5] = mx.z + r;
-    if (!EE && dh < 0.0f) {
-        box[0] = box[1] = box[2] = __int_as_float(0x7f800000);
-        box[3] = box[4] = box[5] = __int_as_float(0xff800000);
-    }
-}
-
 template <bool EE>
 __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide4, uint32_t n_leaves,
                                                const float4* __restrict__ x0, const float4* __restrict__ x1,
@@ -444,38 +366,51 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide4,
                                                const float* __restrict__ dhat, const float* __restrict__ thickness,
                                                uint2* __restrict__ pairs, uint32_t capacity, uint32_t* d_count,
                                                const uint32_t* __restrict__ order, uint32_t* capped,
-                                               const uint32_t* __restrict__ maxdepth, uint32_t* work)
+                                               const uint32_t* __restrict__ maxdepth)
 {
     if (__ldg(maxdepth) >= kRefStack) return;
-    uint32_t cb = 0, ce = 0;
-    bool dry = false, finished = false;
-    uint32_t q = 0, loop = 0;
-    float box[6];
-    uint32_t stack[kStack4];
-    int sp = 0;
-    for (;;) {
-        // queries in the order of `order` (the tree's Morton order when the queries are its own leaves):
-        // the walks a warp runs side by side then visit nearly the same nodes
-        const uint32_t got = take_query(work, n_queries, sp == 0 && !finished, cb, ce, dry);
-        if (got == kQueriesDone) {
-            finished = true;
-        } else if (got != kNoQuery) {
-            q = order ? __ldg(&order[got]) : got;
-            query_box<EE>(q, x0, x1, edges, dhat, thickness, box);
-            sp = 0;
-            stack[sp++] = 0;
-            loop = 0;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_queries; t += gridDim.x * blockDim.x) {
+        // queries in the order of `order` (the tree's Morton order when the queries are its own
+        // leaves): neighbouring threads then walk nearly the same nodes
+        const uint32_t q = order ? __ldg(&order[t]) : t;
+        float box[6];
+        {
+            v3 mn, mx;
+            uint32_t v0;
+            if (EE) {
+                uint2 ed = __ldg(&edges[q]);
+                v3 s0 = ld3(x0, ed.x), s1 = ld3(x0, ed.y), e0 = ld3(x1, ed.x), e1 = ld3(x1, ed.y);
+                mn = min3(min3(s0, s1), min3(e0, e1));
+                mx = max3(max3(s0, s1), max3(e0, e1));
+                v0 = ed.x;
+            } else {
+                v3 a = ld3(x0, q), b = ld3(x1, q);
+                mn = min3(a, b);
+                mx = max3(a, b);
+                v0 = q;
+            }
+            const float dh = __ldg(&dhat[v0]);
+            const float r = __ldg(&thickness[v0]) + dh;
+            box[0] = mn.x - r; box[1] = mn.y - r; box[2] = mn.z - r;
+            box[3] = mx.x + r; box[4] = mx.y + r; box[5] = mx.z + r;
+            if (!EE && dh < 0.0f) {  // a vertex with a negative d_hat (affine-body DOF slot) queries nothing
+                box[0] = box[1] = box[2] = __int_as_float(0x7f800000);
+                box[3] = box[4] = box[5] = __int_as_float(0xff800000);
+            }
         }
-        if (__all_sync(0xFFFFFFFFu, finished)) break;
-        uint2 hit[4];
-        uint32_t nhit = 0;
-        if (sp > 0) {
+        uint32_t stack[kStack4];
+        int sp = 0;
+        uint32_t loop = 0;
+        stack[sp++] = 0;
+        while (sp > 0) {
             const uint32_t node = stack[--sp];
             const float4* r = wide4 + 8 * node;
             float4 rec[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) rec[j] = __ldg(r + j);
             bool stop = false;
+            uint2 hit[4];
+            uint32_t nhit = 0;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const float4 mn = rec[2 * k], mx = rec[2 * k + 1];
@@ -487,18 +422,17 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide4,
                     } else if (sp < kStack4) {
                         stack[sp++] = code;
                     } else {
-                        stop = true;  // cannot happen below depth 32 (48 entries at most); reported if it did
+                        stop = true;  // a full stack ends the whole traversal (lbvh.cpp:344-351)
                     }
                 }
             }
-            if (stop || ++loop > 100000u) {  // the walk ends; reported so callers know the list may lack pairs
-                if (capped) atomicOr(capped, 1u);
-                sp = 0;
+            emit_pairs(hit, nhit, pairs, capacity, d_count);
+            if (stop || ++loop > 100000u) {  // the reference's early exits; reported so callers know the
+                if (capped) atomicOr(capped, 1u);  // list may lack pairs a complete traversal would find
+                break;
             }
         }
-        emit_pairs(hit, nhit, pairs, capacity, d_count);
     }
-    finish_queries(work);
 }
 
 // query_template2 as the reference runs it (lbvh.cpp:293-360) on the binary records, for trees with an
@@ -591,49 +525,37 @@ __global__ void __launch_bounds__(128) k_query_ee_sym(const float4* __restrict__
                                                       const float4* __restrict__ x1, const uint2* __restrict__ edges,
                                                       float r, uint2* __restrict__ pairs, uint32_t capacity,
                                                       uint32_t* d_count, uint32_t* capped,
-                                                      const uint32_t* __restrict__ maxdepth, uint32_t* work)
+                                                      const uint32_t* __restrict__ maxdepth)
 {
     if (__ldg(maxdepth) >= kRefStack) return;  // a deep tree: k_query_ref<true> (the full EE walk) instead
-    uint32_t cb = 0, ce = 0;
-    bool dry = false, finished = false;
-    uint32_t t = 0, q = 0, loop = 0;
-    float4 own_mn = make_float4(0.f, 0.f, 0.f, 0.f), own_mx = own_mn;
-    float box[6], cull[6];
-    uint32_t stack[kStack4];
-    int sp = 0;
-    for (;;) {
-        const uint32_t got = take_query(work, n_leaves, sp == 0 && !finished, cb, ce, dry);
-        if (got == kQueriesDone) {
-            finished = true;
-        } else if (got != kNoQuery) {
-            t = got;  // the query's sorted position
-            q = __ldg(&sgo[t]);
-            const uint2 ed = __ldg(&edges[q]);
-            const v3 s0 = ld3(x0, ed.x), s1 = ld3(x0, ed.y), e0 = ld3(x1, ed.x), e1 = ld3(x1, ed.y);
-            const v3 mn = min3(min3(s0, s1), min3(e0, e1)), mx = max3(max3(s0, s1), max3(e0, e1));
-            own_mn = make_float4(mn.x, mn.y, mn.z, 0.f);
-            own_mx = make_float4(mx.x, mx.y, mx.z, 0.f);
-            box[0] = mn.x - r; box[1] = mn.y - r; box[2] = mn.z - r;
-            box[3] = mx.x + r; box[4] = mx.y + r; box[5] = mx.z + r;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_leaves; t += gridDim.x * blockDim.x) {
+        const uint32_t q = __ldg(&sgo[t]);
+        const uint2 ed = __ldg(&edges[q]);
+        const v3 s0 = ld3(x0, ed.x), s1 = ld3(x0, ed.y), e0 = ld3(x1, ed.x), e1 = ld3(x1, ed.y);
+        const v3 mn = min3(min3(s0, s1), min3(e0, e1)), mx = max3(max3(s0, s1), max3(e0, e1));
+        const float4 own_mn = make_float4(mn.x, mn.y, mn.z, 0.f), own_mx = make_float4(mx.x, mx.y, mx.z, 0.f);
+        const float box[6] = {mn.x - r, mn.y - r, mn.z - r, mx.x + r, mx.y + r, mx.z + r};
+        float cull[6];
+        {
             const float mgx = (fabsf(mn.x) + fabsf(mx.x) + r) * 9.5367431640625e-07f;  // 2^-20
             const float mgy = (fabsf(mn.y) + fabsf(mx.y) + r) * 9.5367431640625e-07f;
             const float mgz = (fabsf(mn.z) + fabsf(mx.z) + r) * 9.5367431640625e-07f;
             cull[0] = box[0] - mgx; cull[1] = box[1] - mgy; cull[2] = box[2] - mgz;
             cull[3] = box[3] + mgx; cull[4] = box[4] + mgy; cull[5] = box[5] + mgz;
-            sp = 0;
-            stack[sp++] = 0;
-            loop = 0;
         }
-        if (__all_sync(0xFFFFFFFFu, finished)) break;
-        uint2 hit[4];
-        uint32_t nhit = 0;
-        if (sp > 0) {
+        uint32_t stack[kStack4];
+        int sp = 0;
+        uint32_t loop = 0;
+        stack[sp++] = 0;
+        while (sp > 0) {
             const uint32_t node = stack[--sp];
             const float4* node_rec = wide4 + 8 * node;
             float4 rec[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) rec[j] = __ldg(node_rec + j);
             bool stop = false;
+            uint2 hit[4];
+            uint32_t nhit = 0;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const float4 cmn = rec[2 * k], cmx = rec[2 * k + 1];
@@ -654,14 +576,13 @@ __global__ void __launch_bounds__(128) k_query_ee_sym(const float4* __restrict__
                     }
                 }
             }
+            emit_pairs(hit, nhit, pairs, capacity, d_count);
             if (stop || ++loop > 100000u) {
                 if (capped) atomicOr(capped, 1u);
-                sp = 0;
+                break;
             }
         }
-        emit_pairs(hit, nhit, pairs, capacity, d_count);
     }
-    finish_queries(work);
 }
 
 // Candidate filter: the pairs of `in` whose boxes overlap at positions x (static boxes, the
@@ -785,9 +706,7 @@ extern "C" int lcs_bvh_create(int kind, uint32_t n_leaves, lcs_bvh** out)
     A(alloc(h->counters, nw));
     A(alloc(h->healthy, 1));
     A(alloc(h->maxdepth, 1));
-    A(alloc(h->work, 4));
     if (e == cudaSuccess) e = cudaMemset(h->maxdepth, 0, sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMemset(h->work, 0, 4 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(h->counters, 0, sizeof(uint32_t) * nw);
     if (e == cudaSuccess) e = cudaMemset(h->wide, 0, sizeof(float4) * 4 * nw);
     if (e == cudaSuccess) e = cudaMemset(h->wide4, 0, sizeof(float4) * 8 * nw);
@@ -808,7 +727,7 @@ extern "C" int lcs_bvh_destroy(lcs_bvh* h)
     if (!h) return LCS_OK;
     void* ptrs[] = {h->centers, h->block_aabb, h->gaabb, h->m30, h->keys, h->keys_alt, h->vals, h->vals_alt,
                     h->hist, h->ms64, h->parent, h->children, h->slot, h->wide, h->wide4, h->even, h->counters,
-                    h->healthy, h->maxdepth, h->work};
+                    h->healthy, h->maxdepth};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete h;
@@ -956,7 +875,7 @@ int lcs_bvh_query_vf_capped(const lcs_bvh* t, const float* x0, const float* x1, 
     if (t->n == 0 || n_verts == 0) return LCS_OK;
     k_query<false><<<grid_for(n_verts, 128, 16), 128, 0, (cudaStream_t)stream>>>(
         t->wide4, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1), nullptr, n_verts,
-        d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count, nullptr, capped, t->maxdepth, t->work);
+        d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count, nullptr, capped, t->maxdepth);
     lcs_count_launch();
     if (t->ni > 0) {
         k_query_ref<false><<<grid_for(n_verts, 128, 16), 128, 0, (cudaStream_t)stream>>>(
@@ -987,7 +906,7 @@ int lcs_bvh_query_ee_capped(const lcs_bvh* t, const float* x0, const float* x1, 
     k_query<true><<<grid_for(n_edges, 128, 16), 128, 0, (cudaStream_t)stream>>>(
         t->wide4, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
         reinterpret_cast<const uint2*>(edges), n_edges, d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity,
-        d_count, n_edges == t->n ? t->sgo : nullptr, capped, t->maxdepth, t->work);
+        d_count, n_edges == t->n ? t->sgo : nullptr, capped, t->maxdepth);
     lcs_count_launch();
     if (t->ni > 0) {
         k_query_ref<true><<<grid_for(n_edges, 128, 16), 128, 0, (cudaStream_t)stream>>>(
@@ -1018,7 +937,7 @@ int lcs_bvh_query_ee_sym_capped(const lcs_bvh* t, const float* x0, const float* 
     k_query_ee_sym<<<grid_for(t->n, 128, 16), 128, 0, (cudaStream_t)stream>>>(
         t->wide4, t->sgo, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
         reinterpret_cast<const uint2*>(edges), d_hat, reinterpret_cast<uint2*>(pairs), capacity, d_count, capped,
-        t->maxdepth, t->work + 2);
+        t->maxdepth);
     lcs_count_launch();
     if (t->ni > 0) {  // a deep tree: the reference's full EE walk (its early exits break the symmetry)
         k_query_ref<true><<<grid_for(t->n, 128, 16), 128, 0, (cudaStream_t)stream>>>(

@@ -2600,6 +2600,14 @@ extern "C" int lcs_newton_reset_profile(lcs_newton* h)
     return LCS_OK;
 }
 
+extern "C" int lcs_newton_batch_query_tuning(const lcs_newton* h, uint32_t* vf_threads, uint32_t* ee_threads)
+{
+    if (!h || !h->batch) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_batch_query_tuning: needs a batch handle");
+    int rc = lcs_forest_query_tuning(h->face_forest, vf_threads, nullptr);
+    if (rc == LCS_OK) rc = lcs_forest_query_tuning(h->edge_forest, ee_threads, nullptr);
+    return rc;
+}
+
 extern "C" int lcs_newton_batch_tuning(const lcs_newton* h, uint32_t* chunks_per_cta, float* solve_ms)
 {
     if (!h || !h->pcg) return lcs_fail(LCS_ERR_INVALID, "lcs_newton_batch_tuning: bad handle");

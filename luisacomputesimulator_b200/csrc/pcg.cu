@@ -1141,12 +1141,28 @@ struct ResArgs {
 // takes the slices whose cost prefix reaches c / P of the total, with at most `cap` slices per block and
 // at least one, and every later block still able to take the rest.  One block of 1024 threads: the
 // prefix by block scans, the ideal cuts by one binary search per block, the clamping in one thread.
-constexpr uint32_t kResSliceBase = 2;
+// Cost weights of a slice's work (compile-time; the defaults count every group alike): material groups held
+// in shared memory (the first `gres` of the slice), material groups read from L2, contact groups (their
+// columns mostly belong to other blocks), and the diagonal and vectors.
+#ifndef LCS_RES_W_SMEM
+#define LCS_RES_W_SMEM 1
+#endif
+#ifndef LCS_RES_W_L2
+#define LCS_RES_W_L2 1
+#endif
+#ifndef LCS_RES_W_CONTACT
+#define LCS_RES_W_CONTACT 1
+#endif
+#ifndef LCS_RES_SLICE_BASE
+#define LCS_RES_SLICE_BASE 2
+#endif
+constexpr uint32_t kResSliceBase = LCS_RES_SLICE_BASE;
 constexpr uint32_t kResMaxSlices = kResMaxBlocks * (kResThreads / 32);  // the partition's shared prefix
 
 __global__ void __launch_bounds__(1024) k_res_partition(uint32_t S, uint32_t P, uint32_t cap, const uint32_t* __restrict__ m_ptr,
                                                         const uint32_t* __restrict__ c_ptr, const int* __restrict__ c_ok,
-                                                        uint32_t* __restrict__ part, uint32_t* __restrict__ owner)
+                                                        uint32_t* __restrict__ part, uint32_t* __restrict__ owner,
+                                                        uint32_t gres)
 {
     __shared__ uint32_t prefix[kResMaxSlices + 1];  // cost of slices [0, s)
     __shared__ uint32_t cut[kResMaxBlocks + 1];
@@ -1160,8 +1176,9 @@ __global__ void __launch_bounds__(1024) k_res_partition(uint32_t S, uint32_t P, 
         const uint32_t sl = base + t;
         uint32_t v = 0u;
         if (sl < S) {
-            v = ((m_ptr[sl + 1] - m_ptr[sl]) >> 2) + kResSliceBase;
-            if (cs) v += (c_ptr[sl + 1] - c_ptr[sl]) >> 2;
+            const uint32_t mg = (m_ptr[sl + 1] - m_ptr[sl]) >> 2, ms = mg < gres ? mg : gres;
+            v = LCS_RES_W_SMEM * ms + LCS_RES_W_L2 * (mg - ms) + kResSliceBase;
+            if (cs) v += LCS_RES_W_CONTACT * ((c_ptr[sl + 1] - c_ptr[sl]) >> 2);
         }
         uint32_t incl = v;
 #pragma unroll
@@ -2090,7 +2107,7 @@ static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* 
     const int grid = (int)((P->n + kRowThreads - 1) / kRowThreads);
     if (pipe && sell && !(o.flags & kPcgNoResident) && res_setup(P) == LCS_OK) {
         k_res_partition<<<1, 1024, 0, s>>>(P->res_slices, P->res_blocks, P->res_max_slices, m_ptr, a.c_ptr, a.c_ok,
-                                           P->res_part, P->res_owner);
+                                           P->res_part, P->res_owner, (uint32_t)P->res_gres);
         lcs_count_launch();
         ResArgs ra{a, P->res_part, P->res_owner, P->flags, P->res_slices, P->res_max_slices, P->res_gres};
         void* rargs[] = {&ra};

@@ -267,6 +267,13 @@ class NewtonBatch:
         A.check(self.lib.lcs_newton_batch_tuning(self.h, C.byref(t), C.byref(ms)), "lcs_newton_batch_tuning")
         return int(t.value), float(ms.value)
 
+    def query_tuning(self):
+        """(VF, EE) threads per block picked by the traversal autotuner on the first step (0 before it)."""
+        a, b = C.c_uint32(), C.c_uint32()
+        A.check(self.lib.lcs_newton_batch_query_tuning(self.h, C.byref(a), C.byref(b)),
+                "lcs_newton_batch_query_tuning")
+        return int(a.value), int(b.value)
+
     def scene_stats(self, k):
         st = A.NewtonStats()
         A.check(self.lib.lcs_newton_scene_stats(self.h, k, C.byref(st)), "lcs_newton_scene_stats")

@@ -102,16 +102,22 @@ def test_forest_candidate_sets_equal_per_scene_oracle(batch):
         want_vf.append(np.asarray(vf, np.int64).reshape(-1, 2) + np.array([c["vo"][k], c["fo"][k]]))
         want_ee.append(np.asarray(ee, np.int64).reshape(-1, 2) + c["eo"][k])
     want_vf, want_ee = np.concatenate(want_vf), np.concatenate(want_ee)
+    # the first query of a forest tunes its launch shape (one run per shape, the count restored in between);
+    # the second uses the tuned shape and appends behind the first: both must give the oracle's sets
     for q, want in (("vf", want_vf), ("ee", want_ee)):
-        cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
-        pairs = torch.zeros((len(want) + 64, 2), dtype=torch.int32, device="cuda")
-        if q == "vf":
-            ff.query_vf(xd, x1d, dev(c["vscene"]), dh, off, pairs, cnt)
-        else:
-            fe.query_ee(xd, x1d, edd, dh, off, pairs, cnt)
-        n = int(host(cnt, np.uint32)[0])
-        assert n == len(want)
-        np.testing.assert_array_equal(SC.sorted_pairs(host(pairs, np.uint32)[:n]), SC.sorted_pairs(want))
+        cnt = torch.full((1,), 5, dtype=torch.int32, device="cuda")  # appends start behind 5 earlier pairs
+        pairs = torch.zeros((2 * len(want) + 64, 2), dtype=torch.int32, device="cuda")
+        for rep in range(2):
+            if q == "vf":
+                ff.query_vf(xd, x1d, dev(c["vscene"]), dh, off, pairs, cnt)
+            else:
+                fe.query_ee(xd, x1d, edd, dh, off, pairs, cnt)
+            n = int(host(cnt, np.uint32)[0])
+            assert n == 5 + (rep + 1) * len(want)
+            got = host(pairs, np.uint32)[5 + rep * len(want): n]
+            np.testing.assert_array_equal(SC.sorted_pairs(got), SC.sorted_pairs(want))
+        threads, ms = (ff if q == "vf" else fe).query_tuning()
+        assert threads in (64, 128, 256) and ms > 0.0
 
 
 @pytest.mark.parametrize("fp64", [False, True])
