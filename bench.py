@@ -68,8 +68,10 @@ def args_():
     p.add_argument("--plain-sample", type=int, default=32, help="requests/scenes timed through the plain loop")
     p.add_argument("--requests", type=int, default=64, help="serve workload: requests")
     p.add_argument("--rate", type=float, default=200.0, help="serve workload: Poisson arrival rate (1/s)")
-    p.add_argument("--max-batches", type=int, default=2, help="serve workload: batches in flight")
-    p.add_argument("--gather", type=float, default=0.4, help="serve workload: admission gather window (s)")
+    p.add_argument("--max-batches", type=int, default=3, help="serve workload: batches in flight")
+    p.add_argument("--gather", type=float, default=0.05,
+                   help="serve workload: admission gather window (s); requests arriving while the batches in flight "
+                        "run wait for a free slot and are admitted together")
     p.add_argument("--no-plain", action="store_true", help="batch/serve: skip the plain-loop comparator")
     return p.parse_args()
 
@@ -716,6 +718,9 @@ def run_serve(a):
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                       "max": float(lat.max())},
         "batches": [{k: round(v, 3) if isinstance(v, float) else v for k, v in b.items()} for b in server.log],
+        # batches admitted while another batch was still on the GPU (continuous batching at work)
+        "batches_admitted_while_others_ran": sum(
+            1 for b in server.log if any(o is not b and o["start"] < b["start"] < o["done"] for o in server.log)),
         "wall_s": wall, "gpu_launches": int(launches),
         "alone_vs_mix_max_rel_dev": max(dev) if dev else None,
         "alone_vs_alone_max_rel_dev": max(rerun) if rerun else None,
