@@ -314,7 +314,9 @@ __global__ void __launch_bounds__(256) k_f_query(const float4* __restrict__ wide
         while (sp > 0) {
             const uint32_t node = stack[--sp];
             const float4* r = wide + 4 * node;
-            const float4 a0 = __ldg(r + 0), a1 = __ldg(r + 1), b0 = __ldg(r + 2), b1 = __ldg(r + 3);
+            float4 a0, a1, b0, b1;
+            ld_slot(r, a0, a1);
+            ld_slot(r + 2, b0, b1);
             bool stop = false;
             uint32_t hit[2];
             uint32_t nhit = 0;

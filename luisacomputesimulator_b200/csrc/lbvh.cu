@@ -407,7 +407,7 @@ __global__ void __launch_bounds__(128) k_query(const float4* __restrict__ wide4,
             const float4* r = wide4 + 8 * node;
             float4 rec[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) rec[j] = __ldg(r + j);
+            for (int j = 0; j < 4; ++j) ld_slot(r + 2 * j, rec[2 * j], rec[2 * j + 1]);
             bool stop = false;
             uint2 hit[4];
             uint32_t nhit = 0;
@@ -489,7 +489,8 @@ __global__ void __launch_bounds__(128) k_query_ref(const float4* __restrict__ wi
             uint32_t nhit = 0;
 #pragma unroll
             for (int side = 0; side < 2; ++side) {
-                const float4 mn = __ldg(rec + 2 * side), mx = __ldg(rec + 2 * side + 1);
+                float4 mn, mx;
+                ld_slot(rec + 2 * side, mn, mx);
                 if (!stop && overlap(mn, mx, box)) {
                     const uint32_t code = __float_as_uint(mn.w);
                     if (code & 0x80000000u) {
@@ -552,7 +553,7 @@ __global__ void __launch_bounds__(128) k_query_ee_sym(const float4* __restrict__
             const float4* node_rec = wide4 + 8 * node;
             float4 rec[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) rec[j] = __ldg(node_rec + j);
+            for (int j = 0; j < 4; ++j) ld_slot(node_rec + 2 * j, rec[2 * j], rec[2 * j + 1]);
             bool stop = false;
             uint2 hit[4];
             uint32_t nhit = 0;
