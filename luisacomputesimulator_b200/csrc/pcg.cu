@@ -1742,6 +1742,11 @@ struct lcs_pcg {
     std::vector<uint32_t> class_host;
     cudaStream_t class_stream[5] = {};
     cudaEvent_t class_fork = nullptr, class_join[5] = {};
+    // the CSR material matrix of lcs_pcg_solve rewritten as SELL-32 for the row-resident solves
+    uint32_t *msell_width = nullptr, *msell_ptr = nullptr, *msell_col = nullptr;
+    float* msell_val = nullptr;
+    int* msell_ok = nullptr;
+    uint32_t msell_cap = 0;  // slots the buffers hold
 };
 
 static constexpr int kRowLanes = 4;
@@ -1833,7 +1838,8 @@ extern "C" int lcs_pcg_destroy(lcs_pcg* p)
 {
     if (!p) return LCS_OK;
     void* ptrs[] = {p->r, p->z, p->p, p->q, p->minv, p->part, p->part_f, p->scal, p->bar, p->flags, p->d_stats,
-                    p->cpart, p->class_scenes, p->res_part, p->res_owner};
+                    p->cpart, p->class_scenes, p->res_part, p->res_owner, p->msell_width, p->msell_ptr,
+                    p->msell_col, p->msell_val, p->msell_ok};
     for (int k = 0; k < 5; ++k) {
         if (p->class_stream[k]) {
             cudaStreamSynchronize(p->class_stream[k]);
@@ -2065,6 +2071,50 @@ int lcs_contact_to_sell(uint32_t n, const lcs_bsr* B, uint32_t* width, uint32_t*
 
 int lcs_pcg_resident(lcs_pcg* P) { return P && res_setup(P) == LCS_OK ? 1 : 0; }
 
+// The CSR material matrix of lcs_pcg_solve as SELL-32, the layout the Newton loop's producers write: slot
+// order is CSR order, so each row's block products are summed in the order of the CSR walk.  The padded
+// slot count is read back once per call; the buffers grow when it exceeds the last call's.
+static int material_to_sell(lcs_pcg* P, const lcs_bsr* A, cudaStream_t s)
+{
+    const uint32_t n = P->n, S = (n + 31) / 32;
+    if (!P->msell_width) {
+        if (cudaMalloc((void**)&P->msell_width, sizeof(uint32_t) * S) != cudaSuccess ||
+            cudaMalloc((void**)&P->msell_ptr, sizeof(uint32_t) * (S + 1)) != cudaSuccess ||
+            cudaMalloc((void**)&P->msell_ok, sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            return lcs_fail(LCS_ERR_CUDA, "lcs_pcg_solve: SELL buffers for the material matrix: allocation failed");
+        }
+    }
+    k_csell_width<<<grid_for((uint64_t)S * 32, 256), 256, 0, s>>>(n, A->row_ptr, P->msell_width);
+    k_csell_scan<<<1, 1024, 0, s>>>(S, P->msell_width, P->msell_ptr, P->msell_cap, P->msell_ok);
+    lcs_count_launch();
+    lcs_count_launch();
+    uint32_t slots = 0;
+    LCS_CUDA_TRY(cudaMemcpyAsync(&slots, P->msell_ptr + S, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    LCS_CUDA_TRY(cudaStreamSynchronize(s));
+    if (slots > P->msell_cap) {
+        if (P->msell_col) cudaFree(P->msell_col);
+        if (P->msell_val) cudaFree(P->msell_val);
+        P->msell_col = nullptr;
+        P->msell_val = nullptr;
+        P->msell_cap = 0;
+        const uint32_t cap = slots + slots / 8 + 128;
+        if (cudaMalloc((void**)&P->msell_col, sizeof(uint32_t) * 32 * (size_t)cap) != cudaSuccess ||
+            cudaMalloc((void**)&P->msell_val, sizeof(float) * 9 * 32 * (size_t)cap) != cudaSuccess) {
+            cudaGetLastError();
+            return lcs_fail(LCS_ERR_CUDA, "lcs_pcg_solve: SELL buffers for the material matrix: allocation failed");
+        }
+        P->msell_cap = cap;
+        k_csell_scan<<<1, 1024, 0, s>>>(S, P->msell_width, P->msell_ptr, P->msell_cap, P->msell_ok);
+        lcs_count_launch();
+    }
+    k_csell_fill<<<grid_for((uint64_t)S * 32, 256), 256, 0, s>>>(n, A->row_ptr, A->col, A->val, P->msell_ptr,
+                                                                  P->msell_ok, P->msell_col, P->msell_val);
+    lcs_count_launch();
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
 // row-resident solve; LCS_ERR_CAPACITY when one thread per row does not fit co-resident
 static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* m_ptr, const uint32_t* m_col,
                       const float* m_val, Bsr B, const float4* b, float4* x, const lcs_pcg_opts& o,
@@ -2166,8 +2216,16 @@ extern "C" int lcs_pcg_solve(lcs_pcg* P, const float* diag, const lcs_bsr* A, co
     const float4* b4 = reinterpret_cast<const float4*>(b);
     float4* x4 = reinterpret_cast<float4*>(x);
     if ((o.flags & LCS_PCG_ROWS) && !(o.flags & LCS_PCG_PLAIN)) {
-        const Bsr Am = to_bsr(A);
-        const int rc = rows_solve(P, d4, 0, Am.rp, Am.col, Am.val, to_bsr(B), b4, x4, o, stats, s);
+        if (P->rows_capacity < 0) P->rows_capacity = (int)lcs_pcg_rows_capacity();
+        int rc = LCS_ERR_CAPACITY;
+        if ((int64_t)P->n <= P->rows_capacity) {
+            if (A && A->row_ptr) {  // the material matrix as SELL-32: coalesced block loads, slice-resident solve
+                if ((rc = material_to_sell(P, A, s))) return rc;
+                rc = rows_solve(P, d4, 1, P->msell_ptr, P->msell_col, P->msell_val, to_bsr(B), b4, x4, o, stats, s);
+            } else {
+                rc = rows_solve(P, d4, 0, nullptr, nullptr, nullptr, to_bsr(B), b4, x4, o, stats, s);
+            }
+        }
         if (rc != LCS_ERR_CAPACITY) return rc;  // too many rows for one thread each: persistent solve below
     }
     if (o.flags & LCS_PCG_PLAIN) {
