@@ -1123,6 +1123,9 @@ __global__ void __launch_bounds__(BS, 3) k_pcg_cg1(RowArgs a)
 // contact blocks in CSR order; the dot products in a fixed order over warps and blocks.
 constexpr int kResThreads = 640;                           // at most 20 slices (640 rows) per block
 constexpr int kResGroupBytes = 9 * 32 * 16 + 32 * 16;      // values + columns of one group of a slice
+// contact blocks of a block's rows are multiplied by all its threads, kResContactChunk at a time, the products
+// kept in shared memory (3 floats each) for the rows' owners
+constexpr int kResContactChunk = 1536;
 constexpr int kResMaxBlocks = 512;
 constexpr int kResDepWords = kResMaxBlocks / 32;
 
@@ -1304,10 +1307,9 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
     const uint32_t P = gridDim.x, c = blockIdx.x;
     const uint32_t s_lo = __ldcg(&ra.part[c]), s_hi = __ldcg(&ra.part[c + 1]);
     const uint32_t nsl = s_hi - s_lo, row0 = 32u * s_lo;
-    const uint32_t nloc = min(32u * s_hi, a.n) - row0;
     const int G = ra.gres;
-    float4* su = reinterpret_cast<float4*>(res_smem);                      // BT
-    double(*spart)[4] = reinterpret_cast<double(*)[4]>(su + BT);            // P
+    float* cprod = reinterpret_cast<float*>(res_smem);                     // [3][kResContactChunk]
+    double(*spart)[4] = reinterpret_cast<double(*)[4]>(cprod + 3 * kResContactChunk);  // P
     float4* sval = reinterpret_cast<float4*>(spart + P);                   // [max_slices * G][9][32]
     uint4* scol = reinterpret_cast<uint4*>(sval + (size_t)ra.max_slices * G * 9 * 32);  // [max_slices * G][32]
     const uint32_t t = threadIdx.x, ls = t >> 5, lane = t & 31u;
@@ -1380,17 +1382,42 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
         m3 = (cc * h - bb * k) * id; m4 = (aa * k - cc * g) * id; m5 = (bb * g - aa * h) * id;
         m6 = (bb * f - cc * e) * id; m7 = (cc * d - aa * f) * id; m8 = (aa * e - bb * d) * id;
     }
-    const bool c_sell = a.c_ptr && *a.c_ok;
-    // the slice's contact groups (fixed for the solve)
-    const uint32_t cg0 = c_sell && ls < nsl ? __ldcg(&a.c_ptr[slice]) >> 2 : 0u;
-    const uint32_t cg1 = c_sell && ls < nsl ? __ldcg(&a.c_ptr[slice + 1]) >> 2 : 0u;
-    auto ld_u = [&](uint32_t col) -> float4 {
-        const uint32_t lc = col - row0;
-        return lc < nloc ? su[lc] : __ldcg(&a.pg[col]);
+    // the contact blocks of the block's rows, [ce0, ce1) of the CSR, and of the lane's row (fixed for the solve)
+    const uint32_t row_end = min(32u * s_hi, a.n);
+    const uint32_t ce0 = a.B.rp ? __ldcg(&a.B.rp[row0]) : 0u, ce1 = a.B.rp ? __ldcg(&a.B.rp[row_end]) : 0u;
+    const uint32_t re0 = a.B.rp && own ? __ldcg(&a.B.rp[i]) : 0u, re1 = a.B.rp && own ? __ldcg(&a.B.rp[i + 1]) : 0u;
+    const bool c_vec = a.b_vec != 0;
+    const uint32_t c_total = a.B.rp ? __ldcg(&a.B.rp[a.n]) : 0u;
+    auto ld_u = [&](uint32_t col) -> float4 { return __ldcg(&a.pg[col]); };
+    // contact blocks [k0, k0 + cnt) times u, one block per thread, into shared memory
+    auto contact_chunk = [&](uint32_t k0, uint32_t cnt) {
+        for (uint32_t k = t; k < cnt; k += BT) {
+            const uint32_t e = k0 + k;
+            const float4 v = ld_u(__ldcg(&a.B.col[e]));
+            float m[9];
+            block9(fetch_block9(a.B.val, e, !c_vec || e + 1u >= c_total), m);
+            cprod[k] = __fmaf_rn(m[6], v.z, __fmaf_rn(m[3], v.y, m[0] * v.x));
+            cprod[kResContactChunk + k] = __fmaf_rn(m[7], v.z, __fmaf_rn(m[4], v.y, m[1] * v.x));
+            cprod[2 * kResContactChunk + k] = __fmaf_rn(m[8], v.z, __fmaf_rn(m[5], v.y, m[2] * v.x));
+        }
     };
-    // w = A u for the lane's row (k_pcg_cg1's row_matvec with the resident groups and local u); called by
-    // every lane of the block's slices, lanes past n compute a discarded value
+    // the products of chunk [k0, k0 + cnt) that belong to the lane's row, in CSR order
+    auto contact_add = [&](uint32_t k0, uint32_t cnt, float& o0, float& o1, float& o2) {
+        const uint32_t lo = max(re0, k0), hi = min(re1, k0 + cnt);
+        for (uint32_t e = lo; e < hi; ++e) {
+            o0 += cprod[e - k0];
+            o1 += cprod[kResContactChunk + e - k0];
+            o2 += cprod[2 * kResContactChunk + e - k0];
+        }
+    };
+    // w = A u for the lane's row: the diagonal block, the material groups (resident ones from shared memory)
+    // and the contact blocks.  Called by every thread of the block.  The rows that carry contacts sit in a
+    // few slices, so the contact blocks are not walked by their rows' warps: every thread of the block
+    // multiplies one block at a time (the CSR range of the block's rows, in chunks), and each row adds its
+    // own products in CSR order, as the row walk would.  Lanes past n compute a discarded value.
     auto matvec = [&](float v0, float v1, float v2, float& q0, float& q1, float& q2) {
+        const uint32_t first = min(ce1 - ce0, (uint32_t)kResContactChunk);
+        contact_chunk(ce0, first);
         const float4 c0 = __ldg(&a.diag[3 * row]), c1 = __ldg(&a.diag[3 * row + 1]), c2 = __ldg(&a.diag[3 * row + 2]);
         q0 = __fmaf_rn(c2.x, v2, __fmaf_rn(c1.x, v1, c0.x * v0));
         q1 = __fmaf_rn(c2.y, v2, __fmaf_rn(c1.y, v1, c0.y * v0));
@@ -1419,9 +1446,17 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
                 else o2 = o;
             }
         }
-        if (c_sell) sell_range(a.c_col, a.c_val, cg0, cg1, lane, ld_u, o0, o1, o2);
-        else if (a.B.rp)
-            contact_warp(a.B, row0 + 32u * ls, a.n, a.b_vec != 0, ld_u, o0, o1, o2);
+        if (ce1 > ce0) {
+            __syncthreads();
+            contact_add(ce0, first, o0, o1, o2);
+            for (uint32_t k0 = ce0 + first; k0 < ce1; k0 += kResContactChunk) {  // blocks with many contacts
+                const uint32_t cnt = min(ce1 - k0, (uint32_t)kResContactChunk);
+                __syncthreads();
+                contact_chunk(k0, cnt);
+                __syncthreads();
+                contact_add(k0, cnt, o0, o1, o2);
+            }
+        }
         q0 += o0;
         q1 += o1;
         q2 += o2;
@@ -1435,12 +1470,9 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
     float u0, u1, u2, w0 = 0.f, w1 = 0.f, w2 = 0.f;
     LCS_MINV(r0, r1, r2, u0, u1, u2)
     unsigned tag = 1u;
-    if (own) {
-        su[t] = make_float4(u0, u1, u2, 0.0f);
-        __stcg(&a.pg[i], make_float4(u0, u1, u2, 0.0f));
-    }
+    if (own) __stcg(&a.pg[i], make_float4(u0, u1, u2, 0.0f));
     if (!res_publish_wait(ra.flags, tag, s_dep, a.stats, &s_fail)) return;
-    if (ls < nsl) matvec(u0, u1, u2, w0, w1, w2);  // whole warps (the contact product is warp-wide)
+    matvec(u0, u1, u2, w0, w1, w2);  // every warp (block barrier inside)
     float x0 = 0.f, x1 = 0.f, x2 = 0.f, p0 = 0.f, p1 = 0.f, p2 = 0.f, sd0 = 0.f, sd1 = 0.f, sd2 = 0.f;
     float gamma_old = 0.0f, alpha_old = 0.0f, norm_r0 = 0.0f, norm_r = 0.0f, gamma = 0.0f;
     int iter = 0, status = 0;
@@ -1489,12 +1521,9 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
         r0 -= alpha * sd0; r1 -= alpha * sd1; r2 -= alpha * sd2;
         LCS_MINV(r0, r1, r2, u0, u1, u2)
         ++tag;
-        if (own) {
-            su[t] = make_float4(u0, u1, u2, 0.0f);
-            __stcg(&a.pg[i], make_float4(u0, u1, u2, 0.0f));
-        }
+        if (own) __stcg(&a.pg[i], make_float4(u0, u1, u2, 0.0f));
         if (!res_publish_wait(ra.flags, tag, s_dep, a.stats, &s_fail)) return;
-        if (ls < nsl) matvec(u0, u1, u2, w0, w1, w2);
+        matvec(u0, u1, u2, w0, w1, w2);
         gamma_old = gamma;
         alpha_old = alpha;
     }
@@ -1716,6 +1745,14 @@ __global__ void __launch_bounds__(kBatchThreads) k_pcg_batch(BatchArgs a)
 
 }  // namespace
 
+// a CSR matrix rewritten as SELL-32 (4-slot groups): per-slice widths and slot offsets, columns, values
+struct SellBuf {
+    uint32_t *width = nullptr, *ptr = nullptr, *col = nullptr;
+    float* val = nullptr;
+    int* ok = nullptr;
+    uint32_t cap = 0;  // slots the buffers hold
+};
+
 struct lcs_pcg {
     uint32_t n = 0;
     float4 *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *minv = nullptr;
@@ -1742,11 +1779,8 @@ struct lcs_pcg {
     std::vector<uint32_t> class_host;
     cudaStream_t class_stream[5] = {};
     cudaEvent_t class_fork = nullptr, class_join[5] = {};
-    // the CSR material matrix of lcs_pcg_solve rewritten as SELL-32 for the row-resident solves
-    uint32_t *msell_width = nullptr, *msell_ptr = nullptr, *msell_col = nullptr;
-    float* msell_val = nullptr;
-    int* msell_ok = nullptr;
-    uint32_t msell_cap = 0;  // slots the buffers hold
+    // the CSR material and contact matrices of lcs_pcg_solve rewritten as SELL-32 for the row-resident solves
+    SellBuf msell, csell;
 };
 
 static constexpr int kRowLanes = 4;
@@ -1838,8 +1872,9 @@ extern "C" int lcs_pcg_destroy(lcs_pcg* p)
 {
     if (!p) return LCS_OK;
     void* ptrs[] = {p->r, p->z, p->p, p->q, p->minv, p->part, p->part_f, p->scal, p->bar, p->flags, p->d_stats,
-                    p->cpart, p->class_scenes, p->res_part, p->res_owner, p->msell_width, p->msell_ptr,
-                    p->msell_col, p->msell_val, p->msell_ok};
+                    p->cpart, p->class_scenes, p->res_part, p->res_owner, p->msell.width, p->msell.ptr,
+                    p->msell.col, p->msell.val, p->msell.ok, p->csell.width, p->csell.ptr, p->csell.col,
+                    p->csell.val, p->csell.ok};
     for (int k = 0; k < 5; ++k) {
         if (p->class_stream[k]) {
             cudaStreamSynchronize(p->class_stream[k]);
@@ -1947,7 +1982,7 @@ static int res_setup(lcs_pcg* P)
     const uint32_t max_slices = S < (uint32_t)(kResThreads / 32) ? S : (uint32_t)(kResThreads / 32);
     cudaFuncAttributes fa;
     if (cudaFuncGetAttributes(&fa, k_pcg_res<kResThreads>) != cudaSuccess) return LCS_ERR_CAPACITY;
-    const size_t base = 16 * (size_t)kResThreads + 32 * (size_t)blocks;
+    const size_t base = sizeof(float) * 3 * kResContactChunk + 32 * (size_t)blocks;
     const size_t avail = (size_t)optin > fa.sharedSizeBytes + base ? (size_t)optin - fa.sharedSizeBytes - base : 0;
     size_t gres = avail / ((size_t)max_slices * kResGroupBytes);
     if (gres > 8) gres = 8;
@@ -2071,45 +2106,45 @@ int lcs_contact_to_sell(uint32_t n, const lcs_bsr* B, uint32_t* width, uint32_t*
 
 int lcs_pcg_resident(lcs_pcg* P) { return P && res_setup(P) == LCS_OK ? 1 : 0; }
 
-// The CSR material matrix of lcs_pcg_solve as SELL-32, the layout the Newton loop's producers write: slot
-// order is CSR order, so each row's block products are summed in the order of the CSR walk.  The padded
-// slot count is read back once per call; the buffers grow when it exceeds the last call's.
-static int material_to_sell(lcs_pcg* P, const lcs_bsr* A, cudaStream_t s)
+// A CSR matrix of lcs_pcg_solve as SELL-32, the layout the Newton loop's producers write: slot order is
+// CSR order, so each row's block products are summed in the order of the CSR walk.  The padded slot count
+// is read back once per call; the buffers grow when it exceeds the last call's.
+static int csr_to_sell(SellBuf& sb, uint32_t n, const lcs_bsr* M, cudaStream_t s)
 {
-    const uint32_t n = P->n, S = (n + 31) / 32;
-    if (!P->msell_width) {
-        if (cudaMalloc((void**)&P->msell_width, sizeof(uint32_t) * S) != cudaSuccess ||
-            cudaMalloc((void**)&P->msell_ptr, sizeof(uint32_t) * (S + 1)) != cudaSuccess ||
-            cudaMalloc((void**)&P->msell_ok, sizeof(int)) != cudaSuccess) {
+    const uint32_t S = (n + 31) / 32;
+    if (!sb.width) {
+        if (cudaMalloc((void**)&sb.width, sizeof(uint32_t) * S) != cudaSuccess ||
+            cudaMalloc((void**)&sb.ptr, sizeof(uint32_t) * (S + 1)) != cudaSuccess ||
+            cudaMalloc((void**)&sb.ok, sizeof(int)) != cudaSuccess) {
             cudaGetLastError();
-            return lcs_fail(LCS_ERR_CUDA, "lcs_pcg_solve: SELL buffers for the material matrix: allocation failed");
+            return lcs_fail(LCS_ERR_CUDA, "lcs_pcg_solve: SELL-32 buffers: allocation failed");
         }
     }
-    k_csell_width<<<grid_for((uint64_t)S * 32, 256), 256, 0, s>>>(n, A->row_ptr, P->msell_width);
-    k_csell_scan<<<1, 1024, 0, s>>>(S, P->msell_width, P->msell_ptr, P->msell_cap, P->msell_ok);
+    k_csell_width<<<grid_for((uint64_t)S * 32, 256), 256, 0, s>>>(n, M->row_ptr, sb.width);
+    k_csell_scan<<<1, 1024, 0, s>>>(S, sb.width, sb.ptr, sb.cap, sb.ok);
     lcs_count_launch();
     lcs_count_launch();
     uint32_t slots = 0;
-    LCS_CUDA_TRY(cudaMemcpyAsync(&slots, P->msell_ptr + S, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    LCS_CUDA_TRY(cudaMemcpyAsync(&slots, sb.ptr + S, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     LCS_CUDA_TRY(cudaStreamSynchronize(s));
-    if (slots > P->msell_cap) {
-        if (P->msell_col) cudaFree(P->msell_col);
-        if (P->msell_val) cudaFree(P->msell_val);
-        P->msell_col = nullptr;
-        P->msell_val = nullptr;
-        P->msell_cap = 0;
+    if (slots > sb.cap) {
+        if (sb.col) cudaFree(sb.col);
+        if (sb.val) cudaFree(sb.val);
+        sb.col = nullptr;
+        sb.val = nullptr;
+        sb.cap = 0;
         const uint32_t cap = slots + slots / 8 + 128;
-        if (cudaMalloc((void**)&P->msell_col, sizeof(uint32_t) * 32 * (size_t)cap) != cudaSuccess ||
-            cudaMalloc((void**)&P->msell_val, sizeof(float) * 9 * 32 * (size_t)cap) != cudaSuccess) {
+        if (cudaMalloc((void**)&sb.col, sizeof(uint32_t) * 32 * (size_t)cap) != cudaSuccess ||
+            cudaMalloc((void**)&sb.val, sizeof(float) * 9 * 32 * (size_t)cap) != cudaSuccess) {
             cudaGetLastError();
-            return lcs_fail(LCS_ERR_CUDA, "lcs_pcg_solve: SELL buffers for the material matrix: allocation failed");
+            return lcs_fail(LCS_ERR_CUDA, "lcs_pcg_solve: SELL-32 buffers: allocation failed");
         }
-        P->msell_cap = cap;
-        k_csell_scan<<<1, 1024, 0, s>>>(S, P->msell_width, P->msell_ptr, P->msell_cap, P->msell_ok);
+        sb.cap = cap;
+        k_csell_scan<<<1, 1024, 0, s>>>(S, sb.width, sb.ptr, sb.cap, sb.ok);
         lcs_count_launch();
     }
-    k_csell_fill<<<grid_for((uint64_t)S * 32, 256), 256, 0, s>>>(n, A->row_ptr, A->col, A->val, P->msell_ptr,
-                                                                  P->msell_ok, P->msell_col, P->msell_val);
+    k_csell_fill<<<grid_for((uint64_t)S * 32, 256), 256, 0, s>>>(n, M->row_ptr, M->col, M->val, sb.ptr, sb.ok, sb.col,
+                                                                  sb.val);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
     return LCS_OK;
@@ -2219,9 +2254,13 @@ extern "C" int lcs_pcg_solve(lcs_pcg* P, const float* diag, const lcs_bsr* A, co
         if (P->rows_capacity < 0) P->rows_capacity = (int)lcs_pcg_rows_capacity();
         int rc = LCS_ERR_CAPACITY;
         if ((int64_t)P->n <= P->rows_capacity) {
-            if (A && A->row_ptr) {  // the material matrix as SELL-32: coalesced block loads, slice-resident solve
-                if ((rc = material_to_sell(P, A, s))) return rc;
-                rc = rows_solve(P, d4, 1, P->msell_ptr, P->msell_col, P->msell_val, to_bsr(B), b4, x4, o, stats, s);
+            if (A && A->row_ptr) {  // both matrices as SELL-32: coalesced block loads, slice-resident solve
+                if ((rc = csr_to_sell(P->msell, P->n, A, s))) return rc;
+                const bool cb = B && B->row_ptr;
+                if (cb && (rc = csr_to_sell(P->csell, P->n, B, s))) return rc;
+                rc = rows_solve(P, d4, 1, P->msell.ptr, P->msell.col, P->msell.val, to_bsr(B), b4, x4, o, stats, s,
+                                cb ? P->csell.ptr : nullptr, cb ? P->csell.col : nullptr,
+                                cb ? P->csell.val : nullptr, cb ? P->csell.ok : nullptr);
             } else {
                 rc = rows_solve(P, d4, 0, nullptr, nullptr, nullptr, to_bsr(B), b4, x4, o, stats, s);
             }
