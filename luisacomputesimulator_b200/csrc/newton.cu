@@ -1716,7 +1716,9 @@ int newton_iteration(lcs_newton* h)
                                      reinterpret_cast<const float*>(h->b), reinterpret_cast<float*>(h->dx), &o, h->bpcg,
                                      h->cluster, h->s);
         else if (h->sell) {
-            const bool cs = h->cs_val != nullptr;
+            // the slice-resident solve multiplies the contact blocks from the CSR itself; the others read them as SELL-32
+            const bool resident = h->cg1 && !h->global_matrix && lcs_pcg_resident(h->pcg);
+            const bool cs = h->cs_val != nullptr && !resident;
             if (cs && (rc = lcs_contact_to_sell(h->V, &Bc, h->cs_width, h->cs_ptr, h->cs_col, h->cs_val, h->cs_cap,
                                                 h->cs_ok, h->s)))
                 return rc;

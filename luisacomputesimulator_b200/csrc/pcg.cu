@@ -1139,31 +1139,32 @@ struct ResArgs {
     int gres;            // resident groups per slice
 };
 
-// Slices to blocks by cost, before each solve: a slice costs its material groups, its contact groups
-// (when the contact blocks are in SELL form) and kResSliceBase for the diagonal and the vectors; block c
-// takes the slices whose cost prefix reaches c / P of the total, with at most `cap` slices per block and
-// at least one, and every later block still able to take the rest.  One block of 1024 threads: the
-// prefix by block scans, the ideal cuts by one binary search per block, the clamping in one thread.
-// Cost weights of a slice's work (compile-time; the defaults count every group alike): material groups held
-// in shared memory (the first `gres` of the slice), material groups read from L2, contact groups (their
-// columns mostly belong to other blocks), and the diagonal and vectors.
+// Slices to blocks by cost, before each solve: a slice costs its material groups, its contact blocks (CSR)
+// and kResSliceBase for the diagonal and the vectors; block c takes the slices whose cost prefix reaches
+// c / P of the total, with at most `cap` slices per block and at least one, and every later block still
+// able to take the rest.  One block of 1024 threads: the prefix by block scans, the ideal cuts by one
+// binary search per block, the clamping in one thread.
+// Cost weights of a slice's work (compile-time), fitted to per-block A u times measured on the 88,800-row
+// tube system (about 0.02 us per slice, 0.04 per material group, 0.004 per contact block, whose gathers
+// are scattered): material groups held in shared memory (the first `gres` of the slice), material groups
+// read from L2, contact blocks (per 16), and the diagonal and vectors.
 #ifndef LCS_RES_W_SMEM
-#define LCS_RES_W_SMEM 1
+#define LCS_RES_W_SMEM 4
 #endif
 #ifndef LCS_RES_W_L2
-#define LCS_RES_W_L2 1
+#define LCS_RES_W_L2 4
 #endif
 #ifndef LCS_RES_W_CONTACT
-#define LCS_RES_W_CONTACT 1
+#define LCS_RES_W_CONTACT 4
 #endif
 #ifndef LCS_RES_SLICE_BASE
-#define LCS_RES_SLICE_BASE 2
+#define LCS_RES_SLICE_BASE 8
 #endif
 constexpr uint32_t kResSliceBase = LCS_RES_SLICE_BASE;
 constexpr uint32_t kResMaxSlices = kResMaxBlocks * (kResThreads / 32);  // the partition's shared prefix
 
 __global__ void __launch_bounds__(1024) k_res_partition(uint32_t S, uint32_t P, uint32_t cap, const uint32_t* __restrict__ m_ptr,
-                                                        const uint32_t* __restrict__ c_ptr, const int* __restrict__ c_ok,
+                                                        const uint32_t* __restrict__ c_rp, uint32_t n,
                                                         uint32_t* __restrict__ part, uint32_t* __restrict__ owner,
                                                         uint32_t gres)
 {
@@ -1172,7 +1173,6 @@ __global__ void __launch_bounds__(1024) k_res_partition(uint32_t S, uint32_t P, 
     __shared__ uint32_t ws[32];
     __shared__ uint32_t carry;
     const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
-    const bool cs = c_ptr && c_ok && *c_ok;
     if (t == 0) carry = 0u;
     __syncthreads();
     for (uint32_t base = 0; base < S; base += 1024u) {
@@ -1181,7 +1181,7 @@ __global__ void __launch_bounds__(1024) k_res_partition(uint32_t S, uint32_t P, 
         if (sl < S) {
             const uint32_t mg = (m_ptr[sl + 1] - m_ptr[sl]) >> 2, ms = mg < gres ? mg : gres;
             v = LCS_RES_W_SMEM * ms + LCS_RES_W_L2 * (mg - ms) + kResSliceBase;
-            if (cs) v += LCS_RES_W_CONTACT * ((c_ptr[sl + 1] - c_ptr[sl]) >> 2);
+            if (c_rp) v += (LCS_RES_W_CONTACT * (c_rp[min(32u * sl + 32u, n)] - c_rp[32u * sl])) >> 4;
         }
         uint32_t incl = v;
 #pragma unroll
@@ -2191,7 +2191,7 @@ static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* 
     void* args[] = {&a};
     const int grid = (int)((P->n + kRowThreads - 1) / kRowThreads);
     if (pipe && sell && !(o.flags & kPcgNoResident) && res_setup(P) == LCS_OK) {
-        k_res_partition<<<1, 1024, 0, s>>>(P->res_slices, P->res_blocks, P->res_max_slices, m_ptr, a.c_ptr, a.c_ok,
+        k_res_partition<<<1, 1024, 0, s>>>(P->res_slices, P->res_blocks, P->res_max_slices, m_ptr, a.B.rp, P->n,
                                            P->res_part, P->res_owner, (uint32_t)P->res_gres);
         lcs_count_launch();
         ResArgs ra{a, P->res_part, P->res_owner, P->flags, P->res_slices, P->res_max_slices, P->res_gres};
@@ -2254,9 +2254,11 @@ extern "C" int lcs_pcg_solve(lcs_pcg* P, const float* diag, const lcs_bsr* A, co
         if (P->rows_capacity < 0) P->rows_capacity = (int)lcs_pcg_rows_capacity();
         int rc = LCS_ERR_CAPACITY;
         if ((int64_t)P->n <= P->rows_capacity) {
-            if (A && A->row_ptr) {  // both matrices as SELL-32: coalesced block loads, slice-resident solve
+            if (A && A->row_ptr) {  // the material matrix as SELL-32: coalesced block loads, slice-resident solve
                 if ((rc = csr_to_sell(P->msell, P->n, A, s))) return rc;
-                const bool cb = B && B->row_ptr;
+                // contacts as SELL-32 for the row-resident kernels; the slice-resident one reads the CSR itself
+                const bool cb = B && B->row_ptr &&
+                                !((o.flags & LCS_PCG_SINGLE_REDUCTION) && !(o.flags & kPcgNoResident) && lcs_pcg_resident(P));
                 if (cb && (rc = csr_to_sell(P->csell, P->n, B, s))) return rc;
                 rc = rows_solve(P, d4, 1, P->msell.ptr, P->msell.col, P->msell.val, to_bsr(B), b4, x4, o, stats, s,
                                 cb ? P->csell.ptr : nullptr, cb ? P->csell.col : nullptr,
