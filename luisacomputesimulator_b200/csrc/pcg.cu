@@ -1271,15 +1271,92 @@ __device__ __forceinline__ bool res_publish_wait(unsigned* flags, unsigned tag, 
     return *s_fail == 0;
 }
 
-// The two bounded waits of the slice-resident solve (the reduction barrier and the neighbour-flag wait)
+// Grid-wide sums of the blocks' three partials without a counter barrier: block c stores its partials
+// tagged with the iteration (the low four mantissa bits of each double set to iter mod 15; 15 marks an
+// empty slot, the host fills the buffers with it before a solve), every block polls the 3 P slots of the
+// iteration's buffer until each carries the tag, clears the tag bits and sums the partials in block order
+// (the same sums in every block).  Slots alternate between two buffers by iteration parity: a block can
+// only rewrite a buffer after every block has read it, since its next partial needs the next iteration's
+// sums, which need every block's next partial, which each block writes only after reading this one.
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+constexpr unsigned long long kTagMask = 0xFull;
+
+template <int BT>
+__device__ __forceinline__ bool res_allgather3(double v0, double v1, double v2, unsigned long long* part, unsigned tag,
+                                               double (*spart)[4], lcs_pcg_stats* stats, volatile int* s_fail,
+                                               double& o0, double& o1, double& o2,
+                                               unsigned spin_limit = kBarrierSpinLimit)
+{
+    __shared__ double s[BT / 32][3];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v0 += __shfl_xor_sync(0xFFFFFFFFu, v0, o);
+        v1 += __shfl_xor_sync(0xFFFFFFFFu, v1, o);
+        v2 += __shfl_xor_sync(0xFFFFFFFFu, v2, o);
+    }
+    if (lane_id() == 0) {
+        s[threadIdx.x >> 5][0] = v0;
+        s[threadIdx.x >> 5][1] = v1;
+        s[threadIdx.x >> 5][2] = v2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+#pragma unroll
+        for (int w = 0; w < BT / 32; ++w) {
+            t0 += s[w][0];
+            t1 += s[w][1];
+            t2 += s[w][2];
+        }
+        unsigned long long* dst = part + 4 * (size_t)blockIdx.x;
+        st_relaxed_u64(dst + 0, ((unsigned long long)__double_as_longlong(t0) & ~kTagMask) | tag);
+        st_relaxed_u64(dst + 1, ((unsigned long long)__double_as_longlong(t1) & ~kTagMask) | tag);
+        st_relaxed_u64(dst + 2, ((unsigned long long)__double_as_longlong(t2) & ~kTagMask) | tag);
+    }
+    for (uint32_t k = threadIdx.x; k < 3 * gridDim.x; k += BT) {
+        const unsigned long long* src = part + 4 * (size_t)(k / 3) + k % 3;
+        unsigned long long bits;
+        unsigned it = 0;
+        while (((bits = ld_relaxed_u64(src)) & kTagMask) != tag) {
+            if (++it > spin_limit) {
+                *s_fail = 1;
+                stats->status = LCS_ERR_TIMEOUT;
+                break;
+            }
+        }
+        spart[k / 3][k % 3] = __longlong_as_double((long long)(bits & ~kTagMask));
+    }
+    __syncthreads();
+    if (*s_fail) return false;
+    Fetch3 f{0.0, 0.0, 0.0};
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += BT) {
+        f.v0 += spart[b][0];
+        f.v1 += spart[b][1];
+        f.v2 += spart[b][2];
+    }
+    grid_reduce3<BT>(f, o0, o1, o2);
+    return true;
+}
+
+// The two bounded waits of the slice-resident solve (the tagged reduction and the neighbour-flag wait)
 // with a wait that nothing satisfies: block `missing` neither arrives nor publishes, so every other block
 // must give up after spin_limit polls and report LCS_ERR_TIMEOUT (missing < 0: every block takes part and
 // the waits complete).  Each block waits for every other one.
-__global__ void k_wait_probe(int which, int missing, unsigned spin_limit, unsigned* count, unsigned* gen,
+__global__ void k_wait_probe(int which, int missing, unsigned spin_limit, unsigned long long* part,
                              unsigned* flags, lcs_pcg_stats* stats)
 {
     __shared__ int s_fail;
     __shared__ unsigned s_dep[kResDepWords];
+    __shared__ double spart[32][4];
     if (threadIdx.x == 0) s_fail = 0;
     for (uint32_t w = threadIdx.x; w < (uint32_t)kResDepWords; w += blockDim.x) {
         unsigned m = 0u;
@@ -1290,8 +1367,8 @@ __global__ void k_wait_probe(int which, int missing, unsigned spin_limit, unsign
     __syncthreads();
     if ((int)blockIdx.x == missing) return;
     if (which == 0) {
-        unsigned gen_seen = threadIdx.x == 0 ? ld_acquire(gen) : 0u;
-        pipe_barrier(count, gen, gen_seen, stats, &s_fail, spin_limit);
+        double o0, o1, o2;
+        res_allgather3<128>(1.0, 2.0, 3.0, part, 0u, spart, stats, &s_fail, o0, o1, o2, spin_limit);
     } else {
         res_publish_wait(flags, 1u, s_dep, stats, &s_fail, spin_limit);
     }
@@ -1319,7 +1396,6 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
     const uint32_t slice = s_lo + ls;
     if (t == 0) s_fail = 0;
     for (int w = t; w < kResDepWords; w += BT) s_dep[w] = 0u;
-    unsigned gen_seen = t == 0 ? ld_acquire(a.bar_gen) : 0u;
     const uint4* C4 = reinterpret_cast<const uint4*>(a.m_col);
     const float4* V4 = reinterpret_cast<const float4*>(a.m_val);
     uint32_t g0 = 0, g1 = 0;
@@ -1488,12 +1564,9 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
             dr = __fmaf_rn(r2, r2, __fmaf_rn(r1, r1, r0 * r0));
         }
         if (!own) dg = dd = dr = 0.0;
-        double* part = a.part + 4 * (size_t)P * (iter & 1);
-        block_partial3<BT>(dg, dd, dr, &part[4 * c]);
-        if (!pipe_barrier(a.bar_count, a.bar_gen, gen_seen, a.stats, &s_fail)) return;
-        grid_prefetch3<BT>(part, spart);
+        unsigned long long* part = reinterpret_cast<unsigned long long*>(a.part) + 4 * (size_t)P * (iter & 1);
         double sg, sdd, sr;
-        grid_collect3<BT>(spart, sg, sdd, sr);
+        if (!res_allgather3<BT>(dg, dd, dr, part, (unsigned)(iter % 15), spart, a.stats, &s_fail, sg, sdd, sr)) return;
         gamma = (float)sg;
         const float delta = (float)sdd;
         norm_r = sqrtf((float)sr);
@@ -1798,9 +1871,9 @@ extern "C" int lcs_debug_pcg_wait(int32_t which, int32_t missing_block, uint32_t
         return lcs_fail(LCS_ERR_INVALID, "lcs_debug_pcg_wait: spin_limit must be in [1, 2^24]");
     if (missing_block >= (int32_t)blocks) return lcs_fail(LCS_ERR_INVALID, "lcs_debug_pcg_wait: no such block");
     cudaStream_t s = (cudaStream_t)stream;
-    unsigned* words = nullptr;  // count, gen, flags (kResFlagStride per block)
+    unsigned* words = nullptr;  // tagged partials (8 words per block), flags (kResFlagStride per block)
     lcs_pcg_stats* st = nullptr;
-    const size_t n_words = 2 + (size_t)kResFlagStride * blocks;
+    const size_t n_words = 8 * (size_t)blocks + (size_t)kResFlagStride * blocks;
     LCS_CUDA_TRY(cudaMalloc(&words, 4 * n_words));
     if (cudaMalloc(&st, sizeof(lcs_pcg_stats)) != cudaSuccess) {
         cudaGetLastError();
@@ -1809,12 +1882,13 @@ extern "C" int lcs_debug_pcg_wait(int32_t which, int32_t missing_block, uint32_t
     }
     lcs_pcg_stats h{};
     int rc = LCS_OK;
-    if (cudaMemsetAsync(words, 0, 4 * n_words, s) != cudaSuccess || cudaMemsetAsync(st, 0, sizeof(h), s) != cudaSuccess)
+    if (cudaMemsetAsync(words, 0xFF, 32 * (size_t)blocks, s) != cudaSuccess ||
+        cudaMemsetAsync(words + 8 * (size_t)blocks, 0, 4 * (size_t)kResFlagStride * blocks, s) != cudaSuccess ||
+        cudaMemsetAsync(st, 0, sizeof(h), s) != cudaSuccess)
         rc = LCS_ERR_CUDA;
-    unsigned* count = words;
-    unsigned* gen = words + 1;
-    unsigned* flags = words + 2;
-    void* args[] = {&which, &missing_block, &spin_limit, &count, &gen, &flags, &st};
+    unsigned long long* part = reinterpret_cast<unsigned long long*>(words);
+    unsigned* flags = words + 8 * (size_t)blocks;
+    void* args[] = {&which, &missing_block, &spin_limit, &part, &flags, &st};
     if (rc == LCS_OK &&
         cudaLaunchCooperativeKernel((const void*)k_wait_probe, dim3(blocks), dim3(128), args, 0, s) != cudaSuccess)
         rc = LCS_ERR_CUDA;
@@ -2197,6 +2271,7 @@ static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* 
         ResArgs ra{a, P->res_part, P->res_owner, P->flags, P->res_slices, P->res_max_slices, P->res_gres};
         void* rargs[] = {&ra};
         LCS_CUDA_TRY(cudaMemsetAsync(P->flags, 0, sizeof(unsigned) * kResFlagStride * P->res_blocks, s));
+        LCS_CUDA_TRY(cudaMemsetAsync(P->part, 0xFF, sizeof(double) * 8 * P->res_blocks, s));  // empty slots
         LCS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_pcg_res<kResThreads>, dim3(P->res_blocks),
                                                  dim3(kResThreads), rargs, P->res_smem, s));
     } else if (pipe)
