@@ -1466,10 +1466,12 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
     const uint32_t c_total = a.B.rp ? __ldcg(&a.B.rp[a.n]) : 0u;
     auto ld_u = [&](uint32_t col) -> float4 { return __ldcg(&a.pg[col]); };
     // contact blocks [k0, k0 + cnt) times u, one block per thread, into shared memory
+    // the column of the thread's first contact block, fixed for the solve, stays in a register
+    const uint32_t c_col0 = t < ce1 - ce0 ? __ldcg(&a.B.col[ce0 + t]) : 0u;
     auto contact_chunk = [&](uint32_t k0, uint32_t cnt) {
         for (uint32_t k = t; k < cnt; k += BT) {
             const uint32_t e = k0 + k;
-            const float4 v = ld_u(__ldcg(&a.B.col[e]));
+            const float4 v = ld_u(e == ce0 + t ? c_col0 : __ldcg(&a.B.col[e]));
             float m[9];
             block9(fetch_block9(a.B.val, e, !c_vec || e + 1u >= c_total), m);
             cprod[k] = __fmaf_rn(m[6], v.z, __fmaf_rn(m[3], v.y, m[0] * v.x));
