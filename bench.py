@@ -688,7 +688,7 @@ def run_serve(a):
     lat = np.array([r.latency for r in done])
     span = max(r.done for r in done) - min(r.arrival for r in done)
     # alone == in the mix: two requests re-run alone through the same batched solver, and one of them alone
-    # twice (the run-to-run spread that float atomics alone produce over the solve)
+    # twice (the batches sum in a fixed order, LCS_NEWTON_DETERMINISTIC: both deviations are 0)
     dev, rerun = [], []
     for r in done[:2]:
         xs = []

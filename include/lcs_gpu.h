@@ -541,10 +541,19 @@ enum {
                                          pairs; FP64 sums) decreases (newton_solver.cpp:3790-3834).  Single scenes;
                                          the fused loop evaluates 7 step lengths per launch and decides on the
                                          device, the plain loop one per host round trip as the reference does. */
-    LCS_NEWTON_PCG_GLOBAL_MATRIX = 64 /* with LCS_NEWTON_PCG_SINGLE_REDUCTION: read the material matrix from
+    LCS_NEWTON_PCG_GLOBAL_MATRIX = 64, /* with LCS_NEWTON_PCG_SINGLE_REDUCTION: read the material matrix from
                                          global memory every iteration (the grid of 256-row blocks) instead of
                                          the slice-resident solve (one block per SM, its rows' leading matrix
                                          groups held in shared memory), which is used where the rows fit */
+    LCS_NEWTON_DETERMINISTIC = 128 /* sums without atomics: the cloth terms are evaluated per element and summed
+                                      per row and per block in element order, the contact pairs are sorted into a
+                                      canonical order (by type and vertex indices) before their gradient,
+                                      diagonal and off-diagonal blocks are summed in that order.  A scene's step
+                                      is then bit-identical from run to run and, in a batch, whatever the other
+                                      scenes are.  The reference accumulates with atomics (narrow_phase.cpp:
+                                      2550-2676, newton_solver.cpp:705-814); this flag has no counterpart
+                                      there.  Not with affine bodies or the energy line search; scenes below
+                                      2^21 vertices. */
 };
 
 typedef struct lcs_newton_stats {

@@ -182,6 +182,7 @@ LCS_NEWTON_PLAIN, LCS_NEWTON_FP64, LCS_NEWTON_PROFILE, LCS_NEWTON_PCG_SINGLE_RED
     1, 2, 4, 8, 16
 LCS_NEWTON_ENERGY_LINESEARCH = 32
 LCS_NEWTON_PCG_GLOBAL_MATRIX = 64
+LCS_NEWTON_DETERMINISTIC = 128
 PHASES = ["build", "material", "dcd_broad", "dcd_narrow", "assembly", "pcg", "ccd_broad", "ccd_narrow", "apply"]
 
 _lib = None

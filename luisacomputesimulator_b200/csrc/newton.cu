@@ -32,6 +32,7 @@
 #include "lcs_geom.cuh"
 #include "material.cuh"
 #include "abd.cuh"
+#include "radix_sort.cuh"
 
 using namespace lcs;
 
@@ -566,6 +567,321 @@ __global__ void k_bending_dihedral(uint32_t nb, const uint4* __restrict__ stenci
     }
 }
 
+// ---- deterministic assembly (LCS_NEWTON_DETERMINISTIC)
+// The producers above, split in two: each element writes its terms (gradient, Hessian blocks) to its own
+// slots of `el`, then every row and every material block sums its elements' terms in element order.  The
+// terms are computed by the same expressions as above and each sum adds them one at a time onto the same
+// start value (the inertia term for b and the diagonal, zero for a block), so only the order of the
+// additions is fixed.  Per element: spring 12 floats (gradient of end 0, then the Hessian block), face 64
+// (the three corner gradients, then the blocks (0,0) (1,1) (2,2) (0,1) (0,2) (1,2)), stencil 16 (dihedral:
+// the four gradients, stiffness, stiffness x angle defect; quadratic: the four gradients).
+__global__ void k_springs_det(uint32_t ne, const uint2* __restrict__ edges, const float* __restrict__ rest_len,
+                              const float* __restrict__ kper, float k_scalar, const float4* __restrict__ x,
+                              float* __restrict__ el)
+{
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+        const float k = kper ? kper[e] : k_scalar;
+        const uint2 ed = edges[e];
+        const float4 p0 = x[ed.x], p1 = x[ed.y];
+        const float dx = p0.x - p1.x, dy = p0.y - p1.y, dz = p0.z - p1.z;
+        const float l = fmaxf(sqrtf(dx * dx + dy * dy + dz * dz), 1.19209290E-7f);
+        const float L = rest_len[e];
+        const float C = l - L;
+        const float il = 1.0f / l, il2 = il * il;
+        float* o = el + 12 * (size_t)e;
+        o[0] = k * dx * il * C;
+        o[1] = k * dy * il * C;
+        o[2] = k * dz * il * C;
+        const float a = k * il2, c = k * fmaxf(1.0f - L * il, 0.0f);
+        const float d[3] = {dx, dy, dz};
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+            for (int r = 0; r < 3; ++r) o[3 + 3 * cc + r] = a * d[r] * d[cc] + c * ((r == cc ? 1.0f : 0.0f) - il2 * d[r] * d[cc]);
+    }
+}
+
+__global__ void k_stretch_bw98_det(uint32_t nf, const uint4* __restrict__ faces, const float4* __restrict__ dm,
+                                   const float* __restrict__ area, const float2* __restrict__ ml, float mu,
+                                   float lambda, const float4* __restrict__ x, float* __restrict__ el)
+{
+    for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x) {
+        const uint4 fc = faces[f];
+        const float2 m = ml ? ml[f] : make_float2(mu, lambda);
+        Bw98Out o;
+        bw98_face(ld3(x, fc.x), ld3(x, fc.y), ld3(x, fc.z), dm[f], m.x, m.y, area[f], o);
+        float* q = el + 64 * (size_t)f;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            q[3 * a] = o.g[a].x;
+            q[3 * a + 1] = o.g[a].y;
+            q[3 * a + 2] = o.g[a].z;
+        }
+#pragma unroll
+        for (int b = 0; b < 6; ++b)
+#pragma unroll
+            for (int c = 0; c < 9; ++c) q[9 + 9 * b + c] = o.K[b][c];
+    }
+}
+
+__global__ void k_bending_dihedral_det(uint32_t nb, const uint4* __restrict__ stencil, const float* __restrict__ rest_angle,
+                                       const float* __restrict__ hbar, const float* __restrict__ kper, float k,
+                                       float scaling, const float4* __restrict__ x, float* __restrict__ el)
+{
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nb; s += gridDim.x * blockDim.x) {
+        const uint4 e = stencil[s];
+        v3 g[4];
+        const float theta = dihedral_angle_grad(ld3(x, e.x), ld3(x, e.y), ld3(x, e.z), ld3(x, e.w), g);
+        const float stiff = ((kper ? kper[s] : k) * scaling) * hbar[s];
+        float* q = el + 16 * (size_t)s;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            q[3 * i] = g[i].x;
+            q[3 * i + 1] = g[i].y;
+            q[3 * i + 2] = g[i].z;
+        }
+        q[12] = stiff;
+        q[13] = stiff * (theta - rest_angle[s]);
+    }
+}
+
+__global__ void k_bending_det(uint32_t nb, const uint4* __restrict__ stencil, const float* __restrict__ Q, float k,
+                              const float4* __restrict__ x, const float4* __restrict__ rest, float* __restrict__ el)
+{
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nb; s += gridDim.x * blockDim.x) {
+        const uint4 st = stencil[s];
+        const uint32_t v[4] = {st.x, st.y, st.z, st.w};
+        float3 u[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float4 p = x[v[j]], r = rest[v[j]];
+            u[j] = make_float3(p.x - r.x, p.y - r.y, p.z - r.z);
+        }
+        const float* qq = Q + 16 * (size_t)s;
+        float* o = el + 16 * (size_t)s;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            float3 g = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float qij = k * qq[4 * i + j];
+                g.x += qij * u[j].x;
+                g.y += qij * u[j].y;
+                g.z += qij * u[j].z;
+            }
+            o[3 * i] = g.x;
+            o[3 * i + 1] = g.y;
+            o[3 * i + 2] = g.z;
+        }
+    }
+}
+
+// local pair t of a stencil's 12 ordered pairs (i, j), i != j, in the producers' loop order
+__device__ __forceinline__ void stencil_pair(uint32_t t, int& i, int& j)
+{
+    i = (int)(t / 3);
+    const int jj = (int)(t % 3);
+    j = jj < i ? jj : jj + 1;
+}
+
+struct DetEl {
+    const float* el;
+    size_t off_face, off_bend;
+    const float* Q;  // quadratic bending
+    float k_quad;
+};
+
+// b and the diagonal of each row: the inertia term already there, then its elements' terms in element order
+__global__ void k_det_rows(uint32_t n, const uint32_t* __restrict__ vptr, const uint2* __restrict__ vent, DetEl D,
+                           float4* __restrict__ b, float4* __restrict__ diag)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        float4 bv = b[v];
+        float4 dc[3] = {diag[3 * (size_t)v], diag[3 * (size_t)v + 1], diag[3 * (size_t)v + 2]};
+        auto add_block = [&](const float* K) {  // column-major [3 c + r]
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                dc[c].x += K[3 * c];
+                dc[c].y += K[3 * c + 1];
+                dc[c].z += K[3 * c + 2];
+            }
+        };
+        const uint32_t e1 = vptr[v + 1];
+        for (uint32_t q = vptr[v]; q < e1; ++q) {
+            const uint2 en = vent[q];
+            const uint32_t kind = en.y >> 4, a = en.y & 15u;
+            if (kind == 0) {  // spring: end 0 takes -g, end 1 +g; both the block
+                const float* o = D.el + 12 * (size_t)en.x;
+                if (a == 0) { bv.x += -o[0]; bv.y += -o[1]; bv.z += -o[2]; }
+                else { bv.x += o[0]; bv.y += o[1]; bv.z += o[2]; }
+                add_block(o + 3);
+            } else if (kind == 1) {  // face corner a
+                const float* o = D.el + D.off_face + 64 * (size_t)en.x;
+                bv.x += -o[3 * a]; bv.y += -o[3 * a + 1]; bv.z += -o[3 * a + 2];
+                add_block(o + 9 + 9 * a);
+            } else if (kind == 2) {  // dihedral stencil vertex a: -sd g_a, block stiff g_a g_a^T
+                const float* o = D.el + D.off_bend + 16 * (size_t)en.x;
+                const float stiff = o[12], sd = o[13];
+                const float gi[3] = {o[3 * a], o[3 * a + 1], o[3 * a + 2]};
+                bv.x += -(sd * gi[0]); bv.y += -(sd * gi[1]); bv.z += -(sd * gi[2]);
+                float K[9];
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int r = 0; r < 3; ++r) K[3 * c + r] = stiff * (gi[r] * gi[c]);
+                add_block(K);
+            } else {  // quadratic stencil vertex a: -g_a, block k Q_aa I
+                const float* o = D.el + D.off_bend + 16 * (size_t)en.x;
+                bv.x += -o[3 * a]; bv.y += -o[3 * a + 1]; bv.z += -o[3 * a + 2];
+                const float qaa = D.k_quad * D.Q[16 * (size_t)en.x + 5 * a];
+                dc[0].x += qaa;
+                dc[1].y += qaa;
+                dc[2].z += qaa;
+            }
+        }
+        b[v] = bv;
+        diag[3 * (size_t)v] = dc[0];
+        diag[3 * (size_t)v + 1] = dc[1];
+        diag[3 * (size_t)v + 2] = dc[2];
+    }
+}
+
+// each material block from zero: its elements' blocks in element order, written at its base (components cs apart)
+__global__ void k_det_blocks(uint32_t nblk, const uint32_t* __restrict__ bptr, const uint2* __restrict__ bent,
+                             const uint32_t* __restrict__ bbase, DetEl D, uint32_t cs, float* __restrict__ mat_val)
+{
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nblk; j += gridDim.x * blockDim.x) {
+        float acc[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) acc[q] = 0.0f;
+        const uint32_t e1 = bptr[j + 1];
+        for (uint32_t q = bptr[j]; q < e1; ++q) {
+            const uint2 en = bent[q];
+            const uint32_t kind = en.y >> 4, t = en.y & 15u;
+            if (kind == 0) {  // spring: -H in both directions
+                const float* H = D.el + 12 * (size_t)en.x + 3;
+#pragma unroll
+                for (int c = 0; c < 9; ++c) acc[c] += -H[c];
+            } else if (kind == 1) {  // face pair t: (0,1) (0,2) (1,0) (1,2) (2,0) (2,1) from blocks 3, 4, 3^T, 5, 4^T, 5^T
+                const float* o = D.el + D.off_face + 64 * (size_t)en.x;
+                const int m = t == 0 || t == 2 ? 3 : t == 1 || t == 4 ? 4 : 5;
+                const bool tr = t == 2 || t == 4 || t == 5;
+                const float* K = o + 9 + 9 * m;
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int r = 0; r < 3; ++r) acc[3 * c + r] += tr ? K[3 * r + c] : K[3 * c + r];
+            } else if (kind == 2) {  // dihedral pair (i, j): stiff g_i g_j^T
+                const float* o = D.el + D.off_bend + 16 * (size_t)en.x;
+                int i, jj;
+                stencil_pair(t, i, jj);
+                const float stiff = o[12];
+                const float gi[3] = {o[3 * i], o[3 * i + 1], o[3 * i + 2]};
+                const float gj[3] = {o[3 * jj], o[3 * jj + 1], o[3 * jj + 2]};
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int r = 0; r < 3; ++r) acc[3 * c + r] += stiff * (gi[r] * gj[c]);
+            } else {  // quadratic pair (i, j): k Q_ij I
+                int i, jj;
+                stencil_pair(t, i, jj);
+                const float qij = D.k_quad * D.Q[16 * (size_t)en.x + 4 * i + jj];
+                acc[0] += qij;
+                acc[4] += qij;
+                acc[8] += qij;
+            }
+        }
+        float* O = mat_val + bbase[j];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) O[(size_t)cs * c] = acc[c];
+    }
+}
+
+// Contact pairs in a canonical order: by (type, v0, v1) after (v2, v3), 21 bits per vertex index.
+// keys_lo: pass 1 (v2, v3); pass 2 re-keys the pass-1 order by (type, v0, v1) and sorts stably.
+__global__ void k_pair_keys(const lcs_pair* __restrict__ pairs, const uint32_t* d_count, uint32_t cap, int hi,
+                            const uint32_t* __restrict__ order, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                            uint32_t* d_n)
+{
+    const uint32_t n = pair_count(d_count, cap);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d_n = n;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t p = order ? order[k] : k;
+        const PairView P = load_pair(pairs, p);
+        keys[k] = hi ? ((uint64_t)P.type << 42) | ((uint64_t)P.v[0] << 21) | (uint64_t)P.v[1]
+                     : ((uint64_t)P.v[2] << 21) | (uint64_t)P.v[3];
+        vals[k] = p;
+    }
+}
+
+__global__ void k_pair_gather(const lcs_pair* __restrict__ pairs, const uint32_t* d_n, const uint32_t* __restrict__ order,
+                              lcs_pair* __restrict__ out)
+{
+    const uint32_t n = *d_n;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) out[k] = pairs[order[k]];
+}
+
+// row keys of the contact gradient / diagonal terms: 4 per pair (vertex i), pairs without contact last
+__global__ void k_cg_keys(const lcs_pair* __restrict__ pairs, const uint32_t* d_n, uint32_t n_rows,
+                          uint64_t* __restrict__ keys, uint32_t* __restrict__ vals, uint32_t* d_n4)
+{
+    const uint32_t n = *d_n;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d_n4 = 4 * n;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const PairView P = load_pair(pairs, k);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            keys[4 * (size_t)k + i] = P.type ? P.v[i] : n_rows;
+            vals[4 * (size_t)k + i] = 4u * k + (uint32_t)i;
+        }
+    }
+}
+
+// each row's contact gradient and diagonal block (k_grad_diag's terms), summed in canonical pair order and
+// added once; one thread per row segment
+__global__ void k_cg_rows(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals, const uint32_t* d_n4,
+                          uint32_t n_rows, const lcs_pair* __restrict__ pairs, float4* __restrict__ b,
+                          float4* __restrict__ diag)
+{
+    const uint32_t n = *d_n4;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const uint64_t key = keys[s];
+        if (key >= n_rows || (s > 0 && keys[s - 1] == key)) continue;
+        float g3[3] = {0.f, 0.f, 0.f}, h9[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) h9[q] = 0.0f;
+        for (uint32_t t = s; t < n && keys[t] == key; ++t) {
+            const uint32_t v = vals[t];
+            const PairView P = load_pair(pairs, v >> 2);
+            const float w = P.w[v & 3u];
+            const float g = P.k1 * w;
+            g3[0] += g * P.n.x;
+            g3[1] += g * P.n.y;
+            g3[2] += g * P.n.z;
+            const float h = P.k2 * w * w;
+            const float nn[3] = {P.n.x, P.n.y, P.n.z};
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int r = 0; r < 3; ++r) h9[3 * c + r] += h * (nn[r] * nn[c]);
+        }
+        const uint32_t r = (uint32_t)key;
+        float4 bv = b[r];
+        bv.x += g3[0];
+        bv.y += g3[1];
+        bv.z += g3[2];
+        b[r] = bv;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float4 d = diag[3 * (size_t)r + c];
+            d.x += h9[3 * c];
+            d.y += h9[3 * c + 1];
+            d.z += h9[3 * c + 2];
+            diag[3 * (size_t)r + c] = d;
+        }
+    }
+}
+
 // fn_apply_dx (newton_solver.cpp:491-503) with alpha = 1, and the |dx|_inf of the small-step test
 __global__ void k_apply_unit(uint32_t n, const float4* __restrict__ x0, const float4* __restrict__ dx, float4* __restrict__ x,
                              Status* st, AbdDev abd)
@@ -998,6 +1314,20 @@ struct lcs_newton {
     uint32_t *mat_rp = nullptr, *mat_col = nullptr, *spring_slots = nullptr, *bend_slots = nullptr, *face_slots = nullptr;
     float* mat_val = nullptr;
     bool sell = false;             // material matrix in SELL-32 for the row-resident PCG (fused mode)
+    // LCS_NEWTON_DETERMINISTIC: the cloth terms per element (det_el), then summed per row over the vertex's
+    // elements (det_vptr / det_vent) and per material block over its elements (det_bptr / det_bent, written at
+    // det_bbase), in element order; the contact pairs sorted into a canonical order and their gradient and
+    // diagonal blocks summed per row in that order
+    bool det = false;
+    float* det_el = nullptr;
+    size_t det_off_face = 0, det_off_bend = 0;  // float offsets of the face and stencil terms in det_el
+    uint32_t det_nblk = 0;
+    uint32_t *det_vptr = nullptr, *det_bptr = nullptr, *det_bbase = nullptr;
+    uint2 *det_vent = nullptr, *det_bent = nullptr;  // (element, kind << 4 | local index)
+    uint64_t *det_keys = nullptr, *det_keys_alt = nullptr;
+    uint32_t *det_vals = nullptr, *det_vals_alt = nullptr, *det_hist = nullptr, *det_n = nullptr;
+    lcs_pair* det_pairs = nullptr;  // the pairs in canonical order (scratch)
+    uint32_t det_cap = 0;           // pairs the contact scratch holds
     bool cg1 = false;              // single-reduction row-resident PCG (two grid synchronisations per iteration)
     size_t sell_vals = 0;          // floats in mat_val
     uint32_t *sell_ptr = nullptr, *sell_col = nullptr;
@@ -1084,6 +1414,13 @@ void free_contact(lcs_newton* h)
     h->dcd_ee = nullptr;
     h->pairs = nullptr;
     h->asmb = nullptr;
+    for (void* q : {(void*)h->det_keys, (void*)h->det_keys_alt, (void*)h->det_vals, (void*)h->det_vals_alt,
+                    (void*)h->det_hist, (void*)h->det_pairs})
+        if (q) cudaFree(q);
+    h->det_keys = h->det_keys_alt = nullptr;
+    h->det_vals = h->det_vals_alt = h->det_hist = nullptr;
+    h->det_pairs = nullptr;
+    h->det_cap = 0;
 }
 
 // (re)allocates the contact buffers whose capacity changed since they were allocated; the
@@ -1116,6 +1453,23 @@ int alloc_contact(lcs_newton* h)
         h->asmb = nullptr;
         e = dalloc(h->pairs, h->cap_pairs);
         h->alloc_pairs = h->cap_pairs;
+        if (e == cudaSuccess && h->det) {  // canonical pair order: 4 row keys per pair for the gradient sums
+            for (void* q : {(void*)h->det_keys, (void*)h->det_keys_alt, (void*)h->det_vals, (void*)h->det_vals_alt,
+                            (void*)h->det_hist, (void*)h->det_pairs})
+                if (q) cudaFree(q);
+            const uint32_t kc = 4 * h->cap_pairs;
+            h->det_keys = h->det_keys_alt = nullptr;
+            h->det_vals = h->det_vals_alt = h->det_hist = nullptr;
+            h->det_pairs = nullptr;
+            e = dalloc(h->det_keys, kc);
+            if (e == cudaSuccess) e = dalloc(h->det_keys_alt, kc);
+            if (e == cudaSuccess) e = dalloc(h->det_vals, kc);
+            if (e == cudaSuccess) e = dalloc(h->det_vals_alt, kc);
+            if (e == cudaSuccess) e = dalloc(h->det_hist, rs::hist_words(kc));
+            if (e == cudaSuccess) e = dalloc(h->det_pairs, h->cap_pairs);
+            if (e == cudaSuccess && !h->det_n) e = dalloc(h->det_n, 2);
+            h->det_cap = h->cap_pairs;
+        }
         if (e == cudaSuccess && h->sell) {
             // SELL copy of the contact blocks: twice the assembler's block capacity plus a padded
             // group per slice; a step whose slices need more uses the CSR form
@@ -1270,6 +1624,56 @@ int build_material_pattern(lcs_newton* h, const lcs_scene_desc* d)
             else as[k - KS - KF - KB] = v;
         }
     });
+    if (h->det) {
+        // per material block (CSR position j): its contributions in contribution order -- springs, faces,
+        // stencils, each by element and then by local pair -- the order the gather sums them in
+        const size_t KE = KS + KF + KB;
+        std::vector<uint32_t> jof(KE ? KE : 1);
+        parallel_ranges(KE, [&](size_t kb, size_t ke) {
+            for (size_t k = kb; k < ke; ++k) jof[k] = slot_of(k);
+        });
+        std::vector<uint32_t> bptr(nnz + 1, 0);
+        for (size_t k = 0; k < KE; ++k) bptr[jof[k] + 1]++;
+        for (size_t j = 0; j < nnz; ++j) bptr[j + 1] += bptr[j];
+        std::vector<uint2> bent(KE ? KE : 1);
+        std::vector<uint32_t> cur(bptr.begin(), bptr.end() - 1);
+        const uint32_t bkind = h->d.bending_model == LCS_BENDING_QUADRATIC ? 3u : 2u;
+        for (size_t k = 0; k < KE; ++k) {
+            uint2 en;
+            if (k < KS) en = make_uint2((uint32_t)(k >> 1), 0u << 4 | (uint32_t)(k & 1));
+            else if (k < KS + KF) en = make_uint2((uint32_t)((k - KS) / 6), 1u << 4 | (uint32_t)((k - KS) % 6));
+            else en = make_uint2((uint32_t)((k - KS - KF) / 12), bkind << 4 | (uint32_t)((k - KS - KF) % 12));
+            bent[cur[jof[k]]++] = en;
+        }
+        // per vertex: its springs (end 0 or 1), faces (corner 0..2) and stencils (vertex 0..3), in that order
+        std::vector<uint32_t> vptr(h->V + 1, 0);
+        auto each_vertex_entry = [&](auto&& f) {
+            if (KS)
+                for (uint32_t e = 0; e < h->E; ++e)
+                    for (uint32_t a = 0; a < 2; ++a) f(d->edges[2 * e + a], make_uint2(e, 0u << 4 | a));
+            if (KF)
+                for (uint32_t fc = 0; fc < h->Fs; ++fc)
+                    for (uint32_t a = 0; a < 3; ++a) f(d->stretch_faces[4 * fc + a], make_uint2(fc, 1u << 4 | a));
+            if (KB)
+                for (uint32_t st = 0; st < h->B; ++st)
+                    for (uint32_t a = 0; a < 4; ++a) f(d->bending[4 * st + a], make_uint2(st, bkind << 4 | a));
+        };
+        each_vertex_entry([&](uint32_t v, uint2) { vptr[v + 1]++; });
+        for (uint32_t v = 0; v < h->V; ++v) vptr[v + 1] += vptr[v];
+        std::vector<uint2> vent(vptr[h->V] ? vptr[h->V] : 1);
+        std::vector<uint32_t> vc(vptr.begin(), vptr.end() - 1);
+        each_vertex_entry([&](uint32_t v, uint2 en) { vent[vc[v]++] = en; });
+        h->det_nblk = (uint32_t)nnz;
+        h->det_off_face = KS ? 12 * (size_t)h->E : 0;
+        h->det_off_bend = h->det_off_face + (KF ? 64 * (size_t)h->Fs : 0);
+        const size_t nel = h->det_off_bend + (KB ? 16 * (size_t)h->B : 0);
+        if (upload(h->det_bptr, bptr.data(), bptr.size()) != cudaSuccess ||
+            upload(h->det_bent, bent.data(), bent.size()) != cudaSuccess ||
+            upload(h->det_bbase, base.data(), base.size()) != cudaSuccess ||
+            upload(h->det_vptr, vptr.data(), vptr.size()) != cudaSuccess ||
+            upload(h->det_vent, vent.data(), vent.size()) != cudaSuccess || dalloc(h->det_el, nel ? nel : 1) != cudaSuccess)
+            return lcs_fail(LCS_ERR_CUDA, "lcs_newton: deterministic assembly tables: upload failed");
+    }
     if (upload(h->mat_rp, rp.data(), rp.size()) != cudaSuccess || upload(h->mat_col, col.data(), col.size()) != cudaSuccess ||
         upload(h->spring_slots, ss.data(), ss.size()) != cudaSuccess ||
         upload(h->face_slots, fs.data(), fs.size()) != cudaSuccess ||
@@ -1287,6 +1691,49 @@ inline int grid256(uint64_t n) { return grid_for(n, 256); }
 void mark(lcs_newton* h, int phase)
 {
     if (h->profile) cudaEventRecord(h->ev[phase], h->s);
+}
+
+// LCS_NEWTON_DETERMINISTIC: the contact pairs into canonical order (two stable radix passes over 42 + 44 key
+// bits, then a gather into the scratch list, which becomes the pair list)
+int det_sort_pairs(lcs_newton* h)
+{
+    cudaStream_t s = h->s;
+    const uint32_t cap = h->cap_pairs;
+    const uint32_t* cnt = &h->st->cnt[2];
+    k_pair_keys<<<grid256(cap), 256, 0, s>>>(h->pairs, cnt, cap, 0, nullptr, h->det_keys, h->det_vals, h->det_n);
+    lcs_count_launch();
+    const bool alt = rs::sort_pairs<uint64_t>(h->det_keys, h->det_vals, h->det_keys_alt, h->det_vals_alt, h->det_n, 0,
+                                              cap, 0, 42, h->det_hist, s);
+    const uint32_t* ord = alt ? h->det_vals_alt : h->det_vals;
+    uint64_t* k2 = alt ? h->det_keys : h->det_keys_alt;
+    uint32_t* v2 = alt ? h->det_vals : h->det_vals_alt;
+    uint64_t* k3 = alt ? h->det_keys_alt : h->det_keys;
+    uint32_t* v3 = alt ? h->det_vals_alt : h->det_vals;
+    k_pair_keys<<<grid256(cap), 256, 0, s>>>(h->pairs, cnt, cap, 1, ord, k2, v2, h->det_n);
+    lcs_count_launch();
+    const bool alt2 = rs::sort_pairs<uint64_t>(k2, v2, k3, v3, h->det_n, 0, cap, 0, 44, h->det_hist, s);
+    k_pair_gather<<<grid256(cap), 256, 0, s>>>(h->pairs, h->det_n, alt2 ? v3 : v2, h->det_pairs);
+    lcs_count_launch();
+    std::swap(h->pairs, h->det_pairs);
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
+}
+
+// LCS_NEWTON_DETERMINISTIC: the contact gradient and diagonal blocks, summed per row in canonical pair order
+int det_contact_rows(lcs_newton* h, cudaStream_t s)
+{
+    const uint32_t cap4 = 4 * h->cap_pairs;
+    k_cg_keys<<<grid256(h->cap_pairs), 256, 0, s>>>(h->pairs, h->det_n, h->V, h->det_keys, h->det_vals, h->det_n + 1);
+    lcs_count_launch();
+    int bits = 1;
+    while (bits < 40 && (1ull << bits) <= h->V) ++bits;
+    const bool alt = rs::sort_pairs<uint64_t>(h->det_keys, h->det_vals, h->det_keys_alt, h->det_vals_alt, h->det_n + 1,
+                                              0, cap4, 0, bits, h->det_hist, s);
+    k_cg_rows<<<grid256(cap4), 256, 0, s>>>(alt ? h->det_keys_alt : h->det_keys, alt ? h->det_vals_alt : h->det_vals,
+                                            h->det_n + 1, h->V, h->pairs, h->b, h->diag);
+    lcs_count_launch();
+    LCS_LAUNCH_CHECK();
+    return LCS_OK;
 }
 
 // counts the plain comparator reads back where the reference does (download_*_count)
@@ -1579,18 +2026,49 @@ int newton_iteration(lcs_newton* h)
         lcs_count_launch();
         LCS_CUDA_TRY(cudaMemsetAsync(h->mat_val, 0, sizeof(float) * h->sell_vals, ms));
         const uint32_t cs = h->sell ? 128u : 1u;
-        if (h->E && d.stretch_model == LCS_STRETCH_SPRING) {
+        if (h->det) {  // per-element terms, then per-row and per-block sums in element order
+            if (h->E && d.stretch_model == LCS_STRETCH_SPRING) {
+                k_springs_det<<<grid256(h->E), 256, 0, ms>>>(h->E, h->edges, h->rest_len, h->spring_kper, d.spring_k,
+                                                               h->x, h->det_el);
+                lcs_count_launch();
+            }
+            if (h->Fs && d.stretch_model == LCS_STRETCH_BW98) {
+                k_stretch_bw98_det<<<grid256(h->Fs), 256, 0, ms>>>(h->Fs, h->sfaces, h->dm, h->sarea, h->ml, d.stretch_mu,
+                                                                     d.stretch_lambda, h->x, h->det_el + h->det_off_face);
+                lcs_count_launch();
+            }
+            if (h->B && d.bending_model == LCS_BENDING_DIHEDRAL) {
+                k_bending_dihedral_det<<<grid256(h->B), 256, 0, ms>>>(h->B, h->bend, h->rest_angle, h->hbar, h->bend_kper,
+                                                                        d.bending_k, d.bending_scaling, h->x,
+                                                                        h->det_el + h->det_off_bend);
+                lcs_count_launch();
+            } else if (h->B && d.bending_model == LCS_BENDING_QUADRATIC) {
+                k_bending_det<<<grid256(h->B), 256, 0, ms>>>(h->B, h->bend, h->Q, d.bending_k, h->x, h->rest,
+                                                             h->det_el + h->det_off_bend);
+                lcs_count_launch();
+            }
+            const DetEl D{h->det_el, h->det_off_face, h->det_off_bend, h->Q, d.bending_k};
+            k_det_rows<<<grid256(V), 256, 0, ms>>>(V, h->det_vptr, h->det_vent, D, h->b, h->diag);
+            lcs_count_launch();
+            if (h->det_nblk) {
+                k_det_blocks<<<grid256(h->det_nblk), 256, 0, ms>>>(h->det_nblk, h->det_bptr, h->det_bent, h->det_bbase, D,
+                                                                     cs, h->mat_val);
+                lcs_count_launch();
+            }
+        }
+        if (!h->det && h->E && d.stretch_model == LCS_STRETCH_SPRING) {
             k_springs<<<grid256(h->E), 256, 0, ms>>>(h->E, h->edges, h->rest_len, h->spring_kper, d.spring_k, h->x,
                                                        h->b, h->diag, h->spring_slots, cs, h->mat_val);
             lcs_count_launch();
         }
-        if (h->Fs && d.stretch_model == LCS_STRETCH_BW98) {
+        if (!h->det && h->Fs && d.stretch_model == LCS_STRETCH_BW98) {
             k_stretch_bw98<<<grid256(h->Fs), 256, 0, ms>>>(h->Fs, h->sfaces, h->dm, h->sarea, h->ml, d.stretch_mu,
                                                              d.stretch_lambda, h->x, h->b, h->diag, h->face_slots, cs,
                                                              h->mat_val);
             lcs_count_launch();
         }
-        if (h->B && d.bending_model == LCS_BENDING_DIHEDRAL) {
+        if (h->det) {
+        } else if (h->B && d.bending_model == LCS_BENDING_DIHEDRAL) {
             k_bending_dihedral<<<grid256(h->B), 256, 0, ms>>>(h->B, h->bend, h->rest_angle, h->hbar, h->bend_kper,
                                                                 d.bending_k, d.bending_scaling, h->x, h->b, h->diag,
                                                                 h->bend_slots, cs, h->mat_val);
@@ -1667,6 +2145,7 @@ int newton_iteration(lcs_newton* h)
             if ((rc = host_readback(h))) return rc;  // download_narrowphase_collision_count
             if (grow(h)) { if ((rc = alloc_contact(h))) return rc; continue; }
         }
+        if (h->det && (rc = det_sort_pairs(h))) return rc;
         if (ms != h->s) {
             LCS_CUDA_TRY(cudaEventRecord(h->join_m, ms));
             LCS_CUDA_TRY(cudaStreamWaitEvent(h->s, h->join_m, 0));
@@ -1686,9 +2165,13 @@ int newton_iteration(lcs_newton* h)
                 return rc;
             if ((rc = lcs_contact_offdiag_bsr_abd(h->asmb, h->pairs, &h->st->cnt[2], h->cap_pairs, &av, h->s))) return rc;
         } else {
-            if ((rc = lcs_contact_grad_diag(h->pairs, &h->st->cnt[2], h->cap_pairs, reinterpret_cast<float*>(h->b),
-                                            reinterpret_cast<float*>(h->diag), gs)))
+            if (h->det) {
+                if ((rc = det_contact_rows(h, gs))) return rc;
+            } else if ((rc = lcs_contact_grad_diag(h->pairs, &h->st->cnt[2], h->cap_pairs,
+                                                   reinterpret_cast<float*>(h->b), reinterpret_cast<float*>(h->diag),
+                                                   gs))) {
                 return rc;
+            }
             if ((rc = lcs_contact_offdiag_bsr(h->asmb, h->pairs, &h->st->cnt[2], h->cap_pairs, h->s))) return rc;
         }
         if (dlanes) {
@@ -1920,7 +2403,13 @@ int create_impl(const lcs_scene_desc* d, int flags, lcs_stream stream, bool batc
     h->full_traversal = (flags & LCS_NEWTON_FULL_TRAVERSAL) != 0;
     h->energy_ls = (flags & LCS_NEWTON_ENERGY_LINESEARCH) != 0;
     h->global_matrix = (flags & LCS_NEWTON_PCG_GLOBAL_MATRIX) != 0;
+    h->det = (flags & LCS_NEWTON_DETERMINISTIC) != 0;
     h->batch = batch;
+    if (h->det && (d->n_bodies || h->energy_ls || h->plain || d->n_verts >= (1u << 21))) {
+        delete h;
+        return lcs_fail(LCS_ERR_INVALID, "lcs_newton_create: LCS_NEWTON_DETERMINISTIC covers fused cloth scenes below "
+                                         "2^21 vertices without affine bodies or the energy line search");
+    }
     h->V = d->n_verts;
     h->F = d->n_faces;
     h->E = d->n_edges;
@@ -2297,7 +2786,8 @@ extern "C" int lcs_newton_destroy(lcs_newton* h)
                     h->Q, h->rest_len, h->vert_area, h->face_area, h->edge_area,
                     h->mass, h->dhat, h->offset, h->body, h->pinned, h->group, h->anim, h->rest, h->x, h->v,
                     h->x_step, h->x_iter, h->x_tilde, h->target, h->dx, h->b, h->diag, h->mat_rp, h->mat_col,
-                    h->spring_slots, h->bend_slots, h->mat_val, h->st, h->sell_ptr, h->sell_col, h->prev_ccd};
+                    h->spring_slots, h->bend_slots, h->mat_val, h->st, h->sell_ptr, h->sell_col, h->prev_ccd,
+                    h->det_el, h->det_vptr, h->det_bptr, h->det_bbase, h->det_vent, h->det_bent, h->det_n};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_st) cudaFreeHost(h->h_st);

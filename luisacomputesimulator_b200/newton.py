@@ -104,7 +104,7 @@ class NewtonSolver:
     def __init__(self, scene, plain=False, fp64=False, profile=False, nonlinear_iters=3, pcg_max_iter=100,
                  pcg_rel_tol=1e-4, pcg_abs_rz_tol=1e-10, pcg_check_every=25, damping=2.0, use_floor=False,
                  floor_y=0.0, stream=None, single_reduction=False, full_traversal=False, energy_linesearch=False,
-                 global_matrix=False):
+                 global_matrix=False, deterministic=False):
         self.lib = A.load()
         self.scene = scene
         sc = scene
@@ -117,7 +117,8 @@ class NewtonSolver:
             (A.LCS_NEWTON_PROFILE if profile else 0) | (A.LCS_NEWTON_PCG_SINGLE_REDUCTION if single_reduction else 0) | \
             (A.LCS_NEWTON_FULL_TRAVERSAL if full_traversal else 0) | \
             (A.LCS_NEWTON_ENERGY_LINESEARCH if energy_linesearch else 0) | \
-            (A.LCS_NEWTON_PCG_GLOBAL_MATRIX if global_matrix else 0)
+            (A.LCS_NEWTON_PCG_GLOBAL_MATRIX if global_matrix else 0) | \
+            (A.LCS_NEWTON_DETERMINISTIC if deterministic else 0)
         s = C.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
         h = C.c_void_p()
         A.check(self.lib.lcs_newton_create(C.byref(d), flags, s, C.byref(h)), "lcs_newton_create")
@@ -234,17 +235,23 @@ class NewtonSolver:
 class NewtonBatch:
     """Many independent scenes stepped together (lcs_newton_create_batch): one set of launches per
     Newton phase for all scenes, per-scene trees, step bounds and PCG (one thread-block cluster of
-    `cluster` CTAs per scene).  A scene's trajectory does not depend on the other scenes."""
+    `cluster` CTAs per scene).  A scene's trajectory does not depend on the other scenes: with
+    deterministic=True (the default when no scene has affine bodies) every sum runs in a fixed order, so a
+    scene's result is bit-identical alone and in any mix (LCS_NEWTON_DETERMINISTIC)."""
 
     def __init__(self, scenes, fp64=False, profile=False, cluster=0, nonlinear_iters=3, pcg_max_iter=100,
-                 pcg_rel_tol=1e-4, pcg_abs_rz_tol=1e-10, damping=2.0, stream=None):
+                 pcg_rel_tol=1e-4, pcg_abs_rz_tol=1e-10, damping=2.0, stream=None, deterministic=None):
         self.lib = A.load()
         self.scenes = list(scenes)
         keep = []
         descs = (A.SceneDesc * len(self.scenes))()
         for k, sc in enumerate(self.scenes):
             descs[k] = scene_desc(sc, keep, nonlinear_iters, pcg_max_iter, pcg_rel_tol, pcg_abs_rz_tol, 1, damping)
-        flags = (A.LCS_NEWTON_FP64 if fp64 else 0) | (A.LCS_NEWTON_PROFILE if profile else 0)
+        if deterministic is None:  # sums in a fixed order wherever the deterministic mode covers the scenes
+            deterministic = all(sc.num_bodies == 0 for sc in self.scenes)
+        self.deterministic = bool(deterministic)
+        flags = (A.LCS_NEWTON_FP64 if fp64 else 0) | (A.LCS_NEWTON_PROFILE if profile else 0) | \
+            (A.LCS_NEWTON_DETERMINISTIC if deterministic else 0)
         s = C.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
         h = C.c_void_p()
         A.check(self.lib.lcs_newton_create_batch(descs, len(self.scenes), flags, s, int(cluster), C.byref(h)),

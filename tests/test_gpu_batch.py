@@ -238,11 +238,38 @@ def _drapes():
     return [S.random_cloth_scene(n, seed) for n, seed in ((400, 1), (900, 2), (1600, 3))]
 
 
-def test_batched_newton_alone_equals_in_mix_and_stays_intersection_free():
+def test_deterministic_batch_is_bit_identical_alone_and_in_mix():
+    """LCS_NEWTON_DETERMINISTIC (the batch default): the cloth terms summed per row and per block in element
+    order, the contact pairs sorted into a canonical order before their sums -- a scene's 8 contact steps are
+    bit-identical in a mix of three, alone, and alone once more."""
     scs = _drapes()
-    mix = NewtonBatch(scs)
-    alone = [NewtonBatch([sc]) for sc in scs]
-    again = [NewtonBatch([sc]) for sc in scs]  # the same scene alone once more: the run-to-run spread
+    mix = NewtonBatch(scs, deterministic=True)
+    alone = [NewtonBatch([sc], deterministic=True) for sc in scs]
+    again = [NewtonBatch([sc], deterministic=True) for sc in scs]
+    assert mix.deterministic
+    pairs = 0
+    for _ in range(8):
+        st = mix.step()
+        assert st.status == 0
+        pairs = max(pairs, st.contact_pairs)
+        for a in alone + again:
+            assert a.step().status == 0
+    assert pairs > 0, "the drapes touch their colliders"
+    for k, sc in enumerate(scs):
+        xm, xa, xb = mix.positions(k), alone[k].positions(0), again[k].positions(0)
+        np.testing.assert_array_equal(xm, xa)
+        np.testing.assert_array_equal(xb, xa)
+        np.testing.assert_array_equal(mix.velocities(k), alone[k].velocities(0))
+        assert np.abs(xa[:, :3] - sc.x[:, :3]).max() > 0
+        assert O.min_distance(sc, xm) > 0.0
+
+
+def test_batched_newton_alone_equals_in_mix_and_stays_intersection_free():
+    """The same with float atomics (deterministic=False): within the run-to-run spread of the atomics."""
+    scs = _drapes()
+    mix = NewtonBatch(scs, deterministic=False)
+    alone = [NewtonBatch([sc], deterministic=False) for sc in scs]
+    again = [NewtonBatch([sc], deterministic=False) for sc in scs]  # the same scene alone once more: the run-to-run spread
     for _ in range(8):
         st = mix.step()
         assert st.status == 0

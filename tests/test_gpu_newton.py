@@ -206,3 +206,37 @@ def test_floor_ccd_bounds_the_step_like_the_reference():
         assert got <= want and abs(got - want) <= 1e-6 * want, (plain, got, want)
         x = gpu.positions()
         assert (x[:, 1] - sc.offset > 0.0).all()  # nothing below the floor
+
+
+def test_deterministic_single_scene_repeats_bit_for_bit():
+    """LCS_NEWTON_DETERMINISTIC on one scene (slice-resident PCG): two runs of 30 contact steps of the cloth
+    falling on the sphere give the same bits.  The atomic form adds the same terms in another order: after the
+    first step the two agree to 1e-3 of the step's motion (measured 1.4e-4 after the step's capped PCG solves;
+    later contact steps amplify such rounding, as two atomic runs show)."""
+    sc = S.cloth_on_sphere(n=32)
+    runs = [NewtonSolver(sc, single_reduction=True, deterministic=True) for _ in range(2)]
+    atomic = NewtonSolver(sc, single_reduction=True)
+    assert atomic.step().status == 0
+    pairs = 0
+    for k in range(30):
+        for g in runs:
+            st = g.step()
+            assert st.status == 0
+            pairs = max(pairs, st.contact_pairs)
+        if k == 0:
+            xd, xc = runs[0].positions(), atomic.positions()
+            scale = np.abs(xd[:, :3] - sc.x[:, :3]).max()
+            assert scale > 0
+            assert np.abs(xc[:, :3] - xd[:, :3]).max() <= 1e-3 * scale
+    assert pairs > 0
+    xa, xb = runs[0].positions(), runs[1].positions()
+    np.testing.assert_array_equal(xa, xb)
+    np.testing.assert_array_equal(runs[0].velocities(), runs[1].velocities())
+    assert O.min_distance(sc, xa) > 0.0
+
+
+def test_deterministic_mode_refuses_affine_bodies():
+    from luisacomputesimulator_b200 import _capi as A
+    sc = S.cloth_box_scene(400, 3)
+    with pytest.raises(A.LcsError):
+        NewtonSolver(sc, deterministic=True)
