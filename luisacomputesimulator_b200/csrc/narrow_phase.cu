@@ -421,6 +421,67 @@ __global__ void k_segments(const uint64_t* __restrict__ keys, const uint32_t* __
     }
 }
 
+// The (row, column, triplet) order of the contact triplets without a global radix sort (pairs without affine
+// bodies): the 12 directed vertex pairs of every contact pair are bucketed by row (a count, a scan and a
+// scatter with per-row cursors), and each entry finds its place in its row's bucket by counting the entries
+// that precede it in (column, triplet index) order -- the order the stable radix sort gives.  Rows hold at
+// most a few hundred entries.  k_heads, k_segments and k_row_ptr then run on the result as after the sort.
+__global__ void k_row_count(const lcs_pair* __restrict__ pairs, const uint32_t* d_count, uint32_t cap,
+                            uint32_t* __restrict__ rcnt)
+{
+    const uint32_t n = pair_count(d_count, cap);
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const PairView P = load_pair(pairs, k);
+        if (!P.type) continue;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) atomicAdd(&rcnt[P.v[i]], 3u);
+    }
+}
+
+__global__ void k_row_scatter(const lcs_pair* __restrict__ pairs, const uint32_t* d_count, uint32_t cap, int bits,
+                              const uint32_t* __restrict__ rstart, uint32_t* __restrict__ rcur,
+                              uint64_t* __restrict__ tkeys, uint32_t* __restrict__ tvals)
+{
+    const uint32_t n = pair_count(d_count, cap);
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const PairView P = load_pair(pairs, k);
+        if (!P.type) continue;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t base = rstart[P.v[i]] + atomicAdd(&rcur[P.v[i]], 3u);
+            uint32_t t = 0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (i != j) {
+                    tkeys[base + t] = ((uint64_t)P.v[i] << bits) | (uint64_t)P.v[j];
+                    tvals[base + t] = 16u * k + 4u * i + j;
+                    ++t;
+                }
+        }
+    }
+}
+
+__global__ void k_row_rank(uint32_t n_rows, const uint32_t* __restrict__ rstart, int bits,
+                           const uint64_t* __restrict__ tkeys, const uint32_t* __restrict__ tvals,
+                           uint64_t* __restrict__ keys, uint32_t* __restrict__ vals, uint32_t* d_n)
+{
+    const uint32_t n = rstart[n_rows];
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d_n = n;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const uint64_t k = tkeys[e];
+        const uint32_t v = tvals[e];
+        const uint32_t r = (uint32_t)(k >> bits);
+        const uint32_t lo = rstart[r], hi = rstart[r + 1];
+        uint32_t rank = 0;
+        for (uint32_t q = lo; q < hi; ++q) {
+            const uint64_t kq = tkeys[q];
+            rank += (kq < k || (kq == k && tvals[q] < v)) ? 1u : 0u;
+        }
+        keys[lo + rank] = k;
+        vals[lo + rank] = v;
+    }
+}
+
 // row_ptr[r] = first block whose row >= r (binary search over the sorted block rows)
 __global__ void k_row_ptr(const uint32_t* __restrict__ brow, const uint32_t* d_nnzb, uint32_t n_rows,
                           uint32_t* __restrict__ row_ptr)
@@ -448,6 +509,9 @@ struct lcs_assembler {
     uint32_t *d_ntrip = nullptr, *d_nnzb = nullptr;
     uint32_t *row_ptr = nullptr, *col = nullptr, *brow = nullptr;
     float* val = nullptr;
+    // row bucketing (pairs without affine bodies): per-row counts / starts / cursors, n_rows + 1 each
+    uint32_t *rcnt = nullptr, *rstart = nullptr, *rcur = nullptr, *d_rows1 = nullptr;
+    uint32_t* rscan_tmp = nullptr;
 };
 
 namespace {
@@ -480,6 +544,16 @@ int assembler_create(uint32_t n_rows, uint32_t pair_capacity, bool abd, lcs_asse
     A((void**)&a->col, 4 * T);
     A((void**)&a->brow, 4 * T);
     A((void**)&a->val, 36 * T);
+    const size_t R1 = (size_t)n_rows + 1;
+    A((void**)&a->rcnt, 4 * R1);
+    A((void**)&a->rstart, 4 * R1);
+    A((void**)&a->rcur, 4 * R1);
+    A((void**)&a->d_rows1, 4);
+    A((void**)&a->rscan_tmp, 4 * scan::tmp_words((uint32_t)R1));
+    if (e == cudaSuccess) {
+        const uint32_t r1 = (uint32_t)R1;
+        e = cudaMemcpy(a->d_rows1, &r1, 4, cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) e = cudaMemset(a->row_ptr, 0, 4 * ((size_t)n_rows + 1));
     if (e == cudaSuccess) e = cudaMemset(a->d_nnzb, 0, 4);
     if (e != cudaSuccess) {
@@ -505,7 +579,8 @@ extern "C" int lcs_assembler_destroy(lcs_assembler* a)
 {
     if (!a) return LCS_OK;
     void* ptrs[] = {a->keys, a->keys_alt, a->vals, a->vals_alt, a->hist, a->flags, a->excl, a->scan_tmp,
-                    a->d_ntrip, a->d_nnzb, a->row_ptr, a->col, a->brow, a->val};
+                    a->d_ntrip, a->d_nnzb, a->row_ptr, a->col, a->brow, a->val, a->rcnt, a->rstart, a->rcur,
+                    a->d_rows1, a->rscan_tmp};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete a;
@@ -529,17 +604,36 @@ int offdiag_bsr(lcs_assembler* a, const lcs_pair* pairs, const uint32_t* d_count
     const AbdView av = abd_view(abdv);
     cudaStream_t s = (cudaStream_t)stream;
     const uint32_t tcap = (abd ? 56u : 12u) * capacity;
-    if (abd)
+    const uint64_t* keys;
+    const uint32_t* vals;
+    if (!abd) {  // row bucketing: count, scan, scatter, rank within the row
+        const uint32_t R1 = a->n_rows + 1;
+        LCS_CUDA_TRY(cudaMemsetAsync(a->rcnt, 0, 4 * (size_t)R1, s));
+        LCS_CUDA_TRY(cudaMemsetAsync(a->rcur, 0, 4 * (size_t)R1, s));
+        if (capacity) {
+            k_row_count<<<grid_for(capacity, 256), 256, 0, s>>>(pairs, d_count, capacity, a->rcnt);
+            lcs_count_launch();
+        }
+        scan::exclusive_u32(a->rcnt, a->rstart, a->d_rows1, R1, a->rscan_tmp, s);
+        if (capacity) {
+            k_row_scatter<<<grid_for(capacity, 256), 256, 0, s>>>(pairs, d_count, capacity, a->bits, a->rstart, a->rcur,
+                                                                   a->keys_alt, a->vals_alt);
+            lcs_count_launch();
+        }
+        k_row_rank<<<grid_for(tcap, 256), 256, 0, s>>>(a->n_rows, a->rstart, a->bits, a->keys_alt, a->vals_alt,
+                                                       a->keys, a->vals, a->d_ntrip);
+        lcs_count_launch();
+        keys = a->keys;
+        vals = a->vals;
+    } else {
         k_trip_keys<true><<<grid_for(capacity, 256), 256, 0, s>>>(pairs, d_count, capacity, a->bits, a->n_rows,
                                                                   a->keys, a->vals, a->d_ntrip, av);
-    else
-        k_trip_keys<false><<<grid_for(capacity, 256), 256, 0, s>>>(pairs, d_count, capacity, a->bits, a->n_rows,
-                                                                   a->keys, a->vals, a->d_ntrip, av);
-    lcs_count_launch();
-    const bool alt = rs::sort_pairs<uint64_t>(a->keys, a->vals, a->keys_alt, a->vals_alt, a->d_ntrip, 0, tcap, 0,
-                                              2 * a->bits, a->hist, s);
-    const uint64_t* keys = alt ? a->keys_alt : a->keys;
-    const uint32_t* vals = alt ? a->vals_alt : a->vals;
+        lcs_count_launch();
+        const bool alt = rs::sort_pairs<uint64_t>(a->keys, a->vals, a->keys_alt, a->vals_alt, a->d_ntrip, 0, tcap, 0,
+                                                  2 * a->bits, a->hist, s);
+        keys = alt ? a->keys_alt : a->keys;
+        vals = alt ? a->vals_alt : a->vals;
+    }
     const int g = grid_for(tcap, 256);
     k_heads<<<g, 256, 0, s>>>(keys, a->d_ntrip, tcap, a->bits, a->n_rows, a->flags);
     lcs_count_launch();
