@@ -1137,7 +1137,52 @@ struct ResArgs {
     uint32_t n_slices;
     uint32_t max_slices; // slices of the largest block (shared-memory stride)
     int gres;            // resident groups per slice
+    int gtm;             // further groups per slice held in tensor memory (0: none)
 };
+
+// Tensor memory (TMEM, 256 KB per SM) as on-chip storage for the material groups beyond the shared-memory ones:
+// warp w of the block reaches TMEM lanes 32 (w mod 4) .. 32 (w mod 4) + 31, one per thread, and keeps its slice's
+// groups there, 40 columns each (the group's column word, then its nine value words), from column 80 (w / 4).
+// With at most 20 warps that is columns 0..399 of the 512 the block allocates.
+constexpr int kResTmemGroups = 2;
+constexpr uint32_t kResTmemCols = 512;
+__device__ __forceinline__ void tmem_alloc(uint32_t* smem_dst, uint32_t ncols)
+{
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(a), "r"(ncols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, uint4 v)
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(v.x), "r"(v.y),
+                 "r"(v.z), "r"(v.w)
+                 : "memory");
+}
+__device__ __forceinline__ uint4 tmem_ld4(uint32_t taddr)
+{
+    uint4 v;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "r"(taddr)
+                 : "memory");
+    return v;
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ float4 as_f4(uint4 v)
+{
+    return make_float4(__uint_as_float(v.x), __uint_as_float(v.y), __uint_as_float(v.z), __uint_as_float(v.w));
+}
+__device__ __forceinline__ uint4 as_u4(float4 v)
+{
+    return make_uint4(__float_as_uint(v.x), __float_as_uint(v.y), __float_as_uint(v.z), __float_as_uint(v.w));
+}
 
 // Slices to blocks by cost, before each solve: a slice costs its material groups, its contact blocks (CSR)
 // and kResSliceBase for the diagonal and the vectors; block c takes the slices whose cost prefix reaches
@@ -1381,10 +1426,12 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
     extern __shared__ __align__(16) unsigned char res_smem[];
     __shared__ int s_fail;
     __shared__ unsigned s_dep[kResDepWords];
+    __shared__ uint32_t s_taddr;
     const uint32_t P = gridDim.x, c = blockIdx.x;
     const uint32_t s_lo = __ldcg(&ra.part[c]), s_hi = __ldcg(&ra.part[c + 1]);
     const uint32_t nsl = s_hi - s_lo, row0 = 32u * s_lo;
     const int G = ra.gres;
+    const int GT = ra.gtm;
     float* cprod = reinterpret_cast<float*>(res_smem);                     // [3][kResContactChunk]
     double(*spart)[4] = reinterpret_cast<double(*)[4]>(cprod + 3 * kResContactChunk);  // P
     float4* sval = reinterpret_cast<float4*>(spart + P);                   // [max_slices * G][9][32]
@@ -1412,7 +1459,28 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
             scol[((size_t)ls * G + j) * 32 + lane] = __ldg(&C4[(size_t)(g0 + j) * 32 + lane]);
         }
     }
-    __syncthreads();  // s_dep cleared
+    if (GT > 0) {
+        if (ls == 0) tmem_alloc(&s_taddr, kResTmemCols);
+        tmem_fence_before();
+    }
+    __syncthreads();  // s_dep cleared, tensor memory allocated
+    // this warp's slice: the next GT groups to tensor memory (warp-uniform: every lane of the warp takes part)
+    uint32_t tbase = 0;
+    if (GT > 0) {
+        tmem_fence_after();
+        tbase = s_taddr + ((32u * (ls & 3u)) << 16) + 80u * (ls >> 2);
+        if (ls < nsl && g1 - g0 > (uint32_t)G) {
+            const uint32_t nt = min((uint32_t)GT, g1 - g0 - (uint32_t)G);
+            for (uint32_t jt = 0; jt < nt; ++jt) {
+                const uint32_t g = g0 + (uint32_t)G + jt;
+                const uint32_t cb = tbase + 40u * jt;
+                tmem_st4(cb, __ldg(&C4[(size_t)g * 32 + lane]));
+#pragma unroll
+                for (int k = 0; k < 9; ++k) tmem_st4(cb + 4u + 4u * k, as_u4(ld_stream4(V4 + ((size_t)g * 9 + k) * 32 + lane)));
+            }
+            tmem_wait_st();
+        }
+    }
     // the blocks this block's rows read u from: a window of 32 blocks around c by warp vote, others
     // (distant contacts) one shared-memory OR each
     {
@@ -1504,7 +1572,17 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
         for (uint32_t g = g0; g < g1; ++g) {
             const uint32_t j = g - g0;
             const bool res = j < (uint32_t)G;
-            const uint4 jc = res ? scol[((size_t)ls * G + j) * 32 + lane] : __ldg(&C4[(size_t)g * 32 + lane]);
+            const bool tm = !res && j < (uint32_t)(G + GT);  // the same in every lane of the warp
+            const uint32_t cb = tbase + 40u * (j - (uint32_t)G);
+            uint4 jc;
+            if (res) {
+                jc = scol[((size_t)ls * G + j) * 32 + lane];
+            } else if (tm) {
+                jc = tmem_ld4(cb);
+                tmem_wait_ld();
+            } else {
+                jc = __ldg(&C4[(size_t)g * 32 + lane]);
+            }
             const float4 pv[4] = {ld_u(jc.x), ld_u(jc.y), ld_u(jc.z), ld_u(jc.w)};
             const float4* vg = res ? sval + ((size_t)ls * G + j) * 9 * 32 + lane : V4 + (size_t)g * 9 * 32 + lane;
 #pragma unroll
@@ -1512,6 +1590,11 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
                 float4 ma, mb, mc;
                 if (res) {
                     ma = vg[32 * rr]; mb = vg[32 * (rr + 3)]; mc = vg[32 * (rr + 6)];
+                } else if (tm) {
+                    const uint4 ua = tmem_ld4(cb + 4u + 4u * rr), ub = tmem_ld4(cb + 4u + 4u * (rr + 3)),
+                                uc = tmem_ld4(cb + 4u + 4u * (rr + 6));
+                    tmem_wait_ld();
+                    ma = as_f4(ua); mb = as_f4(ub); mc = as_f4(uc);
                 } else {
                     ma = ld_stream4(vg + 32 * rr); mb = ld_stream4(vg + 32 * (rr + 3)); mc = ld_stream4(vg + 32 * (rr + 6));
                 }
@@ -1549,12 +1632,14 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
     LCS_MINV(r0, r1, r2, u0, u1, u2)
     unsigned tag = 1u;
     if (own) __stcg(&a.pg[i], make_float4(u0, u1, u2, 0.0f));
-    if (!res_publish_wait(ra.flags, tag, s_dep, a.stats, &s_fail)) return;
-    matvec(u0, u1, u2, w0, w1, w2);  // every warp (block barrier inside)
+    // a wait that ran out ends the solve (ok false in every thread of the block: the fail flag is shared);
+    // the tensor memory is released on every path
+    bool ok = res_publish_wait(ra.flags, tag, s_dep, a.stats, &s_fail);
+    if (ok) matvec(u0, u1, u2, w0, w1, w2);  // every warp (block barrier inside)
     float x0 = 0.f, x1 = 0.f, x2 = 0.f, p0 = 0.f, p1 = 0.f, p2 = 0.f, sd0 = 0.f, sd1 = 0.f, sd2 = 0.f;
     float gamma_old = 0.0f, alpha_old = 0.0f, norm_r0 = 0.0f, norm_r = 0.0f, gamma = 0.0f;
     int iter = 0, status = 0;
-    for (iter = 0; iter < a.max_iter; ++iter) {
+    for (iter = 0; ok && iter < a.max_iter; ++iter) {
         double dg, dd, dr;
         if (a.fp64) {
             dg = (double)r0 * u0 + (double)r1 * u1 + (double)r2 * u2;
@@ -1568,7 +1653,10 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
         if (!own) dg = dd = dr = 0.0;
         unsigned long long* part = reinterpret_cast<unsigned long long*>(a.part) + 4 * (size_t)P * (iter & 1);
         double sg, sdd, sr;
-        if (!res_allgather3<BT>(dg, dd, dr, part, (unsigned)(iter % 15), spart, a.stats, &s_fail, sg, sdd, sr)) return;
+        if (!res_allgather3<BT>(dg, dd, dr, part, (unsigned)(iter % 15), spart, a.stats, &s_fail, sg, sdd, sr)) {
+            ok = false;
+            break;
+        }
         gamma = (float)sg;
         const float delta = (float)sdd;
         norm_r = sqrtf((float)sr);
@@ -1597,18 +1685,28 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
         LCS_MINV(r0, r1, r2, u0, u1, u2)
         ++tag;
         if (own) __stcg(&a.pg[i], make_float4(u0, u1, u2, 0.0f));
-        if (!res_publish_wait(ra.flags, tag, s_dep, a.stats, &s_fail)) return;
+        if (!res_publish_wait(ra.flags, tag, s_dep, a.stats, &s_fail)) {
+            ok = false;
+            break;
+        }
         matvec(u0, u1, u2, w0, w1, w2);
         gamma_old = gamma;
         alpha_old = alpha;
     }
 #undef LCS_MINV
-    if (own) a.x[i] = make_float4(x0, x1, x2, 0.0f);
-    if (c == 0 && t == 0) {
-        a.stats->iterations = iter;
-        a.stats->rel_residual = norm_r0 > 0.0f ? norm_r / norm_r0 : 0.0f;
-        a.stats->dot_rz = gamma;
-        if (a.stats->status == LCS_OK) a.stats->status = status;
+    if (ok) {
+        if (own) a.x[i] = make_float4(x0, x1, x2, 0.0f);
+        if (c == 0 && t == 0) {
+            a.stats->iterations = iter;
+            a.stats->rel_residual = norm_r0 > 0.0f ? norm_r / norm_r0 : 0.0f;
+            a.stats->dot_rz = gamma;
+            if (a.stats->status == LCS_OK) a.stats->status = status;
+        }
+    }
+    if (GT > 0) {  // every warp's tensor-memory reads are complete (each waited for them)
+        tmem_fence_before();
+        __syncthreads();
+        if (ls == 0) tmem_dealloc(s_taddr, kResTmemCols);
     }
 }
 
@@ -2270,7 +2368,8 @@ static int rows_solve(lcs_pcg* P, const float4* diag, int sell, const uint32_t* 
         k_res_partition<<<1, 1024, 0, s>>>(P->res_slices, P->res_blocks, P->res_max_slices, m_ptr, a.B.rp, P->n,
                                            P->res_part, P->res_owner, (uint32_t)P->res_gres);
         lcs_count_launch();
-        ResArgs ra{a, P->res_part, P->res_owner, P->flags, P->res_slices, P->res_max_slices, P->res_gres};
+        ResArgs ra{a, P->res_part, P->res_owner, P->flags, P->res_slices, P->res_max_slices, P->res_gres,
+                   kResTmemGroups};
         void* rargs[] = {&ra};
         LCS_CUDA_TRY(cudaMemsetAsync(P->flags, 0, sizeof(unsigned) * kResFlagStride * P->res_blocks, s));
         LCS_CUDA_TRY(cudaMemsetAsync(P->part, 0xFF, sizeof(double) * 8 * P->res_blocks, s));  // empty slots
