@@ -1142,8 +1142,9 @@ struct ResArgs {
 
 // Tensor memory (TMEM, 256 KB per SM) as on-chip storage for the material groups beyond the shared-memory ones:
 // warp w of the block reaches TMEM lanes 32 (w mod 4) .. 32 (w mod 4) + 31, one per thread, and keeps its slice's
-// groups there, 40 columns each (the group's column word, then its nine value words), from column 80 (w / 4).
-// With at most 20 warps that is columns 0..399 of the 512 the block allocates.
+// groups there, 40 columns each (the group's column word, then its nine value words), from column 80 (w / 4),
+// and the lanes' diagonal blocks (three float4 columns, 12 words) from column 400 + 12 (w / 4).  With at most
+// 20 warps that is columns 0..459 of the 512 the block allocates.
 constexpr int kResTmemGroups = 2;
 constexpr uint32_t kResTmemCols = 512;
 __device__ __forceinline__ void tmem_alloc(uint32_t* smem_dst, uint32_t ncols)
@@ -1478,8 +1479,13 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
 #pragma unroll
                 for (int k = 0; k < 9; ++k) tmem_st4(cb + 4u + 4u * k, as_u4(ld_stream4(V4 + ((size_t)g * 9 + k) * 32 + lane)));
             }
-            tmem_wait_st();
         }
+        if (ls < nsl) {  // the diagonal blocks of the warp's rows
+            const uint32_t db = s_taddr + ((32u * (ls & 3u)) << 16) + 400u + 12u * (ls >> 2);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) tmem_st4(db + 4u * k, as_u4(__ldg(&a.diag[3 * row + k])));
+        }
+        tmem_wait_st();
     }
     // the blocks this block's rows read u from: a window of 32 blocks around c by warp vote, others
     // (distant contacts) one shared-memory OR each
@@ -1564,7 +1570,15 @@ __global__ void __launch_bounds__(BT, 1) k_pcg_res(ResArgs ra)
     auto matvec = [&](float v0, float v1, float v2, float& q0, float& q1, float& q2) {
         const uint32_t first = min(ce1 - ce0, (uint32_t)kResContactChunk);
         contact_chunk(ce0, first);
-        const float4 c0 = __ldg(&a.diag[3 * row]), c1 = __ldg(&a.diag[3 * row + 1]), c2 = __ldg(&a.diag[3 * row + 2]);
+        float4 c0, c1, c2;
+        if (GT > 0 && ls < nsl) {  // the same in every lane of the warp
+            const uint32_t db = tbase - 80u * (ls >> 2) + 400u + 12u * (ls >> 2);
+            const uint4 d0 = tmem_ld4(db), d1 = tmem_ld4(db + 4u), d2 = tmem_ld4(db + 8u);
+            tmem_wait_ld();
+            c0 = as_f4(d0); c1 = as_f4(d1); c2 = as_f4(d2);
+        } else {
+            c0 = __ldg(&a.diag[3 * row]); c1 = __ldg(&a.diag[3 * row + 1]); c2 = __ldg(&a.diag[3 * row + 2]);
+        }
         q0 = __fmaf_rn(c2.x, v2, __fmaf_rn(c1.x, v1, c0.x * v0));
         q1 = __fmaf_rn(c2.y, v2, __fmaf_rn(c1.y, v1, c0.y * v0));
         q2 = __fmaf_rn(c2.z, v2, __fmaf_rn(c1.z, v1, c0.z * v0));
