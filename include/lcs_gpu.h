@@ -111,7 +111,8 @@ LCS_API int lcs_bvh_construct(lcs_bvh* h, lcs_stream stream);
 LCS_API int lcs_bvh_update_leaves(lcs_bvh* h, const float* thickness, const float* x0, const float* x1,
                           const uint32_t* elems, lcs_stream stream);
 
-/* LBVH::refit (lbvh.cpp:1038-1045): bottom-up union of the inner boxes. */
+/* LBVH::refit (lbvh.cpp:1038-1045): the inner boxes as unions of their children's, bit for bit the
+ * reference's bottom-up walk (computed from each inner node's sorted leaf range, without a serial climb). */
 LCS_API int lcs_bvh_refit(lcs_bvh* h, lcs_stream stream);
 
 /* update_*_tree_leave_aabb + refit in one launch (no reference counterpart as one call). */

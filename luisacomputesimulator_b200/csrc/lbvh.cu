@@ -41,7 +41,11 @@ struct lcs_bvh {
     float4* wide = nullptr;          // 4 * max(ni, 1)
     float4* wide4 = nullptr;         // 8 * max(ni, 1): 4-child records of the even-depth inner nodes
     uint8_t* even = nullptr;         // max(ni, 1): inner node at even depth (root: depth 0)
-    uint32_t* counters = nullptr;    // max(ni, 1), refit arrival counters (self-resetting)
+    uint2* range = nullptr;          // max(ni, 1): sorted leaf positions [first, last] under each inner node
+    uint32_t* spans = nullptr;       // max(ni, 1): inner nodes whose leaves lie in more than one refit chunk
+    uint32_t* span_count = nullptr;  // 1
+    float4* seg_box = nullptr;       // 2 per 32 sorted leaves (whole refit chunks): {min | 0}{max | 0}
+    float4* chunk_box = nullptr;     // 2 per refit chunk: its union
     uint32_t* healthy = nullptr;     // 1
     uint32_t* maxdepth = nullptr;    // 1: depth of the deepest inner node (root: 0), capped at 256
 };
@@ -140,11 +144,19 @@ __global__ void k_apply_sorted(const uint32_t* __restrict__ m30s, const uint32_t
     }
 }
 
+// sorted leaves per block of the chunked refit (k_refit_chunks); a multiple of 32
+constexpr uint32_t kRefitChunk = 512;
+constexpr uint32_t kRefitSegs = kRefitChunk / 32;  // 32-leaf segments per chunk
+constexpr int kRefitLevels = 4;                    // sparse-table levels over a chunk's segments (2^4 = 16)
+static_assert((1u << kRefitLevels) == kRefitSegs, "one sparse-table level per doubling of the segment count");
+
 // fn_build_inner_nodes with determineRange / findSplit, lbvh.cpp:204-291, 541-596; also the
-// traversal records' child codes and the child -> parent slot map
+// traversal records' child codes, the child -> parent slot map, each inner node's leaf range and the list
+// of inner nodes whose range crosses a refit chunk boundary (any order: each is refitted on its own)
 __global__ void k_build_inner(const uint64_t* __restrict__ ms, const uint32_t* __restrict__ sgo, uint32_t n,
                               uint32_t* __restrict__ parent, uint2* __restrict__ children,
-                              uint32_t* __restrict__ slot, float4* __restrict__ wide, uint32_t* __restrict__ maxdepth)
+                              uint32_t* __restrict__ slot, float4* __restrict__ wide, uint32_t* __restrict__ maxdepth,
+                              uint2* __restrict__ range, uint32_t* __restrict__ spans, uint32_t* span_count)
 {
     const int ni = (int)n - 1;
     if (blockIdx.x == 0 && threadIdx.x == 0) *maxdepth = 0u;  // raised by k_depth_parity, launched after this
@@ -165,6 +177,8 @@ __global__ void k_build_inner(const uint64_t* __restrict__ ms, const uint32_t* _
             j = nid + l * d;
         }
         int a = i < j ? i : j, b = i < j ? j : i;
+        range[nid] = make_uint2((uint32_t)a, (uint32_t)b);
+        if ((uint32_t)a / kRefitChunk != (uint32_t)b / kRefitChunk) spans[atomicAdd(span_count, 1u)] = (uint32_t)nid;
         int split;
         {
             const uint64_t ma = ms[a], mb = ms[b];
@@ -203,8 +217,9 @@ __global__ void k_build_inner(const uint64_t* __restrict__ ms, const uint32_t* _
 
 // 4-wide traversal records.  The binary tree stays the reference's (topology, refit and export are
 // bit-exact against it); during each refit every inner node b at even depth gets a record of its four
-// grandchild slots (a leaf child keeps its own slot), written by the thread that completes b in the
-// bottom-up walk: {min.xyz | code}{max.xyz | last} x 4, 128 B, empty slots as inverted boxes that no strict
+// grandchild slots (a leaf child keeps its own slot), written once its children's slots are final (by the
+// chunk kernel of the refit for nodes inside one chunk, else by k_refit_span_records):
+// {min.xyz | code}{max.xyz | last} x 4, 128 B, empty slots as inverted boxes that no strict
 // overlap test passes.  A traversal then takes one dependent
 // 128-B fetch where the binary walk took two 64-B ones.  k_depth_parity marks the even-depth inner nodes
 // after each build (a climb to the root per node, at most 256 levels).
@@ -288,61 +303,274 @@ __global__ void k_check(const uint2* __restrict__ children, const uint32_t* __re
 
 __global__ void k_set_healthy(uint32_t* healthy) { *healthy = 1u; }
 
-__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v)
-{
-    unsigned old;
-    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-    return old;
-}
-
-// fn_update_*_tree_leave_aabb_v2 (lbvh.cpp:617-683) and, when `climb`, fn_refit_tree_aabb
-// (lbvh.cpp:702-754): the second child to arrive at a parent unions the two slot boxes and
-// carries on upwards; arrival counters reset themselves, so no init pass is needed.
+// fn_update_*_tree_leave_aabb_v2 (lbvh.cpp:617-683) alone: the leaf slots (a one-leaf tree also gets its
+// 4-wide record, both of whose slots are the leaf)
 __device__ __forceinline__ void collapse_node(const float4* wide, uint32_t b, bool leaf_only, float4* wide4);
 
-__global__ void k_leaves_refit(int kind, uint32_t n, const uint32_t* __restrict__ sgo,
-                               const uint32_t* __restrict__ slot, const uint32_t* __restrict__ parent,
-                               const float* __restrict__ thickness, const float4* __restrict__ x0,
-                               const float4* __restrict__ x1, const uint32_t* __restrict__ elems, float4* wide,
-                               uint32_t* counters, uint32_t* healthy, int write_leaf, int climb,
-                               const uint8_t* __restrict__ even, float4* __restrict__ wide4)
+__global__ void k_leaves(int kind, uint32_t n, const uint32_t* __restrict__ sgo, const uint32_t* __restrict__ slot,
+                         const float* __restrict__ thickness, const float4* __restrict__ x0,
+                         const float4* __restrict__ x1, const uint32_t* __restrict__ elems, float4* wide,
+                         float4* __restrict__ wide4)
 {
     const uint32_t ni = n - 1;
     for (uint32_t lid = blockIdx.x * blockDim.x + threadIdx.x; lid < n; lid += gridDim.x * blockDim.x) {
         const uint32_t e = sgo[lid];
+        v3 mn, mx;
+        leaf_box(kind, e, thickness, x0, x1, elems, mn, mx);
+        if (n == 1) {
+            store_slot(wide, 0, mn, mx, 0x80000000u | e);
+            store_slot(wide, 1, mn, mx, 0x80000000u | e);
+            collapse_node(wide, 0, true, wide4);
+        } else {
+            store_slot(wide, slot[ni + lid], mn, mx, 0x80000000u | e, lid);
+        }
+    }
+}
+
+// fn_refit_tree_aabb (lbvh.cpp:702-754) without its bottom-up walk.  The walk makes every inner box the
+// union of its children's, fmin / fmax of the form `a < b ? a : b` with the left child first; over the
+// leaves of a node that is the fold of their boxes in sorted order, and since that operation is associative
+// and idempotent on everything but NaN (it keeps the rightmost of equal extremes, +0 / -0 included), any
+// split of a node's leaf range into pieces combined left to right -- overlapping pieces too -- gives the
+// same bits.  So every inner box is computed straight from its leaf range, with no serial climb:
+//   * k_refit_chunks: one block per kRefitChunk sorted leaves keeps their boxes, the prefix and suffix
+//     unions of each 32-leaf segment (warp scans) and a sparse table over the segment unions in shared
+//     memory; every inner node whose range lies in the chunk is then one segment's fold, or a suffix, at
+//     most two overlapping sparse-table entries and a prefix.  It writes the segment and chunk unions and,
+//     after a block barrier, the 4-wide records of its even-depth nodes.
+//   * k_refit_spans: one warp per node whose range crosses a chunk boundary (listed by the build): leaves
+//     of the first and last segment, segments of the first and last chunk and whole chunks in between,
+//     each piece reduced across the warp in lane order.
+//   * k_refit_span_records: the 4-wide records of the crossing nodes at even depth.
+// NaN coordinates (a diverged state, reported by the solver) may give other bits than the walk does.
+
+__device__ __forceinline__ void box_id(float (&v)[6])
+{
+    v[0] = v[1] = v[2] = __int_as_float(0x7f800000);
+    v[3] = v[4] = v[5] = __int_as_float(0xff800000);
+}
+
+// l = l (on the left) joined with r (on the right)
+__device__ __forceinline__ void box_join(float (&l)[6], const float (&r)[6])
+{
+#pragma unroll
+    for (int c = 0; c < 3; ++c) l[c] = fmn(l[c], r[c]);
+#pragma unroll
+    for (int c = 3; c < 6; ++c) l[c] = fmx(l[c], r[c]);
+}
+
+// the lanes' pieces joined in lane order (lane 0 holds the result): pieces of 1, 2, 4, ... lanes
+__device__ __forceinline__ void box_warp_fold(float (&v)[6])
+{
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        float o[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) o[c] = __shfl_down_sync(0xFFFFFFFFu, v[c], d);
+        if ((lane_id() & (2 * d - 1)) == 0) box_join(v, o);
+    }
+}
+
+__device__ __forceinline__ void box_ld(const float4* p, float (&v)[6])
+{
+    const float4 mn = __ldcg(p), mx = __ldcg(p + 1);
+    v[0] = mn.x; v[1] = mn.y; v[2] = mn.z;
+    v[3] = mx.x; v[4] = mx.y; v[5] = mx.z;
+}
+
+__global__ void __launch_bounds__(kRefitChunk) k_refit_chunks(
+    int kind, uint32_t n, const uint32_t* __restrict__ sgo, const uint32_t* __restrict__ slot,
+    const uint2* __restrict__ range, const uint8_t* __restrict__ even, const float* __restrict__ thickness,
+    const float4* __restrict__ x0, const float4* __restrict__ x1, const uint32_t* __restrict__ elems, int write_leaf,
+    float4* wide, float4* __restrict__ wide4, float4* __restrict__ seg_box, float4* __restrict__ chunk_box)
+{
+    __shared__ float s_leaf[6][kRefitChunk], s_pre[6][kRefitChunk], s_suf[6][kRefitChunk];
+    __shared__ float s_tab[kRefitLevels][6][kRefitSegs];  // s_tab[k][.][s]: segments s .. s + 2^k - 1
+    const uint32_t ni = n - 1, t = threadIdx.x, lane = t & 31u, w = t >> 5;
+    const uint32_t c0 = blockIdx.x * kRefitChunk, lid = c0 + t;
+    float b[6];
+    box_id(b);
+    if (lid < n) {
+        const uint32_t sl = slot[ni + lid];
         if (write_leaf) {
+            const uint32_t e = sgo[lid];
             v3 mn, mx;
             leaf_box(kind, e, thickness, x0, x1, elems, mn, mx);
-            if (n == 1) {
-                store_slot(wide, 0, mn, mx, 0x80000000u | e);
-                store_slot(wide, 1, mn, mx, 0x80000000u | e);
-                collapse_node(wide, 0, true, wide4);
+            store_slot(wide, sl, mn, mx, 0x80000000u | e, lid);
+            b[0] = mn.x; b[1] = mn.y; b[2] = mn.z;
+            b[3] = mx.x; b[4] = mx.y; b[5] = mx.z;
+        } else {
+            box_ld(wide + 4 * (sl >> 1) + 2 * (sl & 1u), b);
+        }
+    }
+    float pre[6], suf[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) pre[c] = suf[c] = b[c];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        float up[6], dn[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            up[c] = __shfl_up_sync(0xFFFFFFFFu, pre[c], d);
+            dn[c] = __shfl_down_sync(0xFFFFFFFFu, suf[c], d);
+        }
+        if (lane >= (uint32_t)d) {  // lanes lane - 2d + 1 .. lane - d, then this piece
+            box_join(up, pre);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) pre[c] = up[c];
+        }
+        if (lane + d < 32u) box_join(suf, dn);
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        s_leaf[c][t] = b[c];
+        s_pre[c][t] = pre[c];
+        s_suf[c][t] = suf[c];
+    }
+    if (lane == 31u) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) s_tab[0][c][w] = pre[c];
+        float4* o = seg_box + 2 * (c0 / 32u + w);
+        __stcg(o, make_float4(pre[0], pre[1], pre[2], 0.0f));
+        __stcg(o + 1, make_float4(pre[3], pre[4], pre[5], 0.0f));
+    }
+    __syncthreads();
+    if (w == 0) {
+        float v[6];
+        if (lane < kRefitSegs) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) v[c] = s_tab[0][c][lane];
+        } else {
+            box_id(v);
+        }
+        float all[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) all[c] = v[c];
+#pragma unroll
+        for (int k = 1; k < kRefitLevels; ++k) {
+            float o[6];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) o[c] = __shfl_down_sync(0xFFFFFFFFu, v[c], 1 << (k - 1));
+            box_join(v, o);  // entries whose window runs past the chunk are never read
+            if (lane < kRefitSegs) {
+#pragma unroll
+                for (int c = 0; c < 6; ++c) s_tab[k][c][lane] = v[c];
+            }
+        }
+        box_warp_fold(all);
+        if (lane == 0) {
+            __stcg(chunk_box + 2 * blockIdx.x, make_float4(all[0], all[1], all[2], 0.0f));
+            __stcg(chunk_box + 2 * blockIdx.x + 1, make_float4(all[3], all[4], all[5], 0.0f));
+        }
+    }
+    __syncthreads();
+    bool mine = false;
+    if (lid < ni) {
+        const uint2 r = __ldg(&range[lid]);
+        if (r.x >= c0 && r.y < c0 + kRefitChunk) {
+            mine = true;
+            const uint32_t la = r.x - c0, lb = r.y - c0, sa = la >> 5, sb = lb >> 5;
+            float v[6];
+            if (sa == sb) {
+                box_id(v);
+                for (uint32_t j = la; j <= lb; ++j) {
+                    float o[6];
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) o[c] = s_leaf[c][j];
+                    box_join(v, o);
+                }
             } else {
-                store_slot(wide, slot[ni + lid], mn, mx, 0x80000000u | e, lid);
+                float o[6];
+#pragma unroll
+                for (int c = 0; c < 6; ++c) v[c] = s_suf[c][la];
+                if (sb > sa + 1) {
+                    const uint32_t len = sb - sa - 1;
+                    const int k = 31 - __clz((int)len);
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) o[c] = s_tab[k][c][sa + 1];
+                    box_join(v, o);
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) o[c] = s_tab[k][c][sb - (1u << k)];
+                    box_join(v, o);
+                }
+#pragma unroll
+                for (int c = 0; c < 6; ++c) o[c] = s_pre[c][lb];
+                box_join(v, o);
+            }
+            if (lid != 0) store_slot(wide, slot[lid], mk3(v[0], v[1], v[2]), mk3(v[3], v[4], v[5]), lid, r.y);
+        }
+    }
+    __syncthreads();  // the chunk's slots are written: its nodes' children records are final
+    if (mine && even[lid]) collapse_node(wide, lid, false, wide4);
+}
+
+__global__ void __launch_bounds__(256) k_refit_spans(uint32_t n, const uint32_t* __restrict__ spans,
+                                                     const uint32_t* __restrict__ span_count,
+                                                     const uint2* __restrict__ range, const uint32_t* __restrict__ slot,
+                                                     const float4* __restrict__ seg_box,
+                                                     const float4* __restrict__ chunk_box, float4* wide)
+{
+    const uint32_t ni = n - 1, lane = lane_id();
+    const uint32_t cnt = *span_count;
+    for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < cnt; j += (gridDim.x * blockDim.x) >> 5) {
+        const uint32_t i = spans[j];
+        const uint2 r = range[i];
+        const uint32_t a = r.x, b = r.y, ca = a / kRefitChunk, cb = b / kRefitChunk, sa = a >> 5, sb = b >> 5;
+        float acc[6], v[6];
+        box_id(acc);
+        // 1: leaves a .. the end of segment sa (a full segment: chunk ca is not the last)
+        box_id(v);
+        if ((sa << 5) + lane >= a) {
+            const uint32_t sl = slot[ni + (sa << 5) + lane];
+            box_ld(wide + 4 * (sl >> 1) + 2 * (sl & 1u), v);
+        }
+        box_warp_fold(v);
+        box_join(acc, v);
+        // 2: the segments of chunk ca after sa
+        box_id(v);
+        if (sa + 1 + lane < (ca + 1) * kRefitSegs) box_ld(seg_box + 2 * (sa + 1 + lane), v);
+        box_warp_fold(v);
+        box_join(acc, v);
+        // 3: chunks ca + 1 .. cb - 1, a contiguous run per lane
+        box_id(v);
+        {
+            const uint32_t nc = cb - ca - 1, per = (nc + 31) >> 5;
+            for (uint32_t k = 0; k < per; ++k) {
+                const uint32_t c = ca + 1 + lane * per + k;
+                if (c < cb) {
+                    float o[6];
+                    box_ld(chunk_box + 2 * c, o);
+                    box_join(v, o);
+                }
             }
         }
-        if (!climb || n == 1) continue;
-        uint32_t p = parent[ni + lid];
-        for (int guard = 0;; ++guard) {
-            if (guard > 256 || p >= ni) {  // deeper than any Karras tree over 62-bit keys: links are broken
-                *healthy = 0u;
-                break;
-            }
-            // acq_rel arrival: releases this child's box to the sibling and, for the second
-            // arrival, acquires the sibling's box (no full fences)
-            if (atom_add_acq_rel_gpu(&counters[p], 1u) == 0u) break;  // first arrival: the sibling finishes
-            counters[p] = 0u;  // re-armed for the next refit (launch boundary orders it)
-            const float4* r = wide + 4 * p;
-            float4 a0 = __ldcg(r + 0), a1 = __ldcg(r + 1), b0 = __ldcg(r + 2), b1 = __ldcg(r + 3);
-            v3 mn = mk3(fmn(a0.x, b0.x), fmn(a0.y, b0.y), fmn(a0.z, b0.z));
-            v3 mx = mk3(fmx(a1.x, b1.x), fmx(a1.y, b1.y), fmx(a1.z, b1.z));
-            // p's 4-wide record: its children's records are final (their last writers arrived before us)
-            if (even[p]) collapse_node(wide, p, false, wide4);
-            if (p == 0) break;
-            const uint32_t la = __float_as_uint(a1.w), lb = __float_as_uint(b1.w);
-            store_slot(wide, slot[p], mn, mx, p, la > lb ? la : lb);
-            p = parent[p];
+        box_warp_fold(v);
+        box_join(acc, v);
+        // 4: the segments of chunk cb before sb
+        box_id(v);
+        if (cb * kRefitSegs + lane < sb) box_ld(seg_box + 2 * (cb * kRefitSegs + lane), v);
+        box_warp_fold(v);
+        box_join(acc, v);
+        // 5: leaves of segment sb up to b
+        box_id(v);
+        if ((sb << 5) + lane <= b) {
+            const uint32_t sl = slot[ni + (sb << 5) + lane];
+            box_ld(wide + 4 * (sl >> 1) + 2 * (sl & 1u), v);
         }
+        box_warp_fold(v);
+        box_join(acc, v);
+        if (lane == 0 && i != 0)
+            store_slot(wide, slot[i], mk3(acc[0], acc[1], acc[2]), mk3(acc[3], acc[4], acc[5]), i, b);
+    }
+}
+
+__global__ void k_refit_span_records(const uint32_t* __restrict__ spans, const uint32_t* __restrict__ span_count,
+                                     const uint8_t* __restrict__ even, const float4* wide, float4* __restrict__ wide4)
+{
+    const uint32_t cnt = *span_count;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
+        const uint32_t i = spans[j];
+        if (even[i]) collapse_node(wide, i, false, wide4);
     }
 }
 
@@ -704,11 +932,16 @@ extern "C" int lcs_bvh_create(int kind, uint32_t n_leaves, lcs_bvh** out)
     A(alloc(h->wide, 4 * nw));
     A(alloc(h->wide4, 8 * nw));
     A(alloc(h->even, nw));
-    A(alloc(h->counters, nw));
+    A(alloc(h->range, nw));
+    A(alloc(h->spans, nw));
+    A(alloc(h->span_count, 1));
+    const size_t chunks = (n_leaves + kRefitChunk - 1) / kRefitChunk;  // every chunk writes all its segments
+    A(alloc(h->seg_box, 2 * chunks * kRefitSegs));
+    A(alloc(h->chunk_box, 2 * chunks));
     A(alloc(h->healthy, 1));
     A(alloc(h->maxdepth, 1));
     if (e == cudaSuccess) e = cudaMemset(h->maxdepth, 0, sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMemset(h->counters, 0, sizeof(uint32_t) * nw);
+    if (e == cudaSuccess) e = cudaMemset(h->span_count, 0, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(h->wide, 0, sizeof(float4) * 4 * nw);
     if (e == cudaSuccess) e = cudaMemset(h->wide4, 0, sizeof(float4) * 8 * nw);
     if (e == cudaSuccess) e = cudaMemset(h->even, 1, nw);
@@ -727,8 +960,8 @@ extern "C" int lcs_bvh_destroy(lcs_bvh* h)
 {
     if (!h) return LCS_OK;
     void* ptrs[] = {h->centers, h->block_aabb, h->gaabb, h->m30, h->keys, h->keys_alt, h->vals, h->vals_alt,
-                    h->hist, h->ms64, h->parent, h->children, h->slot, h->wide, h->wide4, h->even, h->counters,
-                    h->healthy, h->maxdepth};
+                    h->hist, h->ms64, h->parent, h->children, h->slot, h->wide, h->wide4, h->even, h->range,
+                    h->spans, h->span_count, h->seg_box, h->chunk_box, h->healthy, h->maxdepth};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete h;
@@ -773,8 +1006,9 @@ extern "C" int lcs_bvh_construct(lcs_bvh* h, lcs_stream stream)
     lcs_count_launch();
     if (h->ni > 0) {
         const int gi = grid_for(h->ni, 256);
+        LCS_CUDA_TRY(cudaMemsetAsync(h->span_count, 0, sizeof(uint32_t), s));
         k_build_inner<<<gi, 256, 0, s>>>(h->ms64, h->sgo, h->n, h->parent, h->children, h->slot, h->wide,
-                                         h->maxdepth);
+                                         h->maxdepth, h->range, h->spans, h->span_count);
         lcs_count_launch();
         k_check<<<gi, 256, 0, s>>>(h->children, h->parent, h->ni, h->healthy);
         lcs_count_launch();
@@ -813,8 +1047,9 @@ int lcs_bvh_construct_host_sort(lcs_bvh* h, lcs_stream stream)
     lcs_count_launch();
     if (h->ni > 0) {
         const int gi = grid_for(h->ni, 256);
+        LCS_CUDA_TRY(cudaMemsetAsync(h->span_count, 0, sizeof(uint32_t), s));
         k_build_inner<<<gi, 256, 0, s>>>(h->ms64, h->sgo, h->n, h->parent, h->children, h->slot, h->wide,
-                                         h->maxdepth);
+                                         h->maxdepth, h->range, h->spans, h->span_count);
         lcs_count_launch();
         k_check<<<gi, 256, 0, s>>>(h->children, h->parent, h->ni, h->healthy);
         lcs_count_launch();
@@ -833,12 +1068,27 @@ static int leaves_refit(lcs_bvh* h, const float* thickness, const float* x0, con
         return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_update/refit: bad argument");
     if (h->n == 0) return LCS_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    k_leaves_refit<<<grid_for(h->n, 256), 256, 0, s>>>(h->kind, h->n, h->sgo, h->slot, h->parent, thickness,
-                                                       reinterpret_cast<const float4*>(x0),
-                                                       reinterpret_cast<const float4*>(x1), elems, h->wide,
-                                                       h->counters, h->healthy, write_leaf, climb, h->even,
-                                                       h->wide4);
-    lcs_count_launch();
+    const float4* px0 = reinterpret_cast<const float4*>(x0);
+    const float4* px1 = reinterpret_cast<const float4*>(x1);
+    if (climb && h->n > 1) {
+        const uint32_t chunks = (h->n + kRefitChunk - 1) / kRefitChunk;
+        k_refit_chunks<<<chunks, kRefitChunk, 0, s>>>(h->kind, h->n, h->sgo, h->slot, h->range, h->even, thickness,
+                                                      px0, px1, elems, write_leaf, h->wide, h->wide4, h->seg_box,
+                                                      h->chunk_box);
+        lcs_count_launch();
+        if (chunks > 1) {
+            k_refit_spans<<<2 * kNumSMs, 256, 0, s>>>(h->n, h->spans, h->span_count, h->range, h->slot,
+                                                            h->seg_box, h->chunk_box, h->wide);
+            lcs_count_launch();
+            k_refit_span_records<<<kNumSMs, 256, 0, s>>>(h->spans, h->span_count, h->even, h->wide,
+                                                               h->wide4);
+            lcs_count_launch();
+        }
+    } else if (write_leaf) {
+        k_leaves<<<grid_for(h->n, 256), 256, 0, s>>>(h->kind, h->n, h->sgo, h->slot, thickness, px0, px1, elems,
+                                                     h->wide, h->wide4);
+        lcs_count_launch();
+    }
     LCS_LAUNCH_CHECK();
     return LCS_OK;
 }

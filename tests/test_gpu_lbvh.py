@@ -60,6 +60,56 @@ def test_topology_bit_exact(scene, kind_name):
     np.testing.assert_array_equal(host(e["object_idx"], np.uint32), t_o.object_idx)
 
 
+def _refit_both(kind, x, x1, elems, off):
+    t_o = O.lbvh_build(kind, x, elems, x.shape[0])
+    bvh = LBVH(kind, elems.shape[0])
+    xd, ed = dev(x), dev(elems)
+    if kind == O.TREE_FACE:
+        bvh.reduce_face_tree_aabb(xd, ed)
+    else:
+        bvh.reduce_edge_tree_aabb(xd, ed)
+    bvh.construct_tree()
+    O.lbvh_refit(t_o, x, x1, elems, off)
+    bvh.update_and_refit(dev(off), xd, dev(x1), ed)
+    e = bvh.export()
+    torch.cuda.synchronize()
+    return t_o, host(e["node_aabb"])
+
+
+@pytest.mark.parametrize("m", [2, 3, 40, 511, 512, 513, 1025, 1600])
+def test_refit_bit_exact_across_chunk_sizes(m):
+    """Trees of one, two and several 512-leaf refit chunks (the refit computes each inner box from its
+    sorted leaf range, in one chunk or across chunks) against the oracle's bottom-up walk."""
+    sc, x = _scene("folded")
+    faces = np.ascontiguousarray(sc.faces[:m])
+    x1 = SC.random_motion(x, 1e-3, seed=m)
+    t_o, got = _refit_both(O.TREE_FACE, x, x1, faces, sc.offset + np.float32(1e-4))
+    np.testing.assert_array_equal(got[:, 0:3], t_o.node_aabb[:, 0:3])
+    np.testing.assert_array_equal(got[:, 4:7], t_o.node_aabb[:, 4:7])
+
+
+def test_refit_signed_zero_ties_bit_exact():
+    """Leaf boxes whose extremes tie at +0 and -0 (zero thickness, coordinates of both signs of zero): the
+    reference's union `a < b ? a : b` keeps the later of two equal values, so the node boxes' zero signs
+    depend on the order of the unions; compared as bit patterns."""
+    rng = np.random.default_rng(3)
+    g = 48
+    ii, jj = np.meshgrid(np.arange(g), np.arange(g), indexing="ij")
+    x = np.zeros((g * g, 4), np.float32)
+    x[:, 0] = np.where(rng.random(g * g) < 0.5, np.float32(0.0), np.float32(-0.0))
+    x[:, 1] = (ii.ravel() * 0.01).astype(np.float32)
+    x[:, 2] = np.where(rng.random(g * g) < 0.5, np.float32(0.0), np.float32(-0.0))
+    x[(jj.ravel() % 7) == 3, 2] = np.float32(0.01) * (jj.ravel()[(jj.ravel() % 7) == 3]).astype(np.float32)
+    idx = (ii * g + jj)
+    edges = np.concatenate([np.stack([idx[:, :-1].ravel(), idx[:, 1:].ravel()], 1),
+                            np.stack([idx[:-1, :].ravel(), idx[1:, :].ravel()], 1)]).astype(np.uint32)
+    off = np.zeros(g * g, np.float32)
+    t_o, got = _refit_both(O.TREE_EDGE, x, x.copy(), edges, off)
+    assert (np.signbit(t_o.node_aabb[:, 0:3]).any() and (~np.signbit(t_o.node_aabb[:, 0:3])).any())
+    np.testing.assert_array_equal(got[:, 0:3].view(np.uint32), t_o.node_aabb[:, 0:3].view(np.uint32))
+    np.testing.assert_array_equal(got[:, 4:7].view(np.uint32), t_o.node_aabb[:, 4:7].view(np.uint32))
+
+
 @pytest.mark.parametrize("scene", ["cloth_sphere", "folded", "tube"])
 @pytest.mark.parametrize("kind_name", ["face", "edge"])
 @pytest.mark.parametrize("fused", [False, True])
@@ -70,7 +120,7 @@ def test_refit_bit_exact(scene, kind_name, fused):
     x1d = dev(x1)
     off = dev(sc.offset + np.float32(1e-4))
     O.lbvh_refit(t_o, x, x1, getattr(sc, KINDS[kind_name][1]), sc.offset + np.float32(1e-4))
-    for _ in range(2):  # twice: the arrival counters must have reset themselves
+    for _ in range(2):  # twice: a refit over its own previous output
         if fused:
             bvh.update_and_refit(off, xd, x1d, ed)
         else:
