@@ -17,6 +17,7 @@
 #include "lbvh_common.cuh"
 #include "lcs_internal.h"
 #include "radix_sort.cuh"
+#include "scan.cuh"
 
 using namespace lcs;
 
@@ -41,7 +42,15 @@ struct lcs_bvh {
     float4* wide = nullptr;          // 4 * max(ni, 1)
     float4* wide4 = nullptr;         // 8 * max(ni, 1): 4-child records of the even-depth inner nodes
     uint8_t* even = nullptr;         // max(ni, 1): inner node at even depth (root: depth 0)
+    // the refit's tables, rebuilt with the topology (see k_eorder)
     uint2* range = nullptr;          // max(ni, 1): sorted leaf positions [first, last] under each inner node
+    uint32_t* swap_diff = nullptr;   // n + 1: +1 / -1 at the ends of each swapped node's left range
+    uint32_t* swap_cov = nullptr;    // n + 1: its exclusive prefix sum
+    uint32_t* scan_tmp = nullptr;
+    uint32_t* n_plus_1 = nullptr;    // 1: n + 1, the scan's element count
+    uint32_t* leaf_at = nullptr;     // n: sorted leaf position at each position of the union order
+    uint32_t* node_at = nullptr;     // max(ni, 1): inner node whose two children meet after each position
+    uint4* order_range = nullptr;    // max(ni, 1): {first, last} union-order positions, last sorted position
     uint32_t* spans = nullptr;       // max(ni, 1): inner nodes whose leaves lie in more than one refit chunk
     uint32_t* span_count = nullptr;  // 1
     float4* seg_box = nullptr;       // 2 per 32 sorted leaves (whole refit chunks): {min | 0}{max | 0}
@@ -151,12 +160,13 @@ constexpr int kRefitLevels = 4;                    // sparse-table levels over a
 static_assert((1u << kRefitLevels) == kRefitSegs, "one sparse-table level per doubling of the segment count");
 
 // fn_build_inner_nodes with determineRange / findSplit, lbvh.cpp:204-291, 541-596; also the
-// traversal records' child codes, the child -> parent slot map, each inner node's leaf range and the list
-// of inner nodes whose range crosses a refit chunk boundary (any order: each is refitted on its own)
+// traversal records' child codes, the child -> parent slot map, each inner node's sorted leaf range and,
+// for a node whose right child is a leaf (put first in the reference's child layout), +1 / -1 at the ends of
+// its left child's range in swap_diff (see k_eorder)
 __global__ void k_build_inner(const uint64_t* __restrict__ ms, const uint32_t* __restrict__ sgo, uint32_t n,
                               uint32_t* __restrict__ parent, uint2* __restrict__ children,
                               uint32_t* __restrict__ slot, float4* __restrict__ wide, uint32_t* __restrict__ maxdepth,
-                              uint2* __restrict__ range, uint32_t* __restrict__ spans, uint32_t* span_count)
+                              uint2* __restrict__ range, uint32_t* __restrict__ swap_diff)
 {
     const int ni = (int)n - 1;
     if (blockIdx.x == 0 && threadIdx.x == 0) *maxdepth = 0u;  // raised by k_depth_parity, launched after this
@@ -178,7 +188,6 @@ __global__ void k_build_inner(const uint64_t* __restrict__ ms, const uint32_t* _
         }
         int a = i < j ? i : j, b = i < j ? j : i;
         range[nid] = make_uint2((uint32_t)a, (uint32_t)b);
-        if ((uint32_t)a / kRefitChunk != (uint32_t)b / kRefitChunk) spans[atomicAdd(span_count, 1u)] = (uint32_t)nid;
         int split;
         {
             const uint64_t ma = ms[a], mb = ms[b];
@@ -198,7 +207,9 @@ __global__ void k_build_inner(const uint64_t* __restrict__ ms, const uint32_t* _
         }
         int cleft = (a == split) ? ni + split : split;
         int cright = (b == split + 1) ? ni + split + 1 : split + 1;
-        if (cright >= ni) {
+        if (cright >= ni) {  // the right child is the leaf b: it becomes the first child
+            atomicAdd(&swap_diff[a], 1u);
+            atomicAdd(&swap_diff[b], 0xFFFFFFFFu);
             int t = cleft;
             cleft = cright;
             cright = t;
@@ -303,6 +314,42 @@ __global__ void k_check(const uint2* __restrict__ children, const uint32_t* __re
 
 __global__ void k_set_healthy(uint32_t* healthy) { *healthy = 1u; }
 
+// The union order of the refit.  The reference's walk makes each inner box fmin / fmax of its children's in
+// the child layout's order: left then right, except where the right child is a leaf, which k_build_inner puts
+// first.  A node's box is then the fold of its leaves' boxes in the in-order sequence of the tree taken in
+// layout order, and those positions have a closed form: a leaf at sorted position p moves one place later
+// for every swapped ancestor whose left child holds it -- cov(p), the number of left ranges [a, b - 1] of
+// swapped nodes containing p, a prefix sum of swap_diff -- and the swapped leaf b of a node [a, b] goes to
+// the front of it, to a + cov(b); an inner node [a, b] holds the positions a + cov(b) .. a + cov(b) + b - a.
+// Each inner node also gets the position after which its two children meet (one node per position
+// 0 .. n - 2), so that a refit block finds the nodes of its chunk, and the nodes whose positions cross a
+// chunk boundary are listed (in any order: each is refitted on its own).
+__global__ void k_eorder(uint32_t n, const uint32_t* __restrict__ parent, const uint2* __restrict__ children,
+                         const uint2* __restrict__ range, const uint32_t* __restrict__ cov_excl,
+                         uint32_t* __restrict__ leaf_at, uint32_t* __restrict__ node_at,
+                         uint4* __restrict__ order_range, uint32_t* __restrict__ spans, uint32_t* span_count)
+{
+    const uint32_t ni = n - 1;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n + ni; k += gridDim.x * blockDim.x) {
+        if (k < n) {
+            const uint32_t P = parent[ni + k];
+            const uint2 r = range[P];
+            const bool front = children[P].x == ni + k && k == r.y;
+            const uint32_t pos = (front ? r.x : k) + cov_excl[k + 1];
+            if (pos < n) leaf_at[pos] = k;
+        } else {
+            const uint32_t i = k - n;
+            const uint2 r = range[i];
+            const uint32_t first = r.x + cov_excl[r.y + 1], last = first + (r.y - r.x);
+            const uint32_t c0 = children[i].x;
+            const uint32_t size0 = c0 >= ni ? 1u : range[c0].y - range[c0].x + 1u;
+            if (first + size0 - 1 < ni) node_at[first + size0 - 1] = i;
+            order_range[i] = make_uint4(first, last, r.y, 0u);
+            if (first / kRefitChunk != last / kRefitChunk) spans[atomicAdd(span_count, 1u)] = i;
+        }
+    }
+}
+
 // fn_update_*_tree_leave_aabb_v2 (lbvh.cpp:617-683) alone: the leaf slots (a one-leaf tree also gets its
 // 4-wide record, both of whose slots are the leaf)
 __device__ __forceinline__ void collapse_node(const float4* wide, uint32_t b, bool leaf_only, float4* wide4);
@@ -328,11 +375,12 @@ __global__ void k_leaves(int kind, uint32_t n, const uint32_t* __restrict__ sgo,
 }
 
 // fn_refit_tree_aabb (lbvh.cpp:702-754) without its bottom-up walk.  The walk makes every inner box the
-// union of its children's, fmin / fmax of the form `a < b ? a : b` with the left child first; over the
-// leaves of a node that is the fold of their boxes in sorted order, and since that operation is associative
-// and idempotent on everything but NaN (it keeps the rightmost of equal extremes, +0 / -0 included), any
-// split of a node's leaf range into pieces combined left to right -- overlapping pieces too -- gives the
-// same bits.  So every inner box is computed straight from its leaf range, with no serial climb:
+// union of its children's, fmin / fmax of the form `a < b ? a : b` in the child layout's order; over the
+// leaves of a node that is the fold of their boxes in the union order (k_eorder), and since that operation
+// is associative and idempotent on everything but NaN (it keeps the later of equal extremes, +0 / -0
+// included), any split of a node's union-order range into pieces combined in order -- overlapping pieces
+// too -- gives the same bits.  So every inner box is computed straight from its range of leaves in union
+// order, with no serial climb; "chunks" and "segments" below are runs of union-order positions:
 //   * k_refit_chunks: one block per kRefitChunk sorted leaves keeps their boxes, the prefix and suffix
 //     unions of each 32-leaf segment (warp scans) and a sparse table over the segment unions in shared
 //     memory; every inner node whose range lies in the chunk is then one segment's fold, or a suffix, at
@@ -380,17 +428,19 @@ __device__ __forceinline__ void box_ld(const float4* p, float (&v)[6])
 
 __global__ void __launch_bounds__(kRefitChunk) k_refit_chunks(
     int kind, uint32_t n, const uint32_t* __restrict__ sgo, const uint32_t* __restrict__ slot,
-    const uint2* __restrict__ range, const uint8_t* __restrict__ even, const float* __restrict__ thickness,
+    const uint32_t* __restrict__ leaf_at, const uint32_t* __restrict__ node_at,
+    const uint4* __restrict__ order_range, const uint8_t* __restrict__ even, const float* __restrict__ thickness,
     const float4* __restrict__ x0, const float4* __restrict__ x1, const uint32_t* __restrict__ elems, int write_leaf,
     float4* wide, float4* __restrict__ wide4, float4* __restrict__ seg_box, float4* __restrict__ chunk_box)
 {
     __shared__ float s_leaf[6][kRefitChunk], s_pre[6][kRefitChunk], s_suf[6][kRefitChunk];
     __shared__ float s_tab[kRefitLevels][6][kRefitSegs];  // s_tab[k][.][s]: segments s .. s + 2^k - 1
     const uint32_t ni = n - 1, t = threadIdx.x, lane = t & 31u, w = t >> 5;
-    const uint32_t c0 = blockIdx.x * kRefitChunk, lid = c0 + t;
+    const uint32_t c0 = blockIdx.x * kRefitChunk, pos = c0 + t;
     float b[6];
     box_id(b);
-    if (lid < n) {
+    if (pos < n) {
+        const uint32_t lid = __ldg(&leaf_at[pos]);
         const uint32_t sl = slot[ni + lid];
         if (write_leaf) {
             const uint32_t e = sgo[lid];
@@ -465,8 +515,10 @@ __global__ void __launch_bounds__(kRefitChunk) k_refit_chunks(
     }
     __syncthreads();
     bool mine = false;
-    if (lid < ni) {
-        const uint2 r = __ldg(&range[lid]);
+    uint32_t node = 0;
+    if (pos < ni) {
+        node = __ldg(&node_at[pos]);
+        const uint4 r = __ldg(&order_range[node]);
         if (r.x >= c0 && r.y < c0 + kRefitChunk) {
             mine = true;
             const uint32_t la = r.x - c0, lb = r.y - c0, sa = la >> 5, sb = lb >> 5;
@@ -497,16 +549,17 @@ __global__ void __launch_bounds__(kRefitChunk) k_refit_chunks(
                 for (int c = 0; c < 6; ++c) o[c] = s_pre[c][lb];
                 box_join(v, o);
             }
-            if (lid != 0) store_slot(wide, slot[lid], mk3(v[0], v[1], v[2]), mk3(v[3], v[4], v[5]), lid, r.y);
+            if (node != 0) store_slot(wide, slot[node], mk3(v[0], v[1], v[2]), mk3(v[3], v[4], v[5]), node, r.z);
         }
     }
     __syncthreads();  // the chunk's slots are written: its nodes' children records are final
-    if (mine && even[lid]) collapse_node(wide, lid, false, wide4);
+    if (mine && even[node]) collapse_node(wide, node, false, wide4);
 }
 
 __global__ void __launch_bounds__(256) k_refit_spans(uint32_t n, const uint32_t* __restrict__ spans,
                                                      const uint32_t* __restrict__ span_count,
-                                                     const uint2* __restrict__ range, const uint32_t* __restrict__ slot,
+                                                     const uint4* __restrict__ order_range,
+                                                     const uint32_t* __restrict__ leaf_at, const uint32_t* __restrict__ slot,
                                                      const float4* __restrict__ seg_box,
                                                      const float4* __restrict__ chunk_box, float4* wide)
 {
@@ -514,14 +567,14 @@ __global__ void __launch_bounds__(256) k_refit_spans(uint32_t n, const uint32_t*
     const uint32_t cnt = *span_count;
     for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < cnt; j += (gridDim.x * blockDim.x) >> 5) {
         const uint32_t i = spans[j];
-        const uint2 r = range[i];
+        const uint4 r = order_range[i];
         const uint32_t a = r.x, b = r.y, ca = a / kRefitChunk, cb = b / kRefitChunk, sa = a >> 5, sb = b >> 5;
         float acc[6], v[6];
         box_id(acc);
         // 1: leaves a .. the end of segment sa (a full segment: chunk ca is not the last)
         box_id(v);
         if ((sa << 5) + lane >= a) {
-            const uint32_t sl = slot[ni + (sa << 5) + lane];
+            const uint32_t sl = slot[ni + leaf_at[(sa << 5) + lane]];
             box_ld(wide + 4 * (sl >> 1) + 2 * (sl & 1u), v);
         }
         box_warp_fold(v);
@@ -554,13 +607,13 @@ __global__ void __launch_bounds__(256) k_refit_spans(uint32_t n, const uint32_t*
         // 5: leaves of segment sb up to b
         box_id(v);
         if ((sb << 5) + lane <= b) {
-            const uint32_t sl = slot[ni + (sb << 5) + lane];
+            const uint32_t sl = slot[ni + leaf_at[(sb << 5) + lane]];
             box_ld(wide + 4 * (sl >> 1) + 2 * (sl & 1u), v);
         }
         box_warp_fold(v);
         box_join(acc, v);
         if (lane == 0 && i != 0)
-            store_slot(wide, slot[i], mk3(acc[0], acc[1], acc[2]), mk3(acc[3], acc[4], acc[5]), i, b);
+            store_slot(wide, slot[i], mk3(acc[0], acc[1], acc[2]), mk3(acc[3], acc[4], acc[5]), i, r.z);
     }
 }
 
@@ -933,6 +986,13 @@ extern "C" int lcs_bvh_create(int kind, uint32_t n_leaves, lcs_bvh** out)
     A(alloc(h->wide4, 8 * nw));
     A(alloc(h->even, nw));
     A(alloc(h->range, nw));
+    A(alloc(h->swap_diff, (size_t)n_leaves + 1));
+    A(alloc(h->swap_cov, (size_t)n_leaves + 1));
+    A(alloc(h->scan_tmp, scan::tmp_words(n_leaves + 1)));
+    A(alloc(h->n_plus_1, 1));
+    A(alloc(h->leaf_at, n_leaves));
+    A(alloc(h->node_at, nw));
+    A(alloc(h->order_range, nw));
     A(alloc(h->spans, nw));
     A(alloc(h->span_count, 1));
     const size_t chunks = (n_leaves + kRefitChunk - 1) / kRefitChunk;  // every chunk writes all its segments
@@ -942,6 +1002,8 @@ extern "C" int lcs_bvh_create(int kind, uint32_t n_leaves, lcs_bvh** out)
     A(alloc(h->maxdepth, 1));
     if (e == cudaSuccess) e = cudaMemset(h->maxdepth, 0, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(h->span_count, 0, sizeof(uint32_t));
+    const uint32_t np1 = n_leaves + 1;
+    if (e == cudaSuccess) e = cudaMemcpy(h->n_plus_1, &np1, sizeof(uint32_t), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(h->wide, 0, sizeof(float4) * 4 * nw);
     if (e == cudaSuccess) e = cudaMemset(h->wide4, 0, sizeof(float4) * 8 * nw);
     if (e == cudaSuccess) e = cudaMemset(h->even, 1, nw);
@@ -961,7 +1023,8 @@ extern "C" int lcs_bvh_destroy(lcs_bvh* h)
     if (!h) return LCS_OK;
     void* ptrs[] = {h->centers, h->block_aabb, h->gaabb, h->m30, h->keys, h->keys_alt, h->vals, h->vals_alt,
                     h->hist, h->ms64, h->parent, h->children, h->slot, h->wide, h->wide4, h->even, h->range,
-                    h->spans, h->span_count, h->seg_box, h->chunk_box, h->healthy, h->maxdepth};
+                    h->swap_diff, h->swap_cov, h->scan_tmp, h->n_plus_1, h->leaf_at, h->node_at,
+                    h->order_range, h->spans, h->span_count, h->seg_box, h->chunk_box, h->healthy, h->maxdepth};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete h;
@@ -990,6 +1053,19 @@ extern "C" int lcs_bvh_reduce_aabb(lcs_bvh* h, const float* x, const uint32_t* e
     return LCS_OK;
 }
 
+// the refit's union-order tables of a freshly built topology (k_eorder)
+static cudaError_t union_order(lcs_bvh* h, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(h->span_count, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    scan::exclusive_u32(h->swap_diff, h->swap_cov, h->n_plus_1, h->n + 1, h->scan_tmp, s);
+    k_eorder<<<grid_for((uint64_t)h->n + h->ni, 256), 256, 0, s>>>(h->n, h->parent, h->children, h->range,
+                                                                   h->swap_cov, h->leaf_at, h->node_at,
+                                                                   h->order_range, h->spans, h->span_count);
+    lcs_count_launch();
+    return cudaGetLastError();
+}
+
 extern "C" int lcs_bvh_construct(lcs_bvh* h, lcs_stream stream)
 {
     if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_construct: null handle");
@@ -1006,14 +1082,15 @@ extern "C" int lcs_bvh_construct(lcs_bvh* h, lcs_stream stream)
     lcs_count_launch();
     if (h->ni > 0) {
         const int gi = grid_for(h->ni, 256);
-        LCS_CUDA_TRY(cudaMemsetAsync(h->span_count, 0, sizeof(uint32_t), s));
+        LCS_CUDA_TRY(cudaMemsetAsync(h->swap_diff, 0, sizeof(uint32_t) * ((size_t)h->n + 1), s));
         k_build_inner<<<gi, 256, 0, s>>>(h->ms64, h->sgo, h->n, h->parent, h->children, h->slot, h->wide,
-                                         h->maxdepth, h->range, h->spans, h->span_count);
+                                         h->maxdepth, h->range, h->swap_diff);
         lcs_count_launch();
         k_check<<<gi, 256, 0, s>>>(h->children, h->parent, h->ni, h->healthy);
         lcs_count_launch();
         k_depth_parity<<<gi, 256, 0, s>>>(h->parent, h->ni, h->even, h->maxdepth);
         lcs_count_launch();
+        LCS_CUDA_TRY(union_order(h, s));
     } else {
         cudaMemcpyAsync(h->slot, &kInvalid, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
     }
@@ -1047,14 +1124,15 @@ int lcs_bvh_construct_host_sort(lcs_bvh* h, lcs_stream stream)
     lcs_count_launch();
     if (h->ni > 0) {
         const int gi = grid_for(h->ni, 256);
-        LCS_CUDA_TRY(cudaMemsetAsync(h->span_count, 0, sizeof(uint32_t), s));
+        LCS_CUDA_TRY(cudaMemsetAsync(h->swap_diff, 0, sizeof(uint32_t) * ((size_t)h->n + 1), s));
         k_build_inner<<<gi, 256, 0, s>>>(h->ms64, h->sgo, h->n, h->parent, h->children, h->slot, h->wide,
-                                         h->maxdepth, h->range, h->spans, h->span_count);
+                                         h->maxdepth, h->range, h->swap_diff);
         lcs_count_launch();
         k_check<<<gi, 256, 0, s>>>(h->children, h->parent, h->ni, h->healthy);
         lcs_count_launch();
         k_depth_parity<<<gi, 256, 0, s>>>(h->parent, h->ni, h->even, h->maxdepth);
         lcs_count_launch();
+        LCS_CUDA_TRY(union_order(h, s));
     }
     LCS_CUDA_TRY(cudaStreamSynchronize(s));  // host buffers go out of scope
     LCS_LAUNCH_CHECK();
@@ -1072,12 +1150,14 @@ static int leaves_refit(lcs_bvh* h, const float* thickness, const float* x0, con
     const float4* px1 = reinterpret_cast<const float4*>(x1);
     if (climb && h->n > 1) {
         const uint32_t chunks = (h->n + kRefitChunk - 1) / kRefitChunk;
-        k_refit_chunks<<<chunks, kRefitChunk, 0, s>>>(h->kind, h->n, h->sgo, h->slot, h->range, h->even, thickness,
+        k_refit_chunks<<<chunks, kRefitChunk, 0, s>>>(h->kind, h->n, h->sgo, h->slot, h->leaf_at, h->node_at,
+                                                      h->order_range, h->even, thickness,
                                                       px0, px1, elems, write_leaf, h->wide, h->wide4, h->seg_box,
                                                       h->chunk_box);
         lcs_count_launch();
         if (chunks > 1) {
-            k_refit_spans<<<2 * kNumSMs, 256, 0, s>>>(h->n, h->spans, h->span_count, h->range, h->slot,
+            k_refit_spans<<<2 * kNumSMs, 256, 0, s>>>(h->n, h->spans, h->span_count, h->order_range, h->leaf_at,
+                                                      h->slot,
                                                             h->seg_box, h->chunk_box, h->wide);
             lcs_count_launch();
             k_refit_span_records<<<kNumSMs, 256, 0, s>>>(h->spans, h->span_count, h->even, h->wide,
