@@ -1156,7 +1156,10 @@ static int leaves_refit(lcs_bvh* h, const float* thickness, const float* x0, con
                                                       h->chunk_box);
         lcs_count_launch();
         if (chunks > 1) {
-            k_refit_spans<<<2 * kNumSMs, 256, 0, s>>>(h->n, h->spans, h->span_count, h->order_range, h->leaf_at,
+            // one warp per crossing node in one round: about ten crossing nodes per chunk on the tube's trees,
+            // 8 warps per block, at most the 5 blocks per SM that 44 registers a thread allow
+            const uint32_t span_blocks = 2 * chunks < 5u * kNumSMs ? 2 * chunks : 5u * kNumSMs;
+            k_refit_spans<<<span_blocks, 256, 0, s>>>(h->n, h->spans, h->span_count, h->order_range, h->leaf_at,
                                                       h->slot,
                                                             h->seg_box, h->chunk_box, h->wide);
             lcs_count_launch();
