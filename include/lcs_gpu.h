@@ -112,7 +112,8 @@ LCS_API int lcs_bvh_update_leaves(lcs_bvh* h, const float* thickness, const floa
                           const uint32_t* elems, lcs_stream stream);
 
 /* LBVH::refit (lbvh.cpp:1038-1045): the inner boxes as unions of their children's, bit for bit the
- * reference's bottom-up walk (computed from each inner node's sorted leaf range, without a serial climb). */
+ * reference's bottom-up walk (computed from each inner node's range of leaves in the walk's union order,
+ * without a serial climb; the ranges are tables lcs_bvh_construct derives from the topology it builds). */
 LCS_API int lcs_bvh_refit(lcs_bvh* h, lcs_stream stream);
 
 /* update_*_tree_leave_aabb + refit in one launch (no reference counterpart as one call). */
@@ -164,7 +165,9 @@ LCS_API int lcs_bvh_check_construction(lcs_bvh* h, lcs_stream stream);
 
 /* Device buffers of the tree in the reference's LbvhData layout (lbvh.h:79-152: sa_parrent, sa_children,
  * sa_morton_sorted, sa_sorted_get_original, sa_is_healthy), valid until the handle is destroyed.  A caller
- * that writes into them must run lcs_bvh_check_construction before any refit or query. */
+ * that writes into them must run lcs_bvh_check_construction before any refit or query.  Refit and queries
+ * follow the topology of the last lcs_bvh_construct (its traversal records and refit tables), not edits
+ * made here; rebuild to change the topology. */
 typedef struct lcs_bvh_data_view {
     uint32_t n_leaves;
     uint32_t* parent;              /* 2 n - 1 */
