@@ -53,7 +53,7 @@ struct lcs_bvh {
     uint4* order_range = nullptr;    // max(ni, 1): {first, last} union-order positions, last sorted position
     uint32_t* spans = nullptr;       // max(ni, 1): inner nodes whose leaves lie in more than one refit chunk
     uint32_t* span_count = nullptr;  // 1
-    float4* seg_box = nullptr;       // 2 per 32 sorted leaves (whole refit chunks): {min | 0}{max | 0}
+    float4* seg_box = nullptr;       // 2 per 32 union-order positions (whole refit chunks): {min | 0}{max | 0}
     float4* chunk_box = nullptr;     // 2 per refit chunk: its union
     uint32_t* healthy = nullptr;     // 1
     uint32_t* maxdepth = nullptr;    // 1: depth of the deepest inner node (root: 0), capped at 256
@@ -153,9 +153,9 @@ __global__ void k_apply_sorted(const uint32_t* __restrict__ m30s, const uint32_t
     }
 }
 
-// sorted leaves per block of the chunked refit (k_refit_chunks); a multiple of 32
+// union-order positions per block of the chunked refit (k_refit_chunks); a multiple of 32
 constexpr uint32_t kRefitChunk = 512;
-constexpr uint32_t kRefitSegs = kRefitChunk / 32;  // 32-leaf segments per chunk
+constexpr uint32_t kRefitSegs = kRefitChunk / 32;  // 32-position segments per chunk
 constexpr int kRefitLevels = 4;                    // sparse-table levels over a chunk's segments (2^4 = 16)
 static_assert((1u << kRefitLevels) == kRefitSegs, "one sparse-table level per doubling of the segment count");
 
@@ -381,12 +381,12 @@ __global__ void k_leaves(int kind, uint32_t n, const uint32_t* __restrict__ sgo,
 // included), any split of a node's union-order range into pieces combined in order -- overlapping pieces
 // too -- gives the same bits.  So every inner box is computed straight from its range of leaves in union
 // order, with no serial climb; "chunks" and "segments" below are runs of union-order positions:
-//   * k_refit_chunks: one block per kRefitChunk sorted leaves keeps their boxes, the prefix and suffix
-//     unions of each 32-leaf segment (warp scans) and a sparse table over the segment unions in shared
+//   * k_refit_chunks: one block per kRefitChunk positions keeps their leaves' boxes, the prefix and suffix
+//     unions of each 32-position segment (warp scans) and a sparse table over the segment unions in shared
 //     memory; every inner node whose range lies in the chunk is then one segment's fold, or a suffix, at
 //     most two overlapping sparse-table entries and a prefix.  It writes the segment and chunk unions and,
 //     after a block barrier, the 4-wide records of its even-depth nodes.
-//   * k_refit_spans: one warp per node whose range crosses a chunk boundary (listed by the build): leaves
+//   * k_refit_spans: one warp per node whose range crosses a chunk boundary (listed by k_eorder): leaves
 //     of the first and last segment, segments of the first and last chunk and whole chunks in between,
 //     each piece reduced across the warp in lane order.
 //   * k_refit_span_records: the 4-wide records of the crossing nodes at even depth.
