@@ -107,7 +107,8 @@ LCS_API int lcs_bvh_reduce_aabb(lcs_bvh* h, const float* x, const uint32_t* elem
 LCS_API int lcs_bvh_construct(lcs_bvh* h, lcs_stream stream);
 
 /* LBVH::update_{vert,edge,face}_tree_leave_aabb (lbvh.cpp:1001-1031): swept leaf boxes
- * [x0, x1] +- thickness of the element's first vertex. */
+ * [x0, x1] +- thickness of the element's first vertex.  This and the two refit calls below return
+ * LCS_ERR_INVALID on a non-empty tree that no lcs_bvh_construct has built yet. */
 LCS_API int lcs_bvh_update_leaves(lcs_bvh* h, const float* thickness, const float* x0, const float* x1,
                           const uint32_t* elems, lcs_stream stream);
 

@@ -57,6 +57,7 @@ struct lcs_bvh {
     float4* chunk_box = nullptr;     // 2 per refit chunk: its union
     uint32_t* healthy = nullptr;     // 1
     uint32_t* maxdepth = nullptr;    // 1: depth of the deepest inner node (root: 0), capped at 256
+    bool built = false;              // a construct has written the topology, slots and refit tables
 };
 
 namespace {
@@ -1095,6 +1096,7 @@ extern "C" int lcs_bvh_construct(lcs_bvh* h, lcs_stream stream)
         cudaMemcpyAsync(h->slot, &kInvalid, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
     }
     LCS_LAUNCH_CHECK();
+    h->built = true;
     return LCS_OK;
 }
 
@@ -1136,6 +1138,7 @@ int lcs_bvh_construct_host_sort(lcs_bvh* h, lcs_stream stream)
     }
     LCS_CUDA_TRY(cudaStreamSynchronize(s));  // host buffers go out of scope
     LCS_LAUNCH_CHECK();
+    h->built = true;
     return LCS_OK;
 }
 
@@ -1145,6 +1148,8 @@ static int leaves_refit(lcs_bvh* h, const float* thickness, const float* x0, con
     if (!h || (write_leaf && (!thickness || !x0 || !x1 || (h->kind != LCS_TREE_VERT && !elems))))
         return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_update/refit: bad argument");
     if (h->n == 0) return LCS_OK;
+    // the slots and refit tables are written by the build: before it they hold no valid indices
+    if (!h->built) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_update/refit: the tree has not been constructed");
     cudaStream_t s = (cudaStream_t)stream;
     const float4* px0 = reinterpret_cast<const float4*>(x0);
     const float4* px1 = reinterpret_cast<const float4*>(x1);

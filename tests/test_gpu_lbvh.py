@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 import torch
 
+from luisacomputesimulator_b200 import _capi as A
 from luisacomputesimulator_b200.collision import LBVH
 from oracle import oracle as O
 from tests import scenarios as SC
@@ -158,6 +159,24 @@ def test_candidate_sets_bit_exact(scene, swept):
         assert n == n_want
         got = host(pairs, np.uint32)[:n]
         np.testing.assert_array_equal(SC.sorted_pairs(got), SC.sorted_pairs(want))
+
+
+def test_update_and_refit_before_construct_is_refused():
+    """Leaf slots and refit tables come from the build: before it, update / refit are refused
+    (LCS_ERR_INVALID) instead of reading tables that hold no indices; after it they run."""
+    sc, x = _scene("folded")
+    faces = np.ascontiguousarray(sc.faces[:700])
+    bvh = LBVH(O.TREE_FACE, faces.shape[0])
+    xd, fd, off = dev(x), dev(faces), dev(sc.offset)
+    for call in (lambda: bvh.update_and_refit(off, xd, xd, fd), lambda: bvh.update_leaves(off, xd, xd, fd),
+                 bvh.refit):
+        with pytest.raises(A.LcsError, match="LCS_ERR_INVALID"):
+            call()
+    bvh.reduce_face_tree_aabb(xd, fd)
+    bvh.construct_tree()
+    bvh.update_and_refit(off, xd, xd, fd)
+    torch.cuda.synchronize()
+    assert bvh.check_health()
 
 
 def test_query_overflow_counts_without_writing_past_capacity():
