@@ -203,7 +203,7 @@ LCS_API int lcs_forest_create(int kind, uint32_t n_scenes, const uint32_t* elem_
 LCS_API int lcs_forest_destroy(lcs_forest* f);
 /* reduce_*_tree_aabb + construct_tree for every scene in one set of launches */
 LCS_API int lcs_forest_build(lcs_forest* f, const float* x, const uint32_t* elems, lcs_stream stream);
-/* update_*_tree_leave_aabb + refit for every scene */
+/* update_*_tree_leave_aabb + refit for every scene; LCS_ERR_INVALID before the first lcs_forest_build */
 LCS_API int lcs_forest_update_refit(lcs_forest* f, const float* thickness, const float* x0, const float* x1,
                                     const uint32_t* elems, lcs_stream stream);
 /* broad_phase_query_from_verts for all scenes: vertex v queries the tree of vert_scene[v] */

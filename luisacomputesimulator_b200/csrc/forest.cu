@@ -50,6 +50,7 @@ struct lcs_forest {
     uint32_t* counters = nullptr; // NI
     uint32_t* healthy = nullptr;
     uint32_t* saved_count = nullptr;  // 1: the candidate count before a tuning query (restored between trials)
+    bool built = false;               // a build has written the sorted order, topology and slots
     mutable uint32_t q_threads = 0;   // tuned threads per block of the queries (0: not tuned yet)
     mutable float q_ms = 0.0f;        // the tuned configuration's query time
 };
@@ -237,7 +238,8 @@ __device__ __forceinline__ unsigned atom_add_acq_rel_f(unsigned* p, unsigned v)
     return old;
 }
 
-// leaf update + bottom-up refit (the lbvh.cu k_leaves_refit walk; a scene's root has no parent)
+// leaf update + the reference's bottom-up refit walk (fn_refit_tree_aabb, lbvh.cpp:702-754): the second child to
+// arrive at a node unions the two boxes and goes on up; a scene's root has no parent
 __global__ void k_f_refit(int kind, uint32_t n, uint32_t NI, const uint32_t* __restrict__ sgo,
                           const uint32_t* __restrict__ slot, const uint32_t* __restrict__ parent,
                           const float* __restrict__ thickness, const float4* __restrict__ x0,
@@ -531,6 +533,7 @@ extern "C" int lcs_forest_build(lcs_forest* f, const float* x, const uint32_t* e
     k_f_check<<<gi, 256, 0, s>>>(f->children, f->parent, f->NI, f->healthy);
     lcs_count_launch();
     LCS_LAUNCH_CHECK();
+    f->built = true;
     return LCS_OK;
 }
 
@@ -538,6 +541,8 @@ extern "C" int lcs_forest_update_refit(lcs_forest* f, const float* thickness, co
                                        const uint32_t* elems, lcs_stream stream)
 {
     if (!f || !thickness || !x0 || !x1 || !elems) return lcs_fail(LCS_ERR_INVALID, "lcs_forest_update_refit: bad argument");
+    // the sorted order and the slots are written by the build: before it they hold no valid indices
+    if (!f->built) return lcs_fail(LCS_ERR_INVALID, "lcs_forest_update_refit: the forest has not been built");
     k_f_refit<<<grid_for(f->N, 256), 256, 0, (cudaStream_t)stream>>>(
         f->kind, f->N, f->NI, f->sgo, f->slot, f->parent, thickness, reinterpret_cast<const float4*>(x0),
         reinterpret_cast<const float4*>(x1), elems, f->wide, f->counters, f->healthy);

@@ -4,6 +4,7 @@ import numpy as np
 import pytest
 import torch
 
+from luisacomputesimulator_b200 import _capi as A
 from luisacomputesimulator_b200 import scenes as S
 from luisacomputesimulator_b200.collision import Forest, NarrowPhasesDetector
 from luisacomputesimulator_b200.linear import ConjugateGradientSolver, make_bsr, solve_batch
@@ -50,6 +51,18 @@ def _concat(items):
 def batch():
     items = _scenes()
     return items, _concat(items)
+
+
+def test_forest_update_before_build_is_refused(batch):
+    """A forest's sorted order and slots come from its build: an update before it is refused (LCS_ERR_INVALID)."""
+    items, c = batch
+    f = Forest(O.TREE_FACE, c["fo"], c["vo"])
+    xd, ed = dev(c["x"]), dev(c["faces"])
+    with pytest.raises(A.LcsError, match="LCS_ERR_INVALID"):
+        f.update_refit(dev(c["offset"]), xd, xd, ed)
+    f.build(xd, ed)
+    f.update_refit(dev(c["offset"]), xd, xd, ed)
+    assert f.check_health()
 
 
 @pytest.mark.parametrize("kind_name", ["face", "edge"])
