@@ -107,8 +107,8 @@ LCS_API int lcs_bvh_reduce_aabb(lcs_bvh* h, const float* x, const uint32_t* elem
 LCS_API int lcs_bvh_construct(lcs_bvh* h, lcs_stream stream);
 
 /* LBVH::update_{vert,edge,face}_tree_leave_aabb (lbvh.cpp:1001-1031): swept leaf boxes
- * [x0, x1] +- thickness of the element's first vertex.  This and the two refit calls below return
- * LCS_ERR_INVALID on a non-empty tree that no lcs_bvh_construct has built yet. */
+ * [x0, x1] +- thickness of the element's first vertex.  This, the two refit calls below, the queries and
+ * lcs_bvh_export return LCS_ERR_INVALID on a non-empty tree that no lcs_bvh_construct has built yet. */
 LCS_API int lcs_bvh_update_leaves(lcs_bvh* h, const float* thickness, const float* x0, const float* x1,
                           const uint32_t* elems, lcs_stream stream);
 
@@ -203,7 +203,8 @@ LCS_API int lcs_forest_create(int kind, uint32_t n_scenes, const uint32_t* elem_
 LCS_API int lcs_forest_destroy(lcs_forest* f);
 /* reduce_*_tree_aabb + construct_tree for every scene in one set of launches */
 LCS_API int lcs_forest_build(lcs_forest* f, const float* x, const uint32_t* elems, lcs_stream stream);
-/* update_*_tree_leave_aabb + refit for every scene; LCS_ERR_INVALID before the first lcs_forest_build */
+/* update_*_tree_leave_aabb + refit for every scene; this, the queries and lcs_forest_export_scene return
+ * LCS_ERR_INVALID before the first lcs_forest_build */
 LCS_API int lcs_forest_update_refit(lcs_forest* f, const float* thickness, const float* x0, const float* x1,
                                     const uint32_t* elems, lcs_stream stream);
 /* broad_phase_query_from_verts for all scenes: vertex v queries the tree of vert_scene[v] */

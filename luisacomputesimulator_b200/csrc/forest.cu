@@ -640,6 +640,7 @@ int lcs_forest_query_vf_capped(const lcs_forest* face_forest, const float* x0, c
         (capacity && !pairs))
         return lcs_fail(LCS_ERR_INVALID, "lcs_forest_query_vf: bad argument");
     if (n_verts == 0) return LCS_OK;
+    if (!f->built) return lcs_fail(LCS_ERR_INVALID, "lcs_forest_query_vf: the forest has not been built");
     return f_query_tuned<false>(f, n_verts, vert_scene, reinterpret_cast<const float4*>(x0),
                                 reinterpret_cast<const float4*>(x1), nullptr, d_hat, thickness,
                                 reinterpret_cast<uint2*>(pairs), capacity, d_count, nullptr, capped, only,
@@ -662,6 +663,7 @@ int lcs_forest_query_ee_capped(const lcs_forest* edge_forest, const float* x0, c
     if (!f || f->kind != LCS_TREE_EDGE || !x0 || !x1 || !edges || !d_hat || !thickness || !d_count ||
         (capacity && !pairs))
         return lcs_fail(LCS_ERR_INVALID, "lcs_forest_query_ee: bad argument");
+    if (!f->built) return lcs_fail(LCS_ERR_INVALID, "lcs_forest_query_ee: the forest has not been built");
     return f_query_tuned<true>(f, f->N, f->escene, reinterpret_cast<const float4*>(x0),
                                reinterpret_cast<const float4*>(x1), reinterpret_cast<const uint2*>(edges), d_hat,
                                thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count, f->sgo, capped, only,
@@ -683,6 +685,7 @@ extern "C" int lcs_forest_export_scene(const lcs_forest* f, uint32_t scene, uint
                                        float* node_aabb, float* global_aabb6, lcs_stream stream)
 {
     if (!f || scene >= f->S) return lcs_fail(LCS_ERR_INVALID, "lcs_forest_export_scene: bad argument");
+    if (!f->built) return lcs_fail(LCS_ERR_INVALID, "lcs_forest_export_scene: the forest has not been built");
     cudaStream_t s = (cudaStream_t)stream;
     const uint32_t n = f->h_eoff[scene + 1] - f->h_eoff[scene];
     const ForestView v{f->eoff, f->ioff, f->parent, f->slot, f->sgo, f->children, f->ms64, f->wide, f->NI};

@@ -1212,6 +1212,7 @@ int lcs_bvh_query_vf_capped(const lcs_bvh* t, const float* x0, const float* x1, 
     if (!t || t->kind != LCS_TREE_FACE || !x0 || !x1 || !d_hat || !thickness || !d_count || (capacity && !pairs))
         return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_vf: bad argument (needs a face tree)");
     if (t->n == 0 || n_verts == 0) return LCS_OK;
+    if (!t->built) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_vf: the tree has not been constructed");
     k_query<false><<<grid_for(n_verts, 128, 16), 128, 0, (cudaStream_t)stream>>>(
         t->wide4, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1), nullptr, n_verts,
         d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity, d_count, nullptr, capped, t->maxdepth);
@@ -1242,6 +1243,7 @@ int lcs_bvh_query_ee_capped(const lcs_bvh* t, const float* x0, const float* x1, 
         (capacity && !pairs))
         return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_ee: bad argument (needs an edge tree)");
     if (t->n == 0 || n_edges == 0) return LCS_OK;
+    if (!t->built) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_ee: the tree has not been constructed");
     k_query<true><<<grid_for(n_edges, 128, 16), 128, 0, (cudaStream_t)stream>>>(
         t->wide4, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
         reinterpret_cast<const uint2*>(edges), n_edges, d_hat, thickness, reinterpret_cast<uint2*>(pairs), capacity,
@@ -1273,6 +1275,7 @@ int lcs_bvh_query_ee_sym_capped(const lcs_bvh* t, const float* x0, const float* 
         !(d_hat >= 0.0f))
         return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_ee_sym: bad argument (needs an edge tree, d_hat >= 0)");
     if (t->n == 0) return LCS_OK;
+    if (!t->built) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_query_ee_sym: the tree has not been constructed");
     k_query_ee_sym<<<grid_for(t->n, 128, 16), 128, 0, (cudaStream_t)stream>>>(
         t->wide4, t->sgo, t->n, reinterpret_cast<const float4*>(x0), reinterpret_cast<const float4*>(x1),
         reinterpret_cast<const uint2*>(edges), d_hat, reinterpret_cast<uint2*>(pairs), capacity, d_count, capped,
@@ -1332,6 +1335,7 @@ extern "C" int lcs_bvh_export(const lcs_bvh* h, uint32_t* parent, uint32_t* chil
 {
     if (!h) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_export: null handle");
     if (h->n == 0) return LCS_OK;
+    if (!h->built) return lcs_fail(LCS_ERR_INVALID, "lcs_bvh_export: the tree has not been constructed");
     cudaStream_t s = (cudaStream_t)stream;
     const size_t nn = 2 * (size_t)h->n - 1;
     if (parent) LCS_CUDA_TRY(cudaMemcpyAsync(parent, h->parent, 4 * nn, cudaMemcpyDeviceToDevice, s));

@@ -54,12 +54,17 @@ def batch():
 
 
 def test_forest_update_before_build_is_refused(batch):
-    """A forest's sorted order and slots come from its build: an update before it is refused (LCS_ERR_INVALID)."""
+    """A forest's sorted order and slots come from its build: an update, query or export before it is refused
+    (LCS_ERR_INVALID)."""
     items, c = batch
     f = Forest(O.TREE_FACE, c["fo"], c["vo"])
     xd, ed = dev(c["x"]), dev(c["faces"])
-    with pytest.raises(A.LcsError, match="LCS_ERR_INVALID"):
-        f.update_refit(dev(c["offset"]), xd, xd, ed)
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    pairs = torch.zeros((1024, 2), dtype=torch.int32, device="cuda")
+    for call in (lambda: f.update_refit(dev(c["offset"]), xd, xd, ed), lambda: f.export_scene(0),
+                 lambda: f.query_vf(xd, xd, dev(c["vscene"]), dev(c["d_hat"]), dev(c["offset"]), pairs, cnt)):
+        with pytest.raises(A.LcsError, match="LCS_ERR_INVALID"):
+            call()
     f.build(xd, ed)
     f.update_refit(dev(c["offset"]), xd, xd, ed)
     assert f.check_health()

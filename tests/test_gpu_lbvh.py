@@ -162,19 +162,26 @@ def test_candidate_sets_bit_exact(scene, swept):
 
 
 def test_update_and_refit_before_construct_is_refused():
-    """Leaf slots and refit tables come from the build: before it, update / refit are refused
-    (LCS_ERR_INVALID) instead of reading tables that hold no indices; after it they run."""
+    """Leaf order, slots and refit tables come from the build: before it, update / refit / query / export
+    are refused (LCS_ERR_INVALID) instead of reading tables that hold no indices; after it they run."""
     sc, x = _scene("folded")
     faces = np.ascontiguousarray(sc.faces[:700])
+    edges = np.ascontiguousarray(sc.edges[:900])
     bvh = LBVH(O.TREE_FACE, faces.shape[0])
-    xd, fd, off = dev(x), dev(faces), dev(sc.offset)
+    ebvh = LBVH(O.TREE_EDGE, edges.shape[0])
+    xd, fd, edd, off, dh = dev(x), dev(faces), dev(edges), dev(sc.offset), dev(sc.d_hat)
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    pairs = torch.zeros((1024, 2), dtype=torch.int32, device="cuda")
     for call in (lambda: bvh.update_and_refit(off, xd, xd, fd), lambda: bvh.update_leaves(off, xd, xd, fd),
-                 bvh.refit):
+                 bvh.refit, bvh.export, lambda: bvh.broad_phase_query_from_verts(xd, xd, cnt, pairs, dh, off),
+                 lambda: ebvh.broad_phase_query_from_edges(xd, xd, edd, cnt, pairs, dh, off),
+                 lambda: ebvh.broad_phase_query_from_edges_sym(xd, xd, edd, cnt, pairs, float(sc.d_hat[0]))):
         with pytest.raises(A.LcsError, match="LCS_ERR_INVALID"):
             call()
     bvh.reduce_face_tree_aabb(xd, fd)
     bvh.construct_tree()
     bvh.update_and_refit(off, xd, xd, fd)
+    bvh.broad_phase_query_from_verts(xd, xd, cnt, pairs, dh, off)
     torch.cuda.synchronize()
     assert bvh.check_health()
 
